@@ -1,0 +1,357 @@
+#!/usr/bin/env python
+"""Throughput benchmark: molecule-steps/s of the particle engine on B200.
+
+Workload (one GPU): the scale-up configuration - periodic cube of side 1000,
+10^7 molecules uniform at random (45% A, 45% B, 10% C), A+B->C kf=0.05,
+C->A+B kr=0.1, 0->A at 1e-4 per unit volume per unit time, D = 1, 1, 0.5,
+dt = 0.01.  A step is one simulated time step over all molecules.
+
+  value     device time of K steps (graph replays), inputs resident in HBM
+  e2e       the same work through the libsmoldyn C API with host buffers:
+            upload of the molecules from host memory, K smolRunTimeStep calls
+            each followed by a per-species smolGetMoleculeCount read-back
+  roofline  the dominant kernel's algorithmic bytes per launch / its average
+            CUDA-event duration, against the measured HBM copy bandwidth
+  cpu_baseline  the reference Smoldyn binary (compiled from the reference's
+            sources by oracle/Makefile) on a bounded sample of the same
+            workload on this host's cores
+
+With --impl reference the reference CPU engine itself is timed (all host
+cores, one independent process per core).  Under torchrun each rank runs an
+independent replica (the workload shards as independent replicas; no data
+collective) and rank 0 prints the job total over the slowest rank's time.
+"""
+import argparse
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "molecule-steps/s"
+L_SIDE = 1000.0
+N_MOL = 10_000_000
+FRAC = (0.45, 0.45, 0.10)
+DIFC = (1.0, 1.0, 0.5)
+KF, KR, K0 = 0.05, 0.1, 1e-4
+DT = 0.01
+# algorithmic bytes per molecule-step: read 16 B (position + packed species/state)
+# and write 16 B in box order in the fused move/rebin pass, read 16 B again in
+# the pair search
+ALG_BYTES_PER_MOLSTEP = 48
+# per-kernel algorithmic bytes per molecule
+KERNEL_BYTES = {"k_advance_count": 16, "k_advance_scatter": 32, "k_pairs": 16}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                      "--format=csv,noheader,nounits", "-lms", "100"],
+                                     stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_sim(sb, n_mol, side, seed):
+    s = sb.Sim(3, (0, 0, 0), (side, side, side))
+    for nm, d in zip(("A", "B", "C"), DIFC):
+        s.add_species(nm, d)
+    for d in range(3):
+        s.boundary(d, -1, "p")
+    s.set_times(0, 1e9, DT)
+    s.seed(seed)
+    s.add_reaction("fwd", "A", "B", ["C"], KF)
+    s.add_reaction("rev", "C", None, ["A", "B"], KR)
+    s.add_reaction("birth", None, None, ["A"], K0)
+    counts = [int(round(n_mol * f)) for f in FRAC]
+    counts[0] += n_mol - sum(counts)
+    for nm, c in zip(("A", "B", "C"), counts):
+        s.add_molecules(nm, c)
+    return s
+
+
+def reference_config(path, n_mol, side, steps, seed):
+    counts = [int(round(n_mol * f)) for f in FRAC]
+    with open(path, "w") as f:
+        f.write("dim 3\nspecies A B C\n")
+        for nm, d in zip(("A", "B", "C"), DIFC):
+            f.write("difc %s %g\n" % (nm, d))
+        for d in range(3):
+            f.write("boundaries %d 0 %.10g p\n" % (d, side))
+        f.write("time_start 0\ntime_stop %.10g\ntime_step %g\nrandom_seed %d\n" % (steps * DT, DT, seed))
+        f.write("reaction fwd A + B -> C %g\nreaction rev C -> A + B %g\nreaction birth 0 -> A %g\n" % (KF, KR, K0))
+        for nm, c in zip(("A", "B", "C"), counts):
+            f.write("mol %d %s u u u\n" % (c, nm))
+        f.write("end_file\n")
+
+
+def time_reference_sample(n_mol, steps_lo, steps_hi, procs, seed0=1):
+    """Per-step wall time of the reference binary on a same-density sample,
+    from the difference of two runs (so setup is excluded)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "smoldyn")
+    if not os.path.exists(exe):
+        return None, "reference binary not built (make -C oracle ref)"
+    side = L_SIDE * (n_mol / N_MOL) ** (1.0 / 3.0)
+    tmp = tempfile.mkdtemp(prefix="smolref_")
+    try:
+        walls = {}
+        for steps in (steps_lo, steps_hi):
+            cfgs = []
+            for p in range(procs):
+                c = os.path.join(tmp, "s%d_%d.txt" % (steps, p))
+                reference_config(c, n_mol, side, steps, seed0 + p)
+                cfgs.append(c)
+            t0 = time.perf_counter()
+            ps = [subprocess.Popen([exe, c, "-qt"], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, cwd=tmp)
+                  for c in cfgs]
+            rcs = [p.wait() for p in ps]
+            walls[steps] = time.perf_counter() - t0
+            if any(rcs):
+                return None, "reference exited with %s" % rcs
+        per_step = (walls[steps_hi] - walls[steps_lo]) / (steps_hi - steps_lo)
+        return dict(per_step_s=per_step, side=side, n_mol=n_mol, procs=procs, walls=walls), None
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    procs = os.cpu_count() or 1
+    n_s = args.ref_sample
+    res, why = time_reference_sample(n_s, 2, 2 + max(1, args.steps), procs)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": why}))
+        return 0
+    value = procs * n_s / res["per_step_s"]
+    sample = ("%d independent reference processes, each %d molecules in a periodic cube of side %.1f (the "
+              "workload's density and rates), per-step time from runs of 2 and %d steps" %
+              (procs, n_s, res["side"], 2 + max(1, args.steps)))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["per_step_s"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": workload_config(args),
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": procs, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def workload_config(args):
+    return {"workload": "scale-up: periodic cube 1000, 1e7 molecules (45% A, 45% B, 10% C), A+B->C 0.05, "
+                        "C->A+B 0.1, 0->A 1e-4, D=1,1,0.5, dt=0.01",
+            "molecules": N_MOL, "box": L_SIDE, "dt": DT, "l2": "inputs larger than L2 (>=240 MB per buffer)",
+            "parallelism": "replicas" if args.gpus > 1 else "single"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--ref-sample", type=int, default=100000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    import smoldyn_b200 as sb
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # ---- device-resident throughput
+    s = build_sim(sb, N_MOL, L_SIDE, 1 + rank)
+    s.update()
+    stream = torch.cuda.Stream()
+    s.set_stream(stream.cuda_stream)
+    s.run_steps(args.warmup)
+    s.synchronize()
+    n0 = s.total()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    l0 = s.launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    s.run_steps(args.steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = s.launches() - l0
+    barrier()
+    ck = clocks.stop()
+    n1 = s.total()
+    mol_steps = 0.5 * (n0 + n1) * args.steps
+    t_s = ms / 1e3
+    if dist is not None:
+        tt = torch.tensor([t_s, mol_steps], device="cuda", dtype=torch.float64)
+        tmax = tt[:1].clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        tsum = tt[1:].clone()
+        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+        t_s, mol_steps = float(tmax.item()), float(tsum.item())
+    value = mol_steps / t_s
+
+    # ---- per-kernel breakdown (events between launches) for the roofline
+    prof = s.profile_steps(max(4, min(20, args.steps)))
+    s.synchronize()
+    nprof = max(4, min(20, args.steps))
+    tot_ms = sum(v[0] for v in prof.values())
+    top = max(prof.items(), key=lambda kv: kv[1][0])
+    hbm, peak_kind = peaks()
+    nmol_avg = 0.5 * (n0 + n1)
+    roof = None
+    if top[0] in KERNEL_BYTES:
+        per_launch_ms = top[1][0] / top[1][1]
+        bytes_launch = KERNEL_BYTES[top[0]] * nmol_avg
+        achieved = bytes_launch / (per_launch_ms / 1e3) / 1e9
+        roof = {"bound": "hbm", "kernel": top[0], "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
+                "alg_bytes_per_molecule": KERNEL_BYTES[top[0]]}
+    step_frac = (ALG_BYTES_PER_MOLSTEP * value / (world if world > 1 else 1)) / (hbm * 1e9)
+    kernels = {k: {"ms_per_step": v[0] / nprof, "share": v[0] / tot_ms} for k, v in prof.items()}
+    s.close()
+    torch.cuda.synchronize()
+
+    # ---- end to end through the C API with host buffers
+    s2 = build_sim(sb, N_MOL, L_SIDE, 101 + rank)
+    pos, sp, sn = s2.molecules()  # host arrays (pending molecules)
+    pos = np.ascontiguousarray(pos)
+    sp = np.ascontiguousarray(sp)
+    s2.update()
+    s2.run_steps(args.warmup)
+    s2.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    s2.set_molecules(pos, sp)
+    names = [b"A", b"B", b"C"]
+    for _ in range(args.steps):
+        s2.lib.smolRunTimeStep(s2.ptr)
+        for nm in names:
+            s2.lib.smolGetMoleculeCount(s2.ptr, nm, 0)
+    e2e_s = time.perf_counter() - t0
+    e2e_molsteps = len(sp) * args.steps
+    if dist is not None:
+        tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+        e2e_molsteps *= world
+    e2e = {"value": e2e_molsteps / e2e_s, "unit": METRIC,
+           "h2d_bytes_per_step": int((pos.nbytes + sp.nbytes) / args.steps),
+           "d2h_bytes_per_step": 3 * 8 * 3,
+           "note": "includes the host->device upload of all molecules (amortised over the steps) and a "
+                   "per-step species-count read-back"}
+    s2.close()
+
+    # ---- CPU baseline (rank 0, single GPU run only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        n_s = args.ref_sample
+        res, why = time_reference_sample(n_s, 2, 12, 1)
+        if res is not None:
+            cpu = {"value": n_s / res["per_step_s"], "unit": METRIC, "cores": 1, "kind": "reference",
+                   "sample": "reference smoldyn binary, %d molecules in a periodic cube of side %.1f (same density "
+                             "and rates), per-step time from runs of 2 and 12 steps" % (n_s, res["side"])}
+        else:
+            cpu = {"value": None, "unit": METRIC, "cores": 1, "kind": "reference", "sample": why}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_s * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(args), "e2e": e2e, "gpu_launches": int(launches),
+            "roofline": roof, "step_roofline_frac": step_frac, "kernels": kernels, "cpu_baseline": cpu,
+            "clocks": ck,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,188 @@
+/* smoldyn_b200.h -- C ABI of libsmoldyn_b200.so.
+ *
+ * Part 1 is a drop-in subset of Smoldyn's public C API
+ * (source/Smoldyn/libsmoldyn.h): a program written against libsmoldyn that
+ * uses only these calls links against libsmoldyn_b200.so unchanged and runs
+ * Smoldyn's per-timestep particle engine (diffusion, walls, sphere/rectangle
+ * surfaces, virtual-box binning, zeroth/first/second-order reactions and
+ * product placement) on one NVIDIA B200.  Enum values equal the reference's
+ * (smoldyn.h:251-512, libsmoldyn.h:13-26).  simptr is opaque here: callers that
+ * read simstruct fields directly are not supported.
+ *
+ * Part 2 (smolgpu*) holds entry points with no libsmoldyn counterpart:
+ * ensembles of independent replicates in one engine, state transfer, the
+ * deterministic (injected-displacement) mode, the FP64 radius solver on the
+ * device, the surrogate network, and timing hooks.
+ *
+ * Every function returns (or records) a status in the reference's ErrorCode
+ * convention: 0 = ok, negative = notify/warning/error; the last error is kept
+ * per process and read with smolGetError (libsmoldyn.cpp:23-37 behaviour).
+ */
+#ifndef SMOLDYN_B200_H
+#define SMOLDYN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- enums (values as in the reference) ---------------------------------- */
+enum ErrorCode { /* libsmoldyn.h:13-26 */
+  ECok = 0, ECnotify = -1, ECwarning = -2, ECnonexist = -3, ECall = -4, ECmissing = -5,
+  ECbounds = -6, ECsyntax = -7, ECerror = -8, ECmemory = -9, ECbug = -10, ECsame = -11,
+  ECwildcard = -12
+};
+enum MolecState { /* smoldyn.h:251 */
+  MSsoln, MSfront, MSback, MSup, MSdown, MSbsoln, MSall, MSnone, MSsome
+};
+enum RevParam { /* smoldyn.h:358 */
+  RPnone, RPirrev, RPconfspread, RPbounce, RPpgem, RPpgemmax, RPpgemmaxw, RPratio, RPunbindrad,
+  RPpgem2, RPpgemmax2, RPratio2, RPoffset, RPfixed
+};
+enum PanelFace { PFfront, PFback, PFnone, PFboth };                         /* smoldyn.h:484 */
+enum PanelShape { PSrect, PStri, PSsph, PScyl, PShemi, PSdisk, PSall, PSnone }; /* smoldyn.h:491 */
+enum SrfAction {                                                             /* smoldyn.h:503 */
+  SAreflect, SAtrans, SAabsorb, SAjump, SAport, SAmult, SAno, SAnone, SAadsorb, SArevdes,
+  SAirrevdes, SAflip
+};
+
+typedef struct smolb_sim *simptr; /* opaque; replaces struct simstruct* (smoldyn.h:1027) */
+
+/* ==== Part 1: libsmoldyn subset ========================================== */
+
+/* libsmoldyn.h:37 */
+double smolGetVersion(void);
+/* libsmoldyn.h:44-46: last error, process-global as in the reference */
+enum ErrorCode smolGetError(char *errorfunction, char *errorstring, int clearerror);
+void smolClearError(void);
+void smolSetDebugMode(int debugmode);
+char *smolErrorCodeToString(enum ErrorCode erc, char *string);
+
+/* libsmoldyn.h:49-55 */
+simptr smolNewSim(int dim, double *lowbounds, double *highbounds);
+enum ErrorCode smolUpdateSim(simptr sim);
+enum ErrorCode smolRunTimeStep(simptr sim);
+enum ErrorCode smolRunSim(simptr sim);
+enum ErrorCode smolRunSimUntil(simptr sim, double breaktime);
+enum ErrorCode smolFreeSim(simptr sim);
+
+/* libsmoldyn.h:59-61: text configuration (statement subset, see the reader) */
+simptr smolPrepareSimFromFile(const char *filepath, const char *filename, const char *flags);
+enum ErrorCode smolLoadSimFromFile(const char *filepath, const char *filename, simptr *simpointer,
+                                   const char *flags);
+enum ErrorCode smolReadConfigString(simptr sim, const char *statement, char *parameters);
+
+/* libsmoldyn.h:65-72 */
+enum ErrorCode smolSetSimTimes(simptr sim, double timestart, double timestop, double timestep);
+enum ErrorCode smolSetTimeStart(simptr sim, double timestart);
+enum ErrorCode smolSetTimeStop(simptr sim, double timestop);
+enum ErrorCode smolSetTimeNow(simptr sim, double timenow);
+enum ErrorCode smolSetTimeStep(simptr sim, double timestep);
+enum ErrorCode smolSetRandomSeed(simptr sim, long int seed);
+/* method "molperbox" or "boxsize" (libsmoldyn.h:72) */
+enum ErrorCode smolSetPartitions(simptr sim, const char *method, double value);
+
+/* libsmoldyn.h:94: output data tables filled by runtime commands */
+enum ErrorCode smolAddOutputData(simptr sim, char *dataname);
+enum ErrorCode smolAddCommandFromString(simptr sim, char *string);
+enum ErrorCode smolGetOutputData(simptr sim, char *dataname, int *nrow, int *ncol, double **array,
+                                 int erase);
+
+/* libsmoldyn.h:99-117 */
+enum ErrorCode smolAddSpecies(simptr sim, const char *species, const char *mollist);
+int smolGetSpeciesIndex(simptr sim, const char *species);
+int smolGetSpeciesIndexNT(simptr sim, const char *species);
+void smolGetSpeciesName(simptr sim, int speciesindex, char *species);
+enum ErrorCode smolSetSpeciesMobility(simptr sim, const char *species, enum MolecState state,
+                                      double difc, double *drift, double *difmatrix);
+enum ErrorCode smolSetMaxMolecules(simptr sim, int maxmolecules);
+enum ErrorCode smolAddSolutionMolecules(simptr sim, const char *species, int number,
+                                        double *lowposition, double *highposition);
+int smolGetMoleculeCount(simptr sim, const char *species, enum MolecState state);
+
+/* libsmoldyn.h:122-130: walls and the sphere/rectangle surface subset */
+enum ErrorCode smolSetBoundaryType(simptr sim, int dimension, int highside, char type);
+enum ErrorCode smolAddSurface(simptr sim, const char *surface);
+enum ErrorCode smolSetSurfaceAction(simptr sim, const char *surface, enum PanelFace face,
+                                    const char *species, enum MolecState state,
+                                    enum SrfAction action, const char *newspecies);
+enum ErrorCode smolAddPanel(simptr sim, const char *surface, enum PanelShape panelshape,
+                            const char *panel, const char *axisstring, double *params);
+
+/* libsmoldyn.h:152-158 */
+enum ErrorCode smolAddReaction(simptr sim, const char *reaction, const char *reactant1,
+                               enum MolecState rstate1, const char *reactant2,
+                               enum MolecState rstate2, int nproduct, const char **productspecies,
+                               enum MolecState *productstates, double rate);
+int smolGetReactionIndex(simptr sim, int *orderptr, const char *reaction);
+enum ErrorCode smolSetReactionRate(simptr sim, const char *reaction, double rate, int type);
+enum ErrorCode smolSetReactionProducts(simptr sim, const char *reaction, enum RevParam method,
+                                       double parameter, const char *product, double *position);
+/* Alias: smolAddReaction with a non-empty reactant2 (no separate entry exists
+ * in the reference; provided because callers look for this name). */
+enum ErrorCode smolAddBimolecularReaction(simptr sim, const char *reaction, const char *reactant1,
+                                          const char *reactant2, int nproduct,
+                                          const char **productspecies, double rate);
+
+/* ==== Part 2: smolgpu extensions ========================================= */
+
+/* Derived reaction parameters after smolUpdateSim (reference fields
+ * rxn->bindrad2, rxn->unbindrad, rxn->prob; smolreact.c:1307-1577). */
+enum ErrorCode smolgpuGetReactionParams(simptr sim, const char *reaction, double *bindrad,
+                                        double *unbindrad, double *prob);
+/* Simulated time and step counter. */
+double smolgpuGetTime(simptr sim);
+long long smolgpuGetStepCount(simptr sim);
+/* Number of live molecules (all species). */
+long long smolgpuGetTotalMolecules(simptr sim);
+/* Copy all molecules to host arrays (pos: 3*n doubles, absolute coordinates;
+ * species: n ints; serno: n uint64).  *n is in: capacity, out: count. */
+enum ErrorCode smolgpuGetMolecules(simptr sim, long long *n, double *pos, int *species,
+                                   uint64_t *serno);
+/* Replace the molecule set (absolute coordinates; serno 0 = assign). */
+enum ErrorCode smolgpuSetMolecules(simptr sim, long long n, const double *pos, const int *species,
+                                   const uint64_t *serno);
+/* Event counters since start: [0]=wall [1]=rxn0 [2]=rxn1 [3]=rxn2 [4]=unresolved
+ * pair conflicts [5]=multi-candidate molecules [6]=capacity overflows. */
+enum ErrorCode smolgpuGetEventCounts(simptr sim, long long counts[8]);
+
+/* Deterministic mode: while set, the next smolRunTimeStep uses displacement
+ * (dx,dy,dz) = disp[3*k..3*k+2] for the molecule whose serno equals sernos[k]
+ * instead of drawing Gaussian steps (molecules not listed do not move), and
+ * every first-order / pair coin uses 0 (always fires when allowed).  n=0 clears. */
+enum ErrorCode smolgpuSetInjectedDisplacements(simptr sim, long long n, const uint64_t *sernos,
+                                               const double *disp);
+
+/* Device stream the engine launches on (a cudaStream_t passed as void*); NULL
+ * = the engine's own stream.  Lets a caller time launches with its own events. */
+enum ErrorCode smolgpuSetStream(simptr sim, void *stream);
+/* Number of engine kernel launches issued since the sim was created. */
+long long smolgpuGetLaunchCount(simptr sim);
+/* Advance n time steps with no runtime commands (the hot loop of smolRunSim,
+ * smolsim.cpp:2755, as one replayed CUDA graph of two steps per launch). */
+enum ErrorCode smolgpuRunSteps(simptr sim, long long nsteps);
+/* Advance n steps launching kernels one by one and timing each with CUDA
+ * events.  On return names[k*32..] holds kernel k's name, ms[k] its summed
+ * device time and launches[k] its launch count, for k < *nkernels (in: array
+ * capacity, out: number of kernels). */
+enum ErrorCode smolgpuProfileSteps(simptr sim, long long nsteps, int *nkernels, char *names, double *ms,
+                                   long long *launches);
+/* Synchronise the engine's stream. */
+enum ErrorCode smolgpuSynchronize(simptr sim);
+
+/* FP64 radius solver, batched on the device (rxnparam.c:558-716 on the GPU).
+ * mode 0: bindingradius(rate[i], dt, difc[i], b[i], rel) -> out[i]
+ * mode 1: unbindingradius(pgem=rate[i], dt, difc[i], a=b[i]) -> out[i]
+ * Host arrays of length n. */
+enum ErrorCode smolgpuSolveRadii(int mode, long long n, const double *rate, double dt,
+                                 const double *difc, const double *b, int rel, double *out);
+/* Same solver on the host CPU (product path used by parameter updates). */
+double smolgpuBindingRadiusHost(double rate, double dt, double difc, double b, int rel);
+double smolgpuUnbindingRadiusHost(double pgem, double dt, double difc, double a);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SMOLDYN_B200_H */

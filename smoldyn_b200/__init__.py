@@ -1,0 +1,307 @@
+"""Python access to libsmoldyn_b200.so, the B200 particle engine behind a
+libsmoldyn-compatible C API (Smoldyn source/Smoldyn/libsmoldyn.h).
+
+This module only loads the in-tree shared library and declares the C
+prototypes for ctypes; every computation happens in the library.  Importing
+fails loudly if the library has not been built (run
+``python -m smoldyn_b200.build``).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsmoldyn_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "smoldyn_b200.h")
+
+# enum values (libsmoldyn.h:13-26, smoldyn.h:251-512)
+ECok, ECnotify, ECwarning, ECnonexist, ECall, ECmissing, ECbounds, ECsyntax, ECerror, ECmemory, \
+    ECbug, ECsame, ECwildcard = 0, -1, -2, -3, -4, -5, -6, -7, -8, -9, -10, -11, -12
+MSsoln, MSfront, MSback, MSup, MSdown, MSbsoln, MSall, MSnone, MSsome = range(9)
+(RPnone, RPirrev, RPconfspread, RPbounce, RPpgem, RPpgemmax, RPpgemmaxw, RPratio, RPunbindrad,
+ RPpgem2, RPpgemmax2, RPratio2, RPoffset, RPfixed) = range(14)
+PFfront, PFback, PFnone, PFboth = range(4)
+PSrect, PStri, PSsph, PScyl, PShemi, PSdisk, PSall, PSnone = range(8)
+SAreflect, SAtrans, SAabsorb = 0, 1, 2
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_u64p = C.POINTER(C.c_uint64)
+_vp = C.c_void_p
+_sim = C.c_void_p
+
+# name -> (restype, argtypes); every function declared in include/smoldyn_b200.h
+PROTOTYPES = {
+    "smolGetVersion": (C.c_double, []),
+    "smolGetError": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int]),
+    "smolClearError": (None, []),
+    "smolSetDebugMode": (None, [C.c_int]),
+    "smolErrorCodeToString": (C.c_char_p, [C.c_int, C.c_char_p]),
+    "smolNewSim": (_sim, [C.c_int, _dp, _dp]),
+    "smolUpdateSim": (C.c_int, [_sim]),
+    "smolRunTimeStep": (C.c_int, [_sim]),
+    "smolRunSim": (C.c_int, [_sim]),
+    "smolRunSimUntil": (C.c_int, [_sim, C.c_double]),
+    "smolFreeSim": (C.c_int, [_sim]),
+    "smolPrepareSimFromFile": (_sim, [C.c_char_p, C.c_char_p, C.c_char_p]),
+    "smolLoadSimFromFile": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(_sim), C.c_char_p]),
+    "smolReadConfigString": (C.c_int, [_sim, C.c_char_p, C.c_char_p]),
+    "smolSetSimTimes": (C.c_int, [_sim, C.c_double, C.c_double, C.c_double]),
+    "smolSetTimeStart": (C.c_int, [_sim, C.c_double]),
+    "smolSetTimeStop": (C.c_int, [_sim, C.c_double]),
+    "smolSetTimeNow": (C.c_int, [_sim, C.c_double]),
+    "smolSetTimeStep": (C.c_int, [_sim, C.c_double]),
+    "smolSetRandomSeed": (C.c_int, [_sim, C.c_long]),
+    "smolSetPartitions": (C.c_int, [_sim, C.c_char_p, C.c_double]),
+    "smolAddOutputData": (C.c_int, [_sim, C.c_char_p]),
+    "smolAddCommandFromString": (C.c_int, [_sim, C.c_char_p]),
+    "smolGetOutputData": (C.c_int, [_sim, C.c_char_p, _ip, _ip, C.POINTER(_dp), C.c_int]),
+    "smolAddSpecies": (C.c_int, [_sim, C.c_char_p, C.c_char_p]),
+    "smolGetSpeciesIndex": (C.c_int, [_sim, C.c_char_p]),
+    "smolGetSpeciesIndexNT": (C.c_int, [_sim, C.c_char_p]),
+    "smolGetSpeciesName": (None, [_sim, C.c_int, C.c_char_p]),
+    "smolSetSpeciesMobility": (C.c_int, [_sim, C.c_char_p, C.c_int, C.c_double, _dp, _dp]),
+    "smolSetMaxMolecules": (C.c_int, [_sim, C.c_int]),
+    "smolAddSolutionMolecules": (C.c_int, [_sim, C.c_char_p, C.c_int, _dp, _dp]),
+    "smolGetMoleculeCount": (C.c_int, [_sim, C.c_char_p, C.c_int]),
+    "smolSetBoundaryType": (C.c_int, [_sim, C.c_int, C.c_int, C.c_char]),
+    "smolAddSurface": (C.c_int, [_sim, C.c_char_p]),
+    "smolSetSurfaceAction": (C.c_int, [_sim, C.c_char_p, C.c_int, C.c_char_p, C.c_int, C.c_int, C.c_char_p]),
+    "smolAddPanel": (C.c_int, [_sim, C.c_char_p, C.c_int, C.c_char_p, C.c_char_p, _dp]),
+    "smolAddReaction": (C.c_int, [_sim, C.c_char_p, C.c_char_p, C.c_int, C.c_char_p, C.c_int, C.c_int,
+                                  C.POINTER(C.c_char_p), _ip, C.c_double]),
+    "smolGetReactionIndex": (C.c_int, [_sim, _ip, C.c_char_p]),
+    "smolSetReactionRate": (C.c_int, [_sim, C.c_char_p, C.c_double, C.c_int]),
+    "smolSetReactionProducts": (C.c_int, [_sim, C.c_char_p, C.c_int, C.c_double, C.c_char_p, _dp]),
+    "smolAddBimolecularReaction": (C.c_int, [_sim, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int,
+                                             C.POINTER(C.c_char_p), C.c_double]),
+    "smolgpuGetReactionParams": (C.c_int, [_sim, C.c_char_p, _dp, _dp, _dp]),
+    "smolgpuGetTime": (C.c_double, [_sim]),
+    "smolgpuGetStepCount": (C.c_longlong, [_sim]),
+    "smolgpuGetTotalMolecules": (C.c_longlong, [_sim]),
+    "smolgpuGetMolecules": (C.c_int, [_sim, C.POINTER(C.c_longlong), _dp, _ip, _u64p]),
+    "smolgpuSetMolecules": (C.c_int, [_sim, C.c_longlong, _dp, _ip, _u64p]),
+    "smolgpuGetEventCounts": (C.c_int, [_sim, C.POINTER(C.c_longlong)]),
+    "smolgpuSetInjectedDisplacements": (C.c_int, [_sim, C.c_longlong, _u64p, _dp]),
+    "smolgpuSetStream": (C.c_int, [_sim, _vp]),
+    "smolgpuGetLaunchCount": (C.c_longlong, [_sim]),
+    "smolgpuSynchronize": (C.c_int, [_sim]),
+    "smolgpuRunSteps": (C.c_int, [_sim, C.c_longlong]),
+    "smolgpuProfileSteps": (C.c_int, [_sim, C.c_longlong, _ip, C.c_char_p, _dp, C.POINTER(C.c_longlong)]),
+    "smolgpuSolveRadii": (C.c_int, [C.c_int, C.c_longlong, _dp, C.c_double, _dp, _dp, C.c_int, _dp]),
+    "smolgpuBindingRadiusHost": (C.c_double, [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int]),
+    "smolgpuUnbindingRadiusHost": (C.c_double, [C.c_double, C.c_double, C.c_double, C.c_double]),
+}
+
+_lib = None
+
+
+def load():
+    """Load libsmoldyn_b200.so and declare its prototypes (raises if absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("libsmoldyn_b200.so is not built; run python -m smoldyn_b200.build")
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in PROTOTYPES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def dptr(a):
+    return a.ctypes.data_as(_dp)
+
+
+def last_error():
+    lib = load()
+    fn = C.create_string_buffer(256)
+    msg = C.create_string_buffer(256)
+    code = lib.smolGetError(fn, msg, 0)
+    return code, fn.value.decode(), msg.value.decode()
+
+
+def check(code):
+    if code < ECwarning:
+        c, fn, msg = last_error()
+        raise RuntimeError("libsmoldyn_b200 error %d in %s: %s" % (code, fn, msg))
+    return code
+
+
+class Sim:
+    """Thin owner of a simptr with helpers; all methods call the C ABI."""
+
+    def __init__(self, dim=3, low=(0, 0, 0), high=(1, 1, 1), ptr=None):
+        self.lib = load()
+        if ptr is None:
+            lo = np.asarray(low[:dim], dtype=np.float64)
+            hi = np.asarray(high[:dim], dtype=np.float64)
+            ptr = self.lib.smolNewSim(dim, dptr(lo), dptr(hi))
+            if not ptr:
+                check(ECerror)
+        self.ptr = ptr
+        self.dim = dim
+
+    @classmethod
+    def from_file(cls, path, flags=""):
+        lib = load()
+        d, f = os.path.split(os.path.abspath(path))
+        ptr = lib.smolPrepareSimFromFile(d.encode(), f.encode(), flags.encode())
+        if not ptr:
+            check(ECerror)
+        return cls(ptr=ptr)
+
+    def close(self):
+        if self.ptr:
+            self.lib.smolFreeSim(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- configuration
+    def statement(self, word, params=""):
+        return check(self.lib.smolReadConfigString(self.ptr, word.encode(), params.encode()))
+
+    def set_times(self, t0, t1, dt):
+        return check(self.lib.smolSetSimTimes(self.ptr, t0, t1, dt))
+
+    def seed(self, s):
+        return check(self.lib.smolSetRandomSeed(self.ptr, s))
+
+    def add_species(self, name, difc=None):
+        check(self.lib.smolAddSpecies(self.ptr, name.encode(), None))
+        if difc is not None:
+            check(self.lib.smolSetSpeciesMobility(self.ptr, name.encode(), MSsoln, float(difc), None, None))
+
+    def boundary(self, dim, high, t):
+        return check(self.lib.smolSetBoundaryType(self.ptr, dim, high, t.encode()))
+
+    def add_molecules(self, species, n, low=None, high=None):
+        lo = None if low is None else dptr(np.asarray(low, dtype=np.float64))
+        hi = None if high is None else dptr(np.asarray(high, dtype=np.float64))
+        return check(self.lib.smolAddSolutionMolecules(self.ptr, species.encode(), int(n), lo, hi))
+
+    def add_reaction(self, name, r1, r2, products, rate):
+        arr = (C.c_char_p * max(1, len(products)))(*[p.encode() for p in products])
+        return check(self.lib.smolAddReaction(self.ptr, name.encode(), r1.encode() if r1 else None, MSsoln,
+                                              r2.encode() if r2 else None, MSsoln, len(products), arr, None,
+                                              float(rate)))
+
+    def set_products(self, rxn, method, param):
+        return check(self.lib.smolSetReactionProducts(self.ptr, rxn.encode(), method, float(param), None, None))
+
+    def update(self):
+        return check(self.lib.smolUpdateSim(self.ptr))
+
+    def run_step(self):
+        return check(self.lib.smolRunTimeStep(self.ptr))
+
+    def run(self):
+        return check(self.lib.smolRunSim(self.ptr))
+
+    def run_until(self, t):
+        return check(self.lib.smolRunSimUntil(self.ptr, float(t)))
+
+    def run_steps(self, n):
+        return check(self.lib.smolgpuRunSteps(self.ptr, int(n)))
+
+    def profile_steps(self, n):
+        cap = 64
+        nk = C.c_int(cap)
+        names = C.create_string_buffer(32 * cap)
+        ms = np.zeros(cap)
+        launches = np.zeros(cap, dtype=np.int64)
+        check(self.lib.smolgpuProfileSteps(self.ptr, int(n), C.byref(nk), names, dptr(ms),
+                                           launches.ctypes.data_as(C.POINTER(C.c_longlong))))
+        out = {}
+        for k in range(min(nk.value, cap)):
+            nm = names.raw[32 * k:32 * k + 32].split(b"\0")[0].decode()
+            out[nm] = (float(ms[k]), int(launches[k]))
+        return out
+
+    def set_stream(self, stream_ptr):
+        return check(self.lib.smolgpuSetStream(self.ptr, C.c_void_p(stream_ptr)))
+
+    def synchronize(self):
+        return check(self.lib.smolgpuSynchronize(self.ptr))
+
+    def launches(self):
+        return self.lib.smolgpuGetLaunchCount(self.ptr)
+
+    # ---- state
+    def count(self, species="all"):
+        n = self.lib.smolGetMoleculeCount(self.ptr, species.encode(), MSsoln)
+        check(n if n < 0 else 0)
+        return n
+
+    def total(self):
+        return self.lib.smolgpuGetTotalMolecules(self.ptr)
+
+    def time(self):
+        return self.lib.smolgpuGetTime(self.ptr)
+
+    def molecules(self):
+        n = C.c_longlong(0)
+        check(self.lib.smolgpuGetMolecules(self.ptr, C.byref(n), None, None, None))
+        cnt = n.value
+        pos = np.zeros((max(cnt, 1), 3), dtype=np.float64)
+        sp = np.zeros(max(cnt, 1), dtype=np.int32)
+        sn = np.zeros(max(cnt, 1), dtype=np.uint64)
+        n = C.c_longlong(max(cnt, 1))
+        check(self.lib.smolgpuGetMolecules(self.ptr, C.byref(n), dptr(pos), sp.ctypes.data_as(_ip),
+                                           sn.ctypes.data_as(_u64p)))
+        k = n.value
+        return pos[:k], sp[:k], sn[:k]
+
+    def set_molecules(self, pos, species, serno=None):
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        species = np.ascontiguousarray(species, dtype=np.int32)
+        sp = serno
+        if serno is not None:
+            sp = np.ascontiguousarray(serno, dtype=np.uint64).ctypes.data_as(_u64p)
+        return check(self.lib.smolgpuSetMolecules(self.ptr, len(species), dptr(pos),
+                                                  species.ctypes.data_as(_ip), sp))
+
+    def inject(self, sernos, disp4):
+        sernos = np.ascontiguousarray(sernos, dtype=np.uint64)
+        disp4 = np.ascontiguousarray(disp4, dtype=np.float64)
+        return check(self.lib.smolgpuSetInjectedDisplacements(self.ptr, len(sernos),
+                                                              sernos.ctypes.data_as(_u64p), dptr(disp4)))
+
+    def events(self):
+        a = (C.c_longlong * 8)()
+        check(self.lib.smolgpuGetEventCounts(self.ptr, a))
+        return list(a)
+
+    def reaction_params(self, rxn):
+        b, u, p = C.c_double(), C.c_double(), C.c_double()
+        check(self.lib.smolgpuGetReactionParams(self.ptr, rxn.encode(), C.byref(b), C.byref(u), C.byref(p)))
+        return b.value, u.value, p.value
+
+    def output_data(self, name, erase=False):
+        nr, nc = C.c_int(), C.c_int()
+        arr = _dp()
+        check(self.lib.smolGetOutputData(self.ptr, name.encode(), C.byref(nr), C.byref(nc), C.byref(arr),
+                                         int(erase)))
+        out = np.ctypeslib.as_array(arr, shape=(nr.value * nc.value,)).copy().reshape(nr.value, nc.value) \
+            if nr.value * nc.value else np.zeros((0, nc.value))
+        C.CDLL(None).free(arr)
+        return out
+
+
+def solve_radii_device(mode, rate, dt, difc, b, rel=0):
+    lib = load()
+    rate = np.ascontiguousarray(rate, dtype=np.float64)
+    difc = np.ascontiguousarray(difc, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    out = np.zeros_like(rate)
+    check(lib.smolgpuSolveRadii(mode, len(rate), dptr(rate), dt, dptr(difc), dptr(b), rel, dptr(out)))
+    return out

@@ -1,0 +1,798 @@
+// libsmoldyn-compatible C API (source/Smoldyn/libsmoldyn.h subset) over the
+// B200 engine, plus the smolgpu* extensions.  Error reporting follows
+// libsmoldyn.cpp:23-37: every failing call records (function, code, message)
+// in process-global state read by smolGetError.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/smoldyn_b200.h"
+#include "engine.h"
+#include "rxnparam.cuh"
+#include "sim.h"
+
+struct smolb_sim {
+  smolb::Sim s;
+};
+
+using smolb::Sim;
+
+namespace {
+std::mutex g_err_mu;
+ErrorCode g_errcode = ECok;
+std::string g_errfunc, g_errstr;
+int g_debug = 0;
+
+ErrorCode set_error(const char *func, ErrorCode code, const std::string &msg) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  g_errcode = code;
+  g_errfunc = func;
+  g_errstr = msg;
+  if (g_debug && code < ECwarning) fprintf(stderr, "libsmoldyn_b200 %s: %s\n", func, msg.c_str());
+  return code;
+}
+
+ErrorCode from_rc(int rc) {
+  if (rc >= 0) return ECok;
+  if (rc < ECwildcard) return ECerror;
+  return (ErrorCode)rc;
+}
+
+#define LCHECK(cond, code, msg)                    \
+  do {                                             \
+    if (!(cond)) return set_error(__func__, code, msg); \
+  } while (0)
+
+long long total_pending(const Sim &s) { return (long long)s.pend_sp.size(); }
+
+// Download molecules from the engine into the pending lists (before a rebuild).
+int pull_molecules(Sim &s, std::string *err) {
+  if (!s.eng || !s.started) return 0;
+  std::vector<double> pos;
+  std::vector<int> sp, rep;
+  std::vector<uint64_t> serno;
+  int rc = s.eng->get_molecules(&pos, &sp, &rep, &serno, err);
+  if (rc) return rc;
+  s.pend_pos = pos;
+  s.pend_sp = sp;
+  s.started = false;
+  return 0;
+}
+
+// simupdate equivalent: derive parameters, (re)build the engine, upload molecules.
+ErrorCode update_sim(Sim &s, const char *func) {
+  std::string err;
+  if (!s.need_update && !s.need_rebuild && s.eng) return ECok;
+  if (s.dt <= 0) return set_error(func, ECerror, "time step must be > 0");
+  if (s.need_rebuild && s.eng && s.started) {
+    if (pull_molecules(s, &err)) return set_error(func, ECerror, err);
+  }
+  int rc = smolb::derive_reaction_params(s, &err);
+  if (rc) return set_error(func, ECerror, err);
+  smolb::NetSpec net;
+  smolb::RepSpec rep;
+  rc = smolb::build_engine_specs(s, &net, &rep, &err);
+  if (rc) return set_error(func, from_rc(rc), err);
+  if (s.need_rebuild || !s.eng) {
+    long long n = total_pending(s);
+    long long cap = s.max_mol > 0 ? s.max_mol : std::max<long long>(2 * n + 4096, n + (1 << 20));
+    if (!s.eng) s.eng.reset(new smolb::Engine());
+    rc = s.eng->init(net, {rep}, s.dt, (uint64_t)s.seed, cap, &err);
+    if (rc) { s.eng.reset(); return set_error(func, from_rc(rc), err); }
+    rc = s.eng->set_molecules(n, s.pend_pos.data(), s.pend_sp.data(), nullptr, nullptr, &err);
+    if (rc) { s.eng.reset(); return set_error(func, from_rc(rc), err); }
+    s.pend_pos.clear();
+    s.pend_sp.clear();
+    s.started = true;
+  } else {
+    rc = s.eng->update_reps({rep}, &err);
+    if (rc) return set_error(func, from_rc(rc), err);
+  }
+  s.need_update = s.need_rebuild = false;
+  return ECok;
+}
+
+void record_molcount(Sim &s, const std::string &dataname) {
+  std::vector<long long> counts;
+  std::string err;
+  std::vector<double> row;
+  row.push_back(s.time);
+  if (s.eng && s.started && !s.eng->species_counts(&counts, &err)) {
+    for (size_t i = 1; i < s.species.size(); ++i) row.push_back((double)counts[i]);
+  } else {
+    std::vector<long long> c(s.species.size(), 0);
+    for (int sp : s.pend_sp) c[sp]++;
+    for (size_t i = 1; i < s.species.size(); ++i) row.push_back((double)c[i]);
+  }
+  s.outdata[dataname].push_back(row);
+}
+
+// runtime commands (smolcmd.c docommand subset: molcount)
+void do_commands(Sim &s, bool at_start) {
+  for (smolb::Command &c : s.cmds) {
+    bool run = false;
+    if (c.type == 'b') run = at_start;
+    else if (c.type == 'a' || c.type == 'e') run = false;
+    else if (c.type == 'E') run = true;
+    else if (c.type == 'N' || c.type == 'n') run = (s.steps % std::max<long long>(1, c.every)) == 0;
+    else if (c.type == 'i') {
+      if (s.time + 1e-12 >= c.next && s.time <= c.off + 1e-12 && s.time + 1e-12 >= c.on) {
+        run = true;
+        c.next = std::max(c.next, c.on) + c.dt;
+      }
+    }
+    if (!run) continue;
+    char name[256] = {0}, arg[256] = {0};
+    if (sscanf(c.text.c_str(), "%255s %255s", name, arg) < 1) continue;
+    if (!strcmp(name, "molcount")) record_molcount(s, arg[0] ? arg : "molcount");
+  }
+}
+
+void do_end_commands(Sim &s) {
+  for (smolb::Command &c : s.cmds) {
+    if (c.type != 'a' && c.type != 'e') continue;
+    char name[256] = {0}, arg[256] = {0};
+    if (sscanf(c.text.c_str(), "%255s %255s", name, arg) < 1) continue;
+    if (!strcmp(name, "molcount")) record_molcount(s, arg[0] ? arg : "molcount");
+  }
+}
+
+bool has_step_commands(const Sim &s) {
+  for (const smolb::Command &c : s.cmds)
+    if (c.type == 'E' || c.type == 'N' || c.type == 'n' || c.type == 'i') return true;
+  return false;
+}
+
+// Run steps until time >= stop (smolsimulate loop, smolsim.cpp:2747-2760).
+ErrorCode run_until(Sim &s, double stop, const char *func, bool one_step) {
+  ErrorCode ec = update_sim(s, func);
+  if (ec != ECok) return ec;
+  std::string err;
+  if (s.steps == 0 && !one_step) do_commands(s, true);
+  if (s.steps == 0 && one_step && s.time == s.tstart) do_commands(s, true);
+  const bool percmd = has_step_commands(s);
+  long long n = 0;
+  double t = s.time;
+  if (one_step) n = 1;
+  else
+    while (t < stop) { t += s.dt; ++n; }
+  if (!percmd) {
+    if (n > 0 && s.eng->run(n, &err)) return set_error(func, ECerror, err);
+    for (long long k = 0; k < n; ++k) { s.time += s.dt; s.steps++; }
+  } else {
+    for (long long k = 0; k < n; ++k) {
+      if (s.eng->run(1, &err)) return set_error(func, ECerror, err);
+      s.time += s.dt;
+      s.steps++;
+      do_commands(s, false);
+    }
+  }
+  const int st = s.eng->status_flags();
+  if (st) return set_error(func, ECerror, "engine capacity exceeded (status flags " + std::to_string(st) + ")");
+  if (s.time >= s.tstop) {
+    do_end_commands(s);
+    return set_error(func, ECnotify, "Simulation complete");
+  }
+  return ECok;
+}
+}  // namespace
+
+extern "C" {
+
+double smolGetVersion(void) { return 2.76; }
+
+enum ErrorCode smolGetError(char *errorfunction, char *errorstring, int clearerror) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  const ErrorCode c = g_errcode;
+  if (errorfunction) { strncpy(errorfunction, g_errfunc.c_str(), 255); errorfunction[255] = 0; }
+  if (errorstring) { strncpy(errorstring, g_errstr.c_str(), 255); errorstring[255] = 0; }
+  if (clearerror) { g_errcode = ECok; g_errfunc.clear(); g_errstr.clear(); }
+  return c;
+}
+
+void smolClearError(void) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  g_errcode = ECok;
+  g_errfunc.clear();
+  g_errstr.clear();
+}
+
+void smolSetDebugMode(int debugmode) { g_debug = debugmode; }
+
+char *smolErrorCodeToString(enum ErrorCode erc, char *string) {
+  static const char *names[] = {"ok", "notify", "warning", "nonexistant", "all", "missing", "bounds",
+                                "syntax", "error", "memory", "bug", "same", "wildcard"};
+  const int k = -(int)erc;
+  strcpy(string, (k >= 0 && k <= 12) ? names[k] : "unknown");
+  return string;
+}
+
+simptr smolNewSim(int dim, double *lowbounds, double *highbounds) {
+  if (dim < 1 || dim > 3) { set_error(__func__, ECbounds, "dim must be 1..3"); return nullptr; }
+  if (!lowbounds || !highbounds) { set_error(__func__, ECmissing, "missing bounds"); return nullptr; }
+  for (int d = 0; d < dim; ++d)
+    if (!(lowbounds[d] < highbounds[d])) { set_error(__func__, ECbounds, "lowbounds must be < highbounds"); return nullptr; }
+  simptr sim = new smolb_sim();
+  sim->s.dim = dim;
+  for (int d = 0; d < dim; ++d) {
+    sim->s.lo[d] = lowbounds[d];
+    sim->s.hi[d] = highbounds[d];
+  }
+  return sim;
+}
+
+enum ErrorCode smolUpdateSim(simptr sim) {
+  LCHECK(sim, ECmissing, "missing sim");
+  return update_sim(sim->s, __func__);
+}
+
+enum ErrorCode smolRunTimeStep(simptr sim) {
+  LCHECK(sim, ECmissing, "missing sim");
+  return run_until(sim->s, sim->s.time + sim->s.dt / 2, __func__, true);
+}
+
+enum ErrorCode smolRunSim(simptr sim) {
+  LCHECK(sim, ECmissing, "missing sim");
+  ErrorCode e = run_until(sim->s, sim->s.tstop, __func__, false);
+  return e == ECnotify ? ECok : e;
+}
+
+enum ErrorCode smolRunSimUntil(simptr sim, double breaktime) {
+  LCHECK(sim, ECmissing, "missing sim");
+  ErrorCode e = run_until(sim->s, std::min(breaktime, sim->s.tstop), __func__, false);
+  return e == ECnotify ? ECok : e;
+}
+
+enum ErrorCode smolFreeSim(simptr sim) {
+  delete sim;
+  return ECok;
+}
+
+simptr smolPrepareSimFromFile(const char *filepath, const char *filename, const char *flags) {
+  simptr sim = nullptr;
+  if (smolLoadSimFromFile(filepath, filename, &sim, flags) != ECok) return nullptr;
+  if (smolUpdateSim(sim) != ECok) { delete sim; return nullptr; }
+  return sim;
+}
+
+enum ErrorCode smolLoadSimFromFile(const char *filepath, const char *filename, simptr *simpointer,
+                                   const char *flags) {
+  LCHECK(filename && simpointer, ECmissing, "missing filename or sim pointer");
+  bool fresh = (*simpointer == nullptr);
+  if (fresh) *simpointer = new smolb_sim();
+  Sim &s = (*simpointer)->s;
+  if (flags) s.flags = flags;
+  std::string err;
+  int rc = smolb::load_config_file(s, filepath ? filepath : "", filename, &err);
+  if (rc) {
+    if (fresh) { delete *simpointer; *simpointer = nullptr; }
+    return set_error(__func__, from_rc(rc), err);
+  }
+  return ECok;
+}
+
+enum ErrorCode smolReadConfigString(simptr sim, const char *statement, char *parameters) {
+  LCHECK(sim && statement, ECmissing, "missing sim or statement");
+  std::string err;
+  int rc = smolb::read_config_statement(sim->s, statement, parameters ? parameters : "", &err);
+  if (rc) return set_error(__func__, from_rc(rc), err);
+  return ECok;
+}
+
+enum ErrorCode smolSetSimTimes(simptr sim, double timestart, double timestop, double timestep) {
+  LCHECK(sim, ECmissing, "missing sim");
+  LCHECK(timestep > 0, ECbounds, "timestep must be > 0");
+  sim->s.tstart = sim->s.time = timestart;
+  sim->s.tstop = timestop;
+  if (sim->s.dt != timestep) sim->s.need_update = sim->s.need_rebuild = true;
+  sim->s.dt = timestep;
+  return ECok;
+}
+enum ErrorCode smolSetTimeStart(simptr sim, double t) { LCHECK(sim, ECmissing, "missing sim"); sim->s.tstart = t; return ECok; }
+enum ErrorCode smolSetTimeStop(simptr sim, double t) { LCHECK(sim, ECmissing, "missing sim"); sim->s.tstop = t; return ECok; }
+enum ErrorCode smolSetTimeNow(simptr sim, double t) { LCHECK(sim, ECmissing, "missing sim"); sim->s.time = t; return ECok; }
+enum ErrorCode smolSetTimeStep(simptr sim, double t) {
+  LCHECK(sim, ECmissing, "missing sim");
+  LCHECK(t > 0, ECbounds, "timestep must be > 0");
+  sim->s.dt = t;
+  sim->s.need_update = sim->s.need_rebuild = true;
+  return ECok;
+}
+enum ErrorCode smolSetRandomSeed(simptr sim, long int seed) {
+  LCHECK(sim, ECmissing, "missing sim");
+  sim->s.seed = seed;
+  sim->s.host_rng = (uint64_t)seed * 0x9E3779B97F4A7C15ull + 0x2545F4914F6CDD1Dull;
+  sim->s.need_rebuild = true;
+  return ECok;
+}
+enum ErrorCode smolSetPartitions(simptr sim, const char *method, double value) {
+  LCHECK(sim && method, ECmissing, "missing sim or method");
+  if (!strcmp(method, "molperbox")) { sim->s.molperbox = value; sim->s.boxsize = -1; }
+  else if (!strcmp(method, "boxsize")) { sim->s.boxsize = value; sim->s.molperbox = -1; }
+  else return set_error(__func__, ECsyntax, "method must be molperbox or boxsize");
+  sim->s.need_rebuild = true;
+  return ECok;
+}
+
+enum ErrorCode smolAddOutputData(simptr sim, char *dataname) {
+  LCHECK(sim && dataname, ECmissing, "missing sim or name");
+  sim->s.outdata[dataname];
+  return ECok;
+}
+
+enum ErrorCode smolAddCommandFromString(simptr sim, char *string) {
+  LCHECK(sim && string, ECmissing, "missing sim or string");
+  std::string err;
+  int rc = smolb::read_config_statement(sim->s, "cmd", string, &err);
+  if (rc) return set_error(__func__, from_rc(rc), err);
+  return ECok;
+}
+
+enum ErrorCode smolGetOutputData(simptr sim, char *dataname, int *nrow, int *ncol, double **array, int erase) {
+  LCHECK(sim && dataname && nrow && ncol && array, ECmissing, "missing argument");
+  auto it = sim->s.outdata.find(dataname);
+  LCHECK(it != sim->s.outdata.end(), ECnonexist, "no such output data");
+  const auto &rows = it->second;
+  *nrow = (int)rows.size();
+  *ncol = rows.empty() ? 0 : (int)rows[0].size();
+  double *a = (double *)calloc((size_t)(*nrow) * (*ncol) + 1, sizeof(double));
+  LCHECK(a, ECmemory, "out of memory");
+  for (int r = 0; r < *nrow; ++r)
+    for (int c = 0; c < *ncol && c < (int)rows[r].size(); ++c) a[r * (*ncol) + c] = rows[r][c];
+  *array = a;
+  if (erase) it->second.clear();
+  return ECok;
+}
+
+enum ErrorCode smolAddSpecies(simptr sim, const char *species, const char *mollist) {
+  (void)mollist;
+  LCHECK(sim && species, ECmissing, "missing sim or species");
+  LCHECK(sim->s.species_index(species) < 0, ECsame, "species already exists");
+  LCHECK((int)sim->s.species.size() < smolb::kMaxSpecies, ECbounds, "too many species (max 31)");
+  sim->s.species.push_back(smolb::SpeciesDef{species});
+  sim->s.need_update = sim->s.need_rebuild = true;
+  return ECok;
+}
+
+int smolGetSpeciesIndex(simptr sim, const char *species) {
+  const int i = smolGetSpeciesIndexNT(sim, species);
+  if (i < 0) set_error(__func__, ECnonexist, "species not found");
+  return i;
+}
+
+int smolGetSpeciesIndexNT(simptr sim, const char *species) {
+  if (!sim || !species) return (int)ECmissing;
+  if (!strcmp(species, "all")) return (int)ECall;
+  const int i = sim->s.species_index(species);
+  return i < 0 ? (int)ECnonexist : i;
+}
+
+void smolGetSpeciesName(simptr sim, int speciesindex, char *species) {
+  if (!sim || !species) return;
+  if (speciesindex < 0 || speciesindex >= (int)sim->s.species.size()) { species[0] = 0; return; }
+  strcpy(species, sim->s.species[speciesindex].name.c_str());
+}
+
+enum ErrorCode smolSetSpeciesMobility(simptr sim, const char *species, enum MolecState state, double difc,
+                                      double *drift, double *difmatrix) {
+  LCHECK(sim && species, ECmissing, "missing sim or species");
+  LCHECK(state == MSsoln || state == MSall, ECbounds, "only solution-state species are supported");
+  LCHECK(!difmatrix, ECbounds, "anisotropic diffusion is not supported by the GPU engine");
+  LCHECK(difc >= 0, ECbounds, "difc must be >= 0");
+  std::vector<int> ids;
+  if (!strcmp(species, "all")) for (size_t i = 1; i < sim->s.species.size(); ++i) ids.push_back((int)i);
+  else {
+    const int i = sim->s.species_index(species);
+    LCHECK(i > 0, ECnonexist, "species not found");
+    ids.push_back(i);
+  }
+  for (int i : ids) {
+    sim->s.species[i].difc = difc;
+    if (drift) for (int d = 0; d < sim->s.dim; ++d) sim->s.species[i].drift[d] = drift[d];
+  }
+  sim->s.need_update = true;
+  return ECok;
+}
+
+enum ErrorCode smolSetMaxMolecules(simptr sim, int maxmolecules) {
+  LCHECK(sim, ECmissing, "missing sim");
+  LCHECK(maxmolecules > 0, ECbounds, "maxmolecules must be > 0");
+  sim->s.max_mol = maxmolecules;
+  sim->s.need_rebuild = true;
+  return ECok;
+}
+
+enum ErrorCode smolAddSolutionMolecules(simptr sim, const char *species, int number, double *lowposition,
+                                        double *highposition) {
+  LCHECK(sim && species, ECmissing, "missing sim or species");
+  LCHECK(number >= 0, ECbounds, "number must be >= 0");
+  Sim &s = sim->s;
+  const int i = s.species_index(species);
+  LCHECK(i > 0, ECnonexist, "species not found");
+  std::string err;
+  if (s.eng && s.started) {
+    if (pull_molecules(s, &err)) return set_error(__func__, ECerror, err);
+  }
+  for (int k = 0; k < number; ++k) {
+    for (int d = 0; d < 3; ++d) {
+      double x = 0;
+      if (d < s.dim) {
+        const double lo = lowposition ? lowposition[d] : s.lo[d];
+        const double hi = highposition ? highposition[d] : s.hi[d];
+        x = (lo == hi) ? lo : lo + s.rand_u01() * (hi - lo);
+      }
+      s.pend_pos.push_back(x);
+    }
+    s.pend_sp.push_back(i);
+  }
+  s.need_rebuild = true;
+  return ECok;
+}
+
+int smolGetMoleculeCount(simptr sim, const char *species, enum MolecState state) {
+  (void)state;
+  if (!sim || !species) return (int)set_error(__func__, ECmissing, "missing sim or species");
+  Sim &s = sim->s;
+  int idx = -1;
+  if (strcmp(species, "all")) {
+    idx = s.species_index(species);
+    if (idx < 0) return (int)set_error(__func__, ECnonexist, "species not found");
+  }
+  long long n = 0;
+  if (s.eng && s.started && !s.need_rebuild) {
+    std::vector<long long> c;
+    std::string err;
+    if (s.eng->species_counts(&c, &err)) return (int)set_error(__func__, ECerror, err);
+    for (size_t i = 1; i < s.species.size(); ++i)
+      if (idx < 0 || (int)i == idx) n += c[i];
+  } else {
+    for (int sp : s.pend_sp)
+      if (idx < 0 || sp == idx) n++;
+  }
+  return (int)n;
+}
+
+enum ErrorCode smolSetBoundaryType(simptr sim, int dimension, int highside, char type) {
+  LCHECK(sim, ECmissing, "missing sim");
+  LCHECK(dimension >= -1 && dimension < sim->s.dim, ECbounds, "dimension out of range");
+  LCHECK(highside >= -1 && highside <= 1, ECbounds, "highside must be -1, 0 or 1");
+  LCHECK(type == 'r' || type == 'p' || type == 'a' || type == 't', ECsyntax, "type must be r, p, a or t");
+  for (int d = 0; d < sim->s.dim && d < 3; ++d) {
+    if (dimension >= 0 && d != dimension) continue;
+    for (int side = 0; side < 2; ++side)
+      if (highside < 0 || side == highside) sim->s.btype[d][side] = type;
+  }
+  sim->s.need_rebuild = true;
+  return ECok;
+}
+
+enum ErrorCode smolAddSurface(simptr sim, const char *surface) {
+  LCHECK(sim && surface, ECmissing, "missing sim or surface");
+  for (const smolb::SurfaceDef &sf : sim->s.surfaces) LCHECK(sf.name != surface, ECsame, "surface exists");
+  smolb::SurfaceDef sf;
+  sf.name = surface;
+  sim->s.surfaces.push_back(sf);
+  sim->s.need_rebuild = true;
+  return ECok;
+}
+
+enum ErrorCode smolSetSurfaceAction(simptr sim, const char *surface, enum PanelFace face, const char *species,
+                                    enum MolecState state, enum SrfAction action, const char *newspecies) {
+  (void)state;
+  LCHECK(sim && surface && species, ECmissing, "missing argument");
+  LCHECK(!newspecies || !newspecies[0], ECbounds, "species conversion at surfaces is not supported");
+  int a;
+  if (action == SAreflect) a = 0;
+  else if (action == SAtrans) a = 1;
+  else if (action == SAabsorb) a = 2;
+  else return set_error(__func__, ECbounds, "surface action not supported by the GPU engine");
+  smolb::SurfaceDef *sf = nullptr;
+  for (smolb::SurfaceDef &x : sim->s.surfaces)
+    if (x.name == surface) sf = &x;
+  LCHECK(sf, ECnonexist, "surface not found");
+  const bool f = (face == PFfront || face == PFboth), b = (face == PFback || face == PFboth);
+  if (!strcmp(species, "all")) {
+    if (f) { sf->act_front = a; sf->absorb_front = sf->trans_front = sf->refl_front = 0; }
+    if (b) { sf->act_back = a; sf->absorb_back = sf->trans_back = sf->refl_back = 0; }
+  } else {
+    const int i = sim->s.species_index(species);
+    LCHECK(i > 0, ECnonexist, "species not found");
+    const uint32_t bit = 1u << i;
+    auto apply = [&](uint32_t &abs, uint32_t &tr, uint32_t &rf) {
+      abs &= ~bit; tr &= ~bit; rf &= ~bit;
+      if (a == 2) abs |= bit; else if (a == 1) tr |= bit; else rf |= bit;
+    };
+    if (f) apply(sf->absorb_front, sf->trans_front, sf->refl_front);
+    if (b) apply(sf->absorb_back, sf->trans_back, sf->refl_back);
+  }
+  sim->s.need_rebuild = true;
+  return ECok;
+}
+
+enum ErrorCode smolAddPanel(simptr sim, const char *surface, enum PanelShape panelshape, const char *panel,
+                            const char *axisstring, double *params) {
+  (void)panel;
+  LCHECK(sim && surface && params, ECmissing, "missing argument");
+  smolb::SurfaceDef *sf = nullptr;
+  for (smolb::SurfaceDef &x : sim->s.surfaces)
+    if (x.name == surface) sf = &x;
+  LCHECK(sf, ECnonexist, "surface not found");
+  LCHECK((int)sf->panels.size() < smolb::kMaxPanels, ECbounds, "too many panels");
+  smolb::PanelSpec p{};
+  p.front_sign = 1;
+  if (panelshape == PSsph) {
+    p.shape = 2;
+    for (int d = 0; d < 3; ++d) p.center[d] = d < sim->s.dim ? params[d] : 0;
+    p.radius = params[sim->s.dim];
+    if (p.radius < 0) { p.radius = -p.radius; p.front_sign = -1; }
+  } else if (panelshape == PSrect) {
+    LCHECK(axisstring, ECmissing, "missing axis string");
+    p.shape = 0;
+    p.front_sign = (axisstring[0] == '-') ? -1 : 1;
+    const char ax = axisstring[strlen(axisstring) - 1];
+    p.axis = (ax >= '0' && ax <= '2') ? ax - '0' : ax - 'x';
+    LCHECK(p.axis >= 0 && p.axis < 3, ECsyntax, "bad axis");
+    p.pos = params[p.axis];
+    int k = sim->s.dim;
+    for (int d = 0; d < 3; ++d) {
+      if (d == p.axis) { p.lo[d] = p.hi[d] = params[d]; continue; }
+      const double ext = (d < sim->s.dim) ? params[k++] : 0;
+      p.lo[d] = std::min(params[d], params[d] + ext);
+      p.hi[d] = std::max(params[d], params[d] + ext);
+    }
+  } else {
+    return set_error(__func__, ECbounds, "panel shape not supported by the GPU engine (rect, sphere)");
+  }
+  sf->panels.push_back(p);
+  sim->s.need_rebuild = true;
+  return ECok;
+}
+
+enum ErrorCode smolAddReaction(simptr sim, const char *reaction, const char *reactant1, enum MolecState rstate1,
+                               const char *reactant2, enum MolecState rstate2, int nproduct,
+                               const char **productspecies, enum MolecState *productstates, double rate) {
+  (void)rstate1; (void)rstate2; (void)productstates;
+  LCHECK(sim && reaction, ECmissing, "missing sim or reaction name");
+  Sim &s = sim->s;
+  LCHECK(s.reaction_index(reaction, nullptr) < 0, ECsame, "reaction already exists");
+  LCHECK(nproduct >= 0 && nproduct <= smolb::kMaxProd, ECbounds, "0..4 products supported");
+  smolb::RxnDef x;
+  x.name = reaction;
+  int order = 0;
+  const char *rr[2] = {reactant1, reactant2};
+  for (int k = 0; k < 2; ++k) {
+    if (rr[k] && rr[k][0]) {
+      const int i = s.species_index(rr[k]);
+      LCHECK(i > 0, ECnonexist, "reactant species not found");
+      x.rct[order++] = i;
+    }
+  }
+  x.order = order;
+  x.nprod = nproduct;
+  for (int q = 0; q < nproduct; ++q) {
+    const int i = s.species_index(productspecies[q]);
+    LCHECK(i > 0, ECnonexist, "product species not found");
+    x.prd[q] = i;
+  }
+  x.rate = rate;
+  LCHECK((int)s.rxn[order].size() < smolb::kMaxRxn, ECbounds, "too many reactions of this order (max 16)");
+  s.rxn[order].push_back(x);
+  s.need_update = s.need_rebuild = true;
+  return ECok;
+}
+
+enum ErrorCode smolAddBimolecularReaction(simptr sim, const char *reaction, const char *reactant1,
+                                          const char *reactant2, int nproduct, const char **productspecies,
+                                          double rate) {
+  LCHECK(reactant1 && reactant2 && reactant1[0] && reactant2[0], ECmissing, "two reactants required");
+  return smolAddReaction(sim, reaction, reactant1, MSsoln, reactant2, MSsoln, nproduct, productspecies, nullptr, rate);
+}
+
+int smolGetReactionIndex(simptr sim, int *orderptr, const char *reaction) {
+  if (!sim || !reaction) return (int)set_error(__func__, ECmissing, "missing argument");
+  const int r = sim->s.reaction_index(reaction, orderptr);
+  if (r < 0) return (int)set_error(__func__, ECnonexist, "reaction not found");
+  return r;
+}
+
+enum ErrorCode smolSetReactionRate(simptr sim, const char *reaction, double rate, int type) {
+  (void)type;
+  LCHECK(sim && reaction, ECmissing, "missing argument");
+  int o;
+  const int r = sim->s.reaction_index(reaction, &o);
+  LCHECK(r >= 0, ECnonexist, "reaction not found");
+  sim->s.rxn[o][r].rate = rate;
+  sim->s.need_update = true;
+  return ECok;
+}
+
+enum ErrorCode smolSetReactionProducts(simptr sim, const char *reaction, enum RevParam method, double parameter,
+                                       const char *product, double *position) {
+  LCHECK(sim && reaction, ECmissing, "missing argument");
+  int o;
+  const int r = sim->s.reaction_index(reaction, &o);
+  LCHECK(r >= 0, ECnonexist, "reaction not found");
+  smolb::RxnDef &x = sim->s.rxn[o][r];
+  x.rparamt = (int)method;
+  x.rparam = parameter;
+  if ((method == RPoffset || method == RPfixed) && product && position) {
+    const int q = sim->s.species_index(product);
+    for (int k = 0; k < x.nprod; ++k)
+      if (x.prd[k] == q) {
+        for (int d = 0; d < sim->s.dim; ++d) x.user_prdpos[k][d] = position[d];
+        break;
+      }
+  }
+  sim->s.need_update = true;
+  return ECok;
+}
+
+// ---- smolgpu extensions ----------------------------------------------------
+
+enum ErrorCode smolgpuGetReactionParams(simptr sim, const char *reaction, double *bindrad, double *unbindrad,
+                                        double *prob) {
+  LCHECK(sim && reaction, ECmissing, "missing argument");
+  LCHECK(sim->s.dt > 0, ECerror, "time step must be > 0");
+  // parameter derivation only (host FP64); no engine is built here
+  std::string err;
+  if (smolb::derive_reaction_params(sim->s, &err)) return set_error(__func__, ECerror, err);
+  int o;
+  const int r = sim->s.reaction_index(reaction, &o);
+  LCHECK(r >= 0, ECnonexist, "reaction not found");
+  smolb::RxnDef &x = sim->s.rxn[o][r];
+  if (bindrad) *bindrad = x.bindrad2 >= 0 ? std::sqrt(x.bindrad2) : -1;
+  if (unbindrad) *unbindrad = x.unbindrad;
+  if (prob) *prob = x.prob;
+  return ECok;
+}
+
+double smolgpuGetTime(simptr sim) { return sim ? sim->s.time : 0; }
+long long smolgpuGetStepCount(simptr sim) { return sim ? sim->s.steps : 0; }
+
+long long smolgpuGetTotalMolecules(simptr sim) {
+  if (!sim) return -1;
+  if (sim->s.eng && sim->s.started && !sim->s.need_rebuild) return sim->s.eng->total_molecules();
+  return (long long)sim->s.pend_sp.size();
+}
+
+enum ErrorCode smolgpuGetMolecules(simptr sim, long long *n, double *pos, int *species, uint64_t *serno) {
+  LCHECK(sim && n, ECmissing, "missing argument");
+  Sim &s = sim->s;
+  std::string err;
+  std::vector<double> p;
+  std::vector<int> sp;
+  std::vector<uint64_t> sn;
+  if (s.eng && s.started && !s.need_rebuild) {
+    if (s.eng->get_molecules(&p, &sp, nullptr, &sn, &err)) return set_error(__func__, ECerror, err);
+  } else {
+    p = s.pend_pos;
+    sp = s.pend_sp;
+    sn.resize(sp.size());
+    for (size_t i = 0; i < sp.size(); ++i) sn[i] = i + 1;
+  }
+  const long long cnt = (long long)sp.size();
+  LCHECK(*n >= cnt || (!pos && !species && !serno), ECbounds, "buffer too small");
+  *n = cnt;
+  if (pos) memcpy(pos, p.data(), p.size() * sizeof(double));
+  if (species) memcpy(species, sp.data(), sp.size() * sizeof(int));
+  if (serno) memcpy(serno, sn.data(), sn.size() * sizeof(uint64_t));
+  return ECok;
+}
+
+enum ErrorCode smolgpuSetMolecules(simptr sim, long long n, const double *pos, const int *species,
+                                   const uint64_t *serno) {
+  LCHECK(sim && (n == 0 || (pos && species)), ECmissing, "missing argument");
+  Sim &s = sim->s;
+  for (long long i = 0; i < n; ++i)
+    LCHECK(species[i] > 0 && species[i] < (int)s.species.size(), ECbounds, "species index out of range");
+  s.pend_pos.assign(pos, pos + 3 * n);
+  s.pend_sp.assign(species, species + n);
+  ErrorCode ec = update_sim(s, __func__);
+  if (ec != ECok) return ec;
+  std::string err;
+  if (s.eng->set_molecules(n, pos, species, nullptr, serno, &err)) return set_error(__func__, ECerror, err);
+  s.pend_pos.clear();
+  s.pend_sp.clear();
+  s.started = true;
+  return ECok;
+}
+
+enum ErrorCode smolgpuGetEventCounts(simptr sim, long long counts[8]) {
+  LCHECK(sim && counts, ECmissing, "missing argument");
+  for (int k = 0; k < 8; ++k) counts[k] = 0;
+  if (!sim->s.eng) return ECok;
+  smolb::EngineStats st;
+  std::string err;
+  if (sim->s.eng->stats(&st, &err)) return set_error(__func__, ECerror, err);
+  counts[0] = st.wall; counts[1] = st.rxn0; counts[2] = st.rxn1; counts[3] = st.rxn2;
+  counts[4] = st.unresolved; counts[5] = st.multicand; counts[6] = st.overflow;
+  return ECok;
+}
+
+enum ErrorCode smolgpuSetInjectedDisplacements(simptr sim, long long n, const uint64_t *sernos, const double *disp) {
+  LCHECK(sim, ECmissing, "missing sim");
+  LCHECK(n == 0 || (sernos && disp), ECmissing, "missing arrays");
+  ErrorCode ec = update_sim(sim->s, __func__);
+  if (ec != ECok) return ec;
+  std::string err;
+  if (sim->s.eng->set_injection(n, sernos, disp, 0, &err)) return set_error(__func__, ECerror, err);
+  return ECok;
+}
+
+enum ErrorCode smolgpuSetStream(simptr sim, void *stream) {
+  LCHECK(sim, ECmissing, "missing sim");
+  ErrorCode ec = update_sim(sim->s, __func__);
+  if (ec != ECok) return ec;
+  sim->s.eng->set_stream(stream);
+  return ECok;
+}
+
+long long smolgpuGetLaunchCount(simptr sim) { return (sim && sim->s.eng) ? sim->s.eng->launches() : 0; }
+
+enum ErrorCode smolgpuRunSteps(simptr sim, long long nsteps) {
+  LCHECK(sim, ECmissing, "missing sim");
+  LCHECK(nsteps >= 0, ECbounds, "nsteps must be >= 0");
+  Sim &s = sim->s;
+  ErrorCode ec = update_sim(s, __func__);
+  if (ec != ECok) return ec;
+  std::string err;
+  if (s.eng->run(nsteps, &err)) return set_error(__func__, ECerror, err);
+  for (long long k = 0; k < nsteps; ++k) s.time += s.dt;
+  s.steps += nsteps;
+  return ECok;
+}
+
+enum ErrorCode smolgpuProfileSteps(simptr sim, long long nsteps, int *nkernels, char *names, double *ms,
+                                   long long *launches) {
+  LCHECK(sim && nkernels, ECmissing, "missing argument");
+  Sim &s = sim->s;
+  ErrorCode ec = update_sim(s, __func__);
+  if (ec != ECok) return ec;
+  std::vector<std::string> nm;
+  std::vector<double> t;
+  std::vector<long long> l;
+  std::string err;
+  if (s.eng->profile(nsteps, &nm, &t, &l, &err)) return set_error(__func__, ECerror, err);
+  for (long long k = 0; k < nsteps; ++k) s.time += s.dt;
+  s.steps += nsteps;
+  const int cap = *nkernels;
+  *nkernels = (int)nm.size();
+  for (int k = 0; k < (int)nm.size() && k < cap; ++k) {
+    if (names) { strncpy(names + 32 * k, nm[k].c_str(), 31); names[32 * k + 31] = 0; }
+    if (ms) ms[k] = t[k];
+    if (launches) launches[k] = l[k];
+  }
+  return ECok;
+}
+
+enum ErrorCode smolgpuSynchronize(simptr sim) {
+  LCHECK(sim, ECmissing, "missing sim");
+  if (!sim->s.eng) return ECok;
+  std::string err;
+  if (sim->s.eng->synchronize(&err)) return set_error(__func__, ECerror, err);
+  return ECok;
+}
+
+enum ErrorCode smolgpuSolveRadii(int mode, long long n, const double *rate, double dt, const double *difc,
+                                 const double *b, int rel, double *out) {
+  LCHECK(n >= 0, ECbounds, "n must be >= 0");
+  LCHECK(n == 0 || (rate && difc && b && out), ECmissing, "missing arrays");
+  LCHECK(mode == 0 || mode == 1, ECbounds, "mode must be 0 or 1");
+  std::string err;
+  if (smolb::solve_radii_device(mode, n, rate, dt, difc, b, rel, out, &err)) return set_error(__func__, ECerror, err);
+  return ECok;
+}
+
+double smolgpuBindingRadiusHost(double rate, double dt, double difc, double b, int rel) {
+  return smolb::rxnp::bindingradius(rate, dt, difc, b, rel);
+}
+
+double smolgpuUnbindingRadiusHost(double pgem, double dt, double difc, double a) {
+  return smolb::rxnp::unbindingradius(pgem, dt, difc, a);
+}
+
+}  // extern "C"

@@ -1,0 +1,138 @@
+// Device-side building blocks shared by the engine kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "engine.h"
+
+namespace smolb {
+
+typedef unsigned long long ull;
+
+// ---- molecule identity word ------------------------------------------------
+// bits 63..58 species (63 = dead), 57..42 replicate, 41..0 serial number.
+constexpr int kSpShift = 58;
+constexpr int kRepShift = 42;
+constexpr ull kSernoMask = (1ull << 42) - 1;
+constexpr ull kRepMask = 0xFFFFull;
+constexpr int kDeadSpecies = 63;
+constexpr ull kProductSernoBit = 1ull << 41;  // product serial numbers have this bit set
+
+__host__ __device__ __forceinline__ int id_species(ull id) { return (int)(id >> kSpShift); }
+__host__ __device__ __forceinline__ int id_rep(ull id) { return (int)((id >> kRepShift) & kRepMask); }
+__host__ __device__ __forceinline__ ull id_serno(ull id) { return id & kSernoMask; }
+__host__ __device__ __forceinline__ ull make_id(int sp, int rep, ull serno) {
+  return ((ull)sp << kSpShift) | ((ull)rep << kRepShift) | (serno & kSernoMask);
+}
+__host__ __device__ __forceinline__ ull id_mark_dead(ull id) {
+  return (id & ~(63ull << kSpShift)) | ((ull)kDeadSpecies << kSpShift);
+}
+// identity without the species field (stable RNG stream key of a molecule)
+__host__ __device__ __forceinline__ ull id_stream(ull id) { return id & ((1ull << kSpShift) - 1); }
+
+// ---- cell coordinates packed into the w lane of the position float4 --------
+__host__ __device__ __forceinline__ uint32_t pack_cell(int ix, int iy, int iz) {
+  return (uint32_t)ix | ((uint32_t)iy << 10) | ((uint32_t)iz << 20);
+}
+__host__ __device__ __forceinline__ void unpack_cell(uint32_t w, int &ix, int &iy, int &iz) {
+  ix = (int)(w & 1023u);
+  iy = (int)((w >> 10) & 1023u);
+  iz = (int)((w >> 20) & 1023u);
+}
+
+// ---- Philox4x32-10 (Salmon, Moraes, Dror, Shaw; SC'11) ----------------------
+__host__ __device__ __forceinline__ uint32_t mulhi32(uint32_t a, uint32_t b) {
+#ifdef __CUDA_ARCH__
+  return __umulhi(a, b);
+#else
+  return (uint32_t)(((uint64_t)a * b) >> 32);
+#endif
+}
+
+__host__ __device__ __forceinline__ uint4 philox(uint4 c, uint2 k) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t hi0 = mulhi32(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+    const uint32_t hi1 = mulhi32(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    k.x += 0x9E3779B9u;
+    k.y += 0xBB67AE85u;
+  }
+  return c;
+}
+
+// uniform in [0,1) with 32-bit resolution (matches randCOD's granularity)
+__host__ __device__ __forceinline__ double u01d(uint32_t x) { return x * 2.3283064365386963e-10; }
+// uniform in (0,1) as float with 24-bit resolution
+__host__ __device__ __forceinline__ float u01f_open(uint32_t x) {
+  return ((x >> 8) + 0.5f) * (1.0f / 16777216.0f);
+}
+
+// SplitMix64 finaliser, used to derive product serial numbers and birth keys.
+__host__ __device__ __forceinline__ ull mix64(ull z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// ---- engine constants (one copy per library, set before each launch batch) --
+struct DevNet {
+  int nsp, nrep;
+  int nr[3];
+  int rxn_base[3];     // order o reaction r -> index rxn_base[o]+r in per-rep product tables
+  int nrx_total;
+  uint32_t gmask;      // gaussian table size - 1
+  uint32_t key0, key1; // Philox key (seed)
+  int any_drift;
+  int any_absorb;
+  int inject;          // deterministic mode active
+  int npanel;
+  int rounds;          // pair conflict-resolution rounds
+  int uni_n[kMaxSpecies];
+  uint8_t uni_list[kMaxSpecies][kMaxUniPerSpecies];
+  uint32_t pair_mask[kMaxSpecies];
+  uint8_t pair_n[kMaxSpecies][kMaxSpecies];
+  uint8_t pair_list[kMaxSpecies][kMaxSpecies][kMaxPairRxn];
+  uint8_t rct[3][kMaxRxn][2];
+  uint8_t nprod[3][kMaxRxn];
+  uint8_t prd[3][kMaxRxn][kMaxProd];
+  uint8_t fixed[3][kMaxRxn];
+  uint8_t has_offset[3][kMaxRxn];
+};
+
+// Per-replicate geometry.  Cells are cubes of size h; the last cell in each
+// dimension extends to the high wall, which sits at local coordinate whi.
+struct DevGeo {
+  float h[3], inv_h[3], whi[3];
+  int n[3];
+  int cell0;   // first global cell index of this replicate
+  int dim;
+  uint8_t wall[6];
+  uint8_t pad[2];
+  float vol;
+};
+
+// Per-replicate surface panel set (shared by replicates; absolute double
+// coordinates relative to the replicate's low corner are converted on the fly).
+struct DevPanel {
+  int shape;        // 0 rect, 2 sphere
+  int axis;
+  int front_sign;
+  float pos;        // rect plane coordinate (relative to low corner)
+  float lo[3], hi[3];
+  float center[3];  // sphere centre (relative to low corner)
+  float radius;
+  int act_front, act_back;   // 0 reflect 1 transmit 2 absorb
+  uint32_t abs_front, abs_back, tr_front, tr_back;
+};
+
+struct Event {      // one reaction or birth; products are placed by k_products
+  float4 site;      // reaction site: local coordinates + packed cell (orders 1, 2)
+  ull key;          // parent identity (stream key) used for product RNG and serial numbers
+  uint32_t rxn;     // order << 8 | reaction index
+  uint32_t rep;
+};
+
+}  // namespace smolb

@@ -1,0 +1,1670 @@
+// B200 particle engine: kernels and host driver.
+//
+// One time step (Smoldyn smolsim.cpp:2607-2692 order) is the launch sequence
+//   k_begin          step counter, per-step counters
+//   k_advance(count) diffuse + walls + first-order decisions, histogram of the
+//                    new virtual box of every survivor (warp-aggregated atomics)
+//   scan (3 kernels) exclusive scan of box counts -> box start offsets
+//   k_advance(scat.) recomputes the same move (same Philox counters) and
+//                    scatters survivors in box order; first-order events out
+//   k_births         zeroth-order births (Poisson per replicate and reaction)
+//   k_pairs          27-box neighbour search within each pair's binding radius;
+//                    closest candidate per molecule as a packed (dist2, index) key
+//   k_commit / k_research (rounds) mutual-closest pairs react, losers retry
+//   k_products       product placement (site, unbinding offsets under one random
+//                    rotation per event), walls for the new molecules
+// Molecules live in two ping-pong box-sorted SoA buffers (float4 position in
+// box-local FP32 coordinates with the box index packed in .w, plus a 64-bit
+// identity word) and two ping-pong product buffers.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "devcommon.cuh"
+#include "engine.h"
+#include "rxnparam.cuh"
+
+namespace smolb {
+
+__constant__ DevNet c_net;
+__constant__ DevPanel c_panels[kMaxPanels];
+
+struct KParams {
+  const DevGeo *geo;
+  const float *difstep;    // [rep*nsp + sp]  sqrt(2 D dt)
+  const float *driftdt;    // [(rep*nsp + sp)*3] drift*dt or null
+  const uint32_t *unithr;  // [(rep*nsp + sp)*kMaxUniPerSpecies] cumulative thresholds
+  const float *bind2;      // [rep*nr2 + r]
+  const float *pairprob;   // [rep*nr2 + r]
+  const double *births;    // [rep*nr0 + r]
+  const float *prdpos;     // [((rep*nrx + k)*kMaxProd + p)*3]
+  const float *gtab;       // gaussian table
+  // molecules: a = sorted input, p = product input, b = sorted output, q = product output
+  const float4 *a_pc;
+  ull *a_id;
+  const int *a_n;
+  const float4 *p_pc;
+  const ull *p_id;
+  const int *p_n;
+  float4 *b_pc;
+  ull *b_id;
+  int *b_n;
+  float4 *q_pc;
+  ull *q_id;
+  int *q_n;
+  int cap, pcap;
+  int *cnt;
+  int *start;
+  int ncell;
+  int *blocksums;
+  Event *ev;
+  int *nev;
+  int evcap;
+  int *cand;
+  int *ncand;
+  int candcap;
+  ull *best;
+  unsigned long long *counters;  // [0]=wall [1]=rxn0 [2]=rxn1 [3]=rxn2 [4]=unresolved [5]=multicand
+  long long *spcount;            // [rep*nsp + sp]
+  int *status;
+  uint32_t *step;
+  // deterministic mode
+  const ull *inj_key;            // sorted stream keys
+  const float4 *inj_val;         // dx, dy, dz, forced order-1 reaction (or -1)
+  int inj_n;
+};
+
+enum StatusBits { kStMolCap = 1, kStEvCap = 2, kStProdCap = 4, kStCandCap = 8 };
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Bring local coordinate w (relative to the origin of cell j, j maybe out of
+// range) into cell form.
+__device__ __forceinline__ void renorm(float &w, int &j, float h, float inv_h) {
+  if (w >= 0.f && w < h) return;
+  const int k = (int)floorf(w * inv_h);
+  j += k;
+  w -= (float)k * h;
+  if (w < 0.f) { j -= 1; w += h; }
+  else if (w >= h) { j += 1; w -= h; }
+}
+
+// Apply the low and high wall of one dimension to (w, j) (smolwall.c:368-427,
+// low wall first).  Returns 1 if the molecule crossed an absorbing wall.
+__device__ __forceinline__ int walls_dim(float &w, int &j, const DevGeo &g, int d, int &hits) {
+  const float h = g.h[d], inv_h = g.inv_h[d], whi = g.whi[d];
+  const int n = g.n[d];
+  if (j < 0) {  // beyond the low wall (position j*h + w < 0)
+    const int kind = g.wall[2 * d];
+    hits++;
+    if (kind == kWallReflect) {
+      float p = -((float)j * h + w);
+      j = 0;
+      w = p;
+      renorm(w, j, h, inv_h);
+    } else if (kind == kWallPeriodic) {
+      j += n;
+      w += whi - h;
+      renorm(w, j, h, inv_h);
+    } else if (kind == kWallAbsorb) {
+      return 1;
+    } else {
+      w = (float)j * h + w;
+      j = 0;
+    }
+  }
+  if (j >= n - 1) {
+    const float e = (float)(j - (n - 1)) * h + w - whi;  // signed distance beyond the high wall
+    if (e > 0.f) {
+      const int kind = g.wall[2 * d + 1];
+      hits++;
+      if (kind == kWallReflect) {
+        j = n - 1;
+        w = whi - e;
+        renorm(w, j, h, inv_h);
+        if (j < 0) {  // reflected past the low wall too (step longer than the box)
+          if (g.wall[2 * d] == kWallReflect) { w = -((float)j * h + w); j = 0; renorm(w, j, h, inv_h); }
+          else { w = (float)j * h + w; j = 0; }
+        }
+      } else if (kind == kWallPeriodic) {
+        j -= n;
+        w += h - whi;
+        renorm(w, j, h, inv_h);
+      } else if (kind == kWallAbsorb) {
+        return 1;
+      } else {
+        w = e + whi;
+        j = n - 1;
+      }
+    } else if (j > n - 1) {  // inside the box but past the nominal last cell
+      w = e + whi;
+      j = n - 1;
+    }
+  }
+  return 0;
+}
+
+// Last line of defence for the box index: a displacement of several box
+// lengths in one step (huge D*dt) or a non-finite position must still give an
+// in-range box, so the index is clamped and the local offset kept relative to
+// that box.  Only pathological inputs reach the clamp.
+__device__ __forceinline__ void clamp_cell(float &w, int &j, const DevGeo &g, int d) {
+  if (!(w == w)) w = 0.f;  // NaN
+  const int n = g.n[d];
+  if (j < 0) {
+    if (g.wall[2 * d] == kWallPeriodic && j > -(1 << 20)) {
+      const int k = (-j + n - 1) / n;
+      j += k * n;
+    } else {
+      w += (float)j * g.h[d];
+      j = 0;
+    }
+  }
+  if (j > n - 1) {
+    if (g.wall[2 * d + 1] == kWallPeriodic && j < (1 << 20)) {
+      const int k = j / n;
+      j -= k * n;
+    } else {
+      w += (float)(j - (n - 1)) * g.h[d];
+      j = n - 1;
+    }
+  }
+  if (j < 0) j = 0;
+  if (j > n - 1) j = n - 1;
+}
+
+// Distance of a (cell, local) coordinate from the low / high wall.
+__device__ __forceinline__ float dist_low(int j, float w, float h) { return (float)j * h + w; }
+__device__ __forceinline__ float dist_high(int j, float w, const DevGeo &g, int d) {
+  return (float)(g.n[d] - 1 - j) * g.h[d] + g.whi[d] - w;
+}
+
+__device__ __forceinline__ int find_injection(const KParams &p, ull key) {
+  int lo = 0, hi = p.inj_n - 1;
+  while (lo <= hi) {
+    const int mid = (lo + hi) >> 1;
+    const ull k = p.inj_key[mid];
+    if (k == key) return mid;
+    if (k < key) lo = mid + 1;
+    else hi = mid - 1;
+  }
+  return -1;
+}
+
+// Move one molecule by one step: returns 0 alive, 1 removed by a wall,
+// 2+r first-order reaction r fired (position is the post-move position).
+__device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, const KParams &p,
+                                           const float *gtab, int rebin_only, int &hits) {
+  const int sp = id_species(id);
+  const int rep = id_rep(id);
+  const DevGeo g = p.geo[rep];
+  int ix[3];
+  unpack_cell(__float_as_uint(pc.w), ix[0], ix[1], ix[2]);
+  float u[3] = {pc.x, pc.y, pc.z};
+  if (rebin_only) {
+    for (int d = 0; d < 3; ++d) renorm(u[d], ix[d], g.h[d], g.inv_h[d]);
+    for (int d = 0; d < 3; ++d) {
+      if (ix[d] < 0) { u[d] = (float)ix[d] * g.h[d] + u[d]; ix[d] = 0; }
+      if (ix[d] > g.n[d] - 1) { u[d] = (float)(ix[d] - (g.n[d] - 1)) * g.h[d] + u[d]; ix[d] = g.n[d] - 1; }
+      clamp_cell(u[d], ix[d], g, d);
+    }
+    pc = make_float4(u[0], u[1], u[2], __uint_as_float(pack_cell(ix[0], ix[1], ix[2])));
+    return 0;
+  }
+  const ull skey = id_stream(id);
+  const uint2 key = make_uint2(c_net.key0, c_net.key1);
+  const uint4 r = philox(make_uint4((uint32_t)skey, (uint32_t)(skey >> 32), step, 0u), key);
+  float dsp[3];
+  int forced = -1;
+  if (c_net.inject) {
+    const int k = find_injection(p, skey);
+    if (k >= 0) {
+      const float4 v = p.inj_val[k];
+      dsp[0] = v.x; dsp[1] = v.y; dsp[2] = v.z;
+      forced = (int)v.w;
+    } else {
+      dsp[0] = dsp[1] = dsp[2] = 0.f;
+    }
+  } else {
+    const float ds = p.difstep[rep * c_net.nsp + sp];
+    const uint32_t gm = c_net.gmask;
+    dsp[0] = ds * gtab[r.x & gm];
+    dsp[1] = ds * gtab[r.y & gm];
+    dsp[2] = ds * gtab[r.z & gm];
+    if (c_net.any_drift) {
+      const float *dr = p.driftdt + (size_t)(rep * c_net.nsp + sp) * 3;
+      dsp[0] += dr[0]; dsp[1] += dr[1]; dsp[2] += dr[2];
+    }
+  }
+  const int ix0[3] = {ix[0], ix[1], ix[2]};
+  const float u0[3] = {u[0], u[1], u[2]};
+  for (int d = 0; d < 3; ++d) {
+    if (d >= g.dim) continue;
+    float w = u[d] + dsp[d];
+    int j = ix[d];
+    renorm(w, j, g.h[d], g.inv_h[d]);
+    if (j <= 0 || j >= g.n[d] - 1) {
+      if (walls_dim(w, j, g, d, hits)) return 1;
+    }
+    clamp_cell(w, j, g, d);
+    u[d] = w;
+    ix[d] = j;
+  }
+  if (c_net.any_absorb && !c_net.inject) {
+    // Absorbing walls also remove molecules that stayed inside with probability
+    // exp(-2*dold*dnew/step^2) (smolwall.c:417-420); the reference applies that
+    // test in both wall passes of a step (smolsim.cpp:2625 and :2662), so the
+    // survival probability is (1-p)^2.
+    const float ds = p.difstep[rep * c_net.nsp + sp];
+    const float inv2 = (ds > 0.f) ? 1.f / (ds * ds) : 0.f;
+    uint4 r2 = make_uint4(0, 0, 0, 0);
+    int have = 0;
+    for (int d = 0; d < g.dim; ++d) {
+      for (int side = 0; side < 2; ++side) {
+        if (g.wall[2 * d + side] != kWallAbsorb || ds <= 0.f) continue;
+        float dn, dold;
+        if (side == 0) { dn = dist_low(ix[d], u[d], g.h[d]); dold = dist_low(ix0[d], u0[d], g.h[d]); }
+        else { dn = dist_high(ix[d], u[d], g, d); dold = dist_high(ix0[d], u0[d], g, d); }
+        const float x = 2.f * dn * dold * inv2;
+        if (x > 80.f) continue;
+        const float pr = __expf(-x);
+        const float pe = pr * (2.f - pr);  // 1-(1-p)^2
+        if (!have) { r2 = philox(make_uint4((uint32_t)skey, (uint32_t)(skey >> 32), step, 1u), key); have = 1; }
+        const uint32_t bits = (d == 0) ? (side ? r2.y : r2.x) : (d == 1) ? (side ? r2.w : r2.z)
+                                        : (side ? (r2.x ^ r2.w) : (r2.y ^ r2.z));
+        if (u01f_open(bits) < pe) { hits++; return 1; }
+      }
+    }
+  }
+  pc = make_float4(u[0], u[1], u[2], __uint_as_float(pack_cell(ix[0], ix[1], ix[2])));
+  const int nuni = c_net.uni_n[sp];
+  if (nuni) {
+    if (c_net.inject) {
+      if (forced >= 0) return 2 + forced;
+    } else {
+      const uint32_t *thr = p.unithr + (size_t)(rep * c_net.nsp + sp) * kMaxUniPerSpecies;
+      for (int m = 0; m < nuni; ++m)
+        if (r.w < thr[m]) return 2 + c_net.uni_list[sp][m];
+    }
+  }
+  return 0;
+}
+
+__device__ __forceinline__ int global_cell(const DevGeo &g, uint32_t w) {
+  int ix, iy, iz;
+  unpack_cell(w, ix, iy, iz);
+  return g.cell0 + (iz * g.n[1] + iy) * g.n[0] + ix;
+}
+
+__device__ __forceinline__ void push_event(const KParams &p, const Event &e) {
+  const int k = atomicAdd(p.nev, 1);
+  if (k < p.evcap) p.ev[k] = e;
+  else atomicOr(p.status, kStEvCap);
+}
+
+// ---------------------------------------------------------------------------
+__global__ void k_begin(KParams p, int bump_step) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    if (bump_step) *p.step += 1;
+    *p.nev = 0;
+    *p.ncand = 0;
+    *p.q_n = 0;
+  }
+}
+
+// phase bit 0: 0 = count, 1 = scatter.  bit 1: rebin only (no motion, no reactions).
+__global__ void __launch_bounds__(256) k_advance(KParams p, int phase) {
+  extern __shared__ float s_gtab[];
+  const int rebin_only = (phase >> 1) & 1;
+  const int scatter = phase & 1;
+  const int gsize = (int)c_net.gmask + 1;
+  const float *gtab = p.gtab;
+  if (!rebin_only && gsize <= 8192) {
+    for (int k = threadIdx.x; k < gsize; k += blockDim.x) s_gtab[k] = p.gtab[k];
+    __syncthreads();
+    gtab = s_gtab;
+  }
+  const int na = *p.a_n, np = *p.p_n;
+  const int total = na + np;
+  const uint32_t step = *p.step;
+  const int lane = threadIdx.x & 31;
+  int hits_acc = 0;
+  for (int base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
+    const int i = base + threadIdx.x;
+    float4 pc = make_float4(0.f, 0.f, 0.f, 0.f);
+    ull id = 0;
+    bool valid = false;
+    if (i < total) {
+      if (i < na) { pc = p.a_pc[i]; id = p.a_id[i]; }
+      else { pc = p.p_pc[i - na]; id = p.p_id[i - na]; }
+      valid = id_species(id) != kDeadSpecies;
+    }
+    int fate = -1;
+    int hits = 0;
+    if (valid) fate = advance_one(pc, id, step, p, gtab, rebin_only, hits);
+    const bool alive = (fate == 0);
+    const unsigned act = __ballot_sync(0xffffffffu, alive);
+    if (alive) {
+      const int rep = id_rep(id);
+      const int cell = global_cell(p.geo[rep], __float_as_uint(pc.w));
+      const unsigned peers = __match_any_sync(act, cell);
+      const int leader = __ffs(peers) - 1;
+      const int npeer = __popc(peers);
+      const int rank = __popc(peers & lanemask_lt());
+      if (!scatter) {
+        if (lane == leader) atomicAdd(&p.cnt[cell], npeer);
+      } else {
+        int old = 0;
+        if (lane == leader) old = atomicSub(&p.cnt[cell], npeer);
+        old = __shfl_sync(peers, old, leader);
+        const int slot = p.start[cell] + old - npeer + rank;
+        if (slot >= 0 && slot < p.cap) {
+          p.b_pc[slot] = pc;
+          p.b_id[slot] = id;
+        } else {
+          atomicOr(p.status, kStMolCap);
+        }
+      }
+    }
+    if (scatter && valid) {
+      hits_acc += hits;
+      if (fate == 1) {
+        atomicAdd((unsigned long long *)&p.spcount[id_rep(id) * c_net.nsp + id_species(id)],
+                  (unsigned long long)(-1ll));
+      } else if (fate >= 2) {
+        Event e;
+        e.site = pc;
+        e.key = id_stream(id);
+        e.rxn = (1u << 8) | (uint32_t)(fate - 2);
+        e.rep = (uint32_t)id_rep(id);
+        push_event(p, e);
+      }
+    }
+  }
+  if (scatter && hits_acc) atomicAdd(&p.counters[0], (unsigned long long)hits_acc);
+}
+
+// ---- exclusive scan of the box histogram ------------------------------------
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int *s_warp, int &total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    int w = (lane < nw) ? s_warp[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < nw) s_warp[lane] = w;
+  }
+  __syncthreads();
+  const int warp_excl = (warp > 0) ? s_warp[warp - 1] : 0;
+  total = s_warp[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return warp_excl + x - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const int *cnt, int n, int *bsum) {
+  __shared__ int s_warp[32];
+  const int base = blockIdx.x * kScanTile;
+  int sum = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const int i = base + k * kScanThreads + threadIdx.x;
+    if (i < n) sum += cnt[i];
+  }
+  int total;
+  block_exclusive_scan(sum, s_warp, total);
+  if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_blocks(int *bsum, int nb) {
+  __shared__ int s_warp[32];
+  __shared__ int s_carry;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  for (int off = 0; off < nb; off += blockDim.x) {
+    const int i = off + threadIdx.x;
+    const int v = (i < nb) ? bsum[i] : 0;
+    int total;
+    const int ex = block_exclusive_scan(v, s_warp, total);
+    const int carry = s_carry;
+    if (i < nb) bsum[i] = carry + ex;
+    __syncthreads();
+    if (threadIdx.x == 0) s_carry = carry + total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) bsum[nb] = s_carry;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(const int *cnt, int n, const int *bsum,
+                                                              int nb, int *start, int *n_out, int cap) {
+  __shared__ int s_warp[32];
+  const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  int v[kScanItems];
+  int sum = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const int i = base + k;
+    v[k] = (i < n) ? cnt[i] : 0;
+    sum += v[k];
+  }
+  int total;
+  int ex = block_exclusive_scan(sum, s_warp, total) + bsum[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const int i = base + k;
+    if (i < n) start[i] = ex;
+    ex += v[k];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const int tot = bsum[nb];
+    start[n] = tot;
+    *n_out = tot < cap ? tot : cap;
+  }
+}
+
+// ---- zeroth-order births ---------------------------------------------------
+__device__ int poisson_sample(double mean, uint2 key, uint4 ctr) {
+  if (mean <= 0) return 0;
+  uint32_t it = 0;
+  if (mean < 12.0) {  // product of uniforms (Knuth)
+    const double g = exp(-mean);
+    int n = 0;
+    uint4 r = philox(ctr, key);
+    double t = u01d(r.x) + 1.1641532182693481e-10;
+    int used = 1;
+    while (t > g && n < 100000) {
+      if (used == 4) { ctr.w = ++it; r = philox(ctr, key); used = 0; }
+      const uint32_t b = (used == 0) ? r.x : (used == 1) ? r.y : (used == 2) ? r.z : r.w;
+      used++;
+      t *= u01d(b) + 1.1641532182693481e-10;
+      n++;
+    }
+    return n;
+  }
+  // transformed rejection with squeeze, PTRS (W. Hormann, Insurance: Math. Econ. 12, 1993)
+  const double smu = sqrt(mean);
+  const double b = 0.931 + 2.53 * smu;
+  const double a = -0.059 + 0.02483 * b;
+  const double inv_alpha = 1.1239 + 1.1328 / (b - 3.4);
+  const double vr = 0.9277 - 3.6224 / (b - 2.0);
+  const double lmu = log(mean);
+  for (int guard = 0; guard < 1000; ++guard) {
+    ctr.w = ++it;
+    const uint4 r = philox(ctr, key);
+    const double U = u01d(r.x) - 0.5 + 1.1641532182693481e-10;
+    const double V = u01d(r.y) + 1.1641532182693481e-10;
+    const double us = 0.5 - fabs(U);
+    const double k = floor((2.0 * a / us + b) * U + mean + 0.43);
+    if (us >= 0.07 && V <= vr) return (int)k;
+    if (k < 0 || (us < 0.013 && V > us)) continue;
+    if (log(V) + log(inv_alpha) - log(a / (us * us) + b) <= -mean + k * lmu - lgamma(k + 1.0))
+      return (int)k;
+  }
+  return (int)floor(mean + 0.5);
+}
+
+__global__ void k_births(KParams p) {
+  const int nr0 = c_net.nr[0];
+  if (nr0 == 0) return;
+  const uint32_t step = *p.step;
+  const uint2 key = make_uint2(c_net.key0 ^ 0x5bd1e995u, c_net.key1);
+  const int total = c_net.nrep * nr0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int rep = t / nr0, r = t % nr0;
+    const double mean = p.births[t];
+    const int nb = poisson_sample(mean, key, make_uint4((uint32_t)rep, (uint32_t)r, step, 0u));
+    if (nb <= 0) continue;
+    const int base = atomicAdd(p.nev, nb);
+    for (int k = 0; k < nb; ++k) {
+      if (base + k >= p.evcap) { atomicOr(p.status, kStEvCap); break; }
+      Event e;
+      e.site = make_float4(0.f, 0.f, 0.f, 0.f);
+      e.key = mix64(((ull)rep << 40) ^ ((ull)r << 32) ^ ((ull)step << 8) ^ 0xB17Aull ^
+                    mix64((ull)k + 0x9E37ull * (ull)step)) & ((1ull << kSpShift) - 1);
+      e.rxn = (0u << 8) | (uint32_t)r;
+      e.rep = (uint32_t)rep;
+      p.ev[base + k] = e;
+    }
+    atomicAdd(&p.counters[1], (unsigned long long)nb);
+  }
+}
+
+// ---- bimolecular neighbour search ------------------------------------------
+// Deterministic per-pair coin for reactions with probability < 1.
+__device__ __forceinline__ bool pair_coin(ull ka, ull kb, int r, uint32_t step, float prob) {
+  if (prob >= 1.f) return true;
+  const ull lo = ka < kb ? ka : kb, hi = ka < kb ? kb : ka;
+  const uint4 x = philox(make_uint4((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32)),
+                         make_uint2(c_net.key0 ^ step, c_net.key1 ^ (0x7F4A7C15u + (uint32_t)r)));
+  return u01d(x.x) < (double)prob;
+}
+
+// First reaction (in list order) that fires for this pair, or -1.
+__device__ __forceinline__ int pair_reaction(const KParams &p, int rep, int spa, int spb, float d2,
+                                             ull ka, ull kb, uint32_t step) {
+  const int nl = c_net.pair_n[spa][spb];
+  const int nr2 = c_net.nr[2];
+  for (int m = 0; m < nl; ++m) {
+    const int r = c_net.pair_list[spa][spb][m];
+    if (d2 <= p.bind2[rep * nr2 + r] && pair_coin(ka, kb, r, step, p.pairprob[rep * nr2 + r])) return r;
+  }
+  return -1;
+}
+
+// Closest live partner of molecule i within its pair binding radii.
+// Returns packed (dist2 bits << 32 | index) or ~0 when none; *ncand counts candidates.
+__device__ ull search_partner(const KParams &p, int i, float4 pc, ull id, uint32_t step, int &ncand) {
+  const int nsorted = *p.b_n;
+  const int sp = id_species(id);
+  const int rep = id_rep(id);
+  const DevGeo g = p.geo[rep];
+  const uint32_t mask = c_net.pair_mask[sp];
+  int ix, iy, iz;
+  unpack_cell(__float_as_uint(pc.w), ix, iy, iz);
+  const bool px = g.wall[0] == kWallPeriodic, py = g.wall[2] == kWallPeriodic, pz = g.wall[4] == kWallPeriodic;
+  const ull ka = id_stream(id);
+  ull best = ~0ull;
+  ncand = 0;
+  for (int dz = -1; dz <= 1; ++dz) {
+    int z = iz + dz;
+    if (z < 0 || z >= g.n[2]) {
+      if (!pz) continue;
+      z = (z < 0) ? z + g.n[2] : z - g.n[2];
+    }
+    for (int dy = -1; dy <= 1; ++dy) {
+      int y = iy + dy;
+      if (y < 0 || y >= g.n[1]) {
+        if (!py) continue;
+        y = (y < 0) ? y + g.n[1] : y - g.n[1];
+      }
+      const int rowbase = g.cell0 + (z * g.n[1] + y) * g.n[0];
+      for (int dx = -1; dx <= 1; ++dx) {
+        int x = ix + dx;
+        if (x < 0 || x >= g.n[0]) {
+          if (!px) continue;
+          x = (x < 0) ? x + g.n[0] : x - g.n[0];
+        }
+        const int c = rowbase + x;
+        const int s = p.start[c], e = min(p.start[c + 1], nsorted);
+        for (int j = s; j < e; ++j) {
+          if (j == i) continue;
+          const ull jd = p.b_id[j];
+          const int spj = id_species(jd);
+          if (spj == kDeadSpecies || !((mask >> spj) & 1u)) continue;
+          const float4 q = p.b_pc[j];
+          // antisymmetric differences keep dist2 identical from both sides
+          const float vx = (q.x - pc.x) + (float)dx * g.h[0];
+          const float vy = (q.y - pc.y) + (float)dy * g.h[1];
+          const float vz = (q.z - pc.z) + (float)dz * g.h[2];
+          const float d2 = vx * vx + vy * vy + vz * vz;
+          if (pair_reaction(p, rep, sp, spj, d2, ka, id_stream(jd), step) < 0) continue;
+          ncand++;
+          const ull k = ((ull)__float_as_uint(d2) << 32) | (uint32_t)j;
+          if (k < best) best = k;
+        }
+      }
+    }
+  }
+  return best;
+}
+
+__global__ void __launch_bounds__(256) k_pairs(KParams p) {
+  const int n = *p.b_n;
+  const uint32_t step = *p.step;
+  int multi = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const ull id = p.b_id[i];
+    const int sp = id_species(id);
+    if (sp == kDeadSpecies || c_net.pair_mask[sp] == 0) continue;
+    int nc;
+    const ull best = search_partner(p, i, p.b_pc[i], id, step, nc);
+    if (best != ~0ull) {
+      p.best[i] = best;
+      const int k = atomicAdd(p.ncand, 1);
+      if (k < p.candcap) p.cand[k] = i;
+      else atomicOr(p.status, kStCandCap);
+      if (nc > 1) multi++;
+    }
+  }
+  if (multi) atomicAdd(&p.counters[5], (unsigned long long)multi);
+}
+
+// Re-search for candidates still alive (conflict-resolution rounds >= 2).
+__global__ void k_research(KParams p) {
+  const int nc = min(*p.ncand, p.candcap);
+  const uint32_t step = *p.step;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nc; t += gridDim.x * blockDim.x) {
+    const int i = p.cand[t];
+    const ull id = p.b_id[i];
+    if (id_species(id) == kDeadSpecies) continue;
+    int ncd;
+    p.best[i] = search_partner(p, i, p.b_pc[i], id, step, ncd);
+  }
+}
+
+// Site of a bimolecular reaction, in the local frame of molecule i
+// (x = D2/(D1+D2) weighting, smolreact.c:2693-2697).
+__device__ __forceinline__ float4 pair_site(const KParams &p, int i, int j, int r, int rep) {
+  const float4 a = p.b_pc[i], b = p.b_pc[j];
+  const DevGeo g = p.geo[rep];
+  int ia[3], ib[3];
+  unpack_cell(__float_as_uint(a.w), ia[0], ia[1], ia[2]);
+  unpack_cell(__float_as_uint(b.w), ib[0], ib[1], ib[2]);
+  const float ua[3] = {a.x, a.y, a.z}, ub[3] = {b.x, b.y, b.z};
+  const int spa = id_species(p.b_id[i]);
+  const int r1 = c_net.rct[2][r][0];
+  const int spb = id_species(p.b_id[j]);
+  const float da = p.difstep[rep * c_net.nsp + spa], db = p.difstep[rep * c_net.nsp + spb];
+  // difstep^2 is proportional to D, so the weights follow from difstep^2
+  const float Da = da * da, Db = db * db;
+  float fa;  // fraction of the way from a toward b
+  if (Da == 0.f && Db == 0.f) fa = 0.5f;
+  else fa = Da / (Da + Db);
+  (void)r1;
+  (void)spb;
+  int cell[3];
+  float w[3];
+  for (int d = 0; d < 3; ++d) {
+    int dc = ib[d] - ia[d];
+    if (dc > 1) dc -= g.n[d];
+    else if (dc < -1) dc += g.n[d];
+    const float v = (ub[d] - ua[d]) + (float)dc * g.h[d];
+    w[d] = ua[d] + fa * v;
+    cell[d] = ia[d];
+    renorm(w[d], cell[d], g.h[d], g.inv_h[d]);
+    int hits = 0;
+    if (cell[d] < 0 || cell[d] > g.n[d] - 1 || (cell[d] == g.n[d] - 1 && w[d] > g.whi[d]))
+      walls_dim(w[d], cell[d], g, d, hits);
+    clamp_cell(w[d], cell[d], g, d);
+  }
+  return make_float4(w[0], w[1], w[2], __uint_as_float(pack_cell(cell[0], cell[1], cell[2])));
+}
+
+__global__ void k_commit(KParams p) {
+  const int nc = min(*p.ncand, p.candcap);
+  const uint32_t step = *p.step;
+  int done = 0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nc; t += gridDim.x * blockDim.x) {
+    const int i = p.cand[t];
+    const ull bi = p.best[i];
+    if (bi == ~0ull) continue;
+    const int j = (int)(uint32_t)bi;
+    if (j <= i) continue;
+    const ull bj = p.best[j];
+    if ((int)(uint32_t)bj != i) continue;
+    const ull idi = p.b_id[i], idj = p.b_id[j];
+    const int spi = id_species(idi), spj = id_species(idj);
+    if (spi == kDeadSpecies || spj == kDeadSpecies) continue;
+    const int rep = id_rep(idi);
+    const float d2 = __uint_as_float((uint32_t)(bi >> 32));
+    const int r = pair_reaction(p, rep, spi, spj, d2, id_stream(idi), id_stream(idj), step);
+    if (r < 0) continue;
+    // reactant 1 of reaction r is molecule a
+    const bool i_first = (c_net.rct[2][r][0] == spi);
+    const int a = i_first ? i : j, b = i_first ? j : i;
+    Event e;
+    e.site = pair_site(p, a, b, r, rep);
+    const ull ka = id_stream(p.b_id[a]), kb = id_stream(p.b_id[b]);
+    e.key = mix64(ka * 0x9E3779B97F4A7C15ull ^ kb) & ((1ull << kSpShift) - 1);
+    e.rxn = (2u << 8) | (uint32_t)r;
+    e.rep = (uint32_t)rep;
+    push_event(p, e);
+    p.b_id[i] = id_mark_dead(idi);
+    p.b_id[j] = id_mark_dead(idj);
+    atomicAdd((unsigned long long *)&p.spcount[rep * c_net.nsp + spi], (unsigned long long)(-1ll));
+    atomicAdd((unsigned long long *)&p.spcount[rep * c_net.nsp + spj], (unsigned long long)(-1ll));
+    done++;
+  }
+  if (done) atomicAdd(&p.counters[3], (unsigned long long)done);
+}
+
+// ---- product placement -----------------------------------------------------
+// Uniformly random rotation matrix from a random unit quaternion (Shoemake,
+// Graphics Gems III, 1992).
+__device__ __forceinline__ void random_rotation(uint4 r, float m[9]) {
+  const float u1 = u01f_open(r.x), u2 = u01f_open(r.y) * 6.28318530718f, u3 = u01f_open(r.z) * 6.28318530718f;
+  const float s1 = sqrtf(1.f - u1), s2 = sqrtf(u1);
+  float sn2, cs2, sn3, cs3;
+  __sincosf(u2, &sn2, &cs2);
+  __sincosf(u3, &sn3, &cs3);
+  const float qx = s1 * sn2, qy = s1 * cs2, qz = s2 * sn3, qw = s2 * cs3;
+  m[0] = 1.f - 2.f * (qy * qy + qz * qz); m[1] = 2.f * (qx * qy - qz * qw); m[2] = 2.f * (qx * qz + qy * qw);
+  m[3] = 2.f * (qx * qy + qz * qw); m[4] = 1.f - 2.f * (qx * qx + qz * qz); m[5] = 2.f * (qy * qz - qx * qw);
+  m[6] = 2.f * (qx * qz - qy * qw); m[7] = 2.f * (qy * qz + qx * qw); m[8] = 1.f - 2.f * (qx * qx + qy * qy);
+}
+
+__global__ void k_products(KParams p) {
+  const int ne = min(*p.nev, p.evcap);
+  const uint32_t step = *p.step;
+  const uint2 key = make_uint2(c_net.key0 ^ 0x68E31DA4u, c_net.key1 ^ 0xB5297A4Du);
+  int uni = 0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ne; t += gridDim.x * blockDim.x) {
+    const Event e = p.ev[t];
+    const int order = (int)(e.rxn >> 8), r = (int)(e.rxn & 0xFF), rep = (int)e.rep;
+    const DevGeo g = p.geo[rep];
+    const uint4 rr = philox(make_uint4((uint32_t)e.key, (uint32_t)(e.key >> 32), step, 7u), key);
+    float site[3];
+    int cell[3];
+    if (order == 0) {  // uniform position in the system (smolwall.c:42)
+      const uint32_t bits[3] = {rr.x, rr.y, rr.z};
+      for (int d = 0; d < 3; ++d) {
+        if (d >= g.dim) { site[d] = 0.f; cell[d] = 0; continue; }
+        const float L = (float)(g.n[d] - 1) * g.h[d] + g.whi[d];
+        float w = u01f_open(bits[d]) * L;
+        int j = 0;
+        renorm(w, j, g.h[d], g.inv_h[d]);
+        if (j > g.n[d] - 1) { w += (float)(j - (g.n[d] - 1)) * g.h[d]; j = g.n[d] - 1; }
+        clamp_cell(w, j, g, d);
+        site[d] = w;
+        cell[d] = j;
+      }
+    } else {
+      site[0] = e.site.x; site[1] = e.site.y; site[2] = e.site.z;
+      unpack_cell(__float_as_uint(e.site.w), cell[0], cell[1], cell[2]);
+      if (order == 1) {
+        uni++;
+        atomicAdd((unsigned long long *)&p.spcount[rep * c_net.nsp + c_net.rct[1][r][0]],
+                  (unsigned long long)(-1ll));
+      }
+    }
+    const int np = c_net.nprod[order][r];
+    float m[9];
+    bool rot = false;
+    if (c_net.has_offset[order][r] && !c_net.fixed[order][r] && !c_net.inject) {
+      random_rotation(philox(make_uint4((uint32_t)e.key, (uint32_t)(e.key >> 32), step, 8u), key), m);
+      rot = true;
+    }
+    const int kx = c_net.rxn_base[order] + r;
+    for (int q = 0; q < np; ++q) {
+      const int psp = c_net.prd[order][r][q];
+      float off[3] = {0.f, 0.f, 0.f};
+      if (c_net.has_offset[order][r]) {
+        const float *pp = p.prdpos + ((size_t)(rep * c_net.nrx_total + kx) * kMaxProd + q) * 3;
+        if (rot) {
+          off[0] = m[0] * pp[0] + m[1] * pp[1] + m[2] * pp[2];
+          off[1] = m[3] * pp[0] + m[4] * pp[1] + m[5] * pp[2];
+          off[2] = m[6] * pp[0] + m[7] * pp[1] + m[8] * pp[2];
+        } else {
+          off[0] = pp[0]; off[1] = pp[1]; off[2] = pp[2];
+        }
+      }
+      float w[3];
+      int c[3];
+      bool dead = false;
+      int hits = 0;
+      for (int d = 0; d < 3; ++d) {
+        w[d] = site[d] + (d < g.dim ? off[d] : 0.f);
+        c[d] = cell[d];
+        renorm(w[d], c[d], g.h[d], g.inv_h[d]);
+        if (d < g.dim && (c[d] <= 0 || c[d] >= g.n[d] - 1))
+          if (walls_dim(w[d], c[d], g, d, hits)) dead = true;
+        clamp_cell(w[d], c[d], g, d);
+      }
+      if (hits) atomicAdd(&p.counters[0], (unsigned long long)hits);
+      if (dead) continue;
+      const ull serno = kProductSernoBit |
+                        (mix64(e.key ^ ((ull)q << 50) ^ ((ull)step << 20) ^ (ull)(order * 97 + r)) &
+                         (kProductSernoBit - 1));
+      const int slot = atomicAdd(p.q_n, 1);
+      if (slot < p.pcap) {
+        p.q_pc[slot] = make_float4(w[0], w[1], w[2], __uint_as_float(pack_cell(c[0], c[1], c[2])));
+        p.q_id[slot] = make_id(psp, rep, serno);
+        atomicAdd((unsigned long long *)&p.spcount[rep * c_net.nsp + psp], 1ull);
+      } else {
+        atomicOr(p.status, kStProdCap);
+      }
+    }
+  }
+  if (uni) atomicAdd(&p.counters[2], (unsigned long long)uni);
+  // clear the candidate keys of this step
+  const int nc = min(*p.ncand, p.candcap);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nc; t += gridDim.x * blockDim.x)
+    p.best[p.cand[t]] = ~0ull;
+}
+
+__global__ void k_fix_count(int *q_n, int pcap) {
+  if (threadIdx.x == 0 && *q_n > pcap) *q_n = pcap;
+}
+
+// Count live molecules per (rep, species) from scratch (used after uploads).
+__global__ void k_species_count(const ull *id, const int *n, long long *spcount, int nsp) {
+  const int nn = *n;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
+    const ull x = id[i];
+    const int sp = id_species(x);
+    if (sp == kDeadSpecies) continue;
+    atomicAdd((unsigned long long *)&spcount[id_rep(x) * nsp + sp], 1ull);
+  }
+}
+
+// Batched FP64 radius solve (one thread per problem).
+__global__ void k_solve_radii(int mode, long long n, const double *rate, double dt, const double *difc,
+                              const double *b, int rel, double *out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    if (mode == 0) out[i] = rxnp::bindingradius(rate[i], dt, difc[i], b[i], rel);
+    else out[i] = rxnp::unbindingradius(rate[i], dt, difc[i], b[i]);
+  }
+}
+
+// ===========================================================================
+// Host driver
+// ===========================================================================
+#define CK(call)                                                                        \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess) {                                                            \
+      if (err) *err = std::string(#call) + ": " + cudaGetErrorString(e_);               \
+      return -8;                                                                        \
+    }                                                                                   \
+  } while (0)
+
+static int g_sm_count = 0;
+
+static int sm_count() {
+  if (!g_sm_count) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sm_count <= 0) g_sm_count = 148;
+  }
+  return g_sm_count;
+}
+
+class EngineImpl {
+ public:
+  NetSpec net;
+  std::vector<RepSpec> reps;
+  DevNet dnet{};
+  std::vector<DevGeo> geo;
+  std::vector<DevPanel> panels;
+  double dt = 0;
+  uint64_t seed = 0;
+  long long cap = 0, pcap = 0, evcap = 0, candcap = 0;
+  int ncell = 0, nscanblocks = 0;
+  cudaStream_t own_stream = nullptr, stream = nullptr;
+  bool use_graph = true;
+  cudaGraphExec_t graph2 = nullptr;  // two steps (even + odd parity)
+  long long nlaunch = 0;
+  long long nsteps = 0;
+  int parity = 0;  // 0: A/P are inputs; 1: B/Q are inputs
+
+  // device memory
+  DevGeo *d_geo = nullptr;
+  float *d_difstep = nullptr, *d_driftdt = nullptr, *d_bind2 = nullptr, *d_pairprob = nullptr,
+        *d_prdpos = nullptr, *d_gtab = nullptr;
+  uint32_t *d_unithr = nullptr;
+  double *d_births = nullptr;
+  float4 *d_pc[2] = {nullptr, nullptr}, *d_ppc[2] = {nullptr, nullptr};
+  ull *d_id[2] = {nullptr, nullptr}, *d_pid[2] = {nullptr, nullptr};
+  int *d_counts = nullptr;  // [0]=n sorted A [1]=n sorted B [2]=n prod P [3]=n prod Q [4]=nev [5]=ncand [6]=status
+  uint32_t *d_step = nullptr;
+  int *d_cnt = nullptr, *d_start = nullptr, *d_bsum = nullptr;
+  Event *d_ev = nullptr;
+  int *d_cand = nullptr;
+  ull *d_best = nullptr;
+  unsigned long long *d_counters = nullptr;
+  long long *d_spcount = nullptr;
+  ull *d_injkey = nullptr;
+  float4 *d_injval = nullptr;
+  int inj_n = 0;
+  bool inj_pending = false;
+
+  ~EngineImpl() {
+    release();
+    for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
+  }
+
+  void release() {
+    if (graph2) cudaGraphExecDestroy(graph2);
+    graph2 = nullptr;
+    void *ptrs[] = {d_geo, d_difstep, d_driftdt, d_bind2, d_pairprob, d_prdpos, d_gtab, d_unithr,
+                    d_births, d_pc[0], d_pc[1], d_ppc[0], d_ppc[1], d_id[0], d_id[1], d_pid[0],
+                    d_pid[1], d_counts, d_step, d_cnt, d_start, d_bsum, d_ev, d_cand, d_best,
+                    d_counters, d_spcount, d_injkey, d_injval};
+    for (void *q : ptrs)
+      if (q) cudaFree(q);
+    d_geo = nullptr; d_difstep = d_driftdt = d_bind2 = d_pairprob = d_prdpos = d_gtab = nullptr;
+    d_unithr = nullptr; d_births = nullptr;
+    d_pc[0] = d_pc[1] = d_ppc[0] = d_ppc[1] = nullptr;
+    d_id[0] = d_id[1] = d_pid[0] = d_pid[1] = nullptr;
+    d_counts = nullptr; d_step = nullptr; d_cnt = d_start = d_bsum = nullptr; d_ev = nullptr;
+    d_cand = nullptr; d_best = nullptr; d_counters = nullptr; d_spcount = nullptr;
+    d_injkey = nullptr; d_injval = nullptr;
+    if (own_stream) cudaStreamDestroy(own_stream);
+    own_stream = nullptr;
+  }
+
+  KParams params(int par) const {
+    KParams p{};
+    p.geo = d_geo;
+    p.difstep = d_difstep;
+    p.driftdt = d_driftdt;
+    p.unithr = d_unithr;
+    p.bind2 = d_bind2;
+    p.pairprob = d_pairprob;
+    p.births = d_births;
+    p.prdpos = d_prdpos;
+    p.gtab = d_gtab;
+    const int in = par, out = 1 - par;
+    p.a_pc = d_pc[in]; p.a_id = d_id[in]; p.a_n = d_counts + in;
+    p.p_pc = d_ppc[in]; p.p_id = d_pid[in]; p.p_n = d_counts + 2 + in;
+    p.b_pc = d_pc[out]; p.b_id = d_id[out]; p.b_n = d_counts + out;
+    p.q_pc = d_ppc[out]; p.q_id = d_pid[out]; p.q_n = d_counts + 2 + out;
+    p.cap = (int)cap;
+    p.pcap = (int)pcap;
+    p.cnt = d_cnt;
+    p.start = d_start;
+    p.ncell = ncell;
+    p.blocksums = d_bsum;
+    p.ev = d_ev;
+    p.nev = d_counts + 4;
+    p.evcap = (int)evcap;
+    p.cand = d_cand;
+    p.ncand = d_counts + 5;
+    p.candcap = (int)candcap;
+    p.best = d_best;
+    p.counters = d_counters;
+    p.spcount = d_spcount;
+    p.status = d_counts + 6;
+    p.step = d_step;
+    p.inj_key = d_injkey;
+    p.inj_val = d_injval;
+    p.inj_n = inj_n;
+    return p;
+  }
+
+  int grid_mol() const { return sm_count() * 4; }
+  int grid_small() const { return sm_count(); }
+
+  size_t adv_smem() const {
+    const int gsize = (int)dnet.gmask + 1;
+    return gsize <= 8192 ? (size_t)gsize * sizeof(float) : 0;
+  }
+
+  // per-kernel timing (profiling mode only)
+  bool prof = false;
+  std::vector<std::pair<const char *, cudaEvent_t>> marks;
+  std::vector<cudaEvent_t> event_pool;
+  size_t pool_used = 0;
+
+  void mark(const char *name) {
+    ++nlaunch;
+    if (!prof) return;
+    if (pool_used == event_pool.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      event_pool.push_back(e);
+    }
+    cudaEvent_t e = event_pool[pool_used++];
+    cudaEventRecord(e, stream);
+    marks.push_back({name, e});
+  }
+
+  // Enqueue one step with the given parity.
+  void enqueue_step(int par, bool rebin_only) {
+    KParams p = params(par);
+    cudaStream_t s = stream;
+    k_begin<<<1, 32, 0, s>>>(p, rebin_only ? 0 : 1);
+    mark("k_begin");
+    const int ph = rebin_only ? 2 : 0;
+    k_advance<<<grid_mol(), 256, rebin_only ? 0 : adv_smem(), s>>>(p, ph | 0);
+    mark("k_advance_count");
+    k_scan_reduce<<<nscanblocks, kScanThreads, 0, s>>>(d_cnt, ncell, d_bsum);
+    mark("k_scan_reduce");
+    k_scan_blocks<<<1, 1024, 0, s>>>(d_bsum, nscanblocks);
+    mark("k_scan_blocks");
+    k_scan_apply<<<nscanblocks, kScanThreads, 0, s>>>(d_cnt, ncell, d_bsum, nscanblocks, d_start,
+                                                      p.b_n, (int)cap);
+    mark("k_scan_apply");
+    k_advance<<<grid_mol(), 256, rebin_only ? 0 : adv_smem(), s>>>(p, ph | 1);
+    mark("k_advance_scatter");
+    if (rebin_only) return;
+    k_births<<<grid_small(), 128, 0, s>>>(p);
+    mark("k_births");
+    k_pairs<<<grid_mol(), 256, 0, s>>>(p);
+    mark("k_pairs");
+    k_commit<<<grid_small(), 128, 0, s>>>(p);
+    mark("k_commit");
+    for (int round = 1; round < dnet.rounds; ++round) {
+      k_research<<<grid_small(), 128, 0, s>>>(p);
+      mark("k_research");
+      k_commit<<<grid_small(), 128, 0, s>>>(p);
+      mark("k_commit");
+    }
+    k_products<<<grid_small(), 128, 0, s>>>(p);
+    mark("k_products");
+    k_fix_count<<<1, 32, 0, s>>>(p.q_n, (int)pcap);
+    mark("k_fix_count");
+  }
+
+  int launches_per_step() const { return 11 + 2 * (dnet.rounds - 1); }
+
+  int upload_const(std::string *err) {
+    CK(cudaMemcpyToSymbolAsync(c_net, &dnet, sizeof(DevNet), 0, cudaMemcpyHostToDevice, stream));
+    if (!panels.empty())
+      CK(cudaMemcpyToSymbolAsync(c_panels, panels.data(), panels.size() * sizeof(DevPanel), 0,
+                                 cudaMemcpyHostToDevice, stream));
+    return 0;
+  }
+
+  int build_rep_tables(std::string *err) {
+    const int R = (int)reps.size(), nsp = net.nspecies;
+    std::vector<float> difstep((size_t)R * nsp), driftdt((size_t)R * nsp * 3);
+    std::vector<uint32_t> unithr((size_t)R * nsp * kMaxUniPerSpecies, 0);
+    const int nr2 = std::max(1, net.nrxn[2]), nr0 = std::max(1, net.nrxn[0]);
+    std::vector<float> bind2((size_t)R * nr2, 0.f), pairprob((size_t)R * nr2, 1.f);
+    std::vector<double> births((size_t)R * nr0, 0.0);
+    const int nrx = std::max(1, dnet.nrx_total);
+    std::vector<float> prdpos((size_t)R * nrx * kMaxProd * 3, 0.f);
+    bool any_drift = false;
+    for (int rp = 0; rp < R; ++rp) {
+      const RepSpec &s = reps[rp];
+      for (int sp = 0; sp < nsp; ++sp) {
+        difstep[(size_t)rp * nsp + sp] = (float)std::sqrt(2.0 * s.difc[sp] * dt);
+        for (int d = 0; d < 3; ++d) {
+          driftdt[((size_t)rp * nsp + sp) * 3 + d] = (float)(s.drift[sp][d] * dt);
+          if (s.drift[sp][d] != 0) any_drift = true;
+        }
+        // cumulative thresholds: reaction k of the species fires with probability
+        // prob_k * prod_{m<k}(1-prob_m) (sequential coins of smolreact.c:3036-3055)
+        double surv = 1.0, cum = 0.0;
+        for (int m = 0; m < dnet.uni_n[sp]; ++m) {
+          const int r = dnet.uni_list[sp][m];
+          const double pr = std::min(1.0, std::max(0.0, s.uni_prob[r]));
+          cum += pr * surv;
+          surv *= (1.0 - pr);
+          const double t = std::min(4294967295.0, std::floor(cum * 4294967296.0));
+          unithr[((size_t)rp * nsp + sp) * kMaxUniPerSpecies + m] = (uint32_t)t;
+        }
+      }
+      for (int r = 0; r < net.nrxn[2]; ++r) {
+        bind2[(size_t)rp * nr2 + r] = (float)s.bind2[r];
+        pairprob[(size_t)rp * nr2 + r] = (float)s.pair_prob[r];
+      }
+      for (int r = 0; r < net.nrxn[0]; ++r) births[(size_t)rp * nr0 + r] = s.birth_mean[r];
+      for (int o = 0; o < 3; ++o)
+        for (int r = 0; r < net.nrxn[o]; ++r)
+          for (int q = 0; q < kMaxProd; ++q)
+            for (int d = 0; d < 3; ++d)
+              prdpos[(((size_t)rp * nrx + dnet.rxn_base[o] + r) * kMaxProd + q) * 3 + d] =
+                  (float)s.prdpos[o][r][q][d];
+    }
+    dnet.any_drift = any_drift ? 1 : 0;
+    auto put = [&](void **dst, const void *src, size_t bytes) -> int {
+      if (!*dst) CK(cudaMalloc(dst, bytes));
+      CK(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, stream));
+      return 0;
+    };
+    if (put((void **)&d_difstep, difstep.data(), difstep.size() * 4)) return -8;
+    if (put((void **)&d_driftdt, driftdt.data(), driftdt.size() * 4)) return -8;
+    if (put((void **)&d_unithr, unithr.data(), unithr.size() * 4)) return -8;
+    if (put((void **)&d_bind2, bind2.data(), bind2.size() * 4)) return -8;
+    if (put((void **)&d_pairprob, pairprob.data(), pairprob.size() * 4)) return -8;
+    if (put((void **)&d_births, births.data(), births.size() * 8)) return -8;
+    if (put((void **)&d_prdpos, prdpos.data(), prdpos.size() * 4)) return -8;
+    // the host copies are staged; wait before the vectors go out of scope
+    CK(cudaStreamSynchronize(stream));
+    return upload_const(err);
+  }
+
+  void invalidate_graph() {
+    if (graph2) cudaGraphExecDestroy(graph2);
+    graph2 = nullptr;
+  }
+
+  int build_graph(std::string *err) {
+    invalidate_graph();
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    const long long before = nlaunch;
+    const bool was = prof;
+    prof = false;
+    enqueue_step(0, false);
+    enqueue_step(1, false);
+    prof = was;
+    nlaunch = before;
+    CK(cudaStreamEndCapture(stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&graph2, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      graph2 = nullptr;
+      if (err) *err = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e);
+      return -8;
+    }
+    return 0;
+  }
+};
+
+Engine::Engine() : impl_(new EngineImpl) {}
+Engine::~Engine() { delete impl_; }
+
+static float f_of(double x) { return (float)x; }
+
+int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt, uint64_t seed,
+                 long long capacity, std::string *err) {
+  EngineImpl &E = *impl_;
+  E.release();
+  E.net = net;
+  E.reps = reps;
+  E.dt = dt;
+  E.seed = seed;
+  if (reps.empty() || reps.size() > 65536) { if (err) *err = "replicate count must be 1..65536"; return -6; }
+  if (net.nspecies > kMaxSpecies) { if (err) *err = "too many species for the GPU engine (max 31)"; return -6; }
+  for (int o = 0; o < 3; ++o)
+    if (net.nrxn[o] > kMaxRxn) { if (err) *err = "too many reactions of one order (max 16)"; return -6; }
+  int gs = net.gauss_table_size;
+  if (gs < 2 || gs > 65536 || (gs & (gs - 1))) { if (err) *err = "gauss table size must be a power of 2 <= 65536"; return -6; }
+  if (!E.own_stream) CK(cudaStreamCreateWithFlags(&E.own_stream, cudaStreamNonBlocking));
+  if (!E.stream) E.stream = E.own_stream;
+
+  // ---- network constants
+  DevNet &D = E.dnet;
+  memset(&D, 0, sizeof(D));
+  D.nsp = net.nspecies;
+  D.nrep = (int)reps.size();
+  for (int o = 0; o < 3; ++o) D.nr[o] = net.nrxn[o];
+  D.rxn_base[0] = 0;
+  D.rxn_base[1] = net.nrxn[0];
+  D.rxn_base[2] = net.nrxn[0] + net.nrxn[1];
+  D.nrx_total = net.nrxn[0] + net.nrxn[1] + net.nrxn[2];
+  D.gmask = (uint32_t)(gs - 1);
+  D.key0 = (uint32_t)seed ^ 0xA511E9B3u;
+  D.key1 = (uint32_t)(seed >> 32) ^ 0x63D83595u;
+  D.rounds = 3;
+  D.npanel = (int)net.panels.size();
+  for (int r = 0; r < net.nrxn[1]; ++r) {
+    const int sp = net.rct[1][r][0];
+    if (D.uni_n[sp] >= kMaxUniPerSpecies) { if (err) *err = "too many first-order reactions for one species"; return -6; }
+    D.uni_list[sp][D.uni_n[sp]++] = (uint8_t)r;
+    D.rct[1][r][0] = (uint8_t)sp;
+  }
+  for (int r = 0; r < net.nrxn[2]; ++r) {
+    const int a = net.rct[2][r][0], b = net.rct[2][r][1];
+    D.rct[2][r][0] = (uint8_t)a;
+    D.rct[2][r][1] = (uint8_t)b;
+    for (int pass = 0; pass < (a == b ? 1 : 2); ++pass) {
+      const int x = pass ? b : a, y = pass ? a : b;
+      if (D.pair_n[x][y] >= kMaxPairRxn) { if (err) *err = "too many reactions for one reactant pair"; return -6; }
+      D.pair_list[x][y][D.pair_n[x][y]++] = (uint8_t)r;
+      D.pair_mask[x] |= 1u << y;
+    }
+  }
+  for (int o = 0; o < 3; ++o)
+    for (int r = 0; r < net.nrxn[o]; ++r) {
+      D.nprod[o][r] = (uint8_t)net.nprod[o][r];
+      D.fixed[o][r] = (uint8_t)net.fixed_placement[o][r];
+      for (int q = 0; q < net.nprod[o][r]; ++q) D.prd[o][r][q] = (uint8_t)net.prd[o][r][q];
+      bool off = false;
+      for (const RepSpec &s : reps)
+        for (int q = 0; q < net.nprod[o][r]; ++q)
+          for (int d = 0; d < 3; ++d)
+            if (s.prdpos[o][r][q][d] != 0) off = true;
+      D.has_offset[o][r] = off ? 1 : 0;
+    }
+
+  // ---- replicate geometry
+  E.geo.resize(reps.size());
+  long long cells = 0;
+  bool any_absorb = false;
+  for (size_t k = 0; k < reps.size(); ++k) {
+    const RepSpec &s = reps[k];
+    DevGeo &g = E.geo[k];
+    memset(&g, 0, sizeof(g));
+    g.dim = s.dim;
+    for (int d = 0; d < 3; ++d) {
+      int n = std::max(1, s.ncell[d]);
+      const double L = s.hi[d] - s.lo[d];
+      if (d < s.dim && (s.wall[2 * d] == kWallPeriodic || s.wall[2 * d + 1] == kWallPeriodic) && n < 3) n = 3;
+      if (n > 1023) n = 1023;
+      const double h = (d < s.dim) ? L / n : 1.0;
+      g.n[d] = n;
+      g.h[d] = f_of(h);
+      g.inv_h[d] = 1.0f / g.h[d];
+      g.whi[d] = (d < s.dim) ? f_of(L - (n - 1) * h) : f_of(h);
+      g.wall[2 * d] = (d < s.dim) ? s.wall[2 * d] : kWallTransparent;
+      g.wall[2 * d + 1] = (d < s.dim) ? s.wall[2 * d + 1] : kWallTransparent;
+      if (g.wall[2 * d] == kWallAbsorb || g.wall[2 * d + 1] == kWallAbsorb) any_absorb = true;
+    }
+    g.vol = (float)((s.hi[0] - s.lo[0]) * (s.dim > 1 ? s.hi[1] - s.lo[1] : 1) * (s.dim > 2 ? s.hi[2] - s.lo[2] : 1));
+    g.cell0 = (int)cells;
+    cells += (long long)g.n[0] * g.n[1] * g.n[2];
+    if (cells > (1ll << 30)) { if (err) *err = "too many virtual boxes"; return -6; }
+  }
+  D.any_absorb = any_absorb ? 1 : 0;
+  E.ncell = (int)cells;
+  E.nscanblocks = (E.ncell + kScanTile - 1) / kScanTile;
+
+  // ---- capacities
+  E.cap = std::max<long long>(capacity, 1024);
+  E.pcap = std::max<long long>(E.cap / 4, 65536);
+  E.evcap = std::max<long long>(E.cap / 8, 32768);
+  E.candcap = std::max<long long>(E.cap / 8, 32768);
+  if (E.cap > (1ll << 31) - 2) { if (err) *err = "molecule capacity too large"; return -6; }
+
+  CK(cudaMalloc(&E.d_geo, E.geo.size() * sizeof(DevGeo)));
+  CK(cudaMemcpyAsync(E.d_geo, E.geo.data(), E.geo.size() * sizeof(DevGeo), cudaMemcpyHostToDevice, E.stream));
+  for (int k = 0; k < 2; ++k) {
+    CK(cudaMalloc(&E.d_pc[k], E.cap * sizeof(float4)));
+    CK(cudaMalloc(&E.d_id[k], E.cap * sizeof(ull)));
+    CK(cudaMalloc(&E.d_ppc[k], E.pcap * sizeof(float4)));
+    CK(cudaMalloc(&E.d_pid[k], E.pcap * sizeof(ull)));
+  }
+  CK(cudaMalloc(&E.d_counts, 16 * sizeof(int)));
+  CK(cudaMemsetAsync(E.d_counts, 0, 16 * sizeof(int), E.stream));
+  CK(cudaMalloc(&E.d_step, sizeof(uint32_t)));
+  CK(cudaMemsetAsync(E.d_step, 0, sizeof(uint32_t), E.stream));
+  CK(cudaMalloc(&E.d_cnt, ((size_t)E.ncell + 1) * sizeof(int)));
+  CK(cudaMemsetAsync(E.d_cnt, 0, ((size_t)E.ncell + 1) * sizeof(int), E.stream));
+  CK(cudaMalloc(&E.d_start, ((size_t)E.ncell + 1) * sizeof(int)));
+  CK(cudaMemsetAsync(E.d_start, 0, ((size_t)E.ncell + 1) * sizeof(int), E.stream));
+  CK(cudaMalloc(&E.d_bsum, ((size_t)E.nscanblocks + 1) * sizeof(int)));
+  CK(cudaMalloc(&E.d_ev, E.evcap * sizeof(Event)));
+  CK(cudaMalloc(&E.d_cand, E.candcap * sizeof(int)));
+  CK(cudaMalloc(&E.d_best, E.cap * sizeof(ull)));
+  CK(cudaMemsetAsync(E.d_best, 0xFF, E.cap * sizeof(ull), E.stream));
+  CK(cudaMalloc(&E.d_counters, 8 * sizeof(unsigned long long)));
+  CK(cudaMemsetAsync(E.d_counters, 0, 8 * sizeof(unsigned long long), E.stream));
+  CK(cudaMalloc(&E.d_spcount, (size_t)reps.size() * net.nspecies * sizeof(long long)));
+  CK(cudaMemsetAsync(E.d_spcount, 0, (size_t)reps.size() * net.nspecies * sizeof(long long), E.stream));
+
+  // gaussian quantile table: sqrt(2)*erfinv((i+1/2)*2/n - 1) (random2.c:339-352);
+  // the reference shuffles it, which does not matter for counter-based indices
+  {
+    std::vector<float> gt(gs);
+    for (int i = 0; i < gs / 2; ++i) {
+      const double pq = (i + 0.5) / gs;  // lower-tail probability
+      double lo = -40, hi = 0;           // solve 0.5*erfc(-x/sqrt2) = pq by bisection
+      for (int it = 0; it < 200; ++it) {
+        const double mid = 0.5 * (lo + hi);
+        if (0.5 * std::erfc(-mid / std::sqrt(2.0)) < pq) lo = mid;
+        else hi = mid;
+      }
+      gt[i] = (float)(0.5 * (lo + hi));
+      gt[gs - 1 - i] = -gt[i];
+    }
+    CK(cudaMalloc(&E.d_gtab, gs * sizeof(float)));
+    CK(cudaMemcpyAsync(E.d_gtab, gt.data(), gs * sizeof(float), cudaMemcpyHostToDevice, E.stream));
+    CK(cudaStreamSynchronize(E.stream));
+  }
+  if (!E.net.panels.empty()) {
+    if ((int)E.net.panels.size() > kMaxPanels) { if (err) *err = "too many panels (max 16)"; return -6; }
+    E.panels.clear();
+    for (const PanelSpec &ps : E.net.panels) {
+      DevPanel dp{};
+      const RepSpec &s0 = reps[0];
+      dp.shape = ps.shape;
+      dp.axis = ps.axis;
+      dp.front_sign = ps.front_sign;
+      dp.pos = (float)(ps.pos - s0.lo[ps.axis]);
+      for (int d = 0; d < 3; ++d) {
+        dp.lo[d] = (float)(ps.lo[d] - s0.lo[d]);
+        dp.hi[d] = (float)(ps.hi[d] - s0.lo[d]);
+        dp.center[d] = (float)(ps.center[d] - s0.lo[d]);
+      }
+      dp.radius = (float)ps.radius;
+      dp.act_front = ps.action_front;
+      dp.act_back = ps.action_back;
+      dp.abs_front = ps.absorb_front_mask;
+      dp.abs_back = ps.absorb_back_mask;
+      dp.tr_front = ps.trans_front_mask;
+      dp.tr_back = ps.trans_back_mask;
+      E.panels.push_back(dp);
+    }
+  }
+  int rc = E.build_rep_tables(err);
+  if (rc) return rc;
+  CK(cudaFuncSetAttribute(k_advance, cudaFuncAttributeMaxDynamicSharedMemorySize, 32768));
+  E.nsteps = 0;
+  E.parity = 0;
+  return 0;
+}
+
+int Engine::update_reps(const std::vector<RepSpec> &reps, std::string *err) {
+  EngineImpl &E = *impl_;
+  if (reps.size() != E.reps.size()) { if (err) *err = "replicate count changed"; return -6; }
+  E.reps = reps;
+  return E.build_rep_tables(err);
+}
+
+int Engine::set_molecules(long long n, const double *pos, const int *species, const int *rep,
+                          const uint64_t *serno, std::string *err) {
+  EngineImpl &E = *impl_;
+  if (n > E.pcap) {
+    // grow the product buffers so the upload fits (they are the upload staging area)
+    for (int k = 0; k < 2; ++k) {
+      cudaFree(E.d_ppc[k]);
+      cudaFree(E.d_pid[k]);
+      E.d_ppc[k] = nullptr;
+      E.d_pid[k] = nullptr;
+    }
+    E.pcap = n;
+    for (int k = 0; k < 2; ++k) {
+      CK(cudaMalloc(&E.d_ppc[k], E.pcap * sizeof(float4)));
+      CK(cudaMalloc(&E.d_pid[k], E.pcap * sizeof(ull)));
+    }
+    E.invalidate_graph();
+  }
+  if (n > E.cap) { if (err) *err = "more molecules than the engine capacity"; return -9; }
+  std::vector<float4> pc((size_t)n);
+  std::vector<ull> id((size_t)n);
+  std::vector<ull> next_serno(E.reps.size(), 1);
+  if (serno)
+    for (long long i = 0; i < n; ++i) {
+      const int rp = rep ? rep[i] : 0;
+      if (rp >= 0 && rp < (int)E.reps.size()) next_serno[rp] = std::max<ull>(next_serno[rp], (ull)serno[i] + 1);
+    }
+  for (long long i = 0; i < n; ++i) {
+    const int rp = rep ? rep[i] : 0;
+    if (rp < 0 || rp >= (int)E.reps.size()) { if (err) *err = "replicate index out of range"; return -6; }
+    const int sp = species[i];
+    if (sp <= 0 || sp >= E.net.nspecies) { if (err) *err = "species index out of range"; return -6; }
+    const RepSpec &s = E.reps[rp];
+    const DevGeo &g = E.geo[rp];
+    int ix[3];
+    float w[3];
+    for (int d = 0; d < 3; ++d) {
+      if (d >= s.dim) { ix[d] = 0; w[d] = 0.f; continue; }
+      const double L = s.hi[d] - s.lo[d];
+      const double h = L / g.n[d];
+      const double x = pos[3 * i + d] - s.lo[d];
+      int j = (int)std::floor(x / h);
+      if (j < 0) j = 0;
+      if (j > g.n[d] - 1) j = g.n[d] - 1;
+      ix[d] = j;
+      w[d] = (float)(x - j * h);
+    }
+    pc[i] = make_float4(w[0], w[1], w[2], 0.f);
+    uint32_t packed = pack_cell(ix[0], ix[1], ix[2]);
+    memcpy(&pc[i].w, &packed, 4);
+    ull sn = (serno && serno[i]) ? (ull)serno[i] : next_serno[rp]++;
+    id[i] = make_id(sp, rp, sn);
+  }
+  int zero[16] = {0};
+  int staged = (int)n;
+  CK(cudaMemcpyAsync(E.d_counts, zero, sizeof(zero), cudaMemcpyHostToDevice, E.stream));
+  E.parity = 0;
+  CK(cudaMemcpyAsync(E.d_ppc[0], pc.data(), n * sizeof(float4), cudaMemcpyHostToDevice, E.stream));
+  CK(cudaMemcpyAsync(E.d_pid[0], id.data(), n * sizeof(ull), cudaMemcpyHostToDevice, E.stream));
+  CK(cudaMemcpyAsync(E.d_counts + 2, &staged, sizeof(int), cudaMemcpyHostToDevice, E.stream));
+  CK(cudaMemsetAsync(E.d_cnt, 0, ((size_t)E.ncell + 1) * sizeof(int), E.stream));
+  E.enqueue_step(0, true);  // rebin only: P[0] -> sorted B (index 1)
+  // sorted array now in buffer 1; make it the input of the next step
+  E.parity = 1;
+  CK(cudaMemsetAsync(E.d_counts + 2, 0, 2 * sizeof(int), E.stream));
+  CK(cudaMemsetAsync(E.d_spcount, 0, E.reps.size() * E.net.nspecies * sizeof(long long), E.stream));
+  k_species_count<<<E.grid_mol(), 256, 0, E.stream>>>(E.d_id[1], E.d_counts + 1, E.d_spcount, E.net.nspecies);
+  E.nlaunch++;
+  CK(cudaStreamSynchronize(E.stream));
+  CK(cudaGetLastError());
+  int st = 0;
+  CK(cudaMemcpy(&st, E.d_counts + 6, sizeof(int), cudaMemcpyDeviceToHost));
+  if (st) { if (err) *err = "capacity overflow during upload"; return -9; }
+  return 0;
+}
+
+int Engine::run(long long nsteps, std::string *err) {
+  EngineImpl &E = *impl_;
+  if (nsteps <= 0) return 0;
+  const bool inj = E.dnet.inject != 0;
+  if (inj) {
+    if (nsteps != 1) { if (err) *err = "injected displacements apply to one step"; return -6; }
+  }
+  long long done = 0;
+  if (E.use_graph && !inj) {
+    // odd parity first step if needed so that graph replays start at parity 0
+    if (E.parity == 1) {
+      E.enqueue_step(1, false);
+      E.parity = 0;
+      done++;
+    }
+    if (nsteps - done >= 2 && !E.graph2) {
+      int rc = E.build_graph(err);
+      if (rc) return rc;
+    }
+    while (nsteps - done >= 2) {
+      CK(cudaGraphLaunch(E.graph2, E.stream));
+      E.nlaunch += 2 * E.launches_per_step();
+      done += 2;
+    }
+  }
+  while (done < nsteps) {
+    E.enqueue_step(E.parity, false);
+    E.parity ^= 1;
+    done++;
+  }
+  E.nsteps += nsteps;
+  CK(cudaGetLastError());
+  if (inj) {
+    E.dnet.inject = 0;
+    CK(cudaMemcpyToSymbolAsync(c_net, &E.dnet, sizeof(DevNet), 0, cudaMemcpyHostToDevice, E.stream));
+    CK(cudaStreamSynchronize(E.stream));
+  }
+  return 0;
+}
+
+int Engine::synchronize(std::string *err) {
+  CK(cudaStreamSynchronize(impl_->stream));
+  return 0;
+}
+
+int Engine::status_flags() {
+  int st = 0;
+  cudaStreamSynchronize(impl_->stream);
+  cudaMemcpy(&st, impl_->d_counts + 6, sizeof(int), cudaMemcpyDeviceToHost);
+  return st;
+}
+
+long long Engine::total_molecules() {
+  EngineImpl &E = *impl_;
+  int c[4] = {0, 0, 0, 0};
+  cudaStreamSynchronize(E.stream);
+  cudaMemcpy(c, E.d_counts, sizeof(c), cudaMemcpyDeviceToHost);
+  std::vector<long long> sc;
+  std::string err;
+  if (species_counts(&sc, &err)) return -1;
+  long long t = 0;
+  for (long long v : sc) t += v;
+  return t;
+}
+
+int Engine::species_counts(std::vector<long long> *out, std::string *err) {
+  EngineImpl &E = *impl_;
+  out->assign(E.reps.size() * E.net.nspecies, 0);
+  CK(cudaMemcpyAsync(out->data(), E.d_spcount, out->size() * sizeof(long long), cudaMemcpyDeviceToHost, E.stream));
+  CK(cudaStreamSynchronize(E.stream));
+  return 0;
+}
+
+int Engine::stats(EngineStats *s, std::string *err) {
+  EngineImpl &E = *impl_;
+  unsigned long long c[8];
+  CK(cudaMemcpyAsync(c, E.d_counters, sizeof(c), cudaMemcpyDeviceToHost, E.stream));
+  int st = 0;
+  CK(cudaMemcpyAsync(&st, E.d_counts + 6, sizeof(int), cudaMemcpyDeviceToHost, E.stream));
+  CK(cudaStreamSynchronize(E.stream));
+  s->wall = (long long)c[0];
+  s->rxn0 = (long long)c[1];
+  s->rxn1 = (long long)c[2];
+  s->rxn2 = (long long)c[3];
+  s->unresolved = (long long)c[4];
+  s->multicand = (long long)c[5];
+  s->overflow = st;
+  return 0;
+}
+
+int Engine::get_molecules(std::vector<double> *pos, std::vector<int> *species, std::vector<int> *rep,
+                          std::vector<uint64_t> *serno, std::string *err) {
+  EngineImpl &E = *impl_;
+  int c[4];
+  CK(cudaStreamSynchronize(E.stream));
+  CK(cudaMemcpy(c, E.d_counts, sizeof(c), cudaMemcpyDeviceToHost));
+  const int in = E.parity;
+  const int na = c[in], np = c[2 + in];
+  std::vector<float4> pc((size_t)na + np);
+  std::vector<ull> id((size_t)na + np);
+  if (na) {
+    CK(cudaMemcpy(pc.data(), E.d_pc[in], (size_t)na * sizeof(float4), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(id.data(), E.d_id[in], (size_t)na * sizeof(ull), cudaMemcpyDeviceToHost));
+  }
+  if (np) {
+    CK(cudaMemcpy(pc.data() + na, E.d_ppc[in], (size_t)np * sizeof(float4), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(id.data() + na, E.d_pid[in], (size_t)np * sizeof(ull), cudaMemcpyDeviceToHost));
+  }
+  std::vector<size_t> idx;
+  idx.reserve(pc.size());
+  for (size_t i = 0; i < pc.size(); ++i)
+    if (id_species(id[i]) != kDeadSpecies) idx.push_back(i);
+  std::sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
+    const int ra = id_rep(id[a]), rb = id_rep(id[b]);
+    if (ra != rb) return ra < rb;
+    return id_serno(id[a]) < id_serno(id[b]);
+  });
+  pos->resize(idx.size() * 3);
+  species->resize(idx.size());
+  if (rep) rep->resize(idx.size());
+  serno->resize(idx.size());
+  for (size_t k = 0; k < idx.size(); ++k) {
+    const size_t i = idx[k];
+    const int rp = id_rep(id[i]);
+    const RepSpec &s = E.reps[rp];
+    const DevGeo &g = E.geo[rp];
+    uint32_t w;
+    memcpy(&w, &pc[i].w, 4);
+    int ix[3];
+    unpack_cell(w, ix[0], ix[1], ix[2]);
+    const float u[3] = {pc[i].x, pc[i].y, pc[i].z};
+    for (int d = 0; d < 3; ++d) {
+      if (d >= s.dim) { (*pos)[3 * k + d] = 0; continue; }
+      const double h = (s.hi[d] - s.lo[d]) / g.n[d];
+      (*pos)[3 * k + d] = s.lo[d] + ix[d] * h + (double)u[d];
+    }
+    (*species)[k] = id_species(id[i]);
+    if (rep) (*rep)[k] = rp;
+    (*serno)[k] = id_serno(id[i]);
+  }
+  return 0;
+}
+
+int Engine::set_injection(long long n, const uint64_t *sernos, const double *disp, int rep,
+                          std::string *err) {
+  EngineImpl &E = *impl_;
+  if (E.d_injkey) { cudaFree(E.d_injkey); E.d_injkey = nullptr; }
+  if (E.d_injval) { cudaFree(E.d_injval); E.d_injval = nullptr; }
+  E.inj_n = 0;
+  if (n <= 0) {
+    E.dnet.inject = 0;
+    return E.upload_const(err);
+  }
+  std::vector<std::pair<ull, float4>> v((size_t)n);
+  for (long long i = 0; i < n; ++i) {
+    const ull key = id_stream(make_id(0, rep, sernos[i]));
+    v[i] = {key, make_float4((float)disp[4 * i], (float)disp[4 * i + 1], (float)disp[4 * i + 2],
+                             (float)disp[4 * i + 3])};
+  }
+  std::sort(v.begin(), v.end(), [](const std::pair<ull, float4> &a, const std::pair<ull, float4> &b) {
+    return a.first < b.first;
+  });
+  std::vector<ull> keys((size_t)n);
+  std::vector<float4> vals((size_t)n);
+  for (long long i = 0; i < n; ++i) { keys[i] = v[i].first; vals[i] = v[i].second; }
+  CK(cudaMalloc(&E.d_injkey, n * sizeof(ull)));
+  CK(cudaMalloc(&E.d_injval, n * sizeof(float4)));
+  CK(cudaMemcpy(E.d_injkey, keys.data(), n * sizeof(ull), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(E.d_injval, vals.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+  E.inj_n = (int)n;
+  E.dnet.inject = 1;
+  E.invalidate_graph();
+  return E.upload_const(err);
+}
+
+int Engine::profile(long long nsteps, std::vector<std::string> *names, std::vector<double> *ms,
+                    std::vector<long long> *launches, std::string *err) {
+  EngineImpl &E = *impl_;
+  names->clear();
+  ms->clear();
+  launches->clear();
+  E.prof = true;
+  E.marks.clear();
+  E.pool_used = 0;
+  E.mark("start");
+  E.nlaunch--;
+  for (long long k = 0; k < nsteps; ++k) {
+    E.enqueue_step(E.parity, false);
+    E.parity ^= 1;
+  }
+  E.nsteps += nsteps;
+  E.prof = false;
+  CK(cudaStreamSynchronize(E.stream));
+  CK(cudaGetLastError());
+  for (size_t k = 1; k < E.marks.size(); ++k) {
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, E.marks[k - 1].second, E.marks[k].second));
+    const std::string nm = E.marks[k].first;
+    size_t j = 0;
+    while (j < names->size() && (*names)[j] != nm) ++j;
+    if (j == names->size()) {
+      names->push_back(nm);
+      ms->push_back(0);
+      launches->push_back(0);
+    }
+    (*ms)[j] += t;
+    (*launches)[j] += 1;
+  }
+  E.marks.clear();
+  return 0;
+}
+
+void Engine::set_stream(void *stream) {
+  impl_->invalidate_graph();
+  impl_->stream = stream ? (cudaStream_t)stream : impl_->own_stream;
+}
+void *Engine::stream() const { return (void *)impl_->stream; }
+long long Engine::launches() const { return impl_->nlaunch; }
+long long Engine::steps_done() const { return impl_->nsteps; }
+void Engine::set_use_graph(bool on) {
+  impl_->use_graph = on;
+  if (!on) impl_->invalidate_graph();
+}
+
+int solve_radii_device(int mode, long long n, const double *rate, double dt, const double *difc,
+                       const double *b, int rel, double *out, std::string *err) {
+  if (n <= 0) return 0;
+  double *d = nullptr;
+  CK(cudaMalloc(&d, (size_t)n * 4 * sizeof(double)));
+  CK(cudaMemcpy(d, rate, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d + n, difc, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d + 2 * n, b, n * sizeof(double), cudaMemcpyHostToDevice));
+  k_solve_radii<<<sm_count() * 2, 128>>>(mode, n, d, dt, d + n, d + 2 * n, rel, d + 3 * n);
+  CK(cudaGetLastError());
+  CK(cudaMemcpy(out, d + 3 * n, n * sizeof(double), cudaMemcpyDeviceToHost));
+  cudaFree(d);
+  return 0;
+}
+
+}  // namespace smolb
+

@@ -1,0 +1,127 @@
+// Host-side interface of the B200 particle engine (no CUDA types here).
+//
+// The engine replaces the body of Smoldyn's simulatetimestep
+// (source/Smoldyn/smolsim.cpp:2607-2692): diffuse (smolmolec.c:3115),
+// checkwalls (smolwall.c:368), reassignmolecs/molsort (smolboxes.c:896,
+// smolmolec.c:2943), zeroreact/unireact/bireact (smolreact.c:2905/2997/3201)
+// and doreact product placement (smolreact.c:2662).  One engine holds an
+// ensemble of R >= 1 independent replicates that share the reaction network
+// but have their own box, walls, rates and radii; a plain simulation is R=1.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace smolb {
+
+constexpr int kMaxSpecies = 32;   // species indices 0..31 (0 = "empty" as in the reference)
+constexpr int kMaxRxn = 16;       // reactions per order
+constexpr int kMaxProd = 4;       // products per reaction
+constexpr int kMaxUniPerSpecies = 8;
+constexpr int kMaxPairRxn = 4;    // reactions per reactant species pair
+constexpr int kMaxPanels = 16;
+
+enum WallKind : uint8_t { kWallReflect = 0, kWallPeriodic = 1, kWallAbsorb = 2, kWallTransparent = 3 };
+
+// Surface panel (sphere or axis-aligned rectangle) with one action for all
+// species on each face (smolsurface.c:4930 dosurfinteract subset).
+struct PanelSpec {
+  int shape;            // 0 = rect (PSrect), 2 = sphere (PSsph)
+  int axis;             // rect: perpendicular axis 0..2; front face toward +axis if front_sign>0
+  int front_sign;       // rect: +1 / -1; sphere: +1 = front outward, -1 = front inward
+  double pos;           // rect: coordinate of the plane along axis
+  double lo[3], hi[3];  // rect: extent in the two in-plane axes (lo/hi per axis)
+  double center[3];     // sphere
+  double radius;        // sphere
+  int action_front;     // 0 reflect, 1 transmit, 2 absorb (per species below overrides)
+  int action_back;
+  uint32_t absorb_front_mask;   // species bitmask overriding to absorb on front
+  uint32_t absorb_back_mask;
+  uint32_t trans_front_mask;    // species bitmask overriding to transmit on front
+  uint32_t trans_back_mask;
+};
+
+// Reaction network shared by every replicate.
+struct NetSpec {
+  int nspecies = 1;                          // including index 0
+  int nrxn[3] = {0, 0, 0};
+  int rct[3][kMaxRxn][2] = {};               // reactant species (order 1: [0]; order 2: both)
+  int nprod[3][kMaxRxn] = {};
+  int prd[3][kMaxRxn][kMaxProd] = {};
+  int fixed_placement[3][kMaxRxn] = {};      // 1: product offsets not rotated (RPfixed)
+  int gauss_table_size = 4096;               // power of two (smolmolec.c:781)
+  std::vector<PanelSpec> panels;
+};
+
+// One replicate's geometry and rate-derived parameters.
+struct RepSpec {
+  double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+  int ncell[3] = {1, 1, 1};
+  uint8_t wall[6] = {0, 0, 0, 0, 0, 0};      // [2*d+side]
+  int dim = 3;
+  double difc[kMaxSpecies] = {};
+  double drift[kMaxSpecies][3] = {};
+  double uni_prob[kMaxRxn] = {};             // rxn->prob for order 1 (smolreact.c:1333-1357)
+  double bind2[kMaxRxn] = {};                // rxn->bindrad2 for order 2
+  double pair_prob[kMaxRxn] = {};            // rxn->prob for order 2 (1 unless set)
+  double birth_mean[kMaxRxn] = {};           // rxn->prob for order 0 (expected births/step)
+  double prdpos[3][kMaxRxn][kMaxProd][3] = {};
+};
+
+struct EngineStats {
+  long long wall = 0, rxn0 = 0, rxn1 = 0, rxn2 = 0, unresolved = 0, multicand = 0, overflow = 0;
+};
+
+class EngineImpl;
+
+class Engine {
+ public:
+  Engine();
+  ~Engine();
+  Engine(const Engine &) = delete;
+  Engine &operator=(const Engine &) = delete;
+
+  // Allocates device memory for `capacity` molecules in total.  Returns 0 or
+  // an ErrorCode-style negative value with *err set.
+  int init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt, uint64_t seed,
+           long long capacity, std::string *err);
+  // Replace all molecules.  pos: 3*n absolute coordinates; rep may be null (all 0);
+  // serno: null or 0 entries -> assigned 1,2,... per replicate in input order.
+  int set_molecules(long long n, const double *pos, const int *species, const int *rep,
+                    const uint64_t *serno, std::string *err);
+  // Advance `nsteps` time steps (asynchronous unless sync is requested).
+  int run(long long nsteps, std::string *err);
+  // Copy molecules back (absolute coordinates, sorted by (rep, serno)).
+  int get_molecules(std::vector<double> *pos, std::vector<int> *species, std::vector<int> *rep,
+                    std::vector<uint64_t> *serno, std::string *err);
+  // Live molecule count per (rep, species): out[rep*nspecies + sp].
+  int species_counts(std::vector<long long> *out, std::string *err);
+  long long total_molecules();
+  int stats(EngineStats *s, std::string *err);
+  int status_flags();
+  // Update rate-derived parameters of every replicate (no reallocation).
+  int update_reps(const std::vector<RepSpec> &reps, std::string *err);
+  // Deterministic mode: per-serno displacements for the next step only.
+  int set_injection(long long n, const uint64_t *sernos, const double *disp, int rep,
+                    std::string *err);
+  void set_stream(void *stream);
+  void *stream() const;
+  int synchronize(std::string *err);
+  long long launches() const;
+  long long steps_done() const;
+  // Capture the 2-step kernel sequence in a CUDA graph and replay it (on by default).
+  void set_use_graph(bool on);
+  // Run n steps timing every kernel launch with CUDA events.
+  int profile(long long nsteps, std::vector<std::string> *names, std::vector<double> *ms,
+              std::vector<long long> *launches, std::string *err);
+
+ private:
+  EngineImpl *impl_;
+};
+
+// Batched FP64 radius solver on the device (mode 0: binding, 1: unbinding).
+int solve_radii_device(int mode, long long n, const double *rate, double dt, const double *difc,
+                       const double *b, int rel, double *out, std::string *err);
+
+}  // namespace smolb

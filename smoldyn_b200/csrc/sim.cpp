@@ -1,0 +1,822 @@
+// Host-side parameter derivation and text configuration reader.
+#include "sim.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+
+#include "rxnparam.cuh"
+
+namespace smolb {
+
+// host copies of the radius tables (generated from the reference's rxnparam.c)
+namespace rxnp {
+const double h_yi[SMOLB_TAB_YI_LEN] = SMOLB_TAB_YI_INIT;
+const double h_yr[SMOLB_TAB_YR_LEN] = SMOLB_TAB_YR_INIT;
+const double h_yb[SMOLB_TAB_YB_LEN] = SMOLB_TAB_YB_INIT;
+const double h_kirr[SMOLB_TAB_KIRR_LEN] = SMOLB_TAB_KIRR_INIT;
+const double h_krev[SMOLB_TAB_KREV_LEN] = SMOLB_TAB_KREV_INIT;
+const double h_kb[SMOLB_TAB_KB_LEN] = SMOLB_TAB_KB_INIT;
+}  // namespace rxnp
+
+// RevParam values (smoldyn.h:358)
+enum {
+  RP_none, RP_irrev, RP_confspread, RP_bounce, RP_pgem, RP_pgemmax, RP_pgemmaxw, RP_ratio,
+  RP_unbindrad, RP_pgem2, RP_pgemmax2, RP_ratio2, RP_offset, RP_fixed
+};
+
+Sim::Sim() {
+  species.push_back(SpeciesDef{"empty"});
+}
+
+int Sim::species_index(const std::string &name) const {
+  for (size_t i = 1; i < species.size(); ++i)
+    if (species[i].name == name) return (int)i;
+  return -1;
+}
+
+int Sim::reaction_index(const std::string &name, int *order) const {
+  for (int o = 0; o < 3; ++o)
+    for (size_t r = 0; r < rxn[o].size(); ++r)
+      if (rxn[o][r].name == name) {
+        if (order) *order = o;
+        return (int)r;
+      }
+  return -1;
+}
+
+double Sim::rand_u01() {
+  // SplitMix64 stream for host-side placement of initial molecules
+  uint64_t z = (host_rng += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  return (z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+static bool same_set2(int a0, int a1, int b0, int b1) {
+  return (a0 == b0 && a1 == b1) || (a0 == b1 && a1 == b0);
+}
+
+// findreverserxn (smolreact.c:345-381): rev=1 when a reaction of order nprod
+// consumes exactly this reaction's products and makes its reactants; rev=2
+// when the products only react onward.
+static int find_reverse(const Sim &s, int order, int r, int *o2, int *r2) {
+  const RxnDef &x = s.rxn[order][r];
+  *o2 = 0;
+  *r2 = 0;
+  if (order == 0 || x.nprod == 0 || x.nprod >= 3) return 0;
+  const int orr = x.nprod;
+  if (s.rxn[orr].empty()) return 0;
+  *o2 = orr;
+  int rev = 0;
+  for (size_t k = 0; k < s.rxn[orr].size(); ++k) {
+    const RxnDef &y = s.rxn[orr][k];
+    bool rct_match = (orr == 1) ? (y.rct[0] == x.prd[0]) : same_set2(y.rct[0], y.rct[1], x.prd[0], x.prd[1]);
+    if (!rct_match) continue;
+    if (rev != 1 && y.nprod == order) {
+      bool back = (order == 1) ? (y.prd[0] == x.rct[0]) : same_set2(y.prd[0], y.prd[1], x.rct[0], x.rct[1]);
+      if (back) {
+        rev = 1;
+        *r2 = (int)k;
+      }
+    }
+    if (!rev) {
+      rev = 2;
+      *r2 = (int)k;
+    }
+  }
+  return rev;
+}
+
+static double system_volume(const Sim &s) {
+  double v = 1;
+  for (int d = 0; d < s.dim; ++d) v *= s.hi[d] - s.lo[d];
+  return v;
+}
+
+// rxnsetrate (smolreact.c:1307-1414) for every reaction, then rxnsetproduct
+// (smolreact.c:1431-1577), in the reference's order.
+int derive_reaction_params(Sim &sim, std::string *err) {
+  const double dt = sim.dt;
+  // order 0
+  for (RxnDef &x : sim.rxn[0]) {
+    if (x.disabled) { x.prob = 0; continue; }
+    if (x.rate < 0) { if (err) *err = "reaction " + x.name + " rate is undefined"; return -8; }
+    x.prob = x.rate * dt * system_volume(sim);
+  }
+  // order 1
+  for (size_t r = 0; r < sim.rxn[1].size(); ++r) {
+    RxnDef &x = sim.rxn[1][r];
+    if (x.disabled) { x.prob = 0; }
+    else if (x.rate < 0) { if (err) *err = "reaction " + x.name + " rate is undefined"; return -8; }
+    else if (x.rate == 0) x.prob = 0;
+    else {
+      const int i = x.rct[0];
+      double sum = 0;
+      for (const RxnDef &y : sim.rxn[1])
+        if (y.rct[0] == i && y.rate > 0) sum += y.rate;
+      x.prob = x.rate / sum * (1.0 - std::exp(-sum * dt));
+      double product = 1.0;
+      for (size_t k = 0; k < r; ++k) {
+        const RxnDef &y = sim.rxn[1][k];
+        if (y.rct[0] != i) continue;
+        const double pr = y.prob * product;
+        product *= 1.0 - pr;
+      }
+      x.prob /= product;
+      if (!(x.prob >= 0 && x.prob <= 1)) {
+        if (err) *err = "reaction " + x.name + " probability out of range";
+        return -8;
+      }
+    }
+    int o2, r2;
+    const int rev = find_reverse(sim, 1, (int)r, &o2, &r2);
+    if (rev > 0 && o2 == 2 && x.rparamt == RP_none) {
+      x.rparamt = RP_pgemmaxw;
+      x.rparam = 0.2;
+    }
+  }
+  // order 2
+  for (size_t r = 0; r < sim.rxn[2].size(); ++r) {
+    RxnDef &x = sim.rxn[2][r];
+    const int i1 = x.rct[0], i2 = x.rct[1];
+    if (x.disabled) { x.prob = 0; x.bindrad2 = 0; continue; }
+    if (x.rate < 0) {
+      // rate undefined: a user binding radius (binding_radius statement) stands
+      if (x.prob_user >= 0) x.prob = x.prob_user;
+      else x.prob = 1;
+      if (x.bindrad_user >= 0) { x.bindrad2 = x.bindrad_user * x.bindrad_user; continue; }
+      if (err) *err = "reaction rate " + x.name + " is undefined";
+      return -8;
+    }
+    double rate3 = x.rate;
+    if (i1 == i2) rate3 *= 2;
+    const double dsum = sim.species[i1].difc + sim.species[i2].difc;
+    int o2, r2;
+    const int rev = find_reverse(sim, 2, (int)r, &o2, &r2);
+    if (rev > 0 && o2 == 2 && x.rparamt == RP_none) {
+      x.rparamt = RP_pgemmaxw;
+      x.rparam = 0.2;
+    }
+    int rpt = RP_none;
+    double rpar = 0;
+    if (rev == 1) {
+      RxnDef &rv = sim.rxn[o2][r2];
+      if (rv.rparamt == RP_none) {
+        rv.rparamt = RP_pgemmaxw;
+        rv.rparam = 0.2;
+      }
+      rpt = rv.rparamt;
+      rpar = rv.rparam;
+    }
+    double prob = (x.prob_user >= 0) ? x.prob_user : -1;
+    if (prob < 0) prob = 1;
+    double a;
+    if (rate3 <= 0) a = 0;
+    else if (dsum <= 0) { if (err) *err = "Both diffusion coefficients are 0"; return -8; }
+    else if (rpt == RP_unbindrad) a = rxnp::bindingradiusprob(rate3, dt, dsum, rpar, 0, x.chi, &prob);
+    else if (rpt == RP_ratio) a = rxnp::bindingradiusprob(rate3, dt, dsum, rpar, 1, x.chi, &prob);
+    else if (rpt == RP_pgem) a = rxnp::bindingradiusprob(rate3 * (1.0 - rpar), dt, dsum, -1, 0, x.chi, &prob);
+    else if (rpt == RP_pgemmax || rpt == RP_pgemmaxw) {
+      a = rxnp::bindingradiusprob(rate3, dt, dsum, 0, 0, x.chi, &prob);
+      const double ub = rxnp::unbindingradius(rpar, dt, dsum, a);
+      if (ub > 0) a = rxnp::bindingradiusprob(rate3 * (1.0 - rpar), dt, dsum, -1, 0, x.chi, &prob);
+    } else {
+      a = rxnp::bindingradiusprob(rate3, dt, dsum, -1, 0, x.chi, &prob);
+    }
+    x.prob = prob;
+    if (x.bindrad_user >= 0) a = x.bindrad_user;
+    x.bindrad2 = a * a;
+  }
+  // products
+  for (int order = 0; order < 3; ++order)
+    for (size_t r = 0; r < sim.rxn[order].size(); ++r) {
+      RxnDef &x = sim.rxn[order][r];
+      const int dim = sim.dim;
+      for (int q = 0; q < kMaxProd; ++q)
+        for (int d = 0; d < 3; ++d) x.prdpos[q][d] = 0;
+      const int np = x.nprod;
+      const int rpt = x.rparamt;
+      double rpar = x.rparam;
+      if (np == 0) {
+        if (rpt == RP_none || rpt == RP_irrev || rpt == RP_confspread) x.unbindrad = 0;
+        else { if (err) *err = "Illegal product parameter because reaction has no products"; return -8; }
+      } else if (rpt == RP_offset || rpt == RP_fixed) {
+        for (int q = 0; q < np; ++q)
+          for (int d = 0; d < dim; ++d) x.prdpos[q][d] = x.user_prdpos[q][d];
+        double dist = 0;
+        if (np == 1) for (int d = 0; d < dim; ++d) dist = x.prdpos[0][d];
+        else for (int d = 0; d < dim; ++d) dist += x.prdpos[0][d] - x.prdpos[1][d];
+        x.unbindrad = std::sqrt(dist);
+      } else if (np == 1) {
+        if (rpt == RP_none || rpt == RP_irrev || rpt == RP_confspread) x.unbindrad = 0;
+        else { if (err) *err = "Illegal product parameter because reaction only has one product"; return -8; }
+      } else if (rpt == RP_bounce) {
+        if (err) *err = "bounce product placement is not supported by the GPU engine";
+        return -8;
+      } else {
+        double dc1 = sim.species[x.prd[0]].difc, dc2 = sim.species[x.prd[1]].difc;
+        const double dsum = dc1 + dc2;
+        if (dsum == 0) dc1 = dc2 = 0.5;
+        else { dc1 /= dsum; dc2 /= dsum; }
+        int o2, r2;
+        const int rev = find_reverse(sim, order, (int)r, &o2, &r2);
+        if (rpt == RP_irrev || rpt == RP_confspread) {
+          x.unbindrad = 0;
+        } else if (rev == 0) {
+          if (rpt == RP_pgem || rpt == RP_pgemmax || rpt == RP_pgemmaxw || rpt == RP_ratio ||
+              rpt == RP_pgem2 || rpt == RP_pgemmax2 || rpt == RP_ratio2) {
+            if (err) *err = "Illegal product parameter because products don't react";
+            return -8;
+          } else if (rpt == RP_unbindrad) {
+            x.unbindrad = rpar;
+            x.prdpos[0][0] = rpar * dc1;
+            x.prdpos[1][0] = -rpar * dc2;
+          } else {
+            x.unbindrad = 0;
+          }
+        } else {
+          const RxnDef &rv = sim.rxn[o2][r2];
+          const double bindradr = (rv.bindrad2 >= 0) ? std::sqrt(rv.bindrad2) : -1;
+          if (rpt == RP_none) { if (err) *err = "Undefined product placement for reversible reaction"; return -8; }
+          else if (rpt == RP_unbindrad) {
+            x.unbindrad = rpar;
+            x.prdpos[0][0] = rpar * dc1;
+            x.prdpos[1][0] = -rpar * dc2;
+          } else if (rv.bindrad2 < 0) {
+            if (err) *err = "Binding radius of reaction products is undefined";
+            return -8;
+          } else if (rv.bindrad2 == 0) {
+            x.unbindrad = 0;
+          } else if (rpt == RP_ratio || rpt == RP_ratio2) {
+            x.unbindrad = rpar * bindradr;
+            x.prdpos[0][0] = rpar * bindradr * dc1;
+            x.prdpos[1][0] = -rpar * bindradr * dc2;
+          } else if (dsum <= 0) {
+            if (err) *err = "Cannot set unbinding distance because sum of product diffusion constants is 0";
+            return -8;
+          } else if (rpt == RP_pgem || rpt == RP_pgem2) {
+            rpar = rxnp::unbindingradius(rpar, sim.dt, dsum, bindradr);
+            if (rpar == -2) { if (err) *err = "Cannot create an unbinding radius due to illegal input values"; return -8; }
+            if (rpar < 0) {
+              char buf[128];
+              snprintf(buf, sizeof buf, "Maximum possible geminate binding probability is %g", -rpar);
+              if (err) *err = buf;
+              return -8;
+            }
+            x.unbindrad = rpar;
+            x.prdpos[0][0] = rpar * dc1;
+            x.prdpos[1][0] = -rpar * dc2;
+          } else if (rpt == RP_pgemmax || rpt == RP_pgemmaxw || rpt == RP_pgemmax2) {
+            rpar = rxnp::unbindingradius(rpar, sim.dt, dsum, bindradr);
+            if (rpar == -2) { if (err) *err = "Illegal input values"; return -8; }
+            if (rpar <= 0) x.unbindrad = 0;
+            else {
+              x.unbindrad = rpar;
+              x.prdpos[0][0] = rpar * dc1;
+              x.prdpos[1][0] = -rpar * dc2;
+            }
+          }
+        }
+      }
+    }
+  return 0;
+}
+
+// Virtual-box grid: side = ceil(L * (N/molperbox/V)^(1/dim)) (smolboxes.c:717-749),
+// widened where needed so that a box is at least one binding radius wide (the
+// pair search looks one box deep) and capped at 1023 boxes per dimension.
+static void choose_grid(const Sim &s, long long nmol, int ncell[3]) {
+  double mpbox = s.molperbox, boxsize = s.boxsize;
+  if (mpbox <= 0 && boxsize <= 0) mpbox = 4;
+  double f;
+  if (mpbox > 0) f = std::pow((double)nmol / mpbox / system_volume(s), 1.0 / s.dim);
+  else f = 1.0 / boxsize;
+  double maxrad = 0;
+  for (const RxnDef &x : s.rxn[2])
+    if (x.bindrad2 > 0) maxrad = std::max(maxrad, std::sqrt(x.bindrad2));
+  for (int d = 0; d < 3; ++d) {
+    if (d >= s.dim) { ncell[d] = 1; continue; }
+    const double L = s.hi[d] - s.lo[d];
+    int n = (int)std::ceil(L * f);
+    if (n < 1) n = 1;
+    if (maxrad > 0 && L / n < maxrad) n = std::max(1, (int)std::floor(L / maxrad));
+    if (n > 1023) n = 1023;
+    ncell[d] = n;
+  }
+}
+
+int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err) {
+  *net = NetSpec();
+  *rep = RepSpec();
+  if ((int)sim.species.size() > kMaxSpecies) { if (err) *err = "too many species (max 31)"; return -6; }
+  net->nspecies = (int)sim.species.size();
+  net->gauss_table_size = sim.gauss_table_size;
+  for (int o = 0; o < 3; ++o) {
+    if ((int)sim.rxn[o].size() > kMaxRxn) { if (err) *err = "too many reactions of one order (max 16)"; return -6; }
+    net->nrxn[o] = (int)sim.rxn[o].size();
+    for (size_t r = 0; r < sim.rxn[o].size(); ++r) {
+      const RxnDef &x = sim.rxn[o][r];
+      net->rct[o][r][0] = x.rct[0];
+      net->rct[o][r][1] = x.rct[1];
+      net->nprod[o][r] = x.nprod;
+      for (int q = 0; q < x.nprod; ++q) net->prd[o][r][q] = x.prd[q];
+      net->fixed_placement[o][r] = (x.rparamt == RP_fixed) ? 1 : 0;
+      for (int q = 0; q < x.nprod; ++q)
+        for (int d = 0; d < 3; ++d) rep->prdpos[o][r][q][d] = x.prdpos[q][d];
+      if (o == 0) rep->birth_mean[r] = x.prob;
+      if (o == 1) rep->uni_prob[r] = x.prob;
+      if (o == 2) {
+        rep->bind2[r] = std::max(0.0, x.bindrad2);
+        rep->pair_prob[r] = x.prob;
+      }
+    }
+  }
+  rep->dim = sim.dim;
+  const bool surfaces = !sim.surfaces.empty();
+  for (int d = 0; d < 3; ++d) {
+    rep->lo[d] = (d < sim.dim) ? sim.lo[d] : 0;
+    rep->hi[d] = (d < sim.dim) ? sim.hi[d] : 1;
+    for (int side = 0; side < 2; ++side) {
+      const char t = sim.btype[d][side];
+      uint8_t k = kWallTransparent;
+      if (!surfaces) {  // walls are transparent once surfaces exist (smolwall.c:328, 374)
+        if (t == 'r') k = kWallReflect;
+        else if (t == 'p') k = kWallPeriodic;
+        else if (t == 'a') k = kWallAbsorb;
+      }
+      rep->wall[2 * d + side] = (d < sim.dim) ? k : kWallTransparent;
+    }
+  }
+  for (size_t i = 0; i < sim.species.size(); ++i) {
+    rep->difc[i] = sim.species[i].difc;
+    for (int d = 0; d < 3; ++d) rep->drift[i][d] = (d < sim.dim) ? sim.species[i].drift[d] : 0;
+  }
+  choose_grid(sim, (long long)sim.pend_sp.size(), rep->ncell);
+  for (const SurfaceDef &sf : sim.surfaces)
+    for (PanelSpec ps : sf.panels) {
+      ps.action_front = sf.act_front;
+      ps.action_back = sf.act_back;
+      ps.absorb_front_mask = sf.absorb_front;
+      ps.absorb_back_mask = sf.absorb_back;
+      ps.trans_front_mask = sf.trans_front;
+      ps.trans_back_mask = sf.trans_back;
+      net->panels.push_back(ps);
+    }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Text configuration reader (subset of smolsim.cpp:626-2270 simreadstring).
+
+static std::vector<std::string> split_ws(const std::string &s) {
+  std::vector<std::string> out;
+  std::istringstream is(s);
+  std::string w;
+  while (is >> w) out.push_back(w);
+  return out;
+}
+
+static bool parse_double(const std::string &s, double *v) {
+  char *end = nullptr;
+  *v = strtod(s.c_str(), &end);
+  return end && *end == '\0' && end != s.c_str();
+}
+
+static int species_arg(Sim &sim, const std::string &w, std::vector<int> *out) {
+  out->clear();
+  std::string name = w;
+  const size_t paren = name.find('(');
+  if (paren != std::string::npos) name = name.substr(0, paren);  // state suffix: soln only
+  if (name == "all") {
+    for (size_t i = 1; i < sim.species.size(); ++i) out->push_back((int)i);
+    return 0;
+  }
+  const int i = sim.species_index(name);
+  if (i < 0) return -3;
+  out->push_back(i);
+  return 0;
+}
+
+static int add_reaction_from_words(Sim &sim, const std::vector<std::string> &w, std::string *err) {
+  // reaction [name] r1 [+ r2] -> p1 [+ p2 ...] [rate]
+  if (w.size() < 3) { if (err) *err = "reaction: too few words"; return -7; }
+  size_t k = 0;
+  std::string name = w[0];
+  size_t arrow = std::find(w.begin(), w.end(), "->") - w.begin();
+  bool reversible = false;
+  if (arrow == w.size()) {
+    arrow = std::find(w.begin(), w.end(), "<->") - w.begin();
+    reversible = arrow != w.size();
+  }
+  if (arrow == w.size()) { if (err) *err = "reaction: missing ->"; return -7; }
+  k = 1;
+  std::vector<std::string> rct, prd;
+  for (size_t j = k; j < arrow; ++j)
+    if (w[j] != "+") rct.push_back(w[j]);
+  // products run up to the trailing numeric rate(s); a lone "0" means none
+  std::vector<double> rates;
+  size_t end = w.size();
+  while (end > arrow + 1) {
+    double v;
+    if (!parse_double(w[end - 1], &v) || sim.species_index(w[end - 1]) >= 0) break;
+    if (end - 1 == arrow + 1 && w[end - 1] == "0") break;  // "-> 0" with no rate
+    rates.insert(rates.begin(), v);
+    --end;
+  }
+  for (size_t j = arrow + 1; j < end; ++j)
+    if (w[j] != "+") prd.push_back(w[j]);
+  if (rct.size() == 1 && rct[0] == "0") rct.clear();
+  if (prd.size() == 1 && prd[0] == "0") prd.clear();
+  if (rct.size() > 2 || prd.size() > (size_t)kMaxProd) { if (err) *err = "reaction: too many reactants or products"; return -7; }
+  auto mk = [&](const std::string &nm, const std::vector<std::string> &r, const std::vector<std::string> &p,
+                double rate) -> int {
+    RxnDef x;
+    x.name = nm;
+    x.order = (int)r.size();
+    for (size_t q = 0; q < r.size(); ++q) {
+      const int i = sim.species_index(r[q]);
+      if (i < 0) { if (err) *err = "unknown species " + r[q]; return -3; }
+      x.rct[q] = i;
+    }
+    x.nprod = (int)p.size();
+    for (size_t q = 0; q < p.size(); ++q) {
+      const int i = sim.species_index(p[q]);
+      if (i < 0) { if (err) *err = "unknown species " + p[q]; return -3; }
+      x.prd[q] = i;
+    }
+    x.rate = rate;
+    if ((int)sim.rxn[x.order].size() >= kMaxRxn) { if (err) *err = "too many reactions"; return -6; }
+    sim.rxn[x.order].push_back(x);
+    return 0;
+  };
+  int rc = mk(reversible ? name + "fwd" : name, rct, prd, rates.empty() ? -1 : rates[0]);
+  if (rc) return rc;
+  if (reversible) rc = mk(name + "rev", prd, rct, rates.size() > 1 ? rates[1] : -1);
+  sim.need_update = sim.need_rebuild = true;
+  return rc;
+}
+
+static int rp_from_string(const std::string &s) {
+  static const char *names[] = {"none", "irrev", "confspread", "bounce", "pgem", "pgemmax", "pgemmaxw",
+                                "ratio", "unbindrad", "pgem2", "pgemmax2", "ratio2", "offset", "fixed"};
+  static const char *abbr[] = {"", "i", "a", "", "p", "x", "", "r", "b", "q", "y", "s", "o", "f"};
+  for (int k = 0; k < 14; ++k)
+    if (s == names[k] || (abbr[k][0] && s == abbr[k])) return k;
+  return -1;
+}
+
+int read_config_statement(Sim &sim, const std::string &word, const std::string &rest, std::string *err) {
+  const std::vector<std::string> w = split_ws(rest);
+  auto need = [&](size_t n) -> bool {
+    if (w.size() < n) { if (err) *err = word + ": missing parameters"; return false; }
+    return true;
+  };
+  double v;
+  if (word == "dim") {
+    if (!need(1)) return -7;
+    sim.dim = atoi(w[0].c_str());
+    if (sim.dim < 1 || sim.dim > 3) { if (err) *err = "dim must be 1..3"; return -6; }
+  } else if (word == "species" || word == "names") {
+    for (const std::string &s : w)
+      if (sim.species_index(s) < 0) sim.species.push_back(SpeciesDef{s});
+    sim.need_rebuild = true;
+  } else if (word == "difc") {
+    if (!need(2)) return -7;
+    std::vector<int> ids;
+    if (species_arg(sim, w[0], &ids)) { if (err) *err = "difc: unknown species " + w[0]; return -3; }
+    if (!parse_double(w[1], &v)) { if (err) *err = "difc: bad value"; return -7; }
+    for (int i : ids) sim.species[i].difc = v;
+    sim.need_update = true;
+  } else if (word == "drift") {
+    if (!need(1 + (size_t)sim.dim)) return -7;
+    std::vector<int> ids;
+    if (species_arg(sim, w[0], &ids)) { if (err) *err = "drift: unknown species " + w[0]; return -3; }
+    for (int i : ids)
+      for (int d = 0; d < sim.dim; ++d) sim.species[i].drift[d] = atof(w[1 + d].c_str());
+    sim.need_update = true;
+  } else if (word == "boundaries") {
+    if (!need(3)) return -7;
+    const int d = atoi(w[0].c_str());
+    if (d < 0 || d >= 3) { if (err) *err = "boundaries: bad dimension"; return -6; }
+    sim.lo[d] = atof(w[1].c_str());
+    sim.hi[d] = atof(w[2].c_str());
+    const char t = (w.size() > 3) ? w[3][0] : 'r';
+    sim.btype[d][0] = sim.btype[d][1] = t;
+    sim.need_rebuild = true;
+  } else if (word == "low_wall" || word == "high_wall") {
+    if (!need(3)) return -7;
+    const int d = atoi(w[0].c_str());
+    const int side = (word == "high_wall") ? 1 : 0;
+    (side ? sim.hi : sim.lo)[d] = atof(w[1].c_str());
+    sim.btype[d][side] = w[2][0];
+    sim.need_rebuild = true;
+  } else if (word == "time_start") {
+    if (!need(1)) return -7;
+    sim.tstart = sim.time = atof(w[0].c_str());
+  } else if (word == "time_stop") {
+    if (!need(1)) return -7;
+    sim.tstop = atof(w[0].c_str());
+  } else if (word == "time_step") {
+    if (!need(1)) return -7;
+    sim.dt = atof(w[0].c_str());
+    sim.need_update = sim.need_rebuild = true;
+  } else if (word == "time_now") {
+    if (!need(1)) return -7;
+    sim.time = atof(w[0].c_str());
+  } else if (word == "random_seed") {
+    if (!need(1)) return -7;
+    sim.seed = atoll(w[0].c_str());
+    sim.host_rng = (uint64_t)sim.seed * 0x9E3779B97F4A7C15ull + 0x2545F4914F6CDD1Dull;
+    sim.need_rebuild = true;
+  } else if (word == "molperbox") {
+    if (!need(1)) return -7;
+    sim.molperbox = atof(w[0].c_str());
+    sim.boxsize = -1;
+    sim.need_rebuild = true;
+  } else if (word == "boxsize") {
+    if (!need(1)) return -7;
+    sim.boxsize = atof(w[0].c_str());
+    sim.molperbox = -1;
+    sim.need_rebuild = true;
+  } else if (word == "accuracy") {
+    if (!need(1)) return -7;
+    sim.accuracy = atoi(w[0].c_str());
+  } else if (word == "gauss_table_size") {
+    if (!need(1)) return -7;
+    sim.gauss_table_size = atoi(w[0].c_str());
+    sim.need_rebuild = true;
+  } else if (word == "max_mol") {
+    if (!need(1)) return -7;
+    sim.max_mol = atoll(w[0].c_str());
+    sim.need_rebuild = true;
+  } else if (word == "mol" || word == "molecule") {
+    if (!need(2)) return -7;
+    const long long n = atoll(w[0].c_str());
+    const int i = sim.species_index(w[1]);
+    if (i < 0) { if (err) *err = "mol: unknown species " + w[1]; return -3; }
+    for (long long k = 0; k < n; ++k) {
+      for (int d = 0; d < 3; ++d) {
+        double x = 0;
+        if (d < sim.dim) {
+          const std::string &t = (2 + (size_t)d < w.size()) ? w[2 + d] : std::string("u");
+          if (t == "u") x = sim.lo[d] + sim.rand_u01() * (sim.hi[d] - sim.lo[d]);
+          else {
+            const size_t dash = t.find('-', 1);
+            if (dash != std::string::npos) {
+              const double a = atof(t.substr(0, dash).c_str()), b = atof(t.substr(dash + 1).c_str());
+              x = a + sim.rand_u01() * (b - a);
+            } else x = atof(t.c_str());
+          }
+        }
+        sim.pend_pos.push_back(x);
+      }
+      sim.pend_sp.push_back(i);
+    }
+    sim.need_rebuild = true;
+  } else if (word == "reaction") {
+    return add_reaction_from_words(sim, w, err);
+  } else if (word == "reaction_rate") {
+    if (!need(2)) return -7;
+    int o;
+    const int r = sim.reaction_index(w[0], &o);
+    if (r < 0) { if (err) *err = "reaction_rate: unknown reaction"; return -3; }
+    sim.rxn[o][r].rate = atof(w[1].c_str());
+    sim.need_update = true;
+  } else if (word == "reaction_probability") {
+    if (!need(2)) return -7;
+    int o;
+    const int r = sim.reaction_index(w[0], &o);
+    if (r < 0) { if (err) *err = "reaction_probability: unknown reaction"; return -3; }
+    sim.rxn[o][r].prob_user = atof(w[1].c_str());
+    sim.need_update = true;
+  } else if (word == "binding_radius") {
+    if (!need(2)) return -7;
+    int o;
+    const int r = sim.reaction_index(w[0], &o);
+    if (r < 0 || o != 2) { if (err) *err = "binding_radius: unknown bimolecular reaction"; return -3; }
+    sim.rxn[2][r].bindrad_user = atof(w[1].c_str());
+    sim.need_update = true;
+  } else if (word == "product_placement") {
+    if (!need(2)) return -7;
+    int o;
+    const int r = sim.reaction_index(w[0], &o);
+    if (r < 0) { if (err) *err = "product_placement: unknown reaction"; return -3; }
+    const int rp = rp_from_string(w[1]);
+    if (rp < 0) { if (err) *err = "product_placement: unknown type " + w[1]; return -7; }
+    RxnDef &x = sim.rxn[o][r];
+    x.rparamt = rp;
+    x.rparam = (w.size() > 2) ? atof(w[2].c_str()) : 0;
+    if ((rp == RP_offset || rp == RP_fixed) && w.size() >= 3 + 1 + (size_t)sim.dim) {
+      const int q = sim.species_index(w[2]);
+      int slot = -1;
+      for (int k = 0; k < x.nprod; ++k)
+        if (x.prd[k] == q) { slot = k; break; }
+      if (slot >= 0)
+        for (int d = 0; d < sim.dim; ++d) x.user_prdpos[slot][d] = atof(w[3 + d].c_str());
+    }
+    sim.need_update = true;
+  } else if (word == "start_surface" || word == "new_surface") {
+    SurfaceDef s;
+    s.name = w.empty() ? "surf" + std::to_string(sim.surfaces.size()) : w[0];
+    sim.surfaces.push_back(s);
+    sim.need_rebuild = true;
+  } else if (word == "output_files") {
+    for (const std::string &s : w) sim.outfiles.push_back(s);
+  } else if (word == "cmd") {
+    if (!need(2)) return -7;
+    Command c;
+    c.type = w[0][0];
+    size_t k = 1;
+    if (c.type == 'N' || c.type == 'n') { c.every = atoll(w[1].c_str()); k = 2; }
+    else if (c.type == 'i') {
+      if (!need(5)) return -7;
+      c.on = atof(w[1].c_str()); c.off = atof(w[2].c_str()); c.dt = atof(w[3].c_str());
+      k = 4;
+    }
+    for (; k < w.size(); ++k) c.text += (c.text.empty() ? "" : " ") + w[k];
+    sim.cmds.push_back(c);
+  } else if (word == "graphics" || word == "graphic_iter" || word == "graphic_delay" || word == "color" ||
+             word == "display_size" || word == "text_display" || word == "frame_thickness" ||
+             word == "frame_color" || word == "grid_thickness" || word == "background_color" ||
+             word == "tiff_name" || word == "tiff_iter" || word == "light" || word == "text_color" ||
+             word == "molecule_lists" || word == "mol_list" || word == "quit_at_end" ||
+             word == "output_root" || word == "output_format" || word == "output_precision") {
+    // display, list-layout and output formatting statements: no effect on the engine
+  } else {
+    if (err) *err = "unsupported statement: " + word;
+    return -7;
+  }
+  return 0;
+}
+
+// surface block statements (smolsurface.c surfreadstring subset)
+static int read_surface_statement(Sim &sim, SurfaceDef &sf, const std::string &word,
+                                  const std::vector<std::string> &w, std::string *err) {
+  auto act_of = [](const std::string &s) -> int {
+    if (s == "reflect" || s == "r") return 0;
+    if (s == "transmit" || s == "t") return 1;
+    if (s == "absorb" || s == "a") return 2;
+    return -1;
+  };
+  if (word == "name") {
+    if (!w.empty()) sf.name = w[0];
+  } else if (word == "action") {
+    // action face species action
+    if (w.size() < 3) { if (err) *err = "action: missing parameters"; return -7; }
+    const std::string &face = w[0];
+    const int a = act_of(w[2]);
+    if (a < 0) { if (err) *err = "surface action not supported: " + w[2]; return -7; }
+    std::vector<int> ids;
+    const bool all = (w[1] == "all" || w[1] == "all(all)");
+    if (!all && species_arg(sim, w[1], &ids)) { if (err) *err = "action: unknown species " + w[1]; return -3; }
+    const bool f = (face == "front" || face == "both" || face == "all");
+    const bool b = (face == "back" || face == "both" || face == "all");
+    if (all) {
+      if (f) { sf.act_front = a; sf.absorb_front = sf.trans_front = sf.refl_front = 0; }
+      if (b) { sf.act_back = a; sf.absorb_back = sf.trans_back = sf.refl_back = 0; }
+    } else {
+      for (int i : ids) {
+        const uint32_t bit = 1u << i;
+        auto setmask = [&](uint32_t &abs, uint32_t &tr, uint32_t &rf) {
+          abs &= ~bit; tr &= ~bit; rf &= ~bit;
+          if (a == 2) abs |= bit;
+          else if (a == 1) tr |= bit;
+          else rf |= bit;
+        };
+        if (f) setmask(sf.absorb_front, sf.trans_front, sf.refl_front);
+        if (b) setmask(sf.absorb_back, sf.trans_back, sf.refl_back);
+      }
+    }
+  } else if (word == "panel") {
+    if (w.empty()) { if (err) *err = "panel: missing shape"; return -7; }
+    PanelSpec p{};
+    p.front_sign = 1;
+    if (w[0] == "sphere" || w[0] == "sph") {
+      if (w.size() < 5) { if (err) *err = "panel sphere: missing parameters"; return -7; }
+      p.shape = 2;
+      for (int d = 0; d < 3; ++d) p.center[d] = atof(w[1 + d].c_str());
+      p.radius = atof(w[4].c_str());
+      if (p.radius < 0) { p.radius = -p.radius; p.front_sign = -1; }
+    } else if (w[0] == "rect" || w[0] == "r") {
+      // panel rect +x x y z dy dz  (axis sign + perpendicular axis, corner, extents)
+      if (w.size() < 7) { if (err) *err = "panel rect: missing parameters"; return -7; }
+      p.shape = 0;
+      const std::string &ax = w[1];
+      p.front_sign = (ax[0] == '-') ? -1 : 1;
+      p.axis = ax.back() - 'x';
+      if (p.axis < 0 || p.axis > 2) { if (err) *err = "panel rect: bad axis"; return -7; }
+      double corner[3];
+      for (int d = 0; d < 3; ++d) corner[d] = atof(w[2 + d].c_str());
+      p.pos = corner[p.axis];
+      int k = 5;
+      for (int d = 0; d < 3; ++d) {
+        if (d == p.axis) { p.lo[d] = p.hi[d] = corner[d]; continue; }
+        const double ext = atof(w[k++].c_str());
+        p.lo[d] = std::min(corner[d], corner[d] + ext);
+        p.hi[d] = std::max(corner[d], corner[d] + ext);
+      }
+    } else {
+      if (err) *err = "panel shape not supported by the GPU engine: " + w[0];
+      return -7;
+    }
+    if ((int)sf.panels.size() >= kMaxPanels) { if (err) *err = "too many panels"; return -6; }
+    sf.panels.push_back(p);
+  } else if (word == "color" || word == "thickness" || word == "polygon" || word == "stipple" ||
+             word == "shininess") {
+  } else {
+    if (err) *err = "unsupported surface statement: " + word;
+    return -7;
+  }
+  return 0;
+}
+
+int load_config_file(Sim &sim, const std::string &path, const std::string &name, std::string *err) {
+  std::string full = path.empty() ? name : (path + "/" + name);
+  std::ifstream in(full);
+  if (!in) { if (err) *err = "cannot open " + full; return -3; }
+  sim.filepath = path;
+  std::string line;
+  std::vector<int> skip;  // ifdefine nesting: 1 = skipping
+  SurfaceDef *cur_srf = nullptr;
+  int lineno = 0;
+  while (std::getline(in, line)) {
+    ++lineno;
+    const size_t hash = line.find('#');
+    if (hash != std::string::npos) line = line.substr(0, hash);
+    for (auto &kv : sim.defines) {  // textual substitution of defined names
+      size_t pos = 0;
+      while ((pos = line.find(kv.first, pos)) != std::string::npos) {
+        const bool lb = pos == 0 || isspace((unsigned char)line[pos - 1]);
+        const size_t e = pos + kv.first.size();
+        const bool rb = e >= line.size() || isspace((unsigned char)line[e]);
+        if (lb && rb) { line.replace(pos, kv.first.size(), kv.second); pos += kv.second.size(); }
+        else pos = e;
+      }
+    }
+    std::istringstream is(line);
+    std::string word;
+    if (!(is >> word)) continue;
+    std::string rest;
+    std::getline(is, rest);
+    const bool skipping = !skip.empty() && skip.back();
+    if (word == "ifdefine" || word == "ifundefine") {
+      std::string nm;
+      std::istringstream(rest) >> nm;
+      bool def = sim.defines.count(nm) > 0;
+      bool take = (word == "ifdefine") ? def : !def;
+      skip.push_back(skipping || !take);
+      continue;
+    }
+    if (word == "else") {
+      if (!skip.empty()) {
+        const bool outer = skip.size() > 1 && skip[skip.size() - 2];
+        skip.back() = outer || !skip.back();
+      }
+      continue;
+    }
+    if (word == "endif") {
+      if (!skip.empty()) skip.pop_back();
+      continue;
+    }
+    if (skipping) continue;
+    if (word == "end_file") break;
+    if (word == "define") {
+      std::istringstream rs(rest);
+      std::string k, vv;
+      rs >> k;
+      std::getline(rs, vv);
+      const size_t b = vv.find_first_not_of(" \t");
+      sim.defines[k] = (b == std::string::npos) ? "" : vv.substr(b);
+      continue;
+    }
+    if (word == "start_surface") {
+      std::string nm;
+      std::istringstream(rest) >> nm;
+      SurfaceDef s;
+      s.name = nm.empty() ? "surf" + std::to_string(sim.surfaces.size()) : nm;
+      sim.surfaces.push_back(s);
+      cur_srf = &sim.surfaces.back();
+      sim.need_rebuild = true;
+      continue;
+    }
+    if (word == "end_surface") {
+      cur_srf = nullptr;
+      continue;
+    }
+    int rc;
+    if (cur_srf) rc = read_surface_statement(sim, *cur_srf, word, split_ws(rest), err);
+    else rc = read_config_statement(sim, word, rest, err);
+    if (rc) {
+      if (err) *err = full + ":" + std::to_string(lineno) + ": " + *err;
+      return rc;
+    }
+  }
+  return 0;
+}
+
+}  // namespace smolb

@@ -1,0 +1,105 @@
+// Host-side simulation description behind the libsmoldyn-compatible C API.
+#pragma once
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+
+namespace smolb {
+
+struct SpeciesDef {
+  std::string name;
+  double difc = 0;
+  double drift[3] = {0, 0, 0};
+};
+
+// One reaction (smoldyn.h:389 rxnstruct subset).
+struct RxnDef {
+  std::string name;
+  int order = 0;
+  int rct[2] = {0, 0};
+  int nprod = 0;
+  int prd[kMaxProd] = {0, 0, 0, 0};
+  double rate = -1;         // requested rate constant; <0 undefined
+  int rparamt = 0;          // RevParam
+  double rparam = 0;
+  double user_prdpos[kMaxProd][3] = {};  // for offset / fixed placement
+  double prob_user = -1;    // reaction_probability (order 2)
+  double bindrad_user = -1; // binding_radius (order 2)
+  double chi = -1;
+  bool disabled = false;
+  // derived by update (smolreact.c:1307-1577)
+  double prob = 0;
+  double bindrad2 = -1;
+  double unbindrad = 0;
+  double prdpos[kMaxProd][3] = {};
+};
+
+struct SurfaceDef {
+  std::string name;
+  // action per face for all species unless overridden: 0 reflect 1 transmit 2 absorb
+  int act_front = 1, act_back = 1;
+  uint32_t absorb_front = 0, absorb_back = 0, trans_front = 0, trans_back = 0, refl_front = 0,
+           refl_back = 0;
+  std::vector<PanelSpec> panels;
+};
+
+struct Command {
+  char type = 'E';        // 'E' every step, 'N' every n steps, 'i' interval
+  double on = 0, off = 1e300, dt = 0;
+  long long every = 1;
+  std::string text;       // e.g. "molcount out"
+  double next = 0;
+};
+
+struct Sim {
+  int dim = 3;
+  double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+  char btype[3][2] = {{'t', 't'}, {'t', 't'}, {'t', 't'}};
+  std::vector<SpeciesDef> species;   // [0] = "empty"
+  std::vector<RxnDef> rxn[3];
+  std::vector<SurfaceDef> surfaces;
+  double tstart = 0, tstop = 0, dt = 0, time = 0;
+  bool time_set = false;
+  long long seed = 0;
+  double molperbox = -1, boxsize = -1;
+  int gauss_table_size = 4096;
+  long long max_mol = -1;
+  int accuracy = 10;
+  // molecules waiting to be uploaded (absolute positions)
+  std::vector<double> pend_pos;
+  std::vector<int> pend_sp;
+  uint64_t host_rng = 0x853C49E6748FEA9Bull;
+  // runtime commands and output data tables
+  std::vector<Command> cmds;
+  std::map<std::string, std::vector<std::vector<double>>> outdata;
+  std::vector<std::string> outfiles;
+  std::map<std::string, std::string> defines;
+  std::string filepath;
+  // engine state
+  std::unique_ptr<Engine> eng;
+  bool need_update = true;     // parameters or structure changed
+  bool need_rebuild = true;    // engine must be (re)created
+  long long steps = 0;
+  bool started = false;
+  std::string flags;
+
+  Sim();
+  int species_index(const std::string &name) const;
+  int reaction_index(const std::string &name, int *order) const;
+  double rand_u01();
+};
+
+// Restatements of the reference's parameter derivation.
+int derive_reaction_params(Sim &sim, std::string *err);
+// Build engine inputs for a single-replicate simulation.
+int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err);
+// Text configuration reader (statement subset of smolsim.cpp:626 simreadstring).
+int read_config_statement(Sim &sim, const std::string &word, const std::string &rest, std::string *err);
+int load_config_file(Sim &sim, const std::string &path, const std::string &name, std::string *err);
+
+}  // namespace smolb

@@ -1,0 +1,196 @@
+"""GPU engine parity and behaviour tests (run on a B200 through the C ABI).
+
+Deterministic parity: one time step with injected displacements and injected
+first-order decisions, compared with the oracle's restatement of the
+reference step (oracle/engine_oracle.c) on the same inputs: survivor
+positions to 1e-5 of the box size (the engine stores FP32 box-local
+coordinates), identical sets of molecules consumed by second-order reactions
+away from binding-radius ties, identical product multisets.
+"""
+import numpy as np
+import pytest
+
+import smoldyn_b200 as sb
+from tests import gpu_cases as gc
+from tests import oracle_lib
+
+pytestmark = pytest.mark.gpu
+
+
+def _one_step_parity(n, L, wall, seed, rev_placement=None, frac=(0.4, 0.4, 0.2), uni_frac=0.1, kf=20.0,
+                     molperbox=None):
+    rng = np.random.default_rng(seed)
+    difc = (1.0, 1.0, 0.5)
+    dt = 0.01
+    s = gc.make_sim(L=L, wall=wall, kf=kf, difc=difc, dt=dt, rev_placement=rev_placement, molperbox=molperbox)
+    pos, sp, serno = gc.random_state(n, L, rng, frac)
+    s.set_molecules(pos, sp, serno)
+    bind, unb, _ = s.reaction_params("fwd")
+    _, unb_rev, _ = s.reaction_params("rev")
+    steps = np.sqrt(2 * np.asarray(difc)[sp - 1] * dt)
+    disp = rng.normal(size=(n, 3)) * steps[:, None]
+    force = np.where((sp == 3) & (rng.uniform(size=n) < uni_frac), 0, -1).astype(np.int32)
+    disp4 = np.concatenate([disp, force[:, None].astype(np.float64)], axis=1)
+    s.inject(serno, disp4)
+    s.run_steps(1)
+    gpos, gsp, gsn = s.molecules()
+    # oracle
+    dA, dB = difc[0], difc[1]
+    prdpos = (0.0, 0.0)
+    if unb_rev > 0:
+        prdpos = (unb_rev * dA / (dA + dB), -unb_rev * dB / (dA + dB))
+    net = gc.oracle_net(s, L, wall, difc, bind * bind, prdpos)
+    o = oracle_lib.ora_step(net, pos, sp, serno, disp, force)
+    return s, dict(pos=pos, sp=sp, serno=serno, disp=disp, bind=bind), (gpos, gsp, gsn), o
+
+
+def _compare(inp, g, o, L, wall):
+    gpos, gsp, gsn = g
+    periodic = wall == "p"
+    moved = gc.apply_walls_np(inp["pos"] + inp["disp"], L, wall)
+    ties = gc.near_threshold(moved, inp["sp"], inp["bind"] ** 2, L, periodic)
+    alive = o["fate"] != 2
+    amb = gc.ambiguous_set(moved, inp["sp"], inp["bind"] ** 2, L, periodic, alive)
+    tie_sn = {int(inp["serno"][i]) for i in ties | amb}
+    # survivors: molecules with original serial numbers
+    orig = gsn < (1 << 41)
+    g_surv = dict(zip(gsn[orig].tolist(), range(int(orig.sum()))))
+    gp = gpos[orig]
+    o_surv = o["serno"][o["parent"] == 0]
+    o_pos = o["pos"][o["parent"] == 0]
+    o_set = set(o_surv.tolist())
+    g_set = set(g_surv.keys())
+    diff = (o_set ^ g_set) - tie_sn
+    assert not diff, (len(diff), sorted(diff)[:10])
+    common = sorted(o_set & g_set)
+    oi = {int(k): i for i, k in enumerate(o_surv.tolist())}
+    a = np.array([o_pos[oi[k]] for k in common])
+    b = np.array([gp[g_surv[k]] for k in common])
+    d = gc.min_image(a - b, L, periodic)
+    assert np.abs(d).max() <= 1e-5 * L, np.abs(d).max()
+    # products: same count per species (ties excepted), same positions as a multiset
+    g_prod = gpos[~orig]
+    g_psp = gsp[~orig]
+    o_prod = o["pos"][o["parent"] != 0]
+    o_psp = o["sp"][o["parent"] != 0]
+    if not tie_sn:
+        for spc in (1, 2, 3):
+            assert (g_psp == spc).sum() == (o_psp == spc).sum(), spc
+        for spc in (1, 2, 3):
+            A = o_prod[o_psp == spc]
+            B = g_prod[g_psp == spc]
+            for x in A:
+                dd = np.abs(gc.min_image(B - x, L, periodic)).max(1)
+                assert dd.min() <= 1e-4 * L
+    return len(common)
+
+
+@pytest.mark.parametrize("wall", ["r", "p"])
+def test_deterministic_step_matches_oracle(wall):
+    L = 20.0
+    s, inp, g, o = _one_step_parity(4000, L, wall, seed=11, rev_placement=(sb.RPirrev, 0.0))
+    ncommon = _compare(inp, g, o, L, wall)
+    assert ncommon > 3000
+    ev = s.events()
+    assert ev[3] > 0  # some second-order events happened
+    assert ev[2] > 0  # and first-order ones
+
+
+def test_deterministic_step_small_boxes_and_long_steps():
+    # molperbox 0.5: boxes barely above the binding radius; large displacements
+    # cross several boxes and reflect off walls
+    L = 6.0
+    s, inp, g, o = _one_step_parity(1500, L, "r", seed=3, rev_placement=(sb.RPirrev, 0.0), molperbox=0.5)
+    _compare(inp, g, o, L, "r")
+
+
+def test_deterministic_products_with_unbinding_radius():
+    """C -> A + B with a fixed unbinding radius: products land at distance
+    sigma_u apart, split by D (smolreact.c:1545-1548); orientation is random."""
+    L = 20.0
+    s, inp, g, o = _one_step_parity(2000, L, "p", seed=8, rev_placement=(sb.RPunbindrad, 0.5), frac=(0.0, 0.0, 1.0),
+                                    uni_frac=0.3)
+    gpos, gsp, gsn = g
+    prod = gsn >= (1 << 41)
+    nA = int(((gsp == 1) & prod).sum())
+    nB = int(((gsp == 2) & prod).sum())
+    nfired = int((o["fate"] == 2).sum())
+    assert nA == nfired and nB == nfired and nfired > 400
+    # every A product has a B product at distance 0.5 (pairs share the rotation)
+    A = gpos[(gsp == 1) & prod]
+    B = gpos[(gsp == 2) & prod]
+    for x in A[:200]:
+        d = np.sqrt((gc.min_image(B - x, L, True) ** 2).sum(1))
+        assert np.abs(d - 0.5).min() < 1e-4
+
+
+def test_counts_conserved_and_positions_inside_reflective_box():
+    s = gc.make_sim(L=10.0, wall="r", kf=0.0, kr=0.0)
+    s.add_molecules("A", 3000)
+    s.add_molecules("B", 2000)
+    s.update()
+    s.run_steps(200)
+    pos, sp, sn = s.molecules()
+    assert len(sp) == 5000 and s.count("A") == 3000 and s.count("B") == 2000
+    assert pos.min() >= 0.0 and pos.max() <= 10.0
+
+
+def test_free_diffusion_msd():
+    """Mean squared displacement of free diffusion = 6 D t within 3 sigma."""
+    L = 1000.0
+    s = sb.Sim(3, (0, 0, 0), (L, L, L))
+    s.add_species("A", 1.0)
+    s.set_times(0, 100, 0.01)
+    s.seed(99)
+    for d in range(3):
+        s.boundary(d, -1, "r")
+    n = 20000
+    s.add_molecules("A", n, (450, 450, 450), (550, 550, 550))
+    s.update()
+    p0, _, sn0 = s.molecules()
+    s.run_steps(100)
+    p1, _, sn1 = s.molecules()
+    assert (sn0 == sn1).all()
+    r2 = ((p1 - p0) ** 2).sum(1)
+    t = 1.0
+    expect = 6 * 1.0 * t
+    sd = np.sqrt(24) * 1.0 * t / np.sqrt(n)
+    assert abs(r2.mean() - expect) < 3 * sd + 0.01 * expect, (r2.mean(), expect)
+    # per-axis displacement distribution is Gaussian with variance 2Dt
+    dx = (p1 - p0)[:, 0]
+    assert abs(dx.var() - 2.0) < 0.05
+
+
+def test_runs_are_reproducible():
+    out = []
+    for _ in range(2):
+        s = gc.make_sim(L=15.0, wall="p", kf=20.0, kr=5.0)
+        s.add_molecules("A", 3000)
+        s.add_molecules("B", 3000)
+        s.run_steps(50)
+        out.append(s.molecules())
+    assert len(out[0][1]) == len(out[1][1])
+    assert (out[0][2] == out[1][2]).all()
+    assert np.abs(out[0][0] - out[1][0]).max() == 0.0
+
+
+def test_device_radius_solver_matches_reference():
+    ref = oracle_lib.reference_rxnparam()
+    if ref is None:
+        pytest.skip("reference rxnparam not compiled")
+    rng = np.random.default_rng(4)
+    n = 2000
+    rate = 10 ** rng.uniform(-4, 2, n)
+    difc = 10 ** rng.uniform(-2, 1, n)
+    dt = 0.01
+    b = np.where(rng.uniform(size=n) < 0.5, -1.0, rng.uniform(1.1, 10, n))
+    out = sb.solve_radii_device(0, rate, dt, difc, b, rel=1)
+    exp = np.array([ref.bindingradius(rate[k], dt, difc[k], b[k], 1) for k in range(n)])
+    rel = np.abs(out - exp) / np.abs(exp)
+    assert rel.max() < 1e-9, rel.max()
+    pg = rng.uniform(0.05, 0.5, n)
+    uo = sb.solve_radii_device(1, pg, dt, difc, exp)
+    ue = np.array([ref.unbindingradius(pg[k], dt, difc[k], exp[k]) for k in range(n)])
+    ok = ue > 0
+    assert (np.abs(uo[ok] - ue[ok]) / ue[ok]).max() < 1e-9
+    assert np.array_equal(uo[~ok] <= 0, ue[~ok] <= 0)
