@@ -216,6 +216,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--ref-sample", type=int, default=100000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -297,6 +298,39 @@ def main():
     torch.cuda.synchronize()
 
     # ---- end to end through the C API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(sb, args, rank, world, dist, barrier)
+
+    # ---- CPU baseline (rank 0, single GPU run only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        n_s = args.ref_sample
+        res, why = time_reference_sample(n_s, 2, 12, 1)
+        if res is not None:
+            cpu = {"value": n_s / res["per_step_s"], "unit": METRIC, "cores": 1, "kind": "reference",
+                   "sample": "reference smoldyn binary, %d molecules in a periodic cube of side %.1f (same density "
+                             "and rates), per-step time from runs of 2 and 12 steps" % (n_s, res["side"])}
+        else:
+            cpu = {"value": None, "unit": METRIC, "cores": 1, "kind": "reference", "sample": why}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_s * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(args), "e2e": e2e, "gpu_launches": int(launches),
+            "roofline": roof, "step_roofline_frac": step_frac, "kernels": kernels, "cpu_baseline": cpu,
+            "clocks": ck,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def run_e2e(sb, args, rank, world, dist, barrier):
+    import torch
     s2 = build_sim(sb, N_MOL, L_SIDE, 101 + rank)
     pos, sp, sn = s2.molecules()  # host arrays (pending molecules)
     pos = np.ascontiguousarray(pos)
@@ -325,32 +359,7 @@ def main():
            "note": "includes the host->device upload of all molecules (amortised over the steps) and a "
                    "per-step species-count read-back"}
     s2.close()
-
-    # ---- CPU baseline (rank 0, single GPU run only)
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        n_s = args.ref_sample
-        res, why = time_reference_sample(n_s, 2, 12, 1)
-        if res is not None:
-            cpu = {"value": n_s / res["per_step_s"], "unit": METRIC, "cores": 1, "kind": "reference",
-                   "sample": "reference smoldyn binary, %d molecules in a periodic cube of side %.1f (same density "
-                             "and rates), per-step time from runs of 2 and 12 steps" % (n_s, res["side"])}
-        else:
-            cpu = {"value": None, "unit": METRIC, "cores": 1, "kind": "reference", "sample": why}
-
-    if rank == 0:
-        line = {
-            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": t_s * 1e3 / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": workload_config(args), "e2e": e2e, "gpu_launches": int(launches),
-            "roofline": roof, "step_roofline_frac": step_frac, "kernels": kernels, "cpu_baseline": cpu,
-            "clocks": ck,
-        }
-        print(json.dumps(line))
-    if dist is not None:
-        dist.destroy_process_group()
-    return 0
+    return e2e
 
 
 if __name__ == "__main__":

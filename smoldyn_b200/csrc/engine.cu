@@ -42,6 +42,7 @@ struct KParams {
   const uint32_t *unithr;  // [(rep*nsp + sp)*kMaxUniPerSpecies] cumulative thresholds
   const float *bind2;      // [rep*nr2 + r]
   const float *pairprob;   // [rep*nr2 + r]
+  const float *rsearch;    // [rep*nsp + sp] stencil radius of the pair search
   const double *births;    // [rep*nr0 + r]
   const float *prdpos;     // [((rep*nrx + k)*kMaxProd + p)*3]
   const float *gtab;       // gaussian table
@@ -212,7 +213,9 @@ __device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, co
   unpack_cell(__float_as_uint(pc.w), ix[0], ix[1], ix[2]);
   float u[3] = {pc.x, pc.y, pc.z};
   if (rebin_only) {
+#pragma unroll
     for (int d = 0; d < 3; ++d) renorm(u[d], ix[d], g.h[d], g.inv_h[d]);
+#pragma unroll
     for (int d = 0; d < 3; ++d) {
       if (ix[d] < 0) { u[d] = (float)ix[d] * g.h[d] + u[d]; ix[d] = 0; }
       if (ix[d] > g.n[d] - 1) { u[d] = (float)(ix[d] - (g.n[d] - 1)) * g.h[d] + u[d]; ix[d] = g.n[d] - 1; }
@@ -248,6 +251,7 @@ __device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, co
   }
   const int ix0[3] = {ix[0], ix[1], ix[2]};
   const float u0[3] = {u[0], u[1], u[2]};
+#pragma unroll
   for (int d = 0; d < 3; ++d) {
     if (d >= g.dim) continue;
     float w = u[d] + dsp[d];
@@ -269,7 +273,10 @@ __device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, co
     const float inv2 = (ds > 0.f) ? 1.f / (ds * ds) : 0.f;
     uint4 r2 = make_uint4(0, 0, 0, 0);
     int have = 0;
-    for (int d = 0; d < g.dim; ++d) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      if (d >= g.dim) continue;
+#pragma unroll
       for (int side = 0; side < 2; ++side) {
         if (g.wall[2 * d + side] != kWallAbsorb || ds <= 0.f) continue;
         float dn, dold;
@@ -527,20 +534,32 @@ __device__ int poisson_sample(double mean, uint2 key, uint4 ctr) {
   return (int)floor(mean + 0.5);
 }
 
+// One block per (replicate, reaction): thread 0 draws the Poisson number of
+// births and reserves event slots, then the block writes the events.
 __global__ void k_births(KParams p) {
   const int nr0 = c_net.nr[0];
   if (nr0 == 0) return;
+  __shared__ int s_base, s_n;
   const uint32_t step = *p.step;
   const uint2 key = make_uint2(c_net.key0 ^ 0x5bd1e995u, c_net.key1);
   const int total = c_net.nrep * nr0;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+  for (int t = blockIdx.x; t < total; t += gridDim.x) {
     const int rep = t / nr0, r = t % nr0;
-    const double mean = p.births[t];
-    const int nb = poisson_sample(mean, key, make_uint4((uint32_t)rep, (uint32_t)r, step, 0u));
-    if (nb <= 0) continue;
-    const int base = atomicAdd(p.nev, nb);
-    for (int k = 0; k < nb; ++k) {
-      if (base + k >= p.evcap) { atomicOr(p.status, kStEvCap); break; }
+    if (threadIdx.x == 0) {
+      const int nb = poisson_sample(p.births[t], key, make_uint4((uint32_t)rep, (uint32_t)r, step, 0u));
+      int base = 0;
+      if (nb > 0) {
+        base = atomicAdd(p.nev, nb);
+        atomicAdd(&p.counters[1], (unsigned long long)nb);
+        if (base + nb > p.evcap) atomicOr(p.status, kStEvCap);
+      }
+      s_base = base;
+      s_n = nb;
+    }
+    __syncthreads();
+    const int base = s_base, nb = s_n;
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+      if (base + k >= p.evcap) break;
       Event e;
       e.site = make_float4(0.f, 0.f, 0.f, 0.f);
       e.key = mix64(((ull)rep << 40) ^ ((ull)r << 32) ^ ((ull)step << 8) ^ 0xB17Aull ^
@@ -549,7 +568,7 @@ __global__ void k_births(KParams p) {
       e.rep = (uint32_t)rep;
       p.ev[base + k] = e;
     }
-    atomicAdd(&p.counters[1], (unsigned long long)nb);
+    __syncthreads();
   }
 }
 
@@ -589,20 +608,32 @@ __device__ ull search_partner(const KParams &p, int i, float4 pc, ull id, uint32
   const ull ka = id_stream(id);
   ull best = ~0ull;
   ncand = 0;
-  for (int dz = -1; dz <= 1; ++dz) {
+  // Only boxes that the sphere of the largest binding radius of this species
+  // can reach are scanned: the own box, plus a neighbour along an axis when
+  // the molecule lies within that radius of the shared face.  Boxes are at
+  // least one binding radius wide, so this covers every partner the full
+  // 27-box neighbourhood would (smolreact.c:3248-3298 scans all 26 neighbours).
+  const float rs = p.rsearch[rep * c_net.nsp + sp];
+  const float ub0 = (ix == g.n[0] - 1) ? g.whi[0] : g.h[0];
+  const float ub1 = (iy == g.n[1] - 1) ? g.whi[1] : g.h[1];
+  const float ub2 = (iz == g.n[2] - 1) ? g.whi[2] : g.h[2];
+  const int xlo = pc.x < rs ? -1 : 0, xhi = pc.x > ub0 - rs ? 1 : 0;
+  const int ylo = pc.y < rs ? -1 : 0, yhi = pc.y > ub1 - rs ? 1 : 0;
+  const int zlo = pc.z < rs ? -1 : 0, zhi = pc.z > ub2 - rs ? 1 : 0;
+  for (int dz = zlo; dz <= zhi; ++dz) {
     int z = iz + dz;
     if (z < 0 || z >= g.n[2]) {
       if (!pz) continue;
       z = (z < 0) ? z + g.n[2] : z - g.n[2];
     }
-    for (int dy = -1; dy <= 1; ++dy) {
+    for (int dy = ylo; dy <= yhi; ++dy) {
       int y = iy + dy;
       if (y < 0 || y >= g.n[1]) {
         if (!py) continue;
         y = (y < 0) ? y + g.n[1] : y - g.n[1];
       }
       const int rowbase = g.cell0 + (z * g.n[1] + y) * g.n[0];
-      for (int dx = -1; dx <= 1; ++dx) {
+      for (int dx = xlo; dx <= xhi; ++dx) {
         int x = ix + dx;
         if (x < 0 || x >= g.n[0]) {
           if (!px) continue;
@@ -915,6 +946,7 @@ class EngineImpl {
 
   // device memory
   DevGeo *d_geo = nullptr;
+  float *d_rsearch = nullptr;
   float *d_difstep = nullptr, *d_driftdt = nullptr, *d_bind2 = nullptr, *d_pairprob = nullptr,
         *d_prdpos = nullptr, *d_gtab = nullptr;
   uint32_t *d_unithr = nullptr;
@@ -942,12 +974,13 @@ class EngineImpl {
   void release() {
     if (graph2) cudaGraphExecDestroy(graph2);
     graph2 = nullptr;
-    void *ptrs[] = {d_geo, d_difstep, d_driftdt, d_bind2, d_pairprob, d_prdpos, d_gtab, d_unithr,
+    void *ptrs[] = {d_rsearch, d_geo, d_difstep, d_driftdt, d_bind2, d_pairprob, d_prdpos, d_gtab, d_unithr,
                     d_births, d_pc[0], d_pc[1], d_ppc[0], d_ppc[1], d_id[0], d_id[1], d_pid[0],
                     d_pid[1], d_counts, d_step, d_cnt, d_start, d_bsum, d_ev, d_cand, d_best,
                     d_counters, d_spcount, d_injkey, d_injval};
     for (void *q : ptrs)
       if (q) cudaFree(q);
+    d_rsearch = nullptr;
     d_geo = nullptr; d_difstep = d_driftdt = d_bind2 = d_pairprob = d_prdpos = d_gtab = nullptr;
     d_unithr = nullptr; d_births = nullptr;
     d_pc[0] = d_pc[1] = d_ppc[0] = d_ppc[1] = nullptr;
@@ -967,6 +1000,7 @@ class EngineImpl {
     p.unithr = d_unithr;
     p.bind2 = d_bind2;
     p.pairprob = d_pairprob;
+    p.rsearch = d_rsearch;
     p.births = d_births;
     p.prdpos = d_prdpos;
     p.gtab = d_gtab;
@@ -1078,6 +1112,7 @@ class EngineImpl {
     std::vector<uint32_t> unithr((size_t)R * nsp * kMaxUniPerSpecies, 0);
     const int nr2 = std::max(1, net.nrxn[2]), nr0 = std::max(1, net.nrxn[0]);
     std::vector<float> bind2((size_t)R * nr2, 0.f), pairprob((size_t)R * nr2, 1.f);
+    std::vector<float> rsearch((size_t)R * nsp, 0.f);
     std::vector<double> births((size_t)R * nr0, 0.0);
     const int nrx = std::max(1, dnet.nrx_total);
     std::vector<float> prdpos((size_t)R * nrx * kMaxProd * 3, 0.f);
@@ -1105,6 +1140,14 @@ class EngineImpl {
       for (int r = 0; r < net.nrxn[2]; ++r) {
         bind2[(size_t)rp * nr2 + r] = (float)s.bind2[r];
         pairprob[(size_t)rp * nr2 + r] = (float)s.pair_prob[r];
+        // stencil radius: largest binding radius of the species' pair reactions,
+        // padded so FP32 rounding of a distance at the radius cannot fall outside
+        const double hmin = std::min(geo[rp].h[0], std::min(geo[rp].h[1], geo[rp].h[2]));
+        const double rr = std::sqrt(std::max(0.0, s.bind2[r])) * (1.0 + 1e-4) + 1e-6 * hmin;
+        for (int k = 0; k < 2; ++k) {
+          float &v = rsearch[(size_t)rp * nsp + net.rct[2][r][k]];
+          v = std::max(v, (float)rr);
+        }
       }
       for (int r = 0; r < net.nrxn[0]; ++r) births[(size_t)rp * nr0 + r] = s.birth_mean[r];
       for (int o = 0; o < 3; ++o)
@@ -1124,6 +1167,7 @@ class EngineImpl {
     if (put((void **)&d_driftdt, driftdt.data(), driftdt.size() * 4)) return -8;
     if (put((void **)&d_unithr, unithr.data(), unithr.size() * 4)) return -8;
     if (put((void **)&d_bind2, bind2.data(), bind2.size() * 4)) return -8;
+    if (put((void **)&d_rsearch, rsearch.data(), rsearch.size() * 4)) return -8;
     if (put((void **)&d_pairprob, pairprob.data(), pairprob.size() * 4)) return -8;
     if (put((void **)&d_births, births.data(), births.size() * 8)) return -8;
     if (put((void **)&d_prdpos, prdpos.data(), prdpos.size() * 4)) return -8;
