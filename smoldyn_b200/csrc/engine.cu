@@ -34,6 +34,7 @@ namespace smolb {
 
 __constant__ DevNet c_net;
 __constant__ DevPanel c_panels[kMaxPanels];
+__constant__ DevGeo c_geo0;  // geometry of replicate 0 (used when the engine holds one replicate)
 
 struct KParams {
   const DevGeo *geo;
@@ -89,15 +90,24 @@ __device__ __forceinline__ unsigned lanemask_lt() {
   return m;
 }
 
+// Every floating-point operation on the move path below goes through an
+// explicitly rounded intrinsic (__fadd_rn, __fmul_rn, ...): the same molecule
+// move is evaluated in more than one kernel (the box histogram and the box
+// scatter), and those evaluations must agree bit for bit, which rules out
+// compiler-chosen FMA contraction.
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+
 // Bring local coordinate w (relative to the origin of cell j, j maybe out of
 // range) into cell form.
 __device__ __forceinline__ void renorm(float &w, int &j, float h, float inv_h) {
   if (w >= 0.f && w < h) return;
-  const int k = (int)floorf(w * inv_h);
+  const int k = (int)floorf(fmul(w, inv_h));
   j += k;
-  w -= (float)k * h;
-  if (w < 0.f) { j -= 1; w += h; }
-  else if (w >= h) { j += 1; w -= h; }
+  w = fsub(w, fmul((float)k, h));
+  if (w < 0.f) { j -= 1; w = fadd(w, h); }
+  else if (w >= h) { j += 1; w = fsub(w, h); }
 }
 
 // Apply the low and high wall of one dimension to (w, j) (smolwall.c:368-427,
@@ -109,46 +119,53 @@ __device__ __forceinline__ int walls_dim(float &w, int &j, const DevGeo &g, int 
     const int kind = g.wall[2 * d];
     hits++;
     if (kind == kWallReflect) {
-      float p = -((float)j * h + w);
+      const float q = -fadd(fmul((float)j, h), w);
       j = 0;
-      w = p;
+      w = q;
       renorm(w, j, h, inv_h);
     } else if (kind == kWallPeriodic) {
       j += n;
-      w += whi - h;
+      w = fadd(w, fsub(whi, h));
       renorm(w, j, h, inv_h);
     } else if (kind == kWallAbsorb) {
       return 1;
     } else {
-      w = (float)j * h + w;
+      w = fadd(fmul((float)j, h), w);
       j = 0;
     }
   }
   if (j >= n - 1) {
-    const float e = (float)(j - (n - 1)) * h + w - whi;  // signed distance beyond the high wall
+    // signed distance beyond the high wall
+    const float e = fsub(fadd(fmul((float)(j - (n - 1)), h), w), whi);
     if (e > 0.f) {
       const int kind = g.wall[2 * d + 1];
       hits++;
       if (kind == kWallReflect) {
         j = n - 1;
-        w = whi - e;
+        w = fsub(whi, e);
         renorm(w, j, h, inv_h);
         if (j < 0) {  // reflected past the low wall too (step longer than the box)
-          if (g.wall[2 * d] == kWallReflect) { w = -((float)j * h + w); j = 0; renorm(w, j, h, inv_h); }
-          else { w = (float)j * h + w; j = 0; }
+          if (g.wall[2 * d] == kWallReflect) {
+            w = -fadd(fmul((float)j, h), w);
+            j = 0;
+            renorm(w, j, h, inv_h);
+          } else {
+            w = fadd(fmul((float)j, h), w);
+            j = 0;
+          }
         }
       } else if (kind == kWallPeriodic) {
         j -= n;
-        w += h - whi;
+        w = fadd(w, fsub(h, whi));
         renorm(w, j, h, inv_h);
       } else if (kind == kWallAbsorb) {
         return 1;
       } else {
-        w = e + whi;
+        w = fadd(e, whi);
         j = n - 1;
       }
     } else if (j > n - 1) {  // inside the box but past the nominal last cell
-      w = e + whi;
+      w = fadd(e, whi);
       j = n - 1;
     }
   }
@@ -167,7 +184,7 @@ __device__ __forceinline__ void clamp_cell(float &w, int &j, const DevGeo &g, in
       const int k = (-j + n - 1) / n;
       j += k * n;
     } else {
-      w += (float)j * g.h[d];
+      w = fadd(w, fmul((float)j, g.h[d]));
       j = 0;
     }
   }
@@ -176,7 +193,7 @@ __device__ __forceinline__ void clamp_cell(float &w, int &j, const DevGeo &g, in
       const int k = j / n;
       j -= k * n;
     } else {
-      w += (float)(j - (n - 1)) * g.h[d];
+      w = fadd(w, fmul((float)(j - (n - 1)), g.h[d]));
       j = n - 1;
     }
   }
@@ -185,9 +202,9 @@ __device__ __forceinline__ void clamp_cell(float &w, int &j, const DevGeo &g, in
 }
 
 // Distance of a (cell, local) coordinate from the low / high wall.
-__device__ __forceinline__ float dist_low(int j, float w, float h) { return (float)j * h + w; }
+__device__ __forceinline__ float dist_low(int j, float w, float h) { return fadd(fmul((float)j, h), w); }
 __device__ __forceinline__ float dist_high(int j, float w, const DevGeo &g, int d) {
-  return (float)(g.n[d] - 1 - j) * g.h[d] + g.whi[d] - w;
+  return fsub(fadd(fmul((float)(g.n[d] - 1 - j), g.h[d]), g.whi[d]), w);
 }
 
 __device__ __forceinline__ int find_injection(const KParams &p, ull key) {
@@ -202,23 +219,31 @@ __device__ __forceinline__ int find_injection(const KParams &p, ull key) {
   return -1;
 }
 
-// Move one molecule by one step: returns 0 alive, 1 removed by a wall,
-// 2+r first-order reaction r fired (position is the post-move position).
+// Geometry of a replicate: from constant memory when the engine holds one
+// replicate (a plain simulation), else from the per-replicate table.
+template <bool SINGLE>
+__device__ __forceinline__ const DevGeo &geo_of(const KParams &p, int rep) {
+  if (SINGLE) return c_geo0;
+  return p.geo[rep];
+}
+
+// Move one molecule by one step (diffuse smolmolec.c:3115, checkwalls
+// smolwall.c:368, unireact decision smolreact.c:2997): returns 0 alive,
+// 1 removed by a wall, 2+r first-order reaction r fired (position is the
+// post-move position).
+template <bool SINGLE>
 __device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, const KParams &p,
                                            const float *gtab, int rebin_only, int &hits) {
   const int sp = id_species(id);
-  const int rep = id_rep(id);
-  const DevGeo g = p.geo[rep];
+  const int rep = SINGLE ? 0 : id_rep(id);
+  const DevGeo &g = geo_of<SINGLE>(p, rep);
   int ix[3];
   unpack_cell(__float_as_uint(pc.w), ix[0], ix[1], ix[2]);
   float u[3] = {pc.x, pc.y, pc.z};
   if (rebin_only) {
 #pragma unroll
-    for (int d = 0; d < 3; ++d) renorm(u[d], ix[d], g.h[d], g.inv_h[d]);
-#pragma unroll
     for (int d = 0; d < 3; ++d) {
-      if (ix[d] < 0) { u[d] = (float)ix[d] * g.h[d] + u[d]; ix[d] = 0; }
-      if (ix[d] > g.n[d] - 1) { u[d] = (float)(ix[d] - (g.n[d] - 1)) * g.h[d] + u[d]; ix[d] = g.n[d] - 1; }
+      renorm(u[d], ix[d], g.h[d], g.inv_h[d]);
       clamp_cell(u[d], ix[d], g, d);
     }
     pc = make_float4(u[0], u[1], u[2], __uint_as_float(pack_cell(ix[0], ix[1], ix[2])));
@@ -241,12 +266,14 @@ __device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, co
   } else {
     const float ds = p.difstep[rep * c_net.nsp + sp];
     const uint32_t gm = c_net.gmask;
-    dsp[0] = ds * gtab[r.x & gm];
-    dsp[1] = ds * gtab[r.y & gm];
-    dsp[2] = ds * gtab[r.z & gm];
+    dsp[0] = fmul(ds, gtab[r.x & gm]);
+    dsp[1] = fmul(ds, gtab[r.y & gm]);
+    dsp[2] = fmul(ds, gtab[r.z & gm]);
     if (c_net.any_drift) {
       const float *dr = p.driftdt + (size_t)(rep * c_net.nsp + sp) * 3;
-      dsp[0] += dr[0]; dsp[1] += dr[1]; dsp[2] += dr[2];
+      dsp[0] = fadd(dsp[0], dr[0]);
+      dsp[1] = fadd(dsp[1], dr[1]);
+      dsp[2] = fadd(dsp[2], dr[2]);
     }
   }
   const int ix0[3] = {ix[0], ix[1], ix[2]};
@@ -254,7 +281,7 @@ __device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, co
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     if (d >= g.dim) continue;
-    float w = u[d] + dsp[d];
+    float w = fadd(u[d], dsp[d]);
     int j = ix[d];
     renorm(w, j, g.h[d], g.inv_h[d]);
     if (j <= 0 || j >= g.n[d] - 1) {
@@ -270,7 +297,7 @@ __device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, co
     // test in both wall passes of a step (smolsim.cpp:2625 and :2662), so the
     // survival probability is (1-p)^2.
     const float ds = p.difstep[rep * c_net.nsp + sp];
-    const float inv2 = (ds > 0.f) ? 1.f / (ds * ds) : 0.f;
+    const float inv2 = (ds > 0.f) ? __frcp_rn(fmul(ds, ds)) : 0.f;
     uint4 r2 = make_uint4(0, 0, 0, 0);
     int have = 0;
 #pragma unroll
@@ -282,10 +309,10 @@ __device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, co
         float dn, dold;
         if (side == 0) { dn = dist_low(ix[d], u[d], g.h[d]); dold = dist_low(ix0[d], u0[d], g.h[d]); }
         else { dn = dist_high(ix[d], u[d], g, d); dold = dist_high(ix0[d], u0[d], g, d); }
-        const float x = 2.f * dn * dold * inv2;
+        const float x = fmul(fmul(2.f, fmul(dn, dold)), inv2);
         if (x > 80.f) continue;
         const float pr = __expf(-x);
-        const float pe = pr * (2.f - pr);  // 1-(1-p)^2
+        const float pe = fmul(pr, fsub(2.f, pr));  // 1-(1-p)^2
         if (!have) { r2 = philox(make_uint4((uint32_t)skey, (uint32_t)(skey >> 32), step, 1u), key); have = 1; }
         const uint32_t bits = (d == 0) ? (side ? r2.y : r2.x) : (d == 1) ? (side ? r2.w : r2.z)
                                         : (side ? (r2.x ^ r2.w) : (r2.y ^ r2.z));
@@ -329,18 +356,48 @@ __global__ void k_begin(KParams p, int bump_step) {
   }
 }
 
+// Stage the Gaussian quantile table in shared memory (16 KB at the default
+// 4096 levels); larger tables are read from global memory.
+__device__ __forceinline__ const float *stage_gtab(const KParams &p, float *s_gtab) {
+  const int gsize = (int)c_net.gmask + 1;
+  if (gsize > 8192) return p.gtab;
+  for (int k = threadIdx.x; k < gsize; k += blockDim.x) s_gtab[k] = p.gtab[k];
+  __syncthreads();
+  return s_gtab;
+}
+
+// Warp-aggregated increment of the box histogram for every lane with `alive`
+// set (one atomic per distinct box in the warp).
+template <bool SINGLE>
+__device__ __forceinline__ void count_box(const KParams &p, bool alive, float4 pc, ull id) {
+  const unsigned act = __ballot_sync(0xffffffffu, alive);
+  if (alive) {
+    const DevGeo &g = geo_of<SINGLE>(p, SINGLE ? 0 : id_rep(id));
+    const int cell = global_cell(g, __float_as_uint(pc.w));
+    const unsigned peers = __match_any_sync(act, cell);
+    if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&p.cnt[cell], __popc(peers));
+  }
+}
+
+// Next-step destination box of one molecule, counted (+1) or uncounted (-1)
+// outside the bulk passes (reacting pairs, new products).
+template <bool SINGLE>
+__device__ __forceinline__ void recount_next(const KParams &p, float4 pc, ull id, uint32_t nstep, int sign) {
+  int hits = 0;
+  if (advance_one<SINGLE>(pc, id, nstep, p, p.gtab, 0, hits) != 0) return;
+  const DevGeo &g = geo_of<SINGLE>(p, SINGLE ? 0 : id_rep(id));
+  atomicAdd(&p.cnt[global_cell(g, __float_as_uint(pc.w))], sign);
+}
+
 // phase bit 0: 0 = count, 1 = scatter.  bit 1: rebin only (no motion, no reactions).
+// In steady state the count of step t+1 is taken inside k_pairs of step t (it
+// reads every molecule anyway), so only the scatter phase runs per step.
+template <bool SINGLE>
 __global__ void __launch_bounds__(256) k_advance(KParams p, int phase) {
   extern __shared__ float s_gtab[];
   const int rebin_only = (phase >> 1) & 1;
   const int scatter = phase & 1;
-  const int gsize = (int)c_net.gmask + 1;
-  const float *gtab = p.gtab;
-  if (!rebin_only && gsize <= 8192) {
-    for (int k = threadIdx.x; k < gsize; k += blockDim.x) s_gtab[k] = p.gtab[k];
-    __syncthreads();
-    gtab = s_gtab;
-  }
+  const float *gtab = rebin_only ? p.gtab : stage_gtab(p, s_gtab);
   const int na = *p.a_n, np = *p.p_n;
   const int total = na + np;
   const uint32_t step = *p.step;
@@ -358,32 +415,32 @@ __global__ void __launch_bounds__(256) k_advance(KParams p, int phase) {
     }
     int fate = -1;
     int hits = 0;
-    if (valid) fate = advance_one(pc, id, step, p, gtab, rebin_only, hits);
+    if (valid) fate = advance_one<SINGLE>(pc, id, step, p, gtab, rebin_only, hits);
     const bool alive = (fate == 0);
+    if (!scatter) {
+      count_box<SINGLE>(p, alive, pc, id);
+      continue;
+    }
     const unsigned act = __ballot_sync(0xffffffffu, alive);
     if (alive) {
-      const int rep = id_rep(id);
-      const int cell = global_cell(p.geo[rep], __float_as_uint(pc.w));
+      const DevGeo &g = geo_of<SINGLE>(p, SINGLE ? 0 : id_rep(id));
+      const int cell = global_cell(g, __float_as_uint(pc.w));
       const unsigned peers = __match_any_sync(act, cell);
       const int leader = __ffs(peers) - 1;
       const int npeer = __popc(peers);
       const int rank = __popc(peers & lanemask_lt());
-      if (!scatter) {
-        if (lane == leader) atomicAdd(&p.cnt[cell], npeer);
+      int old = 0;
+      if (lane == leader) old = atomicSub(&p.cnt[cell], npeer);
+      old = __shfl_sync(peers, old, leader);
+      const int slot = p.start[cell] + old - npeer + rank;
+      if (slot >= 0 && slot < p.cap) {
+        p.b_pc[slot] = pc;
+        p.b_id[slot] = id;
       } else {
-        int old = 0;
-        if (lane == leader) old = atomicSub(&p.cnt[cell], npeer);
-        old = __shfl_sync(peers, old, leader);
-        const int slot = p.start[cell] + old - npeer + rank;
-        if (slot >= 0 && slot < p.cap) {
-          p.b_pc[slot] = pc;
-          p.b_id[slot] = id;
-        } else {
-          atomicOr(p.status, kStMolCap);
-        }
+        atomicOr(p.status, kStMolCap);
       }
     }
-    if (scatter && valid) {
+    if (valid) {
       hits_acc += hits;
       if (fate == 1) {
         atomicAdd((unsigned long long *)&p.spcount[id_rep(id) * c_net.nsp + id_species(id)],
@@ -663,22 +720,41 @@ __device__ ull search_partner(const KParams &p, int i, float4 pc, ull id, uint32
   return best;
 }
 
-__global__ void __launch_bounds__(256) k_pairs(KParams p) {
+// Pair search over the box-sorted molecules; also counts every molecule's
+// box for the next step (the histogram the next scatter needs).
+template <bool SINGLE>
+__global__ void __launch_bounds__(256, 2) k_pairs(KParams p, int count_next) {
+  extern __shared__ float s_gtab[];
+  const float *gtab = count_next ? stage_gtab(p, s_gtab) : p.gtab;
   const int n = *p.b_n;
   const uint32_t step = *p.step;
   int multi = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const ull id = p.b_id[i];
-    const int sp = id_species(id);
-    if (sp == kDeadSpecies || c_net.pair_mask[sp] == 0) continue;
-    int nc;
-    const ull best = search_partner(p, i, p.b_pc[i], id, step, nc);
-    if (best != ~0ull) {
-      p.best[i] = best;
-      const int k = atomicAdd(p.ncand, 1);
-      if (k < p.candcap) p.cand[k] = i;
-      else atomicOr(p.status, kStCandCap);
-      if (nc > 1) multi++;
+  for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const int i = base + threadIdx.x;
+    bool valid = i < n;
+    float4 pc = make_float4(0.f, 0.f, 0.f, 0.f);
+    ull id = 0;
+    if (valid) {
+      pc = p.b_pc[i];
+      id = p.b_id[i];
+      valid = id_species(id) != kDeadSpecies;
+    }
+    if (valid && c_net.pair_mask[id_species(id)] != 0) {
+      int nc;
+      const ull best = search_partner(p, i, pc, id, step, nc);
+      if (best != ~0ull) {
+        p.best[i] = best;
+        const int k = atomicAdd(p.ncand, 1);
+        if (k < p.candcap) p.cand[k] = i;
+        else atomicOr(p.status, kStCandCap);
+        if (nc > 1) multi++;
+      }
+    }
+    if (count_next) {
+      int fate = -1, hits = 0;
+      float4 npc = pc;
+      if (valid) fate = advance_one<SINGLE>(npc, id, step + 1, p, gtab, 0, hits);
+      count_box<SINGLE>(p, fate == 0, npc, id);
     }
   }
   if (multi) atomicAdd(&p.counters[5], (unsigned long long)multi);
@@ -735,7 +811,8 @@ __device__ __forceinline__ float4 pair_site(const KParams &p, int i, int j, int 
   return make_float4(w[0], w[1], w[2], __uint_as_float(pack_cell(cell[0], cell[1], cell[2])));
 }
 
-__global__ void k_commit(KParams p) {
+template <bool SINGLE>
+__global__ void k_commit(KParams p, int count_next) {
   const int nc = min(*p.ncand, p.candcap);
   const uint32_t step = *p.step;
   int done = 0;
@@ -766,6 +843,10 @@ __global__ void k_commit(KParams p) {
     push_event(p, e);
     p.b_id[i] = id_mark_dead(idi);
     p.b_id[j] = id_mark_dead(idj);
+    if (count_next) {  // they were counted for the next step in k_pairs
+      recount_next<SINGLE>(p, p.b_pc[i], idi, step + 1, -1);
+      recount_next<SINGLE>(p, p.b_pc[j], idj, step + 1, -1);
+    }
     atomicAdd((unsigned long long *)&p.spcount[rep * c_net.nsp + spi], (unsigned long long)(-1ll));
     atomicAdd((unsigned long long *)&p.spcount[rep * c_net.nsp + spj], (unsigned long long)(-1ll));
     done++;
@@ -788,7 +869,8 @@ __device__ __forceinline__ void random_rotation(uint4 r, float m[9]) {
   m[6] = 2.f * (qx * qz - qy * qw); m[7] = 2.f * (qy * qz + qx * qw); m[8] = 1.f - 2.f * (qx * qx + qy * qy);
 }
 
-__global__ void k_products(KParams p) {
+template <bool SINGLE>
+__global__ void k_products(KParams p, int count_next) {
   const int ne = min(*p.nev, p.evcap);
   const uint32_t step = *p.step;
   const uint2 key = make_uint2(c_net.key0 ^ 0x68E31DA4u, c_net.key1 ^ 0xB5297A4Du);
@@ -862,8 +944,11 @@ __global__ void k_products(KParams p) {
                          (kProductSernoBit - 1));
       const int slot = atomicAdd(p.q_n, 1);
       if (slot < p.pcap) {
-        p.q_pc[slot] = make_float4(w[0], w[1], w[2], __uint_as_float(pack_cell(c[0], c[1], c[2])));
-        p.q_id[slot] = make_id(psp, rep, serno);
+        const float4 npc = make_float4(w[0], w[1], w[2], __uint_as_float(pack_cell(c[0], c[1], c[2])));
+        const ull nid = make_id(psp, rep, serno);
+        p.q_pc[slot] = npc;
+        p.q_id[slot] = nid;
+        if (count_next) recount_next<SINGLE>(p, npc, nid, step + 1, +1);
         atomicAdd((unsigned long long *)&p.spcount[rep * c_net.nsp + psp], 1ull);
       } else {
         atomicOr(p.status, kStProdCap);
@@ -881,15 +966,28 @@ __global__ void k_fix_count(int *q_n, int pcap) {
   if (threadIdx.x == 0 && *q_n > pcap) *q_n = pcap;
 }
 
-// Count live molecules per (rep, species) from scratch (used after uploads).
-__global__ void k_species_count(const ull *id, const int *n, long long *spcount, int nsp) {
+// Count live molecules per (rep, species) from scratch (used after uploads);
+// per-block shared-memory tallies when the table is small, so that millions
+// of molecules of a few species do not serialise on a handful of addresses.
+__global__ void k_species_count(const ull *id, const int *n, long long *spcount, int nsp, int ntab) {
+  __shared__ unsigned int s_cnt[1024];
+  const bool local = ntab <= 1024;
+  if (local)
+    for (int k = threadIdx.x; k < ntab; k += blockDim.x) s_cnt[k] = 0;
+  __syncthreads();
   const int nn = *n;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
     const ull x = id[i];
     const int sp = id_species(x);
     if (sp == kDeadSpecies) continue;
-    atomicAdd((unsigned long long *)&spcount[id_rep(x) * nsp + sp], 1ull);
+    const int k = id_rep(x) * nsp + sp;
+    if (local) atomicAdd(&s_cnt[k], 1u);
+    else atomicAdd((unsigned long long *)&spcount[k], 1ull);
   }
+  __syncthreads();
+  if (local)
+    for (int k = threadIdx.x; k < ntab; k += blockDim.x)
+      if (s_cnt[k]) atomicAdd((unsigned long long *)&spcount[k], (unsigned long long)s_cnt[k]);
 }
 
 // Batched FP64 radius solve (one thread per problem).
@@ -1059,15 +1157,23 @@ class EngineImpl {
     marks.push_back({name, e});
   }
 
-  // Enqueue one step with the given parity.
-  void enqueue_step(int par, bool rebin_only) {
+  // Box histogram of the next step is already in d_cnt (taken by the previous
+  // step's k_pairs / k_commit / k_products).  False after uploads, injected
+  // steps and profiling changes; then a step starts with an explicit count pass.
+  bool counts_ready = false;
+
+  template <bool SINGLE>
+  void enqueue_step_t(int par, bool rebin_only, bool fuse_next) {
     KParams p = params(par);
     cudaStream_t s = stream;
     k_begin<<<1, 32, 0, s>>>(p, rebin_only ? 0 : 1);
     mark("k_begin");
     const int ph = rebin_only ? 2 : 0;
-    k_advance<<<grid_mol(), 256, rebin_only ? 0 : adv_smem(), s>>>(p, ph | 0);
-    mark("k_advance_count");
+    if (rebin_only || !counts_ready) {
+      cudaMemsetAsync(d_cnt, 0, ((size_t)ncell + 1) * sizeof(int), s);
+      k_advance<SINGLE><<<grid_mol(), 256, rebin_only ? 0 : adv_smem(), s>>>(p, ph | 0);
+      mark("k_advance_count");
+    }
     k_scan_reduce<<<nscanblocks, kScanThreads, 0, s>>>(d_cnt, ncell, d_bsum);
     mark("k_scan_reduce");
     k_scan_blocks<<<1, 1024, 0, s>>>(d_bsum, nscanblocks);
@@ -1075,31 +1181,46 @@ class EngineImpl {
     k_scan_apply<<<nscanblocks, kScanThreads, 0, s>>>(d_cnt, ncell, d_bsum, nscanblocks, d_start,
                                                       p.b_n, (int)cap);
     mark("k_scan_apply");
-    k_advance<<<grid_mol(), 256, rebin_only ? 0 : adv_smem(), s>>>(p, ph | 1);
+    k_advance<SINGLE><<<grid_mol(), 256, rebin_only ? 0 : adv_smem(), s>>>(p, ph | 1);
     mark("k_advance_scatter");
-    if (rebin_only) return;
+    if (rebin_only) {
+      counts_ready = false;
+      return;
+    }
+    const int cn = fuse_next ? 1 : 0;
     k_births<<<grid_small(), 128, 0, s>>>(p);
     mark("k_births");
-    k_pairs<<<grid_mol(), 256, 0, s>>>(p);
+    k_pairs<SINGLE><<<grid_mol(), 256, cn ? adv_smem() : 0, s>>>(p, cn);
     mark("k_pairs");
-    k_commit<<<grid_small(), 128, 0, s>>>(p);
+    k_commit<SINGLE><<<grid_small(), 128, 0, s>>>(p, cn);
     mark("k_commit");
     for (int round = 1; round < dnet.rounds; ++round) {
       k_research<<<grid_small(), 128, 0, s>>>(p);
       mark("k_research");
-      k_commit<<<grid_small(), 128, 0, s>>>(p);
+      k_commit<SINGLE><<<grid_small(), 128, 0, s>>>(p, cn);
       mark("k_commit");
     }
-    k_products<<<grid_small(), 128, 0, s>>>(p);
+    k_products<SINGLE><<<grid_small(), 128, 0, s>>>(p, cn);
     mark("k_products");
     k_fix_count<<<1, 32, 0, s>>>(p.q_n, (int)pcap);
     mark("k_fix_count");
+    counts_ready = fuse_next;
   }
 
-  int launches_per_step() const { return 11 + 2 * (dnet.rounds - 1); }
+  // Enqueue one step with the given parity.  fuse_next: take the next step's
+  // box histogram inside this step (not when the next step's moves will differ,
+  // e.g. after an injected step).
+  void enqueue_step(int par, bool rebin_only, bool fuse_next = true) {
+    if (reps.size() == 1) enqueue_step_t<true>(par, rebin_only, fuse_next);
+    else enqueue_step_t<false>(par, rebin_only, fuse_next);
+  }
+
+  int launches_per_step() const { return 10 + 2 * (dnet.rounds - 1); }
 
   int upload_const(std::string *err) {
     CK(cudaMemcpyToSymbolAsync(c_net, &dnet, sizeof(DevNet), 0, cudaMemcpyHostToDevice, stream));
+    if (!geo.empty())
+      CK(cudaMemcpyToSymbolAsync(c_geo0, geo.data(), sizeof(DevGeo), 0, cudaMemcpyHostToDevice, stream));
     if (!panels.empty())
       CK(cudaMemcpyToSymbolAsync(c_panels, panels.data(), panels.size() * sizeof(DevPanel), 0,
                                  cudaMemcpyHostToDevice, stream));
@@ -1382,7 +1503,6 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
   }
   int rc = E.build_rep_tables(err);
   if (rc) return rc;
-  CK(cudaFuncSetAttribute(k_advance, cudaFuncAttributeMaxDynamicSharedMemorySize, 32768));
   E.nsteps = 0;
   E.parity = 0;
   return 0;
@@ -1392,6 +1512,7 @@ int Engine::update_reps(const std::vector<RepSpec> &reps, std::string *err) {
   EngineImpl &E = *impl_;
   if (reps.size() != E.reps.size()) { if (err) *err = "replicate count changed"; return -6; }
   E.reps = reps;
+  E.counts_ready = false;  // first-order probabilities and step lengths changed
   return E.build_rep_tables(err);
 }
 
@@ -1461,7 +1582,8 @@ int Engine::set_molecules(long long n, const double *pos, const int *species, co
   E.parity = 1;
   CK(cudaMemsetAsync(E.d_counts + 2, 0, 2 * sizeof(int), E.stream));
   CK(cudaMemsetAsync(E.d_spcount, 0, E.reps.size() * E.net.nspecies * sizeof(long long), E.stream));
-  k_species_count<<<E.grid_mol(), 256, 0, E.stream>>>(E.d_id[1], E.d_counts + 1, E.d_spcount, E.net.nspecies);
+  k_species_count<<<E.grid_mol(), 256, 0, E.stream>>>(E.d_id[1], E.d_counts + 1, E.d_spcount, E.net.nspecies,
+                                                      (int)E.reps.size() * E.net.nspecies);
   E.nlaunch++;
   CK(cudaStreamSynchronize(E.stream));
   CK(cudaGetLastError());
@@ -1479,9 +1601,21 @@ int Engine::run(long long nsteps, std::string *err) {
     if (nsteps != 1) { if (err) *err = "injected displacements apply to one step"; return -6; }
   }
   long long done = 0;
+  if (inj) {
+    // the injected moves differ from the next step's, so nothing is fused
+    E.counts_ready = false;
+    E.enqueue_step(E.parity, false, false);
+    E.parity ^= 1;
+    done = 1;
+  }
   if (E.use_graph && !inj) {
-    // odd parity first step if needed so that graph replays start at parity 0
-    if (E.parity == 1) {
+    // graph replays start at parity 0 with the next histogram already taken
+    if (E.parity == 1 || !E.counts_ready) {
+      E.enqueue_step(E.parity, false);
+      E.parity ^= 1;
+      done++;
+    }
+    if (E.parity == 1 && nsteps - done >= 1) {
       E.enqueue_step(1, false);
       E.parity = 0;
       done++;
@@ -1642,6 +1776,7 @@ int Engine::set_injection(long long n, const uint64_t *sernos, const double *dis
   CK(cudaMemcpy(E.d_injval, vals.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
   E.inj_n = (int)n;
   E.dnet.inject = 1;
+  E.counts_ready = false;
   E.invalidate_graph();
   return E.upload_const(err);
 }
