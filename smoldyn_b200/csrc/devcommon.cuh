@@ -92,7 +92,8 @@ struct DevNet {
   int rounds;          // pair conflict-resolution rounds
   int uni_n[kMaxSpecies];
   uint8_t uni_list[kMaxSpecies][kMaxUniPerSpecies];
-  uint32_t pair_mask[kMaxSpecies];
+  uint32_t pair_mask[kMaxSpecies];    // partner species of a pair reaction
+  uint32_t search_mask[kMaxSpecies];  // partners searched in round 1: each pair once
   uint8_t pair_n[kMaxSpecies][kMaxSpecies];
   uint8_t pair_list[kMaxSpecies][kMaxSpecies][kMaxPairRxn];
   uint8_t rct[3][kMaxRxn][2];

@@ -720,12 +720,93 @@ __device__ ull search_partner(const KParams &p, int i, float4 pc, ull id, uint32
   return best;
 }
 
+// Record candidate key k in best[x]; the first registration of x appends it
+// to the candidate list.  Returns 1 if x already had a candidate.
+__device__ __forceinline__ int register_candidate(const KParams &p, int x, ull k) {
+  const ull old = atomicMin(&p.best[x], k);
+  if (old == ~0ull) {
+    const int t = atomicAdd(p.ncand, 1);
+    if (t < p.candcap) p.cand[t] = x;
+    else atomicOr(p.status, kStCandCap);
+    return 0;
+  }
+  return 1;
+}
+
+// Round-1 pair search: every in-radius pair is tested once, by its molecule of
+// the lower species index (or the lower sorted index for like species), and
+// registered on both molecules as packed (dist2 bits << 32 | partner) keys.
+__device__ int search_round1(const KParams &p, int i, float4 pc, ull id, uint32_t step) {
+  const int nsorted = *p.b_n;
+  const int sp = id_species(id);
+  const int rep = id_rep(id);
+  const DevGeo &g = p.geo[rep];
+  const uint32_t mask = c_net.search_mask[sp];
+  int ix, iy, iz;
+  unpack_cell(__float_as_uint(pc.w), ix, iy, iz);
+  const bool px = g.wall[0] == kWallPeriodic, py = g.wall[2] == kWallPeriodic, pz = g.wall[4] == kWallPeriodic;
+  const ull ka = id_stream(id);
+  const float rs = p.rsearch[rep * c_net.nsp + sp];
+  const float rs2 = rs * rs;
+  const float ub0 = (ix == g.n[0] - 1) ? g.whi[0] : g.h[0];
+  const float ub1 = (iy == g.n[1] - 1) ? g.whi[1] : g.h[1];
+  const float ub2 = (iz == g.n[2] - 1) ? g.whi[2] : g.h[2];
+  const int xlo = pc.x < rs ? -1 : 0, xhi = pc.x > ub0 - rs ? 1 : 0;
+  const int ylo = pc.y < rs ? -1 : 0, yhi = pc.y > ub1 - rs ? 1 : 0;
+  const int zlo = pc.z < rs ? -1 : 0, zhi = pc.z > ub2 - rs ? 1 : 0;
+  ull best = ~0ull;
+  int extra = 0;
+  for (int dz = zlo; dz <= zhi; ++dz) {
+    int z = iz + dz;
+    if (z < 0 || z >= g.n[2]) {
+      if (!pz) continue;
+      z = (z < 0) ? z + g.n[2] : z - g.n[2];
+    }
+    for (int dy = ylo; dy <= yhi; ++dy) {
+      int y = iy + dy;
+      if (y < 0 || y >= g.n[1]) {
+        if (!py) continue;
+        y = (y < 0) ? y + g.n[1] : y - g.n[1];
+      }
+      const int rowbase = g.cell0 + (z * g.n[1] + y) * g.n[0];
+      for (int dx = xlo; dx <= xhi; ++dx) {
+        int x = ix + dx;
+        if (x < 0 || x >= g.n[0]) {
+          if (!px) continue;
+          x = (x < 0) ? x + g.n[0] : x - g.n[0];
+        }
+        const int c = rowbase + x;
+        const int s = p.start[c], e = min(p.start[c + 1], nsorted);
+        for (int j = s; j < e; ++j) {
+          const ull jd = p.b_id[j];
+          const int spj = id_species(jd);
+          if (!((mask >> spj) & 1u) || (spj == sp && j <= i)) continue;
+          const float4 q = p.b_pc[j];
+          const float vx = (q.x - pc.x) + (float)dx * g.h[0];
+          const float vy = (q.y - pc.y) + (float)dy * g.h[1];
+          const float vz = (q.z - pc.z) + (float)dz * g.h[2];
+          const float d2 = vx * vx + vy * vy + vz * vz;
+          if (d2 > rs2) continue;
+          if (pair_reaction(p, rep, sp, spj, d2, ka, id_stream(jd), step) < 0) continue;
+          const uint32_t db = __float_as_uint(d2);
+          const ull k = ((ull)db << 32) | (uint32_t)j;
+          if (best != ~0ull) extra++;
+          if (k < best) best = k;
+          extra += register_candidate(p, j, ((ull)db << 32) | (uint32_t)i);
+        }
+      }
+    }
+  }
+  if (best != ~0ull) extra += register_candidate(p, i, best);
+  return extra;
+}
+
 // Pair search over the box-sorted molecules; also counts every molecule's
 // box for the next step (the histogram the next scatter needs).
-template <bool SINGLE>
-__global__ void __launch_bounds__(256, 2) k_pairs(KParams p, int count_next) {
+template <bool SINGLE, bool FUSE>
+__global__ void __launch_bounds__(256, 2) k_pairs(KParams p) {
   extern __shared__ float s_gtab[];
-  const float *gtab = count_next ? stage_gtab(p, s_gtab) : p.gtab;
+  const float *gtab = FUSE ? stage_gtab(p, s_gtab) : p.gtab;
   const int n = *p.b_n;
   const uint32_t step = *p.step;
   int multi = 0;
@@ -739,18 +820,8 @@ __global__ void __launch_bounds__(256, 2) k_pairs(KParams p, int count_next) {
       id = p.b_id[i];
       valid = id_species(id) != kDeadSpecies;
     }
-    if (valid && c_net.pair_mask[id_species(id)] != 0) {
-      int nc;
-      const ull best = search_partner(p, i, pc, id, step, nc);
-      if (best != ~0ull) {
-        p.best[i] = best;
-        const int k = atomicAdd(p.ncand, 1);
-        if (k < p.candcap) p.cand[k] = i;
-        else atomicOr(p.status, kStCandCap);
-        if (nc > 1) multi++;
-      }
-    }
-    if (count_next) {
+    if (valid && c_net.search_mask[id_species(id)] != 0) multi += search_round1(p, i, pc, id, step);
+    if (FUSE) {
       int fate = -1, hits = 0;
       float4 npc = pc;
       if (valid) fate = advance_one<SINGLE>(npc, id, step + 1, p, gtab, 0, hits);
@@ -1161,6 +1232,11 @@ class EngineImpl {
   // step's k_pairs / k_commit / k_products).  False after uploads, injected
   // steps and profiling changes; then a step starts with an explicit count pass.
   bool counts_ready = false;
+  // Take the next step's histogram inside k_pairs/k_commit/k_products instead
+  // of a separate count pass (saves one read of every molecule; off by default:
+  // on B200 the extra move evaluation made the pair kernel slower than the
+  // count pass it replaced).
+  bool fuse_count = false;
 
   template <bool SINGLE>
   void enqueue_step_t(int par, bool rebin_only, bool fuse_next) {
@@ -1190,7 +1266,8 @@ class EngineImpl {
     const int cn = fuse_next ? 1 : 0;
     k_births<<<grid_small(), 128, 0, s>>>(p);
     mark("k_births");
-    k_pairs<SINGLE><<<grid_mol(), 256, cn ? adv_smem() : 0, s>>>(p, cn);
+    if (cn) k_pairs<SINGLE, true><<<grid_mol(), 256, adv_smem(), s>>>(p);
+    else k_pairs<SINGLE, false><<<grid_mol(), 256, 0, s>>>(p);
     mark("k_pairs");
     k_commit<SINGLE><<<grid_small(), 128, 0, s>>>(p, cn);
     mark("k_commit");
@@ -1211,6 +1288,7 @@ class EngineImpl {
   // box histogram inside this step (not when the next step's moves will differ,
   // e.g. after an injected step).
   void enqueue_step(int par, bool rebin_only, bool fuse_next = true) {
+    fuse_next = fuse_next && fuse_count;
     if (reps.size() == 1) enqueue_step_t<true>(par, rebin_only, fuse_next);
     else enqueue_step_t<false>(par, rebin_only, fuse_next);
   }
@@ -1377,6 +1455,7 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
       if (D.pair_n[x][y] >= kMaxPairRxn) { if (err) *err = "too many reactions for one reactant pair"; return -6; }
       D.pair_list[x][y][D.pair_n[x][y]++] = (uint8_t)r;
       D.pair_mask[x] |= 1u << y;
+      if (x <= y) D.search_mask[x] |= 1u << y;  // the lower species index searches
     }
   }
   for (int o = 0; o < 3; ++o)
