@@ -801,6 +801,141 @@ __device__ int search_round1(const KParams &p, int i, float4 pc, ull id, uint32_
   return extra;
 }
 
+// Pair test shared by the staged and the neighbour-box paths: if i and j react
+// this step, fold the key into i's running best and register i on j.
+__device__ __forceinline__ void try_pair(const KParams &p, int i, ull idi, int sp, int rep, float d2, int j, ull jd,
+                                         float rs2, uint32_t step, ull &best, int &extra) {
+  const int spj = id_species(jd);
+  if (spj == kDeadSpecies || !((c_net.pair_mask[sp] >> spj) & 1u) || d2 > rs2) return;
+  if (pair_reaction(p, rep, sp, spj, d2, id_stream(idi), id_stream(jd), step) < 0) return;
+  const uint32_t db = __float_as_uint(d2);
+  const ull k = ((ull)db << 32) | (uint32_t)j;
+  if (best != ~0ull) extra++;
+  if (k < best) best = k;
+  extra += register_candidate(p, j, ((ull)db << 32) | (uint32_t)i);
+}
+
+constexpr int kPairTile = 256;  // molecules per block tile
+constexpr int kPairHalo = 32;   // extra molecules staged past the tile
+
+// Round-1 pair search, block-cooperative.  Each block stages a tile of 256
+// box-sorted molecules plus a 32-molecule halo in shared memory.  Pairs inside
+// a box are tested from shared memory by the lower-indexed molecule (boxes are
+// contiguous runs of the sorted array, so partners sit at i+1, i+2, ...).
+// Pairs across boxes exist only for molecules within the stencil radius of a
+// box face; those are tested from global memory by the molecule in the
+// lower-numbered box.  Every in-radius pair is thus tested exactly once and
+// registered on both molecules (smolreact.c:3201-3298 tests each pair once).
+template <bool SINGLE>
+__global__ void __launch_bounds__(kPairTile, 4) k_pairs_tile(KParams p) {
+  __shared__ float4 s_pc[kPairTile + kPairHalo];
+  __shared__ ull s_id[kPairTile + kPairHalo];
+  __shared__ int s_cell[kPairTile + kPairHalo];
+  const int n = *p.b_n;
+  const uint32_t step = *p.step;
+  int extra = 0;
+  for (int base = blockIdx.x * kPairTile; base < n; base += gridDim.x * kPairTile) {
+    __syncthreads();
+    for (int t = threadIdx.x; t < kPairTile + kPairHalo; t += blockDim.x) {
+      const int g = base + t;
+      if (g < n) {
+        const float4 q = p.b_pc[g];
+        const ull qd = p.b_id[g];
+        s_pc[t] = q;
+        s_id[t] = qd;
+        const DevGeo &gg = geo_of<SINGLE>(p, SINGLE ? 0 : id_rep(qd));
+        s_cell[t] = global_cell(gg, __float_as_uint(q.w));
+      } else {
+        s_cell[t] = -1;
+        s_id[t] = make_id(kDeadSpecies, 0, 0);
+      }
+    }
+    __syncthreads();
+    const int t = threadIdx.x;
+    const int i = base + t;
+    const ull idi = s_id[t];
+    const int sp = id_species(idi);
+    const bool act = i < n && sp != kDeadSpecies && c_net.pair_mask[sp] != 0;
+    const int rep = SINGLE ? 0 : id_rep(idi);
+    const float4 pc = s_pc[t];
+    const int cell = s_cell[t];
+    const float rs = act ? p.rsearch[rep * c_net.nsp + sp] : 0.f;
+    const float rs2 = rs * rs;
+    ull best = ~0ull;
+    // same-box partners from the staged tile
+    int k = 1;
+    for (; k < kPairHalo; ++k) {
+      const int u = t + k;
+      const bool same = act && s_cell[u] == cell;
+      if (!__any_sync(0xffffffffu, same)) break;
+      if (same) {
+        const float4 q = s_pc[u];
+        const float vx = q.x - pc.x, vy = q.y - pc.y, vz = q.z - pc.z;
+        try_pair(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, i + k, s_id[u], rs2, step, best, extra);
+      }
+    }
+    // a box longer than the staged window continues in global memory
+    if (act && k == kPairHalo && s_cell[t + kPairHalo - 1] == cell) {
+      const int e = min(p.start[cell + 1], n);
+      for (int j = i + kPairHalo; j < e; ++j) {
+        const float4 q = p.b_pc[j];
+        const float vx = q.x - pc.x, vy = q.y - pc.y, vz = q.z - pc.z;
+        try_pair(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, j, p.b_id[j], rs2, step, best, extra);
+      }
+    }
+    // neighbouring boxes, only near a face
+    if (act) {
+      const DevGeo &g = geo_of<SINGLE>(p, rep);
+      int ix, iy, iz;
+      unpack_cell(__float_as_uint(pc.w), ix, iy, iz);
+      const float ub0 = (ix == g.n[0] - 1) ? g.whi[0] : g.h[0];
+      const float ub1 = (iy == g.n[1] - 1) ? g.whi[1] : g.h[1];
+      const float ub2 = (iz == g.n[2] - 1) ? g.whi[2] : g.h[2];
+      const int xlo = pc.x < rs ? -1 : 0, xhi = pc.x > ub0 - rs ? 1 : 0;
+      const int ylo = pc.y < rs ? -1 : 0, yhi = pc.y > ub1 - rs ? 1 : 0;
+      const int zlo = pc.z < rs ? -1 : 0, zhi = pc.z > ub2 - rs ? 1 : 0;
+      if ((xlo | xhi | ylo | yhi | zlo | zhi) != 0) {
+        const bool px = g.wall[0] == kWallPeriodic, py = g.wall[2] == kWallPeriodic, pz = g.wall[4] == kWallPeriodic;
+        for (int dz = zlo; dz <= zhi; ++dz) {
+          int z = iz + dz;
+          if (z < 0 || z >= g.n[2]) {
+            if (!pz) continue;
+            z = (z < 0) ? z + g.n[2] : z - g.n[2];
+          }
+          for (int dy = ylo; dy <= yhi; ++dy) {
+            int y = iy + dy;
+            if (y < 0 || y >= g.n[1]) {
+              if (!py) continue;
+              y = (y < 0) ? y + g.n[1] : y - g.n[1];
+            }
+            const int rowbase = g.cell0 + (z * g.n[1] + y) * g.n[0];
+            for (int dx = xlo; dx <= xhi; ++dx) {
+              if (dx == 0 && dy == 0 && dz == 0) continue;
+              int x = ix + dx;
+              if (x < 0 || x >= g.n[0]) {
+                if (!px) continue;
+                x = (x < 0) ? x + g.n[0] : x - g.n[0];
+              }
+              const int c = rowbase + x;
+              if (c <= cell) continue;  // the molecule in the lower box tests the pair
+              const int s0 = p.start[c], e0 = min(p.start[c + 1], n);
+              for (int j = s0; j < e0; ++j) {
+                const float4 q = p.b_pc[j];
+                const float vx = (q.x - pc.x) + (float)dx * g.h[0];
+                const float vy = (q.y - pc.y) + (float)dy * g.h[1];
+                const float vz = (q.z - pc.z) + (float)dz * g.h[2];
+                try_pair(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, j, p.b_id[j], rs2, step, best, extra);
+              }
+            }
+          }
+        }
+      }
+    }
+    if (best != ~0ull) extra += register_candidate(p, i, best);
+  }
+  if (extra) atomicAdd(&p.counters[5], (unsigned long long)extra);
+}
+
 // Pair search over the box-sorted molecules; also counts every molecule's
 // box for the next step (the histogram the next scatter needs).
 template <bool SINGLE, bool FUSE>
@@ -1202,6 +1337,7 @@ class EngineImpl {
   }
 
   int grid_mol() const { return sm_count() * 4; }
+  int grid_tiles() const { return sm_count() * 4; }
   int grid_small() const { return sm_count(); }
 
   size_t adv_smem() const {
@@ -1267,7 +1403,7 @@ class EngineImpl {
     k_births<<<grid_small(), 128, 0, s>>>(p);
     mark("k_births");
     if (cn) k_pairs<SINGLE, true><<<grid_mol(), 256, adv_smem(), s>>>(p);
-    else k_pairs<SINGLE, false><<<grid_mol(), 256, 0, s>>>(p);
+    else k_pairs_tile<SINGLE><<<grid_tiles(), kPairTile, 0, s>>>(p);
     mark("k_pairs");
     k_commit<SINGLE><<<grid_small(), 128, 0, s>>>(p, cn);
     mark("k_commit");
