@@ -72,6 +72,8 @@ struct KParams {
   int *ncand;
   int candcap;
   ull *best;
+  int *face;                     // molecules near a box face (cross-box pair search)
+  int *nface;
   unsigned long long *counters;  // [0]=wall [1]=rxn0 [2]=rxn1 [3]=rxn2 [4]=unresolved [5]=multicand
   long long *spcount;            // [rep*nsp + sp]
   int *status;
@@ -353,6 +355,7 @@ __global__ void k_begin(KParams p, int bump_step) {
     *p.nev = 0;
     *p.ncand = 0;
     *p.q_n = 0;
+    *p.nface = 0;
   }
 }
 
@@ -805,8 +808,9 @@ __device__ int search_round1(const KParams &p, int i, float4 pc, ull id, uint32_
 // this step, fold the key into i's running best and register i on j.
 __device__ __forceinline__ void try_pair(const KParams &p, int i, ull idi, int sp, int rep, float d2, int j, ull jd,
                                          float rs2, uint32_t step, ull &best, int &extra) {
+  if (d2 > rs2) return;
   const int spj = id_species(jd);
-  if (spj == kDeadSpecies || !((c_net.pair_mask[sp] >> spj) & 1u) || d2 > rs2) return;
+  if (spj == kDeadSpecies || !((c_net.pair_mask[sp] >> spj) & 1u)) return;
   if (pair_reaction(p, rep, sp, spj, d2, id_stream(idi), id_stream(jd), step) < 0) return;
   const uint32_t db = __float_as_uint(d2);
   const ull k = ((ull)db << 32) | (uint32_t)j;
@@ -883,7 +887,9 @@ __global__ void __launch_bounds__(kPairTile, 4) k_pairs_tile(KParams p) {
         try_pair(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, j, p.b_id[j], rs2, step, best, extra);
       }
     }
-    // neighbouring boxes, only near a face
+    // molecules near a box face also need the neighbouring boxes: queue them for
+    // k_pairs_faces (a serial global-memory walk here would stall the warp)
+    bool face = false;
     if (act) {
       const DevGeo &g = geo_of<SINGLE>(p, rep);
       int ix, iy, iz;
@@ -891,42 +897,83 @@ __global__ void __launch_bounds__(kPairTile, 4) k_pairs_tile(KParams p) {
       const float ub0 = (ix == g.n[0] - 1) ? g.whi[0] : g.h[0];
       const float ub1 = (iy == g.n[1] - 1) ? g.whi[1] : g.h[1];
       const float ub2 = (iz == g.n[2] - 1) ? g.whi[2] : g.h[2];
-      const int xlo = pc.x < rs ? -1 : 0, xhi = pc.x > ub0 - rs ? 1 : 0;
-      const int ylo = pc.y < rs ? -1 : 0, yhi = pc.y > ub1 - rs ? 1 : 0;
-      const int zlo = pc.z < rs ? -1 : 0, zhi = pc.z > ub2 - rs ? 1 : 0;
-      if ((xlo | xhi | ylo | yhi | zlo | zhi) != 0) {
-        const bool px = g.wall[0] == kWallPeriodic, py = g.wall[2] == kWallPeriodic, pz = g.wall[4] == kWallPeriodic;
-        for (int dz = zlo; dz <= zhi; ++dz) {
-          int z = iz + dz;
-          if (z < 0 || z >= g.n[2]) {
-            if (!pz) continue;
-            z = (z < 0) ? z + g.n[2] : z - g.n[2];
+      face = pc.x < rs || pc.x > ub0 - rs || pc.y < rs || pc.y > ub1 - rs || pc.z < rs || pc.z > ub2 - rs;
+    }
+    const unsigned fm = __ballot_sync(0xffffffffu, face);
+    if (fm) {
+      const int lane = threadIdx.x & 31;
+      int slot = 0;
+      if (lane == __ffs(fm) - 1) slot = atomicAdd(p.nface, __popc(fm));
+      slot = __shfl_sync(0xffffffffu, slot, __ffs(fm) - 1) + __popc(fm & lanemask_lt());
+      if (face) {
+        if (slot < p.cap) p.face[slot] = i;
+        else atomicOr(p.status, kStCandCap);
+      }
+    }
+    if (best != ~0ull) extra += register_candidate(p, i, best);
+  }
+  if (extra) atomicAdd(&p.counters[5], (unsigned long long)extra);
+}
+
+// Cross-box pairs for the molecules queued by k_pairs_tile (those within the
+// stencil radius of a box face): one thread per queued molecule walks the
+// neighbouring boxes its stencil reaches; a pair across boxes is tested by the
+// molecule in the lower-numbered box.
+template <bool SINGLE>
+__global__ void __launch_bounds__(256) k_pairs_faces(KParams p) {
+  const int nf = min(*p.nface, p.cap);
+  const int n = *p.b_n;
+  const uint32_t step = *p.step;
+  int extra = 0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nf; t += gridDim.x * blockDim.x) {
+    const int i = p.face[t];
+    const float4 pc = p.b_pc[i];
+    const ull idi = p.b_id[i];
+    const int sp = id_species(idi);
+    const int rep = SINGLE ? 0 : id_rep(idi);
+    const DevGeo &g = geo_of<SINGLE>(p, rep);
+    const float rs = p.rsearch[rep * c_net.nsp + sp];
+    const float rs2 = rs * rs;
+    int ix, iy, iz;
+    unpack_cell(__float_as_uint(pc.w), ix, iy, iz);
+    const int cell = global_cell(g, __float_as_uint(pc.w));
+    const float ub0 = (ix == g.n[0] - 1) ? g.whi[0] : g.h[0];
+    const float ub1 = (iy == g.n[1] - 1) ? g.whi[1] : g.h[1];
+    const float ub2 = (iz == g.n[2] - 1) ? g.whi[2] : g.h[2];
+    const int xlo = pc.x < rs ? -1 : 0, xhi = pc.x > ub0 - rs ? 1 : 0;
+    const int ylo = pc.y < rs ? -1 : 0, yhi = pc.y > ub1 - rs ? 1 : 0;
+    const int zlo = pc.z < rs ? -1 : 0, zhi = pc.z > ub2 - rs ? 1 : 0;
+    const bool px = g.wall[0] == kWallPeriodic, py = g.wall[2] == kWallPeriodic, pz = g.wall[4] == kWallPeriodic;
+    ull best = ~0ull;
+    for (int dz = zlo; dz <= zhi; ++dz) {
+      int z = iz + dz;
+      if (z < 0 || z >= g.n[2]) {
+        if (!pz) continue;
+        z = (z < 0) ? z + g.n[2] : z - g.n[2];
+      }
+      for (int dy = ylo; dy <= yhi; ++dy) {
+        int y = iy + dy;
+        if (y < 0 || y >= g.n[1]) {
+          if (!py) continue;
+          y = (y < 0) ? y + g.n[1] : y - g.n[1];
+        }
+        const int rowbase = g.cell0 + (z * g.n[1] + y) * g.n[0];
+        for (int dx = xlo; dx <= xhi; ++dx) {
+          if (dx == 0 && dy == 0 && dz == 0) continue;
+          int x = ix + dx;
+          if (x < 0 || x >= g.n[0]) {
+            if (!px) continue;
+            x = (x < 0) ? x + g.n[0] : x - g.n[0];
           }
-          for (int dy = ylo; dy <= yhi; ++dy) {
-            int y = iy + dy;
-            if (y < 0 || y >= g.n[1]) {
-              if (!py) continue;
-              y = (y < 0) ? y + g.n[1] : y - g.n[1];
-            }
-            const int rowbase = g.cell0 + (z * g.n[1] + y) * g.n[0];
-            for (int dx = xlo; dx <= xhi; ++dx) {
-              if (dx == 0 && dy == 0 && dz == 0) continue;
-              int x = ix + dx;
-              if (x < 0 || x >= g.n[0]) {
-                if (!px) continue;
-                x = (x < 0) ? x + g.n[0] : x - g.n[0];
-              }
-              const int c = rowbase + x;
-              if (c <= cell) continue;  // the molecule in the lower box tests the pair
-              const int s0 = p.start[c], e0 = min(p.start[c + 1], n);
-              for (int j = s0; j < e0; ++j) {
-                const float4 q = p.b_pc[j];
-                const float vx = (q.x - pc.x) + (float)dx * g.h[0];
-                const float vy = (q.y - pc.y) + (float)dy * g.h[1];
-                const float vz = (q.z - pc.z) + (float)dz * g.h[2];
-                try_pair(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, j, p.b_id[j], rs2, step, best, extra);
-              }
-            }
+          const int c = rowbase + x;
+          if (c <= cell) continue;
+          const int s0 = p.start[c], e0 = min(p.start[c + 1], n);
+          for (int j = s0; j < e0; ++j) {
+            const float4 q = p.b_pc[j];
+            const float vx = (q.x - pc.x) + (float)dx * g.h[0];
+            const float vy = (q.y - pc.y) + (float)dy * g.h[1];
+            const float vz = (q.z - pc.z) + (float)dz * g.h[2];
+            try_pair(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, j, p.b_id[j], rs2, step, best, extra);
           }
         }
       }
@@ -1263,6 +1310,7 @@ class EngineImpl {
   Event *d_ev = nullptr;
   int *d_cand = nullptr;
   ull *d_best = nullptr;
+  int *d_face = nullptr;
   unsigned long long *d_counters = nullptr;
   long long *d_spcount = nullptr;
   ull *d_injkey = nullptr;
@@ -1280,7 +1328,7 @@ class EngineImpl {
     graph2 = nullptr;
     void *ptrs[] = {d_rsearch, d_geo, d_difstep, d_driftdt, d_bind2, d_pairprob, d_prdpos, d_gtab, d_unithr,
                     d_births, d_pc[0], d_pc[1], d_ppc[0], d_ppc[1], d_id[0], d_id[1], d_pid[0],
-                    d_pid[1], d_counts, d_step, d_cnt, d_start, d_bsum, d_ev, d_cand, d_best,
+                    d_pid[1], d_face, d_counts, d_step, d_cnt, d_start, d_bsum, d_ev, d_cand, d_best,
                     d_counters, d_spcount, d_injkey, d_injval};
     for (void *q : ptrs)
       if (q) cudaFree(q);
@@ -1290,7 +1338,7 @@ class EngineImpl {
     d_pc[0] = d_pc[1] = d_ppc[0] = d_ppc[1] = nullptr;
     d_id[0] = d_id[1] = d_pid[0] = d_pid[1] = nullptr;
     d_counts = nullptr; d_step = nullptr; d_cnt = d_start = d_bsum = nullptr; d_ev = nullptr;
-    d_cand = nullptr; d_best = nullptr; d_counters = nullptr; d_spcount = nullptr;
+    d_cand = nullptr; d_best = nullptr; d_face = nullptr; d_counters = nullptr; d_spcount = nullptr;
     d_injkey = nullptr; d_injval = nullptr;
     if (own_stream) cudaStreamDestroy(own_stream);
     own_stream = nullptr;
@@ -1326,6 +1374,8 @@ class EngineImpl {
     p.ncand = d_counts + 5;
     p.candcap = (int)candcap;
     p.best = d_best;
+    p.face = d_face;
+    p.nface = d_counts + 7;
     p.counters = d_counters;
     p.spcount = d_spcount;
     p.status = d_counts + 6;
@@ -1402,9 +1452,15 @@ class EngineImpl {
     const int cn = fuse_next ? 1 : 0;
     k_births<<<grid_small(), 128, 0, s>>>(p);
     mark("k_births");
-    if (cn) k_pairs<SINGLE, true><<<grid_mol(), 256, adv_smem(), s>>>(p);
-    else k_pairs_tile<SINGLE><<<grid_tiles(), kPairTile, 0, s>>>(p);
-    mark("k_pairs");
+    if (cn) {
+      k_pairs<SINGLE, true><<<grid_mol(), 256, adv_smem(), s>>>(p);
+      mark("k_pairs");
+    } else {
+      k_pairs_tile<SINGLE><<<grid_tiles(), kPairTile, 0, s>>>(p);
+      mark("k_pairs");
+      k_pairs_faces<SINGLE><<<grid_mol(), 256, 0, s>>>(p);
+      mark("k_pairs_faces");
+    }
     k_commit<SINGLE><<<grid_small(), 128, 0, s>>>(p, cn);
     mark("k_commit");
     for (int round = 1; round < dnet.rounds; ++round) {
@@ -1429,7 +1485,7 @@ class EngineImpl {
     else enqueue_step_t<false>(par, rebin_only, fuse_next);
   }
 
-  int launches_per_step() const { return 10 + 2 * (dnet.rounds - 1); }
+  int launches_per_step() const { return 11 + 2 * (dnet.rounds - 1); }
 
   int upload_const(std::string *err) {
     CK(cudaMemcpyToSymbolAsync(c_net, &dnet, sizeof(DevNet), 0, cudaMemcpyHostToDevice, stream));
@@ -1666,6 +1722,7 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
   CK(cudaMalloc(&E.d_ev, E.evcap * sizeof(Event)));
   CK(cudaMalloc(&E.d_cand, E.candcap * sizeof(int)));
   CK(cudaMalloc(&E.d_best, E.cap * sizeof(ull)));
+  CK(cudaMalloc(&E.d_face, E.cap * sizeof(int)));
   CK(cudaMemsetAsync(E.d_best, 0xFF, E.cap * sizeof(ull), E.stream));
   CK(cudaMalloc(&E.d_counters, 8 * sizeof(unsigned long long)));
   CK(cudaMemsetAsync(E.d_counters, 0, 8 * sizeof(unsigned long long), E.stream));
