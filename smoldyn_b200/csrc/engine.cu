@@ -288,8 +288,8 @@ __device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, co
     renorm(w, j, g.h[d], g.inv_h[d]);
     if (j <= 0 || j >= g.n[d] - 1) {
       if (walls_dim(w, j, g, d, hits)) return 1;
+      clamp_cell(w, j, g, d);
     }
-    clamp_cell(w, j, g, d);
     u[d] = w;
     ix[d] = j;
   }
@@ -369,17 +369,44 @@ __device__ __forceinline__ const float *stage_gtab(const KParams &p, float *s_gt
   return s_gtab;
 }
 
+// Runs of consecutive lanes that hold live molecules of the same box.  The
+// lanes process box-sorted molecules, so most of a warp falls into a few runs
+// and one atomic per run replaces one per molecule (cheaper than match.any).
+struct BoxRun {
+  int head;   // first lane of this lane's run
+  int count;  // live lanes in the run
+  int rank;   // live lanes of the run before this lane
+};
+
+__device__ __forceinline__ BoxRun box_run(bool alive, int cell) {
+  const int lane = threadIdx.x & 31;
+  const unsigned live = __ballot_sync(0xffffffffu, alive);
+  const int c = alive ? cell : -1;
+  const int prev = __shfl_up_sync(0xffffffffu, c, 1);
+  const bool head = alive && (lane == 0 || prev != c);
+  const unsigned heads = __ballot_sync(0xffffffffu, head);
+  const unsigned le = lanemask_lt() | (1u << lane);
+  BoxRun r;
+  r.head = max(0, 31 - __clz(heads & le));  // only meaningful for live lanes
+  const unsigned after = heads & ~le;
+  const int next = after ? __ffs(after) - 1 : 32;
+  const unsigned run_mask = (next == 32 ? 0xffffffffu : ((1u << next) - 1u)) & ~((1u << r.head) - 1u);
+  r.count = __popc(live & run_mask);
+  r.rank = __popc(live & run_mask & lanemask_lt());
+  return r;
+}
+
 // Warp-aggregated increment of the box histogram for every lane with `alive`
-// set (one atomic per distinct box in the warp).
+// set.
 template <bool SINGLE>
 __device__ __forceinline__ void count_box(const KParams &p, bool alive, float4 pc, ull id) {
-  const unsigned act = __ballot_sync(0xffffffffu, alive);
+  int cell = -1;
   if (alive) {
     const DevGeo &g = geo_of<SINGLE>(p, SINGLE ? 0 : id_rep(id));
-    const int cell = global_cell(g, __float_as_uint(pc.w));
-    const unsigned peers = __match_any_sync(act, cell);
-    if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&p.cnt[cell], __popc(peers));
+    cell = global_cell(g, __float_as_uint(pc.w));
   }
+  const BoxRun r = box_run(alive, cell);
+  if (alive && r.rank == 0) atomicAdd(&p.cnt[cell], r.count);
 }
 
 // Next-step destination box of one molecule, counted (+1) or uncounted (-1)
@@ -424,18 +451,18 @@ __global__ void __launch_bounds__(256) k_advance(KParams p, int phase) {
       count_box<SINGLE>(p, alive, pc, id);
       continue;
     }
-    const unsigned act = __ballot_sync(0xffffffffu, alive);
+    int cell = -1;
     if (alive) {
       const DevGeo &g = geo_of<SINGLE>(p, SINGLE ? 0 : id_rep(id));
-      const int cell = global_cell(g, __float_as_uint(pc.w));
-      const unsigned peers = __match_any_sync(act, cell);
-      const int leader = __ffs(peers) - 1;
-      const int npeer = __popc(peers);
-      const int rank = __popc(peers & lanemask_lt());
-      int old = 0;
-      if (lane == leader) old = atomicSub(&p.cnt[cell], npeer);
-      old = __shfl_sync(peers, old, leader);
-      const int slot = p.start[cell] + old - npeer + rank;
+      cell = global_cell(g, __float_as_uint(pc.w));
+    }
+    const BoxRun run = box_run(alive, cell);
+    // the run's first live lane takes `count` slots from the top of the box
+    int old = 0;
+    if (alive && run.rank == 0) old = atomicSub(&p.cnt[cell], run.count);
+    old = __shfl_sync(0xffffffffu, old, alive ? run.head : lane);
+    if (alive) {
+      const int slot = p.start[cell] + old - run.count + run.rank;
       if (slot >= 0 && slot < p.cap) {
         p.b_pc[slot] = pc;
         p.b_id[slot] = id;
