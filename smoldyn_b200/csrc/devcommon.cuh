@@ -62,6 +62,19 @@ __host__ __device__ __forceinline__ uint4 philox(uint4 c, uint2 k) {
   return c;
 }
 
+// Same generator with the 10 round keys precomputed (ks[2r], ks[2r+1]); used
+// with a key schedule held in constant memory so no per-thread key arithmetic
+// is issued.  Produces exactly philox(c, {ks[0], ks[1]}).
+__host__ __device__ __forceinline__ uint4 philox_ks(uint4 c, const uint32_t *ks) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t hi0 = mulhi32(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+    const uint32_t hi1 = mulhi32(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+    c = make_uint4(hi1 ^ c.y ^ ks[2 * r], lo1, hi0 ^ c.w ^ ks[2 * r + 1], lo0);
+  }
+  return c;
+}
+
 // uniform in [0,1) with 32-bit resolution (matches randCOD's granularity)
 __host__ __device__ __forceinline__ double u01d(uint32_t x) { return x * 2.3283064365386963e-10; }
 // uniform in (0,1) as float with 24-bit resolution
@@ -85,6 +98,7 @@ struct DevNet {
   int nrx_total;
   uint32_t gmask;      // gaussian table size - 1
   uint32_t key0, key1; // Philox key (seed)
+  uint32_t move_ks[20]; // round keys of the move generator (key0, key1 scheduled)
   int any_drift;
   int any_absorb;
   int inject;          // deterministic mode active

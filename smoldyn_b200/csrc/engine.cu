@@ -105,6 +105,23 @@ __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b)
 // range) into cell form.
 __device__ __forceinline__ void renorm(float &w, int &j, float h, float inv_h) {
   if (w >= 0.f && w < h) return;
+  // one box over: the common case when a step crosses a face
+  if (w < 0.f && w >= -h) {
+    j -= 1;
+    w = fadd(w, h);
+    if (w < h) return;
+    w = fsub(w, h);  // rounding put it on the face: stay in the original box
+    j += 1;
+    return;
+  }
+  if (w >= h && w < fadd(h, h)) {
+    j += 1;
+    w = fsub(w, h);
+    if (w >= 0.f) return;
+    w = fadd(w, h);
+    j -= 1;
+    return;
+  }
   const int k = (int)floorf(fmul(w, inv_h));
   j += k;
   w = fsub(w, fmul((float)k, h));
@@ -253,7 +270,7 @@ __device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, co
   }
   const ull skey = id_stream(id);
   const uint2 key = make_uint2(c_net.key0, c_net.key1);
-  const uint4 r = philox(make_uint4((uint32_t)skey, (uint32_t)(skey >> 32), step, 0u), key);
+  const uint4 r = philox_ks(make_uint4((uint32_t)skey, (uint32_t)(skey >> 32), step, 0u), c_net.move_ks);
   float dsp[3];
   int forced = -1;
   if (c_net.inject) {
@@ -1657,6 +1674,10 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
   D.gmask = (uint32_t)(gs - 1);
   D.key0 = (uint32_t)seed ^ 0xA511E9B3u;
   D.key1 = (uint32_t)(seed >> 32) ^ 0x63D83595u;
+  for (int r = 0; r < 10; ++r) {  // Philox round keys (bumped by the Weyl constants)
+    D.move_ks[2 * r] = D.key0 + (uint32_t)r * 0x9E3779B9u;
+    D.move_ks[2 * r + 1] = D.key1 + (uint32_t)r * 0xBB67AE85u;
+  }
   D.rounds = 3;
   D.npanel = (int)net.panels.size();
   for (int r = 0; r < net.nrxn[1]; ++r) {
