@@ -2,14 +2,15 @@
 //
 // One time step (Smoldyn smolsim.cpp:2607-2692 order) is the launch sequence
 //   k_begin          step counter, per-step counters
-//   k_advance(count) diffuse + walls + first-order decisions, histogram of the
-//                    new virtual box of every survivor (warp-aggregated atomics)
+//   k_move           diffuse + walls + first-order decisions for every molecule
+//                    (moved position to tmp, events for the ones that leave),
+//                    histogram of destination virtual boxes (warp-aggregated)
 //   scan (3 kernels) exclusive scan of box counts -> box start offsets
-//   k_advance(scat.) recomputes the same move (same Philox counters) and
-//                    scatters survivors in box order; first-order events out
+//   k_scatter        permutation of the moved molecules into box order
 //   k_births         zeroth-order births (Poisson per replicate and reaction)
-//   k_pairs          27-box neighbour search within each pair's binding radius;
-//                    closest candidate per molecule as a packed (dist2, index) key
+//   k_pairs_tile     same-box pairs from a shared-memory tile of sorted
+//                    molecules; molecules near a box face are queued
+//   k_pairs_faces    cross-box pairs of the queued molecules
 //   k_commit / k_research (rounds) mutual-closest pairs react, losers retry
 //   k_products       product placement (site, unbinding offsets under one random
 //                    rotation per event), walls for the new molecules
@@ -60,6 +61,7 @@ struct KParams {
   float4 *q_pc;
   ull *q_id;
   int *q_n;
+  float4 *tmp;   // moved positions of the step's inputs (sorted input, then products)
   int cap, pcap;
   int *cnt;
   int *start;
@@ -83,6 +85,8 @@ struct KParams {
   const float4 *inj_val;         // dx, dy, dz, forced order-1 reaction (or -1)
   int inj_n;
 };
+
+constexpr uint32_t kTmpGone = 0xFFFFFFFFu;  // tmp[i].w of a molecule that left
 
 enum StatusBits { kStMolCap = 1, kStEvCap = 2, kStProdCap = 4, kStCandCap = 8 };
 
@@ -426,29 +430,18 @@ __device__ __forceinline__ void count_box(const KParams &p, bool alive, float4 p
   if (alive && r.rank == 0) atomicAdd(&p.cnt[cell], r.count);
 }
 
-// Next-step destination box of one molecule, counted (+1) or uncounted (-1)
-// outside the bulk passes (reacting pairs, new products).
+// Move pass (one per step): diffuse + walls + first-order decisions for every
+// molecule of the sorted input and of the product list, events for removed or
+// reacting molecules, the moved position into tmp (w = kTmpGone when the
+// molecule leaves the system), and the histogram of destination boxes.
+// rebin_only: no motion and no reactions (used after uploads).
 template <bool SINGLE>
-__device__ __forceinline__ void recount_next(const KParams &p, float4 pc, ull id, uint32_t nstep, int sign) {
-  int hits = 0;
-  if (advance_one<SINGLE>(pc, id, nstep, p, p.gtab, 0, hits) != 0) return;
-  const DevGeo &g = geo_of<SINGLE>(p, SINGLE ? 0 : id_rep(id));
-  atomicAdd(&p.cnt[global_cell(g, __float_as_uint(pc.w))], sign);
-}
-
-// phase bit 0: 0 = count, 1 = scatter.  bit 1: rebin only (no motion, no reactions).
-// In steady state the count of step t+1 is taken inside k_pairs of step t (it
-// reads every molecule anyway), so only the scatter phase runs per step.
-template <bool SINGLE>
-__global__ void __launch_bounds__(256) k_advance(KParams p, int phase) {
+__global__ void __launch_bounds__(256) k_move(KParams p, int rebin_only) {
   extern __shared__ float s_gtab[];
-  const int rebin_only = (phase >> 1) & 1;
-  const int scatter = phase & 1;
   const float *gtab = rebin_only ? p.gtab : stage_gtab(p, s_gtab);
   const int na = *p.a_n, np = *p.p_n;
   const int total = na + np;
   const uint32_t step = *p.step;
-  const int lane = threadIdx.x & 31;
   int hits_acc = 0;
   for (int base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
     const int i = base + threadIdx.x;
@@ -464,10 +457,41 @@ __global__ void __launch_bounds__(256) k_advance(KParams p, int phase) {
     int hits = 0;
     if (valid) fate = advance_one<SINGLE>(pc, id, step, p, gtab, rebin_only, hits);
     const bool alive = (fate == 0);
-    if (!scatter) {
-      count_box<SINGLE>(p, alive, pc, id);
-      continue;
+    if (i < total) p.tmp[i] = alive ? pc : make_float4(0.f, 0.f, 0.f, __uint_as_float(kTmpGone));
+    count_box<SINGLE>(p, alive, pc, id);
+    if (valid && !alive) {
+      if (fate == 1) {
+        atomicAdd((unsigned long long *)&p.spcount[id_rep(id) * c_net.nsp + id_species(id)],
+                  (unsigned long long)(-1ll));
+      } else {
+        Event e;
+        e.site = pc;
+        e.key = id_stream(id);
+        e.rxn = (1u << 8) | (uint32_t)(fate - 2);
+        e.rep = (uint32_t)id_rep(id);
+        push_event(p, e);
+      }
     }
+    hits_acc += hits;
+  }
+  if (hits_acc) atomicAdd(&p.counters[0], (unsigned long long)hits_acc);
+}
+
+// Scatter pass: a pure permutation of the moved molecules into box order.
+template <bool SINGLE>
+__global__ void __launch_bounds__(256) k_scatter(KParams p) {
+  const int na = *p.a_n, np = *p.p_n;
+  const int total = na + np;
+  const int lane = threadIdx.x & 31;
+  for (int base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
+    const int i = base + threadIdx.x;
+    float4 pc = make_float4(0.f, 0.f, 0.f, __uint_as_float(kTmpGone));
+    ull id = 0;
+    if (i < total) {
+      pc = p.tmp[i];
+      id = (i < na) ? p.a_id[i] : p.p_id[i - na];
+    }
+    const bool alive = __float_as_uint(pc.w) != kTmpGone;
     int cell = -1;
     if (alive) {
       const DevGeo &g = geo_of<SINGLE>(p, SINGLE ? 0 : id_rep(id));
@@ -487,22 +511,7 @@ __global__ void __launch_bounds__(256) k_advance(KParams p, int phase) {
         atomicOr(p.status, kStMolCap);
       }
     }
-    if (valid) {
-      hits_acc += hits;
-      if (fate == 1) {
-        atomicAdd((unsigned long long *)&p.spcount[id_rep(id) * c_net.nsp + id_species(id)],
-                  (unsigned long long)(-1ll));
-      } else if (fate >= 2) {
-        Event e;
-        e.site = pc;
-        e.key = id_stream(id);
-        e.rxn = (1u << 8) | (uint32_t)(fate - 2);
-        e.rep = (uint32_t)id_rep(id);
-        push_event(p, e);
-      }
-    }
   }
-  if (scatter && hits_acc) atomicAdd(&p.counters[0], (unsigned long long)hits_acc);
 }
 
 // ---- exclusive scan of the box histogram ------------------------------------
@@ -1027,36 +1036,6 @@ __global__ void __launch_bounds__(256) k_pairs_faces(KParams p) {
   if (extra) atomicAdd(&p.counters[5], (unsigned long long)extra);
 }
 
-// Pair search over the box-sorted molecules; also counts every molecule's
-// box for the next step (the histogram the next scatter needs).
-template <bool SINGLE, bool FUSE>
-__global__ void __launch_bounds__(256, 2) k_pairs(KParams p) {
-  extern __shared__ float s_gtab[];
-  const float *gtab = FUSE ? stage_gtab(p, s_gtab) : p.gtab;
-  const int n = *p.b_n;
-  const uint32_t step = *p.step;
-  int multi = 0;
-  for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-    const int i = base + threadIdx.x;
-    bool valid = i < n;
-    float4 pc = make_float4(0.f, 0.f, 0.f, 0.f);
-    ull id = 0;
-    if (valid) {
-      pc = p.b_pc[i];
-      id = p.b_id[i];
-      valid = id_species(id) != kDeadSpecies;
-    }
-    if (valid && c_net.search_mask[id_species(id)] != 0) multi += search_round1(p, i, pc, id, step);
-    if (FUSE) {
-      int fate = -1, hits = 0;
-      float4 npc = pc;
-      if (valid) fate = advance_one<SINGLE>(npc, id, step + 1, p, gtab, 0, hits);
-      count_box<SINGLE>(p, fate == 0, npc, id);
-    }
-  }
-  if (multi) atomicAdd(&p.counters[5], (unsigned long long)multi);
-}
-
 // Re-search for candidates still alive (conflict-resolution rounds >= 2).
 __global__ void k_research(KParams p) {
   const int nc = min(*p.ncand, p.candcap);
@@ -1108,8 +1087,7 @@ __device__ __forceinline__ float4 pair_site(const KParams &p, int i, int j, int 
   return make_float4(w[0], w[1], w[2], __uint_as_float(pack_cell(cell[0], cell[1], cell[2])));
 }
 
-template <bool SINGLE>
-__global__ void k_commit(KParams p, int count_next) {
+__global__ void k_commit(KParams p) {
   const int nc = min(*p.ncand, p.candcap);
   const uint32_t step = *p.step;
   int done = 0;
@@ -1140,10 +1118,6 @@ __global__ void k_commit(KParams p, int count_next) {
     push_event(p, e);
     p.b_id[i] = id_mark_dead(idi);
     p.b_id[j] = id_mark_dead(idj);
-    if (count_next) {  // they were counted for the next step in k_pairs
-      recount_next<SINGLE>(p, p.b_pc[i], idi, step + 1, -1);
-      recount_next<SINGLE>(p, p.b_pc[j], idj, step + 1, -1);
-    }
     atomicAdd((unsigned long long *)&p.spcount[rep * c_net.nsp + spi], (unsigned long long)(-1ll));
     atomicAdd((unsigned long long *)&p.spcount[rep * c_net.nsp + spj], (unsigned long long)(-1ll));
     done++;
@@ -1166,8 +1140,7 @@ __device__ __forceinline__ void random_rotation(uint4 r, float m[9]) {
   m[6] = 2.f * (qx * qz - qy * qw); m[7] = 2.f * (qy * qz + qx * qw); m[8] = 1.f - 2.f * (qx * qx + qy * qy);
 }
 
-template <bool SINGLE>
-__global__ void k_products(KParams p, int count_next) {
+__global__ void k_products(KParams p) {
   const int ne = min(*p.nev, p.evcap);
   const uint32_t step = *p.step;
   const uint2 key = make_uint2(c_net.key0 ^ 0x68E31DA4u, c_net.key1 ^ 0xB5297A4Du);
@@ -1245,7 +1218,6 @@ __global__ void k_products(KParams p, int count_next) {
         const ull nid = make_id(psp, rep, serno);
         p.q_pc[slot] = npc;
         p.q_id[slot] = nid;
-        if (count_next) recount_next<SINGLE>(p, npc, nid, step + 1, +1);
         atomicAdd((unsigned long long *)&p.spcount[rep * c_net.nsp + psp], 1ull);
       } else {
         atomicOr(p.status, kStProdCap);
@@ -1355,6 +1327,7 @@ class EngineImpl {
   int *d_cand = nullptr;
   ull *d_best = nullptr;
   int *d_face = nullptr;
+  float4 *d_tmp = nullptr;
   unsigned long long *d_counters = nullptr;
   long long *d_spcount = nullptr;
   ull *d_injkey = nullptr;
@@ -1372,7 +1345,7 @@ class EngineImpl {
     graph2 = nullptr;
     void *ptrs[] = {d_rsearch, d_geo, d_difstep, d_driftdt, d_bind2, d_pairprob, d_prdpos, d_gtab, d_unithr,
                     d_births, d_pc[0], d_pc[1], d_ppc[0], d_ppc[1], d_id[0], d_id[1], d_pid[0],
-                    d_pid[1], d_face, d_counts, d_step, d_cnt, d_start, d_bsum, d_ev, d_cand, d_best,
+                    d_pid[1], d_face, d_tmp, d_counts, d_step, d_cnt, d_start, d_bsum, d_ev, d_cand, d_best,
                     d_counters, d_spcount, d_injkey, d_injval};
     for (void *q : ptrs)
       if (q) cudaFree(q);
@@ -1382,7 +1355,7 @@ class EngineImpl {
     d_pc[0] = d_pc[1] = d_ppc[0] = d_ppc[1] = nullptr;
     d_id[0] = d_id[1] = d_pid[0] = d_pid[1] = nullptr;
     d_counts = nullptr; d_step = nullptr; d_cnt = d_start = d_bsum = nullptr; d_ev = nullptr;
-    d_cand = nullptr; d_best = nullptr; d_face = nullptr; d_counters = nullptr; d_spcount = nullptr;
+    d_cand = nullptr; d_best = nullptr; d_face = nullptr; d_tmp = nullptr; d_counters = nullptr; d_spcount = nullptr;
     d_injkey = nullptr; d_injval = nullptr;
     if (own_stream) cudaStreamDestroy(own_stream);
     own_stream = nullptr;
@@ -1405,6 +1378,7 @@ class EngineImpl {
     p.p_pc = d_ppc[in]; p.p_id = d_pid[in]; p.p_n = d_counts + 2 + in;
     p.b_pc = d_pc[out]; p.b_id = d_id[out]; p.b_n = d_counts + out;
     p.q_pc = d_ppc[out]; p.q_id = d_pid[out]; p.q_n = d_counts + 2 + out;
+    p.tmp = d_tmp;
     p.cap = (int)cap;
     p.pcap = (int)pcap;
     p.cnt = d_cnt;
@@ -1458,28 +1432,14 @@ class EngineImpl {
     marks.push_back({name, e});
   }
 
-  // Box histogram of the next step is already in d_cnt (taken by the previous
-  // step's k_pairs / k_commit / k_products).  False after uploads, injected
-  // steps and profiling changes; then a step starts with an explicit count pass.
-  bool counts_ready = false;
-  // Take the next step's histogram inside k_pairs/k_commit/k_products instead
-  // of a separate count pass (saves one read of every molecule; off by default:
-  // on B200 the extra move evaluation made the pair kernel slower than the
-  // count pass it replaced).
-  bool fuse_count = false;
-
   template <bool SINGLE>
-  void enqueue_step_t(int par, bool rebin_only, bool fuse_next) {
+  void enqueue_step_t(int par, bool rebin_only) {
     KParams p = params(par);
     cudaStream_t s = stream;
     k_begin<<<1, 32, 0, s>>>(p, rebin_only ? 0 : 1);
     mark("k_begin");
-    const int ph = rebin_only ? 2 : 0;
-    if (rebin_only || !counts_ready) {
-      cudaMemsetAsync(d_cnt, 0, ((size_t)ncell + 1) * sizeof(int), s);
-      k_advance<SINGLE><<<grid_mol(), 256, rebin_only ? 0 : adv_smem(), s>>>(p, ph | 0);
-      mark("k_advance_count");
-    }
+    k_move<SINGLE><<<grid_mol(), 256, rebin_only ? 0 : adv_smem(), s>>>(p, rebin_only ? 1 : 0);
+    mark("k_move");
     k_scan_reduce<<<nscanblocks, kScanThreads, 0, s>>>(d_cnt, ncell, d_bsum);
     mark("k_scan_reduce");
     k_scan_blocks<<<1, 1024, 0, s>>>(d_bsum, nscanblocks);
@@ -1487,49 +1447,36 @@ class EngineImpl {
     k_scan_apply<<<nscanblocks, kScanThreads, 0, s>>>(d_cnt, ncell, d_bsum, nscanblocks, d_start,
                                                       p.b_n, (int)cap);
     mark("k_scan_apply");
-    k_advance<SINGLE><<<grid_mol(), 256, rebin_only ? 0 : adv_smem(), s>>>(p, ph | 1);
-    mark("k_advance_scatter");
-    if (rebin_only) {
-      counts_ready = false;
-      return;
-    }
-    const int cn = fuse_next ? 1 : 0;
+    k_scatter<SINGLE><<<grid_mol(), 256, 0, s>>>(p);
+    mark("k_scatter");
+    if (rebin_only) return;
     k_births<<<grid_small(), 128, 0, s>>>(p);
     mark("k_births");
-    if (cn) {
-      k_pairs<SINGLE, true><<<grid_mol(), 256, adv_smem(), s>>>(p);
-      mark("k_pairs");
-    } else {
-      k_pairs_tile<SINGLE><<<grid_tiles(), kPairTile, 0, s>>>(p);
-      mark("k_pairs");
-      k_pairs_faces<SINGLE><<<grid_mol(), 256, 0, s>>>(p);
-      mark("k_pairs_faces");
-    }
-    k_commit<SINGLE><<<grid_small(), 128, 0, s>>>(p, cn);
+    k_pairs_tile<SINGLE><<<grid_tiles(), kPairTile, 0, s>>>(p);
+    mark("k_pairs");
+    k_pairs_faces<SINGLE><<<grid_mol(), 256, 0, s>>>(p);
+    mark("k_pairs_faces");
+    k_commit<<<grid_small(), 128, 0, s>>>(p);
     mark("k_commit");
     for (int round = 1; round < dnet.rounds; ++round) {
       k_research<<<grid_small(), 128, 0, s>>>(p);
       mark("k_research");
-      k_commit<SINGLE><<<grid_small(), 128, 0, s>>>(p, cn);
+      k_commit<<<grid_small(), 128, 0, s>>>(p);
       mark("k_commit");
     }
-    k_products<SINGLE><<<grid_small(), 128, 0, s>>>(p, cn);
+    k_products<<<grid_small(), 128, 0, s>>>(p);
     mark("k_products");
     k_fix_count<<<1, 32, 0, s>>>(p.q_n, (int)pcap);
     mark("k_fix_count");
-    counts_ready = fuse_next;
   }
 
-  // Enqueue one step with the given parity.  fuse_next: take the next step's
-  // box histogram inside this step (not when the next step's moves will differ,
-  // e.g. after an injected step).
-  void enqueue_step(int par, bool rebin_only, bool fuse_next = true) {
-    fuse_next = fuse_next && fuse_count;
-    if (reps.size() == 1) enqueue_step_t<true>(par, rebin_only, fuse_next);
-    else enqueue_step_t<false>(par, rebin_only, fuse_next);
+  // Enqueue one step with the given parity (inputs A/P = buffers `par`).
+  void enqueue_step(int par, bool rebin_only) {
+    if (reps.size() == 1) enqueue_step_t<true>(par, rebin_only);
+    else enqueue_step_t<false>(par, rebin_only);
   }
 
-  int launches_per_step() const { return 11 + 2 * (dnet.rounds - 1); }
+  int launches_per_step() const { return 12 + 2 * (dnet.rounds - 1); }
 
   int upload_const(std::string *err) {
     CK(cudaMemcpyToSymbolAsync(c_net, &dnet, sizeof(DevNet), 0, cudaMemcpyHostToDevice, stream));
@@ -1771,6 +1718,7 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
   CK(cudaMalloc(&E.d_cand, E.candcap * sizeof(int)));
   CK(cudaMalloc(&E.d_best, E.cap * sizeof(ull)));
   CK(cudaMalloc(&E.d_face, E.cap * sizeof(int)));
+  CK(cudaMalloc(&E.d_tmp, (E.cap + E.pcap) * sizeof(float4)));
   CK(cudaMemsetAsync(E.d_best, 0xFF, E.cap * sizeof(ull), E.stream));
   CK(cudaMalloc(&E.d_counters, 8 * sizeof(unsigned long long)));
   CK(cudaMemsetAsync(E.d_counters, 0, 8 * sizeof(unsigned long long), E.stream));
@@ -1832,7 +1780,6 @@ int Engine::update_reps(const std::vector<RepSpec> &reps, std::string *err) {
   EngineImpl &E = *impl_;
   if (reps.size() != E.reps.size()) { if (err) *err = "replicate count changed"; return -6; }
   E.reps = reps;
-  E.counts_ready = false;  // first-order probabilities and step lengths changed
   return E.build_rep_tables(err);
 }
 
@@ -1852,6 +1799,9 @@ int Engine::set_molecules(long long n, const double *pos, const int *species, co
       CK(cudaMalloc(&E.d_ppc[k], E.pcap * sizeof(float4)));
       CK(cudaMalloc(&E.d_pid[k], E.pcap * sizeof(ull)));
     }
+    cudaFree(E.d_tmp);
+    E.d_tmp = nullptr;
+    CK(cudaMalloc(&E.d_tmp, (E.cap + E.pcap) * sizeof(float4)));
     E.invalidate_graph();
   }
   if (n > E.cap) { if (err) *err = "more molecules than the engine capacity"; return -9; }
@@ -1921,21 +1871,9 @@ int Engine::run(long long nsteps, std::string *err) {
     if (nsteps != 1) { if (err) *err = "injected displacements apply to one step"; return -6; }
   }
   long long done = 0;
-  if (inj) {
-    // the injected moves differ from the next step's, so nothing is fused
-    E.counts_ready = false;
-    E.enqueue_step(E.parity, false, false);
-    E.parity ^= 1;
-    done = 1;
-  }
   if (E.use_graph && !inj) {
-    // graph replays start at parity 0 with the next histogram already taken
-    if (E.parity == 1 || !E.counts_ready) {
-      E.enqueue_step(E.parity, false);
-      E.parity ^= 1;
-      done++;
-    }
-    if (E.parity == 1 && nsteps - done >= 1) {
+    // graph replays start at parity 0
+    if (E.parity == 1) {
       E.enqueue_step(1, false);
       E.parity = 0;
       done++;
@@ -2096,7 +2034,6 @@ int Engine::set_injection(long long n, const uint64_t *sernos, const double *dis
   CK(cudaMemcpy(E.d_injval, vals.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
   E.inj_n = (int)n;
   E.dnet.inject = 1;
-  E.counts_ready = false;
   E.invalidate_graph();
   return E.upload_const(err);
 }
