@@ -103,6 +103,7 @@ struct DevNet {
   int any_absorb;
   int inject;          // deterministic mode active
   int npanel;
+  double surf_eps;     // distance kept between a molecule and a panel after an interaction
   int rounds;          // pair conflict-resolution rounds
   int uni_n[kMaxSpecies];
   uint8_t uni_list[kMaxSpecies][kMaxUniPerSpecies];
@@ -129,18 +130,19 @@ struct DevGeo {
   float vol;
 };
 
-// Per-replicate surface panel set (shared by replicates; absolute double
-// coordinates relative to the replicate's low corner are converted on the fly).
+// Surface panel (shared by all replicates; coordinates relative to the low
+// corner of the system, FP64 because crossing tests near a panel need it).
 struct DevPanel {
   int shape;        // 0 rect, 2 sphere
-  int axis;
-  int front_sign;
-  float pos;        // rect plane coordinate (relative to low corner)
-  float lo[3], hi[3];
-  float center[3];  // sphere centre (relative to low corner)
-  float radius;
-  int act_front, act_back;   // 0 reflect 1 transmit 2 absorb
-  uint32_t abs_front, abs_back, tr_front, tr_back;
+  int axis;         // rect: perpendicular axis
+  int front_sign;   // +1: front face toward +axis (rect) / outward (sphere)
+  int pad;
+  double pos;       // rect plane coordinate
+  double lo[3], hi[3];
+  double center[3]; // sphere centre
+  double radius;
+  int act_front, act_back;   // default action per face: 0 reflect 1 transmit 2 absorb
+  uint32_t abs_front, abs_back, tr_front, tr_back, rf_front, rf_back;  // per-species overrides
 };
 
 struct Event {      // one reaction or birth; products are placed by k_products

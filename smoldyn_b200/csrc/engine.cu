@@ -250,6 +250,178 @@ __device__ __forceinline__ const DevGeo &geo_of(const KParams &p, int rep) {
   return p.geo[rep];
 }
 
+// ---- surfaces ---------------------------------------------------------------
+// Solution-phase molecules against sphere and axis-aligned rectangle panels,
+// restating checksurfaces (smolsurface.c:5114-5182): walk the segment from the
+// previous position to the new one, take the nearest panel crossing, apply
+// the face's action (dosurfinteract :4930 - reflect about the tangent plane
+// at the crossing point (surfacereflect :4821), transmit, or absorb), restart
+// from the crossing point nudged to the proper side (fixpt2panel :4460), and
+// stop after 100 rounds by returning the molecule to its prior position.
+// FP64 throughout: the positions come from exact conversions of the FP32
+// box-local coordinates.
+
+// action of panel pn on species sp arriving at face (0 front, 1 back)
+__device__ __forceinline__ int panel_action(const DevPanel &pn, int face, int sp) {
+  const uint32_t bit = 1u << sp;
+  if (face == 0) {
+    if (pn.abs_front & bit) return 2;
+    if (pn.tr_front & bit) return 1;
+    if (pn.rf_front & bit) return 0;
+    return pn.act_front;
+  }
+  if (pn.abs_back & bit) return 2;
+  if (pn.tr_back & bit) return 1;
+  if (pn.rf_back & bit) return 0;
+  return pn.act_back;
+}
+
+// unit normal toward the front face at point x of the panel
+__device__ __forceinline__ void panel_normal(const DevPanel &pn, const double x[3], double n[3]) {
+  if (pn.shape == 2) {
+    double l = 0;
+    for (int d = 0; d < 3; ++d) {
+      n[d] = x[d] - pn.center[d];
+      l += n[d] * n[d];
+    }
+    l = (l > 0) ? pn.front_sign / sqrt(l) : 0.0;
+    for (int d = 0; d < 3; ++d) n[d] *= l;
+  } else {
+    n[0] = n[1] = n[2] = 0.0;
+    n[pn.axis] = (double)pn.front_sign;
+  }
+}
+
+// signed distance from the panel's surface, positive on the front side
+__device__ __forceinline__ double panel_sdist(const DevPanel &pn, const double x[3]) {
+  if (pn.shape == 2) {
+    double r2 = 0;
+    for (int d = 0; d < 3; ++d) r2 += (x[d] - pn.center[d]) * (x[d] - pn.center[d]);
+    return pn.front_sign * (sqrt(r2) - pn.radius);
+  }
+  return pn.front_sign * (x[pn.axis] - pn.pos);
+}
+
+// Crossing of segment a->b with a panel: t in (0,1] and the face hit, or
+// t = 2 when the segment does not cross (smolsurface.c:4000 lineXpanel).
+__device__ __forceinline__ double panel_cross(const DevPanel &pn, const double a[3], const double b[3], int &face) {
+  double v[3];
+  for (int d = 0; d < 3; ++d) v[d] = b[d] - a[d];
+  if (pn.shape == 2) {
+    double w[3], vv = 0, wv = 0, ww = 0;
+    for (int d = 0; d < 3; ++d) {
+      w[d] = a[d] - pn.center[d];
+      vv += v[d] * v[d];
+      wv += w[d] * v[d];
+      ww += w[d] * w[d];
+    }
+    if (vv <= 0) return 2.0;
+    const double c = ww - pn.radius * pn.radius;
+    const double disc = wv * wv - vv * c;
+    if (disc < 0) return 2.0;
+    const double sq = sqrt(disc);
+    const bool inside = c < 0;
+    const double t = inside ? (-wv + sq) / vv : (-wv - sq) / vv;
+    if (!(t > 0 && t <= 1)) return 2.0;
+    // arriving from inside: the inside face is the back one when front faces out
+    face = (inside == (pn.front_sign > 0)) ? 1 : 0;
+    return t;
+  }
+  const int ax = pn.axis;
+  const double d0 = a[ax] - pn.pos, d1 = b[ax] - pn.pos;
+  if (d0 == 0 || (d0 > 0) == (d1 > 0)) return 2.0;
+  const double t = d0 / (d0 - d1);
+  if (!(t > 0 && t <= 1)) return 2.0;
+  for (int d = 0; d < 3; ++d) {
+    if (d == ax) continue;
+    const double x = a[d] + t * v[d];
+    if (x < pn.lo[d] || x > pn.hi[d]) return 2.0;
+  }
+  face = ((d0 > 0) == (pn.front_sign > 0)) ? 0 : 1;
+  return t;
+}
+
+// Returns 1 if the molecule is absorbed; p1 is updated in place.
+__device__ int surface_interact(int sp, const double p0_in[3], double p1[3], double eps, int &hits) {
+  const int np = c_net.npanel;
+  double p0[3] = {p0_in[0], p0_in[1], p0_in[2]};
+  for (int it = 0; it < 100; ++it) {
+    double tmin = 2.0;
+    int kmin = -1, fmin = 0;
+    for (int k = 0; k < np; ++k) {
+      int f = 0;
+      const double t = panel_cross(c_panels[k], p0, p1, f);
+      if (t < tmin) { tmin = t; kmin = k; fmin = f; }
+    }
+    if (kmin < 0) {
+      // keep the final position at least eps off every panel, on its side
+      for (int k = 0; k < np; ++k) {
+        const double sd = panel_sdist(c_panels[k], p1);
+        if (fabs(sd) < eps) {
+          double n[3];
+          panel_normal(c_panels[k], p1, n);
+          const double side = (sd > 0 || (sd == 0 && panel_sdist(c_panels[k], p0) > 0)) ? 1.0 : -1.0;
+          for (int d = 0; d < 3; ++d) p1[d] += (side * eps - sd) * n[d];
+        }
+      }
+      return 0;
+    }
+    hits++;
+    const DevPanel &pn = c_panels[kmin];
+    const int act = panel_action(pn, fmin, sp);
+    if (act == 2) return 1;
+    double x[3], n[3];
+    for (int d = 0; d < 3; ++d) x[d] = p0[d] + tmin * (p1[d] - p0[d]);
+    panel_normal(pn, x, n);
+    const double side = (fmin == 0) ? 1.0 : -1.0;  // incoming side along n
+    if (act == 0) {
+      double dot = 0;
+      for (int d = 0; d < 3; ++d) dot += (p1[d] - x[d]) * n[d];
+      for (int d = 0; d < 3; ++d) p1[d] -= 2.0 * dot * n[d];
+      for (int d = 0; d < 3; ++d) p0[d] = x[d] + side * eps * n[d];
+    } else {
+      for (int d = 0; d < 3; ++d) p0[d] = x[d] - side * eps * n[d];
+    }
+  }
+  for (int d = 0; d < 3; ++d) p1[d] = p0_in[d];  // gave up: prior position
+  return 0;
+}
+
+// absolute position (relative to the low corner) of a box-local coordinate
+__device__ __forceinline__ void to_abs(const DevGeo &g, const int ix[3], const float u[3], double x[3]) {
+  for (int d = 0; d < 3; ++d) x[d] = (double)ix[d] * (double)g.h[d] + (double)u[d];
+}
+
+// back to box-local form (walls are transparent once surfaces exist)
+__device__ __forceinline__ void from_abs(const DevGeo &g, const double x[3], int ix[3], float u[3]) {
+  for (int d = 0; d < 3; ++d) {
+    const double h = (double)g.h[d];
+    int j = (int)floor(x[d] / h);
+    if (j < 0) j = 0;
+    if (j > g.n[d] - 1) j = g.n[d] - 1;
+    ix[d] = j;
+    u[d] = (float)(x[d] - (double)j * h);
+  }
+}
+
+// True when the segment between two molecules crosses a surface panel: such
+// pairs do not react (rxnXsurface, used by bireact smolreact.c:3238).
+__device__ __forceinline__ bool pair_crosses_surface(const DevGeo &g, float4 pc, float vx, float vy, float vz) {
+  int ix[3];
+  unpack_cell(__float_as_uint(pc.w), ix[0], ix[1], ix[2]);
+  const float u[3] = {pc.x, pc.y, pc.z};
+  double a[3], b[3];
+  to_abs(g, ix, u, a);
+  b[0] = a[0] + vx;
+  b[1] = a[1] + vy;
+  b[2] = a[2] + vz;
+  for (int k = 0; k < c_net.npanel; ++k) {
+    int f;
+    if (panel_cross(c_panels[k], a, b, f) <= 1.0) return true;
+  }
+  return false;
+}
+
 // Move one molecule by one step (diffuse smolmolec.c:3115, checkwalls
 // smolwall.c:368, unireact decision smolreact.c:2997): returns 0 alive,
 // 1 removed by a wall, 2+r first-order reaction r fired (position is the
@@ -313,6 +485,13 @@ __device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, co
     }
     u[d] = w;
     ix[d] = j;
+  }
+  if (c_net.npanel > 0) {
+    double x0[3], x1[3];
+    to_abs(g, ix0, u0, x0);
+    to_abs(g, ix, u, x1);
+    if (surface_interact(sp, x0, x1, c_net.surf_eps, hits)) return 1;
+    from_abs(g, x1, ix, u);
   }
   if (c_net.any_absorb && !c_net.inject) {
     // Absorbing walls also remove molecules that stayed inside with probability
@@ -766,6 +945,7 @@ __device__ ull search_partner(const KParams &p, int i, float4 pc, ull id, uint32
           const float vz = (q.z - pc.z) + (float)dz * g.h[2];
           const float d2 = vx * vx + vy * vy + vz * vz;
           if (pair_reaction(p, rep, sp, spj, d2, ka, id_stream(jd), step) < 0) continue;
+          if (c_net.npanel > 0 && pair_crosses_surface(g, pc, vx, vy, vz)) continue;
           ncand++;
           const ull k = ((ull)__float_as_uint(d2) << 32) | (uint32_t)j;
           if (k < best) best = k;
@@ -860,10 +1040,12 @@ __device__ int search_round1(const KParams &p, int i, float4 pc, ull id, uint32_
 // Pair test shared by the staged and the neighbour-box paths: if i and j react
 // this step, fold the key into i's running best and register i on j.
 __device__ __forceinline__ void try_pair(const KParams &p, int i, ull idi, int sp, int rep, float d2, int j, ull jd,
-                                         float rs2, uint32_t step, ull &best, int &extra) {
+                                         float rs2, uint32_t step, ull &best, int &extra, float4 pc, float vx,
+                                         float vy, float vz) {
   if (d2 > rs2) return;
   const int spj = id_species(jd);
   if (spj == kDeadSpecies || !((c_net.pair_mask[sp] >> spj) & 1u)) return;
+  if (c_net.npanel > 0 && pair_crosses_surface(p.geo[rep], pc, vx, vy, vz)) return;
   if (pair_reaction(p, rep, sp, spj, d2, id_stream(idi), id_stream(jd), step) < 0) return;
   const uint32_t db = __float_as_uint(d2);
   const ull k = ((ull)db << 32) | (uint32_t)j;
@@ -928,7 +1110,8 @@ __global__ void __launch_bounds__(kPairTile, 4) k_pairs_tile(KParams p) {
       if (same) {
         const float4 q = s_pc[u];
         const float vx = q.x - pc.x, vy = q.y - pc.y, vz = q.z - pc.z;
-        try_pair(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, i + k, s_id[u], rs2, step, best, extra);
+        try_pair(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, i + k, s_id[u], rs2, step, best, extra, pc, vx,
+                 vy, vz);
       }
     }
     // a box longer than the staged window continues in global memory
@@ -937,7 +1120,8 @@ __global__ void __launch_bounds__(kPairTile, 4) k_pairs_tile(KParams p) {
       for (int j = i + kPairHalo; j < e; ++j) {
         const float4 q = p.b_pc[j];
         const float vx = q.x - pc.x, vy = q.y - pc.y, vz = q.z - pc.z;
-        try_pair(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, j, p.b_id[j], rs2, step, best, extra);
+        try_pair(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, j, p.b_id[j], rs2, step, best, extra, pc, vx, vy,
+                 vz);
       }
     }
     // molecules near a box face also need the neighbouring boxes: queue them for
@@ -1026,7 +1210,8 @@ __global__ void __launch_bounds__(256) k_pairs_faces(KParams p) {
             const float vx = (q.x - pc.x) + (float)dx * g.h[0];
             const float vy = (q.y - pc.y) + (float)dy * g.h[1];
             const float vz = (q.z - pc.z) + (float)dz * g.h[2];
-            try_pair(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, j, p.b_id[j], rs2, step, best, extra);
+            try_pair(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, j, p.b_id[j], rs2, step, best, extra, pc, vx, vy,
+                 vz);
           }
         }
       }
@@ -1206,6 +1391,15 @@ __global__ void k_products(KParams p) {
         if (d < g.dim && (c[d] <= 0 || c[d] >= g.n[d] - 1))
           if (walls_dim(w[d], c[d], g, d, hits)) dead = true;
         clamp_cell(w[d], c[d], g, d);
+      }
+      if (!dead && c_net.npanel > 0) {
+        // new molecules are checked against surfaces from the reaction site
+        // (smolsim.cpp:2656-2660, reborn pass of checksurfaces)
+        double x0[3], x1[3];
+        to_abs(g, cell, site, x0);
+        to_abs(g, c, w, x1);
+        if (surface_interact(psp, x0, x1, c_net.surf_eps, hits)) dead = true;
+        else from_abs(g, x1, c, w);
       }
       if (hits) atomicAdd(&p.counters[0], (unsigned long long)hits);
       if (dead) continue;
@@ -1404,7 +1598,7 @@ class EngineImpl {
     return p;
   }
 
-  int grid_mol() const { return sm_count() * 4; }
+  int grid_mol() const { return sm_count() * 8; }
   int grid_tiles() const { return sm_count() * 4; }
   int grid_small() const { return sm_count(); }
 
@@ -1627,6 +1821,7 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
   }
   D.rounds = 3;
   D.npanel = (int)net.panels.size();
+  D.surf_eps = 0;
   for (int r = 0; r < net.nrxn[1]; ++r) {
     const int sp = net.rct[1][r][0];
     if (D.uni_n[sp] >= kMaxUniPerSpecies) { if (err) *err = "too many first-order reactions for one species"; return -6; }
@@ -1689,6 +1884,14 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
   D.any_absorb = any_absorb ? 1 : 0;
   E.ncell = (int)cells;
   E.nscanblocks = (E.ncell + kScanTile - 1) / kScanTile;
+  {
+    // molecules are kept this far from panels after a surface interaction, so
+    // that rounding to FP32 box-local coordinates cannot move them across
+    float hmin = 1e30f;
+    for (const DevGeo &g : E.geo)
+      for (int d = 0; d < 3; ++d) hmin = std::min(hmin, g.h[d]);
+    D.surf_eps = 1e-5 * (double)hmin;
+  }
 
   // ---- capacities
   E.cap = std::max<long long>(capacity, 1024);
@@ -1753,19 +1956,21 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
       dp.shape = ps.shape;
       dp.axis = ps.axis;
       dp.front_sign = ps.front_sign;
-      dp.pos = (float)(ps.pos - s0.lo[ps.axis]);
+      dp.pos = ps.pos - s0.lo[ps.axis];
       for (int d = 0; d < 3; ++d) {
-        dp.lo[d] = (float)(ps.lo[d] - s0.lo[d]);
-        dp.hi[d] = (float)(ps.hi[d] - s0.lo[d]);
-        dp.center[d] = (float)(ps.center[d] - s0.lo[d]);
+        dp.lo[d] = ps.lo[d] - s0.lo[d];
+        dp.hi[d] = ps.hi[d] - s0.lo[d];
+        dp.center[d] = ps.center[d] - s0.lo[d];
       }
-      dp.radius = (float)ps.radius;
+      dp.radius = ps.radius;
       dp.act_front = ps.action_front;
       dp.act_back = ps.action_back;
       dp.abs_front = ps.absorb_front_mask;
       dp.abs_back = ps.absorb_back_mask;
       dp.tr_front = ps.trans_front_mask;
       dp.tr_back = ps.trans_back_mask;
+      dp.rf_front = ps.refl_front_mask;
+      dp.rf_back = ps.refl_back_mask;
       E.panels.push_back(dp);
     }
   }

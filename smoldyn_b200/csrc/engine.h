@@ -40,6 +40,8 @@ struct PanelSpec {
   uint32_t absorb_back_mask;
   uint32_t trans_front_mask;    // species bitmask overriding to transmit on front
   uint32_t trans_back_mask;
+  uint32_t refl_front_mask;     // species bitmask overriding to reflect on front
+  uint32_t refl_back_mask;
 };
 
 // Reaction network shared by every replicate.

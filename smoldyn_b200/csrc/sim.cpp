@@ -365,6 +365,8 @@ int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err) {
       ps.absorb_back_mask = sf.absorb_back;
       ps.trans_front_mask = sf.trans_front;
       ps.trans_back_mask = sf.trans_back;
+      ps.refl_front_mask = sf.refl_front;
+      ps.refl_back_mask = sf.refl_back;
       net->panels.push_back(ps);
     }
   return 0;
@@ -708,7 +710,8 @@ static int read_surface_statement(Sim &sim, SurfaceDef &sf, const std::string &w
       p.shape = 0;
       const std::string &ax = w[1];
       p.front_sign = (ax[0] == '-') ? -1 : 1;
-      p.axis = ax.back() - 'x';
+      const char ac = ax.back();
+      p.axis = (ac >= '0' && ac <= '2') ? ac - '0' : ac - 'x';
       if (p.axis < 0 || p.axis > 2) { if (err) *err = "panel rect: bad axis"; return -7; }
       double corner[3];
       for (int d = 0; d < 3; ++d) corner[d] = atof(w[2 + d].c_str());
