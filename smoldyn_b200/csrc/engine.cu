@@ -426,7 +426,7 @@ __device__ __forceinline__ bool pair_crosses_surface(const DevGeo &g, float4 pc,
 // smolwall.c:368, unireact decision smolreact.c:2997): returns 0 alive,
 // 1 removed by a wall, 2+r first-order reaction r fired (position is the
 // post-move position).
-template <bool SINGLE>
+template <bool SINGLE, bool SURF>
 __device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, const KParams &p,
                                            const float *gtab, int rebin_only, int &hits) {
   const int sp = id_species(id);
@@ -486,7 +486,7 @@ __device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, co
     u[d] = w;
     ix[d] = j;
   }
-  if (c_net.npanel > 0) {
+  if (SURF) {
     double x0[3], x1[3];
     to_abs(g, ix0, u0, x0);
     to_abs(g, ix, u, x1);
@@ -614,7 +614,7 @@ __device__ __forceinline__ void count_box(const KParams &p, bool alive, float4 p
 // reacting molecules, the moved position into tmp (w = kTmpGone when the
 // molecule leaves the system), and the histogram of destination boxes.
 // rebin_only: no motion and no reactions (used after uploads).
-template <bool SINGLE>
+template <bool SINGLE, bool SURF>
 __global__ void __launch_bounds__(256) k_move(KParams p, int rebin_only) {
   extern __shared__ float s_gtab[];
   const float *gtab = rebin_only ? p.gtab : stage_gtab(p, s_gtab);
@@ -634,7 +634,7 @@ __global__ void __launch_bounds__(256) k_move(KParams p, int rebin_only) {
     }
     int fate = -1;
     int hits = 0;
-    if (valid) fate = advance_one<SINGLE>(pc, id, step, p, gtab, rebin_only, hits);
+    if (valid) fate = advance_one<SINGLE, SURF>(pc, id, step, p, gtab, rebin_only, hits);
     const bool alive = (fate == 0);
     if (i < total) p.tmp[i] = alive ? pc : make_float4(0.f, 0.f, 0.f, __uint_as_float(kTmpGone));
     count_box<SINGLE>(p, alive, pc, id);
@@ -888,6 +888,7 @@ __device__ __forceinline__ int pair_reaction(const KParams &p, int rep, int spa,
 
 // Closest live partner of molecule i within its pair binding radii.
 // Returns packed (dist2 bits << 32 | index) or ~0 when none; *ncand counts candidates.
+template <bool SURF>
 __device__ ull search_partner(const KParams &p, int i, float4 pc, ull id, uint32_t step, int &ncand) {
   const int nsorted = *p.b_n;
   const int sp = id_species(id);
@@ -945,7 +946,7 @@ __device__ ull search_partner(const KParams &p, int i, float4 pc, ull id, uint32
           const float vz = (q.z - pc.z) + (float)dz * g.h[2];
           const float d2 = vx * vx + vy * vy + vz * vz;
           if (pair_reaction(p, rep, sp, spj, d2, ka, id_stream(jd), step) < 0) continue;
-          if (c_net.npanel > 0 && pair_crosses_surface(g, pc, vx, vy, vz)) continue;
+          if (SURF && pair_crosses_surface(g, pc, vx, vy, vz)) continue;
           ncand++;
           const ull k = ((ull)__float_as_uint(d2) << 32) | (uint32_t)j;
           if (k < best) best = k;
@@ -1039,13 +1040,14 @@ __device__ int search_round1(const KParams &p, int i, float4 pc, ull id, uint32_
 
 // Pair test shared by the staged and the neighbour-box paths: if i and j react
 // this step, fold the key into i's running best and register i on j.
+template <bool SURF>
 __device__ __forceinline__ void try_pair(const KParams &p, int i, ull idi, int sp, int rep, float d2, int j, ull jd,
                                          float rs2, uint32_t step, ull &best, int &extra, float4 pc, float vx,
                                          float vy, float vz) {
   if (d2 > rs2) return;
   const int spj = id_species(jd);
   if (spj == kDeadSpecies || !((c_net.pair_mask[sp] >> spj) & 1u)) return;
-  if (c_net.npanel > 0 && pair_crosses_surface(p.geo[rep], pc, vx, vy, vz)) return;
+  if (SURF && pair_crosses_surface(p.geo[rep], pc, vx, vy, vz)) return;
   if (pair_reaction(p, rep, sp, spj, d2, id_stream(idi), id_stream(jd), step) < 0) return;
   const uint32_t db = __float_as_uint(d2);
   const ull k = ((ull)db << 32) | (uint32_t)j;
@@ -1065,7 +1067,7 @@ constexpr int kPairHalo = 32;   // extra molecules staged past the tile
 // box face; those are tested from global memory by the molecule in the
 // lower-numbered box.  Every in-radius pair is thus tested exactly once and
 // registered on both molecules (smolreact.c:3201-3298 tests each pair once).
-template <bool SINGLE>
+template <bool SINGLE, bool SURF>
 __global__ void __launch_bounds__(kPairTile, 4) k_pairs_tile(KParams p) {
   __shared__ float4 s_pc[kPairTile + kPairHalo];
   __shared__ ull s_id[kPairTile + kPairHalo];
@@ -1110,7 +1112,7 @@ __global__ void __launch_bounds__(kPairTile, 4) k_pairs_tile(KParams p) {
       if (same) {
         const float4 q = s_pc[u];
         const float vx = q.x - pc.x, vy = q.y - pc.y, vz = q.z - pc.z;
-        try_pair(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, i + k, s_id[u], rs2, step, best, extra, pc, vx,
+        try_pair<SURF>(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, i + k, s_id[u], rs2, step, best, extra, pc, vx,
                  vy, vz);
       }
     }
@@ -1120,7 +1122,7 @@ __global__ void __launch_bounds__(kPairTile, 4) k_pairs_tile(KParams p) {
       for (int j = i + kPairHalo; j < e; ++j) {
         const float4 q = p.b_pc[j];
         const float vx = q.x - pc.x, vy = q.y - pc.y, vz = q.z - pc.z;
-        try_pair(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, j, p.b_id[j], rs2, step, best, extra, pc, vx, vy,
+        try_pair<SURF>(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, j, p.b_id[j], rs2, step, best, extra, pc, vx, vy,
                  vz);
       }
     }
@@ -1156,7 +1158,7 @@ __global__ void __launch_bounds__(kPairTile, 4) k_pairs_tile(KParams p) {
 // stencil radius of a box face): one thread per queued molecule walks the
 // neighbouring boxes its stencil reaches; a pair across boxes is tested by the
 // molecule in the lower-numbered box.
-template <bool SINGLE>
+template <bool SINGLE, bool SURF>
 __global__ void __launch_bounds__(256) k_pairs_faces(KParams p) {
   const int nf = min(*p.nface, p.cap);
   const int n = *p.b_n;
@@ -1210,7 +1212,7 @@ __global__ void __launch_bounds__(256) k_pairs_faces(KParams p) {
             const float vx = (q.x - pc.x) + (float)dx * g.h[0];
             const float vy = (q.y - pc.y) + (float)dy * g.h[1];
             const float vz = (q.z - pc.z) + (float)dz * g.h[2];
-            try_pair(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, j, p.b_id[j], rs2, step, best, extra, pc, vx, vy,
+            try_pair<SURF>(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, j, p.b_id[j], rs2, step, best, extra, pc, vx, vy,
                  vz);
           }
         }
@@ -1222,6 +1224,7 @@ __global__ void __launch_bounds__(256) k_pairs_faces(KParams p) {
 }
 
 // Re-search for candidates still alive (conflict-resolution rounds >= 2).
+template <bool SURF>
 __global__ void k_research(KParams p) {
   const int nc = min(*p.ncand, p.candcap);
   const uint32_t step = *p.step;
@@ -1230,7 +1233,7 @@ __global__ void k_research(KParams p) {
     const ull id = p.b_id[i];
     if (id_species(id) == kDeadSpecies) continue;
     int ncd;
-    p.best[i] = search_partner(p, i, p.b_pc[i], id, step, ncd);
+    p.best[i] = search_partner<SURF>(p, i, p.b_pc[i], id, step, ncd);
   }
 }
 
@@ -1325,6 +1328,7 @@ __device__ __forceinline__ void random_rotation(uint4 r, float m[9]) {
   m[6] = 2.f * (qx * qz - qy * qw); m[7] = 2.f * (qy * qz + qx * qw); m[8] = 1.f - 2.f * (qx * qx + qy * qy);
 }
 
+template <bool SURF>
 __global__ void k_products(KParams p) {
   const int ne = min(*p.nev, p.evcap);
   const uint32_t step = *p.step;
@@ -1392,7 +1396,7 @@ __global__ void k_products(KParams p) {
           if (walls_dim(w[d], c[d], g, d, hits)) dead = true;
         clamp_cell(w[d], c[d], g, d);
       }
-      if (!dead && c_net.npanel > 0) {
+      if (SURF && !dead) {
         // new molecules are checked against surfaces from the reaction site
         // (smolsim.cpp:2656-2660, reborn pass of checksurfaces)
         double x0[3], x1[3];
@@ -1626,13 +1630,13 @@ class EngineImpl {
     marks.push_back({name, e});
   }
 
-  template <bool SINGLE>
+  template <bool SINGLE, bool SURF>
   void enqueue_step_t(int par, bool rebin_only) {
     KParams p = params(par);
     cudaStream_t s = stream;
     k_begin<<<1, 32, 0, s>>>(p, rebin_only ? 0 : 1);
     mark("k_begin");
-    k_move<SINGLE><<<grid_mol(), 256, rebin_only ? 0 : adv_smem(), s>>>(p, rebin_only ? 1 : 0);
+    k_move<SINGLE, SURF><<<grid_mol(), 256, rebin_only ? 0 : adv_smem(), s>>>(p, rebin_only ? 1 : 0);
     mark("k_move");
     k_scan_reduce<<<nscanblocks, kScanThreads, 0, s>>>(d_cnt, ncell, d_bsum);
     mark("k_scan_reduce");
@@ -1646,19 +1650,19 @@ class EngineImpl {
     if (rebin_only) return;
     k_births<<<grid_small(), 128, 0, s>>>(p);
     mark("k_births");
-    k_pairs_tile<SINGLE><<<grid_tiles(), kPairTile, 0, s>>>(p);
+    k_pairs_tile<SINGLE, SURF><<<grid_tiles(), kPairTile, 0, s>>>(p);
     mark("k_pairs");
-    k_pairs_faces<SINGLE><<<grid_mol(), 256, 0, s>>>(p);
+    k_pairs_faces<SINGLE, SURF><<<grid_mol(), 256, 0, s>>>(p);
     mark("k_pairs_faces");
     k_commit<<<grid_small(), 128, 0, s>>>(p);
     mark("k_commit");
     for (int round = 1; round < dnet.rounds; ++round) {
-      k_research<<<grid_small(), 128, 0, s>>>(p);
+      k_research<SURF><<<grid_small(), 128, 0, s>>>(p);
       mark("k_research");
       k_commit<<<grid_small(), 128, 0, s>>>(p);
       mark("k_commit");
     }
-    k_products<<<grid_small(), 128, 0, s>>>(p);
+    k_products<SURF><<<grid_small(), 128, 0, s>>>(p);
     mark("k_products");
     k_fix_count<<<1, 32, 0, s>>>(p.q_n, (int)pcap);
     mark("k_fix_count");
@@ -1666,8 +1670,11 @@ class EngineImpl {
 
   // Enqueue one step with the given parity (inputs A/P = buffers `par`).
   void enqueue_step(int par, bool rebin_only) {
-    if (reps.size() == 1) enqueue_step_t<true>(par, rebin_only);
-    else enqueue_step_t<false>(par, rebin_only);
+    const bool single = reps.size() == 1, surf = dnet.npanel > 0;
+    if (single && !surf) enqueue_step_t<true, false>(par, rebin_only);
+    else if (single) enqueue_step_t<true, true>(par, rebin_only);
+    else if (!surf) enqueue_step_t<false, false>(par, rebin_only);
+    else enqueue_step_t<false, true>(par, rebin_only);
   }
 
   int launches_per_step() const { return 12 + 2 * (dnet.rounds - 1); }
