@@ -182,6 +182,56 @@ enum ErrorCode smolgpuSolveRadii(int mode, long long n, const double *rate, doub
 double smolgpuBindingRadiusHost(double rate, double dt, double difc, double b, int rel);
 double smolgpuUnbindingRadiusHost(double pgem, double dt, double difc, double a);
 
+/* ==== Part 2b: ensembles of independent replicates ====================== */
+/* One engine runs nrep independent copies of a template simulation (its
+ * species, reactions, product placement, walls, dt and seed), each with its
+ * own box and rate constants, in one launch sequence.  Arrays are per
+ * replicate (boxes: nrep*dim values; counts out: nrep*nspecies with species
+ * index 0 = "empty").  Rate-derived parameters follow smolreact.c:1307-1577 per
+ * replicate; radius mode 0 = exact FP64 on the host, 1 = exact FP64 on the
+ * device (default), 2 = MLP surrogate with exact fallback. */
+typedef struct smolb_ens *ensptr;
+typedef struct smolb_surrogate *surptr;
+ensptr smolgpuNewEnsemble(simptr templ, int nrep);
+enum ErrorCode smolgpuEnsembleSetBoxes(ensptr ens, const double *low, const double *high);
+enum ErrorCode smolgpuEnsembleSetRates(ensptr ens, const char *reaction, const double *rates);
+enum ErrorCode smolgpuEnsembleAddMolecules(ensptr ens, const char *species, const int *counts);
+enum ErrorCode smolgpuEnsembleSetRadiusMode(ensptr ens, int mode);
+enum ErrorCode smolgpuEnsembleAttachSurrogate(ensptr ens, surptr sur);
+enum ErrorCode smolgpuEnsembleUpdate(ensptr ens);
+enum ErrorCode smolgpuEnsembleRunSteps(ensptr ens, long long nsteps);
+enum ErrorCode smolgpuEnsembleGetCounts(ensptr ens, long long *counts);
+enum ErrorCode smolgpuEnsembleGetReactionParams(ensptr ens, const char *reaction, double *bindrad,
+                                                double *unbindrad);
+long long smolgpuEnsembleGetFallbackCount(ensptr ens);
+enum ErrorCode smolgpuEnsembleSetStream(ensptr ens, void *stream);
+long long smolgpuEnsembleGetLaunchCount(ensptr ens);
+enum ErrorCode smolgpuEnsembleSynchronize(ensptr ens);
+enum ErrorCode smolgpuEnsembleFree(ensptr ens);
+
+/* ==== Part 2c: MLP surrogate of the radius solve ========================= */
+/* 3->64->64->2 tanh network on x = (log10 k/(D*s), unbinding ratio, reversible
+ * flag) -> y = (log10 a/s, b/s), s = sqrt(2*D*dt); trained on the device from
+ * samples of the exact FP64 solver (x: n*3, y: n*2 doubles).  Inference uses
+ * BF16 weights with FP32 accumulation and falls back to the exact solver when
+ * one numrxnrate evaluation shows a relative rate error above the tolerance
+ * (default 1e-3). */
+surptr smolgpuSurrogateNew(void);
+enum ErrorCode smolgpuSurrogateFree(surptr sur);
+enum ErrorCode smolgpuSurrogateTrain(surptr sur, long long nsamples, int epochs, int batch, double lr,
+                                     unsigned long long seed, double *final_loss, double *seconds);
+enum ErrorCode smolgpuSurrogateSamples(surptr sur, long long n, unsigned long long seed, double *x, double *y);
+enum ErrorCode smolgpuSurrogateForward(surptr sur, long long n, const double *x, double *y);
+enum ErrorCode smolgpuSurrogateLossGrad(surptr sur, long long n, const double *x, const double *y, double *loss,
+                                        float *grad);
+int smolgpuSurrogateParamCount(void);
+enum ErrorCode smolgpuSurrogateGetParams(surptr sur, float *params);
+enum ErrorCode smolgpuSurrogateSetParams(surptr sur, const float *params);
+enum ErrorCode smolgpuSurrogateSetTolerance(surptr sur, double tol);
+enum ErrorCode smolgpuSurrogatePairRadii(surptr sur, long long n, const double *kf, const double *dsum, double dt,
+                                         int same, int rev, int rparamt, double rparam, double *bind,
+                                         double *unbind, long long *nfallback);
+
 #ifdef __cplusplus
 }
 #endif

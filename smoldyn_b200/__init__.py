@@ -92,6 +92,34 @@ PROTOTYPES = {
     "smolgpuSolveRadii": (C.c_int, [C.c_int, C.c_longlong, _dp, C.c_double, _dp, _dp, C.c_int, _dp]),
     "smolgpuBindingRadiusHost": (C.c_double, [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int]),
     "smolgpuUnbindingRadiusHost": (C.c_double, [C.c_double, C.c_double, C.c_double, C.c_double]),
+    "smolgpuNewEnsemble": (_vp, [_sim, C.c_int]),
+    "smolgpuEnsembleSetBoxes": (C.c_int, [_vp, _dp, _dp]),
+    "smolgpuEnsembleSetRates": (C.c_int, [_vp, C.c_char_p, _dp]),
+    "smolgpuEnsembleAddMolecules": (C.c_int, [_vp, C.c_char_p, _ip]),
+    "smolgpuEnsembleSetRadiusMode": (C.c_int, [_vp, C.c_int]),
+    "smolgpuEnsembleAttachSurrogate": (C.c_int, [_vp, _vp]),
+    "smolgpuEnsembleUpdate": (C.c_int, [_vp]),
+    "smolgpuEnsembleRunSteps": (C.c_int, [_vp, C.c_longlong]),
+    "smolgpuEnsembleGetCounts": (C.c_int, [_vp, C.POINTER(C.c_longlong)]),
+    "smolgpuEnsembleGetReactionParams": (C.c_int, [_vp, C.c_char_p, _dp, _dp]),
+    "smolgpuEnsembleGetFallbackCount": (C.c_longlong, [_vp]),
+    "smolgpuEnsembleSetStream": (C.c_int, [_vp, _vp]),
+    "smolgpuEnsembleGetLaunchCount": (C.c_longlong, [_vp]),
+    "smolgpuEnsembleSynchronize": (C.c_int, [_vp]),
+    "smolgpuEnsembleFree": (C.c_int, [_vp]),
+    "smolgpuSurrogateNew": (_vp, []),
+    "smolgpuSurrogateFree": (C.c_int, [_vp]),
+    "smolgpuSurrogateTrain": (C.c_int, [_vp, C.c_longlong, C.c_int, C.c_int, C.c_double, C.c_ulonglong, _dp,
+                                        _dp]),
+    "smolgpuSurrogateSamples": (C.c_int, [_vp, C.c_longlong, C.c_ulonglong, _dp, _dp]),
+    "smolgpuSurrogateForward": (C.c_int, [_vp, C.c_longlong, _dp, _dp]),
+    "smolgpuSurrogateLossGrad": (C.c_int, [_vp, C.c_longlong, _dp, _dp, _dp, C.POINTER(C.c_float)]),
+    "smolgpuSurrogateParamCount": (C.c_int, []),
+    "smolgpuSurrogateGetParams": (C.c_int, [_vp, C.POINTER(C.c_float)]),
+    "smolgpuSurrogateSetParams": (C.c_int, [_vp, C.POINTER(C.c_float)]),
+    "smolgpuSurrogateSetTolerance": (C.c_int, [_vp, C.c_double]),
+    "smolgpuSurrogatePairRadii": (C.c_int, [_vp, C.c_longlong, _dp, _dp, C.c_double, C.c_int, C.c_int, C.c_int,
+                                            C.c_double, _dp, _dp, C.POINTER(C.c_longlong)]),
 }
 
 _lib = None
@@ -295,6 +323,146 @@ class Sim:
             if nr.value * nc.value else np.zeros((0, nc.value))
         C.CDLL(None).free(arr)
         return out
+
+
+class Ensemble:
+    """Independent replicates of a template Sim in one engine (C ABI owner)."""
+
+    def __init__(self, template, nrep):
+        self.lib = load()
+        self.nrep = nrep
+        self.dim = template.dim
+        self.template = template
+        self.ptr = self.lib.smolgpuNewEnsemble(template.ptr, nrep)
+        if not self.ptr:
+            check(ECerror)
+
+    def close(self):
+        if self.ptr:
+            self.lib.smolgpuEnsembleFree(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_boxes(self, low, high):
+        low = np.ascontiguousarray(low, dtype=np.float64).reshape(-1)
+        high = np.ascontiguousarray(high, dtype=np.float64).reshape(-1)
+        return check(self.lib.smolgpuEnsembleSetBoxes(self.ptr, dptr(low), dptr(high)))
+
+    def set_rates(self, rxn, rates):
+        rates = np.ascontiguousarray(rates, dtype=np.float64)
+        return check(self.lib.smolgpuEnsembleSetRates(self.ptr, rxn.encode(), dptr(rates)))
+
+    def add_molecules(self, species, counts):
+        counts = np.ascontiguousarray(counts, dtype=np.int32)
+        return check(self.lib.smolgpuEnsembleAddMolecules(self.ptr, species.encode(), counts.ctypes.data_as(_ip)))
+
+    def radius_mode(self, mode):
+        return check(self.lib.smolgpuEnsembleSetRadiusMode(self.ptr, mode))
+
+    def attach(self, sur):
+        return check(self.lib.smolgpuEnsembleAttachSurrogate(self.ptr, sur.ptr))
+
+    def update(self):
+        return check(self.lib.smolgpuEnsembleUpdate(self.ptr))
+
+    def run_steps(self, n):
+        return check(self.lib.smolgpuEnsembleRunSteps(self.ptr, int(n)))
+
+    def counts(self, nspecies):
+        out = np.zeros(self.nrep * nspecies, dtype=np.int64)
+        check(self.lib.smolgpuEnsembleGetCounts(self.ptr, out.ctypes.data_as(C.POINTER(C.c_longlong))))
+        return out.reshape(self.nrep, nspecies)
+
+    def reaction_params(self, rxn):
+        b = np.zeros(self.nrep)
+        u = np.zeros(self.nrep)
+        check(self.lib.smolgpuEnsembleGetReactionParams(self.ptr, rxn.encode(), dptr(b), dptr(u)))
+        return b, u
+
+    def fallbacks(self):
+        return self.lib.smolgpuEnsembleGetFallbackCount(self.ptr)
+
+    def set_stream(self, stream_ptr):
+        return check(self.lib.smolgpuEnsembleSetStream(self.ptr, C.c_void_p(stream_ptr)))
+
+    def synchronize(self):
+        return check(self.lib.smolgpuEnsembleSynchronize(self.ptr))
+
+    def launches(self):
+        return self.lib.smolgpuEnsembleGetLaunchCount(self.ptr)
+
+
+class Surrogate:
+    """MLP surrogate of the radius solve (C ABI owner)."""
+
+    def __init__(self):
+        self.lib = load()
+        self.ptr = self.lib.smolgpuSurrogateNew()
+
+    def close(self):
+        if self.ptr:
+            self.lib.smolgpuSurrogateFree(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def train(self, nsamples=1_000_000, epochs=20, batch=1024, lr=2e-3, seed=12345):
+        loss, secs = C.c_double(), C.c_double()
+        check(self.lib.smolgpuSurrogateTrain(self.ptr, int(nsamples), int(epochs), int(batch), float(lr), int(seed),
+                                             C.byref(loss), C.byref(secs)))
+        return loss.value, secs.value
+
+    def samples(self, n, seed=1):
+        x = np.zeros((n, 3))
+        y = np.zeros((n, 2))
+        check(self.lib.smolgpuSurrogateSamples(self.ptr, int(n), int(seed), dptr(x), dptr(y)))
+        return x, y
+
+    def forward(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros((len(x), 2))
+        check(self.lib.smolgpuSurrogateForward(self.ptr, len(x), dptr(x), dptr(y)))
+        return y
+
+    def loss_grad(self, x, y):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        loss = C.c_double()
+        g = np.zeros(self.lib.smolgpuSurrogateParamCount(), dtype=np.float32)
+        check(self.lib.smolgpuSurrogateLossGrad(self.ptr, len(x), dptr(x), dptr(y), C.byref(loss),
+                                                g.ctypes.data_as(C.POINTER(C.c_float))))
+        return loss.value, g
+
+    def params(self):
+        p = np.zeros(self.lib.smolgpuSurrogateParamCount(), dtype=np.float32)
+        check(self.lib.smolgpuSurrogateGetParams(self.ptr, p.ctypes.data_as(C.POINTER(C.c_float))))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        return check(self.lib.smolgpuSurrogateSetParams(self.ptr, p.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def tolerance(self, tol):
+        return check(self.lib.smolgpuSurrogateSetTolerance(self.ptr, float(tol)))
+
+    def pair_radii(self, kf, dsum, dt, same=0, rev=1, rparamt=RPratio, rparam=0.2):
+        kf = np.ascontiguousarray(kf, dtype=np.float64)
+        dsum = np.ascontiguousarray(dsum, dtype=np.float64)
+        b = np.zeros(len(kf))
+        u = np.zeros(len(kf))
+        nfb = C.c_longlong()
+        check(self.lib.smolgpuSurrogatePairRadii(self.ptr, len(kf), dptr(kf), dptr(dsum), float(dt), same, rev,
+                                                 rparamt, float(rparam), dptr(b), dptr(u), C.byref(nfb)))
+        return b, u, nfb.value
 
 
 def solve_radii_device(mode, rate, dt, difc, b, rel=0):

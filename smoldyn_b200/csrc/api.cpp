@@ -796,3 +796,9 @@ double smolgpuUnbindingRadiusHost(double pgem, double dt, double difc, double a)
 }
 
 }  // extern "C"
+
+// Shared with ensemble.cpp and surrogate.cu: record an error in the
+// process-global slot read by smolGetError.
+ErrorCode smolb_record_error(const char *func, ErrorCode code, const std::string &msg) {
+  return set_error(func, code, msg);
+}

@@ -1457,6 +1457,19 @@ __global__ void k_species_count(const ull *id, const int *n, long long *spcount,
       if (s_cnt[k]) atomicAdd((unsigned long long *)&spcount[k], (unsigned long long)s_cnt[k]);
 }
 
+// Batched pair-radius derivation (binding radius + reverse unbinding radius),
+// one thread per replicate: the exact FP64 path for ensembles.
+__global__ void k_pair_radii(long long n, const double *kf, const double *dsum, double dt, int same, int rev,
+                             int rparamt, double rparam, double *bind, double *unbind, int *err) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const rxnp::PairRadii r = rxnp::pair_radii(kf[i], same, dsum[i], dt, rev, rparamt, rparam);
+    bind[i] = r.bindrad;
+    unbind[i] = r.unbindrad;
+    err[i] = r.err;
+  }
+}
+
 // Batched FP64 radius solve (one thread per problem).
 __global__ void k_solve_radii(int mode, long long n, const double *rate, double dt, const double *difc,
                               const double *b, int rel, double *out) {
@@ -2316,3 +2329,24 @@ int solve_radii_device(int mode, long long n, const double *rate, double dt, con
 
 }  // namespace smolb
 
+
+namespace smolb {
+int solve_pair_radii_device(long long n, const double *kf, const double *dsum, double dt, int same, int rev,
+                            int rparamt, double rparam, double *bind, double *unbind, int *errs, std::string *err) {
+  if (n <= 0) return 0;
+  double *d = nullptr;
+  int *de = nullptr;
+  CK(cudaMalloc(&d, (size_t)n * 4 * sizeof(double)));
+  CK(cudaMalloc(&de, (size_t)n * sizeof(int)));
+  CK(cudaMemcpy(d, kf, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d + n, dsum, n * sizeof(double), cudaMemcpyHostToDevice));
+  k_pair_radii<<<sm_count() * 2, 128>>>(n, d, d + n, dt, same, rev, rparamt, rparam, d + 2 * n, d + 3 * n, de);
+  CK(cudaGetLastError());
+  CK(cudaMemcpy(bind, d + 2 * n, n * sizeof(double), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(unbind, d + 3 * n, n * sizeof(double), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(errs, de, n * sizeof(int), cudaMemcpyDeviceToHost));
+  cudaFree(d);
+  cudaFree(de);
+  return 0;
+}
+}  // namespace smolb

@@ -127,3 +127,10 @@ int solve_radii_device(int mode, long long n, const double *rate, double dt, con
                        const double *b, int rel, double *out, std::string *err);
 
 }  // namespace smolb
+
+namespace smolb {
+// Batched pair_radii (binding radius of A+B->C with rate kf[i], mutual
+// diffusion dsum[i], and the reverse's unbinding radius) on the device.
+int solve_pair_radii_device(long long n, const double *kf, const double *dsum, double dt, int same, int rev,
+                            int rparamt, double rparam, double *bind, double *unbind, int *errs, std::string *err);
+}  // namespace smolb

@@ -425,3 +425,64 @@ SMOLB_HD inline double unbindingradius(double pgem, double dt, double difc, doub
 
 }  // namespace rxnp
 }  // namespace smolb
+
+namespace smolb {
+namespace rxnp {
+
+// RevParam codes used below (smoldyn.h:358)
+enum : int { kRPnone = 0, kRPirrev = 1, kRPpgem = 4, kRPpgemmax = 5, kRPpgemmaxw = 6, kRPratio = 7,
+             kRPunbindrad = 8 };
+
+struct PairRadii {
+  double bindrad;    // binding radius of A + B -> C
+  double unbindrad;  // unbinding radius of the reverse C -> A + B (0 if none)
+  int err;           // 0 ok, 1 illegal input, 2 requested pgem unreachable
+};
+
+// Binding radius of a bimolecular reaction with rate constant kf and, when
+// it has a direct reverse (rev != 0), the unbinding radius of that reverse for
+// its product placement (rparamt, rparam).  Restates the order-2 branch of
+// rxnsetrate (smolreact.c:1364-1414, probability 1, no chi) followed by
+// rxnsetproduct for the reverse reaction (smolreact.c:1519-1571); like species
+// double the rate (smolreact.c:1374).  dsum = D_A + D_B.
+SMOLB_HD inline PairRadii pair_radii(double kf, int same_species, double dsum, double dt, int rev, int rparamt,
+                                     double rparam) {
+  PairRadii o{0, 0, 0};
+  double rate3 = same_species ? 2 * kf : kf;
+  if (rev && rparamt == kRPnone) {
+    rparamt = kRPpgemmaxw;
+    rparam = 0.2;
+  }
+  if (!rev) rparamt = kRPnone;
+  if (rate3 <= 0) return o;
+  if (dsum <= 0) { o.err = 1; return o; }
+  double a;
+  if (rparamt == kRPunbindrad) a = bindingradius(rate3, dt, dsum, rparam, 0);
+  else if (rparamt == kRPratio) a = bindingradius(rate3, dt, dsum, rparam, 1);
+  else if (rparamt == kRPpgem) a = bindingradius(rate3 * (1.0 - rparam), dt, dsum, -1, 0);
+  else if (rparamt == kRPpgemmax || rparamt == kRPpgemmaxw) {
+    a = bindingradius(rate3, dt, dsum, 0, 0);
+    const double ub = unbindingradius(rparam, dt, dsum, a);
+    if (ub > 0) a = bindingradius(rate3 * (1.0 - rparam), dt, dsum, -1, 0);
+  } else {
+    a = bindingradius(rate3, dt, dsum, -1, 0);
+  }
+  o.bindrad = a;
+  if (!rev || a <= 0) return o;
+  if (rparamt == kRPunbindrad) o.unbindrad = rparam;
+  else if (rparamt == kRPratio) o.unbindrad = rparam * a;
+  else if (rparamt == kRPpgem) {
+    const double r = unbindingradius(rparam, dt, dsum, a);
+    if (r == -2) o.err = 1;
+    else if (r < 0) o.err = 2;
+    else o.unbindrad = r;
+  } else if (rparamt == kRPpgemmax || rparamt == kRPpgemmaxw) {
+    const double r = unbindingradius(rparam, dt, dsum, a);
+    if (r == -2) o.err = 1;
+    else o.unbindrad = r > 0 ? r : 0;
+  }
+  return o;
+}
+
+}  // namespace rxnp
+}  // namespace smolb

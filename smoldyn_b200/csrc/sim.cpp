@@ -823,3 +823,7 @@ int load_config_file(Sim &sim, const std::string &path, const std::string &name,
 }
 
 }  // namespace smolb
+
+namespace smolb {
+int find_reverse_rxn(const Sim &s, int order, int r, int *o2, int *r2) { return find_reverse(s, order, r, o2, r2); }
+}  // namespace smolb

@@ -101,5 +101,7 @@ int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err);
 // Text configuration reader (statement subset of smolsim.cpp:626 simreadstring).
 int read_config_statement(Sim &sim, const std::string &word, const std::string &rest, std::string *err);
 int load_config_file(Sim &sim, const std::string &path, const std::string &name, std::string *err);
+// findreverserxn (smolreact.c:345): 0 none, 1 direct reverse, 2 continuation.
+int find_reverse_rxn(const Sim &s, int order, int r, int *o2, int *r2);
 
 }  // namespace smolb

@@ -1,0 +1,100 @@
+"""The learned radius surrogate: samples, gradients, training, accuracy.
+
+- Device samples of the exact solver equal the reference's bindingradius
+  (oracle/_ref/librxnparam_ref.so) to 1e-9.
+- The hand-written training kernel's loss and gradient equal the NumPy FP64
+  restatement (oracle/mlp_oracle.py) to FP32 tolerance (1e-4 relative).
+- Training on 10^6 exact samples reaches a loss well below the untrained one;
+  surrogate radii with the fallback rule give rate constants within 1% of the
+  exact solver's (the tabulated rate at the predicted radius), and without
+  fallback most instances are accepted.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import smoldyn_b200 as sb
+from tests import oracle_lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import mlp_oracle  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def test_samples_match_reference_solver():
+    ref = oracle_lib.reference_rxnparam()
+    if ref is None:
+        pytest.skip("reference rxnparam not compiled")
+    s = sb.Surrogate()
+    x, y = s.samples(2000, seed=9)
+    ok = np.isfinite(y[:, 0])
+    assert ok.mean() > 0.5
+    for i in np.where(ok)[0][:500]:
+        lk, rho, rev = x[i]
+        k = 0.5 * 10 ** lk
+        a = ref.bindingradius(k, 1.0, 0.5, rho if rev else -1.0, 1 if rev else 0)
+        assert abs(10 ** y[i, 0] - a) <= 1e-9 * a
+        assert abs(y[i, 1] - (rho * a if rev else 0.0)) <= 1e-9 * max(a, 1e-30)
+
+
+def test_gradient_matches_numpy_oracle():
+    s = sb.Surrogate()
+    x, y = s.samples(4096, seed=3)
+    ok = np.isfinite(y[:, 0])
+    x, y = x[ok][:2048], y[ok][:2048]
+    p = s.params()
+    loss, g = s.loss_grad(x, y)
+    loss_ref, g_ref = mlp_oracle.loss_grad(p, x, y)
+    assert abs(loss - loss_ref) <= 1e-4 * abs(loss_ref)
+    scale = np.abs(g_ref).max()
+    assert np.abs(g - g_ref).max() <= 1e-4 * scale, np.abs(g - g_ref).max() / scale
+    # forward too
+    yf = s.forward(x[:256])
+    assert np.allclose(yf, mlp_oracle.forward(p, x[:256]), rtol=1e-4, atol=1e-4)
+
+
+@pytest.fixture(scope="module")
+def trained():
+    s = sb.Surrogate()
+    loss, secs = s.train(nsamples=1_000_000, epochs=20, batch=1024, lr=2e-3, seed=12345)
+    return s, loss, secs
+
+
+def test_training_reduces_loss(trained):
+    s, loss, secs = trained
+    # standardised targets: an untrained network sits near 1
+    assert loss < 1e-3, loss
+    assert secs < 120
+
+
+def test_surrogate_rate_error_and_fallback(trained):
+    s, _, _ = trained
+    rng = np.random.default_rng(5)
+    n = 20000
+    kf = 10 ** rng.uniform(-3, 0, n)
+    dsum = np.full(n, 2.0)
+    dt = 0.01
+    rho = 0.2
+    b, u, nfb = s.pair_radii(kf, dsum, dt, same=0, rev=1, rparamt=sb.RPratio, rparam=rho)
+    # the tabulated per-step rate at the returned radius reproduces k*dt
+    lib = sb.load()
+    step = np.sqrt(2 * dsum * dt)
+    # exact radii for comparison (device FP64 solver)
+    exact = sb.solve_radii_device(0, kf, dt, dsum, np.full(n, rho), rel=1)
+    rel_rad = np.abs(b - exact) / exact
+    assert np.all(np.abs(u - rho * b) <= 1e-12 * b)
+    assert np.median(rel_rad) < 1e-3
+    assert rel_rad.max() < 2e-2
+    frac_fb = nfb / n
+    assert frac_fb < 0.9, frac_fb
+    # with the fallback rule every accepted radius has rate error <= 1e-3
+    ref = oracle_lib.reference_rxnparam()
+    if ref is not None:
+        idx = rng.choice(n, 300, replace=False)
+        for i in idx:
+            r = ref.numrxnrate(step[i], b[i], rho * b[i])
+            assert abs(r / (kf[i] * dt) - 1) <= 1.01e-3 or abs(b[i] - exact[i]) <= 1e-9 * exact[i]
