@@ -217,6 +217,7 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=100000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--no-batched", action="store_true", help="skip the ensemble and surrogate workloads")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -302,6 +303,12 @@ def main():
     if not args.no_e2e:
         e2e = run_e2e(sb, args, rank, world, dist, barrier)
 
+    # ---- batched ensemble and surrogate sweep (extra workloads, same GPU)
+    batched = surrogate = None
+    if not args.no_batched:
+        batched = run_batched(sb, torch, args, rank)
+        surrogate = run_surrogate(sb, torch, args, rank)
+
     # ---- CPU baseline (rank 0, single GPU run only)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -321,12 +328,165 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": workload_config(args), "e2e": e2e, "gpu_launches": int(launches),
             "roofline": roof, "step_roofline_frac": step_frac, "kernels": kernels, "cpu_baseline": cpu,
-            "clocks": ck,
+            "clocks": ck, "batched": batched, "batched_surrogate": surrogate,
         }
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+def ensemble_template(sb, placement=None):
+    s = sb.Sim(3, (0, 0, 0), (1, 1, 1))
+    for nm, d in zip(("A", "B", "C"), DIFC):
+        s.add_species(nm, d)
+    for d in range(3):
+        s.boundary(d, -1, "r")
+    s.set_times(0, 1e9, DT)
+    s.seed(4242)
+    s.add_reaction("fwd", "A", "B", ["C"], 0.05)
+    s.add_reaction("rev", "C", None, ["A", "B"], 0.1)
+    if placement is not None:
+        s.set_products("rev", *placement)
+    return s
+
+
+def draw_replicates(rng, nrep, lo, hi):
+    n = np.rint(10 ** rng.uniform(np.log10(lo), np.log10(hi), nrep)).astype(np.int64)
+    side = (n / 0.01) ** (1.0 / 3.0)
+    return n, side
+
+
+def time_on_stream(torch, stream, fn):
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / 1e3
+
+
+def run_batched(sb, torch, args, rank):
+    """Ensemble workload: 4096 replicates, N log-uniform in [1e2, 1e5] at
+    density 0.01, kf and kr log-uniform in [1e-3, 1] per replicate, radii from
+    the exact FP64 solver on the device, dt = 0.01."""
+    rng = np.random.default_rng(12345 + rank)
+    R = 4096
+    n, side = draw_replicates(rng, R, 1e2, 1e5)
+    kf = 10 ** rng.uniform(-3, 0, R)
+    kr = 10 ** rng.uniform(-3, 0, R)
+    t = ensemble_template(sb)
+    e = sb.Ensemble(t, R)
+    e.set_boxes(np.zeros((R, 3)), np.repeat(side[:, None], 3, 1))
+    e.set_rates("fwd", kf)
+    e.set_rates("rev", kr)
+    e.add_molecules("A", n // 2 + n % 2)
+    e.add_molecules("B", n // 2)
+    e.radius_mode(1)
+    t0 = time.perf_counter()
+    e.update()
+    setup = time.perf_counter() - t0
+    stream = torch.cuda.Stream()
+    e.set_stream(stream.cuda_stream)
+    e.run_steps(args.warmup)
+    steps = max(10, args.steps)
+    l0 = e.launches()
+    sec = time_on_stream(torch, stream, lambda: e.run_steps(steps))
+    tot = float(n.sum())
+    out = {"workload": "4096 replicates, N log-uniform [1e2,1e5] at density 0.01, kf,kr log-uniform [1e-3,1], "
+                       "reflective cubes, A+B<->C, dt=0.01, radii by the device FP64 solver",
+           "value": tot * steps / sec, "unit": METRIC, "molecules": int(tot), "replicates": R, "steps": steps,
+           "ms_per_step": sec * 1e3 / steps, "setup_s": setup, "gpu_launches": int(e.launches() - l0)}
+    e.close()
+    return out
+
+
+def run_surrogate(sb, torch, args, rank):
+    """Surrogate sweep: 65,536 replicates, N log-uniform in [1e2, 1e4] at
+    density 0.01, rates redrawn every 100 steps; radii from the MLP surrogate
+    (exact fallback above 1e-3 estimated rate error).  Compared with the same
+    ensemble on the exact device solver and with the plain form (each
+    replicate its own simulation) on a sample of replicates."""
+    rng = np.random.default_rng(777 + rank)
+    R = 65536
+    n, side = draw_replicates(rng, R, 1e2, 1e4)
+    rho = 1.5
+    sur = sb.Surrogate()
+    t0 = time.perf_counter()
+    loss, train_s = sur.train(nsamples=1_000_000, epochs=20, batch=1024, lr=2e-3, seed=12345)
+    t = ensemble_template(sb, placement=(sb.RPratio, rho))
+    e = sb.Ensemble(t, R)
+    e.set_boxes(np.zeros((R, 3)), np.repeat(side[:, None], 3, 1))
+
+    def redraw():
+        e.set_rates("fwd", 10 ** rng.uniform(-3, 0, R))
+        e.set_rates("rev", 10 ** rng.uniform(-3, 0, R))
+
+    redraw()
+    e.add_molecules("A", n // 2 + n % 2)
+    e.add_molecules("B", n // 2)
+    e.attach(sur)
+    e.radius_mode(2)
+    e.update()
+    setup = time.perf_counter() - t0
+    stream = torch.cuda.Stream()
+    e.set_stream(stream.cuda_stream)
+    e.run_steps(args.warmup)
+    steps = 200
+    fb = []
+
+    def work():
+        for blk in range(steps // 100):
+            redraw()
+            e.update()
+            fb.append(e.fallbacks())
+            e.run_steps(100)
+
+    sec = time_on_stream(torch, stream, work)
+    tot = float(n.sum())
+    # solver cost of one redraw: surrogate vs exact device vs exact host
+    solver = {}
+    for mode, name in ((2, "surrogate"), (1, "exact_device"), (0, "exact_host")):
+        e.radius_mode(mode)
+        redraw()
+        t1 = time.perf_counter()
+        e.update()
+        solver[name + "_s"] = time.perf_counter() - t1
+    out = {"workload": "65536 replicates, N log-uniform [1e2,1e4] at density 0.01, A+B<->C with unbinding ratio "
+                       "%.1f, kf,kr log-uniform [1e-3,1] redrawn every 100 steps, dt=0.01, radii from the MLP "
+                       "surrogate with exact fallback" % rho,
+           "value": tot * steps / sec, "unit": METRIC, "molecules": int(tot), "replicates": R, "steps": steps,
+           "ms_per_step": sec * 1e3 / steps, "setup_s": setup, "surrogate_train_s": train_s,
+           "surrogate_loss": loss, "fallbacks_per_redraw": fb, "fallback_fraction": float(np.mean(fb)) / R,
+           "update_seconds": solver}
+    e.close()
+    # plain form: sampled replicates run one at a time as ordinary simulations
+    idx = rng.choice(R, 24, replace=False)
+    mol_steps, secs = 0.0, 0.0
+    for k in idx:
+        s = sb.Sim(3, (0, 0, 0), (side[k],) * 3)
+        for nm, d in zip(("A", "B", "C"), DIFC):
+            s.add_species(nm, d)
+        for d in range(3):
+            s.boundary(d, -1, "r")
+        s.set_times(0, 1e9, DT)
+        s.add_reaction("fwd", "A", "B", ["C"], 10 ** rng.uniform(-3, 0))
+        s.add_reaction("rev", "C", None, ["A", "B"], 10 ** rng.uniform(-3, 0))
+        s.set_products("rev", sb.RPratio, rho)
+        s.add_molecules("A", int(n[k] // 2 + n[k] % 2))
+        s.add_molecules("B", int(n[k] // 2))
+        s.update()
+        st = torch.cuda.Stream()
+        s.set_stream(st.cuda_stream)
+        s.run_steps(3)
+        secs += time_on_stream(torch, st, lambda: s.run_steps(100))
+        mol_steps += float(n[k]) * 100
+        s.close()
+    out["plain_form"] = {"value": mol_steps / secs, "unit": METRIC, "sampled_replicates": len(idx),
+                         "note": "each replicate run as its own simulation through the same engine"}
+    out["speedup_vs_plain_form"] = out["value"] / out["plain_form"]["value"]
+    return out
 
 
 def run_e2e(sb, args, rank, world, dist, barrier):

@@ -2004,6 +2004,17 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
 int Engine::update_reps(const std::vector<RepSpec> &reps, std::string *err) {
   EngineImpl &E = *impl_;
   if (reps.size() != E.reps.size()) { if (err) *err = "replicate count changed"; return -6; }
+  // the virtual boxes stay; the pair search looks one box deep, so a new
+  // binding radius must still fit in a box
+  for (size_t k = 0; k < reps.size(); ++k)
+    for (int r = 0; r < E.net.nrxn[2]; ++r) {
+      const double a = std::sqrt(std::max(0.0, reps[k].bind2[r]));
+      for (int d = 0; d < reps[k].dim; ++d)
+        if (a > E.geo[k].h[d]) {
+          if (err) *err = "binding radius exceeds the virtual box size; rebuild the simulation";
+          return -6;
+        }
+    }
   E.reps = reps;
   return E.build_rep_tables(err);
 }
