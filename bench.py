@@ -47,8 +47,10 @@ DT = 0.01
 # and write 16 B in box order in the fused move/rebin pass, read 16 B again in
 # the pair search
 ALG_BYTES_PER_MOLSTEP = 48
-# per-kernel algorithmic bytes per molecule
-KERNEL_BYTES = {"k_advance_count": 16, "k_advance_scatter": 32, "k_pairs": 16}
+# per-kernel share of those algorithmic bytes per molecule: the move pass
+# reads each molecule, the scatter writes it in box order, the pair search
+# reads it again
+KERNEL_BYTES = {"k_move": 16, "k_scatter": 16, "k_pairs": 16}
 
 
 def peaks():
@@ -76,10 +78,15 @@ class ClockSampler:
         if not shutil.which("nvidia-smi"):
             return
         self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
-                                      "--format=csv,noheader,nounits", "-lms", "100"],
+                                      "--format=csv,noheader,nounits", "-lms", "20"],
                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
+        # nvidia-smi needs a moment before its first sample; wait for it so the
+        # samples cover the timed region that follows
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < 5.0:
+            time.sleep(0.01)
 
     def _read(self):
         for ln in self.proc.stdout:
@@ -211,7 +218,7 @@ def workload_config(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--ref-sample", type=int, default=100000)
@@ -247,11 +254,11 @@ def main():
     s.update()
     stream = torch.cuda.Stream()
     s.set_stream(stream.cuda_stream)
+    clocks = ClockSampler(local)
+    clocks.start()
     s.run_steps(args.warmup)
     s.synchronize()
     n0 = s.total()
-    clocks = ClockSampler(local)
-    clocks.start()
     barrier()
     torch.cuda.synchronize()
     l0 = s.launches()
@@ -414,7 +421,7 @@ def run_surrogate(sb, torch, args, rank):
     rho = 1.5
     sur = sb.Surrogate()
     t0 = time.perf_counter()
-    loss, train_s = sur.train(nsamples=1_000_000, epochs=20, batch=1024, lr=2e-3, seed=12345)
+    loss, train_s = sur.train(nsamples=1_000_000, epochs=80, batch=512, lr=3e-3, seed=12345)
     t = ensemble_template(sb, placement=(sb.RPratio, rho))
     e = sb.Ensemble(t, R)
     e.set_boxes(np.zeros((R, 3)), np.repeat(side[:, None], 3, 1))

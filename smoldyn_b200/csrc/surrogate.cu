@@ -39,6 +39,17 @@ struct Norm {
 
 __device__ __forceinline__ float act(float z) { return tanhf(z); }
 
+// Analytic reference for the reduced radius a/s at reduced rate kappa: the
+// diffusion-limited radius kappa/(4 pi) (k = 4 pi D a) blended with the
+// activation-limited one (3 kappa/(8 pi))^(1/3) (k dt = 4/3 pi a^3 with
+// D dt / s^2 = 1/2).  The network fits the residual log10(a/s / approx),
+// a narrow, smooth target.
+__host__ __device__ __forceinline__ double log10_approx(double kappa) {
+  const double aD = kappa / (4.0 * 3.14159265358979323846);
+  const double aA = cbrt(3.0 * kappa / (8.0 * 3.14159265358979323846));
+  return log10(cbrt(aD * aD * aD + aA * aA * aA));
+}
+
 // Exact samples: x = (log10 kappa, rho, rev), y = (log10 a/s, b/s) in units
 // D = 1/2, dt = 1 (so s = 1 and k = kappa/2).  Non-finite solutions (rates a
 // ratio < 1 placement cannot reach) are flagged with y0 = NaN.
@@ -56,8 +67,9 @@ __global__ void k_sur_samples(long long n, uint64_t seed, double *x, double *y) 
     x[3 * i + 1] = rho;
     x[3 * i + 2] = rev ? 1.0 : 0.0;
     const bool ok = isfinite(a) && a > 0;
-    y[2 * i] = ok ? log10(a) : nan("");
-    y[2 * i + 1] = ok ? (rev ? rho * a : 0.0) : nan("");
+    const double la = log10_approx(pow(10.0, lk));
+    y[2 * i] = ok ? log10(a) - la : nan("");
+    y[2 * i + 1] = ok ? (rev ? rho * a / pow(10.0, la) : 0.0) : nan("");
   }
 }
 
@@ -262,11 +274,17 @@ __global__ void k_sur_pair_radii(const __nv_bfloat16 *wg, Norm nm, long long n, 
                             (float)(((ratio ? 1.0 : 0.0) - nm.xo[2]) * nm.xs[2])};
         float y[2];
         mlp_forward_bf16(w, x, y);
-        a = s * pow(10.0, (double)(y[0] * nm.ys[0] + nm.ym[0]));
-        // one evaluation of the tabulated rate at the prediction estimates
-        // the relative rate error (the quantity the radius controls)
-        const double est = rxnp::numrxnrate(s, a, ratio ? rparam * a : -1.0);
-        const double rel = fabs(est / (rate3 * dt) - 1.0);
+        a = s * pow(10.0, (double)(y[0] * nm.ys[0] + nm.ym[0]) + log10_approx(pow(10.0, lk)));
+        // Error estimate without iterating: the tabulated per-step rate at the
+        // prediction and at a 0.1% larger radius give the rate error and the
+        // local slope g = dln(rate)/dln(a); the radius error is about
+        // rate error / g.
+        const double b0 = ratio ? rparam : -1.0;
+        const double r0 = rxnp::numrxnrate(s, a, ratio ? b0 * a : -1.0);
+        const double a1 = a * 1.001;
+        const double r1 = rxnp::numrxnrate(s, a1, ratio ? b0 * a1 : -1.0);
+        const double g = log(r1 / r0) / log(1.001);
+        const double rel = fabs(r0 / (rate3 * dt) - 1.0) / fmax(g, 0.5);
         if (!(rel <= tol)) exact = true;
         else u = ratio ? rparam * a : 0.0;
       }

@@ -7,11 +7,16 @@
 // mutual diffusion coefficient) and on the unbinding parameter.  The surrogate
 // is a 3->64->64->2 tanh network on
 //   inputs  x = (log10 kappa, unbinding ratio rho in [0,2], reversible flag)
-//   outputs y = (log10 a/s, b/s)   with b = rho*a for ratio placement, 0 if irreversible
-// trained on samples of the exact FP64 solver generated on the GPU.  Inference
-// uses BF16 weights with FP32 accumulation, then evaluates numrxnrate once at
-// the predicted radius to estimate its relative error; above the tolerance
-// (default 1e-3) the exact solver runs for that instance instead.
+//   outputs y = (log10 (a/s)/A(kappa), (b/s)/A(kappa))
+// with b = rho*a for ratio placement (0 if irreversible) and A(kappa) the
+// analytic diffusion-/activation-limited radius (cbrt(aD^3 + aA^3), aD =
+// kappa/(4 pi), aA = (3 kappa/(8 pi))^(1/3)), so the network fits a narrow
+// residual.  It is trained on samples of the exact FP64 solver generated on
+// the GPU.  Inference uses BF16 weights with FP32 accumulation, then
+// evaluates numrxnrate at the predicted radius and at a 0.1% larger one: the
+// rate error divided by the local slope dln(rate)/dln(a) estimates the
+// radius error; above the tolerance (default 1e-3) the exact solver runs for
+// that instance instead.
 #pragma once
 
 #include <cstdint>
