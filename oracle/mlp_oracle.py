@@ -5,11 +5,12 @@ TEST INFRASTRUCTURE ONLY: the checker for the GPU training kernels
 layout and input normalisation as the device code:
   W1[64][3] b1[64] W2[64][64] b2[64] W3[2][64] b3[2]
   xn = (x - XO) * XS, h1 = tanh(W1 xn + b1), h2 = tanh(W2 h1 + b2), y = W3 h2 + b3
-  loss = mean over samples of sum over the two outputs of (y - t)^2
+  loss = mean over samples of sum over the two outputs of LOSS_W[o] (y - t)^2
 """
 import numpy as np
 
 NIN, NHID, NOUT = 3, 64, 2
+LOSS_W = np.array([1.0, 0.1])
 LK_LO, LK_HI, RHO_HI = -5.5, 3.1, 2.0
 XO = np.array([0.5 * (LK_LO + LK_HI), 0.5 * RHO_HI, 0.5])
 XS = np.array([2.0 / (LK_HI - LK_LO), 2.0 / RHO_HI, 2.0])
@@ -48,8 +49,8 @@ def loss_grad(p, x, t):
     h2 = np.tanh(z2)
     y = h2 @ W3.T + b3
     e = y - np.asarray(t, dtype=np.float64)
-    loss = (e * e).sum() / n
-    d3 = 2.0 * e / n
+    loss = (LOSS_W * e * e).sum() / n
+    d3 = 2.0 * LOSS_W * e / n
     gW3 = d3.T @ h2
     gb3 = d3.sum(0)
     dz2 = (d3 @ W3) * (1 - h2 * h2)

@@ -74,10 +74,16 @@ __global__ void k_sur_samples(long long n, uint64_t seed, double *x, double *y) 
 }
 
 constexpr int kTile = 128;  // samples per block tile in training
+// Loss weight of each output.  Inference only uses output 0 (the binding
+// radius; ratio placement fixes the unbinding radius as rho times it), so the
+// second output is fitted with a tenth of the weight.
+__constant__ float c_lossw[kMlpOut] = {1.0f, 0.1f};
 
-// Forward + backward over one mini-batch; parameter gradients of the mean
-// squared error are accumulated into grad (zeroed by the caller), the summed
-// loss into loss.  Block: 256 threads, one tile of 128 samples at a time;
+// Forward + backward over one mini-batch; parameter gradients of the weighted
+// mean squared error are accumulated into grad (zeroed by the caller), the
+// summed loss into loss.  w is the parameter set the forward pass uses: the
+// FP32 master copy, or in quantisation-aware steps its BF16-rounded copy (the
+// gradient then updates the master copy: straight-through estimate).  Block: 256 threads, one tile of 128 samples at a time;
 // thread t works on sample t/2, half t%2 of the 64 hidden units.
 __global__ void __launch_bounds__(256) k_mlp_grad(const float *__restrict__ w, int n, const float *xn,
                                                   const float *tn, float *grad, float *loss, float inv_n) {
@@ -119,8 +125,8 @@ __global__ void __launch_bounds__(256) k_mlp_grad(const float *__restrict__ w, i
       float z = w[kMlpB3 + o];
       for (int c = 0; c < kMlpHid; ++c) z += w[kMlpW3 + o * kMlpHid + c] * H2[smp * kMlpHid + c];
       const float e = valid ? (z - tn[i * kMlpOut + o]) : 0.f;
-      lsum += e * e;
-      D3[smp * kMlpOut + o] = 2.f * e * inv_n;
+      lsum += c_lossw[o] * e * e;
+      D3[smp * kMlpOut + o] = 2.f * c_lossw[o] * e * inv_n;
     }
     __syncthreads();
     // dW3, db3 (block partials)
@@ -190,16 +196,16 @@ __global__ void __launch_bounds__(256) k_mlp_grad(const float *__restrict__ w, i
   if ((threadIdx.x & 31) == 0) atomicAdd(loss, lsum * inv_n);
 }
 
-// Adam step (Kingma & Ba 2015) with bias correction; also refreshes the BF16
-// copy used for inference.
-__global__ void k_adam(float *w, float *m, float *v, float *g, __nv_bfloat16 *wb, int np, float lr, float b1,
+// Adam step (Kingma & Ba 2015) with bias correction; also refreshes the
+// BF16-rounded copy (as FP32 values) that quantisation-aware steps run on.
+__global__ void k_adam(float *w, float *m, float *v, float *g, float *wq, int np, float lr, float b1,
                        float b2, float eps, float c1, float c2) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
     const float gk = g[k];
     m[k] = b1 * m[k] + (1.f - b1) * gk;
     v[k] = b2 * v[k] + (1.f - b2) * gk * gk;
     w[k] -= lr * (m[k] / c1) / (sqrtf(v[k] / c2) + eps);
-    wb[k] = __float2bfloat16(w[k]);
+    wq[k] = __bfloat162float(__float2bfloat16(w[k]));
     g[k] = 0.f;
   }
 }
@@ -452,11 +458,9 @@ int Surrogate::train(long long nsamples, int epochs, int batch, double lr, uint6
   normalise(nm, n, xs.data(), ys.data(), &xn, &tn);
   const size_t np = kMlpNParam;
   float *d = nullptr;
-  __nv_bfloat16 *wb = nullptr;
-  SCK(cudaMalloc(&d, (np * 4 + 1 + 5 * (size_t)n) * sizeof(float)));
-  SCK(cudaMalloc(&wb, np * sizeof(__nv_bfloat16)));
-  float *dw = d, *dm = d + np, *dv = d + 2 * np, *dg = d + 3 * np, *dl = d + 4 * np, *dx = dl + 1,
-        *dtn = dx + 3 * (size_t)n;
+  SCK(cudaMalloc(&d, (np * 5 + 1 + 5 * (size_t)n) * sizeof(float)));
+  float *dw = d, *dm = d + np, *dv = d + 2 * np, *dg = d + 3 * np, *dwq = d + 4 * np, *dl = d + 5 * np,
+        *dx = dl + 1, *dtn = dx + 3 * (size_t)n;
   SCK(cudaMemcpy(dw, impl_->w.data(), np * sizeof(float), cudaMemcpyHostToDevice));
   SCK(cudaMemset(dm, 0, np * 3 * sizeof(float)));
   SCK(cudaMemcpy(dx, xn.data(), 3 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice));
@@ -466,33 +470,45 @@ int Surrogate::train(long long nsamples, int epochs, int batch, double lr, uint6
   const int bs = std::max(kTile, batch - batch % kTile);
   const long long nb = n / bs;
   const int blocks = bs / kTile;
+  // Two phases, each with its own cosine learning-rate decay: FP32 training
+  // over the first 4/5 of the epochs, then quantisation-aware steps (forward
+  // and backward on the BF16-rounded weights inference uses) at a tenth of
+  // the learning rate, which recovers most of the accuracy BF16 rounding
+  // costs.
+  const int qat_epochs = epochs >= 5 ? epochs / 5 : 0;
+  const int phase_epochs[2] = {epochs - qat_epochs, qat_epochs};
+  const double phase_lr[2] = {lr, 0.1 * lr};
   long long it = 0;
-  const long long total = (long long)epochs * nb;
-  for (int ep = 0; ep < epochs; ++ep) {
-    for (long long b = 0; b < nb; ++b, ++it) {
-      // cosine decay of the learning rate
-      const double frac = (double)it / std::max<long long>(1, total);
-      const float lrt = (float)(lr * 0.5 * (1.0 + std::cos(3.141592653589793 * frac)) + lr * 1e-3);
-      SCK(cudaMemsetAsync(dl, 0, sizeof(float)));
-      // the samples are in random order already; batches sweep them with an epoch offset
-      const long long off = ((b + (long long)ep * 7919) % nb) * bs;
-      k_mlp_grad<<<blocks, 256, smem>>>(dw, bs, dx + 3 * off, dtn + 2 * off, dg, dl, 1.0f / (float)bs);
-      const float c1 = 1.f - (float)std::pow(0.9, (double)(it + 1));
-      const float c2 = 1.f - (float)std::pow(0.999, (double)(it + 1));
-      k_adam<<<(int)((np + 255) / 256), 256>>>(dw, dm, dv, dg, wb, (int)np, lrt, 0.9f, 0.999f, 1e-8f, c1, c2);
+  SCK(cudaMemcpy(dwq, dw, np * sizeof(float), cudaMemcpyDeviceToDevice));
+  for (int ph = 0; ph < 2; ++ph) {
+    const long long total = (long long)phase_epochs[ph] * nb;
+    const float *wfwd = ph == 0 ? dw : dwq;
+    long long pit = 0;
+    for (int ep = 0; ep < phase_epochs[ph]; ++ep) {
+      for (long long b = 0; b < nb; ++b, ++it, ++pit) {
+        const double frac = (double)pit / std::max<long long>(1, total);
+        const double lr0 = phase_lr[ph];
+        const float lrt = (float)(lr0 * 0.5 * (1.0 + std::cos(3.141592653589793 * frac)) + lr0 * 1e-3);
+        SCK(cudaMemsetAsync(dl, 0, sizeof(float)));
+        // the samples are in random order already; batches sweep them with an epoch offset
+        const long long off = ((b + (long long)(ep + ph * phase_epochs[0]) * 7919) % nb) * bs;
+        k_mlp_grad<<<blocks, 256, smem>>>(wfwd, bs, dx + 3 * off, dtn + 2 * off, dg, dl, 1.0f / (float)bs);
+        const float c1 = 1.f - (float)std::pow(0.9, (double)(it + 1));
+        const float c2 = 1.f - (float)std::pow(0.999, (double)(it + 1));
+        k_adam<<<(int)((np + 255) / 256), 256>>>(dw, dm, dv, dg, dwq, (int)np, lrt, 0.9f, 0.999f, 1e-8f, c1, c2);
+      }
     }
   }
   SCK(cudaGetLastError());
-  // final loss over the first batches
+  // final loss over the first batches, on the BF16-rounded weights inference uses
   float l = 0;
   SCK(cudaMemset(dl, 0, sizeof(float)));
   SCK(cudaMemset(dg, 0, np * sizeof(float)));
   const long long ne = std::min<long long>(n, 65536) / kTile * kTile;
-  k_mlp_grad<<<std::max(1, (int)(ne / kTile)), 256, smem>>>(dw, (int)ne, dx, dtn, dg, dl, 1.0f / (float)ne);
+  k_mlp_grad<<<std::max(1, (int)(ne / kTile)), 256, smem>>>(dwq, (int)ne, dx, dtn, dg, dl, 1.0f / (float)ne);
   SCK(cudaMemcpy(&l, dl, sizeof(float), cudaMemcpyDeviceToHost));
   SCK(cudaMemcpy(impl_->w.data(), dw, np * sizeof(float), cudaMemcpyDeviceToHost));
   cudaFree(d);
-  cudaFree(wb);
   impl_->trained = true;
   if (st) {
     st->final_loss = l;

@@ -12,7 +12,9 @@
 // analytic diffusion-/activation-limited radius (cbrt(aD^3 + aA^3), aD =
 // kappa/(4 pi), aA = (3 kappa/(8 pi))^(1/3)), so the network fits a narrow
 // residual.  It is trained on samples of the exact FP64 solver generated on
-// the GPU.  Inference uses BF16 weights with FP32 accumulation, then
+// the GPU, the last fifth of the epochs quantisation-aware (forward and
+// backward on BF16-rounded weights).  Inference uses BF16 weights with FP32
+// accumulation, then
 // evaluates numrxnrate at the predicted radius and at a 0.1% larger one: the
 // rate error divided by the local slope dln(rate)/dln(a) estimates the
 // radius error; above the tolerance (default 1e-3) the exact solver runs for

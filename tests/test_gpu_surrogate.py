@@ -6,8 +6,9 @@
   restatement (oracle/mlp_oracle.py) to FP32 tolerance (1e-4 relative).
 - Training on 10^6 exact samples reaches a loss well below the untrained one;
   surrogate radii with the fallback rule give rate constants within 1% of the
-  exact solver's (the tabulated rate at the predicted radius), and without
-  fallback most instances are accepted.
+  exact solver's (the tabulated rate at the predicted radius), and most
+  instances are accepted without fallback (BF16 weights after
+  quantisation-aware training).
 """
 import os
 import sys
@@ -93,7 +94,8 @@ def test_surrogate_rate_error_and_fallback(trained):
     assert np.median(rel_rad) < 1e-3
     assert rel_rad.max() < 2e-2
     frac_fb = nfb / n
-    assert frac_fb < 0.9, frac_fb
+    print("surrogate fallback fraction %.3f, median radius error %.2e" % (frac_fb, np.median(rel_rad)))
+    assert frac_fb < 0.5, frac_fb
     # with the fallback rule every accepted radius has rate error <= 1e-3
     ref = oracle_lib.reference_rxnparam()
     if ref is not None:
