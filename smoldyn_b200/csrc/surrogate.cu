@@ -281,16 +281,20 @@ __global__ void k_sur_pair_radii(const __nv_bfloat16 *wg, Norm nm, long long n, 
         float y[2];
         mlp_forward_bf16(w, x, y);
         a = s * pow(10.0, (double)(y[0] * nm.ys[0] + nm.ym[0]) + log10_approx(pow(10.0, lk)));
-        // Error estimate without iterating: the tabulated per-step rate at the
-        // prediction and at a 0.1% larger radius give the rate error and the
-        // local slope g = dln(rate)/dln(a); the radius error is about
-        // rate error / g.
+        // The tabulated per-step rate at the prediction and at a 0.1% larger
+        // radius give the rate error and the local slope
+        // g = dln(rate)/dln(a).  One secant step a *= (target/rate)^(1/g)
+        // corrects the prediction; a third evaluation at the corrected radius
+        // estimates its radius error as rate error / g.
+        const double target = rate3 * dt;
         const double b0 = ratio ? rparam : -1.0;
         const double r0 = rxnp::numrxnrate(s, a, ratio ? b0 * a : -1.0);
         const double a1 = a * 1.001;
         const double r1 = rxnp::numrxnrate(s, a1, ratio ? b0 * a1 : -1.0);
         const double g = log(r1 / r0) / log(1.001);
-        const double rel = fabs(r0 / (rate3 * dt) - 1.0) / fmax(g, 0.5);
+        if (g > 0.1 && r0 > 0) a *= pow(target / r0, 1.0 / g);
+        const double rc = rxnp::numrxnrate(s, a, ratio ? b0 * a : -1.0);
+        const double rel = fabs(rc / target - 1.0) / fmax(g, 0.5);
         if (!(rel <= tol)) exact = true;
         else u = ratio ? rparam * a : 0.0;
       }

@@ -1,0 +1,96 @@
+"""Generate the one-step golden fixtures from the reference engine itself.
+
+Runs oracle/_ref/ref_harness (the reference's libsmoldyn compiled from its
+sources, with its diffuse and unireact wrapped to record displacements and
+first-order outcomes) on the configurations below and writes
+tests/golden/<name>.npz with:
+  pos0, sp0, serno0   state at the start of the step (reference's own initial
+                      placement from its config, seed fixed)
+  disp                the reference's displacement of each molecule this step
+  uni                 1 where the reference's first-order reaction fired
+  bind2               squared binding radius of A + B -> C (reference value)
+  pos1, sp1, serno1   the reference's state after the step
+  L, wall, kf, kr     cube side, boundary type, rate constants
+Usage: python tests/golden/make_golden.py   (needs `make -C oracle ref`)
+"""
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+
+# A + B <-> C with the reverse products at the reaction site (irrev placement:
+# zero unbinding radius), so a step has no random product orientation.
+CONFIG = """dim 3
+species A B C
+difc A 1
+difc B 1
+difc C 0.5
+time_start 0
+time_stop 1
+time_step 0.01
+boundaries 0 0 {L} {w}
+boundaries 1 0 {L} {w}
+boundaries 2 0 {L} {w}
+random_seed {seed}
+reaction fwd A + B -> C {kf}
+reaction rev C -> A + B {kr}
+product_placement rev irrev
+mol {nA} A u u u
+mol {nB} B u u u
+mol {nC} C u u u
+end_file
+"""
+
+CASES = {
+    "onestep_reflect": dict(L=20, w="r", seed=11, kf=20, kr=1, nA=1600, nB=1600, nC=800),
+    "onestep_periodic": dict(L=20, w="p", seed=12, kf=20, kr=1, nA=1600, nB=1600, nC=800),
+    "onestep_sparse": dict(L=20, w="p", seed=13, kf=1, kr=1, nA=1600, nB=1600, nC=800),
+}
+SPECIES = {1: "A", 2: "B", 3: "C"}
+
+
+def run_case(name, cfg):
+    with tempfile.TemporaryDirectory() as tmp:
+        with open(os.path.join(tmp, "cfg.txt"), "w") as f:
+            f.write(CONFIG.format(**cfg))
+        out = os.path.join(tmp, "out.txt")
+        subprocess.run([HARNESS, tmp + "/", "cfg.txt", out], check=True, stdin=subprocess.DEVNULL,
+                       stdout=subprocess.DEVNULL)
+        D, U, F, B = [], [], [], {}
+        for line in open(out):
+            t = line.split()
+            if t[0] == "D":
+                D.append((int(t[1]), int(t[2]), *map(float, t[3:9])))
+            elif t[0] == "U":
+                U.append(int(t[1]))
+            elif t[0] == "F":
+                F.append((int(t[1]), int(t[2]), *map(float, t[3:6])))
+            elif t[0] == "B":
+                B[int(t[1])] = float(t[2])
+    D.sort()
+    F.sort()
+    serno0 = np.array([d[0] for d in D], dtype=np.uint64)
+    uset = set(U)
+    np.savez_compressed(
+        os.path.join(HERE, name + ".npz"),
+        pos0=np.array([d[2:5] for d in D]), sp0=np.array([d[1] for d in D], dtype=np.int32), serno0=serno0,
+        disp=np.array([d[5:8] for d in D]),
+        uni=np.array([1 if int(s) in uset else 0 for s in serno0], dtype=np.int32),
+        bind2=np.float64(B[0]),
+        pos1=np.array([f[2:5] for f in F]), sp1=np.array([f[1] for f in F], dtype=np.int32),
+        serno1=np.array([f[0] for f in F], dtype=np.uint64),
+        L=np.float64(cfg["L"]), wall=np.array(cfg["w"]), kf=np.float64(cfg["kf"]), kr=np.float64(cfg["kr"]))
+    print(name, "molecules", len(D), "->", len(F), "first-order", len(U))
+
+
+if __name__ == "__main__":
+    if not os.path.exists(HARNESS):
+        sys.exit("build the reference first: make -C oracle ref")
+    for k, v in CASES.items():
+        run_case(k, v)

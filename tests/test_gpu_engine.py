@@ -194,3 +194,24 @@ def test_device_radius_solver_matches_reference():
     ok = ue > 0
     assert (np.abs(uo[ok] - ue[ok]) / ue[ok]).max() < 1e-9
     assert np.array_equal(uo[~ok] <= 0, ue[~ok] <= 0)
+
+
+@pytest.mark.parametrize("name", ["onestep_reflect", "onestep_periodic", "onestep_sparse"])
+def test_deterministic_step_matches_reference_recording(name):
+    """One step against the reference engine's own recorded step
+    (tests/golden, made by oracle/ref_harness.c): the reference's start state,
+    displacements and first-order outcomes go in through the injection mode;
+    the result must equal the reference's state after the step (positions to
+    1e-5 of the box side, FP32 box-local storage)."""
+    from tests import golden_cases as gd
+    g = gd.load(name)
+    s = gc.make_sim(L=g["L"], wall=g["wall"], kf=g["kf"], kr=g["kr"], difc=gd.DIFC, dt=gd.DT,
+                    rev_placement=(sb.RPirrev, 0.0))
+    s.set_molecules(g["pos0"], g["sp0"], g["serno0"])
+    force = np.where(g["uni"] == 1, 0, -1).astype(np.float64)
+    s.inject(g["serno0"], np.concatenate([g["disp"], force[:, None]], axis=1))
+    s.run_steps(1)
+    gpos, gsp, gsn = s.molecules()
+    act = dict(pos=gpos, sp=gsp, serno=gsn, orig=gsn < (1 << 41))
+    ncommon, nprod, nties = gd.compare(g, gd.reference_state(g), act, 1e-5)
+    assert ncommon > 2500 and nprod >= 10
