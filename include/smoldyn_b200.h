@@ -178,6 +178,18 @@ enum ErrorCode smolgpuSynchronize(simptr sim);
  * Host arrays of length n. */
 enum ErrorCode smolgpuSolveRadii(int mode, long long n, const double *rate, double dt,
                                  const double *difc, const double *b, int rel, double *out);
+/* smolgpuSolveRadii without device allocation; no counterpart in the
+ * reference.  Inputs and outputs pass through a fixed 2 MiB scratch in static
+ * device memory, so callers that cannot allocate (a radius update issued
+ * while an ensemble steps on another stream, where cudaMalloc/cudaFree could
+ * synchronise the device; a process whose HBM is already full) can still
+ * solve.  At most 65536 problems per call (ECbounds above that).  The
+ * scratch is shared per device and keeps the last call's contents: calls
+ * that overlap on the GPU race and must be serialised by the caller.  The
+ * first call on a device sets up the scratch address; make it before any
+ * stream capture. */
+enum ErrorCode smolgpuSolveRadiiNoAlloc(int mode, long long n, const double *rate, double dt,
+                                        const double *difc, const double *b, int rel, double *out);
 /* Same solver on the host CPU (product path used by parameter updates). */
 double smolgpuBindingRadiusHost(double rate, double dt, double difc, double b, int rel);
 double smolgpuUnbindingRadiusHost(double pgem, double dt, double difc, double a);

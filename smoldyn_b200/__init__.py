@@ -90,6 +90,7 @@ PROTOTYPES = {
     "smolgpuRunSteps": (C.c_int, [_sim, C.c_longlong]),
     "smolgpuProfileSteps": (C.c_int, [_sim, C.c_longlong, _ip, C.c_char_p, _dp, C.POINTER(C.c_longlong)]),
     "smolgpuSolveRadii": (C.c_int, [C.c_int, C.c_longlong, _dp, C.c_double, _dp, _dp, C.c_int, _dp]),
+    "smolgpuSolveRadiiNoAlloc": (C.c_int, [C.c_int, C.c_longlong, _dp, C.c_double, _dp, _dp, C.c_int, _dp]),
     "smolgpuBindingRadiusHost": (C.c_double, [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int]),
     "smolgpuUnbindingRadiusHost": (C.c_double, [C.c_double, C.c_double, C.c_double, C.c_double]),
     "smolgpuNewEnsemble": (_vp, [_sim, C.c_int]),
@@ -472,4 +473,17 @@ def solve_radii_device(mode, rate, dt, difc, b, rel=0):
     b = np.ascontiguousarray(b, dtype=np.float64)
     out = np.zeros_like(rate)
     check(lib.smolgpuSolveRadii(mode, len(rate), dptr(rate), dt, dptr(difc), dptr(b), rel, dptr(out)))
+    return out
+
+
+def solve_radii_device_noalloc(mode, rate, dt, difc, b, rel=0):
+    """smolgpuSolveRadiiNoAlloc: the same solve for callers that cannot
+    allocate device memory, through a fixed device scratch (at most 65536
+    problems per call; calls must not overlap on the GPU)."""
+    lib = load()
+    rate = np.ascontiguousarray(rate, dtype=np.float64)
+    difc = np.ascontiguousarray(difc, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    out = np.zeros_like(rate)
+    check(lib.smolgpuSolveRadiiNoAlloc(mode, len(rate), dptr(rate), dt, dptr(difc), dptr(b), rel, dptr(out)))
     return out
