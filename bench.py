@@ -53,6 +53,19 @@ ALG_BYTES_PER_MOLSTEP = 48
 KERNEL_BYTES = {"k_move": 16, "k_scatter": 16, "k_pairs": 16}
 
 
+def measured_traffic():
+    """DRAM bytes per molecule per launch from the committed ncu capture
+    (profiles/traffic_per_molecule.txt), or {} if absent."""
+    out = {}
+    path = os.path.join(ROOT, "profiles", "traffic_per_molecule.txt")
+    if os.path.exists(path):
+        for line in open(path):
+            t = line.split()
+            if len(t) == 2 and not t[0].startswith("#"):
+                out[t[0]] = float(t[1])
+    return out
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -209,9 +222,11 @@ def run_reference_arm(args, rank, world):
 
 
 def workload_config(args):
-    return {"workload": "scale-up: periodic cube 1000, 1e7 molecules (45% A, 45% B, 10% C), A+B->C 0.05, "
-                        "C->A+B 0.1, 0->A 1e-4, D=1,1,0.5, dt=0.01",
-            "molecules": N_MOL, "box": L_SIDE, "dt": DT, "l2": "inputs larger than L2 (>=240 MB per buffer)",
+    n = getattr(args, "molecules", N_MOL)
+    side = L_SIDE * (n / N_MOL) ** (1.0 / 3.0)
+    return {"workload": "scale-up: periodic cube %g, %g molecules (45%% A, 45%% B, 10%% C), A+B->C 0.05, "
+                        "C->A+B 0.1, 0->A 1e-4, D=1,1,0.5, dt=0.01" % (side, n),
+            "molecules": n, "box": side, "dt": DT, "l2": "inputs larger than L2 (>=240 MB per buffer)",
             "parallelism": "replicas" if args.gpus > 1 else "single"}
 
 
@@ -222,9 +237,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--ref-sample", type=int, default=100000)
+    ap.add_argument("--molecules", type=int, default=N_MOL,
+                    help="molecules of the plain workload at its density (smaller only for profiler captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-batched", action="store_true", help="skip the ensemble and surrogate workloads")
+    ap.add_argument("--no-tune", action="store_true", help="default launch shape and box width (no autotuner)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -250,8 +268,13 @@ def main():
             dist.barrier()
 
     # ---- device-resident throughput
-    s = build_sim(sb, N_MOL, L_SIDE, 1 + rank)
+    n_mol = args.molecules
+    s = build_sim(sb, n_mol, L_SIDE * (n_mol / N_MOL) ** (1.0 / 3.0), 1 + rank)
     s.update()
+    t_tune = time.perf_counter()
+    tune_ms = s.autotune(20) if not args.no_tune else None
+    t_tune = time.perf_counter() - t_tune
+    tuning = s.tuning()
     stream = torch.cuda.Stream()
     s.set_stream(stream.cuda_stream)
     clocks = ClockSampler(local)
@@ -298,7 +321,10 @@ def main():
         bytes_launch = KERNEL_BYTES[top[0]] * nmol_avg
         achieved = bytes_launch / (per_launch_ms / 1e3) / 1e9
         roof = {"bound": "hbm", "kernel": top[0], "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
+                "frac": achieved / hbm, "peak_kind": peak_kind,
+                "traffic": (measured_traffic()[top[0]] * nmol_avg if top[0] in measured_traffic() else None),
+                "traffic_note": "bytes per launch: ncu DRAM read+write per molecule (4e6-molecule capture, "
+                                "profiles/traffic_per_molecule.txt) x molecules of this run",
                 "alg_bytes_per_molecule": KERNEL_BYTES[top[0]]}
     step_frac = (ALG_BYTES_PER_MOLSTEP * value / (world if world > 1 else 1)) / (hbm * 1e9)
     kernels = {k: {"ms_per_step": v[0] / nprof, "share": v[0] / tot_ms} for k, v in prof.items()}
@@ -333,7 +359,8 @@ def main():
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_s * 1e3 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": workload_config(args), "e2e": e2e, "gpu_launches": int(launches),
+            "config": dict(workload_config(args), tuning=tuning, autotune_s=t_tune, autotune_best_trial_ms=tune_ms),
+            "e2e": e2e, "gpu_launches": int(launches),
             "roofline": roof, "step_roofline_frac": step_frac, "kernels": kernels, "cpu_baseline": cpu,
             "clocks": ck, "batched": batched, "batched_surrogate": surrogate,
         }
@@ -393,6 +420,9 @@ def run_batched(sb, torch, args, rank):
     e.radius_mode(1)
     t0 = time.perf_counter()
     e.update()
+    t_tune = time.perf_counter()
+    tune_ms = e.autotune(10) if not args.no_tune else None
+    t_tune = time.perf_counter() - t_tune
     setup = time.perf_counter() - t0
     stream = torch.cuda.Stream()
     e.set_stream(stream.cuda_stream)
@@ -404,7 +434,8 @@ def run_batched(sb, torch, args, rank):
     out = {"workload": "4096 replicates, N log-uniform [1e2,1e5] at density 0.01, kf,kr log-uniform [1e-3,1], "
                        "reflective cubes, A+B<->C, dt=0.01, radii by the device FP64 solver",
            "value": tot * steps / sec, "unit": METRIC, "molecules": int(tot), "replicates": R, "steps": steps,
-           "ms_per_step": sec * 1e3 / steps, "setup_s": setup, "gpu_launches": int(e.launches() - l0)}
+           "ms_per_step": sec * 1e3 / steps, "setup_s": setup, "gpu_launches": int(e.launches() - l0),
+           "tuning": e.tuning(), "autotune_s": t_tune, "autotune_best_trial_ms": tune_ms}
     e.close()
     return out
 
@@ -503,6 +534,8 @@ def run_e2e(sb, args, rank, world, dist, barrier):
     pos = np.ascontiguousarray(pos)
     sp = np.ascontiguousarray(sp)
     s2.update()
+    if not args.no_tune:
+        s2.autotune(20)
     s2.run_steps(args.warmup)
     s2.synchronize()
     barrier()

@@ -171,6 +171,18 @@ enum ErrorCode smolgpuProfileSteps(simptr sim, long long nsteps, int *nkernels, 
                                    long long *launches);
 /* Synchronise the engine's stream. */
 enum ErrorCode smolgpuSynchronize(simptr sim);
+/* Autotuner (no reference counterpart: the reference's box size comes from
+ * molperbox/boxsize, smolboxes.c:717-749).  Runs timed trial steps from the
+ * current state over box widths (1, 2, 4, 8 molecules per box, only when the
+ * configuration sets neither molperbox nor boxsize), pair-search tile size and
+ * blocks per SM, and streaming-kernel blocks per SM; keeps the fastest and
+ * restores the molecules and step counter, so the trajectory is the untuned
+ * one up to FP32 rounding of box-local coordinates.  Call after smolUpdateSim
+ * and before the first time step.  *ms_per_step (optional) = best trial. */
+enum ErrorCode smolgpuAutotune(simptr sim, int trial_steps, double *ms_per_step);
+/* The current choice (molperbox -1 when boxsize is set). */
+enum ErrorCode smolgpuGetTuning(simptr sim, double *molperbox, int *pair_tile, int *tile_blocks_per_sm,
+                                int *mol_blocks_per_sm);
 
 /* FP64 radius solver, batched on the device (rxnparam.c:558-716 on the GPU).
  * mode 0: bindingradius(rate[i], dt, difc[i], b[i], rel) -> out[i]
@@ -219,6 +231,11 @@ long long smolgpuEnsembleGetFallbackCount(ensptr ens);
 enum ErrorCode smolgpuEnsembleSetStream(ensptr ens, void *stream);
 long long smolgpuEnsembleGetLaunchCount(ensptr ens);
 enum ErrorCode smolgpuEnsembleSynchronize(ensptr ens);
+/* Autotuner for an ensemble (same search as smolgpuAutotune; box width per
+ * replicate from its own molecule count). */
+enum ErrorCode smolgpuEnsembleAutotune(ensptr ens, int trial_steps, double *ms_per_step);
+enum ErrorCode smolgpuEnsembleGetTuning(ensptr ens, double *molperbox, int *pair_tile, int *tile_blocks_per_sm,
+                                        int *mol_blocks_per_sm);
 enum ErrorCode smolgpuEnsembleFree(ensptr ens);
 
 /* ==== Part 2c: MLP surrogate of the radius solve ========================= */

@@ -87,6 +87,8 @@ PROTOTYPES = {
     "smolgpuSetStream": (C.c_int, [_sim, _vp]),
     "smolgpuGetLaunchCount": (C.c_longlong, [_sim]),
     "smolgpuSynchronize": (C.c_int, [_sim]),
+    "smolgpuAutotune": (C.c_int, [_sim, C.c_int, _dp]),
+    "smolgpuGetTuning": (C.c_int, [_sim, _dp, _ip, _ip, _ip]),
     "smolgpuRunSteps": (C.c_int, [_sim, C.c_longlong]),
     "smolgpuProfileSteps": (C.c_int, [_sim, C.c_longlong, _ip, C.c_char_p, _dp, C.POINTER(C.c_longlong)]),
     "smolgpuSolveRadii": (C.c_int, [C.c_int, C.c_longlong, _dp, C.c_double, _dp, _dp, C.c_int, _dp]),
@@ -107,6 +109,8 @@ PROTOTYPES = {
     "smolgpuEnsembleSetStream": (C.c_int, [_vp, _vp]),
     "smolgpuEnsembleGetLaunchCount": (C.c_longlong, [_vp]),
     "smolgpuEnsembleSynchronize": (C.c_int, [_vp]),
+    "smolgpuEnsembleAutotune": (C.c_int, [_vp, C.c_int, _dp]),
+    "smolgpuEnsembleGetTuning": (C.c_int, [_vp, _dp, _ip, _ip, _ip]),
     "smolgpuEnsembleFree": (C.c_int, [_vp]),
     "smolgpuSurrogateNew": (_vp, []),
     "smolgpuSurrogateFree": (C.c_int, [_vp]),
@@ -159,6 +163,14 @@ def check(code):
         c, fn, msg = last_error()
         raise RuntimeError("libsmoldyn_b200 error %d in %s: %s" % (code, fn, msg))
     return code
+
+
+def _get_tuning(fn, ptr):
+    mpb = C.c_double()
+    tile, tb, mb = C.c_int(), C.c_int(), C.c_int()
+    check(fn(ptr, C.byref(mpb), C.byref(tile), C.byref(tb), C.byref(mb)))
+    return {"molperbox": mpb.value, "pair_tile": tile.value, "tile_blocks_per_sm": tb.value,
+            "mol_blocks_per_sm": mb.value}
 
 
 class Sim:
@@ -261,6 +273,16 @@ class Sim:
 
     def synchronize(self):
         return check(self.lib.smolgpuSynchronize(self.ptr))
+
+    def autotune(self, trial_steps=20):
+        """Pick box width and kernel launch shape by timed trials (before the
+        first step); returns the best trial's ms per step."""
+        ms = C.c_double()
+        check(self.lib.smolgpuAutotune(self.ptr, int(trial_steps), C.byref(ms)))
+        return ms.value
+
+    def tuning(self):
+        return _get_tuning(self.lib.smolgpuGetTuning, self.ptr)
 
     def launches(self):
         return self.lib.smolgpuGetLaunchCount(self.ptr)
@@ -393,6 +415,14 @@ class Ensemble:
 
     def synchronize(self):
         return check(self.lib.smolgpuEnsembleSynchronize(self.ptr))
+
+    def autotune(self, trial_steps=20):
+        ms = C.c_double()
+        check(self.lib.smolgpuEnsembleAutotune(self.ptr, int(trial_steps), C.byref(ms)))
+        return ms.value
+
+    def tuning(self):
+        return _get_tuning(self.lib.smolgpuEnsembleGetTuning, self.ptr)
 
     def launches(self):
         return self.lib.smolgpuEnsembleGetLaunchCount(self.ptr)

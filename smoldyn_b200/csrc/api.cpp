@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../include/smoldyn_b200.h"
+#include "autotune.h"
 #include "engine.h"
 #include "rxnparam.cuh"
 #include "sim.h"
@@ -82,6 +83,7 @@ ErrorCode update_sim(Sim &s, const char *func) {
     long long cap = s.max_mol > 0 ? s.max_mol : std::max<long long>(2 * n + 4096, n + (1 << 20));
     if (!s.eng) s.eng.reset(new smolb::Engine());
     rc = s.eng->init(net, {rep}, s.dt, (uint64_t)s.seed, cap, &err);
+    if (!rc) rc = s.eng->set_tuning(s.tuning, &err);
     if (rc) { s.eng.reset(); return set_error(func, from_rc(rc), err); }
     rc = s.eng->set_molecules(n, s.pend_pos.data(), s.pend_sp.data(), nullptr, nullptr, &err);
     if (rc) { s.eng.reset(); return set_error(func, from_rc(rc), err); }
@@ -728,6 +730,59 @@ enum ErrorCode smolgpuSetStream(simptr sim, void *stream) {
   ErrorCode ec = update_sim(sim->s, __func__);
   if (ec != ECok) return ec;
   sim->s.eng->set_stream(stream);
+  return ECok;
+}
+
+enum ErrorCode smolgpuAutotune(simptr sim, int trial_steps, double *ms_per_step) {
+  LCHECK(sim, ECmissing, "missing sim");
+  LCHECK(trial_steps >= 2 && trial_steps <= 100000, ECbounds, "trial_steps must be 2..100000");
+  Sim &s = sim->s;
+  ErrorCode ec = update_sim(s, __func__);
+  if (ec != ECok) return ec;
+  LCHECK(s.steps == 0 && s.eng->steps_done() == 0, ECerror, "autotune runs before the first time step");
+  std::string err;
+  std::vector<double> pos;
+  std::vector<int> sp, rep;
+  std::vector<uint64_t> serno;
+  if (s.eng->get_molecules(&pos, &sp, &rep, &serno, &err)) return set_error(__func__, ECerror, err);
+  const bool box_free = s.molperbox <= 0 && s.boxsize <= 0;
+  smolb::TuneSetup ts;
+  if (box_free) ts.box_candidates = {1, 2, 4, 8};
+  ts.box_default = s.auto_molperbox > 0 ? s.auto_molperbox : 4;
+  ts.engine = [&]() { return s.eng.get(); };
+  ts.rebuild = [&](double mpb, std::string *e) -> int {
+    if (box_free) s.auto_molperbox = mpb;
+    smolb::NetSpec net;
+    smolb::RepSpec rs;
+    s.pend_sp = sp;  // the box grid follows the molecule count
+    int rc = smolb::build_engine_specs(s, &net, &rs, e);
+    s.pend_sp.clear();
+    if (rc) return rc;
+    const long long n = (long long)sp.size();
+    const long long cap = s.max_mol > 0 ? s.max_mol : std::max<long long>(2 * n + 4096, n + (1 << 20));
+    const smolb::LaunchTuning keep = s.eng->tuning();
+    rc = s.eng->init(net, {rs}, s.dt, (uint64_t)s.seed, cap, e);
+    if (!rc) rc = s.eng->set_tuning(keep, e);
+    if (!rc) rc = s.eng->set_molecules(n, pos.data(), sp.data(), nullptr, serno.data(), e);
+    return rc;
+  };
+  smolb::TuneResult tr;
+  if (smolb::autotune(ts, trial_steps, &tr, &err)) return set_error(__func__, ECerror, err);
+  s.tuning = tr.launch;
+  if (box_free) s.auto_molperbox = tr.molperbox;
+  if (g_debug) fprintf(stderr, "smolgpuAutotune trials (molperbox tile tileblocks molblocks ms):\n%s", tr.log.c_str());
+  if (ms_per_step) *ms_per_step = tr.ms_per_step;
+  return ECok;
+}
+
+enum ErrorCode smolgpuGetTuning(simptr sim, double *molperbox, int *pair_tile, int *tile_blocks_per_sm,
+                                int *mol_blocks_per_sm) {
+  LCHECK(sim, ECmissing, "missing sim");
+  const Sim &s = sim->s;
+  if (molperbox) *molperbox = s.molperbox > 0 ? s.molperbox : (s.boxsize > 0 ? -1 : (s.auto_molperbox > 0 ? s.auto_molperbox : 4));
+  if (pair_tile) *pair_tile = s.tuning.pair_tile;
+  if (tile_blocks_per_sm) *tile_blocks_per_sm = s.tuning.tile_blocks_per_sm;
+  if (mol_blocks_per_sm) *mol_blocks_per_sm = s.tuning.mol_blocks_per_sm;
   return ECok;
 }
 

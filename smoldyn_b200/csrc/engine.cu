@@ -66,7 +66,6 @@ struct KParams {
   int *cnt;
   int *start;
   int ncell;
-  int *blocksums;
   Event *ev;
   int *nev;
   int evcap;
@@ -88,7 +87,7 @@ struct KParams {
 
 constexpr uint32_t kTmpGone = 0xFFFFFFFFu;  // tmp[i].w of a molecule that left
 
-enum StatusBits { kStMolCap = 1, kStEvCap = 2, kStProdCap = 4, kStCandCap = 8 };
+enum StatusBits { kStMolCap = 1, kStEvCap = 2, kStProdCap = 4, kStCandCap = 8, kStScanWait = 16 };
 
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned m;
@@ -725,61 +724,93 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int *s_warp, int &tot
   return warp_excl + x - v;
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const int *cnt, int n, int *bsum) {
-  __shared__ int s_warp[32];
-  const int base = blockIdx.x * kScanTile;
-  int sum = 0;
-#pragma unroll
-  for (int k = 0; k < kScanItems; ++k) {
-    const int i = base + k * kScanThreads + threadIdx.x;
-    if (i < n) sum += cnt[i];
-  }
-  int total;
-  block_exclusive_scan(sum, s_warp, total);
-  if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+// Single-pass exclusive scan of the box counts (decoupled look-back, Merrill &
+// Garland 2016).  Tiles take ids from a 64-bit ticket counter in launch order,
+// so a tile only waits for tiles that are already running.  Each tile
+// publishes one 64-bit status word: epoch (30 bits) | kind (2 bits: 1 = tile
+// total, 2 = inclusive prefix) | value (32 bits).  The epoch is the launch
+// number, so words left by earlier launches read as "not yet published" and
+// the status array never needs clearing.  Every wait is bounded: after
+// kScanSpinLimit polls the tile records kStScanWait and proceeds.
+constexpr long long kScanSpinLimit = 1ll << 22;
+
+__device__ __forceinline__ ull scan_word(ull tag, int kind, int v) {
+  return tag | ((ull)kind << 32) | (uint32_t)v;
 }
 
-__global__ void __launch_bounds__(1024) k_scan_blocks(int *bsum, int nb) {
+__global__ void __launch_bounds__(kScanThreads) k_scan_lookback(const int *cnt, int n, int nb, ull *ticket,
+                                                                 ull *tile_status, int *start, int *n_out, int cap,
+                                                                 int *status) {
   __shared__ int s_warp[32];
-  __shared__ int s_carry;
-  if (threadIdx.x == 0) s_carry = 0;
+  __shared__ ull s_ticket;
+  __shared__ int s_prefix;
+  if (threadIdx.x == 0) s_ticket = atomicAdd(ticket, 1ull);
   __syncthreads();
-  for (int off = 0; off < nb; off += blockDim.x) {
-    const int i = off + threadIdx.x;
-    const int v = (i < nb) ? bsum[i] : 0;
-    int total;
-    const int ex = block_exclusive_scan(v, s_warp, total);
-    const int carry = s_carry;
-    if (i < nb) bsum[i] = carry + ex;
-    __syncthreads();
-    if (threadIdx.x == 0) s_carry = carry + total;
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) bsum[nb] = s_carry;
-}
-
-__global__ void __launch_bounds__(kScanThreads) k_scan_apply(const int *cnt, int n, const int *bsum,
-                                                              int nb, int *start, int *n_out, int cap) {
-  __shared__ int s_warp[32];
-  const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  const ull T = s_ticket;
+  const int tile = (int)(T % (ull)nb);
+  const ull tag = (((T / (ull)nb) + 1ull) & 0x3FFFFFFFull) << 34;
+  const int base = tile * kScanTile + threadIdx.x * kScanItems;
   int v[kScanItems];
   int sum = 0;
 #pragma unroll
   for (int k = 0; k < kScanItems; ++k) {
-    const int i = base + k;
-    v[k] = (i < n) ? cnt[i] : 0;
+    v[k] = (base + k < n) ? cnt[base + k] : 0;
     sum += v[k];
   }
   int total;
-  int ex = block_exclusive_scan(sum, s_warp, total) + bsum[blockIdx.x];
+  const int ex = block_exclusive_scan(sum, s_warp, total);
+  if (threadIdx.x == 0) {
+    if (tile == 0) {
+      atomicExch(&tile_status[0], scan_word(tag, 2, total));
+      s_prefix = 0;
+    } else {
+      atomicExch(&tile_status[tile], scan_word(tag, 1, total));
+    }
+  }
+  if (tile > 0 && threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    int excl = 0;
+    int look = tile - 1;
+    while (true) {
+      const int idx = look - lane;
+      ull w = scan_word(tag, 2, 0);  // before tile 0: an empty prefix
+      if (idx >= 0) {
+        long long spins = 0;
+        w = *(volatile ull *)&tile_status[idx];
+        while ((w >> 34) != (tag >> 34)) {
+          if (++spins > kScanSpinLimit) {
+            atomicOr(status, kStScanWait);
+            w = scan_word(tag, 2, 0);
+            break;
+          }
+          w = *(volatile ull *)&tile_status[idx];
+        }
+      }
+      const int kind = (int)((w >> 32) & 3u);
+      const int val = (int)(uint32_t)w;
+      const unsigned pm = __ballot_sync(0xffffffffu, kind == 2);
+      const int stop = pm ? __ffs(pm) - 1 : 31;
+      int part = lane <= stop ? val : 0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+      excl += part;
+      if (pm) break;
+      look -= 32;
+    }
+    if (lane == 0) {
+      atomicExch(&tile_status[tile], scan_word(tag, 2, excl + total));
+      s_prefix = excl;
+    }
+  }
+  __syncthreads();
+  int run = s_prefix + ex;
 #pragma unroll
   for (int k = 0; k < kScanItems; ++k) {
-    const int i = base + k;
-    if (i < n) start[i] = ex;
-    ex += v[k];
+    if (base + k < n) start[base + k] = run;
+    run += v[k];
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    const int tot = bsum[nb];
+  if (tile == nb - 1 && threadIdx.x == 0) {
+    const int tot = s_prefix + total;
     start[n] = tot;
     *n_out = tot < cap ? tot : cap;
   }
@@ -1056,74 +1087,137 @@ __device__ __forceinline__ void try_pair(const KParams &p, int i, ull idi, int s
   extra += register_candidate(p, j, ((ull)db << 32) | (uint32_t)i);
 }
 
-constexpr int kPairTile = 256;  // molecules per block tile
 constexpr int kPairHalo = 32;   // extra molecules staged past the tile
 
-// Round-1 pair search, block-cooperative.  Each block stages a tile of 256
-// box-sorted molecules plus a 32-molecule halo in shared memory.  Pairs inside
-// a box are tested from shared memory by the lower-indexed molecule (boxes are
-// contiguous runs of the sorted array, so partners sit at i+1, i+2, ...).
+// Register an in-radius reacting pair on both molecules.
+__device__ __forceinline__ int register_pair(const KParams &p, int i, int j, float d2) {
+  const ull db = (ull)__float_as_uint(d2) << 32;
+  return register_candidate(p, i, db | (uint32_t)j) + register_candidate(p, j, db | (uint32_t)i);
+}
+
+// Round-1 pair search, block-cooperative.  Each block stages a tile of TILE
+// (128 or 256) box-sorted molecules plus a 33-molecule halo in shared memory.
+// Pairs inside a box are tested from shared memory by the lower-indexed
+// molecule (boxes are contiguous runs of the sorted array, so partners sit at
+// i+1, i+2, ...).  The warp's same-box pairs are enumerated flat: each lane
+// counts its forward partners inside a 64-entry window from two ballots of box
+// boundaries, a warp prefix sum numbers the pairs, and the lanes take pair
+// numbers 32 at a time (owner found by a 5-step search over the prefix), so the
+// trip count is (pairs in the warp)/32 instead of the longest box run.
 // Pairs across boxes exist only for molecules within the stencil radius of a
 // box face; those are tested from global memory by the molecule in the
-// lower-numbered box.  Every in-radius pair is thus tested exactly once and
-// registered on both molecules (smolreact.c:3201-3298 tests each pair once).
-template <bool SINGLE, bool SURF>
-__global__ void __launch_bounds__(kPairTile, 4) k_pairs_tile(KParams p) {
-  __shared__ float4 s_pc[kPairTile + kPairHalo];
-  __shared__ ull s_id[kPairTile + kPairHalo];
-  __shared__ int s_cell[kPairTile + kPairHalo];
+// lower-numbered box (k_pairs_faces).  Every in-radius pair is thus tested
+// exactly once and registered on both molecules (smolreact.c:3201-3298 tests
+// each pair once).
+template <bool SINGLE, bool SURF, int TILE>
+__global__ void __launch_bounds__(TILE, 1024 / TILE) k_pairs_tile(KParams p) {
+  constexpr int W = TILE + kPairHalo + 1;  // every lane can read entry t + 33
+  __shared__ float4 s_pc[W];
+  __shared__ ull s_id[W];
+  __shared__ int s_cell[W];
+  __shared__ float s_rs2[TILE];
   const int n = *p.b_n;
   const uint32_t step = *p.step;
+  const int lane = threadIdx.x & 31;
+  const int wbase = threadIdx.x & ~31;
   int extra = 0;
-  for (int base = blockIdx.x * kPairTile; base < n; base += gridDim.x * kPairTile) {
-    __syncthreads();
-    for (int t = threadIdx.x; t < kPairTile + kPairHalo; t += blockDim.x) {
-      const int g = base + t;
-      if (g < n) {
-        const float4 q = p.b_pc[g];
-        const ull qd = p.b_id[g];
-        s_pc[t] = q;
-        s_id[t] = qd;
-        const DevGeo &gg = geo_of<SINGLE>(p, SINGLE ? 0 : id_rep(qd));
-        s_cell[t] = global_cell(gg, __float_as_uint(q.w));
-      } else {
-        s_cell[t] = -1;
-        s_id[t] = make_id(kDeadSpecies, 0, 0);
-      }
+  // The next tile's entries are loaded into registers while the current tile
+  // is processed (thread t stages entries t and, for t < W - TILE, TILE + t).
+  static_assert(W - TILE <= TILE, "two staged entries per thread at most");
+  const int stride = gridDim.x * TILE;
+  float4 pf0 = make_float4(0.f, 0.f, 0.f, 0.f), pf1 = pf0;
+  ull pd0 = 0, pd1 = 0;
+  auto prefetch = [&](int b) {
+    const int g0 = b + threadIdx.x, g1 = b + TILE + threadIdx.x;
+    if (g0 < n) { pf0 = p.b_pc[g0]; pd0 = p.b_id[g0]; }
+    if (threadIdx.x < W - TILE && g1 < n) { pf1 = p.b_pc[g1]; pd1 = p.b_id[g1]; }
+  };
+  auto stage = [&](int slot, int g, float4 q, ull qd) {
+    if (g < n) {
+      s_pc[slot] = q;
+      s_id[slot] = qd;
+      const DevGeo &gg = geo_of<SINGLE>(p, SINGLE ? 0 : id_rep(qd));
+      s_cell[slot] = global_cell(gg, __float_as_uint(q.w));
+    } else {
+      s_cell[slot] = -1;
+      s_id[slot] = make_id(kDeadSpecies, 0, 0);
     }
+  };
+  if (blockIdx.x * TILE < n) prefetch(blockIdx.x * TILE);
+  for (int base = blockIdx.x * TILE; base < n; base += stride) {
     __syncthreads();
+    stage(threadIdx.x, base + threadIdx.x, pf0, pd0);
+    if (threadIdx.x < W - TILE) stage(TILE + threadIdx.x, base + TILE + threadIdx.x, pf1, pd1);
+    if (base + stride < n) prefetch(base + stride);
     const int t = threadIdx.x;
     const int i = base + t;
     const ull idi = s_id[t];
     const int sp = id_species(idi);
     const bool act = i < n && sp != kDeadSpecies && c_net.pair_mask[sp] != 0;
     const int rep = SINGLE ? 0 : id_rep(idi);
-    const float4 pc = s_pc[t];
-    const int cell = s_cell[t];
     const float rs = act ? p.rsearch[rep * c_net.nsp + sp] : 0.f;
     const float rs2 = rs * rs;
-    ull best = ~0ull;
-    // same-box partners from the staged tile
-    int k = 1;
-    for (; k < kPairHalo; ++k) {
-      const int u = t + k;
-      const bool same = act && s_cell[u] == cell;
-      if (!__any_sync(0xffffffffu, same)) break;
-      if (same) {
-        const float4 q = s_pc[u];
-        const float vx = q.x - pc.x, vy = q.y - pc.y, vz = q.z - pc.z;
-        try_pair<SURF>(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, i + k, s_id[u], rs2, step, best, extra, pc, vx,
-                 vy, vz);
+    s_rs2[t] = rs2;
+    __syncthreads();
+    const float4 pc = s_pc[t];
+    const int cell = s_cell[t];
+    // box boundaries in the warp's window [wbase, wbase + 64): bit b set when
+    // entry wbase + b is the last of its box
+    const unsigned b_lo = __ballot_sync(0xffffffffu, s_cell[t] != s_cell[t + 1]);
+    const unsigned b_hi = __ballot_sync(0xffffffffu, s_cell[t + 32] != s_cell[t + 33]);
+    const unsigned long long ahead = (((unsigned long long)b_hi << 32) | b_lo) >> lane;
+    int c = 0;            // same-box partners after t inside the window
+    bool spill = false;   // the box continues past the window
+    if (act) {
+      if (ahead) c = __ffsll((long long)ahead) - 1;
+      else { c = 63 - lane; spill = true; }
+    }
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int excl = incl - c;
+    const int npairs = __shfl_sync(0xffffffffu, incl, 31);
+    for (int q0 = 0; q0 < npairs; q0 += 32) {
+      const int q = q0 + lane;
+      // owner: the last lane whose first pair number is <= q
+      int o = 0;
+#pragma unroll
+      for (int st = 16; st > 0; st >>= 1)
+        if (__shfl_sync(0xffffffffu, excl, o + st) <= q) o += st;
+      const int off = q - __shfl_sync(0xffffffffu, excl, o);
+      if (q < npairs) {
+        const int ti = wbase + o, tj = ti + 1 + off;
+        const float4 a = s_pc[ti], b = s_pc[tj];
+        const float vx = b.x - a.x, vy = b.y - a.y, vz = b.z - a.z;
+        const float d2 = vx * vx + vy * vy + vz * vz;
+        if (d2 <= s_rs2[ti]) {
+          const ull ida = s_id[ti], idb = s_id[tj];
+          const int spa = id_species(ida), spb = id_species(idb);
+          const int repa = SINGLE ? 0 : id_rep(ida);
+          if (spb != kDeadSpecies && ((c_net.pair_mask[spa] >> spb) & 1u) &&
+              !(SURF && pair_crosses_surface(p.geo[repa], a, vx, vy, vz)) &&
+              pair_reaction(p, repa, spa, spb, d2, id_stream(ida), id_stream(idb), step) >= 0)
+            extra += register_pair(p, base + ti, base + tj, d2);
+        }
       }
     }
-    // a box longer than the staged window continues in global memory
-    if (act && k == kPairHalo && s_cell[t + kPairHalo - 1] == cell) {
+    // a box longer than the window continues in global memory
+    if (spill) {
       const int e = min(p.start[cell + 1], n);
-      for (int j = i + kPairHalo; j < e; ++j) {
-        const float4 q = p.b_pc[j];
-        const float vx = q.x - pc.x, vy = q.y - pc.y, vz = q.z - pc.z;
-        try_pair<SURF>(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, j, p.b_id[j], rs2, step, best, extra, pc, vx, vy,
-                 vz);
+      for (int j = base + wbase + 64; j < e; ++j) {
+        const float4 b = p.b_pc[j];
+        const float vx = b.x - pc.x, vy = b.y - pc.y, vz = b.z - pc.z;
+        const float d2 = vx * vx + vy * vy + vz * vz;
+        if (d2 > rs2) continue;
+        const ull idb = p.b_id[j];
+        const int spb = id_species(idb);
+        if (spb != kDeadSpecies && ((c_net.pair_mask[sp] >> spb) & 1u) &&
+            !(SURF && pair_crosses_surface(p.geo[rep], pc, vx, vy, vz)) &&
+            pair_reaction(p, rep, sp, spb, d2, id_stream(idi), id_stream(idb), step) >= 0)
+          extra += register_pair(p, i, j, d2);
       }
     }
     // molecules near a box face also need the neighbouring boxes: queue them for
@@ -1140,7 +1234,6 @@ __global__ void __launch_bounds__(kPairTile, 4) k_pairs_tile(KParams p) {
     }
     const unsigned fm = __ballot_sync(0xffffffffu, face);
     if (fm) {
-      const int lane = threadIdx.x & 31;
       int slot = 0;
       if (lane == __ffs(fm) - 1) slot = atomicAdd(p.nface, __popc(fm));
       slot = __shfl_sync(0xffffffffu, slot, __ffs(fm) - 1) + __popc(fm & lanemask_lt());
@@ -1149,7 +1242,6 @@ __global__ void __launch_bounds__(kPairTile, 4) k_pairs_tile(KParams p) {
         else atomicOr(p.status, kStCandCap);
       }
     }
-    if (best != ~0ull) extra += register_candidate(p, i, best);
   }
   if (extra) atomicAdd(&p.counters[5], (unsigned long long)extra);
 }
@@ -1533,7 +1625,8 @@ class EngineImpl {
   ull *d_id[2] = {nullptr, nullptr}, *d_pid[2] = {nullptr, nullptr};
   int *d_counts = nullptr;  // [0]=n sorted A [1]=n sorted B [2]=n prod P [3]=n prod Q [4]=nev [5]=ncand [6]=status
   uint32_t *d_step = nullptr;
-  int *d_cnt = nullptr, *d_start = nullptr, *d_bsum = nullptr;
+  int *d_cnt = nullptr, *d_start = nullptr;
+  ull *d_scan_ticket = nullptr, *d_scan_status = nullptr;
   Event *d_ev = nullptr;
   int *d_cand = nullptr;
   ull *d_best = nullptr;
@@ -1556,7 +1649,7 @@ class EngineImpl {
     graph2 = nullptr;
     void *ptrs[] = {d_rsearch, d_geo, d_difstep, d_driftdt, d_bind2, d_pairprob, d_prdpos, d_gtab, d_unithr,
                     d_births, d_pc[0], d_pc[1], d_ppc[0], d_ppc[1], d_id[0], d_id[1], d_pid[0],
-                    d_pid[1], d_face, d_tmp, d_counts, d_step, d_cnt, d_start, d_bsum, d_ev, d_cand, d_best,
+                    d_pid[1], d_face, d_tmp, d_counts, d_step, d_cnt, d_start, d_scan_ticket, d_scan_status, d_ev, d_cand, d_best,
                     d_counters, d_spcount, d_injkey, d_injval};
     for (void *q : ptrs)
       if (q) cudaFree(q);
@@ -1565,10 +1658,13 @@ class EngineImpl {
     d_unithr = nullptr; d_births = nullptr;
     d_pc[0] = d_pc[1] = d_ppc[0] = d_ppc[1] = nullptr;
     d_id[0] = d_id[1] = d_pid[0] = d_pid[1] = nullptr;
-    d_counts = nullptr; d_step = nullptr; d_cnt = d_start = d_bsum = nullptr; d_ev = nullptr;
+    d_counts = nullptr; d_step = nullptr; d_cnt = d_start = nullptr; d_scan_ticket = d_scan_status = nullptr; d_ev = nullptr;
     d_cand = nullptr; d_best = nullptr; d_face = nullptr; d_tmp = nullptr; d_counters = nullptr; d_spcount = nullptr;
     d_injkey = nullptr; d_injval = nullptr;
-    if (own_stream) cudaStreamDestroy(own_stream);
+    if (own_stream) {
+      if (stream == own_stream) stream = nullptr;  // a later init creates a new one
+      cudaStreamDestroy(own_stream);
+    }
     own_stream = nullptr;
   }
 
@@ -1595,7 +1691,6 @@ class EngineImpl {
     p.cnt = d_cnt;
     p.start = d_start;
     p.ncell = ncell;
-    p.blocksums = d_bsum;
     p.ev = d_ev;
     p.nev = d_counts + 4;
     p.evcap = (int)evcap;
@@ -1615,8 +1710,9 @@ class EngineImpl {
     return p;
   }
 
-  int grid_mol() const { return sm_count() * 8; }
-  int grid_tiles() const { return sm_count() * 4; }
+  LaunchTuning tune;  // kept across init
+  int grid_mol() const { return sm_count() * tune.mol_blocks_per_sm; }
+  int grid_tiles() const { return sm_count() * tune.tile_blocks_per_sm; }
   int grid_small() const { return sm_count(); }
 
   size_t adv_smem() const {
@@ -1651,19 +1747,16 @@ class EngineImpl {
     mark("k_begin");
     k_move<SINGLE, SURF><<<grid_mol(), 256, rebin_only ? 0 : adv_smem(), s>>>(p, rebin_only ? 1 : 0);
     mark("k_move");
-    k_scan_reduce<<<nscanblocks, kScanThreads, 0, s>>>(d_cnt, ncell, d_bsum);
-    mark("k_scan_reduce");
-    k_scan_blocks<<<1, 1024, 0, s>>>(d_bsum, nscanblocks);
-    mark("k_scan_blocks");
-    k_scan_apply<<<nscanblocks, kScanThreads, 0, s>>>(d_cnt, ncell, d_bsum, nscanblocks, d_start,
-                                                      p.b_n, (int)cap);
-    mark("k_scan_apply");
+    k_scan_lookback<<<nscanblocks, kScanThreads, 0, s>>>(d_cnt, ncell, nscanblocks, d_scan_ticket,
+                                                         d_scan_status, d_start, p.b_n, (int)cap, p.status);
+    mark("k_scan");
     k_scatter<SINGLE><<<grid_mol(), 256, 0, s>>>(p);
     mark("k_scatter");
     if (rebin_only) return;
     k_births<<<grid_small(), 128, 0, s>>>(p);
     mark("k_births");
-    k_pairs_tile<SINGLE, SURF><<<grid_tiles(), kPairTile, 0, s>>>(p);
+    if (tune.pair_tile == 128) k_pairs_tile<SINGLE, SURF, 128><<<grid_tiles(), 128, 0, s>>>(p);
+    else k_pairs_tile<SINGLE, SURF, 256><<<grid_tiles(), 256, 0, s>>>(p);
     mark("k_pairs");
     k_pairs_faces<SINGLE, SURF><<<grid_mol(), 256, 0, s>>>(p);
     mark("k_pairs_faces");
@@ -1690,7 +1783,7 @@ class EngineImpl {
     else enqueue_step_t<false, true>(par, rebin_only);
   }
 
-  int launches_per_step() const { return 12 + 2 * (dnet.rounds - 1); }
+  int launches_per_step() const { return 10 + 2 * (dnet.rounds - 1); }
 
   int upload_const(std::string *err) {
     CK(cudaMemcpyToSymbolAsync(c_net, &dnet, sizeof(DevNet), 0, cudaMemcpyHostToDevice, stream));
@@ -1936,7 +2029,10 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
   CK(cudaMemsetAsync(E.d_cnt, 0, ((size_t)E.ncell + 1) * sizeof(int), E.stream));
   CK(cudaMalloc(&E.d_start, ((size_t)E.ncell + 1) * sizeof(int)));
   CK(cudaMemsetAsync(E.d_start, 0, ((size_t)E.ncell + 1) * sizeof(int), E.stream));
-  CK(cudaMalloc(&E.d_bsum, ((size_t)E.nscanblocks + 1) * sizeof(int)));
+  CK(cudaMalloc(&E.d_scan_ticket, sizeof(ull)));
+  CK(cudaMemsetAsync(E.d_scan_ticket, 0, sizeof(ull), E.stream));
+  CK(cudaMalloc(&E.d_scan_status, (size_t)E.nscanblocks * sizeof(ull)));
+  CK(cudaMemsetAsync(E.d_scan_status, 0, (size_t)E.nscanblocks * sizeof(ull), E.stream));
   CK(cudaMalloc(&E.d_ev, E.evcap * sizeof(Event)));
   CK(cudaMalloc(&E.d_cand, E.candcap * sizeof(int)));
   CK(cudaMalloc(&E.d_best, E.cap * sizeof(ull)));
@@ -2322,6 +2418,19 @@ void Engine::set_use_graph(bool on) {
   impl_->use_graph = on;
   if (!on) impl_->invalidate_graph();
 }
+
+int Engine::set_tuning(const LaunchTuning &t, std::string *err) {
+  if (t.pair_tile != 128 && t.pair_tile != 256) { if (err) *err = "pair tile must be 128 or 256"; return -6; }
+  if (t.mol_blocks_per_sm < 1 || t.mol_blocks_per_sm > 32 || t.tile_blocks_per_sm < 1 || t.tile_blocks_per_sm > 32) {
+    if (err) *err = "blocks per SM must be 1..32";
+    return -6;
+  }
+  impl_->tune = t;
+  impl_->invalidate_graph();
+  return 0;
+}
+
+LaunchTuning Engine::tuning() const { return impl_->tune; }
 
 int solve_radii_device(int mode, long long n, const double *rate, double dt, const double *difc,
                        const double *b, int rel, double *out, std::string *err) {

@@ -71,6 +71,13 @@ struct RepSpec {
   double prdpos[3][kMaxRxn][kMaxProd][3] = {};
 };
 
+// Launch shape of the per-step kernels; the autotuner picks it per workload.
+struct LaunchTuning {
+  int mol_blocks_per_sm = 8;    // k_move, k_scatter, k_pairs_faces: 256-thread blocks per SM
+  int tile_blocks_per_sm = 4;   // k_pairs_tile blocks per SM
+  int pair_tile = 256;          // molecules per k_pairs_tile tile: 128 or 256
+};
+
 struct EngineStats {
   long long wall = 0, rxn0 = 0, rxn1 = 0, rxn2 = 0, unresolved = 0, multicand = 0, overflow = 0;
 };
@@ -114,6 +121,9 @@ class Engine {
   long long steps_done() const;
   // Capture the 2-step kernel sequence in a CUDA graph and replay it (on by default).
   void set_use_graph(bool on);
+  // Launch shape (kept across init); a change re-captures the step graph.
+  int set_tuning(const LaunchTuning &t, std::string *err);
+  LaunchTuning tuning() const;
   // Run n steps timing every kernel launch with CUDA events.
   int profile(long long nsteps, std::vector<std::string> *names, std::vector<double> *ms,
               std::vector<long long> *launches, std::string *err);

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/smoldyn_b200.h"
+#include "autotune.h"
 #include "engine.h"
 #include "rxnparam.cuh"
 #include "sim.h"
@@ -41,6 +42,7 @@ struct smolb_ens {
   std::vector<std::vector<double>> bindrad, unbindrad;
   long long surrogate_fallbacks = 0;
   std::unique_ptr<smolb::Surrogate> sur;
+  smolb::LaunchTuning tuning;  // kernel launch shape (autotuner)
 };
 
 // process-global error record of the C API (api.cpp)
@@ -63,6 +65,33 @@ double rate_of(const smolb_ens &e, int order, int r, int k) {
   auto it = e.rates.find(x.name);
   if (it != e.rates.end()) return it->second[k];
   return x.rate;
+}
+
+// Virtual boxes per replicate (smolboxes.c:717-749 rule, one binding radius
+// wide at least), from the molecule count and the box-size setting (the
+// autotuner's choice when the template sets neither molperbox nor boxsize).
+void assign_boxes(smolb_ens &e) {
+  const smolb::Sim &T = e.templ;
+  const int R = e.nrep;
+  for (int k = 0; k < R; ++k) {
+    smolb::RepSpec &s = e.reps[k];
+    long long n = 0;
+    for (size_t sp = 1; sp < e.counts.size(); ++sp) n += e.counts[sp][k];
+    double mpbox = T.molperbox, boxsize = T.boxsize;
+    if (mpbox <= 0 && boxsize <= 0) mpbox = T.auto_molperbox > 0 ? T.auto_molperbox : 4;
+    double vol = 1;
+    for (int d = 0; d < T.dim; ++d) vol *= s.hi[d] - s.lo[d];
+    const double f = (mpbox > 0) ? std::pow((double)std::max<long long>(n, 1) / mpbox / vol, 1.0 / T.dim) : 1.0 / boxsize;
+    double maxrad = 0;
+    for (size_t r = 0; r < T.rxn[2].size(); ++r) maxrad = std::max(maxrad, std::sqrt(s.bind2[r]));
+    for (int d = 0; d < 3; ++d) {
+      if (d >= T.dim) { s.ncell[d] = 1; continue; }
+      const double L = s.hi[d] - s.lo[d];
+      int nn = std::max(1, (int)std::ceil(L * f));
+      if (maxrad > 0 && L / nn < maxrad) nn = std::max(1, (int)std::floor(L / maxrad));
+      s.ncell[d] = std::min(nn, 1023);
+    }
+  }
 }
 
 // Derive every replicate's parameters (rates, radii, boxes) into e.reps.
@@ -157,26 +186,7 @@ int derive(smolb_ens &e, std::string *err) {
       }
     }
   }
-  // virtual boxes per replicate (smolboxes.c:717-749 rule, one binding radius wide at least)
-  for (int k = 0; k < R; ++k) {
-    smolb::RepSpec &s = e.reps[k];
-    long long n = 0;
-    for (size_t sp = 1; sp < e.counts.size(); ++sp) n += e.counts[sp][k];
-    double mpbox = T.molperbox, boxsize = T.boxsize;
-    if (mpbox <= 0 && boxsize <= 0) mpbox = 4;
-    double vol = 1;
-    for (int d = 0; d < T.dim; ++d) vol *= s.hi[d] - s.lo[d];
-    const double f = (mpbox > 0) ? std::pow((double)std::max<long long>(n, 1) / mpbox / vol, 1.0 / T.dim) : 1.0 / boxsize;
-    double maxrad = 0;
-    for (size_t r = 0; r < T.rxn[2].size(); ++r) maxrad = std::max(maxrad, std::sqrt(s.bind2[r]));
-    for (int d = 0; d < 3; ++d) {
-      if (d >= T.dim) { s.ncell[d] = 1; continue; }
-      const double L = s.hi[d] - s.lo[d];
-      int nn = std::max(1, (int)std::ceil(L * f));
-      if (maxrad > 0 && L / nn < maxrad) nn = std::max(1, (int)std::floor(L / maxrad));
-      s.ncell[d] = std::min(nn, 1023);
-    }
-  }
+  assign_boxes(e);
   return 0;
 }
 
@@ -191,6 +201,7 @@ int build(smolb_ens &e, std::string *err) {
   const long long cap = T.max_mol > 0 ? T.max_mol : std::max<long long>(2 * total + 4096, total + (1 << 20));
   e.eng.reset(new smolb::Engine());
   rc = e.eng->init(e.net, e.reps, T.dt, (uint64_t)T.seed, cap, err);
+  if (!rc) rc = e.eng->set_tuning(e.tuning, err);
   if (rc) return rc;
   std::vector<double> pos;
   std::vector<int> sp, rep;
@@ -338,6 +349,53 @@ enum ErrorCode smolgpuEnsembleSetStream(ensptr ens, void *stream) {
     ens->need_update = false;
   }
   ens->eng->set_stream(stream);
+  return ECok;
+}
+
+enum ErrorCode smolgpuEnsembleAutotune(ensptr ens, int trial_steps, double *ms_per_step) {
+  ECHECK(ens, ECmissing, "missing ensemble");
+  ECHECK(trial_steps >= 2 && trial_steps <= 100000, ECbounds, "trial_steps must be 2..100000");
+  std::string err;
+  if (build(*ens, &err)) return ens_error(__func__, ECerror, err);
+  ECHECK(ens->eng->steps_done() == 0, ECerror, "autotune runs before the first time step");
+  std::vector<double> pos;
+  std::vector<int> sp, rep;
+  std::vector<uint64_t> serno;
+  if (ens->eng->get_molecules(&pos, &sp, &rep, &serno, &err)) return ens_error(__func__, ECerror, err);
+  smolb::Sim &T = ens->templ;
+  const bool box_free = T.molperbox <= 0 && T.boxsize <= 0;
+  smolb::TuneSetup ts;
+  if (box_free) ts.box_candidates = {1, 2, 4, 8};
+  ts.box_default = T.auto_molperbox > 0 ? T.auto_molperbox : 4;
+  ts.engine = [&]() { return ens->eng.get(); };
+  ts.rebuild = [&](double mpb, std::string *e) -> int {
+    if (box_free) T.auto_molperbox = mpb;
+    assign_boxes(*ens);
+    const long long n = (long long)sp.size();
+    const long long cap = T.max_mol > 0 ? T.max_mol : std::max<long long>(2 * n + 4096, n + (1 << 20));
+    const smolb::LaunchTuning keep = ens->eng->tuning();
+    int rc = ens->eng->init(ens->net, ens->reps, T.dt, (uint64_t)T.seed, cap, e);
+    if (!rc) rc = ens->eng->set_tuning(keep, e);
+    if (!rc) rc = ens->eng->set_molecules(n, pos.data(), sp.data(), rep.data(), serno.data(), e);
+    return rc;
+  };
+  smolb::TuneResult tr;
+  if (smolb::autotune(ts, trial_steps, &tr, &err)) return ens_error(__func__, ECerror, err);
+  ens->tuning = tr.launch;
+  if (box_free) T.auto_molperbox = tr.molperbox;
+  if (ms_per_step) *ms_per_step = tr.ms_per_step;
+  return ECok;
+}
+
+enum ErrorCode smolgpuEnsembleGetTuning(ensptr ens, double *molperbox, int *pair_tile, int *tile_blocks_per_sm,
+                                        int *mol_blocks_per_sm) {
+  ECHECK(ens, ECmissing, "missing ensemble");
+  const smolb::Sim &T = ens->templ;
+  if (molperbox)
+    *molperbox = T.molperbox > 0 ? T.molperbox : (T.boxsize > 0 ? -1 : (T.auto_molperbox > 0 ? T.auto_molperbox : 4));
+  if (pair_tile) *pair_tile = ens->tuning.pair_tile;
+  if (tile_blocks_per_sm) *tile_blocks_per_sm = ens->tuning.tile_blocks_per_sm;
+  if (mol_blocks_per_sm) *mol_blocks_per_sm = ens->tuning.mol_blocks_per_sm;
   return ECok;
 }
 

@@ -292,7 +292,7 @@ int derive_reaction_params(Sim &sim, std::string *err) {
 // pair search looks one box deep) and capped at 1023 boxes per dimension.
 static void choose_grid(const Sim &s, long long nmol, int ncell[3]) {
   double mpbox = s.molperbox, boxsize = s.boxsize;
-  if (mpbox <= 0 && boxsize <= 0) mpbox = 4;
+  if (mpbox <= 0 && boxsize <= 0) mpbox = s.auto_molperbox > 0 ? s.auto_molperbox : 4;
   double f;
   if (mpbox > 0) f = std::pow((double)nmol / mpbox / system_volume(s), 1.0 / s.dim);
   else f = 1.0 / boxsize;

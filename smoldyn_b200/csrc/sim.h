@@ -67,6 +67,8 @@ struct Sim {
   bool time_set = false;
   long long seed = 0;
   double molperbox = -1, boxsize = -1;
+  double auto_molperbox = -1;   // box width picked by the autotuner when neither is set
+  LaunchTuning tuning;          // kernel launch shape (autotuner)
   int gauss_table_size = 4096;
   long long max_mol = -1;
   int accuracy = 10;
