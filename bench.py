@@ -337,10 +337,11 @@ def main():
         e2e = run_e2e(sb, args, rank, world, dist, barrier)
 
     # ---- batched ensemble and surrogate sweep (extra workloads, same GPU)
-    batched = surrogate = None
+    batched = surrogate = surfaces = None
     if not args.no_batched:
         batched = run_batched(sb, torch, args, rank)
         surrogate = run_surrogate(sb, torch, args, rank)
+        surfaces = run_surfaces(sb, torch, args, rank)
 
     # ---- CPU baseline (rank 0, single GPU run only)
     cpu = None
@@ -362,7 +363,7 @@ def main():
             "config": dict(workload_config(args), tuning=tuning, autotune_s=t_tune, autotune_best_trial_ms=tune_ms),
             "e2e": e2e, "gpu_launches": int(launches),
             "roofline": roof, "step_roofline_frac": step_frac, "kernels": kernels, "cpu_baseline": cpu,
-            "clocks": ck, "batched": batched, "batched_surrogate": surrogate,
+            "clocks": ck, "batched": batched, "batched_surrogate": surrogate, "surfaces": surfaces,
         }
         print(json.dumps(line))
     if dist is not None:
@@ -525,6 +526,95 @@ def run_surrogate(sb, torch, args, rank):
                          "note": "each replicate run as its own simulation through the same engine"}
     out["speedup_vs_plain_form"] = out["value"] / out["plain_form"]["value"]
     return out
+
+
+SURF_CONFIG = """dim 3
+species A B C
+difc A 2
+difc B 1
+difc C 0.2
+boundaries 0 0 200
+boundaries 1 0 200
+boundaries 2 0 200
+time_start 0
+time_stop 5
+time_step 0.005
+random_seed %d
+start_surface walls
+action both all reflect
+panel rect +0 0 0 0 200 200
+panel rect -0 200 0 0 200 200
+panel rect +1 0 0 0 200 200
+panel rect -1 0 200 0 200 200
+panel rect +2 0 0 0 200 200
+panel rect -2 0 0 200 200 200
+end_surface
+start_surface membrane
+action both all reflect
+panel sphere 100 100 100 80 30 30
+end_surface
+start_surface sink
+action both all absorb
+panel rect +0 190 0 0 200 200
+end_surface
+reaction fwd A + B -> C 0.05
+reaction decay C -> 0 0.01
+end_file
+"""
+
+
+def run_surfaces(sb, torch, args, rank):
+    """Surfaces workload: cube of side 200 closed by reflective panels, a
+    reflective sphere of radius 80 (cell membrane) at the centre, an absorbing
+    plane at x = 190; 4e6 molecules in equal thirds A, B, C (D = 2, 1, 0.2),
+    60% uniform inside the sphere and 40% outside; A + B -> C (0.05) and
+    C -> 0 (0.01); dt = 0.005."""
+    import ctypes as C
+    rng = np.random.default_rng(31 + rank)
+    n = 4_000_000
+    nin = int(0.6 * n)
+    c = np.array([100.0, 100.0, 100.0])
+    # inside: uniform in the ball; outside: uniform in the cube minus the ball
+    u = rng.normal(size=(nin, 3))
+    u /= np.linalg.norm(u, axis=1)[:, None]
+    pin = c + u * (80.0 * (1 - 1e-6)) * rng.uniform(size=(nin, 1)) ** (1.0 / 3.0)
+    pout = np.empty((0, 3))
+    while len(pout) < n - nin:
+        q = rng.uniform(1e-3, 200 - 1e-3, size=(2 * (n - nin), 3))
+        q = q[(np.linalg.norm(q - c, axis=1) > 80.0 * (1 + 1e-6)) & (q[:, 0] < 190.0)]
+        pout = np.concatenate([pout, q])[: n - nin]
+    pos = np.concatenate([pin, pout])
+    sp = rng.integers(1, 4, size=n).astype(np.int32)
+    lib = sb.load()
+    d = tempfile.mkdtemp(prefix="smolsurf_")
+    try:
+        with open(os.path.join(d, "surf.txt"), "w") as f:
+            f.write(SURF_CONFIG % (5 + rank))
+        simp = C.c_void_p()
+        rc = lib.smolLoadSimFromFile((d + "/").encode(), b"surf.txt", C.byref(simp), b"")
+        if rc != 0:
+            return {"error": str(sb.last_error())}
+        s = sb.Sim(ptr=simp.value)
+        s.set_molecules(pos, sp)
+        s.update()
+        tune_ms = s.autotune(10) if not args.no_tune else None
+        stream = torch.cuda.Stream()
+        s.set_stream(stream.cuda_stream)
+        s.run_steps(args.warmup)
+        n0 = s.total()
+        steps = 200
+        sec = time_on_stream(torch, stream, lambda: s.run_steps(steps))
+        n1 = s.total()
+        out = {"workload": "surfaces: cube 200 closed by reflective panels, reflective sphere r=80 at the centre, "
+                           "absorbing plane x=190; 4e6 molecules A/B/C in thirds (D=2,1,0.2), 60% inside the "
+                           "sphere; A+B->C 0.05, C->0 0.01; dt=0.005",
+               "value": 0.5 * (n0 + n1) * steps / sec, "unit": METRIC, "molecules_start": int(n0),
+               "molecules_end": int(n1), "steps": steps, "ms_per_step": sec * 1e3 / steps,
+               "tuning": s.tuning(), "autotune_best_trial_ms": tune_ms}
+        s.close()
+        return out
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
 
 
 def run_e2e(sb, args, rank, world, dist, barrier):

@@ -132,6 +132,12 @@ enum ErrorCode smolAddBimolecularReaction(simptr sim, const char *reaction, cons
  * rxn->bindrad2, rxn->unbindrad, rxn->prob; smolreact.c:1307-1577). */
 enum ErrorCode smolgpuGetReactionParams(simptr sim, const char *reaction, double *bindrad,
                                         double *unbindrad, double *prob);
+/* Effective rate constant implied by the derived parameters (rxncalcrate,
+ * smolreact.c:1592-1680; the reference computes it for its "measured vs
+ * requested" rate report).  *pgem (optional): geminate recombination
+ * probability for a reaction with two products and a reverse, else -1.
+ * Host FP64 only; no engine is built. */
+enum ErrorCode smolgpuGetEffectiveRate(simptr sim, const char *reaction, double *rate, double *pgem);
 /* Simulated time and step counter. */
 double smolgpuGetTime(simptr sim);
 long long smolgpuGetStepCount(simptr sim);

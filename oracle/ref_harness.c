@@ -18,7 +18,9 @@
  *   D <serno> <ident> <x0> <y0> <z0> <dx> <dy> <dz>
  *   U <serno>                          killed by a first-order reaction
  *   F <serno> <ident> <x> <y> <z>      state after the step
- * Usage: ref_harness <dir/> <file.txt> <out.txt>
+ *   R <order> <rxn> <rate> <pgem>      rxncalcrate (smolreact.c:1592) after update
+ * Usage: ref_harness <dir/> <file.txt> <out.txt> [rates]
+ * With "rates" only the R lines are written (no step is run).
  */
 #include <cstdio>
 #include <cstdlib>
@@ -26,6 +28,9 @@
 
 #include "libsmoldyn.h"
 #include "smoldyn.h"
+
+/* smolreact.c:60 declares it file-locally; it has external C linkage */
+extern "C" double rxncalcrate(simptr sim, int order, int r, double *pgemptr);
 
 static FILE *g_out = NULL;
 static diffusefnptr g_diffuse = NULL;
@@ -77,6 +82,18 @@ int main(int argc, char **argv) {
     return 1;
   }
   if (smolUpdateSim(sim) != ECok) return 1;
+  if (argc > 4 && !strcmp(argv[4], "rates")) {
+    for (int order = 0; order < 3; order++)
+      if (sim->rxnss[order])
+        for (int r = 0; r < sim->rxnss[order]->totrxn; r++) {
+          double pgem = 0;
+          const double rate = rxncalcrate(sim, order, r, &pgem);
+          fprintf(g_out, "R %d %d %.17g %.17g\n", order, r, rate, pgem);
+        }
+    fclose(g_out);
+    smolFreeSim(sim);
+    return 0;
+  }
   if (sim->rxnss[2])
     for (int r = 0; r < sim->rxnss[2]->totrxn; r++)
       fprintf(g_out, "B %d %.17g\n", r, sim->rxnss[2]->rxn[r]->bindrad2);

@@ -77,6 +77,7 @@ PROTOTYPES = {
     "smolAddBimolecularReaction": (C.c_int, [_sim, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int,
                                              C.POINTER(C.c_char_p), C.c_double]),
     "smolgpuGetReactionParams": (C.c_int, [_sim, C.c_char_p, _dp, _dp, _dp]),
+    "smolgpuGetEffectiveRate": (C.c_int, [_sim, C.c_char_p, _dp, _dp]),
     "smolgpuGetTime": (C.c_double, [_sim]),
     "smolgpuGetStepCount": (C.c_longlong, [_sim]),
     "smolgpuGetTotalMolecules": (C.c_longlong, [_sim]),
@@ -331,6 +332,12 @@ class Sim:
         a = (C.c_longlong * 8)()
         check(self.lib.smolgpuGetEventCounts(self.ptr, a))
         return list(a)
+
+    def effective_rate(self, rxn):
+        """(rate, pgem) implied by the derived parameters (rxncalcrate)."""
+        rate, pgem = C.c_double(), C.c_double()
+        check(self.lib.smolgpuGetEffectiveRate(self.ptr, rxn.encode(), C.byref(rate), C.byref(pgem)))
+        return rate.value, pgem.value
 
     def reaction_params(self, rxn):
         b, u, p = C.c_double(), C.c_double(), C.c_double()

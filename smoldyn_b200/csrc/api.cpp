@@ -652,6 +652,18 @@ enum ErrorCode smolgpuGetReactionParams(simptr sim, const char *reaction, double
   return ECok;
 }
 
+enum ErrorCode smolgpuGetEffectiveRate(simptr sim, const char *reaction, double *rate, double *pgem) {
+  LCHECK(sim && reaction && rate, ECmissing, "missing argument");
+  LCHECK(sim->s.dt > 0, ECerror, "time step must be > 0");
+  std::string err;
+  if (smolb::derive_reaction_params(sim->s, &err)) return set_error(__func__, ECerror, err);
+  int o;
+  const int r = sim->s.reaction_index(reaction, &o);
+  LCHECK(r >= 0, ECnonexist, "reaction not found");
+  *rate = smolb::calc_rate(sim->s, o, r, pgem);
+  return ECok;
+}
+
 double smolgpuGetTime(simptr sim) { return sim ? sim->s.time : 0; }
 long long smolgpuGetStepCount(simptr sim) { return sim ? sim->s.steps : 0; }
 

@@ -4,10 +4,10 @@
 //   k_begin          step counter, per-step counters
 //   k_move           diffuse + walls + first-order decisions for every molecule
 //                    (moved position to tmp, events for the ones that leave),
-//                    histogram of destination virtual boxes (warp-aggregated)
-//   scan (3 kernels) exclusive scan of box counts -> box start offsets
+//                    histogram of destination virtual boxes (warp-aggregated),
+//                    then zeroth-order births (Poisson per replicate and reaction)
+//   k_scan           single-pass exclusive scan of box counts -> box starts
 //   k_scatter        permutation of the moved molecules into box order
-//   k_births         zeroth-order births (Poisson per replicate and reaction)
 //   k_pairs_tile     same-box pairs from a shared-memory tile of sorted
 //                    molecules; molecules near a box face are queued
 //   k_pairs_faces    cross-box pairs of the queued molecules
@@ -25,6 +25,7 @@
 #include <cstring>
 #include <numeric>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "devcommon.cuh"
@@ -88,6 +89,15 @@ struct KParams {
 constexpr uint32_t kTmpGone = 0xFFFFFFFFu;  // tmp[i].w of a molecule that left
 
 enum StatusBits { kStMolCap = 1, kStEvCap = 2, kStProdCap = 4, kStCandCap = 8, kStScanWait = 16 };
+
+// Programmatic dependent launch: the step's kernels are launched so that the
+// next kernel can be scheduled while the current one runs.  Each kernel lets
+// its dependent launch as soon as all of its blocks have started, and waits
+// for its predecessor to complete (with memory visible) before it touches
+// anything the predecessor wrote.  Both instructions are no-ops when the
+// kernel was launched without the attribute.
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned m;
@@ -548,9 +558,15 @@ __device__ __forceinline__ void push_event(const KParams &p, const Event &e) {
 }
 
 // ---------------------------------------------------------------------------
+// Start of a step: step counter, per-step counters, and the clamp of the
+// previous step's product count (an overflow there is already flagged).
 __global__ void k_begin(KParams p, int bump_step) {
+  pdl_launch_dependents();
+  pdl_wait();
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     if (bump_step) *p.step += 1;
+    int *pn = const_cast<int *>(p.p_n);
+    if (*pn > p.pcap) *pn = p.pcap;
     *p.nev = 0;
     *p.ncand = 0;
     *p.q_n = 0;
@@ -608,6 +624,8 @@ __device__ __forceinline__ void count_box(const KParams &p, bool alive, float4 p
   if (alive && r.rank == 0) atomicAdd(&p.cnt[cell], r.count);
 }
 
+__device__ void births(const KParams &p, uint32_t step);
+
 // Move pass (one per step): diffuse + walls + first-order decisions for every
 // molecule of the sorted input and of the product list, events for removed or
 // reacting molecules, the moved position into tmp (w = kTmpGone when the
@@ -616,7 +634,9 @@ __device__ __forceinline__ void count_box(const KParams &p, bool alive, float4 p
 template <bool SINGLE, bool SURF>
 __global__ void __launch_bounds__(256) k_move(KParams p, int rebin_only) {
   extern __shared__ float s_gtab[];
-  const float *gtab = rebin_only ? p.gtab : stage_gtab(p, s_gtab);
+  pdl_launch_dependents();
+  const float *gtab = rebin_only ? p.gtab : stage_gtab(p, s_gtab);  // constant data: before the wait
+  pdl_wait();
   const int na = *p.a_n, np = *p.p_n;
   const int total = na + np;
   const uint32_t step = *p.step;
@@ -653,11 +673,14 @@ __global__ void __launch_bounds__(256) k_move(KParams p, int rebin_only) {
     hits_acc += hits;
   }
   if (hits_acc) atomicAdd(&p.counters[0], (unsigned long long)hits_acc);
+  if (!rebin_only) births(p, step);
 }
 
 // Scatter pass: a pure permutation of the moved molecules into box order.
 template <bool SINGLE>
 __global__ void __launch_bounds__(256) k_scatter(KParams p) {
+  pdl_launch_dependents();
+  pdl_wait();
   const int na = *p.a_n, np = *p.p_n;
   const int total = na + np;
   const int lane = threadIdx.x & 31;
@@ -744,6 +767,8 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_lookback(const int *cnt, 
   __shared__ int s_warp[32];
   __shared__ ull s_ticket;
   __shared__ int s_prefix;
+  pdl_launch_dependents();
+  pdl_wait();
   if (threadIdx.x == 0) s_ticket = atomicAdd(ticket, 1ull);
   __syncthreads();
   const ull T = s_ticket;
@@ -859,15 +884,19 @@ __device__ int poisson_sample(double mean, uint2 key, uint4 ctr) {
 
 // One block per (replicate, reaction): thread 0 draws the Poisson number of
 // births and reserves event slots, then the block writes the events.
-__global__ void k_births(KParams p) {
+// Zeroth-order births (smolreact.c:2905-2995): one Poisson draw per
+// (replicate, reaction) by the first thread of a block, then one event per
+// birth; products are placed by k_products.  Run by k_move's blocks after
+// their molecules (all threads of the block call it).
+__device__ void births(const KParams &p, uint32_t step) {
   const int nr0 = c_net.nr[0];
   if (nr0 == 0) return;
   __shared__ int s_base, s_n;
-  const uint32_t step = *p.step;
   const uint2 key = make_uint2(c_net.key0 ^ 0x5bd1e995u, c_net.key1);
   const int total = c_net.nrep * nr0;
   for (int t = blockIdx.x; t < total; t += gridDim.x) {
     const int rep = t / nr0, r = t % nr0;
+    __syncthreads();
     if (threadIdx.x == 0) {
       const int nb = poisson_sample(p.births[t], key, make_uint4((uint32_t)rep, (uint32_t)r, step, 0u));
       int base = 0;
@@ -891,7 +920,6 @@ __global__ void k_births(KParams p) {
       e.rep = (uint32_t)rep;
       p.ev[base + k] = e;
     }
-    __syncthreads();
   }
 }
 
@@ -1116,6 +1144,8 @@ __global__ void __launch_bounds__(TILE, 1024 / TILE) k_pairs_tile(KParams p) {
   __shared__ ull s_id[W];
   __shared__ int s_cell[W];
   __shared__ float s_rs2[TILE];
+  pdl_launch_dependents();
+  pdl_wait();
   const int n = *p.b_n;
   const uint32_t step = *p.step;
   const int lane = threadIdx.x & 31;
@@ -1252,6 +1282,8 @@ __global__ void __launch_bounds__(TILE, 1024 / TILE) k_pairs_tile(KParams p) {
 // molecule in the lower-numbered box.
 template <bool SINGLE, bool SURF>
 __global__ void __launch_bounds__(256) k_pairs_faces(KParams p) {
+  pdl_launch_dependents();
+  pdl_wait();
   const int nf = min(*p.nface, p.cap);
   const int n = *p.b_n;
   const uint32_t step = *p.step;
@@ -1318,6 +1350,8 @@ __global__ void __launch_bounds__(256) k_pairs_faces(KParams p) {
 // Re-search for candidates still alive (conflict-resolution rounds >= 2).
 template <bool SURF>
 __global__ void k_research(KParams p) {
+  pdl_launch_dependents();
+  pdl_wait();
   const int nc = min(*p.ncand, p.candcap);
   const uint32_t step = *p.step;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nc; t += gridDim.x * blockDim.x) {
@@ -1368,6 +1402,8 @@ __device__ __forceinline__ float4 pair_site(const KParams &p, int i, int j, int 
 }
 
 __global__ void k_commit(KParams p) {
+  pdl_launch_dependents();
+  pdl_wait();
   const int nc = min(*p.ncand, p.candcap);
   const uint32_t step = *p.step;
   int done = 0;
@@ -1422,6 +1458,8 @@ __device__ __forceinline__ void random_rotation(uint4 r, float m[9]) {
 
 template <bool SURF>
 __global__ void k_products(KParams p) {
+  pdl_launch_dependents();
+  pdl_wait();
   const int ne = min(*p.nev, p.evcap);
   const uint32_t step = *p.step;
   const uint2 key = make_uint2(c_net.key0 ^ 0x68E31DA4u, c_net.key1 ^ 0xB5297A4Du);
@@ -1519,10 +1557,6 @@ __global__ void k_products(KParams p) {
   const int nc = min(*p.ncand, p.candcap);
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nc; t += gridDim.x * blockDim.x)
     p.best[p.cand[t]] = ~0ull;
-}
-
-__global__ void k_fix_count(int *q_n, int pcap) {
-  if (threadIdx.x == 0 && *q_n > pcap) *q_n = pcap;
 }
 
 // Count live molecules per (rep, species) from scratch (used after uploads);
@@ -1739,39 +1773,51 @@ class EngineImpl {
     marks.push_back({name, e});
   }
 
+  // Launch with programmatic stream serialisation (see pdl_wait) when on.
+  bool use_pdl = true;
+  template <typename... Args, typename... Act>
+  void launch(void (*k)(Args...), int grid, int block, size_t smem, Act &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = use_pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, k, std::forward<Act>(args)...);
+  }
+
   template <bool SINGLE, bool SURF>
   void enqueue_step_t(int par, bool rebin_only) {
     KParams p = params(par);
-    cudaStream_t s = stream;
-    k_begin<<<1, 32, 0, s>>>(p, rebin_only ? 0 : 1);
+    launch(k_begin, 1, 32, 0, p, rebin_only ? 0 : 1);
     mark("k_begin");
-    k_move<SINGLE, SURF><<<grid_mol(), 256, rebin_only ? 0 : adv_smem(), s>>>(p, rebin_only ? 1 : 0);
+    launch(k_move<SINGLE, SURF>, grid_mol(), 256, rebin_only ? 0 : adv_smem(), p, rebin_only ? 1 : 0);
     mark("k_move");
-    k_scan_lookback<<<nscanblocks, kScanThreads, 0, s>>>(d_cnt, ncell, nscanblocks, d_scan_ticket,
-                                                         d_scan_status, d_start, p.b_n, (int)cap, p.status);
+    launch(k_scan_lookback, nscanblocks, kScanThreads, 0, (const int *)d_cnt, ncell, nscanblocks, d_scan_ticket,
+           d_scan_status, d_start, p.b_n, (int)cap, p.status);
     mark("k_scan");
-    k_scatter<SINGLE><<<grid_mol(), 256, 0, s>>>(p);
+    launch(k_scatter<SINGLE>, grid_mol(), 256, 0, p);
     mark("k_scatter");
     if (rebin_only) return;
-    k_births<<<grid_small(), 128, 0, s>>>(p);
-    mark("k_births");
-    if (tune.pair_tile == 128) k_pairs_tile<SINGLE, SURF, 128><<<grid_tiles(), 128, 0, s>>>(p);
-    else k_pairs_tile<SINGLE, SURF, 256><<<grid_tiles(), 256, 0, s>>>(p);
+    if (tune.pair_tile == 128) launch(k_pairs_tile<SINGLE, SURF, 128>, grid_tiles(), 128, 0, p);
+    else launch(k_pairs_tile<SINGLE, SURF, 256>, grid_tiles(), 256, 0, p);
     mark("k_pairs");
-    k_pairs_faces<SINGLE, SURF><<<grid_mol(), 256, 0, s>>>(p);
+    launch(k_pairs_faces<SINGLE, SURF>, grid_mol(), 256, 0, p);
     mark("k_pairs_faces");
-    k_commit<<<grid_small(), 128, 0, s>>>(p);
+    launch(k_commit, grid_small(), 128, 0, p);
     mark("k_commit");
     for (int round = 1; round < dnet.rounds; ++round) {
-      k_research<SURF><<<grid_small(), 128, 0, s>>>(p);
+      launch(k_research<SURF>, grid_small(), 128, 0, p);
       mark("k_research");
-      k_commit<<<grid_small(), 128, 0, s>>>(p);
+      launch(k_commit, grid_small(), 128, 0, p);
       mark("k_commit");
     }
-    k_products<SURF><<<grid_small(), 128, 0, s>>>(p);
+    launch(k_products<SURF>, grid_small(), 128, 0, p);
     mark("k_products");
-    k_fix_count<<<1, 32, 0, s>>>(p.q_n, (int)pcap);
-    mark("k_fix_count");
   }
 
   // Enqueue one step with the given parity (inputs A/P = buffers `par`).
@@ -1783,7 +1829,7 @@ class EngineImpl {
     else enqueue_step_t<false, true>(par, rebin_only);
   }
 
-  int launches_per_step() const { return 10 + 2 * (dnet.rounds - 1); }
+  int launches_per_step() const { return 8 + 2 * (dnet.rounds - 1); }
 
   int upload_const(std::string *err) {
     CK(cudaMemcpyToSymbolAsync(c_net, &dnet, sizeof(DevNet), 0, cudaMemcpyHostToDevice, stream));
@@ -1881,12 +1927,19 @@ class EngineImpl {
     enqueue_step(1, false);
     prof = was;
     nlaunch = before;
-    CK(cudaStreamEndCapture(stream, &g));
-    cudaError_t e = cudaGraphInstantiate(&graph2, g, 0);
-    cudaGraphDestroy(g);
+    cudaError_t e = cudaStreamEndCapture(stream, &g);
+    if (e == cudaSuccess) {
+      e = cudaGraphInstantiate(&graph2, g, 0);
+      cudaGraphDestroy(g);
+    }
     if (e != cudaSuccess) {
       graph2 = nullptr;
-      if (err) *err = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e);
+      if (use_pdl) {  // capture without programmatic edges instead
+        cudaGetLastError();
+        use_pdl = false;
+        return build_graph(err);
+      }
+      if (err) *err = std::string("step graph: ") + cudaGetErrorString(e);
       return -8;
     }
     return 0;
@@ -2292,7 +2345,7 @@ int Engine::get_molecules(std::vector<double> *pos, std::vector<int> *species, s
   CK(cudaStreamSynchronize(E.stream));
   CK(cudaMemcpy(c, E.d_counts, sizeof(c), cudaMemcpyDeviceToHost));
   const int in = E.parity;
-  const int na = c[in], np = c[2 + in];
+  const int na = c[in], np = std::min<int>(c[2 + in], (int)E.pcap);
   std::vector<float4> pc((size_t)na + np);
   std::vector<ull> id((size_t)na + np);
   if (na) {

@@ -310,6 +310,77 @@ static void choose_grid(const Sim &s, long long nmol, int ncell[3]) {
   }
 }
 
+// Effective rate constant implied by the derived parameters (rxncalcrate,
+// smolreact.c:1592-1680), for solution-phase reactions: order 0 from the
+// births per step, order 1 from the per-step probabilities of the species'
+// list (undoing the correction for earlier reactions), order 2 from the
+// tabulated per-step rate at the binding radius (with the reverse products'
+// separation when the reverse reaction places them apart).  *pgem, when not
+// null, gets the geminate recombination probability of a reaction with two
+// products and a reverse (1 - ki/kr at the unbinding separation), else -1.
+double calc_rate(const Sim &sim, int order, int r, double *pgem) {
+  if (order < 0 || order > 2 || r < 0 || r >= (int)sim.rxn[order].size()) return -1;
+  const RxnDef &x = sim.rxn[order][r];
+  const double dt = sim.dt;
+  double ans = 0;
+  if (order == 0) {
+    ans = x.prob < 0 ? 0 : x.prob / dt / system_volume(sim);
+  } else if (order == 1) {
+    if (x.prob > 0) {
+      const int i1 = x.rct[0];
+      double probthis = 0, product = 1.0, sum = 0;
+      for (const RxnDef &y : sim.rxn[1]) {
+        if (y.rct[0] != i1 || !(y.prob > 0)) continue;
+        const double pr = y.prob * product;
+        if (&y == &x) probthis = pr;
+        sum += pr;
+        product *= 1.0 - pr;
+      }
+      ans = -std::log(1.0 - sum) / dt * probthis / sum;
+    }
+  } else {
+    if (x.bindrad2 < 0 || x.prob < 0) {
+      ans = 0;
+    } else {
+      const int i1 = x.rct[0], i2 = x.rct[1];
+      const double step = std::sqrt(2.0 * (sim.species[i1].difc + sim.species[i2].difc) * dt);
+      const double a = std::sqrt(x.bindrad2);
+      int o2 = 0, r2 = 0;
+      const int rev = find_reverse(sim, 2, r, &o2, &r2);
+      const int rpt = rev == 1 ? sim.rxn[o2][r2].rparamt : RP_none;
+      if (rpt == RP_pgem || rpt == RP_pgemmax || rpt == RP_pgemmaxw || rpt == RP_ratio || rpt == RP_unbindrad) {
+        const RxnDef &rv = sim.rxn[o2][r2];
+        double b2 = 0;
+        for (int d = 0; d < sim.dim; ++d) {
+          const double v = rv.prdpos[0][d] - rv.prdpos[1][d];
+          b2 += v * v;
+        }
+        ans = rxnp::numrxnrateprob(step, a, std::sqrt(b2), x.prob) / dt;
+      } else {
+        ans = rxnp::numrxnrateprob(step, a, -1, x.prob) / dt;
+      }
+      if (i1 == i2) ans /= 2.0;
+    }
+  }
+  if (pgem) {
+    int o2 = 0, r2 = 0;
+    if (x.nprod != 2 || find_reverse(sim, order, r, &o2, &r2) == 0) {
+      *pgem = -1;
+    } else {
+      const double step = std::sqrt(2.0 * (sim.species[x.prd[0]].difc + sim.species[x.prd[1]].difc) * dt);
+      double b2 = 0;
+      for (int d = 0; d < sim.dim; ++d) {
+        const double v = x.prdpos[0][d] - x.prdpos[1][d];
+        b2 += v * v;
+      }
+      const RxnDef &rv = sim.rxn[o2][r2];
+      const double a = std::sqrt(rv.bindrad2);
+      *pgem = 1.0 - rxnp::numrxnrateprob(step, a, -1, rv.prob) / rxnp::numrxnrateprob(step, a, std::sqrt(b2), rv.prob);
+    }
+  }
+  return ans;
+}
+
 int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err) {
   *net = NetSpec();
   *rep = RepSpec();

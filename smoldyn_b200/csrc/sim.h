@@ -98,6 +98,8 @@ struct Sim {
 
 // Restatements of the reference's parameter derivation.
 int derive_reaction_params(Sim &sim, std::string *err);
+// rxncalcrate (smolreact.c:1592-1680): effective rate from derived parameters.
+double calc_rate(const Sim &sim, int order, int r, double *pgem);
 // Build engine inputs for a single-replicate simulation.
 int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err);
 // Text configuration reader (statement subset of smolsim.cpp:626 simreadstring).
