@@ -75,7 +75,6 @@ struct KParams {
   int candcap;
   ull *best;
   int *face;                     // molecules near a box face (cross-box pair search)
-  int *nface;
   unsigned long long *counters;  // [0]=wall [1]=rxn0 [2]=rxn1 [3]=rxn2 [4]=unresolved [5]=multicand
   long long *spcount;            // [rep*nsp + sp]
   int *status;
@@ -105,14 +104,11 @@ __device__ __forceinline__ unsigned lanemask_lt() {
   return m;
 }
 
-// Every floating-point operation on the move path below goes through an
-// explicitly rounded intrinsic (__fadd_rn, __fmul_rn, ...): the same molecule
-// move is evaluated in more than one kernel (the box histogram and the box
-// scatter), and those evaluations must agree bit for bit, which rules out
-// compiler-chosen FMA contraction.
-__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
-__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
-__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+// Arithmetic helpers of the move path (plain IEEE single precision; the
+// compiler may contract a multiply and an add into one FMA).
+__device__ __forceinline__ float fadd(float a, float b) { return a + b; }
+__device__ __forceinline__ float fsub(float a, float b) { return a - b; }
+__device__ __forceinline__ float fmul(float a, float b) { return a * b; }
 
 // Bring local coordinate w (relative to the origin of cell j, j maybe out of
 // range) into cell form.
@@ -570,7 +566,6 @@ __global__ void k_begin(KParams p, int bump_step) {
     *p.nev = 0;
     *p.ncand = 0;
     *p.q_n = 0;
-    *p.nface = 0;
   }
 }
 
@@ -1115,7 +1110,6 @@ __device__ __forceinline__ void try_pair(const KParams &p, int i, ull idi, int s
   extra += register_candidate(p, j, ((ull)db << 32) | (uint32_t)i);
 }
 
-constexpr int kPairHalo = 32;   // extra molecules staged past the tile
 
 // Register an in-radius reacting pair on both molecules.
 __device__ __forceinline__ int register_pair(const KParams &p, int i, int j, float d2) {
@@ -1123,80 +1117,83 @@ __device__ __forceinline__ int register_pair(const KParams &p, int i, int j, flo
   return register_candidate(p, i, db | (uint32_t)j) + register_candidate(p, j, db | (uint32_t)i);
 }
 
-// Round-1 pair search, block-cooperative.  Each block stages a tile of TILE
-// (128 or 256) box-sorted molecules plus a 33-molecule halo in shared memory.
-// Pairs inside a box are tested from shared memory by the lower-indexed
-// molecule (boxes are contiguous runs of the sorted array, so partners sit at
-// i+1, i+2, ...).  The warp's same-box pairs are enumerated flat: each lane
-// counts its forward partners inside a 64-entry window from two ballots of box
-// boundaries, a warp prefix sum numbers the pairs, and the lanes take pair
-// numbers 32 at a time (owner found by a 5-step search over the prefix), so the
-// trip count is (pairs in the warp)/32 instead of the longest box run.
-// Pairs across boxes exist only for molecules within the stencil radius of a
-// box face; those are tested from global memory by the molecule in the
-// lower-numbered box (k_pairs_faces).  Every in-radius pair is thus tested
-// exactly once and registered on both molecules (smolreact.c:3201-3298 tests
-// each pair once).
-template <bool SINGLE, bool SURF, int TILE>
-__global__ void __launch_bounds__(TILE, 1024 / TILE) k_pairs_tile(KParams p) {
-  constexpr int W = TILE + kPairHalo + 1;  // every lane can read entry t + 33
-  __shared__ float4 s_pc[W];
-  __shared__ ull s_id[W];
-  __shared__ int s_cell[W];
-  __shared__ float s_rs2[TILE];
+// Round-1 pair search, one warp per 32-molecule tile with no block-level
+// synchronisation.  Each warp stages a 65-entry window of box-sorted molecules
+// (its 32 plus the next 33) in its own slice of shared memory, loading the
+// next window into registers while it processes the current one.  Pairs inside
+// a box are tested by the lower-indexed molecule (boxes are contiguous runs of
+// the sorted array, so partners sit at i+1, i+2, ...).  The warp's same-box
+// pairs are enumerated flat: each lane counts its forward partners inside the
+// window from two ballots of box boundaries, a warp prefix sum numbers the
+// pairs, and the lanes take pair numbers 32 at a time (owner found by a
+// 5-step search over the prefix), so the trip count is (pairs in the warp)/32
+// instead of the longest box run.  A molecule within the stencil radius of a
+// box face sets its bit in the face bitmask (one 32-bit word per tile, written
+// without atomics); k_pairs_faces tests its cross-box pairs from the lower-
+// numbered box.  Every in-radius pair is thus tested exactly once and
+// registered on both molecules (smolreact.c:3201-3298 tests each pair once).
+constexpr int kPairWin = 65;
+
+template <bool SINGLE, bool SURF, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_pairs_tile(KParams p) {
+  constexpr int NW = BLOCK / 32;
+  __shared__ float4 s_pc[NW][kPairWin];
+  __shared__ ull s_id[NW][kPairWin];
+  __shared__ int s_cell[NW][kPairWin];
   pdl_launch_dependents();
   pdl_wait();
   const int n = *p.b_n;
   const uint32_t step = *p.step;
   const int lane = threadIdx.x & 31;
-  const int wbase = threadIdx.x & ~31;
+  const int w = threadIdx.x >> 5;
+  const int nwarps = gridDim.x * NW;
+  float4 *wpc = s_pc[w];
+  ull *wid = s_id[w];
+  int *wcell = s_cell[w];
+  uint32_t *facebits = reinterpret_cast<uint32_t *>(p.face);
   int extra = 0;
-  // The next tile's entries are loaded into registers while the current tile
-  // is processed (thread t stages entries t and, for t < W - TILE, TILE + t).
-  static_assert(W - TILE <= TILE, "two staged entries per thread at most");
-  const int stride = gridDim.x * TILE;
-  float4 pf0 = make_float4(0.f, 0.f, 0.f, 0.f), pf1 = pf0;
-  ull pd0 = 0, pd1 = 0;
-  auto prefetch = [&](int b) {
-    const int g0 = b + threadIdx.x, g1 = b + TILE + threadIdx.x;
-    if (g0 < n) { pf0 = p.b_pc[g0]; pd0 = p.b_id[g0]; }
-    if (threadIdx.x < W - TILE && g1 < n) { pf1 = p.b_pc[g1]; pd1 = p.b_id[g1]; }
+  // registers for the next window: entries wb+lane, wb+32+lane, and (lane 0) wb+64
+  float4 pa = make_float4(0.f, 0.f, 0.f, 0.f), pb = pa, pc64 = pa;
+  ull ia = 0, ib = 0, i64 = 0;
+  auto prefetch = [&](int wb) {
+    if (wb + lane < n) { pa = p.b_pc[wb + lane]; ia = p.b_id[wb + lane]; }
+    if (wb + 32 + lane < n) { pb = p.b_pc[wb + 32 + lane]; ib = p.b_id[wb + 32 + lane]; }
+    if (lane == 0 && wb + 64 < n) { pc64 = p.b_pc[wb + 64]; i64 = p.b_id[wb + 64]; }
   };
   auto stage = [&](int slot, int g, float4 q, ull qd) {
     if (g < n) {
-      s_pc[slot] = q;
-      s_id[slot] = qd;
+      wpc[slot] = q;
+      wid[slot] = qd;
       const DevGeo &gg = geo_of<SINGLE>(p, SINGLE ? 0 : id_rep(qd));
-      s_cell[slot] = global_cell(gg, __float_as_uint(q.w));
+      wcell[slot] = global_cell(gg, __float_as_uint(q.w));
     } else {
-      s_cell[slot] = -1;
-      s_id[slot] = make_id(kDeadSpecies, 0, 0);
+      wcell[slot] = -1;
+      wid[slot] = make_id(kDeadSpecies, 0, 0);
     }
   };
-  if (blockIdx.x * TILE < n) prefetch(blockIdx.x * TILE);
-  for (int base = blockIdx.x * TILE; base < n; base += stride) {
-    __syncthreads();
-    stage(threadIdx.x, base + threadIdx.x, pf0, pd0);
-    if (threadIdx.x < W - TILE) stage(TILE + threadIdx.x, base + TILE + threadIdx.x, pf1, pd1);
-    if (base + stride < n) prefetch(base + stride);
-    const int t = threadIdx.x;
-    const int i = base + t;
-    const ull idi = s_id[t];
+  const int first = (blockIdx.x * NW + w) * 32;
+  if (first < n) prefetch(first);
+  for (int wb = first; wb < n; wb += nwarps * 32) {
+    __syncwarp();
+    stage(lane, wb + lane, pa, ia);
+    stage(32 + lane, wb + 32 + lane, pb, ib);
+    if (lane == 0) stage(64, wb + 64, pc64, i64);
+    __syncwarp();
+    if (wb + nwarps * 32 < n) prefetch(wb + nwarps * 32);
+    const int i = wb + lane;
+    const ull idi = wid[lane];
     const int sp = id_species(idi);
     const bool act = i < n && sp != kDeadSpecies && c_net.pair_mask[sp] != 0;
     const int rep = SINGLE ? 0 : id_rep(idi);
     const float rs = act ? p.rsearch[rep * c_net.nsp + sp] : 0.f;
     const float rs2 = rs * rs;
-    s_rs2[t] = rs2;
-    __syncthreads();
-    const float4 pc = s_pc[t];
-    const int cell = s_cell[t];
-    // box boundaries in the warp's window [wbase, wbase + 64): bit b set when
-    // entry wbase + b is the last of its box
-    const unsigned b_lo = __ballot_sync(0xffffffffu, s_cell[t] != s_cell[t + 1]);
-    const unsigned b_hi = __ballot_sync(0xffffffffu, s_cell[t + 32] != s_cell[t + 33]);
+    const float4 pc = wpc[lane];
+    const int cell = wcell[lane];
+    // box boundaries in the window: bit b set when entry b is the last of its box
+    const unsigned b_lo = __ballot_sync(0xffffffffu, wcell[lane] != wcell[lane + 1]);
+    const unsigned b_hi = __ballot_sync(0xffffffffu, wcell[lane + 32] != wcell[lane + 33]);
     const unsigned long long ahead = (((unsigned long long)b_hi << 32) | b_lo) >> lane;
-    int c = 0;            // same-box partners after t inside the window
+    int c = 0;            // same-box partners after this molecule inside the window
     bool spill = false;   // the box continues past the window
     if (act) {
       if (ahead) c = __ffsll((long long)ahead) - 1;
@@ -1218,26 +1215,27 @@ __global__ void __launch_bounds__(TILE, 1024 / TILE) k_pairs_tile(KParams p) {
       for (int st = 16; st > 0; st >>= 1)
         if (__shfl_sync(0xffffffffu, excl, o + st) <= q) o += st;
       const int off = q - __shfl_sync(0xffffffffu, excl, o);
+      const float rs2o = __shfl_sync(0xffffffffu, rs2, o);
       if (q < npairs) {
-        const int ti = wbase + o, tj = ti + 1 + off;
-        const float4 a = s_pc[ti], b = s_pc[tj];
+        const int tj = o + 1 + off;
+        const float4 a = wpc[o], b = wpc[tj];
         const float vx = b.x - a.x, vy = b.y - a.y, vz = b.z - a.z;
         const float d2 = vx * vx + vy * vy + vz * vz;
-        if (d2 <= s_rs2[ti]) {
-          const ull ida = s_id[ti], idb = s_id[tj];
+        if (d2 <= rs2o) {
+          const ull ida = wid[o], idb = wid[tj];
           const int spa = id_species(ida), spb = id_species(idb);
           const int repa = SINGLE ? 0 : id_rep(ida);
           if (spb != kDeadSpecies && ((c_net.pair_mask[spa] >> spb) & 1u) &&
               !(SURF && pair_crosses_surface(p.geo[repa], a, vx, vy, vz)) &&
               pair_reaction(p, repa, spa, spb, d2, id_stream(ida), id_stream(idb), step) >= 0)
-            extra += register_pair(p, base + ti, base + tj, d2);
+            extra += register_pair(p, wb + o, wb + tj, d2);
         }
       }
     }
     // a box longer than the window continues in global memory
     if (spill) {
       const int e = min(p.start[cell + 1], n);
-      for (int j = base + wbase + 64; j < e; ++j) {
+      for (int j = wb + 64; j < e; ++j) {
         const float4 b = p.b_pc[j];
         const float vx = b.x - pc.x, vy = b.y - pc.y, vz = b.z - pc.z;
         const float d2 = vx * vx + vy * vy + vz * vz;
@@ -1250,8 +1248,7 @@ __global__ void __launch_bounds__(TILE, 1024 / TILE) k_pairs_tile(KParams p) {
           extra += register_pair(p, i, j, d2);
       }
     }
-    // molecules near a box face also need the neighbouring boxes: queue them for
-    // k_pairs_faces (a serial global-memory walk here would stall the warp)
+    // molecules near a box face also need the neighbouring boxes
     bool face = false;
     if (act) {
       const DevGeo &g = geo_of<SINGLE>(p, rep);
@@ -1263,86 +1260,112 @@ __global__ void __launch_bounds__(TILE, 1024 / TILE) k_pairs_tile(KParams p) {
       face = pc.x < rs || pc.x > ub0 - rs || pc.y < rs || pc.y > ub1 - rs || pc.z < rs || pc.z > ub2 - rs;
     }
     const unsigned fm = __ballot_sync(0xffffffffu, face);
-    if (fm) {
-      int slot = 0;
-      if (lane == __ffs(fm) - 1) slot = atomicAdd(p.nface, __popc(fm));
-      slot = __shfl_sync(0xffffffffu, slot, __ffs(fm) - 1) + __popc(fm & lanemask_lt());
-      if (face) {
-        if (slot < p.cap) p.face[slot] = i;
-        else atomicOr(p.status, kStCandCap);
-      }
-    }
+    if (lane == 0) facebits[wb >> 5] = fm;
   }
   if (extra) atomicAdd(&p.counters[5], (unsigned long long)extra);
 }
 
-// Cross-box pairs for the molecules queued by k_pairs_tile (those within the
-// stencil radius of a box face): one thread per queued molecule walks the
-// neighbouring boxes its stencil reaches; a pair across boxes is tested by the
-// molecule in the lower-numbered box.
+// Cross-box pairs of one molecule within the stencil radius of a box face:
+// walk the neighbouring boxes its stencil reaches; a pair across boxes is
+// tested by the molecule in the lower-numbered box.
+template <bool SINGLE, bool SURF>
+__device__ __forceinline__ void face_walk(const KParams &p, int i, int n, uint32_t step, int &extra) {
+  const float4 pc = p.b_pc[i];
+  const ull idi = p.b_id[i];
+  const int sp = id_species(idi);
+  const int rep = SINGLE ? 0 : id_rep(idi);
+  const DevGeo &g = geo_of<SINGLE>(p, rep);
+  const float rs = p.rsearch[rep * c_net.nsp + sp];
+  const float rs2 = rs * rs;
+  int ix, iy, iz;
+  unpack_cell(__float_as_uint(pc.w), ix, iy, iz);
+  const int cell = global_cell(g, __float_as_uint(pc.w));
+  const float ub0 = (ix == g.n[0] - 1) ? g.whi[0] : g.h[0];
+  const float ub1 = (iy == g.n[1] - 1) ? g.whi[1] : g.h[1];
+  const float ub2 = (iz == g.n[2] - 1) ? g.whi[2] : g.h[2];
+  const int xlo = pc.x < rs ? -1 : 0, xhi = pc.x > ub0 - rs ? 1 : 0;
+  const int ylo = pc.y < rs ? -1 : 0, yhi = pc.y > ub1 - rs ? 1 : 0;
+  const int zlo = pc.z < rs ? -1 : 0, zhi = pc.z > ub2 - rs ? 1 : 0;
+  const bool px = g.wall[0] == kWallPeriodic, py = g.wall[2] == kWallPeriodic, pz = g.wall[4] == kWallPeriodic;
+  ull best = ~0ull;
+  for (int dz = zlo; dz <= zhi; ++dz) {
+    int z = iz + dz;
+    if (z < 0 || z >= g.n[2]) {
+      if (!pz) continue;
+      z = (z < 0) ? z + g.n[2] : z - g.n[2];
+    }
+    for (int dy = ylo; dy <= yhi; ++dy) {
+      int y = iy + dy;
+      if (y < 0 || y >= g.n[1]) {
+        if (!py) continue;
+        y = (y < 0) ? y + g.n[1] : y - g.n[1];
+      }
+      const int rowbase = g.cell0 + (z * g.n[1] + y) * g.n[0];
+      for (int dx = xlo; dx <= xhi; ++dx) {
+        if (dx == 0 && dy == 0 && dz == 0) continue;
+        int x = ix + dx;
+        if (x < 0 || x >= g.n[0]) {
+          if (!px) continue;
+          x = (x < 0) ? x + g.n[0] : x - g.n[0];
+        }
+        const int c = rowbase + x;
+        if (c <= cell) continue;
+        const int s0 = p.start[c], e0 = min(p.start[c + 1], n);
+        for (int j = s0; j < e0; ++j) {
+          const float4 q = p.b_pc[j];
+          const float vx = (q.x - pc.x) + (float)dx * g.h[0];
+          const float vy = (q.y - pc.y) + (float)dy * g.h[1];
+          const float vz = (q.z - pc.z) + (float)dz * g.h[2];
+          try_pair<SURF>(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, j, p.b_id[j], rs2, step, best, extra, pc, vx, vy,
+               vz);
+        }
+      }
+    }
+  }
+  if (best != ~0ull) extra += register_candidate(p, i, best);
+}
+
+// Cross-box pairs for the molecules flagged in the face bitmask by
+// k_pairs_tile.  Each warp reads 32 bitmask words (1024 molecules), numbers
+// their set bits with a warp prefix sum and hands them out 32 at a time, so
+// every lane walks one flagged molecule per round.
 template <bool SINGLE, bool SURF>
 __global__ void __launch_bounds__(256) k_pairs_faces(KParams p) {
   pdl_launch_dependents();
   pdl_wait();
-  const int nf = min(*p.nface, p.cap);
   const int n = *p.b_n;
+  const int nwords = (n + 31) >> 5;
   const uint32_t step = *p.step;
+  const uint32_t *facebits = reinterpret_cast<const uint32_t *>(p.face);
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
   int extra = 0;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nf; t += gridDim.x * blockDim.x) {
-    const int i = p.face[t];
-    const float4 pc = p.b_pc[i];
-    const ull idi = p.b_id[i];
-    const int sp = id_species(idi);
-    const int rep = SINGLE ? 0 : id_rep(idi);
-    const DevGeo &g = geo_of<SINGLE>(p, rep);
-    const float rs = p.rsearch[rep * c_net.nsp + sp];
-    const float rs2 = rs * rs;
-    int ix, iy, iz;
-    unpack_cell(__float_as_uint(pc.w), ix, iy, iz);
-    const int cell = global_cell(g, __float_as_uint(pc.w));
-    const float ub0 = (ix == g.n[0] - 1) ? g.whi[0] : g.h[0];
-    const float ub1 = (iy == g.n[1] - 1) ? g.whi[1] : g.h[1];
-    const float ub2 = (iz == g.n[2] - 1) ? g.whi[2] : g.h[2];
-    const int xlo = pc.x < rs ? -1 : 0, xhi = pc.x > ub0 - rs ? 1 : 0;
-    const int ylo = pc.y < rs ? -1 : 0, yhi = pc.y > ub1 - rs ? 1 : 0;
-    const int zlo = pc.z < rs ? -1 : 0, zhi = pc.z > ub2 - rs ? 1 : 0;
-    const bool px = g.wall[0] == kWallPeriodic, py = g.wall[2] == kWallPeriodic, pz = g.wall[4] == kWallPeriodic;
-    ull best = ~0ull;
-    for (int dz = zlo; dz <= zhi; ++dz) {
-      int z = iz + dz;
-      if (z < 0 || z >= g.n[2]) {
-        if (!pz) continue;
-        z = (z < 0) ? z + g.n[2] : z - g.n[2];
-      }
-      for (int dy = ylo; dy <= yhi; ++dy) {
-        int y = iy + dy;
-        if (y < 0 || y >= g.n[1]) {
-          if (!py) continue;
-          y = (y < 0) ? y + g.n[1] : y - g.n[1];
-        }
-        const int rowbase = g.cell0 + (z * g.n[1] + y) * g.n[0];
-        for (int dx = xlo; dx <= xhi; ++dx) {
-          if (dx == 0 && dy == 0 && dz == 0) continue;
-          int x = ix + dx;
-          if (x < 0 || x >= g.n[0]) {
-            if (!px) continue;
-            x = (x < 0) ? x + g.n[0] : x - g.n[0];
-          }
-          const int c = rowbase + x;
-          if (c <= cell) continue;
-          const int s0 = p.start[c], e0 = min(p.start[c + 1], n);
-          for (int j = s0; j < e0; ++j) {
-            const float4 q = p.b_pc[j];
-            const float vx = (q.x - pc.x) + (float)dx * g.h[0];
-            const float vy = (q.y - pc.y) + (float)dy * g.h[1];
-            const float vz = (q.z - pc.z) + (float)dz * g.h[2];
-            try_pair<SURF>(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, j, p.b_id[j], rs2, step, best, extra, pc, vx, vy,
-                 vz);
-          }
-        }
+  for (int base = gw * 32; base < nwords; base += nw * 32) {
+    const uint32_t bits = (base + lane < nwords) ? facebits[base + lane] : 0u;
+    const int cnt = __popc(bits);
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int excl = incl - cnt;
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    for (int q0 = 0; q0 < total; q0 += 32) {
+      const int q = q0 + lane;
+      int o = 0;
+#pragma unroll
+      for (int st = 16; st > 0; st >>= 1)
+        if (__shfl_sync(0xffffffffu, excl, o + st) <= q) o += st;
+      uint32_t m = __shfl_sync(0xffffffffu, bits, o);
+      const int r = q - __shfl_sync(0xffffffffu, excl, o);
+      if (q < total) {
+        for (int k = 0; k < r; ++k) m &= m - 1;  // drop the r lower set bits
+        const int i = ((base + o) << 5) + __ffs(m) - 1;
+        face_walk<SINGLE, SURF>(p, i, n, step, extra);
       }
     }
-    if (best != ~0ull) extra += register_candidate(p, i, best);
   }
   if (extra) atomicAdd(&p.counters[5], (unsigned long long)extra);
 }
@@ -1733,7 +1756,6 @@ class EngineImpl {
     p.candcap = (int)candcap;
     p.best = d_best;
     p.face = d_face;
-    p.nface = d_counts + 7;
     p.counters = d_counters;
     p.spcount = d_spcount;
     p.status = d_counts + 6;
