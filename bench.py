@@ -221,6 +221,16 @@ def run_reference_arm(args, rank, world):
     return 0
 
 
+def combine_ranks(dist, torch, t_s, work, device):
+    """Whole-job numbers over the ranks of a replicas run: the slowest rank's
+    time (max) and the work of all ranks (sum)."""
+    tmax = torch.tensor([t_s], device=device, dtype=torch.float64)
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    tsum = torch.tensor([work], device=device, dtype=torch.float64)
+    dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+    return float(tmax.item()), float(tsum.item())
+
+
 def workload_config(args):
     n = getattr(args, "molecules", N_MOL)
     side = L_SIDE * (n / N_MOL) ** (1.0 / 3.0)
@@ -299,12 +309,7 @@ def main():
     mol_steps = 0.5 * (n0 + n1) * args.steps
     t_s = ms / 1e3
     if dist is not None:
-        tt = torch.tensor([t_s, mol_steps], device="cuda", dtype=torch.float64)
-        tmax = tt[:1].clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        tsum = tt[1:].clone()
-        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
-        t_s, mol_steps = float(tmax.item()), float(tsum.item())
+        t_s, mol_steps = combine_ranks(dist, torch, t_s, mol_steps, "cuda")
     value = mol_steps / t_s
 
     # ---- per-kernel breakdown (events between launches) for the roofline

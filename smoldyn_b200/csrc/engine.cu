@@ -1248,7 +1248,10 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_pairs_tile(KParams p) {
           extra += register_pair(p, i, j, d2);
       }
     }
-    // molecules near a box face also need the neighbouring boxes
+    // Molecules near a box face also need the neighbouring boxes.  Cross-box
+    // pairs are tested from the lower-numbered box, so only molecules whose
+    // stencil reaches a higher-numbered box are flagged: those near a high
+    // face, or near a low face that wraps (periodic) to the far end.
     bool face = false;
     if (act) {
       const DevGeo &g = geo_of<SINGLE>(p, rep);
@@ -1257,7 +1260,10 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_pairs_tile(KParams p) {
       const float ub0 = (ix == g.n[0] - 1) ? g.whi[0] : g.h[0];
       const float ub1 = (iy == g.n[1] - 1) ? g.whi[1] : g.h[1];
       const float ub2 = (iz == g.n[2] - 1) ? g.whi[2] : g.h[2];
-      face = pc.x < rs || pc.x > ub0 - rs || pc.y < rs || pc.y > ub1 - rs || pc.z < rs || pc.z > ub2 - rs;
+      face = pc.x > ub0 - rs || pc.y > ub1 - rs || pc.z > ub2 - rs ||
+             (pc.x < rs && ix == 0 && g.wall[0] == kWallPeriodic) ||
+             (pc.y < rs && iy == 0 && g.wall[2] == kWallPeriodic) ||
+             (pc.z < rs && iz == 0 && g.wall[4] == kWallPeriodic);
     }
     const unsigned fm = __ballot_sync(0xffffffffu, face);
     if (lane == 0) facebits[wb >> 5] = fm;
