@@ -672,6 +672,45 @@ __global__ void __launch_bounds__(256) k_move(KParams p, int rebin_only) {
 }
 
 // Scatter pass: a pure permutation of the moved molecules into box order.
+// Each warp takes its slots from a box's count with one atomic per run of
+// same-box lanes.  The pass is latency-bound (load, atomic, box start,
+// store), so every thread handles two molecules per iteration with their
+// chains interleaved.
+struct ScatterItem {
+  float4 pc;
+  ull id;
+  bool alive;
+  int cell;
+};
+
+template <bool SINGLE>
+__device__ __forceinline__ ScatterItem scatter_load(const KParams &p, int i, int na, int total) {
+  ScatterItem it;
+  it.pc = make_float4(0.f, 0.f, 0.f, __uint_as_float(kTmpGone));
+  it.id = 0;
+  if (i < total) {
+    it.pc = p.tmp[i];
+    it.id = (i < na) ? p.a_id[i] : p.p_id[i - na];
+  }
+  it.alive = __float_as_uint(it.pc.w) != kTmpGone;
+  it.cell = -1;
+  if (it.alive) {
+    const DevGeo &g = geo_of<SINGLE>(p, SINGLE ? 0 : id_rep(it.id));
+    it.cell = global_cell(g, __float_as_uint(it.pc.w));
+  }
+  return it;
+}
+
+__device__ __forceinline__ void scatter_store(const KParams &p, const ScatterItem &it, int slot) {
+  if (!it.alive) return;
+  if (slot >= 0 && slot < p.cap) {
+    p.b_pc[slot] = it.pc;
+    p.b_id[slot] = it.id;
+  } else {
+    atomicOr(p.status, kStMolCap);
+  }
+}
+
 template <bool SINGLE>
 __global__ void __launch_bounds__(256) k_scatter(KParams p) {
   pdl_launch_dependents();
@@ -679,34 +718,22 @@ __global__ void __launch_bounds__(256) k_scatter(KParams p) {
   const int na = *p.a_n, np = *p.p_n;
   const int total = na + np;
   const int lane = threadIdx.x & 31;
-  for (int base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
-    const int i = base + threadIdx.x;
-    float4 pc = make_float4(0.f, 0.f, 0.f, __uint_as_float(kTmpGone));
-    ull id = 0;
-    if (i < total) {
-      pc = p.tmp[i];
-      id = (i < na) ? p.a_id[i] : p.p_id[i - na];
-    }
-    const bool alive = __float_as_uint(pc.w) != kTmpGone;
-    int cell = -1;
-    if (alive) {
-      const DevGeo &g = geo_of<SINGLE>(p, SINGLE ? 0 : id_rep(id));
-      cell = global_cell(g, __float_as_uint(pc.w));
-    }
-    const BoxRun run = box_run(alive, cell);
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x; base < total; base += 2 * stride) {
+    const ScatterItem a = scatter_load<SINGLE>(p, base + threadIdx.x, na, total);
+    const ScatterItem b = scatter_load<SINGLE>(p, base + stride + threadIdx.x, na, total);
+    const BoxRun ra = box_run(a.alive, a.cell);
+    const BoxRun rb = box_run(b.alive, b.cell);
     // the run's first live lane takes `count` slots from the top of the box
-    int old = 0;
-    if (alive && run.rank == 0) old = atomicSub(&p.cnt[cell], run.count);
-    old = __shfl_sync(0xffffffffu, old, alive ? run.head : lane);
-    if (alive) {
-      const int slot = p.start[cell] + old - run.count + run.rank;
-      if (slot >= 0 && slot < p.cap) {
-        p.b_pc[slot] = pc;
-        p.b_id[slot] = id;
-      } else {
-        atomicOr(p.status, kStMolCap);
-      }
-    }
+    int olda = 0, oldb = 0;
+    if (a.alive && ra.rank == 0) olda = atomicSub(&p.cnt[a.cell], ra.count);
+    if (b.alive && rb.rank == 0) oldb = atomicSub(&p.cnt[b.cell], rb.count);
+    const int sa = a.alive ? p.start[a.cell] : 0;
+    const int sb = b.alive ? p.start[b.cell] : 0;
+    olda = __shfl_sync(0xffffffffu, olda, a.alive ? ra.head : lane);
+    oldb = __shfl_sync(0xffffffffu, oldb, b.alive ? rb.head : lane);
+    scatter_store(p, a, sa + olda - ra.count + ra.rank);
+    scatter_store(p, b, sb + oldb - rb.count + rb.rank);
   }
 }
 
@@ -1322,8 +1349,9 @@ __device__ __forceinline__ void face_walk(const KParams &p, int i, int n, uint32
           const float vx = (q.x - pc.x) + (float)dx * g.h[0];
           const float vy = (q.y - pc.y) + (float)dy * g.h[1];
           const float vz = (q.z - pc.z) + (float)dz * g.h[2];
-          try_pair<SURF>(p, i, idi, sp, rep, vx * vx + vy * vy + vz * vz, j, p.b_id[j], rs2, step, best, extra, pc, vx, vy,
-               vz);
+          const float d2 = vx * vx + vy * vy + vz * vz;
+          if (d2 <= rs2)  // the partner's identity is read only for in-radius pairs
+            try_pair<SURF>(p, i, idi, sp, rep, d2, j, p.b_id[j], rs2, step, best, extra, pc, vx, vy, vz);
         }
       }
     }
@@ -1673,6 +1701,7 @@ class EngineImpl {
   cudaStream_t own_stream = nullptr, stream = nullptr;
   bool use_graph = true;
   cudaGraphExec_t graph2 = nullptr;  // two steps (even + odd parity)
+  cudaGraphExec_t graph1[2] = {nullptr, nullptr};  // one step of each parity
   long long nlaunch = 0;
   long long nsteps = 0;
   int parity = 0;  // 0: A/P are inputs; 1: B/Q are inputs
@@ -1708,8 +1737,7 @@ class EngineImpl {
   }
 
   void release() {
-    if (graph2) cudaGraphExecDestroy(graph2);
-    graph2 = nullptr;
+    invalidate_graph();
     void *ptrs[] = {d_rsearch, d_geo, d_difstep, d_driftdt, d_bind2, d_pairprob, d_prdpos, d_gtab, d_unithr,
                     d_births, d_pc[0], d_pc[1], d_ppc[0], d_ppc[1], d_id[0], d_id[1], d_pid[0],
                     d_pid[1], d_face, d_tmp, d_counts, d_step, d_cnt, d_start, d_scan_ticket, d_scan_status, d_ev, d_cand, d_best,
@@ -1942,34 +1970,56 @@ class EngineImpl {
   void invalidate_graph() {
     if (graph2) cudaGraphExecDestroy(graph2);
     graph2 = nullptr;
+    for (int k = 0; k < 2; ++k) {
+      if (graph1[k]) cudaGraphExecDestroy(graph1[k]);
+      graph1[k] = nullptr;
+    }
   }
 
-  int build_graph(std::string *err) {
-    invalidate_graph();
+  // Capture the steps of parities first..last (one or two steps) into *out.
+  int capture_steps(int first, int last, cudaGraphExec_t *out, std::string *err) {
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     const long long before = nlaunch;
     const bool was = prof;
     prof = false;
-    enqueue_step(0, false);
-    enqueue_step(1, false);
+    for (int par = first; par <= last; ++par) enqueue_step(par, false);
     prof = was;
     nlaunch = before;
     cudaError_t e = cudaStreamEndCapture(stream, &g);
     if (e == cudaSuccess) {
-      e = cudaGraphInstantiate(&graph2, g, 0);
+      e = cudaGraphInstantiate(out, g, 0);
       cudaGraphDestroy(g);
     }
     if (e != cudaSuccess) {
-      graph2 = nullptr;
+      *out = nullptr;
       if (use_pdl) {  // capture without programmatic edges instead
         cudaGetLastError();
+        invalidate_graph();
         use_pdl = false;
-        return build_graph(err);
+        return capture_steps(first, last, out, err);
       }
       if (err) *err = std::string("step graph: ") + cudaGetErrorString(e);
       return -8;
     }
+    return 0;
+  }
+
+  int build_graph(std::string *err) {
+    if (graph2) cudaGraphExecDestroy(graph2);
+    graph2 = nullptr;
+    return capture_steps(0, 1, &graph2, err);
+  }
+
+  // One step of the current parity through its single-step graph.
+  int run_one(std::string *err) {
+    if (!graph1[parity]) {
+      int rc = capture_steps(parity, parity, &graph1[parity], err);
+      if (rc) return rc;
+    }
+    CK(cudaGraphLaunch(graph1[parity], stream));
+    nlaunch += launches_per_step();
+    parity ^= 1;
     return 0;
   }
 };
@@ -2285,10 +2335,10 @@ int Engine::run(long long nsteps, std::string *err) {
   }
   long long done = 0;
   if (E.use_graph && !inj) {
-    // graph replays start at parity 0
+    // two-step replays start at parity 0
     if (E.parity == 1) {
-      E.enqueue_step(1, false);
-      E.parity = 0;
+      int rc = E.run_one(err);
+      if (rc) return rc;
       done++;
     }
     if (nsteps - done >= 2 && !E.graph2) {
@@ -2299,6 +2349,11 @@ int Engine::run(long long nsteps, std::string *err) {
       CK(cudaGraphLaunch(E.graph2, E.stream));
       E.nlaunch += 2 * E.launches_per_step();
       done += 2;
+    }
+    if (done < nsteps) {
+      int rc = E.run_one(err);
+      if (rc) return rc;
+      done++;
     }
   }
   while (done < nsteps) {
