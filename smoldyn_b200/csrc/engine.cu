@@ -87,7 +87,7 @@ struct KParams {
 
 constexpr uint32_t kTmpGone = 0xFFFFFFFFu;  // tmp[i].w of a molecule that left
 
-enum StatusBits { kStMolCap = 1, kStEvCap = 2, kStProdCap = 4, kStCandCap = 8, kStScanWait = 16 };
+enum StatusBits { kStMolCap = 1, kStEvCap = 2, kStProdCap = 4, kStCandCap = 8, kStScanWait = 16, kStUpload = 32 };
 
 // Programmatic dependent launch: the step's kernels are launched so that the
 // next kernel can be scheduled while the current one runs.  Each kernel lets
@@ -1616,6 +1616,42 @@ __global__ void k_products(KParams p) {
     p.best[p.cand[t]] = ~0ull;
 }
 
+// Upload conversion for one replicate: absolute FP64 positions to box-local
+// FP32 coordinates with the packed box index, and identity words (serial
+// number i+1 unless given).  A species index out of range sets kStUpload.
+struct UploadGeo {
+  double lo[3], h[3];
+  int n[3];
+  int dim;
+};
+
+__global__ void k_upload(long long n, const double *pos, const int *species, const ull *serno, UploadGeo ug,
+                         int nspecies, float4 *pc, ull *id, int *status) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int sp = species[i];
+    if (sp <= 0 || sp >= nspecies) {
+      atomicOr(status, kStUpload);
+      pc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+      id[i] = make_id(kDeadSpecies, 0, 0);
+      continue;
+    }
+    int ix[3];
+    float w[3];
+    for (int d = 0; d < 3; ++d) {
+      if (d >= ug.dim) { ix[d] = 0; w[d] = 0.f; continue; }
+      const double x = pos[3 * i + d] - ug.lo[d];
+      int j = (int)floor(x / ug.h[d]);
+      if (j < 0) j = 0;
+      if (j > ug.n[d] - 1) j = ug.n[d] - 1;
+      ix[d] = j;
+      w[d] = (float)(x - j * ug.h[d]);
+    }
+    pc[i] = make_float4(w[0], w[1], w[2], __uint_as_float(pack_cell(ix[0], ix[1], ix[2])));
+    id[i] = make_id(sp, 0, serno ? serno[i] : (ull)(i + 1));
+  }
+}
+
 // Count live molecules per (rep, species) from scratch (used after uploads);
 // per-block shared-memory tallies when the table is small, so that millions
 // of molecules of a few species do not serialise on a handful of addresses.
@@ -1827,6 +1863,70 @@ class EngineImpl {
     cudaEvent_t e = event_pool[pool_used++];
     cudaEventRecord(e, stream);
     marks.push_back({name, e});
+  }
+
+  // Upload of one replicate's molecules with the conversion on the device:
+  // raw FP64 positions, species and optional serial numbers are copied into a
+  // temporary buffer and k_upload writes the staging product buffer.
+  int upload_device(long long n, const double *pos, const int *species, const uint64_t *serno, std::string *err) {
+    const RepSpec &s = reps[0];
+    UploadGeo ug;
+    for (int d = 0; d < 3; ++d) {
+      ug.lo[d] = s.lo[d];
+      ug.h[d] = (s.hi[d] - s.lo[d]) / geo[0].n[d];
+      ug.n[d] = geo[0].n[d];
+    }
+    ug.dim = s.dim;
+    const size_t bpos = (size_t)n * 3 * sizeof(double), bsp = (size_t)n * sizeof(int),
+                 bsn = serno ? (size_t)n * sizeof(ull) : 0;
+    char *d = nullptr;
+    CK(cudaMalloc(&d, bpos + bsp + bsn + 16));
+    double *dpos = reinterpret_cast<double *>(d);
+    int *dsp = reinterpret_cast<int *>(d + bpos);
+    ull *dsn = serno ? reinterpret_cast<ull *>(d + ((bpos + bsp + 15) & ~(size_t)15)) : nullptr;
+    int zero[16] = {0};
+    cudaError_t e = cudaMemcpyAsync(d_counts, zero, sizeof(zero), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dpos, pos, bpos, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dsp, species, bsp, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess && serno) e = cudaMemcpyAsync(dsn, serno, bsn, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) {
+      k_upload<<<sm_count() * 8, 256, 0, stream>>>(n, dpos, dsp, dsn, ug, net.nspecies, d_ppc[0], d_pid[0],
+                                                   d_counts + 6);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    cudaFree(d);
+    if (e != cudaSuccess) {
+      if (err) *err = std::string("upload: ") + cudaGetErrorString(e);
+      return -8;
+    }
+    int st = 0;
+    CK(cudaMemcpy(&st, d_counts + 6, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st & kStUpload) { if (err) *err = "species index out of range"; return -6; }
+    return finish_upload(n, err);
+  }
+
+  // Rebin the staged molecules (product buffer 0) into the sorted buffer and
+  // count species.
+  int finish_upload(long long n, std::string *err) {
+    int staged = (int)n;
+    parity = 0;
+    CK(cudaMemcpyAsync(d_counts + 2, &staged, sizeof(int), cudaMemcpyHostToDevice, stream));
+    CK(cudaMemsetAsync(d_cnt, 0, ((size_t)ncell + 1) * sizeof(int), stream));
+    enqueue_step(0, true);  // rebin only: P[0] -> sorted B (index 1)
+    // sorted array now in buffer 1; make it the input of the next step
+    parity = 1;
+    CK(cudaMemsetAsync(d_counts + 2, 0, 2 * sizeof(int), stream));
+    CK(cudaMemsetAsync(d_spcount, 0, reps.size() * net.nspecies * sizeof(long long), stream));
+    k_species_count<<<grid_mol(), 256, 0, stream>>>(d_id[1], d_counts + 1, d_spcount, net.nspecies,
+                                                    (int)reps.size() * net.nspecies);
+    nlaunch++;
+    CK(cudaStreamSynchronize(stream));
+    CK(cudaGetLastError());
+    int st = 0;
+    CK(cudaMemcpy(&st, d_counts + 6, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st) { if (err) *err = "capacity overflow during upload"; return -9; }
+    return 0;
   }
 
   // Launch with programmatic stream serialisation (see pdl_wait) when on.
@@ -2268,6 +2368,10 @@ int Engine::set_molecules(long long n, const double *pos, const int *species, co
     E.invalidate_graph();
   }
   if (n > E.cap) { if (err) *err = "more molecules than the engine capacity"; return -9; }
+  bool device_path = rep == nullptr && n > 0;
+  if (device_path && serno)
+    for (long long i = 0; i < n && device_path; ++i) device_path = serno[i] != 0;
+  if (device_path) return E.upload_device(n, pos, species, serno, err);
   std::vector<float4> pc((size_t)n);
   std::vector<ull> id((size_t)n);
   std::vector<ull> next_serno(E.reps.size(), 1);
@@ -2303,27 +2407,10 @@ int Engine::set_molecules(long long n, const double *pos, const int *species, co
     id[i] = make_id(sp, rp, sn);
   }
   int zero[16] = {0};
-  int staged = (int)n;
   CK(cudaMemcpyAsync(E.d_counts, zero, sizeof(zero), cudaMemcpyHostToDevice, E.stream));
-  E.parity = 0;
   CK(cudaMemcpyAsync(E.d_ppc[0], pc.data(), n * sizeof(float4), cudaMemcpyHostToDevice, E.stream));
   CK(cudaMemcpyAsync(E.d_pid[0], id.data(), n * sizeof(ull), cudaMemcpyHostToDevice, E.stream));
-  CK(cudaMemcpyAsync(E.d_counts + 2, &staged, sizeof(int), cudaMemcpyHostToDevice, E.stream));
-  CK(cudaMemsetAsync(E.d_cnt, 0, ((size_t)E.ncell + 1) * sizeof(int), E.stream));
-  E.enqueue_step(0, true);  // rebin only: P[0] -> sorted B (index 1)
-  // sorted array now in buffer 1; make it the input of the next step
-  E.parity = 1;
-  CK(cudaMemsetAsync(E.d_counts + 2, 0, 2 * sizeof(int), E.stream));
-  CK(cudaMemsetAsync(E.d_spcount, 0, E.reps.size() * E.net.nspecies * sizeof(long long), E.stream));
-  k_species_count<<<E.grid_mol(), 256, 0, E.stream>>>(E.d_id[1], E.d_counts + 1, E.d_spcount, E.net.nspecies,
-                                                      (int)E.reps.size() * E.net.nspecies);
-  E.nlaunch++;
-  CK(cudaStreamSynchronize(E.stream));
-  CK(cudaGetLastError());
-  int st = 0;
-  CK(cudaMemcpy(&st, E.d_counts + 6, sizeof(int), cudaMemcpyDeviceToHost));
-  if (st) { if (err) *err = "capacity overflow during upload"; return -9; }
-  return 0;
+  return E.finish_upload(n, err);
 }
 
 int Engine::run(long long nsteps, std::string *err) {
