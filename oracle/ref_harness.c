@@ -86,7 +86,7 @@ int main(int argc, char **argv) {
     for (int order = 0; order < 3; order++)
       if (sim->rxnss[order])
         for (int r = 0; r < sim->rxnss[order]->totrxn; r++) {
-          double pgem = 0;
+          double pgem = -1;  /* left as is when rxncalcrate returns early */
           const double rate = rxncalcrate(sim, order, r, &pgem);
           fprintf(g_out, "R %d %d %.17g %.17g\n", order, r, rate, pgem);
         }

@@ -116,6 +116,10 @@ struct DevNet {
   uint8_t prd[3][kMaxRxn][kMaxProd];
   uint8_t fixed[3][kMaxRxn];
   uint8_t has_offset[3][kMaxRxn];
+  // order-2 product placement: 0 = at the site (with offsets), 1 = confspread
+  // (products take the reactants' places), 2 = bounce (reactants pushed apart)
+  uint8_t placement2[kMaxRxn];
+  float bounce_k[kMaxRxn];   // bounce scaling: 1 (given unbinding radius) or 2 (from the binding radius)
 };
 
 // Per-replicate geometry.  Cells are cubes of size h; the last cell in each
@@ -150,6 +154,7 @@ struct Event {      // one reaction or birth; products are placed by k_products
   ull key;          // parent identity (stream key) used for product RNG and serial numbers
   uint32_t rxn;     // order << 8 | reaction index
   uint32_t rep;
+  int ia, ib;       // order 2: sorted indices of reactants 1 and 2 (else -1)
 };
 
 }  // namespace smolb

@@ -662,6 +662,7 @@ __global__ void __launch_bounds__(256) k_move(KParams p, int rebin_only) {
         e.key = id_stream(id);
         e.rxn = (1u << 8) | (uint32_t)(fate - 2);
         e.rep = (uint32_t)id_rep(id);
+        e.ia = e.ib = -1;
         push_event(p, e);
       }
     }
@@ -940,6 +941,7 @@ __device__ void births(const KParams &p, uint32_t step) {
                     mix64((ull)k + 0x9E37ull * (ull)step)) & ((1ull << kSpShift) - 1);
       e.rxn = (0u << 8) | (uint32_t)r;
       e.rep = (uint32_t)rep;
+      e.ia = e.ib = -1;
       p.ev[base + k] = e;
     }
   }
@@ -1488,6 +1490,8 @@ __global__ void k_commit(KParams p) {
     e.key = mix64(ka * 0x9E3779B97F4A7C15ull ^ kb) & ((1ull << kSpShift) - 1);
     e.rxn = (2u << 8) | (uint32_t)r;
     e.rep = (uint32_t)rep;
+    e.ia = a;
+    e.ib = b;
     push_event(p, e);
     p.b_id[i] = id_mark_dead(idi);
     p.b_id[j] = id_mark_dead(idj);
@@ -1551,9 +1555,54 @@ __global__ void k_products(KParams p) {
       }
     }
     const int np = c_net.nprod[order][r];
+    // confspread / bounce (doreact, smolreact.c:2736-2805): products 1 and 2
+    // take (confspread) or are pushed apart from (bounce) the reactants'
+    // places, keep the reactants' serial numbers, and the rest sit at the site
+    const int place = order == 2 ? c_net.placement2[r] : 0;
+    float cust[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+    ull keep_sn[2] = {0, 0};
+    if (place) {
+      float va[3], vb[3];
+      int cs[3];
+      unpack_cell(__float_as_uint(e.site.w), cs[0], cs[1], cs[2]);
+      const float us[3] = {e.site.x, e.site.y, e.site.z};
+      for (int k = 0; k < 2; ++k) {
+        const int idx = k == 0 ? e.ia : e.ib;
+        const float4 q = p.b_pc[idx];
+        keep_sn[k] = id_serno(p.b_id[idx]);
+        int cq[3];
+        unpack_cell(__float_as_uint(q.w), cq[0], cq[1], cq[2]);
+        const float uq[3] = {q.x, q.y, q.z};
+        float *v = k == 0 ? va : vb;
+        for (int d = 0; d < 3; ++d) {  // site -> reactant, nearest periodic image
+          int dc = cq[d] - cs[d];
+          if (dc > 1) dc -= g.n[d];
+          else if (dc < -1) dc += g.n[d];
+          v[d] = d < g.dim ? (uq[d] - us[d]) + (float)dc * g.h[d] : 0.f;
+        }
+      }
+      if (place == 1) {
+        for (int d = 0; d < 3; ++d) { cust[0][d] = va[d]; cust[1][d] = vb[d]; }
+      } else {
+        float v[3] = {vb[0] - va[0], vb[1] - va[1], vb[2] - va[2]};
+        float dist = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        if (dist == 0.f) {
+          dist = sqrtf(p.bind2[rep * c_net.nr[2] + r]);
+          v[0] = dist;
+        }
+        const int kx2 = c_net.rxn_base[2] + r;
+        const float *pp = p.prdpos + (size_t)(rep * c_net.nrx_total + kx2) * kMaxProd * 3;
+        const float p0 = pp[0], p1 = pp[3];
+        const float x = c_net.bounce_k[r] * (1.f / dist - 1.f / (p0 + p1));
+        for (int d = 0; d < 3; ++d) {
+          cust[0][d] = va[d] - x * p0 * v[d];
+          cust[1][d] = vb[d] + x * p1 * v[d];
+        }
+      }
+    }
     float m[9];
     bool rot = false;
-    if (c_net.has_offset[order][r] && !c_net.fixed[order][r] && !c_net.inject) {
+    if (!place && c_net.has_offset[order][r] && !c_net.fixed[order][r] && !c_net.inject) {
       random_rotation(philox(make_uint4((uint32_t)e.key, (uint32_t)(e.key >> 32), step, 8u), key), m);
       rot = true;
     }
@@ -1561,7 +1610,9 @@ __global__ void k_products(KParams p) {
     for (int q = 0; q < np; ++q) {
       const int psp = c_net.prd[order][r][q];
       float off[3] = {0.f, 0.f, 0.f};
-      if (c_net.has_offset[order][r]) {
+      if (place) {
+        if (q < 2) { off[0] = cust[q][0]; off[1] = cust[q][1]; off[2] = cust[q][2]; }
+      } else if (c_net.has_offset[order][r]) {
         const float *pp = p.prdpos + ((size_t)(rep * c_net.nrx_total + kx) * kMaxProd + q) * 3;
         if (rot) {
           off[0] = m[0] * pp[0] + m[1] * pp[1] + m[2] * pp[2];
@@ -1594,9 +1645,10 @@ __global__ void k_products(KParams p) {
       }
       if (hits) atomicAdd(&p.counters[0], (unsigned long long)hits);
       if (dead) continue;
-      const ull serno = kProductSernoBit |
-                        (mix64(e.key ^ ((ull)q << 50) ^ ((ull)step << 20) ^ (ull)(order * 97 + r)) &
-                         (kProductSernoBit - 1));
+      const ull serno = (place && q < 2) ? keep_sn[q]
+                                         : kProductSernoBit |
+                                               (mix64(e.key ^ ((ull)q << 50) ^ ((ull)step << 20) ^ (ull)(order * 97 + r)) &
+                                                (kProductSernoBit - 1));
       const int slot = atomicAdd(p.q_n, 1);
       if (slot < p.pcap) {
         const float4 npc = make_float4(w[0], w[1], w[2], __uint_as_float(pack_cell(c[0], c[1], c[2])));
@@ -2188,6 +2240,10 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
     for (int r = 0; r < net.nrxn[o]; ++r) {
       D.nprod[o][r] = (uint8_t)net.nprod[o][r];
       D.fixed[o][r] = (uint8_t)net.fixed_placement[o][r];
+      if (o == 2) {
+        D.placement2[r] = (uint8_t)net.placement2[r];
+        D.bounce_k[r] = (float)net.bounce_k[r];
+      }
       for (int q = 0; q < net.nprod[o][r]; ++q) D.prd[o][r][q] = (uint8_t)net.prd[o][r][q];
       bool off = false;
       for (const RepSpec &s : reps)

@@ -52,6 +52,8 @@ struct NetSpec {
   int nprod[3][kMaxRxn] = {};
   int prd[3][kMaxRxn][kMaxProd] = {};
   int fixed_placement[3][kMaxRxn] = {};      // 1: product offsets not rotated (RPfixed)
+  int placement2[kMaxRxn] = {};              // order 2: 1 confspread, 2 bounce, else 0
+  double bounce_k[kMaxRxn] = {};             // bounce: 1 (unbinding radius given) or 2 (from binding radius)
   int gauss_table_size = 4096;               // power of two (smolmolec.c:781)
   std::vector<PanelSpec> panels;
 };
@@ -75,7 +77,7 @@ struct RepSpec {
 struct LaunchTuning {
   int mol_blocks_per_sm = 8;    // k_move, k_scatter, k_pairs_faces: 256-thread blocks per SM
   int tile_blocks_per_sm = 4;   // k_pairs_tile blocks per SM
-  int pair_tile = 256;          // molecules per k_pairs_tile tile: 128 or 256
+  int pair_tile = 256;          // threads per k_pairs_tile block (warp tiles): 128 or 256
 };
 
 struct EngineStats {

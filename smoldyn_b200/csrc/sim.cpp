@@ -145,6 +145,12 @@ int derive_reaction_params(Sim &sim, std::string *err) {
     RxnDef &x = sim.rxn[2][r];
     const int i1 = x.rct[0], i2 = x.rct[1];
     if (x.disabled) { x.prob = 0; x.bindrad2 = 0; continue; }
+    if (x.rparamt == RP_confspread) {  // smolreact.c:1321-1323: probability from the rate, radius as given
+      if (x.rate < 0) { if (err) *err = "reaction " + x.name + " rate is undefined"; return -8; }
+      x.prob = 1.0 - std::exp(-dt * x.rate);
+      x.bindrad2 = x.bindrad_user >= 0 ? x.bindrad_user * x.bindrad_user : -1;
+      continue;
+    }
     if (x.rate < 0) {
       // rate undefined: a user binding radius (binding_radius statement) stands
       if (x.prob_user >= 0) x.prob = x.prob_user;
@@ -215,9 +221,20 @@ int derive_reaction_params(Sim &sim, std::string *err) {
       } else if (np == 1) {
         if (rpt == RP_none || rpt == RP_irrev || rpt == RP_confspread) x.unbindrad = 0;
         else { if (err) *err = "Illegal product parameter because reaction only has one product"; return -8; }
-      } else if (rpt == RP_bounce) {
-        if (err) *err = "bounce product placement is not supported by the GPU engine";
-        return -8;
+      } else if (rpt == RP_bounce) {  // smolreact.c rxnsetproduct, bounce: split by the reactants' D
+        if (order != 2) { if (err) *err = "bounce product placement needs a bimolecular reaction"; return -8; }
+        if (rpar == -2) {
+          if (err) *err = "bounce with ballistic reflection (parameter -2) is not supported by the GPU engine";
+          return -8;
+        }
+        double dc1 = sim.species[x.rct[0]].difc, dc2 = sim.species[x.rct[1]].difc;
+        const double dsum = dc1 + dc2;
+        if (dsum == 0) dc1 = dc2 = 0.5;
+        else { dc1 /= dsum; dc2 /= dsum; }
+        const double len = rpar >= 0 ? rpar : (x.bindrad2 > 0 ? std::sqrt(x.bindrad2) : 0.0);
+        x.unbindrad = rpar;
+        x.prdpos[0][0] = len * dc1;
+        x.prdpos[1][0] = len * dc2;
       } else {
         double dc1 = sim.species[x.prd[0]].difc, dc2 = sim.species[x.prd[1]].difc;
         const double dsum = dc1 + dc2;
@@ -341,6 +358,8 @@ double calc_rate(const Sim &sim, int order, int r, double *pgem) {
   } else {
     if (x.bindrad2 < 0 || x.prob < 0) {
       ans = 0;
+    } else if (x.rparamt == RP_confspread) {
+      ans = -std::log(1.0 - x.prob) / dt;
     } else {
       const int i1 = x.rct[0], i2 = x.rct[1];
       const double step = std::sqrt(2.0 * (sim.species[i1].difc + sim.species[i2].difc) * dt);
@@ -397,6 +416,10 @@ int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err) {
       net->nprod[o][r] = x.nprod;
       for (int q = 0; q < x.nprod; ++q) net->prd[o][r][q] = x.prd[q];
       net->fixed_placement[o][r] = (x.rparamt == RP_fixed) ? 1 : 0;
+      if (o == 2) {
+        net->placement2[r] = x.rparamt == RP_confspread ? 1 : x.rparamt == RP_bounce ? 2 : 0;
+        net->bounce_k[r] = x.rparam >= 0 ? 1.0 : 2.0;
+      }
       for (int q = 0; q < x.nprod; ++q)
         for (int d = 0; d < 3; ++d) rep->prdpos[o][r][q][d] = x.prdpos[q][d];
       if (o == 0) rep->birth_mean[r] = x.prob;
@@ -666,6 +689,16 @@ int read_config_statement(Sim &sim, const std::string &word, const std::string &
     const int r = sim.reaction_index(w[0], &o);
     if (r < 0) { if (err) *err = "reaction_probability: unknown reaction"; return -3; }
     sim.rxn[o][r].prob_user = atof(w[1].c_str());
+    sim.need_update = true;
+  } else if (word == "confspread_radius") {  // smolsim.cpp:1736, smolreact.c:1762
+    if (!need(2)) return -7;
+    int o;
+    const int r = sim.reaction_index(w[0], &o);
+    if (r < 0 || o != 2) { if (err) *err = "confspread_radius: unknown bimolecular reaction"; return -3; }
+    const double v = atof(w[1].c_str());
+    if (v < 0) { if (err) *err = "confspread radius value must be non-negative"; return -6; }
+    sim.rxn[2][r].rparamt = RP_confspread;
+    sim.rxn[2][r].bindrad_user = v;
     sim.need_update = true;
   } else if (word == "binding_radius") {
     if (!need(2)) return -7;

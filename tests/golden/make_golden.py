@@ -11,6 +11,7 @@ tests/golden/<name>.npz with:
   bind2               squared binding radius of A + B -> C (reference value)
   pos1, sp1, serno1   the reference's state after the step
   L, wall, kf, kr     cube side, boundary type, rate constants
+  config              the configuration text the reference ran
 Usage: python tests/golden/make_golden.py   (needs `make -C oracle ref`)
 """
 import os
@@ -47,6 +48,35 @@ mol {nC} C u u u
 end_file
 """
 
+# Bimolecular product placement: confspread (products take the reactants'
+# places and serial numbers) and bounce (reactants pushed apart to the
+# unbinding distance); probability 1 so every in-radius pair is decided by
+# geometry alone.
+PLACEMENT_CONFIG = """dim 3
+species A B C
+difc A 1
+difc B 1
+difc C 0.5
+time_start 0
+time_stop 1
+time_step 0.01
+boundaries 0 0 {L} p
+boundaries 1 0 {L} p
+boundaries 2 0 {L} p
+random_seed {seed}
+{reactions}
+mol {nA} A u u u
+mol {nB} B u u u
+end_file
+"""
+PLACEMENT_CASES = {
+    "onestep_confspread": dict(L=20, seed=21, nA=1500, nB=1500,
+                               reactions="reaction fwd A + B -> A + C 1e6\nconfspread_radius fwd 0.4"),
+    "onestep_bounce": dict(L=20, seed=22, nA=1500, nB=1500,
+                           reactions="reaction fwd A + B -> A + B\nbinding_radius fwd 0.4\n"
+                                     "product_placement fwd bounce 0.6"),
+}
+
 CASES = {
     "onestep_reflect": dict(L=20, w="r", seed=11, kf=20, kr=1, nA=1600, nB=1600, nC=800),
     "onestep_periodic": dict(L=20, w="p", seed=12, kf=20, kr=1, nA=1600, nB=1600, nC=800),
@@ -55,10 +85,11 @@ CASES = {
 SPECIES = {1: "A", 2: "B", 3: "C"}
 
 
-def run_case(name, cfg):
+def run_case(name, cfg, template=CONFIG):
+    text = template.format(**cfg)
     with tempfile.TemporaryDirectory() as tmp:
         with open(os.path.join(tmp, "cfg.txt"), "w") as f:
-            f.write(CONFIG.format(**cfg))
+            f.write(text)
         out = os.path.join(tmp, "out.txt")
         subprocess.run([HARNESS, tmp + "/", "cfg.txt", out], check=True, stdin=subprocess.DEVNULL,
                        stdout=subprocess.DEVNULL)
@@ -85,7 +116,8 @@ def run_case(name, cfg):
         bind2=np.float64(B[0]),
         pos1=np.array([f[2:5] for f in F]), sp1=np.array([f[1] for f in F], dtype=np.int32),
         serno1=np.array([f[0] for f in F], dtype=np.uint64),
-        L=np.float64(cfg["L"]), wall=np.array(cfg["w"]), kf=np.float64(cfg["kf"]), kr=np.float64(cfg["kr"]))
+        L=np.float64(cfg["L"]), wall=np.array(cfg.get("w", "p")), kf=np.float64(cfg.get("kf", -1)),
+        kr=np.float64(cfg.get("kr", -1)), config=np.array(text))
     print(name, "molecules", len(D), "->", len(F), "first-order", len(U))
 
 
@@ -94,3 +126,5 @@ if __name__ == "__main__":
         sys.exit("build the reference first: make -C oracle ref")
     for k, v in CASES.items():
         run_case(k, v)
+    for k, v in PLACEMENT_CASES.items():
+        run_case(k, v, PLACEMENT_CONFIG)

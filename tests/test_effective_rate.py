@@ -44,6 +44,8 @@ CASES = {
     "same_species_and_lists": (["dimer A + A -> D 0.3", "split D -> A + A 0.2", "decay D -> 0 0.05",
                                 "birth 0 -> B 0.001"], []),
     "irreversible": (["fwd A + D -> C 10"], []),
+    "confspread": (["fwd A + B -> A + C 5"], ["confspread_radius fwd 0.3"]),
+    "bounce": (["fwd A + B -> A + B 2"], ["product_placement fwd bounce 0.6"]),
 }
 NAMES = {
     "default_placement": [(2, "fwd"), (1, "rev")],
@@ -52,6 +54,8 @@ NAMES = {
     "pgem": [(2, "fwd"), (1, "rev")],
     "same_species_and_lists": [(2, "dimer"), (1, "split"), (1, "decay"), (0, "birth")],
     "irreversible": [(2, "fwd")],
+    "confspread": [(2, "fwd")],
+    "bounce": [(2, "fwd")],
 }
 
 

@@ -215,3 +215,45 @@ def test_deterministic_step_matches_reference_recording(name):
     act = dict(pos=gpos, sp=gsp, serno=gsn, orig=gsn < (1 << 41))
     ncommon, nprod, nties = gd.compare(g, gd.reference_state(g), act, 1e-5)
     assert ncommon > 2500 and nprod >= 10
+
+
+@pytest.mark.parametrize("name", ["onestep_confspread", "onestep_bounce"])
+def test_bimolecular_placement_matches_reference_recording(name):
+    """confspread and bounce product placement (doreact, smolreact.c:2736-2805)
+    against one step recorded from the reference: every molecule keeps its
+    serial number in both placements, so each one is compared by serial
+    number — species and position (1e-5 of the side) — away from ambiguous
+    multi-candidate groups and binding-radius ties."""
+    import ctypes as C
+    import tempfile
+    from tests import golden_cases as gd
+    g = gd.load(name)
+    with tempfile.TemporaryDirectory() as d:
+        with open(d + "/cfg.txt", "w") as f:
+            f.write(str(g["config"]))
+        lib = sb.load()
+        simp = C.c_void_p()
+        assert lib.smolLoadSimFromFile((d + "/").encode(), b"cfg.txt", C.byref(simp), b"") == 0, sb.last_error()
+    s = sb.Sim(ptr=simp.value)
+    s.set_molecules(g["pos0"], g["sp0"], g["serno0"])
+    s.inject(g["serno0"], np.concatenate([g["disp"], np.full((len(g["sp0"]), 1), -1.0)], axis=1))
+    s.run_steps(1)
+    gpos, gsp, gsn = s.molecules()
+    L, periodic = g["L"], True
+    idx, moved = gd.tie_set(g)
+    tie_sn = {int(g["serno0"][i]) for i in idx}
+    ref = {int(k): i for i, k in enumerate(g["serno1"].tolist())}
+    eng = {int(k): i for i, k in enumerate(gsn.tolist())}
+    assert set(ref) == set(eng)  # nobody is created or removed
+    changed = 0
+    for k in ref:
+        if k in tie_sn:
+            continue
+        i, j = ref[k], eng[k]
+        assert g["sp1"][i] == gsp[j], (k, g["sp1"][i], gsp[j])
+        dpos = gc.min_image(g["pos1"][i] - gpos[j], L, periodic)
+        assert np.abs(dpos).max() <= 1e-5 * L, (k, g["pos1"][i], gpos[j])
+        i0 = int(np.where(g["serno0"] == k)[0][0])
+        changed += int(np.abs(gc.min_image(g["pos1"][i] - moved[i0], L, periodic)).max() > 1e-6 or
+                       g["sp1"][i] != g["sp0"][i0])
+    assert changed > 10  # reactions did happen away from ties
