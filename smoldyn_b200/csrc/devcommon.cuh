@@ -104,6 +104,7 @@ struct DevNet {
   int inject;          // deterministic mode active
   int npanel;
   double surf_eps;     // distance kept between a molecule and a panel after an interaction
+  float surf_tol;      // FP32 screening margin: eps plus the FP32 rounding of absolute positions
   int rounds;          // pair conflict-resolution rounds
   int uni_n[kMaxSpecies];
   uint8_t uni_list[kMaxSpecies][kMaxUniPerSpecies];

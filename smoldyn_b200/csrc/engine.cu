@@ -347,6 +347,38 @@ __device__ __forceinline__ double panel_cross(const DevPanel &pn, const double a
 }
 
 // Returns 1 if the molecule is absorbed; p1 is updated in place.
+// FP32 screen for the surface walk: false when the move a0 -> a1 (absolute
+// coordinates) stays more than the margin away from every panel, so no
+// crossing and no eps adjustment can occur.  Conservative: a rectangle is
+// tested as its whole plane, a sphere through the distances of the end points.
+__device__ __forceinline__ bool surface_near(const float a0[3], const float a1[3]) {
+  const float tol = c_net.surf_tol;
+  const float sx = a1[0] - a0[0], sy = a1[1] - a0[1], sz = a1[2] - a0[2];
+  const float seg = sqrtf(sx * sx + sy * sy + sz * sz);
+  for (int k = 0; k < c_net.npanel; ++k) {
+    const DevPanel &pn = c_panels[k];
+    if (pn.shape == 0) {
+      const float pos = (float)pn.pos;
+      const float s0 = a0[pn.axis] - pos, s1 = a1[pn.axis] - pos;
+      if ((s0 > tol && s1 > tol) || (s0 < -tol && s1 < -tol)) continue;
+      return true;
+    }
+    const float r = (float)pn.radius;
+    float d0 = 0.f, d1 = 0.f;
+    for (int d = 0; d < 3; ++d) {
+      const float c = (float)pn.center[d];
+      d0 += (a0[d] - c) * (a0[d] - c);
+      d1 += (a1[d] - c) * (a1[d] - c);
+    }
+    d0 = sqrtf(d0);
+    d1 = sqrtf(d1);
+    if (d0 - seg > r + tol) continue;              // the whole move stays outside
+    if (fmaxf(d0, d1) < r - tol) continue;         // the whole move stays inside
+    return true;
+  }
+  return false;
+}
+
 __device__ int surface_interact(int sp, const double p0_in[3], double p1[3], double eps, int &hits) {
   const int np = c_net.npanel;
   double p0[3] = {p0_in[0], p0_in[1], p0_in[2]};
@@ -492,11 +524,18 @@ __device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, co
     ix[d] = j;
   }
   if (SURF) {
-    double x0[3], x1[3];
-    to_abs(g, ix0, u0, x0);
-    to_abs(g, ix, u, x1);
-    if (surface_interact(sp, x0, x1, c_net.surf_eps, hits)) return 1;
-    from_abs(g, x1, ix, u);
+    float a0[3], a1[3];
+    for (int d = 0; d < 3; ++d) {
+      a0[d] = (float)ix0[d] * g.h[d] + u0[d];
+      a1[d] = (float)ix[d] * g.h[d] + u[d];
+    }
+    if (surface_near(a0, a1)) {
+      double x0[3], x1[3];
+      to_abs(g, ix0, u0, x0);
+      to_abs(g, ix, u, x1);
+      if (surface_interact(sp, x0, x1, c_net.surf_eps, hits)) return 1;
+      from_abs(g, x1, ix, u);
+    }
   }
   if (c_net.any_absorb && !c_net.inject) {
     // Absorbing walls also remove molecules that stayed inside with probability
@@ -2291,6 +2330,12 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
     for (const DevGeo &g : E.geo)
       for (int d = 0; d < 3; ++d) hmin = std::min(hmin, g.h[d]);
     D.surf_eps = 1e-5 * (double)hmin;
+    // FP32 screening before the FP64 surface walk: absolute positions up to the
+    // largest extent carry about 2^-24 relative error; 64 ulp of margin plus eps
+    double lmax = 0;
+    for (const DevGeo &g : E.geo)
+      for (int d = 0; d < 3; ++d) lmax = std::max(lmax, (double)g.n[d] * g.h[d] + g.whi[d]);
+    D.surf_tol = (float)(D.surf_eps + 64.0 * lmax / 16777216.0);
   }
 
   // ---- capacities
