@@ -1232,8 +1232,14 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_pairs_tile(KParams p) {
     if (g < n) {
       wpc[slot] = q;
       wid[slot] = qd;
-      const DevGeo &gg = geo_of<SINGLE>(p, SINGLE ? 0 : id_rep(qd));
-      wcell[slot] = global_cell(gg, __float_as_uint(q.w));
+      // box key: with one replicate the packed box coordinates identify the
+      // box; across replicates the global box index does
+      if (SINGLE) {
+        wcell[slot] = (int)__float_as_uint(q.w);
+      } else {
+        const DevGeo &gg = geo_of<SINGLE>(p, id_rep(qd));
+        wcell[slot] = global_cell(gg, __float_as_uint(q.w));
+      }
     } else {
       wcell[slot] = -1;
       wid[slot] = make_id(kDeadSpecies, 0, 0);
@@ -1302,7 +1308,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_pairs_tile(KParams p) {
     }
     // a box longer than the window continues in global memory
     if (spill) {
-      const int e = min(p.start[cell + 1], n);
+      const int gcell = SINGLE ? global_cell(geo_of<SINGLE>(p, 0), __float_as_uint(pc.w)) : cell;
+      const int e = min(p.start[gcell + 1], n);
       for (int j = wb + 64; j < e; ++j) {
         const float4 b = p.b_pc[j];
         const float vx = b.x - pc.x, vy = b.y - pc.y, vz = b.z - pc.z;
