@@ -106,6 +106,8 @@ struct DevNet {
   double surf_eps;     // distance kept between a molecule and a panel after an interaction
   float surf_tol;      // FP32 screening margin: eps plus the FP32 rounding of absolute positions
   int rounds;          // pair conflict-resolution rounds
+  uint32_t uni_any;    // species with at least one first-order reaction (bit per species)
+  uint32_t pair_any;   // species with at least one second-order reaction
   int uni_n[kMaxSpecies];
   uint8_t uni_list[kMaxSpecies][kMaxUniPerSpecies];
   uint32_t pair_mask[kMaxSpecies];    // partner species of a pair reaction
