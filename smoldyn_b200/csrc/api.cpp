@@ -383,8 +383,7 @@ enum ErrorCode smolSetSpeciesMobility(simptr sim, const char *species, enum Mole
                                       double *drift, double *difmatrix) {
   LCHECK(sim && species, ECmissing, "missing sim or species");
   LCHECK(state == MSsoln || state == MSall, ECbounds, "only solution-state species are supported");
-  LCHECK(!difmatrix, ECbounds, "anisotropic diffusion is not supported by the GPU engine");
-  LCHECK(difc >= 0, ECbounds, "difc must be >= 0");
+  LCHECK(difc >= 0 || difmatrix, ECbounds, "difc must be >= 0");
   std::vector<int> ids;
   if (!strcmp(species, "all")) for (size_t i = 1; i < sim->s.species.size(); ++i) ids.push_back((int)i);
   else {
@@ -392,9 +391,10 @@ enum ErrorCode smolSetSpeciesMobility(simptr sim, const char *species, enum Mole
     LCHECK(i > 0, ECnonexist, "species not found");
     ids.push_back(i);
   }
-  for (int i : ids) {
-    sim->s.species[i].difc = difc;
+  for (int i : ids) {  // libsmoldyn.cpp:917: difc, then drift, then the matrix (which resets difc)
+    if (difc >= 0) sim->s.species[i].difc = difc;
     if (drift) for (int d = 0; d < sim->s.dim; ++d) sim->s.species[i].drift[d] = drift[d];
+    if (difmatrix) smolb::set_species_difm(sim->s, i, difmatrix);
   }
   sim->s.need_update = true;
   return ECok;

@@ -100,6 +100,7 @@ struct DevNet {
   uint32_t key0, key1; // Philox key (seed)
   uint32_t move_ks[20]; // round keys of the move generator (key0, key1 scheduled)
   int any_drift;
+  uint32_t difm_any;   // species with an anisotropic diffusion matrix
   int any_absorb;
   int inject;          // deterministic mode active
   int npanel;

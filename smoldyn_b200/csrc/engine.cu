@@ -42,6 +42,7 @@ struct KParams {
   const DevGeo *geo;
   const float *difstep;    // [rep*nsp + sp]  sqrt(2 D dt)
   const float *driftdt;    // [(rep*nsp + sp)*3] drift*dt or null
+  const float *difm;       // [(rep*nsp + sp)*9] sqrt(2 dt) * diffusion matrix (species in difm_any)
   const uint32_t *unithr;  // [(rep*nsp + sp)*kMaxUniPerSpecies] cumulative thresholds
   const float *bind2;      // [rep*nr2 + r]
   const float *pairprob;   // [rep*nr2 + r]
@@ -496,11 +497,19 @@ __device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, co
       dsp[0] = dsp[1] = dsp[2] = 0.f;
     }
   } else {
-    const float ds = p.difstep[rep * c_net.nsp + sp];
     const uint32_t gm = c_net.gmask;
-    dsp[0] = fmul(ds, gtab[r.x & gm]);
-    dsp[1] = fmul(ds, gtab[r.y & gm]);
-    dsp[2] = fmul(ds, gtab[r.z & gm]);
+    const float g0 = gtab[r.x & gm], g1 = gtab[r.y & gm], g2 = gtab[r.z & gm];
+    if ((c_net.difm_any >> sp) & 1u) {  // anisotropic (smolmolec.c:3158-3162)
+      const float *M = p.difm + (size_t)(rep * c_net.nsp + sp) * 9;
+      dsp[0] = M[0] * g0 + M[1] * g1 + M[2] * g2;
+      dsp[1] = M[3] * g0 + M[4] * g1 + M[5] * g2;
+      dsp[2] = M[6] * g0 + M[7] * g1 + M[8] * g2;
+    } else {
+      const float ds = p.difstep[rep * c_net.nsp + sp];
+      dsp[0] = fmul(ds, g0);
+      dsp[1] = fmul(ds, g1);
+      dsp[2] = fmul(ds, g2);
+    }
     if (c_net.any_drift) {
       const float *dr = p.driftdt + (size_t)(rep * c_net.nsp + sp) * 3;
       dsp[0] = fadd(dsp[0], dr[0]);
@@ -1850,6 +1859,7 @@ class EngineImpl {
   // device memory
   DevGeo *d_geo = nullptr;
   float *d_rsearch = nullptr;
+  float *d_difm = nullptr;
   float *d_difstep = nullptr, *d_driftdt = nullptr, *d_bind2 = nullptr, *d_pairprob = nullptr,
         *d_prdpos = nullptr, *d_gtab = nullptr;
   uint32_t *d_unithr = nullptr;
@@ -1879,7 +1889,7 @@ class EngineImpl {
 
   void release() {
     invalidate_graph();
-    void *ptrs[] = {d_rsearch, d_geo, d_difstep, d_driftdt, d_bind2, d_pairprob, d_prdpos, d_gtab, d_unithr,
+    void *ptrs[] = {d_difm, d_rsearch, d_geo, d_difstep, d_driftdt, d_bind2, d_pairprob, d_prdpos, d_gtab, d_unithr,
                     d_births, d_pc[0], d_pc[1], d_ppc[0], d_ppc[1], d_id[0], d_id[1], d_pid[0],
                     d_pid[1], d_face, d_tmp, d_counts, d_step, d_cnt, d_start, d_scan_ticket, d_scan_status, d_ev, d_cand, d_best,
                     d_counters, d_spcount, d_injkey, d_injval};
@@ -1887,6 +1897,7 @@ class EngineImpl {
       if (q) cudaFree(q);
     d_rsearch = nullptr;
     d_geo = nullptr; d_difstep = d_driftdt = d_bind2 = d_pairprob = d_prdpos = d_gtab = nullptr;
+    d_difm = nullptr;
     d_unithr = nullptr; d_births = nullptr;
     d_pc[0] = d_pc[1] = d_ppc[0] = d_ppc[1] = nullptr;
     d_id[0] = d_id[1] = d_pid[0] = d_pid[1] = nullptr;
@@ -1905,6 +1916,7 @@ class EngineImpl {
     p.geo = d_geo;
     p.difstep = d_difstep;
     p.driftdt = d_driftdt;
+    p.difm = d_difm;
     p.unithr = d_unithr;
     p.bind2 = d_bind2;
     p.pairprob = d_pairprob;
@@ -2104,7 +2116,8 @@ class EngineImpl {
 
   int build_rep_tables(std::string *err) {
     const int R = (int)reps.size(), nsp = net.nspecies;
-    std::vector<float> difstep((size_t)R * nsp), driftdt((size_t)R * nsp * 3);
+    std::vector<float> difstep((size_t)R * nsp), driftdt((size_t)R * nsp * 3), difm((size_t)R * nsp * 9, 0.f);
+    uint32_t difm_any = 0;
     std::vector<uint32_t> unithr((size_t)R * nsp * kMaxUniPerSpecies, 0);
     const int nr2 = std::max(1, net.nrxn[2]), nr0 = std::max(1, net.nrxn[0]);
     std::vector<float> bind2((size_t)R * nr2, 0.f), pairprob((size_t)R * nr2, 1.f);
@@ -2117,6 +2130,11 @@ class EngineImpl {
       const RepSpec &s = reps[rp];
       for (int sp = 0; sp < nsp; ++sp) {
         difstep[(size_t)rp * nsp + sp] = (float)std::sqrt(2.0 * s.difc[sp] * dt);
+        if (s.has_difm[sp]) {  // anisotropic: step = M * sqrt(2 dt) * g (smolmolec.c:3158-3162)
+          difm_any |= 1u << sp;
+          for (int k = 0; k < 9; ++k)
+            difm[((size_t)rp * nsp + sp) * 9 + k] = (float)(s.difm[sp][k] * std::sqrt(2.0 * dt));
+        }
         for (int d = 0; d < 3; ++d) {
           driftdt[((size_t)rp * nsp + sp) * 3 + d] = (float)(s.drift[sp][d] * dt);
           if (s.drift[sp][d] != 0) any_drift = true;
@@ -2154,12 +2172,14 @@ class EngineImpl {
                   (float)s.prdpos[o][r][q][d];
     }
     dnet.any_drift = any_drift ? 1 : 0;
+    dnet.difm_any = difm_any;
     auto put = [&](void **dst, const void *src, size_t bytes) -> int {
       if (!*dst) CK(cudaMalloc(dst, bytes));
       CK(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, stream));
       return 0;
     };
     if (put((void **)&d_difstep, difstep.data(), difstep.size() * 4)) return -8;
+    if (put((void **)&d_difm, difm.data(), difm.size() * 4)) return -8;
     if (put((void **)&d_driftdt, driftdt.data(), driftdt.size() * 4)) return -8;
     if (put((void **)&d_unithr, unithr.data(), unithr.size() * 4)) return -8;
     if (put((void **)&d_bind2, bind2.data(), bind2.size() * 4)) return -8;

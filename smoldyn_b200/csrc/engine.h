@@ -66,6 +66,8 @@ struct RepSpec {
   int dim = 3;
   double difc[kMaxSpecies] = {};
   double drift[kMaxSpecies][3] = {};
+  bool has_difm[kMaxSpecies] = {};           // anisotropic diffusion matrix present
+  double difm[kMaxSpecies][9] = {};          // 3x3 row-major M (step = M * sqrt(2 dt) * gaussian)
   double uni_prob[kMaxRxn] = {};             // rxn->prob for order 1 (smolreact.c:1333-1357)
   double bind2[kMaxRxn] = {};                // rxn->bindrad2 for order 2
   double pair_prob[kMaxRxn] = {};            // rxn->prob for order 2 (1 unless set)

@@ -400,6 +400,19 @@ double calc_rate(const Sim &sim, int order, int r, double *pgem) {
   return ans;
 }
 
+void set_species_difm(Sim &sim, int sp, const double *m) {
+  SpeciesDef &x = sim.species[sp];
+  const int dim = sim.dim;
+  x.has_difm = true;
+  for (int k = 0; k < 9; ++k) x.difm[k] = 0;
+  for (int r = 0; r < dim; ++r)
+    for (int c = 0; c < dim; ++c) x.difm[3 * r + c] = m[dim * r + c];
+  double tr = 0;  // trace(M*M), as molsetdifm computes it
+  for (int r = 0; r < dim; ++r)
+    for (int c = 0; c < dim; ++c) tr += x.difm[3 * r + c] * x.difm[3 * c + r];
+  x.difc = tr / dim;
+}
+
 int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err) {
   *net = NetSpec();
   *rep = RepSpec();
@@ -448,6 +461,8 @@ int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err) {
   }
   for (size_t i = 0; i < sim.species.size(); ++i) {
     rep->difc[i] = sim.species[i].difc;
+    rep->has_difm[i] = sim.species[i].has_difm;
+    for (int k = 0; k < 9; ++k) rep->difm[i][k] = sim.species[i].difm[k];
     for (int d = 0; d < 3; ++d) rep->drift[i][d] = (d < sim.dim) ? sim.species[i].drift[d] : 0;
   }
   choose_grid(sim, (long long)sim.pend_sp.size(), rep->ncell);
@@ -587,6 +602,15 @@ int read_config_statement(Sim &sim, const std::string &word, const std::string &
     if (species_arg(sim, w[0], &ids)) { if (err) *err = "difc: unknown species " + w[0]; return -3; }
     if (!parse_double(w[1], &v)) { if (err) *err = "difc: bad value"; return -7; }
     for (int i : ids) sim.species[i].difc = v;
+    sim.need_update = true;
+  } else if (word == "difm") {  // smolsim.cpp:863: species then dim*dim values
+    if (!need(1 + (size_t)sim.dim * sim.dim)) return -7;
+    std::vector<int> ids;
+    if (species_arg(sim, w[0], &ids)) { if (err) *err = "difm: unknown species " + w[0]; return -3; }
+    double m[9];
+    for (int k = 0; k < sim.dim * sim.dim; ++k)
+      if (!parse_double(w[1 + k], &m[k])) { if (err) *err = "difm: bad value"; return -7; }
+    for (int i : ids) set_species_difm(sim, i, m);
     sim.need_update = true;
   } else if (word == "drift") {
     if (!need(1 + (size_t)sim.dim)) return -7;

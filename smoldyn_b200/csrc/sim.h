@@ -15,7 +15,10 @@ struct SpeciesDef {
   std::string name;
   double difc = 0;
   double drift[3] = {0, 0, 0};
+  bool has_difm = false;   // anisotropic diffusion (difm statement, smolmolec.c:833)
+  double difm[9] = {};     // matrix M, row-major in a 3x3 layout: step = M * sqrt(2 dt) * gaussian
 };
+
 
 // One reaction (smoldyn.h:389 rxnstruct subset).
 struct RxnDef {
@@ -96,6 +99,9 @@ struct Sim {
   double rand_u01();
 };
 
+// molsetdifm (smolmolec.c:833-867): set the diffusion matrix of a species;
+// its difc becomes trace(M*M)/dim.  m is dim x dim, row-major.
+void set_species_difm(Sim &sim, int sp, const double *m);
 // Restatements of the reference's parameter derivation.
 int derive_reaction_params(Sim &sim, std::string *err);
 // rxncalcrate (smolreact.c:1592-1680): effective rate from derived parameters.

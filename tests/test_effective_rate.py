@@ -46,6 +46,7 @@ CASES = {
     "irreversible": (["fwd A + D -> C 10"], []),
     "confspread": (["fwd A + B -> A + C 5"], ["confspread_radius fwd 0.3"]),
     "bounce": (["fwd A + B -> A + B 2"], ["product_placement fwd bounce 0.6"]),
+    "anisotropic": (["fwd A + B -> C 1"], ["difm A 1 0.5 0 0 2 0 0 0 0.5"]),
 }
 NAMES = {
     "default_placement": [(2, "fwd"), (1, "rev")],
@@ -56,6 +57,7 @@ NAMES = {
     "irreversible": [(2, "fwd")],
     "confspread": [(2, "fwd")],
     "bounce": [(2, "fwd")],
+    "anisotropic": [(2, "fwd")],
 }
 
 

@@ -257,3 +257,30 @@ def test_bimolecular_placement_matches_reference_recording(name):
         changed += int(np.abs(gc.min_image(g["pos1"][i] - moved[i0], L, periodic)).max() > 1e-6 or
                        g["sp1"][i] != g["sp0"][i0])
     assert changed > 10  # reactions did happen away from ties
+
+
+def test_anisotropic_diffusion_covariance():
+    """difm (smolmolec.c:3158-3162): each step is M * sqrt(2 dt) * g, so the
+    displacement covariance after time t is 2 t M M^T.  20000 molecules in a
+    box too large for the walls to matter; every entry within 5 % of the
+    largest (the sampling error of a variance at this count is about 1 %)."""
+    import ctypes as C
+    L, n, dt, steps = 1000.0, 20000, 0.01, 100
+    s = sb.Sim(3, (0, 0, 0), (L, L, L))
+    s.add_species("A", 1.0)
+    for d in range(3):
+        s.boundary(d, -1, "r")
+    s.set_times(0, 1e6, dt)
+    s.seed(17)
+    M = np.array([[1.0, 0.5, 0.0], [0.0, 2.0, 0.0], [0.0, 0.0, 0.5]])
+    mflat = np.ascontiguousarray(M.ravel())
+    assert s.lib.smolSetSpeciesMobility(s.ptr, b"A", sb.MSsoln, -1.0, None, sb.dptr(mflat)) == 0
+    rng = np.random.default_rng(5)
+    pos0 = rng.uniform(400, 600, size=(n, 3))
+    s.set_molecules(pos0, np.ones(n, dtype=np.int32), np.arange(1, n + 1, dtype=np.uint64))
+    s.run_steps(steps)
+    pos1, _, sn = s.molecules()
+    disp = pos1[np.argsort(sn)] - pos0
+    cov = disp.T @ disp / n
+    expect = 2 * steps * dt * M @ M.T
+    assert np.abs(cov - expect).max() <= 0.05 * np.abs(expect).max(), (cov, expect)
