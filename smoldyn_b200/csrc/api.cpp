@@ -173,9 +173,12 @@ ErrorCode run_until(Sim &s, double stop, const char *func, bool one_step) {
       do_commands(s, false);
     }
   }
-  const int st = s.eng->status_flags();
+  // a single step checks the previous step's status (no wait for this one);
+  // longer runs and the end of the simulation check the current one
+  const bool last = s.time >= s.tstop;
+  const int st = (one_step && !last) ? s.eng->status_flags_lagged() : s.eng->status_flags();
   if (st) return set_error(func, ECerror, "engine capacity exceeded (status flags " + std::to_string(st) + ")");
-  if (s.time >= s.tstop) {
+  if (last) {
     do_end_commands(s);
     return set_error(func, ECnotify, "Simulation complete");
   }

@@ -1885,7 +1885,20 @@ class EngineImpl {
   ~EngineImpl() {
     release();
     for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
+    for (int k = 0; k < 2; ++k)
+      if (st_ev[k]) cudaEventDestroy(st_ev[k]);
+    if (h_status) cudaFreeHost(h_status);
   }
+
+  // status word read one call late (see Engine::status_flags_lagged)
+  int *h_status = nullptr;
+  cudaEvent_t st_ev[2] = {nullptr, nullptr};
+  bool st_pending[2] = {false, false};
+  int st_slot = 0;
+  // species counts of the current state (valid while the step count and the
+  // upload generation are unchanged)
+  std::vector<long long> counts_cache;
+  long long counts_step = -1, counts_gen = -1, upload_gen = 0;
 
   void release() {
     invalidate_graph();
@@ -2026,6 +2039,7 @@ class EngineImpl {
   // Rebin the staged molecules (product buffer 0) into the sorted buffer and
   // count species.
   int finish_upload(long long n, std::string *err) {
+    ++upload_gen;
     int staged = (int)n;
     parity = 0;
     CK(cudaMemcpyAsync(d_counts + 2, &staged, sizeof(int), cudaMemcpyHostToDevice, stream));
@@ -2622,10 +2636,38 @@ long long Engine::total_molecules() {
 
 int Engine::species_counts(std::vector<long long> *out, std::string *err) {
   EngineImpl &E = *impl_;
+  if (E.counts_step == E.nsteps && E.counts_gen == E.upload_gen &&
+      E.counts_cache.size() == E.reps.size() * E.net.nspecies) {  // nothing ran since the last read
+    *out = E.counts_cache;
+    return 0;
+  }
   out->assign(E.reps.size() * E.net.nspecies, 0);
   CK(cudaMemcpyAsync(out->data(), E.d_spcount, out->size() * sizeof(long long), cudaMemcpyDeviceToHost, E.stream));
   CK(cudaStreamSynchronize(E.stream));
+  E.counts_cache = *out;
+  E.counts_step = E.nsteps;
+  E.counts_gen = E.upload_gen;
   return 0;
+}
+
+int Engine::status_flags_lagged() {
+  EngineImpl &E = *impl_;
+  if (!E.h_status) {
+    if (cudaMallocHost(&E.h_status, 2 * sizeof(int)) != cudaSuccess) { E.h_status = nullptr; return status_flags(); }
+    for (int k = 0; k < 2; ++k) cudaEventCreateWithFlags(&E.st_ev[k], cudaEventDisableTiming);
+  }
+  const int prev = E.st_slot ^ 1;
+  int st = 0;
+  if (E.st_pending[prev]) {
+    cudaEventSynchronize(E.st_ev[prev]);
+    st = E.h_status[prev];
+    E.st_pending[prev] = false;
+  }
+  cudaMemcpyAsync(&E.h_status[E.st_slot], E.d_counts + 6, sizeof(int), cudaMemcpyDeviceToHost, E.stream);
+  cudaEventRecord(E.st_ev[E.st_slot], E.stream);
+  E.st_pending[E.st_slot] = true;
+  E.st_slot ^= 1;
+  return st;
 }
 
 int Engine::stats(EngineStats *s, std::string *err) {

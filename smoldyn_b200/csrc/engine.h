@@ -113,6 +113,10 @@ class Engine {
   long long total_molecules();
   int stats(EngineStats *s, std::string *err);
   int status_flags();
+  // Status of the previous call's step, without waiting for the current one:
+  // copies the status word asynchronously and returns the copy made by the
+  // previous call (0 on the first call).
+  int status_flags_lagged();
   // Update rate-derived parameters of every replicate (no reallocation).
   int update_reps(const std::vector<RepSpec> &reps, std::string *err);
   // Deterministic mode: per-serno displacements for the next step only.

@@ -102,7 +102,11 @@ int derive(smolb_ens &e, std::string *err) {
   smolb::RepSpec base;
   if (smolb::build_engine_specs(T, &e.net, &base, err)) return -6;
   const int R = e.nrep;
-  e.reps.assign(R, base);
+  // A rate update of a built ensemble keeps each replicate's rate-free fields
+  // and rewrites the rate-dependent ones below; copying the template's whole
+  // parameter set into every replicate dominated the update time of large
+  // ensembles.
+  if (e.need_rebuild || !e.eng || (int)e.reps.size() != R) e.reps.assign(R, base);
   const double dt = T.dt;
   // zeroth and first order, per replicate (same formulas as derive_reaction_params)
   for (int k = 0; k < R; ++k) {
