@@ -151,6 +151,7 @@ struct DevPanel {
   double radius;
   int act_front, act_back;   // default action per face: 0 reflect 1 transmit 2 absorb
   uint32_t abs_front, abs_back, tr_front, tr_back, rf_front, rf_back;  // per-species overrides
+  float posf, radiusf, centerf[3];   // FP32 copies for the screening test
 };
 
 struct Event {      // one reaction or birth; products are placed by k_products

@@ -359,15 +359,15 @@ __device__ __forceinline__ bool surface_near(const float a0[3], const float a1[3
   for (int k = 0; k < c_net.npanel; ++k) {
     const DevPanel &pn = c_panels[k];
     if (pn.shape == 0) {
-      const float pos = (float)pn.pos;
+      const float pos = pn.posf;
       const float s0 = a0[pn.axis] - pos, s1 = a1[pn.axis] - pos;
       if ((s0 > tol && s1 > tol) || (s0 < -tol && s1 < -tol)) continue;
       return true;
     }
-    const float r = (float)pn.radius;
+    const float r = pn.radiusf;
     float d0 = 0.f, d1 = 0.f;
     for (int d = 0; d < 3; ++d) {
-      const float c = (float)pn.center[d];
+      const float c = pn.centerf[d];
       d0 += (a0[d] - c) * (a0[d] - c);
       d1 += (a1[d] - c) * (a1[d] - c);
     }
@@ -677,7 +677,7 @@ __device__ void births(const KParams &p, uint32_t step);
 // molecule leaves the system), and the histogram of destination boxes.
 // rebin_only: no motion and no reactions (used after uploads).
 template <bool SINGLE, bool SURF>
-__global__ void __launch_bounds__(256) k_move(KParams p, int rebin_only) {
+__global__ void __launch_bounds__(256, 4) k_move(KParams p, int rebin_only) {
   extern __shared__ float s_gtab[];
   pdl_launch_dependents();
   const float *gtab = rebin_only ? p.gtab : stage_gtab(p, s_gtab);  // constant data: before the wait
@@ -2461,6 +2461,9 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
         dp.center[d] = ps.center[d] - s0.lo[d];
       }
       dp.radius = ps.radius;
+      dp.posf = (float)dp.pos;
+      dp.radiusf = (float)dp.radius;
+      for (int d = 0; d < 3; ++d) dp.centerf[d] = (float)dp.center[d];
       dp.act_front = ps.action_front;
       dp.act_back = ps.action_back;
       dp.abs_front = ps.absorb_front_mask;
