@@ -342,11 +342,12 @@ def main():
         e2e = run_e2e(sb, args, rank, world, dist, barrier)
 
     # ---- batched ensemble and surrogate sweep (extra workloads, same GPU)
-    batched = surrogate = surfaces = None
+    batched = surrogate = surfaces = rdf = None
     if not args.no_batched:
         batched = run_batched(sb, torch, args, rank)
         surrogate = run_surrogate(sb, torch, args, rank)
         surfaces = run_surfaces(sb, torch, args, rank)
+        rdf = run_rdf_tables(sb, args, rank, world)
 
     # ---- CPU baseline (rank 0, single GPU run only)
     cpu = None
@@ -369,6 +370,7 @@ def main():
             "e2e": e2e, "gpu_launches": int(launches),
             "roofline": roof, "step_roofline_frac": step_frac, "kernels": kernels, "cpu_baseline": cpu,
             "clocks": ck, "batched": batched, "batched_surrogate": surrogate, "surfaces": surfaces,
+            "rdf_tables": rdf,
         }
         print(json.dumps(line))
     if dist is not None:
@@ -657,6 +659,77 @@ def run_surfaces(sb, torch, args, rank):
         return out
     finally:
         shutil.rmtree(d, ignore_errors=True)
+
+
+def run_rdf_tables(sb, args, rank, world):
+    """Radial-distribution-function solver: regenerate the irreversible rate
+    table (600 radial points, eps 1e-5, upward and downward sweeps averaged)
+    and the reversible one (500 points, 16 unbinding radii) on the device.
+    The work unit is one solver iteration (a diffusion step over the grid,
+    n^2 Green's-function pairs, plus an absorption); the CPU baseline times
+    the reference's own rdfsteadystate (compiled from rxnparam.c) on the first
+    two solves of the upward 600-point sweep."""
+    import ctypes as C
+    import time
+    out = {"unit": "rdf iterations/s (600-point grid)"}
+    t0 = time.perf_counter()
+    flux, iters = sb.rdf_table("i", 600, 1e-5, "a")
+    t1 = time.perf_counter()
+    yi = sb.rxn_table("yi")
+    out.update({"value": float(iters.sum()) / (t1 - t0), "table_s": t1 - t0, "iterations": int(iters.sum()),
+                "max_dev_vs_compiled_table": float(np.max(np.abs(flux.reshape(-1) - yi)))})
+    t0 = time.perf_counter()
+    flux_r, iters_r = sb.rdf_table("r", 500, 1e-5, "a")
+    t1 = time.perf_counter()
+    out["reversible_table"] = {"table_s": t1 - t0, "iterations": int(iters_r.sum()), "max_dev_vs_compiled_table":
+                               float(np.max(np.abs(flux_r.reshape(-1) - sb.rxn_table("yr"))))}
+    if rank != 0 or world != 1 or args.no_cpu_baseline:
+        return out
+    here = os.path.dirname(os.path.abspath(__file__))
+    so = os.path.join(here, "oracle", "_ref", "librxnparam_ref.so")
+    if not os.path.exists(so):
+        out["cpu_baseline"] = {"value": None, "sample": "reference rxnparam library not built"}
+        return out
+    ref = C.CDLL(so)
+    ref.rdfsteadystate.restype = C.c_double
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    n = 600
+    r = np.zeros(n)
+    i, dr = 1, 10.0 / n
+    while r[i - 1] < 1:  # table grid, rxnparam.c:965-971
+        r[i] = r[i - 1] + dr
+        i += 1
+    r[i - 1], r[i] = 0.9999, 1.0001
+    for k in range(i + 1, n):
+        r[k] = r[k - 1] + dr
+    trial = np.where(r < 1, 0.0, 1.0 - 1.0 / np.maximum(r, 1e-9))
+    steps = [np.exp(-3.0), np.exp(-3.0) * np.exp(0.2)]
+
+    def sweep(fn, extra):
+        g, d = np.ascontiguousarray(trial.copy()), np.zeros(n)
+        for st in steps:
+            fn(dp(r), dp(g), dp(d), n, C.c_double(st), C.c_double(1.0), C.c_double(-1.0), C.c_double(1e-5),
+               C.c_double(1.0), *extra())
+    t0 = time.perf_counter()
+    sweep(ref.rdfsteadystate, lambda: ())
+    secs = time.perf_counter() - t0
+    # iteration counts from the oracle's restatement, bit-identical to the
+    # reference's rdfsteadystate on these inputs
+    ora = C.CDLL(os.path.join(here, "oracle", "_ref", "liboracle.so"))
+    ora.ora_rdf_steady.restype = C.c_double
+    counts = []
+
+    def counted():
+        it = C.c_int()
+        counts.append(it)
+        return (C.byref(it),)
+    sweep(ora.ora_rdf_steady, counted)
+    it_cpu = sum(c.value for c in counts)
+    out["cpu_baseline"] = {"value": it_cpu / secs, "unit": out["unit"], "cores": 1, "kind": "reference",
+                           "sample": "reference rdfsteadystate (rxnparam.c) on the first two solves of the upward "
+                                     "600-point sweep: %d iterations in %.2f s" % (it_cpu, secs),
+                           "table_s_extrapolated": out["iterations"] / (it_cpu / secs)}
+    return out
 
 
 def run_e2e(sb, args, rank, world, dist, barrier):

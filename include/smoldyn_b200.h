@@ -212,6 +212,41 @@ enum ErrorCode smolgpuSolveRadiiNoAlloc(int mode, long long n, const double *rat
 double smolgpuBindingRadiusHost(double rate, double dt, double difc, double b, int rel);
 double smolgpuUnbindingRadiusHost(double pgem, double dt, double difc, double a);
 
+/* Radial-distribution-function solver on the device: the numerical method
+ * behind the rxnparam tables (rxnparam.c:784-1114), in reduced units
+ * (binding radius 1 for the sweeps).
+ *
+ * smolgpuRdfTable replaces rdfmaketable (rxnparam.c:920) and, with probs,
+ * rdfmaketableprob (rxnparam.c:1008), without their terminal dialogue:
+ *   mode 'i' irreversible (1 row), 'r' reversible with unbinding radius
+ *   b = 1 .. e^3 (16 rows), 'b' reversible with b = 0 .. 1 (11 rows);
+ *   n radial points (10..4000), eps the relative flux tolerance;
+ *   dir 'u' step lengths e^-3 .. e^3 increasing, 'd' decreasing, or 'a' both
+ *   sweeps averaged and listed in decreasing order (the form of the tables in
+ *   numrxnrate, rxnparam.c:58-76);
+ *   probs: nprob reaction probabilities (NULL: one probability of 1).
+ * flux[(row*nprob + p)*31 + k] receives the steady-state flux (the reduced
+ * rate; -1 where rdfsteadystate gives up, and for the rest of that sweep as in
+ * the reference), iters (optional) the iteration counts, *nrows (optional)
+ * the row count.  flux must hold rows*nprob*31 doubles. */
+enum ErrorCode smolgpuRdfTable(char mode, int n, double eps, char dir, int nprob, const double *probs,
+                               double *flux, int *iters, int *nrows);
+/* Batched rdfsteadystate (rxnparam.c:898): nsolve independent solves on n-point
+ * grids r (nsolve*n; r[0] >= 0, the others > 0) from trial profiles rdfa
+ * (in/out, nsolve*n; out: after the last absorption) with step[i], binding
+ * radius a[i], unbinding radius b[i] (< 0: irreversible) and probability
+ * prob[i].  rdfd (optional, nsolve*n) receives the profile after the last
+ * diffusion step, flux[i] the steady-state flux or -1, iters (optional) the
+ * iteration counts. */
+enum ErrorCode smolgpuRdfSteadyState(int nsolve, int n, const double *r, double *rdfa, double *rdfd,
+                                     const double *step, const double *a, const double *b, const double *prob,
+                                     double eps, double *flux, int *iters);
+/* The rate tables compiled into this library (numrxnrate, numrxnrateprob;
+ * rxnparam.c:58-76, 172-490): name "yi", "yr", "yb", "kirr", "krev" or "kb".
+ * Copies min(cap, length) values to out (out may be NULL) and returns the
+ * table length, or -1 for an unknown name. */
+int smolgpuRxnTable(const char *name, double *out, int cap);
+
 /* ==== Part 2b: ensembles of independent replicates ====================== */
 /* One engine runs nrep independent copies of a template simulation (its
  * species, reactions, product placement, walls, dt and seed), each with its

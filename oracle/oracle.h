@@ -31,6 +31,20 @@ double ora_bindingradiusprob(double rate, double dt, double difc, double b, int 
                              double *probptr);
 double ora_unbindingradius(double pgem, double dt, double difc, double a);
 
+/* rxnparam.c:719-1114: the radial-distribution-function solver that produced
+ * the tables above; see rdf_oracle.c. */
+double ora_erfc_nr(double x);
+double ora_rdf_absorb(const double *r, double *rdf, int n, double bindrad, double prob);
+void ora_rdf_diffuse(const double *r, const double *rdfa, double *rdfd, int n, double step);
+void ora_rdf_reverse(const double *r, double *rdf, int n, double step, double b, double flux);
+double ora_rdf_steady(const double *r, double *rdfa, double *rdfd, int n, double step, double a, double b,
+                      double eps, double prob, int *iters);
+int ora_rdf_grid(int mode, int n, double b, double *r);
+int ora_rdf_rows(int mode, double *bvals);
+int ora_rdf_steps(int dir, double *svals);
+int ora_rdf_table(int mode, int n, double eps, int dir, int nprob, const double *probs, double *flux,
+                  int *iters, double *rbuf, double *rdfa, double *rdfd);
+
 /* One deterministic time step in the reference's operator order
  * (smolsim.cpp:2607-2692) with injected displacements; see engine_oracle.c. */
 #define ORA_MAXSP 32

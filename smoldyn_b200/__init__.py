@@ -96,6 +96,10 @@ PROTOTYPES = {
     "smolgpuSolveRadiiNoAlloc": (C.c_int, [C.c_int, C.c_longlong, _dp, C.c_double, _dp, _dp, C.c_int, _dp]),
     "smolgpuBindingRadiusHost": (C.c_double, [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int]),
     "smolgpuUnbindingRadiusHost": (C.c_double, [C.c_double, C.c_double, C.c_double, C.c_double]),
+    "smolgpuRdfTable": (C.c_int, [C.c_char, C.c_int, C.c_double, C.c_char, C.c_int, _dp, _dp, _ip, _ip]),
+    "smolgpuRdfSteadyState": (C.c_int, [C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp, C.c_double, _dp,
+                                        _ip]),
+    "smolgpuRxnTable": (C.c_int, [C.c_char_p, _dp, C.c_int]),
     "smolgpuNewEnsemble": (_vp, [_sim, C.c_int]),
     "smolgpuEnsembleSetBoxes": (C.c_int, [_vp, _dp, _dp]),
     "smolgpuEnsembleSetRates": (C.c_int, [_vp, C.c_char_p, _dp]),
@@ -149,6 +153,10 @@ def load():
 
 def dptr(a):
     return a.ctypes.data_as(_dp)
+
+
+def iptr(a):
+    return a.ctypes.data_as(_ip)
 
 
 def last_error():
@@ -510,6 +518,56 @@ def solve_radii_device(mode, rate, dt, difc, b, rel=0):
     b = np.ascontiguousarray(b, dtype=np.float64)
     out = np.zeros_like(rate)
     check(lib.smolgpuSolveRadii(mode, len(rate), dptr(rate), dt, dptr(difc), dptr(b), rel, dptr(out)))
+    return out
+
+
+RDF_ROWS = {"i": 1, "r": 16, "b": 11}
+RDF_STEPS = 31
+
+
+def rdf_table(mode, n, eps, direction, probs=None):
+    """smolgpuRdfTable: steady-state reaction fluxes over the table sweep of
+    rdfmaketable / rdfmaketableprob (rxnparam.c:920, 1008) on the device.
+    Returns (flux, iters), each [rows, nprob, 31]."""
+    lib = load()
+    pr = None if probs is None else np.ascontiguousarray(probs, dtype=np.float64)
+    nprob = 1 if pr is None else len(pr)
+    rows = RDF_ROWS[mode]
+    flux = np.zeros(rows * nprob * RDF_STEPS)
+    iters = np.zeros(rows * nprob * RDF_STEPS, dtype=np.int32)
+    nrows = C.c_int()
+    check(lib.smolgpuRdfTable(mode.encode(), n, eps, direction.encode(), nprob, None if pr is None else dptr(pr),
+                              dptr(flux), iptr(iters), C.byref(nrows)))
+    assert nrows.value == rows
+    return flux.reshape(rows, nprob, RDF_STEPS), iters.reshape(rows, nprob, RDF_STEPS)
+
+
+def rdf_steady_state(r, rdfa, step, a, b, prob, eps):
+    """smolgpuRdfSteadyState: batched rdfsteadystate (rxnparam.c:898).
+    r, rdfa: [nsolve, n]; step, a, b, prob: [nsolve].  Returns
+    (flux, rdfa_out, rdfd_out, iters)."""
+    lib = load()
+    r = np.ascontiguousarray(np.atleast_2d(r), dtype=np.float64)
+    ra = np.array(np.atleast_2d(rdfa), dtype=np.float64, order="C")
+    nsolve, n = r.shape
+    vec = lambda v: np.ascontiguousarray(np.broadcast_to(np.asarray(v, dtype=np.float64), (nsolve,)))
+    step, a, b, prob = vec(step), vec(a), vec(b), vec(prob)
+    rd = np.zeros_like(ra)
+    flux = np.zeros(nsolve)
+    iters = np.zeros(nsolve, dtype=np.int32)
+    check(lib.smolgpuRdfSteadyState(nsolve, n, dptr(r), dptr(ra), dptr(rd), dptr(step), dptr(a), dptr(b), dptr(prob),
+                                    eps, dptr(flux), iptr(iters)))
+    return flux, ra, rd, iters
+
+
+def rxn_table(name):
+    """smolgpuRxnTable: a rate table compiled into the library."""
+    lib = load()
+    n = lib.smolgpuRxnTable(name.encode(), None, 0)
+    if n < 0:
+        raise KeyError(name)
+    out = np.zeros(n)
+    lib.smolgpuRxnTable(name.encode(), dptr(out), n)
     return out
 
 

@@ -865,6 +865,24 @@ double smolgpuUnbindingRadiusHost(double pgem, double dt, double difc, double a)
   return smolb::rxnp::unbindingradius(pgem, dt, difc, a);
 }
 
+int smolgpuRxnTable(const char *name, double *out, int cap) {
+  using namespace smolb::rxnp;
+  if (!name) return -1;
+  const std::string nm(name);
+  const double *t = nullptr;
+  int len = 0;
+  if (nm == "yi") t = h_yi, len = SMOLB_TAB_YI_LEN;
+  else if (nm == "yr") t = h_yr, len = SMOLB_TAB_YR_LEN;
+  else if (nm == "yb") t = h_yb, len = SMOLB_TAB_YB_LEN;
+  else if (nm == "kirr") t = h_kirr, len = SMOLB_TAB_KIRR_LEN;
+  else if (nm == "krev") t = h_krev, len = SMOLB_TAB_KREV_LEN;
+  else if (nm == "kb") t = h_kb, len = SMOLB_TAB_KB_LEN;
+  else return -1;
+  if (out)
+    for (int i = 0; i < len && i < cap; ++i) out[i] = t[i];
+  return len;
+}
+
 }  // extern "C"
 
 // Shared with ensemble.cpp and surrogate.cu: record an error in the
