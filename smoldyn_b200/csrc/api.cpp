@@ -50,16 +50,36 @@ ErrorCode from_rc(int rc) {
 
 long long total_pending(const Sim &s) { return (long long)s.pend_sp.size(); }
 
-// Download molecules from the engine into the pending lists (before a rebuild).
+// Bring every registered meansqrdisp tracker up to date and copy its last
+// unwrapped positions to the host, before the engine is re-initialised.
+int msd_save(Sim &s, std::string *err) {
+  if (!s.eng) return 0;
+  for (auto &kv : s.msd) {
+    smolb::MsdState &m = kv.second;
+    if (m.handle < 0) continue;
+    int rc = s.eng->msd_update(m.handle, -1, nullptr, nullptr, nullptr, err);
+    if (!rc) rc = s.eng->msd_last(m.handle, &m.last, err);
+    if (rc) return rc;
+    m.handle = -1;
+    m.since = 0;
+  }
+  return 0;
+}
+
+// Download molecules from the engine into the pending lists (before a
+// rebuild); serial numbers are kept, as the reference keeps them.
 int pull_molecules(Sim &s, std::string *err) {
   if (!s.eng || !s.started) return 0;
+  int rc = msd_save(s, err);
+  if (rc) return rc;
   std::vector<double> pos;
   std::vector<int> sp, rep;
   std::vector<uint64_t> serno;
-  int rc = s.eng->get_molecules(&pos, &sp, &rep, &serno, err);
+  rc = s.eng->get_molecules(&pos, &sp, &rep, &serno, err);
   if (rc) return rc;
   s.pend_pos = pos;
   s.pend_sp = sp;
+  s.pend_serno = serno;
   s.started = false;
   return 0;
 }
@@ -85,10 +105,18 @@ ErrorCode update_sim(Sim &s, const char *func) {
     rc = s.eng->init(net, {rep}, s.dt, (uint64_t)s.seed, cap, &err);
     if (!rc) rc = s.eng->set_tuning(s.tuning, &err);
     if (rc) { s.eng.reset(); return set_error(func, from_rc(rc), err); }
-    rc = s.eng->set_molecules(n, s.pend_pos.data(), s.pend_sp.data(), nullptr, nullptr, &err);
+    std::vector<uint64_t> sn;
+    if (!s.pend_serno.empty()) {  // serials kept from a pull; molecules added since get new ones
+      sn.assign((size_t)n, 0);
+      for (size_t k = 0; k < s.pend_serno.size() && k < sn.size(); ++k) sn[k] = s.pend_serno[k];
+    }
+    rc = s.eng->set_molecules(n, s.pend_pos.data(), s.pend_sp.data(), nullptr, sn.empty() ? nullptr : sn.data(), &err);
+    // a rebuild mid-run continues the random streams where they were
+    if (!rc && s.steps > 0) rc = s.eng->set_rng_step((uint64_t)s.steps, &err);
     if (rc) { s.eng.reset(); return set_error(func, from_rc(rc), err); }
     s.pend_pos.clear();
     s.pend_sp.clear();
+    s.pend_serno.clear();
     s.started = true;
   } else {
     rc = s.eng->update_reps({rep}, &err);
@@ -113,7 +141,110 @@ void record_molcount(Sim &s, const std::string &dataname) {
   s.outdata[dataname].push_back(row);
 }
 
-// runtime commands (smolcmd.c docommand subset: molcount)
+// Steps over which a molecule of species sp stays within half a period of
+// every periodic axis with overwhelming probability: 10 standard deviations
+// of its diffusion plus its drift must stay below L/2.  0 when no axis wraps.
+long long msd_interval(const Sim &s, int sp) {
+  long long best = 0;
+  const smolb::SpeciesDef &S = s.species[sp];
+  for (int d = 0; d < s.dim; ++d) {
+    if (s.btype[d][0] != 'p' || s.btype[d][1] != 'p') continue;
+    double var = 2.0 * S.difc * s.dt;  // per-step variance along d
+    if (S.has_difm) {
+      var = 0;
+      for (int k = 0; k < 3; ++k) var += 2.0 * s.dt * S.difm[3 * d + k] * S.difm[3 * d + k];
+    }
+    const double a = std::fabs(S.drift[d]) * s.dt, b = 10.0 * std::sqrt(var), c = (s.hi[d] - s.lo[d]) / 2.0;
+    double rk;
+    if (a > 0)
+      rk = (-b + std::sqrt(b * b + 4 * a * c)) / (2 * a);
+    else if (b > 0)
+      rk = c / b;
+    else
+      continue;
+    const long long k = std::max<long long>(1, (long long)std::floor(rk * rk));
+    best = best ? std::min(best, k) : k;
+  }
+  return best;
+}
+
+// Register a tracker with the current engine if it has none yet.
+int msd_register(Sim &s, smolb::MsdState &m, std::string *err) {
+  if (m.handle >= 0) return 0;
+  const int h = s.eng->msd_track(m.species, (long long)m.keys.size(), m.keys.data(), m.start.data(), m.last.data(), err);
+  if (h < 0) return h;
+  m.handle = h;
+  m.since = 0;
+  return 0;
+}
+
+// meansqrdisp species dim data (cmdmeansqrdisp, smolcmd.c:2505-2606): on the
+// first run record the molecules of the species; on every run append
+// (time, <r^2>, <r^4>) over those still present, r measured from the
+// recorded positions with periodic wraps undone.
+void record_meansqrdisp(Sim &s, const smolb::Command &c) {
+  smolb::MsdState &m = s.msd[c.text];
+  if (m.failed || !s.eng) return;
+  std::string err;
+  if (!m.started) {
+    char name[256] = {0}, spn[256] = {0}, dimstr[256] = {0}, data[256] = {0};
+    const int nw = sscanf(c.text.c_str(), "%255s %255s %255s %255s", name, spn, dimstr, data);
+    std::string spname(spn);
+    const size_t paren = spname.find('(');
+    if (paren != std::string::npos) spname = spname.substr(0, paren);  // solution state only
+    m.species = s.species_index(spname);
+    const std::string ds(dimstr);
+    m.msddim = ds == "all" ? -1 : (ds == "0" || ds == "x") ? 0 : (ds == "1" || ds == "y") ? 1 : (ds == "2" || ds == "z") ? 2 : 3;
+    m.dataname = nw >= 4 ? data : "meansqrdisp";
+    if (nw < 3 || m.species <= 0 || m.msddim >= s.dim) { m.failed = true; return; }
+    std::vector<double> pos;
+    std::vector<int> sp, rep;
+    std::vector<uint64_t> sn;
+    if (s.eng->get_molecules(&pos, &sp, &rep, &sn, &err)) { m.failed = true; return; }
+    for (size_t i = 0; i < sp.size(); ++i) {
+      if (sp[i] != m.species) continue;
+      m.keys.push_back(((uint64_t)rep[i] << 42) | sn[i]);
+      for (int d = 0; d < 3; ++d) m.start.push_back(pos[3 * i + d]);
+    }
+    if (m.keys.empty()) { m.failed = true; return; }  // "no molecules to track"
+    m.last = m.start;
+    m.every = msd_interval(s, m.species);
+    m.started = true;
+  }
+  if (msd_register(s, m, &err)) { m.failed = true; return; }
+  double s2 = 0, s4 = 0;
+  long long cnt = 0;
+  if (s.eng->msd_update(m.handle, m.msddim, &s2, &s4, &cnt, &err)) { m.failed = true; return; }
+  m.since = 0;
+  s.outdata[m.dataname].push_back({s.time, s2 / (double)cnt, s4 / (double)cnt});
+}
+
+// Advance n steps, in chunks short enough that every meansqrdisp tracker
+// gets an unwrapping pass before its molecules can cross half a period.
+int advance_steps(Sim &s, long long n, std::string *err) {
+  while (n > 0) {
+    long long k = n;
+    for (auto &kv : s.msd) {
+      const smolb::MsdState &m = kv.second;
+      if (m.started && !m.failed && m.every > 0) k = std::min(k, std::max<long long>(1, m.every - m.since));
+    }
+    if (s.eng->run(k, err)) return -1;
+    for (long long j = 0; j < k; ++j) s.time += s.dt;
+    s.steps += k;
+    n -= k;
+    for (auto &kv : s.msd) {
+      smolb::MsdState &m = kv.second;
+      if (!m.started || m.failed || m.every <= 0) continue;
+      m.since += k;
+      if (m.since < m.every) continue;
+      if (msd_register(s, m, err) || s.eng->msd_update(m.handle, -1, nullptr, nullptr, nullptr, err)) return -1;
+      m.since = 0;
+    }
+  }
+  return 0;
+}
+
+// runtime commands (smolcmd.c docommand subset: molcount, meansqrdisp)
 void do_commands(Sim &s, bool at_start) {
   for (smolb::Command &c : s.cmds) {
     bool run = false;
@@ -131,6 +262,7 @@ void do_commands(Sim &s, bool at_start) {
     char name[256] = {0}, arg[256] = {0};
     if (sscanf(c.text.c_str(), "%255s %255s", name, arg) < 1) continue;
     if (!strcmp(name, "molcount")) record_molcount(s, arg[0] ? arg : "molcount");
+    else if (!strcmp(name, "meansqrdisp")) record_meansqrdisp(s, c);
   }
 }
 
@@ -140,6 +272,7 @@ void do_end_commands(Sim &s) {
     char name[256] = {0}, arg[256] = {0};
     if (sscanf(c.text.c_str(), "%255s %255s", name, arg) < 1) continue;
     if (!strcmp(name, "molcount")) record_molcount(s, arg[0] ? arg : "molcount");
+    else if (!strcmp(name, "meansqrdisp")) record_meansqrdisp(s, c);
   }
 }
 
@@ -163,13 +296,10 @@ ErrorCode run_until(Sim &s, double stop, const char *func, bool one_step) {
   else
     while (t < stop) { t += s.dt; ++n; }
   if (!percmd) {
-    if (n > 0 && s.eng->run(n, &err)) return set_error(func, ECerror, err);
-    for (long long k = 0; k < n; ++k) { s.time += s.dt; s.steps++; }
+    if (n > 0 && advance_steps(s, n, &err)) return set_error(func, ECerror, err);
   } else {
     for (long long k = 0; k < n; ++k) {
-      if (s.eng->run(1, &err)) return set_error(func, ECerror, err);
-      s.time += s.dt;
-      s.steps++;
+      if (advance_steps(s, 1, &err)) return set_error(func, ECerror, err);
       do_commands(s, false);
     }
   }
@@ -689,7 +819,9 @@ enum ErrorCode smolgpuGetMolecules(simptr sim, long long *n, double *pos, int *s
     p = s.pend_pos;
     sp = s.pend_sp;
     sn.resize(sp.size());
-    for (size_t i = 0; i < sp.size(); ++i) sn[i] = i + 1;
+    uint64_t next = 1;
+    for (uint64_t v : s.pend_serno) next = std::max<uint64_t>(next, v + 1);
+    for (size_t i = 0; i < sp.size(); ++i) sn[i] = i < s.pend_serno.size() ? s.pend_serno[i] : next++;
   }
   const long long cnt = (long long)sp.size();
   LCHECK(*n >= cnt || (!pos && !species && !serno), ECbounds, "buffer too small");
@@ -708,6 +840,7 @@ enum ErrorCode smolgpuSetMolecules(simptr sim, long long n, const double *pos, c
     LCHECK(species[i] > 0 && species[i] < (int)s.species.size(), ECbounds, "species index out of range");
   s.pend_pos.assign(pos, pos + 3 * n);
   s.pend_sp.assign(species, species + n);
+  s.pend_serno.clear();
   ErrorCode ec = update_sim(s, __func__);
   if (ec != ECok) return ec;
   std::string err;
@@ -776,6 +909,8 @@ enum ErrorCode smolgpuAutotune(simptr sim, int trial_steps, double *ms_per_step)
     const long long n = (long long)sp.size();
     const long long cap = s.max_mol > 0 ? s.max_mol : std::max<long long>(2 * n + 4096, n + (1 << 20));
     const smolb::LaunchTuning keep = s.eng->tuning();
+    rc = msd_save(s, e);
+    if (rc) return rc;
     rc = s.eng->init(net, {rs}, s.dt, (uint64_t)s.seed, cap, e);
     if (!rc) rc = s.eng->set_tuning(keep, e);
     if (!rc) rc = s.eng->set_molecules(n, pos.data(), sp.data(), nullptr, serno.data(), e);
@@ -810,9 +945,7 @@ enum ErrorCode smolgpuRunSteps(simptr sim, long long nsteps) {
   ErrorCode ec = update_sim(s, __func__);
   if (ec != ECok) return ec;
   std::string err;
-  if (s.eng->run(nsteps, &err)) return set_error(__func__, ECerror, err);
-  for (long long k = 0; k < nsteps; ++k) s.time += s.dt;
-  s.steps += nsteps;
+  if (advance_steps(s, nsteps, &err)) return set_error(__func__, ECerror, err);
   return ECok;
 }
 

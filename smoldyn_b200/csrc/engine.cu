@@ -1790,6 +1790,83 @@ __global__ void k_species_count(const ull *id, const int *n, long long *spcount,
       if (s_cnt[k]) atomicAdd((unsigned long long *)&spcount[k], (unsigned long long)s_cnt[k]);
 }
 
+// Mean square displacement of tracked molecules (cmdmeansqrdisp,
+// smolcmd.c:2505-2606).  The reference keeps each molecule's periodic image
+// offset (posoffset) and measures pos + posoffset against the value recorded
+// on the first call.  Here the tracker keeps, per tracked molecule (keys
+// sorted by (rep, serial)), the start and the last unwrapped position; a pass
+// moves each present molecule from its last unwrapped position by its
+// displacement, periodic axes taken to the nearest image.  That is exact
+// while no molecule travels half a period between passes, which the host
+// guarantees by spacing the passes; the step kernels carry nothing extra.
+struct MsdGeo {
+  double lo[3], h[3], len[3];
+  int dim, periodic;  // periodic: bit d set when both walls of axis d wrap
+};
+
+constexpr int kMsdBlocks = 296, kMsdThreads = 256;
+
+__global__ void __launch_bounds__(kMsdThreads) k_msd(const float4 *a_pc, const ull *a_id, const int *a_n,
+                                                     const float4 *p_pc, const ull *p_id, const int *p_n, int pcap,
+                                                     const MsdGeo *geo, int nrep, int species, const ull *keys,
+                                                     long long m, const double *start, double *last, int msddim,
+                                                     double *part) {
+  const int na = *a_n, np = min(*p_n, pcap);
+  double s2 = 0.0, s4 = 0.0, cnt = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)na + np;
+       i += (long long)gridDim.x * blockDim.x) {
+    const bool prod = i >= na;
+    const ull x = prod ? p_id[i - na] : a_id[i];
+    if (id_species(x) != species) continue;
+    const int rp = id_rep(x);
+    if (rp >= nrep) continue;
+    const ull key = id_stream(x);
+    long long lo = 0, hi = m;  // first key >= key
+    while (lo < hi) {
+      const long long mid = (lo + hi) >> 1;
+      if (keys[mid] < key) lo = mid + 1;
+      else hi = mid;
+    }
+    if (lo >= m || keys[lo] != key) continue;
+    const float4 c = prod ? p_pc[i - na] : a_pc[i];
+    const MsdGeo &g = geo[rp];
+    int ix[3];
+    unpack_cell(__float_as_uint(c.w), ix[0], ix[1], ix[2]);
+    const float u[3] = {c.x, c.y, c.z};
+    double r2 = 0.0;
+    for (int d = 0; d < g.dim; ++d) {
+      const double xa = g.lo[d] + ix[d] * g.h[d] + (double)u[d];
+      double delta = xa - last[3 * lo + d];
+      if ((g.periodic >> d) & 1) delta -= g.len[d] * rint(delta / g.len[d]);
+      const double xu = last[3 * lo + d] + delta;
+      last[3 * lo + d] = xu;
+      const double df = xu - start[3 * lo + d];
+      if (msddim < 0 || msddim == d) r2 += df * df;
+    }
+    s2 += r2;
+    s4 += r2 * r2;
+    cnt += 1.0;
+  }
+  __shared__ double red[3][kMsdThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) {
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    s4 += __shfl_xor_sync(0xffffffffu, s4, o);
+    cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    red[0][warp] = s2;
+    red[1][warp] = s4;
+    red[2][warp] = cnt;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double v = 0.0;
+    for (int w = 0; w < kMsdThreads / 32; ++w) v += red[threadIdx.x][w];
+    part[3 * blockIdx.x + threadIdx.x] = v;
+  }
+}
+
 // Batched pair-radius derivation (binding radius + reverse unbinding radius),
 // one thread per replicate: the exact FP64 path for ensembles.
 __global__ void k_pair_radii(long long n, const double *kf, const double *dsum, double dt, int same, int rev,
@@ -1899,9 +1976,32 @@ class EngineImpl {
   // upload generation are unchanged)
   std::vector<long long> counts_cache;
   long long counts_step = -1, counts_gen = -1, upload_gen = 0;
+  // mean square displacement trackers (dropped with the molecules on init)
+  struct MsdTrack {
+    int species = 0;
+    long long m = 0;
+    ull *keys = nullptr;
+    double *start = nullptr, *last = nullptr;
+  };
+  std::vector<MsdTrack> msd;
+  MsdGeo *d_msdgeo = nullptr;
+  double *d_msdpart = nullptr;
+  void msd_free() {
+    for (MsdTrack &t : msd) {
+      if (t.keys) cudaFree(t.keys);
+      if (t.start) cudaFree(t.start);
+      if (t.last) cudaFree(t.last);
+    }
+    msd.clear();
+    if (d_msdgeo) cudaFree(d_msdgeo);
+    if (d_msdpart) cudaFree(d_msdpart);
+    d_msdgeo = nullptr;
+    d_msdpart = nullptr;
+  }
 
   void release() {
     invalidate_graph();
+    msd_free();
     void *ptrs[] = {d_difm, d_rsearch, d_geo, d_difstep, d_driftdt, d_bind2, d_pairprob, d_prdpos, d_gtab, d_unithr,
                     d_births, d_pc[0], d_pc[1], d_ppc[0], d_ppc[1], d_id[0], d_id[1], d_pid[0],
                     d_pid[1], d_face, d_tmp, d_counts, d_step, d_cnt, d_start, d_scan_ticket, d_scan_status, d_ev, d_cand, d_best,
@@ -2774,6 +2874,104 @@ int Engine::set_injection(long long n, const uint64_t *sernos, const double *dis
   E.invalidate_graph();
   return E.upload_const(err);
 }
+
+int Engine::set_rng_step(uint64_t step, std::string *err) {
+  EngineImpl &E = *impl_;
+  const uint32_t v = (uint32_t)step;
+  CK(cudaStreamSynchronize(E.stream));
+  CK(cudaMemcpy(E.d_step, &v, sizeof(v), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+int Engine::msd_track(int species, long long m, const uint64_t *keys, const double *start, const double *last,
+                      std::string *err) {
+  EngineImpl &E = *impl_;
+  if (species <= 0 || species >= E.net.nspecies) {
+    if (err) *err = "species index out of range";
+    return -6;
+  }
+  for (long long k = 1; k < m; ++k)
+    if (keys[k] <= keys[k - 1]) {
+      if (err) *err = "tracker keys must be strictly increasing";
+      return -6;
+    }
+  if (!E.d_msdgeo) {
+    std::vector<MsdGeo> g(E.reps.size());
+    for (size_t r = 0; r < E.reps.size(); ++r) {
+      const RepSpec &s = E.reps[r];
+      MsdGeo &q = g[r];
+      q.dim = s.dim;
+      q.periodic = 0;
+      for (int d = 0; d < 3; ++d) {
+        q.lo[d] = s.lo[d];
+        q.len[d] = s.hi[d] - s.lo[d];
+        q.h[d] = d < s.dim ? q.len[d] / E.geo[r].n[d] : 0.0;
+        if (d < s.dim && s.wall[2 * d] == kWallPeriodic && s.wall[2 * d + 1] == kWallPeriodic) q.periodic |= 1 << d;
+      }
+    }
+    CK(cudaMalloc(&E.d_msdgeo, g.size() * sizeof(MsdGeo)));
+    CK(cudaMemcpy(E.d_msdgeo, g.data(), g.size() * sizeof(MsdGeo), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&E.d_msdpart, 3 * kMsdBlocks * sizeof(double)));
+  }
+  EngineImpl::MsdTrack t;
+  t.species = species;
+  t.m = m;
+  const size_t mm = (size_t)std::max<long long>(m, 1);
+  CK(cudaMalloc(&t.keys, mm * sizeof(ull)));
+  CK(cudaMalloc(&t.start, 3 * mm * sizeof(double)));
+  CK(cudaMalloc(&t.last, 3 * mm * sizeof(double)));
+  if (m > 0) {
+    CK(cudaMemcpy(t.keys, keys, (size_t)m * sizeof(ull), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(t.start, start, 3 * (size_t)m * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(t.last, last, 3 * (size_t)m * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  E.msd.push_back(t);
+  return (int)E.msd.size() - 1;
+}
+
+int Engine::msd_update(int handle, int msddim, double *sum2, double *sum4, long long *count, std::string *err) {
+  EngineImpl &E = *impl_;
+  if (handle < 0 || handle >= (int)E.msd.size()) {
+    if (err) *err = "no such tracker";
+    return -6;
+  }
+  const EngineImpl::MsdTrack &t = E.msd[handle];
+  const int in = E.parity;
+  k_msd<<<kMsdBlocks, kMsdThreads, 0, E.stream>>>(E.d_pc[in], E.d_id[in], E.d_counts + in, E.d_ppc[in], E.d_pid[in],
+                                                  E.d_counts + 2 + in, (int)E.pcap, E.d_msdgeo, (int)E.reps.size(),
+                                                  t.species, t.keys, t.m, t.start, t.last, msddim, E.d_msdpart);
+  CK(cudaGetLastError());
+  ++E.nlaunch;
+  if (!sum2 && !sum4 && !count) return 0;
+  std::vector<double> part(3 * kMsdBlocks);
+  CK(cudaMemcpyAsync(part.data(), E.d_msdpart, part.size() * sizeof(double), cudaMemcpyDeviceToHost, E.stream));
+  CK(cudaStreamSynchronize(E.stream));
+  double a = 0, b = 0, c = 0;
+  for (int k = 0; k < kMsdBlocks; ++k) {
+    a += part[3 * k];
+    b += part[3 * k + 1];
+    c += part[3 * k + 2];
+  }
+  if (sum2) *sum2 = a;
+  if (sum4) *sum4 = b;
+  if (count) *count = (long long)c;
+  return 0;
+}
+
+int Engine::msd_last(int handle, std::vector<double> *last, std::string *err) {
+  EngineImpl &E = *impl_;
+  if (handle < 0 || handle >= (int)E.msd.size()) {
+    if (err) *err = "no such tracker";
+    return -6;
+  }
+  const EngineImpl::MsdTrack &t = E.msd[handle];
+  last->resize(3 * (size_t)t.m);
+  CK(cudaStreamSynchronize(E.stream));
+  if (t.m > 0) CK(cudaMemcpy(last->data(), t.last, last->size() * sizeof(double), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int Engine::msd_count() const { return (int)impl_->msd.size(); }
 
 int Engine::profile(long long nsteps, std::vector<std::string> *names, std::vector<double> *ms,
                     std::vector<long long> *launches, std::string *err) {

@@ -127,6 +127,10 @@ class Engine {
   int synchronize(std::string *err);
   long long launches() const;
   long long steps_done() const;
+  // Step index of the random streams (Philox counter; the next step uses
+  // step + 1).  A simulation that rebuilds its engine mid-run sets it to the
+  // steps already taken, so that no molecule replays earlier random numbers.
+  int set_rng_step(uint64_t step, std::string *err);
   // Capture the 2-step kernel sequence in a CUDA graph and replay it (on by default).
   void set_use_graph(bool on);
   // Launch shape (kept across init); a change re-captures the step graph.
@@ -135,6 +139,24 @@ class Engine {
   // Run n steps timing every kernel launch with CUDA events.
   int profile(long long nsteps, std::vector<std::string> *names, std::vector<double> *ms,
               std::vector<long long> *launches, std::string *err);
+
+  // Mean square displacement trackers (cmdmeansqrdisp, smolcmd.c:2505-2606).
+  // A tracker follows the molecules of `species` whose keys
+  // ((rep << 42) | serial, ascending) it is given, from unwrapped start
+  // positions `start` and last unwrapped positions `last` (3 per key).
+  // msd_track returns a handle >= 0 or a negative code.
+  int msd_track(int species, long long m, const uint64_t *keys, const double *start, const double *last,
+                std::string *err);
+  // Brings the tracker's unwrapped positions up to the current step: each
+  // tracked molecule still present moves from its last unwrapped position by
+  // its displacement, with periodic axes taken to the nearest image, so the
+  // caller must call it before any molecule can travel half a period.  With
+  // sums non-null, also returns the sum over tracked molecules present of r^2
+  // (msddim < 0: all axes, else that axis) and of r^4, and their count.
+  int msd_update(int handle, int msddim, double *sum2, double *sum4, long long *count, std::string *err);
+  // Last unwrapped positions (3 per key), e.g. to carry a tracker across a rebuild.
+  int msd_last(int handle, std::vector<double> *last, std::string *err);
+  int msd_count() const;
 
  private:
   EngineImpl *impl_;

@@ -38,6 +38,7 @@ struct smolb_ens {
   smolb::NetSpec net;
   int radius_mode = 1;  // 0 host exact, 1 device exact, 2 surrogate with exact fallback
   bool need_update = true, need_rebuild = true;
+  long long rng_steps = 0;  // steps run by earlier engines of this ensemble (random streams continue past them)
   // per-replicate derived pair parameters, [r2][rep]
   std::vector<std::vector<double>> bindrad, unbindrad;
   long long surrogate_fallbacks = 0;
@@ -203,6 +204,7 @@ int build(smolb_ens &e, std::string *err) {
   for (size_t sp = 1; sp < e.counts.size(); ++sp)
     for (int k = 0; k < e.nrep; ++k) total += e.counts[sp][k];
   const long long cap = T.max_mol > 0 ? T.max_mol : std::max<long long>(2 * total + 4096, total + (1 << 20));
+  if (e.eng) e.rng_steps += e.eng->steps_done();
   e.eng.reset(new smolb::Engine());
   rc = e.eng->init(e.net, e.reps, T.dt, (uint64_t)T.seed, cap, err);
   if (!rc) rc = e.eng->set_tuning(e.tuning, err);
@@ -222,6 +224,7 @@ int build(smolb_ens &e, std::string *err) {
         rep.push_back(k);
       }
   rc = e.eng->set_molecules((long long)sp.size(), pos.data(), sp.data(), rep.data(), nullptr, err);
+  if (!rc && e.rng_steps > 0) rc = e.eng->set_rng_step((uint64_t)e.rng_steps, err);
   if (rc) return rc;
   e.need_rebuild = false;
   return 0;

@@ -59,6 +59,20 @@ struct Command {
   double next = 0;
 };
 
+// One meansqrdisp command's tracker (cmdmeansqrdisp, smolcmd.c:2505-2606):
+// the molecules of `species` present on the command's first run, by
+// (rep << 42) | serial, with their unwrapped start and last positions.
+struct MsdState {
+  bool started = false, failed = false;
+  int species = 0, msddim = -1;      // msddim -1: all axes
+  std::string dataname;
+  std::vector<uint64_t> keys;
+  std::vector<double> start, last;   // host copies; last is refreshed before an engine rebuild
+  int handle = -1;                   // tracker in the current engine, -1 when it must be registered
+  long long every = 0;               // steps between unwrapping passes (0: none needed)
+  long long since = 0;               // steps since the last pass
+};
+
 struct Sim {
   int dim = 3;
   double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
@@ -78,6 +92,8 @@ struct Sim {
   // molecules waiting to be uploaded (absolute positions)
   std::vector<double> pend_pos;
   std::vector<int> pend_sp;
+  std::vector<uint64_t> pend_serno;   // serial numbers of the first pend_serno.size() pending molecules
+  std::map<std::string, MsdState> msd; // meansqrdisp trackers by command text
   uint64_t host_rng = 0x853C49E6748FEA9Bull;
   // runtime commands and output data tables
   std::vector<Command> cmds;
