@@ -657,31 +657,20 @@ enum ErrorCode smolAddPanel(simptr sim, const char *surface, enum PanelShape pan
     if (x.name == surface) sf = &x;
   LCHECK(sf, ECnonexist, "surface not found");
   LCHECK((int)sf->panels.size() < smolb::kMaxPanels, ECbounds, "too many panels");
-  smolb::PanelSpec p{};
-  p.front_sign = 1;
-  if (panelshape == PSsph) {
-    p.shape = 2;
-    for (int d = 0; d < 3; ++d) p.center[d] = d < sim->s.dim ? params[d] : 0;
-    p.radius = params[sim->s.dim];
-    if (p.radius < 0) { p.radius = -p.radius; p.front_sign = -1; }
-  } else if (panelshape == PSrect) {
-    LCHECK(axisstring, ECmissing, "missing axis string");
-    p.shape = 0;
-    p.front_sign = (axisstring[0] == '-') ? -1 : 1;
-    const char ax = axisstring[strlen(axisstring) - 1];
-    p.axis = (ax >= '0' && ax <= '2') ? ax - '0' : ax - 'x';
-    LCHECK(p.axis >= 0 && p.axis < 3, ECsyntax, "bad axis");
-    p.pos = params[p.axis];
-    int k = sim->s.dim;
-    for (int d = 0; d < 3; ++d) {
-      if (d == p.axis) { p.lo[d] = p.hi[d] = params[d]; continue; }
-      const double ext = (d < sim->s.dim) ? params[k++] : 0;
-      p.lo[d] = std::min(params[d], params[d] + ext);
-      p.hi[d] = std::max(params[d], params[d] + ext);
-    }
-  } else {
-    return set_error(__func__, ECbounds, "panel shape not supported by the GPU engine (rect, sphere)");
+  const int dim = sim->s.dim;
+  int np = 0;
+  switch (panelshape) {
+    case PSrect: np = 2 * dim - 1; break;
+    case PSsph: np = dim + 1; break;
+    case PStri: np = 9; break;
+    case PScyl: case PShemi: case PSdisk: np = 7; break;
+    default: return set_error(__func__, ECbounds, "panel shape not supported");
   }
+  LCHECK(panelshape != PSrect || axisstring, ECmissing, "missing axis string");
+  smolb::PanelSpec p{};
+  std::string err;
+  const int rc = smolb::make_panel(dim, (int)panelshape, axisstring ? axisstring : "", params, np, &p, &err);
+  if (rc) return set_error(__func__, from_rc(rc), err);
   sf->panels.push_back(p);
   sim->s.need_rebuild = true;
   return ECok;

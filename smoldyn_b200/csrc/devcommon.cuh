@@ -141,17 +141,22 @@ struct DevGeo {
 // Surface panel (shared by all replicates; coordinates relative to the low
 // corner of the system, FP64 because crossing tests near a panel need it).
 struct DevPanel {
-  int shape;        // 0 rect, 2 sphere
+  int shape;        // 0 rect, 1 tri, 2 sph, 3 cyl, 4 hemi, 5 disk (PanelSpec)
   int axis;         // rect: perpendicular axis
-  int front_sign;   // +1: front face toward +axis (rect) / outward (sphere)
+  int front_sign;   // +1: front face toward +axis (rect) / outward (sph, cyl, hemi); tri, disk: +1
   int pad;
   double pos;       // rect plane coordinate
   double lo[3], hi[3];
-  double center[3]; // sphere centre
+  double center[3]; // sph, hemi, disk centre
   double radius;
+  double pt[3][3];  // tri vertices; cyl axis end points
+  double nrm[3];    // tri, disk: unit front normal; hemi: unit open-side vector; cyl: unit axis
+  double axlen;     // cyl: axis length
   int act_front, act_back;   // default action per face: 0 reflect 1 transmit 2 absorb
   uint32_t abs_front, abs_back, tr_front, tr_back, rf_front, rf_back;  // per-species overrides
   float posf, radiusf, centerf[3];   // FP32 copies for the screening test
+  float p0f[3], nrmf[3];             // screen reference point and unit vector (zero for sph, hemi)
+  int curved;                        // screen: 1 sph, cyl, hemi (radial test); 0 flat (plane test)
 };
 
 struct Event {      // one reaction or birth; products are placed by k_products

@@ -282,16 +282,33 @@ __device__ __forceinline__ int panel_action(const DevPanel &pn, int face, int sp
   return pn.act_back;
 }
 
-// unit normal toward the front face at point x of the panel
+__device__ __forceinline__ double dot3(const double a[3], const double b[3]) {
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+
+// component of x - pt[0] normal to a cylinder's axis
+__device__ __forceinline__ void cyl_radial(const DevPanel &pn, const double x[3], double r[3]) {
+  double w[3];
+  for (int d = 0; d < 3; ++d) w[d] = x[d] - pn.pt[0][d];
+  const double s = dot3(w, pn.nrm);
+  for (int d = 0; d < 3; ++d) r[d] = w[d] - s * pn.nrm[d];
+}
+
+// unit normal toward the front face at point x of the panel (panelnormal,
+// smolsurface.c:3967)
+template <bool GEN>
 __device__ __forceinline__ void panel_normal(const DevPanel &pn, const double x[3], double n[3]) {
-  if (pn.shape == 2) {
-    double l = 0;
-    for (int d = 0; d < 3; ++d) {
-      n[d] = x[d] - pn.center[d];
-      l += n[d] * n[d];
+  if (pn.shape == 2 || (GEN && (pn.shape == 4 || pn.shape == 3))) {  // sph, hemi: from the centre; cyl: from the axis
+    if (GEN && pn.shape == 3) {
+      cyl_radial(pn, x, n);
+    } else {
+      for (int d = 0; d < 3; ++d) n[d] = x[d] - pn.center[d];
     }
-    l = (l > 0) ? pn.front_sign / sqrt(l) : 0.0;
+    const double l2 = dot3(n, n);
+    const double l = (l2 > 0) ? pn.front_sign / sqrt(l2) : 0.0;
     for (int d = 0; d < 3; ++d) n[d] *= l;
+  } else if (GEN && (pn.shape == 1 || pn.shape == 5)) {  // tri, disk: the front normal
+    for (int d = 0; d < 3; ++d) n[d] = pn.nrm[d];
   } else {
     n[0] = n[1] = n[2] = 0.0;
     n[pn.axis] = (double)pn.front_sign;
@@ -299,18 +316,135 @@ __device__ __forceinline__ void panel_normal(const DevPanel &pn, const double x[
 }
 
 // signed distance from the panel's surface, positive on the front side
+// (panelside, smolsurface.c:3930)
+template <bool GEN>
 __device__ __forceinline__ double panel_sdist(const DevPanel &pn, const double x[3]) {
-  if (pn.shape == 2) {
+  if (pn.shape == 2 || (GEN && pn.shape == 4)) {
     double r2 = 0;
     for (int d = 0; d < 3; ++d) r2 += (x[d] - pn.center[d]) * (x[d] - pn.center[d]);
     return pn.front_sign * (sqrt(r2) - pn.radius);
   }
+  if (GEN && pn.shape == 3) {
+    double r[3];
+    cyl_radial(pn, x, r);
+    return pn.front_sign * (sqrt(dot3(r, r)) - pn.radius);
+  }
+  if (GEN && (pn.shape == 1 || pn.shape == 5)) {
+    const double *o = pn.shape == 1 ? pn.pt[0] : pn.center;
+    double w[3];
+    for (int d = 0; d < 3; ++d) w[d] = x[d] - o[d];
+    return dot3(w, pn.nrm);
+  }
   return pn.front_sign * (x[pn.axis] - pn.pos);
+}
+
+// whether a point on a curved panel's full surface lies on the panel: the
+// closed half of a hemisphere away from its open side; a cylinder between
+// its end planes (smolsurface.c:4060-4065, Geo_PtInSlab)
+__device__ __forceinline__ bool on_curved_part(const DevPanel &pn, const double x[3]) {
+  double w[3];
+  if (pn.shape == 4) {
+    for (int d = 0; d < 3; ++d) w[d] = x[d] - pn.center[d];
+    return dot3(w, pn.nrm) <= 0;
+  }
+  if (pn.shape == 3) {
+    for (int d = 0; d < 3; ++d) w[d] = x[d] - pn.pt[0][d];
+    const double s = dot3(w, pn.nrm);
+    return s >= 0 && s <= pn.axlen;
+  }
+  return true;
+}
+
+// Crossings with the shapes other than rect and sphere.  Kernels are compiled
+// in two surface forms: rect and sphere panels only (GEN false, the common
+// case, whose registers the other shapes would otherwise raise), and every
+// shape (GEN true).
+// quadric with an open part: cyl (radial parts only) and hemi
+__device__ __forceinline__ double cross_cyl_hemi(const DevPanel &pn, const double a[3], const double b[3], int &face) {
+  double v[3], w[3], vq[3];
+  for (int d = 0; d < 3; ++d) v[d] = b[d] - a[d];
+  if (pn.shape == 3) {
+    cyl_radial(pn, a, w);
+    const double s = dot3(v, pn.nrm);
+    for (int d = 0; d < 3; ++d) vq[d] = v[d] - s * pn.nrm[d];
+  } else {
+    for (int d = 0; d < 3; ++d) {
+      w[d] = a[d] - pn.center[d];
+      vq[d] = v[d];
+    }
+  }
+  const double vv = dot3(vq, vq), wv = dot3(w, vq), ww = dot3(w, w);
+  if (vv <= 0) return 2.0;
+  const double c = ww - pn.radius * pn.radius;
+  const double disc = wv * wv - vv * c;
+  if (disc < 0) return 2.0;
+  const double sq = sqrt(disc);
+  const bool inside = c < 0;
+  // the inside face is the back one when the front faces out
+  const int face_in = pn.front_sign > 0 ? 1 : 0, face_out = 1 - face_in;
+  const double t2 = (-wv + sq) / vv;  // exit from the full quadric
+  double x[3];
+  if (!inside) {
+    const double t1 = (-wv - sq) / vv;  // entry
+    if (!(t1 > 0 && t1 <= 1)) return 2.0;
+    for (int d = 0; d < 3; ++d) x[d] = a[d] + t1 * v[d];
+    if (on_curved_part(pn, x)) {
+      face = face_out;
+      return t1;
+    }
+    // entered through the open part: the exit may still hit the panel from
+    // inside (smolsurface.c:4062-4069)
+    if (!(t2 > 0 && t2 <= 1)) return 2.0;
+    for (int d = 0; d < 3; ++d) x[d] = a[d] + t2 * v[d];
+    if (!on_curved_part(pn, x)) return 2.0;
+    face = face_in;
+    return t2;
+  }
+  if (!(t2 > 0 && t2 <= 1)) return 2.0;
+  for (int d = 0; d < 3; ++d) x[d] = a[d] + t2 * v[d];
+  if (!on_curved_part(pn, x)) return 2.0;
+  face = face_in;
+  return t2;
+}
+
+// flat: tri and disk in the plane of their front normal
+__device__ __forceinline__ double cross_tri_disk(const DevPanel &pn, const double a[3], const double b[3], int &face) {
+  const double *o = pn.shape == 1 ? pn.pt[0] : pn.center;
+  double w0[3], w1[3];
+  for (int d = 0; d < 3; ++d) {
+    w0[d] = a[d] - o[d];
+    w1[d] = b[d] - o[d];
+  }
+  const double d0 = dot3(w0, pn.nrm), d1 = dot3(w1, pn.nrm);
+  if (d0 == 0 || (d0 > 0) == (d1 > 0)) return 2.0;
+  const double t = d0 / (d0 - d1);
+  if (!(t > 0 && t <= 1)) return 2.0;
+  double x[3];
+  for (int d = 0; d < 3; ++d) x[d] = a[d] + t * (b[d] - a[d]);
+  if (pn.shape == 5) {
+    double r2 = 0;
+    for (int d = 0; d < 3; ++d) r2 += (x[d] - pn.center[d]) * (x[d] - pn.center[d]);
+    if (r2 > pn.radius * pn.radius) return 2.0;
+  } else {
+    // inside when on the inner side of all three edges (Geo_PtInTriangle2)
+    for (int k = 0; k < 3; ++k) {
+      const double *p = pn.pt[k], *q = pn.pt[(k + 1) % 3];
+      const double e[3] = {q[0] - p[0], q[1] - p[1], q[2] - p[2]};
+      const double f[3] = {x[0] - p[0], x[1] - p[1], x[2] - p[2]};
+      const double cr[3] = {e[1] * f[2] - e[2] * f[1], e[2] * f[0] - e[0] * f[2], e[0] * f[1] - e[1] * f[0]};
+      if (dot3(cr, pn.nrm) < 0) return 2.0;
+    }
+  }
+  face = d0 > 0 ? 0 : 1;
+  return t;
 }
 
 // Crossing of segment a->b with a panel: t in (0,1] and the face hit, or
 // t = 2 when the segment does not cross (smolsurface.c:4000 lineXpanel).
+template <bool GEN>
 __device__ __forceinline__ double panel_cross(const DevPanel &pn, const double a[3], const double b[3], int &face) {
+  if (GEN && (pn.shape == 1 || pn.shape == 5)) return cross_tri_disk(pn, a, b, face);
+  if (GEN && (pn.shape == 3 || pn.shape == 4)) return cross_cyl_hemi(pn, a, b, face);
   double v[3];
   for (int d = 0; d < 3; ++d) v[d] = b[d] - a[d];
   if (pn.shape == 2) {
@@ -350,29 +484,45 @@ __device__ __forceinline__ double panel_cross(const DevPanel &pn, const double a
 // Returns 1 if the molecule is absorbed; p1 is updated in place.
 // FP32 screen for the surface walk: false when the move a0 -> a1 (absolute
 // coordinates) stays more than the margin away from every panel, so no
-// crossing and no eps adjustment can occur.  Conservative: a rectangle is
-// tested as its whole plane, a sphere through the distances of the end points.
+// crossing and no eps adjustment can occur.  Conservative: flat panels are
+// tested as their whole plane; spheres and hemispheres through the distances
+// of the end points from the centre, cylinders from the infinite axis (the
+// distance is 1-Lipschitz along the move, so a segment that starts farther
+// than its length outside cannot reach the surface).
+template <bool GEN>
 __device__ __forceinline__ bool surface_near(const float a0[3], const float a1[3]) {
   const float tol = c_net.surf_tol;
   const float sx = a1[0] - a0[0], sy = a1[1] - a0[1], sz = a1[2] - a0[2];
   const float seg = sqrtf(sx * sx + sy * sy + sz * sz);
   for (int k = 0; k < c_net.npanel; ++k) {
     const DevPanel &pn = c_panels[k];
-    if (pn.shape == 0) {
-      const float pos = pn.posf;
-      const float s0 = a0[pn.axis] - pos, s1 = a1[pn.axis] - pos;
-      if ((s0 > tol && s1 > tol) || (s0 < -tol && s1 < -tol)) continue;
+    if (pn.shape == 0) {  // axis-aligned rectangle: its plane along one axis
+      const float q0 = a0[pn.axis] - pn.posf, q1 = a1[pn.axis] - pn.posf;
+      if ((q0 > tol && q1 > tol) || (q0 < -tol && q1 < -tol)) continue;
       return true;
     }
-    const float r = pn.radiusf;
-    float d0 = 0.f, d1 = 0.f;
+    // other shapes: offsets from the panel's reference point; for tri, disk
+    // and cyl also their components along the panel's unit vector
+    float w0[3], w1[3];
     for (int d = 0; d < 3; ++d) {
-      const float c = pn.centerf[d];
-      d0 += (a0[d] - c) * (a0[d] - c);
-      d1 += (a1[d] - c) * (a1[d] - c);
+      w0[d] = a0[d] - pn.p0f[d];
+      w1[d] = a1[d] - pn.p0f[d];
     }
-    d0 = sqrtf(d0);
-    d1 = sqrtf(d1);
+    float q0 = w0[0] * w0[0] + w0[1] * w0[1] + w0[2] * w0[2];
+    float q1 = w1[0] * w1[0] + w1[1] * w1[1] + w1[2] * w1[2];
+    if (GEN && (pn.shape == 1 || pn.shape == 3 || pn.shape == 5)) {
+      const float s0 = w0[0] * pn.nrmf[0] + w0[1] * pn.nrmf[1] + w0[2] * pn.nrmf[2];
+      const float s1 = w1[0] * pn.nrmf[0] + w1[1] * pn.nrmf[1] + w1[2] * pn.nrmf[2];
+      if (!pn.curved) {  // tri, disk: the whole plane
+        if ((s0 > tol && s1 > tol) || (s0 < -tol && s1 < -tol)) continue;
+        return true;
+      }
+      q0 -= s0 * s0;  // cyl: distance from the infinite axis
+      q1 -= s1 * s1;
+    }
+    // curved: distance from the centre (sph, hemi) or the axis (cyl)
+    const float r = pn.radiusf;
+    const float d0 = sqrtf(fmaxf(q0, 0.f)), d1 = sqrtf(fmaxf(q1, 0.f));
     if (d0 - seg > r + tol) continue;              // the whole move stays outside
     if (fmaxf(d0, d1) < r - tol) continue;         // the whole move stays inside
     return true;
@@ -380,6 +530,7 @@ __device__ __forceinline__ bool surface_near(const float a0[3], const float a1[3
   return false;
 }
 
+template <bool GEN>
 __device__ int surface_interact(int sp, const double p0_in[3], double p1[3], double eps, int &hits) {
   const int np = c_net.npanel;
   double p0[3] = {p0_in[0], p0_in[1], p0_in[2]};
@@ -388,17 +539,17 @@ __device__ int surface_interact(int sp, const double p0_in[3], double p1[3], dou
     int kmin = -1, fmin = 0;
     for (int k = 0; k < np; ++k) {
       int f = 0;
-      const double t = panel_cross(c_panels[k], p0, p1, f);
+      const double t = panel_cross<GEN>(c_panels[k], p0, p1, f);
       if (t < tmin) { tmin = t; kmin = k; fmin = f; }
     }
     if (kmin < 0) {
       // keep the final position at least eps off every panel, on its side
       for (int k = 0; k < np; ++k) {
-        const double sd = panel_sdist(c_panels[k], p1);
+        const double sd = panel_sdist<GEN>(c_panels[k], p1);
         if (fabs(sd) < eps) {
           double n[3];
-          panel_normal(c_panels[k], p1, n);
-          const double side = (sd > 0 || (sd == 0 && panel_sdist(c_panels[k], p0) > 0)) ? 1.0 : -1.0;
+          panel_normal<GEN>(c_panels[k], p1, n);
+          const double side = (sd > 0 || (sd == 0 && panel_sdist<GEN>(c_panels[k], p0) > 0)) ? 1.0 : -1.0;
           for (int d = 0; d < 3; ++d) p1[d] += (side * eps - sd) * n[d];
         }
       }
@@ -410,7 +561,7 @@ __device__ int surface_interact(int sp, const double p0_in[3], double p1[3], dou
     if (act == 2) return 1;
     double x[3], n[3];
     for (int d = 0; d < 3; ++d) x[d] = p0[d] + tmin * (p1[d] - p0[d]);
-    panel_normal(pn, x, n);
+    panel_normal<GEN>(pn, x, n);
     const double side = (fmin == 0) ? 1.0 : -1.0;  // incoming side along n
     if (act == 0) {
       double dot = 0;
@@ -444,6 +595,7 @@ __device__ __forceinline__ void from_abs(const DevGeo &g, const double x[3], int
 
 // True when the segment between two molecules crosses a surface panel: such
 // pairs do not react (rxnXsurface, used by bireact smolreact.c:3238).
+template <bool GEN>
 __device__ __forceinline__ bool pair_crosses_surface(const DevGeo &g, float4 pc, float vx, float vy, float vz) {
   int ix[3];
   unpack_cell(__float_as_uint(pc.w), ix[0], ix[1], ix[2]);
@@ -455,16 +607,23 @@ __device__ __forceinline__ bool pair_crosses_surface(const DevGeo &g, float4 pc,
   b[2] = a[2] + vz;
   for (int k = 0; k < c_net.npanel; ++k) {
     int f;
-    if (panel_cross(c_panels[k], a, b, f) <= 1.0) return true;
+    if (panel_cross<GEN>(c_panels[k], a, b, f) <= 1.0) return true;
   }
   return false;
+}
+
+// the same test as a call, for kernels whose hot loop should not carry the
+// panel arithmetic's registers
+template <bool GEN>
+__device__ __noinline__ bool pair_crosses_surface_call(const DevGeo &g, float4 pc, float vx, float vy, float vz) {
+  return pair_crosses_surface<GEN>(g, pc, vx, vy, vz);
 }
 
 // Move one molecule by one step (diffuse smolmolec.c:3115, checkwalls
 // smolwall.c:368, unireact decision smolreact.c:2997): returns 0 alive,
 // 1 removed by a wall, 2+r first-order reaction r fired (position is the
 // post-move position).
-template <bool SINGLE, bool SURF>
+template <bool SINGLE, int SURF>
 __device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, const KParams &p,
                                            const float *gtab, int rebin_only, int &hits) {
   const int sp = id_species(id);
@@ -538,11 +697,11 @@ __device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, co
       a0[d] = (float)ix0[d] * g.h[d] + u0[d];
       a1[d] = (float)ix[d] * g.h[d] + u[d];
     }
-    if (surface_near(a0, a1)) {
+    if (surface_near<SURF == 2>(a0, a1)) {
       double x0[3], x1[3];
       to_abs(g, ix0, u0, x0);
       to_abs(g, ix, u, x1);
-      if (surface_interact(sp, x0, x1, c_net.surf_eps, hits)) return 1;
+      if (surface_interact<SURF == 2>(sp, x0, x1, c_net.surf_eps, hits)) return 1;
       from_abs(g, x1, ix, u);
     }
   }
@@ -676,8 +835,13 @@ __device__ void births(const KParams &p, uint32_t step);
 // reacting molecules, the moved position into tmp (w = kTmpGone when the
 // molecule leaves the system), and the histogram of destination boxes.
 // rebin_only: no motion and no reactions (used after uploads).
-template <bool SINGLE, bool SURF>
-__global__ void __launch_bounds__(256, 4) k_move(KParams p, int rebin_only) {
+// resident 256-thread blocks per SM the register allocation must allow for
+// the surface variant (the plain variant fits 64 registers at 4 blocks)
+#ifndef SMOLB_SURF_MOVE_BLOCKS
+#define SMOLB_SURF_MOVE_BLOCKS 4
+#endif
+template <bool SINGLE, int SURF>
+__global__ void __launch_bounds__(256, SURF ? SMOLB_SURF_MOVE_BLOCKS : 4) k_move(KParams p, int rebin_only) {
   extern __shared__ float s_gtab[];
   pdl_launch_dependents();
   const float *gtab = rebin_only ? p.gtab : stage_gtab(p, s_gtab);  // constant data: before the wait
@@ -1021,7 +1185,7 @@ __device__ __forceinline__ int pair_reaction(const KParams &p, int rep, int spa,
 
 // Closest live partner of molecule i within its pair binding radii.
 // Returns packed (dist2 bits << 32 | index) or ~0 when none; *ncand counts candidates.
-template <bool SURF>
+template <int SURF>
 __device__ ull search_partner(const KParams &p, int i, float4 pc, ull id, uint32_t step, int &ncand) {
   const int nsorted = *p.b_n;
   const int sp = id_species(id);
@@ -1079,7 +1243,7 @@ __device__ ull search_partner(const KParams &p, int i, float4 pc, ull id, uint32
           const float vz = (q.z - pc.z) + (float)dz * g.h[2];
           const float d2 = vx * vx + vy * vy + vz * vz;
           if (pair_reaction(p, rep, sp, spj, d2, ka, id_stream(jd), step) < 0) continue;
-          if (SURF && pair_crosses_surface(g, pc, vx, vy, vz)) continue;
+          if (SURF && pair_crosses_surface_call<SURF == 2>(g, pc, vx, vy, vz)) continue;
           ncand++;
           const ull k = ((ull)__float_as_uint(d2) << 32) | (uint32_t)j;
           if (k < best) best = k;
@@ -1173,14 +1337,14 @@ __device__ int search_round1(const KParams &p, int i, float4 pc, ull id, uint32_
 
 // Pair test shared by the staged and the neighbour-box paths: if i and j react
 // this step, fold the key into i's running best and register i on j.
-template <bool SURF>
+template <int SURF>
 __device__ __forceinline__ void try_pair(const KParams &p, int i, ull idi, int sp, int rep, float d2, int j, ull jd,
                                          float rs2, uint32_t step, ull &best, int &extra, float4 pc, float vx,
                                          float vy, float vz) {
   if (d2 > rs2) return;
   const int spj = id_species(jd);
   if (spj == kDeadSpecies || !((c_net.pair_mask[sp] >> spj) & 1u)) return;
-  if (SURF && pair_crosses_surface(p.geo[rep], pc, vx, vy, vz)) return;
+  if (SURF && pair_crosses_surface_call<SURF == 2>(p.geo[rep], pc, vx, vy, vz)) return;
   if (pair_reaction(p, rep, sp, spj, d2, id_stream(idi), id_stream(jd), step) < 0) return;
   const uint32_t db = __float_as_uint(d2);
   const ull k = ((ull)db << 32) | (uint32_t)j;
@@ -1213,7 +1377,7 @@ __device__ __forceinline__ int register_pair(const KParams &p, int i, int j, flo
 // registered on both molecules (smolreact.c:3201-3298 tests each pair once).
 constexpr int kPairWin = 65;
 
-template <bool SINGLE, bool SURF, int BLOCK>
+template <bool SINGLE, int SURF, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_pairs_tile(KParams p) {
   constexpr int NW = BLOCK / 32;
   __shared__ float4 s_pc[NW][kPairWin];
@@ -1315,9 +1479,11 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_pairs_tile(KParams p) {
           const ull ida = wid[o], idb = wid[tj];
           const int spa = id_species(ida), spb = id_species(idb);
           const int repa = SINGLE ? 0 : id_rep(ida);
+          // the reaction test draws from a stateless stream, so it can go
+          // before the (rarely needed) surface test
           if (spb != kDeadSpecies && ((c_net.pair_mask[spa] >> spb) & 1u) &&
-              !(SURF && pair_crosses_surface(p.geo[repa], a, vx, vy, vz)) &&
-              pair_reaction(p, repa, spa, spb, d2, id_stream(ida), id_stream(idb), step) >= 0)
+              pair_reaction(p, repa, spa, spb, d2, id_stream(ida), id_stream(idb), step) >= 0 &&
+              !(SURF && pair_crosses_surface<SURF == 2>(p.geo[repa], a, vx, vy, vz)))
             extra += register_pair(p, wb + o, wb + tj, d2);
         }
       }
@@ -1334,8 +1500,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_pairs_tile(KParams p) {
         const ull idb = p.b_id[j];
         const int spb = id_species(idb);
         if (spb != kDeadSpecies && ((c_net.pair_mask[sp] >> spb) & 1u) &&
-            !(SURF && pair_crosses_surface(p.geo[rep], pc, vx, vy, vz)) &&
-            pair_reaction(p, rep, sp, spb, d2, id_stream(idi), id_stream(idb), step) >= 0)
+            pair_reaction(p, rep, sp, spb, d2, id_stream(idi), id_stream(idb), step) >= 0 &&
+            !(SURF && pair_crosses_surface<SURF == 2>(p.geo[rep], pc, vx, vy, vz)))
           extra += register_pair(p, i, j, d2);
       }
     }
@@ -1365,7 +1531,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_pairs_tile(KParams p) {
 // Cross-box pairs of one molecule within the stencil radius of a box face:
 // walk the neighbouring boxes its stencil reaches; a pair across boxes is
 // tested by the molecule in the lower-numbered box.
-template <bool SINGLE, bool SURF>
+template <bool SINGLE, int SURF>
 __device__ __forceinline__ void face_walk(const KParams &p, int i, int n, uint32_t step, int &extra) {
   const float4 pc = p.b_pc[i];
   const ull idi = p.b_id[i];
@@ -1427,7 +1593,7 @@ __device__ __forceinline__ void face_walk(const KParams &p, int i, int n, uint32
 // k_pairs_tile.  Each warp reads 32 bitmask words (1024 molecules), numbers
 // their set bits with a warp prefix sum and hands them out 32 at a time, so
 // every lane walks one flagged molecule per round.
-template <bool SINGLE, bool SURF>
+template <bool SINGLE, int SURF>
 __global__ void __launch_bounds__(256) k_pairs_faces(KParams p) {
   pdl_launch_dependents();
   pdl_wait();
@@ -1469,7 +1635,7 @@ __global__ void __launch_bounds__(256) k_pairs_faces(KParams p) {
 }
 
 // Re-search for candidates still alive (conflict-resolution rounds >= 2).
-template <bool SURF>
+template <int SURF>
 __global__ void k_research(KParams p) {
   pdl_launch_dependents();
   pdl_wait();
@@ -1579,7 +1745,7 @@ __device__ __forceinline__ void random_rotation(uint4 r, float m[9]) {
   m[6] = 2.f * (qx * qz - qy * qw); m[7] = 2.f * (qy * qz + qx * qw); m[8] = 1.f - 2.f * (qx * qx + qy * qy);
 }
 
-template <bool SURF>
+template <int SURF>
 __global__ void k_products(KParams p) {
   pdl_launch_dependents();
   pdl_wait();
@@ -1702,7 +1868,7 @@ __global__ void k_products(KParams p) {
         double x0[3], x1[3];
         to_abs(g, cell, site, x0);
         to_abs(g, c, w, x1);
-        if (surface_interact(psp, x0, x1, c_net.surf_eps, hits)) dead = true;
+        if (surface_interact<SURF == 2>(psp, x0, x1, c_net.surf_eps, hits)) dead = true;
         else from_abs(g, x1, c, w);
       }
       if (hits) atomicAdd(&p.counters[0], (unsigned long long)hits);
@@ -2177,7 +2343,8 @@ class EngineImpl {
     cudaLaunchKernelEx(&cfg, k, std::forward<Act>(args)...);
   }
 
-  template <bool SINGLE, bool SURF>
+  bool single_rep() const { return reps.size() == 1; }
+  template <bool SINGLE, int SURF>
   void enqueue_step_t(int par, bool rebin_only) {
     KParams p = params(par);
     launch(k_begin, 1, 32, 0, p, rebin_only ? 0 : 1);
@@ -2209,11 +2376,19 @@ class EngineImpl {
 
   // Enqueue one step with the given parity (inputs A/P = buffers `par`).
   void enqueue_step(int par, bool rebin_only) {
-    const bool single = reps.size() == 1, surf = dnet.npanel > 0;
-    if (single && !surf) enqueue_step_t<true, false>(par, rebin_only);
-    else if (single) enqueue_step_t<true, true>(par, rebin_only);
-    else if (!surf) enqueue_step_t<false, false>(par, rebin_only);
-    else enqueue_step_t<false, true>(par, rebin_only);
+    // surface form: 0 none, 1 rect and sphere panels only, 2 any shape
+    int surf = dnet.npanel > 0 ? 1 : 0;
+    for (const DevPanel &pn : panels)
+      if (pn.shape != 0 && pn.shape != 2) surf = 2;
+    if (single_rep()) {
+      if (surf == 0) enqueue_step_t<true, 0>(par, rebin_only);
+      else if (surf == 1) enqueue_step_t<true, 1>(par, rebin_only);
+      else enqueue_step_t<true, 2>(par, rebin_only);
+    } else {
+      if (surf == 0) enqueue_step_t<false, 0>(par, rebin_only);
+      else if (surf == 1) enqueue_step_t<false, 1>(par, rebin_only);
+      else enqueue_step_t<false, 2>(par, rebin_only);
+    }
   }
 
   int launches_per_step() const { return 8 + 2 * (dnet.rounds - 1); }
@@ -2561,9 +2736,28 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
         dp.center[d] = ps.center[d] - s0.lo[d];
       }
       dp.radius = ps.radius;
+      for (int k = 0; k < 3; ++k)
+        for (int d = 0; d < 3; ++d) dp.pt[k][d] = ps.pt[k][d] - s0.lo[d];
+      for (int d = 0; d < 3; ++d) dp.nrm[d] = ps.normal[d];
+      dp.axlen = 0;
+      if (ps.shape == 3)
+        for (int d = 0; d < 3; ++d) dp.axlen += (dp.pt[1][d] - dp.pt[0][d]) * dp.nrm[d];
       dp.posf = (float)dp.pos;
       dp.radiusf = (float)dp.radius;
-      for (int d = 0; d < 3; ++d) dp.centerf[d] = (float)dp.center[d];
+      dp.curved = (ps.shape == 2 || ps.shape == 3 || ps.shape == 4) ? 1 : 0;
+      for (int d = 0; d < 3; ++d) {
+        dp.centerf[d] = (float)dp.center[d];
+        // screen reference point and unit vector: rect plane point and axis;
+        // tri vertex and normal; disk centre and normal; sph / hemi centre and
+        // no vector; cyl axis start and axis
+        double p0 = 0, n0 = 0;
+        if (ps.shape == 0) { p0 = d == ps.axis ? dp.pos : 0.0; n0 = d == ps.axis ? 1.0 : 0.0; }
+        else if (ps.shape == 1 || ps.shape == 3) { p0 = dp.pt[0][d]; n0 = dp.nrm[d]; }
+        else if (ps.shape == 5) { p0 = dp.center[d]; n0 = dp.nrm[d]; }
+        else { p0 = dp.center[d]; n0 = 0.0; }
+        dp.p0f[d] = (float)p0;
+        dp.nrmf[d] = (float)n0;
+      }
       dp.act_front = ps.action_front;
       dp.act_back = ps.action_back;
       dp.abs_front = ps.absorb_front_mask;

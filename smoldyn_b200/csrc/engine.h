@@ -24,16 +24,20 @@ constexpr int kMaxPanels = 16;
 
 enum WallKind : uint8_t { kWallReflect = 0, kWallPeriodic = 1, kWallAbsorb = 2, kWallTransparent = 3 };
 
-// Surface panel (sphere or axis-aligned rectangle) with one action for all
-// species on each face (smolsurface.c:4930 dosurfinteract subset).
+// Surface panel with one action for all species on each face
+// (smolsurface.c:4930 dosurfinteract subset).  Shapes follow the reference's
+// PanelShape numbering (smoldyn.h:492): 0 rect, 1 tri, 2 sph, 3 cyl, 4 hemi,
+// 5 disk; faces as in panelside (smolsurface.c:3930).
 struct PanelSpec {
-  int shape;            // 0 = rect (PSrect), 2 = sphere (PSsph)
+  int shape;
   int axis;             // rect: perpendicular axis 0..2; front face toward +axis if front_sign>0
-  int front_sign;       // rect: +1 / -1; sphere: +1 = front outward, -1 = front inward
+  int front_sign;       // rect: +1 / -1; sph, cyl, hemi: +1 = front outward, -1 = front inward; tri, disk: +1
   double pos;           // rect: coordinate of the plane along axis
   double lo[3], hi[3];  // rect: extent in the two in-plane axes (lo/hi per axis)
-  double center[3];     // sphere
-  double radius;        // sphere
+  double center[3];     // sph, hemi, disk
+  double radius;        // sph, cyl, hemi, disk
+  double pt[3][3];      // tri: vertices; cyl: axis end points pt[0], pt[1]
+  double normal[3];     // tri, disk: unit front normal; hemi: unit vector out of the open side; cyl: unit axis
   int action_front;     // 0 reflect, 1 transmit, 2 absorb (per species below overrides)
   int action_back;
   uint32_t absorb_front_mask;   // species bitmask overriding to absorb on front

@@ -784,6 +784,95 @@ int read_config_statement(Sim &sim, const std::string &word, const std::string &
   return 0;
 }
 
+// surfaddpanel (smolsurface.c:2432-2640): a panel from its shape's
+// parameters.  rect: axis "+0".."-2" and corner + extents (dim values, then
+// dim-1 extents); sph: centre (dim) and radius (negative: front inside); in 3-D
+// also tri: 3 vertices (front by the right-hand rule, Geo_TriNormal); cyl: the
+// two axis end points and radius (negative: front inside); hemi: centre,
+// radius (sign as sph) and a vector out of the open side; disk: centre, radius
+// and front normal.  Trailing drawing parameters (slices, stacks) are ignored.
+int make_panel(int dim, int shape, const std::string &axis, const double *prm, int np, PanelSpec *out,
+               std::string *err) {
+  PanelSpec p{};
+  p.shape = shape;
+  p.front_sign = 1;
+  auto need = [&](int n, const char *what) {
+    if (np >= n) return true;
+    if (err) *err = std::string("panel ") + what + ": missing parameters";
+    return false;
+  };
+  auto unit = [](double v[3]) {
+    const double l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    if (!(l > 0)) return false;
+    for (int d = 0; d < 3; ++d) v[d] /= l;
+    return true;
+  };
+  if (shape != 0 && shape != 2 && dim != 3) {
+    if (err) *err = "panel: tri, cyl, hemi and disk panels need dim 3";
+    return -6;
+  }
+  if (shape == 0) {
+    if (axis.size() < 2 || (axis[0] != '+' && axis[0] != '-')) { if (err) *err = "panel rect: bad axis"; return -7; }
+    p.front_sign = axis[0] == '-' ? -1 : 1;
+    const char ac = axis.back();
+    p.axis = (ac >= '0' && ac <= '2') ? ac - '0' : ac - 'x';
+    if (p.axis < 0 || p.axis >= dim) { if (err) *err = "panel rect: bad axis"; return -7; }
+    if (!need(dim + dim - 1, "rect")) return -7;
+    double corner[3] = {0, 0, 0};
+    for (int d = 0; d < dim; ++d) corner[d] = prm[d];
+    p.pos = corner[p.axis];
+    int k = dim;
+    for (int d = 0; d < 3; ++d) {
+      if (d == p.axis || d >= dim) { p.lo[d] = p.hi[d] = corner[d]; continue; }
+      const double ext = prm[k++];
+      p.lo[d] = std::min(corner[d], corner[d] + ext);
+      p.hi[d] = std::max(corner[d], corner[d] + ext);
+    }
+  } else if (shape == 2) {
+    if (!need(dim + 1, "sph")) return -7;
+    for (int d = 0; d < dim; ++d) p.center[d] = prm[d];
+    p.radius = prm[dim];
+    if (p.radius < 0) { p.radius = -p.radius; p.front_sign = -1; }
+  } else if (shape == 1) {
+    if (!need(9, "tri")) return -7;
+    for (int k = 0; k < 3; ++k)
+      for (int d = 0; d < 3; ++d) p.pt[k][d] = prm[3 * k + d];
+    const double e1[3] = {p.pt[1][0] - p.pt[0][0], p.pt[1][1] - p.pt[0][1], p.pt[1][2] - p.pt[0][2]};
+    const double e2[3] = {p.pt[2][0] - p.pt[1][0], p.pt[2][1] - p.pt[1][1], p.pt[2][2] - p.pt[1][2]};
+    p.normal[0] = e1[1] * e2[2] - e1[2] * e2[1];
+    p.normal[1] = e1[2] * e2[0] - e1[0] * e2[2];
+    p.normal[2] = e1[0] * e2[1] - e1[1] * e2[0];
+    if (!unit(p.normal)) { if (err) *err = "panel tri: degenerate triangle"; return -6; }
+  } else if (shape == 3) {
+    if (!need(7, "cyl")) return -7;
+    for (int k = 0; k < 2; ++k)
+      for (int d = 0; d < 3; ++d) p.pt[k][d] = prm[3 * k + d];
+    p.radius = prm[6];
+    if (p.radius < 0) { p.radius = -p.radius; p.front_sign = -1; }
+    for (int d = 0; d < 3; ++d) p.normal[d] = p.pt[1][d] - p.pt[0][d];
+    if (!unit(p.normal)) { if (err) *err = "panel cyl: the end points coincide"; return -6; }
+  } else if (shape == 4) {
+    if (!need(7, "hemi")) return -7;
+    for (int d = 0; d < 3; ++d) p.center[d] = prm[d];
+    p.radius = prm[3];
+    if (p.radius < 0) { p.radius = -p.radius; p.front_sign = -1; }
+    for (int d = 0; d < 3; ++d) p.normal[d] = prm[4 + d];
+    if (!unit(p.normal)) { if (err) *err = "panel hemi: zero outward vector"; return -6; }
+  } else if (shape == 5) {
+    if (!need(7, "disk")) return -7;
+    for (int d = 0; d < 3; ++d) p.center[d] = prm[d];
+    p.radius = prm[3];
+    if (!(p.radius > 0)) { if (err) *err = "panel disk: radius must be > 0"; return -6; }
+    for (int d = 0; d < 3; ++d) p.normal[d] = prm[4 + d];
+    if (!unit(p.normal)) { if (err) *err = "panel disk: zero normal"; return -6; }
+  } else {
+    if (err) *err = "panel shape not supported";
+    return -7;
+  }
+  *out = p;
+  return 0;
+}
+
 // surface block statements (smolsurface.c surfreadstring subset)
 static int read_surface_statement(Sim &sim, SurfaceDef &sf, const std::string &word,
                                   const std::vector<std::string> &w, std::string *err) {
@@ -824,37 +913,28 @@ static int read_surface_statement(Sim &sim, SurfaceDef &sf, const std::string &w
     }
   } else if (word == "panel") {
     if (w.empty()) { if (err) *err = "panel: missing shape"; return -7; }
-    PanelSpec p{};
-    p.front_sign = 1;
-    if (w[0] == "sphere" || w[0] == "sph") {
-      if (w.size() < 5) { if (err) *err = "panel sphere: missing parameters"; return -7; }
-      p.shape = 2;
-      for (int d = 0; d < 3; ++d) p.center[d] = atof(w[1 + d].c_str());
-      p.radius = atof(w[4].c_str());
-      if (p.radius < 0) { p.radius = -p.radius; p.front_sign = -1; }
-    } else if (w[0] == "rect" || w[0] == "r") {
-      // panel rect +x x y z dy dz  (axis sign + perpendicular axis, corner, extents)
-      if (w.size() < 7) { if (err) *err = "panel rect: missing parameters"; return -7; }
-      p.shape = 0;
-      const std::string &ax = w[1];
-      p.front_sign = (ax[0] == '-') ? -1 : 1;
-      const char ac = ax.back();
-      p.axis = (ac >= '0' && ac <= '2') ? ac - '0' : ac - 'x';
-      if (p.axis < 0 || p.axis > 2) { if (err) *err = "panel rect: bad axis"; return -7; }
-      double corner[3];
-      for (int d = 0; d < 3; ++d) corner[d] = atof(w[2 + d].c_str());
-      p.pos = corner[p.axis];
-      int k = 5;
-      for (int d = 0; d < 3; ++d) {
-        if (d == p.axis) { p.lo[d] = p.hi[d] = corner[d]; continue; }
-        const double ext = atof(w[k++].c_str());
-        p.lo[d] = std::min(corner[d], corner[d] + ext);
-        p.hi[d] = std::max(corner[d], corner[d] + ext);
-      }
-    } else {
-      if (err) *err = "panel shape not supported by the GPU engine: " + w[0];
-      return -7;
+    const std::string &sh = w[0];
+    const int shape = (sh == "rect" || sh == "r") ? 0 : (sh == "tri" || sh == "t") ? 1
+                      : (sh == "sph" || sh == "sphere" || sh == "s") ? 2 : (sh == "cyl" || sh == "c") ? 3
+                      : (sh == "hemi" || sh == "h") ? 4 : (sh == "disk" || sh == "d") ? 5 : -1;
+    if (shape < 0) { if (err) *err = "panel shape not supported by the GPU engine: " + sh; return -7; }
+    std::string axis;
+    size_t k = 1;
+    if (shape == 0) {
+      if (w.size() < 2) { if (err) *err = "panel rect: missing axis"; return -7; }
+      axis = w[1];
+      k = 2;
     }
+    std::vector<double> prm;
+    for (; k < w.size(); ++k) {
+      char *end = nullptr;
+      const double v = strtod(w[k].c_str(), &end);
+      if (!end || *end) break;  // a trailing panel name
+      prm.push_back(v);
+    }
+    PanelSpec p{};
+    const int rc = make_panel(sim.dim, shape, axis, prm.data(), (int)prm.size(), &p, err);
+    if (rc) return rc;
     if ((int)sf.panels.size() >= kMaxPanels) { if (err) *err = "too many panels"; return -6; }
     sf.panels.push_back(p);
   } else if (word == "color" || word == "thickness" || word == "polygon" || word == "stipple" ||

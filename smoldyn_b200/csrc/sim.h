@@ -118,6 +118,9 @@ struct Sim {
 // molsetdifm (smolmolec.c:833-867): set the diffusion matrix of a species;
 // its difc becomes trace(M*M)/dim.  m is dim x dim, row-major.
 void set_species_difm(Sim &sim, int sp, const double *m);
+// surfaddpanel (smolsurface.c:2432): a panel from its shape's parameters.
+int make_panel(int dim, int shape, const std::string &axis, const double *prm, int np, PanelSpec *out,
+               std::string *err);
 // Restatements of the reference's parameter derivation.
 int derive_reaction_params(Sim &sim, std::string *err);
 // rxncalcrate (smolreact.c:1592-1680): effective rate from derived parameters.
