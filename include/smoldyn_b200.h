@@ -3,9 +3,9 @@
  * Part 1 is a drop-in subset of Smoldyn's public C API
  * (source/Smoldyn/libsmoldyn.h): a program written against libsmoldyn that
  * uses only these calls links against libsmoldyn_b200.so unchanged and runs
- * Smoldyn's per-timestep particle engine (diffusion, walls, sphere/rectangle
- * surfaces, virtual-box binning, zeroth/first/second-order reactions and
- * product placement) on one NVIDIA B200.  Enum values equal the reference's
+ * Smoldyn's per-timestep particle engine (diffusion, walls, surfaces of all six
+ * panel shapes, compartments, virtual-box binning, zeroth/first/second-order
+ * reactions and product placement) on one NVIDIA B200.  Enum values equal the reference's
  * (smoldyn.h:251-512, libsmoldyn.h:13-26).  simptr is opaque here: callers that
  * read simstruct fields directly are not supported.
  *
@@ -43,6 +43,7 @@ enum RevParam { /* smoldyn.h:358 */
 };
 enum PanelFace { PFfront, PFback, PFnone, PFboth };                         /* smoldyn.h:484 */
 enum PanelShape { PSrect, PStri, PSsph, PScyl, PShemi, PSdisk, PSall, PSnone }; /* smoldyn.h:491 */
+enum CmptLogic { CLequal, CLequalnot, CLand, CLor, CLxor, CLandnot, CLornot, CLnone }; /* smoldyn.h:659 */
 enum SrfAction {                                                             /* smoldyn.h:503 */
   SAreflect, SAtrans, SAabsorb, SAjump, SAport, SAmult, SAno, SAnone, SAadsorb, SArevdes,
   SAirrevdes, SAflip
@@ -102,7 +103,7 @@ enum ErrorCode smolAddSolutionMolecules(simptr sim, const char *species, int num
                                         double *lowposition, double *highposition);
 int smolGetMoleculeCount(simptr sim, const char *species, enum MolecState state);
 
-/* libsmoldyn.h:122-130: walls and the sphere/rectangle surface subset */
+/* libsmoldyn.h:122-130: walls and surfaces (solution-state actions) */
 enum ErrorCode smolSetBoundaryType(simptr sim, int dimension, int highside, char type);
 enum ErrorCode smolAddSurface(simptr sim, const char *surface);
 enum ErrorCode smolSetSurfaceAction(simptr sim, const char *surface, enum PanelFace face,
@@ -110,6 +111,25 @@ enum ErrorCode smolSetSurfaceAction(simptr sim, const char *surface, enum PanelF
                                     enum SrfAction action, const char *newspecies);
 enum ErrorCode smolAddPanel(simptr sim, const char *surface, enum PanelShape panelshape,
                             const char *panel, const char *axisstring, double *params);
+
+/* Compartments (libsmoldyn.h:115, :142-148, :157): interior-defining points,
+ * bounding surfaces and logic on earlier compartments; molecules placed
+ * uniformly inside; reactions restricted to a compartment (zeroth order:
+ * births inside at rate x compartment volume; first order: the molecule must
+ * be inside; second order: both reactants).  At most 8 compartments, 8 points
+ * and 4 logic terms each. */
+enum ErrorCode smolAddCompartment(simptr sim, const char *compartment);
+int smolGetCompartmentIndex(simptr sim, const char *compartment);
+int smolGetCompartmentIndexNT(simptr sim, const char *compartment);
+char *smolGetCompartmentName(simptr sim, int compartmentindex, char *compartment);
+enum ErrorCode smolAddCompartmentSurface(simptr sim, const char *compartment, const char *surface);
+enum ErrorCode smolAddCompartmentPoint(simptr sim, const char *compartment, double *point);
+enum ErrorCode smolAddCompartmentLogic(simptr sim, const char *compartment, enum CmptLogic logic,
+                                       const char *compartment2);
+enum ErrorCode smolAddCompartmentMolecules(simptr sim, const char *species, int number, const char *compartment);
+/* surface must be NULL: surface-restricted reactions need surface-bound
+ * molecules, which the engine does not model. */
+enum ErrorCode smolSetReactionRegion(simptr sim, const char *reaction, const char *compartment, const char *surface);
 
 /* libsmoldyn.h:152-158 */
 enum ErrorCode smolAddReaction(simptr sim, const char *reaction, const char *reactant1,

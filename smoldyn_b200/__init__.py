@@ -23,6 +23,7 @@ MSsoln, MSfront, MSback, MSup, MSdown, MSbsoln, MSall, MSnone, MSsome = range(9)
  RPpgem2, RPpgemmax2, RPratio2, RPoffset, RPfixed) = range(14)
 PFfront, PFback, PFnone, PFboth = range(4)
 PSrect, PStri, PSsph, PScyl, PShemi, PSdisk, PSall, PSnone = range(8)
+CLequal, CLequalnot, CLand, CLor, CLxor, CLandnot, CLornot, CLnone = range(8)
 SAreflect, SAtrans, SAabsorb = 0, 1, 2
 
 _dp = C.POINTER(C.c_double)
@@ -67,6 +68,15 @@ PROTOTYPES = {
     "smolGetMoleculeCount": (C.c_int, [_sim, C.c_char_p, C.c_int]),
     "smolSetBoundaryType": (C.c_int, [_sim, C.c_int, C.c_int, C.c_char]),
     "smolAddSurface": (C.c_int, [_sim, C.c_char_p]),
+    "smolAddCompartment": (C.c_int, [_sim, C.c_char_p]),
+    "smolGetCompartmentIndex": (C.c_int, [_sim, C.c_char_p]),
+    "smolGetCompartmentIndexNT": (C.c_int, [_sim, C.c_char_p]),
+    "smolGetCompartmentName": (C.c_char_p, [_sim, C.c_int, C.c_char_p]),
+    "smolAddCompartmentSurface": (C.c_int, [_sim, C.c_char_p, C.c_char_p]),
+    "smolAddCompartmentPoint": (C.c_int, [_sim, C.c_char_p, _dp]),
+    "smolAddCompartmentLogic": (C.c_int, [_sim, C.c_char_p, C.c_int, C.c_char_p]),
+    "smolAddCompartmentMolecules": (C.c_int, [_sim, C.c_char_p, C.c_int, C.c_char_p]),
+    "smolSetReactionRegion": (C.c_int, [_sim, C.c_char_p, C.c_char_p, C.c_char_p]),
     "smolSetSurfaceAction": (C.c_int, [_sim, C.c_char_p, C.c_int, C.c_char_p, C.c_int, C.c_int, C.c_char_p]),
     "smolAddPanel": (C.c_int, [_sim, C.c_char_p, C.c_int, C.c_char_p, C.c_char_p, _dp]),
     "smolAddReaction": (C.c_int, [_sim, C.c_char_p, C.c_char_p, C.c_int, C.c_char_p, C.c_int, C.c_int,

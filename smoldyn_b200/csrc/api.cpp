@@ -672,7 +672,113 @@ enum ErrorCode smolAddPanel(simptr sim, const char *surface, enum PanelShape pan
   const int rc = smolb::make_panel(dim, (int)panelshape, axisstring ? axisstring : "", params, np, &p, &err);
   if (rc) return set_error(__func__, from_rc(rc), err);
   sf->panels.push_back(p);
+  smolb::invalidate_compartments(sim->s);
   sim->s.need_rebuild = true;
+  return ECok;
+}
+
+enum ErrorCode smolAddCompartment(simptr sim, const char *compartment) {
+  LCHECK(sim && compartment, ECmissing, "missing argument");
+  Sim &s = sim->s;
+  LCHECK(s.compartment_index(compartment) < 0, ECsame, "compartment already exists");
+  LCHECK((int)s.cmpts.size() < smolb::kMaxCmpt, ECbounds, "too many compartments");
+  smolb::CompartDef c;
+  c.name = compartment;
+  s.cmpts.push_back(c);
+  s.need_update = s.need_rebuild = true;
+  return ECok;
+}
+
+int smolGetCompartmentIndexNT(simptr sim, const char *compartment) {
+  if (!sim || !compartment) return (int)ECmissing;
+  const int c = sim->s.compartment_index(compartment);
+  return c >= 0 ? c : (int)ECnonexist;
+}
+
+int smolGetCompartmentIndex(simptr sim, const char *compartment) {
+  const int c = smolGetCompartmentIndexNT(sim, compartment);
+  if (c < 0) return (int)set_error(__func__, (ErrorCode)c, "compartment not found");
+  return c;
+}
+
+char *smolGetCompartmentName(simptr sim, int compartmentindex, char *compartment) {
+  if (!sim || !compartment) { set_error(__func__, ECmissing, "missing argument"); return nullptr; }
+  if (compartmentindex < 0 || compartmentindex >= (int)sim->s.cmpts.size()) {
+    set_error(__func__, ECbounds, "compartment index out of range");
+    return nullptr;
+  }
+  strcpy(compartment, sim->s.cmpts[compartmentindex].name.c_str());
+  return compartment;
+}
+
+enum ErrorCode smolAddCompartmentSurface(simptr sim, const char *compartment, const char *surface) {
+  LCHECK(sim && compartment && surface, ECmissing, "missing argument");
+  std::string err;
+  const int c = sim->s.compartment_index(compartment);
+  LCHECK(c >= 0, ECnonexist, "compartment not found");
+  const int rc = smolb::read_compartment_words(sim->s, c, "surface", {surface}, &err);
+  if (rc) return set_error(__func__, from_rc(rc), err);
+  return ECok;
+}
+
+enum ErrorCode smolAddCompartmentPoint(simptr sim, const char *compartment, double *point) {
+  LCHECK(sim && compartment && point, ECmissing, "missing argument");
+  std::string err;
+  const int c = sim->s.compartment_index(compartment);
+  LCHECK(c >= 0, ECnonexist, "compartment not found");
+  std::vector<std::string> w;
+  char buf[64];
+  for (int d = 0; d < sim->s.dim; ++d) {
+    snprintf(buf, sizeof buf, "%.17g", point[d]);
+    w.push_back(buf);
+  }
+  const int rc = smolb::read_compartment_words(sim->s, c, "point", w, &err);
+  if (rc) return set_error(__func__, from_rc(rc), err);
+  return ECok;
+}
+
+enum ErrorCode smolAddCompartmentLogic(simptr sim, const char *compartment, enum CmptLogic logic,
+                                       const char *compartment2) {
+  LCHECK(sim && compartment && compartment2, ECmissing, "missing argument");
+  static const char *syms[] = {"equal", "equalnot", "and", "or", "xor", "andnot", "ornot"};
+  LCHECK(logic >= CLequal && logic <= CLornot, ECbounds, "unrecognized logic symbol");
+  std::string err;
+  const int c = sim->s.compartment_index(compartment);
+  LCHECK(c >= 0, ECnonexist, "compartment not found");
+  const int rc = smolb::read_compartment_words(sim->s, c, "compartment", {syms[logic], compartment2}, &err);
+  if (rc) return set_error(__func__, from_rc(rc), err);
+  return ECok;
+}
+
+enum ErrorCode smolAddCompartmentMolecules(simptr sim, const char *species, int number, const char *compartment) {
+  LCHECK(sim && species && compartment, ECmissing, "missing argument");
+  LCHECK(number >= 0, ECbounds, "number must be >= 0");
+  Sim &s = sim->s;
+  LCHECK(s.species_index(species) > 0, ECnonexist, "species not found");
+  LCHECK(s.compartment_index(compartment) >= 0, ECnonexist, "compartment not found");
+  std::string err;
+  if (s.eng && s.started)
+    if (pull_molecules(s, &err)) return set_error(__func__, ECerror, err);
+  const int rc = smolb::read_config_statement(s, "compartment_mol",
+                                              std::to_string(number) + " " + species + " " + compartment, &err);
+  if (rc) return set_error(__func__, from_rc(rc), err);
+  return ECok;
+}
+
+enum ErrorCode smolSetReactionRegion(simptr sim, const char *reaction, const char *compartment, const char *surface) {
+  LCHECK(sim && reaction, ECmissing, "missing argument");
+  LCHECK(!surface, ECbounds, "surface-restricted reactions are not supported by the GPU engine");
+  Sim &s = sim->s;
+  int o = 0;
+  const int r = s.reaction_index(reaction, &o);
+  LCHECK(r >= 0, ECnonexist, "reaction not found");
+  int c = -1;
+  if (compartment) {
+    c = s.compartment_index(compartment);
+    LCHECK(c >= 0, ECnonexist, "compartment not found");
+  }
+  s.rxn[o][r].cmpt = c;
+  s.need_update = s.need_rebuild = true;
   return ECok;
 }
 

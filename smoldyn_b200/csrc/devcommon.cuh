@@ -124,6 +124,8 @@ struct DevNet {
   // (products take the reactants' places), 2 = bounce (reactants pushed apart)
   uint8_t placement2[kMaxRxn];
   float bounce_k[kMaxRxn];   // bounce scaling: 1 (given unbinding radius) or 2 (from the binding radius)
+  int ncmpt;
+  uint8_t cmpt[3][kMaxRxn];  // compartment of each reaction + 1 (0: anywhere)
 };
 
 // Per-replicate geometry.  Cells are cubes of size h; the last cell in each
@@ -157,6 +159,18 @@ struct DevPanel {
   float posf, radiusf, centerf[3];   // FP32 copies for the screening test
   float p0f[3], nrmf[3];             // screen reference point and unit vector (zero for sph, hemi)
   int curved;                        // screen: 1 sph, cyl, hemi (radial test); 0 flat (plane test)
+};
+
+// Compartment (smolcomparts.c compartstruct subset): interior points, the
+// panels of its bounding surfaces (bit per panel index) and logic terms on
+// earlier compartments (symbol 0 equal, 1 equalnot, 2 and, 3 or, 4 xor,
+// 5 andnot, 6 ornot).  Positions relative to the system's low corner.
+struct DevCmpt {
+  int npts, ncl;
+  uint32_t panels;
+  int pad;
+  double pts[kMaxCmptPts][3];
+  int clsym[kMaxCmptLogic], clcmpt[kMaxCmptLogic];
 };
 
 struct Event {      // one reaction or birth; products are placed by k_products

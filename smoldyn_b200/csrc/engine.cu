@@ -31,11 +31,13 @@
 #include "devcommon.cuh"
 #include "engine.h"
 #include "rxnparam.cuh"
+#include "panelgeom.cuh"
 
 namespace smolb {
 
 __constant__ DevNet c_net;
 __constant__ DevPanel c_panels[kMaxPanels];
+__constant__ DevCmpt c_cmpt[kMaxCmpt];
 __constant__ DevGeo c_geo0;  // geometry of replicate 0 (used when the engine holds one replicate)
 
 struct KParams {
@@ -282,205 +284,6 @@ __device__ __forceinline__ int panel_action(const DevPanel &pn, int face, int sp
   return pn.act_back;
 }
 
-__device__ __forceinline__ double dot3(const double a[3], const double b[3]) {
-  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
-}
-
-// component of x - pt[0] normal to a cylinder's axis
-__device__ __forceinline__ void cyl_radial(const DevPanel &pn, const double x[3], double r[3]) {
-  double w[3];
-  for (int d = 0; d < 3; ++d) w[d] = x[d] - pn.pt[0][d];
-  const double s = dot3(w, pn.nrm);
-  for (int d = 0; d < 3; ++d) r[d] = w[d] - s * pn.nrm[d];
-}
-
-// unit normal toward the front face at point x of the panel (panelnormal,
-// smolsurface.c:3967)
-template <bool GEN>
-__device__ __forceinline__ void panel_normal(const DevPanel &pn, const double x[3], double n[3]) {
-  if (pn.shape == 2 || (GEN && (pn.shape == 4 || pn.shape == 3))) {  // sph, hemi: from the centre; cyl: from the axis
-    if (GEN && pn.shape == 3) {
-      cyl_radial(pn, x, n);
-    } else {
-      for (int d = 0; d < 3; ++d) n[d] = x[d] - pn.center[d];
-    }
-    const double l2 = dot3(n, n);
-    const double l = (l2 > 0) ? pn.front_sign / sqrt(l2) : 0.0;
-    for (int d = 0; d < 3; ++d) n[d] *= l;
-  } else if (GEN && (pn.shape == 1 || pn.shape == 5)) {  // tri, disk: the front normal
-    for (int d = 0; d < 3; ++d) n[d] = pn.nrm[d];
-  } else {
-    n[0] = n[1] = n[2] = 0.0;
-    n[pn.axis] = (double)pn.front_sign;
-  }
-}
-
-// signed distance from the panel's surface, positive on the front side
-// (panelside, smolsurface.c:3930)
-template <bool GEN>
-__device__ __forceinline__ double panel_sdist(const DevPanel &pn, const double x[3]) {
-  if (pn.shape == 2 || (GEN && pn.shape == 4)) {
-    double r2 = 0;
-    for (int d = 0; d < 3; ++d) r2 += (x[d] - pn.center[d]) * (x[d] - pn.center[d]);
-    return pn.front_sign * (sqrt(r2) - pn.radius);
-  }
-  if (GEN && pn.shape == 3) {
-    double r[3];
-    cyl_radial(pn, x, r);
-    return pn.front_sign * (sqrt(dot3(r, r)) - pn.radius);
-  }
-  if (GEN && (pn.shape == 1 || pn.shape == 5)) {
-    const double *o = pn.shape == 1 ? pn.pt[0] : pn.center;
-    double w[3];
-    for (int d = 0; d < 3; ++d) w[d] = x[d] - o[d];
-    return dot3(w, pn.nrm);
-  }
-  return pn.front_sign * (x[pn.axis] - pn.pos);
-}
-
-// whether a point on a curved panel's full surface lies on the panel: the
-// closed half of a hemisphere away from its open side; a cylinder between
-// its end planes (smolsurface.c:4060-4065, Geo_PtInSlab)
-__device__ __forceinline__ bool on_curved_part(const DevPanel &pn, const double x[3]) {
-  double w[3];
-  if (pn.shape == 4) {
-    for (int d = 0; d < 3; ++d) w[d] = x[d] - pn.center[d];
-    return dot3(w, pn.nrm) <= 0;
-  }
-  if (pn.shape == 3) {
-    for (int d = 0; d < 3; ++d) w[d] = x[d] - pn.pt[0][d];
-    const double s = dot3(w, pn.nrm);
-    return s >= 0 && s <= pn.axlen;
-  }
-  return true;
-}
-
-// Crossings with the shapes other than rect and sphere.  Kernels are compiled
-// in two surface forms: rect and sphere panels only (GEN false, the common
-// case, whose registers the other shapes would otherwise raise), and every
-// shape (GEN true).
-// quadric with an open part: cyl (radial parts only) and hemi
-__device__ __forceinline__ double cross_cyl_hemi(const DevPanel &pn, const double a[3], const double b[3], int &face) {
-  double v[3], w[3], vq[3];
-  for (int d = 0; d < 3; ++d) v[d] = b[d] - a[d];
-  if (pn.shape == 3) {
-    cyl_radial(pn, a, w);
-    const double s = dot3(v, pn.nrm);
-    for (int d = 0; d < 3; ++d) vq[d] = v[d] - s * pn.nrm[d];
-  } else {
-    for (int d = 0; d < 3; ++d) {
-      w[d] = a[d] - pn.center[d];
-      vq[d] = v[d];
-    }
-  }
-  const double vv = dot3(vq, vq), wv = dot3(w, vq), ww = dot3(w, w);
-  if (vv <= 0) return 2.0;
-  const double c = ww - pn.radius * pn.radius;
-  const double disc = wv * wv - vv * c;
-  if (disc < 0) return 2.0;
-  const double sq = sqrt(disc);
-  const bool inside = c < 0;
-  // the inside face is the back one when the front faces out
-  const int face_in = pn.front_sign > 0 ? 1 : 0, face_out = 1 - face_in;
-  const double t2 = (-wv + sq) / vv;  // exit from the full quadric
-  double x[3];
-  if (!inside) {
-    const double t1 = (-wv - sq) / vv;  // entry
-    if (!(t1 > 0 && t1 <= 1)) return 2.0;
-    for (int d = 0; d < 3; ++d) x[d] = a[d] + t1 * v[d];
-    if (on_curved_part(pn, x)) {
-      face = face_out;
-      return t1;
-    }
-    // entered through the open part: the exit may still hit the panel from
-    // inside (smolsurface.c:4062-4069)
-    if (!(t2 > 0 && t2 <= 1)) return 2.0;
-    for (int d = 0; d < 3; ++d) x[d] = a[d] + t2 * v[d];
-    if (!on_curved_part(pn, x)) return 2.0;
-    face = face_in;
-    return t2;
-  }
-  if (!(t2 > 0 && t2 <= 1)) return 2.0;
-  for (int d = 0; d < 3; ++d) x[d] = a[d] + t2 * v[d];
-  if (!on_curved_part(pn, x)) return 2.0;
-  face = face_in;
-  return t2;
-}
-
-// flat: tri and disk in the plane of their front normal
-__device__ __forceinline__ double cross_tri_disk(const DevPanel &pn, const double a[3], const double b[3], int &face) {
-  const double *o = pn.shape == 1 ? pn.pt[0] : pn.center;
-  double w0[3], w1[3];
-  for (int d = 0; d < 3; ++d) {
-    w0[d] = a[d] - o[d];
-    w1[d] = b[d] - o[d];
-  }
-  const double d0 = dot3(w0, pn.nrm), d1 = dot3(w1, pn.nrm);
-  if (d0 == 0 || (d0 > 0) == (d1 > 0)) return 2.0;
-  const double t = d0 / (d0 - d1);
-  if (!(t > 0 && t <= 1)) return 2.0;
-  double x[3];
-  for (int d = 0; d < 3; ++d) x[d] = a[d] + t * (b[d] - a[d]);
-  if (pn.shape == 5) {
-    double r2 = 0;
-    for (int d = 0; d < 3; ++d) r2 += (x[d] - pn.center[d]) * (x[d] - pn.center[d]);
-    if (r2 > pn.radius * pn.radius) return 2.0;
-  } else {
-    // inside when on the inner side of all three edges (Geo_PtInTriangle2)
-    for (int k = 0; k < 3; ++k) {
-      const double *p = pn.pt[k], *q = pn.pt[(k + 1) % 3];
-      const double e[3] = {q[0] - p[0], q[1] - p[1], q[2] - p[2]};
-      const double f[3] = {x[0] - p[0], x[1] - p[1], x[2] - p[2]};
-      const double cr[3] = {e[1] * f[2] - e[2] * f[1], e[2] * f[0] - e[0] * f[2], e[0] * f[1] - e[1] * f[0]};
-      if (dot3(cr, pn.nrm) < 0) return 2.0;
-    }
-  }
-  face = d0 > 0 ? 0 : 1;
-  return t;
-}
-
-// Crossing of segment a->b with a panel: t in (0,1] and the face hit, or
-// t = 2 when the segment does not cross (smolsurface.c:4000 lineXpanel).
-template <bool GEN>
-__device__ __forceinline__ double panel_cross(const DevPanel &pn, const double a[3], const double b[3], int &face) {
-  if (GEN && (pn.shape == 1 || pn.shape == 5)) return cross_tri_disk(pn, a, b, face);
-  if (GEN && (pn.shape == 3 || pn.shape == 4)) return cross_cyl_hemi(pn, a, b, face);
-  double v[3];
-  for (int d = 0; d < 3; ++d) v[d] = b[d] - a[d];
-  if (pn.shape == 2) {
-    double w[3], vv = 0, wv = 0, ww = 0;
-    for (int d = 0; d < 3; ++d) {
-      w[d] = a[d] - pn.center[d];
-      vv += v[d] * v[d];
-      wv += w[d] * v[d];
-      ww += w[d] * w[d];
-    }
-    if (vv <= 0) return 2.0;
-    const double c = ww - pn.radius * pn.radius;
-    const double disc = wv * wv - vv * c;
-    if (disc < 0) return 2.0;
-    const double sq = sqrt(disc);
-    const bool inside = c < 0;
-    const double t = inside ? (-wv + sq) / vv : (-wv - sq) / vv;
-    if (!(t > 0 && t <= 1)) return 2.0;
-    // arriving from inside: the inside face is the back one when front faces out
-    face = (inside == (pn.front_sign > 0)) ? 1 : 0;
-    return t;
-  }
-  const int ax = pn.axis;
-  const double d0 = a[ax] - pn.pos, d1 = b[ax] - pn.pos;
-  if (d0 == 0 || (d0 > 0) == (d1 > 0)) return 2.0;
-  const double t = d0 / (d0 - d1);
-  if (!(t > 0 && t <= 1)) return 2.0;
-  for (int d = 0; d < 3; ++d) {
-    if (d == ax) continue;
-    const double x = a[d] + t * v[d];
-    if (x < pn.lo[d] || x > pn.hi[d]) return 2.0;
-  }
-  face = ((d0 > 0) == (pn.front_sign > 0)) ? 0 : 1;
-  return t;
-}
-
 // Returns 1 if the molecule is absorbed; p1 is updated in place.
 // FP32 screen for the surface walk: false when the move a0 -> a1 (absolute
 // coordinates) stays more than the margin away from every panel, so no
@@ -619,6 +422,41 @@ __device__ __noinline__ bool pair_crosses_surface_call(const DevGeo &g, float4 p
   return pair_crosses_surface<GEN>(g, pc, vx, vy, vz);
 }
 
+// First-order decision when the reaction whose coin succeeded (list slot m)
+// is restricted to a compartment (unireact, smolreact.c:3040-3050): it fires
+// only if the molecule's new position lies in the compartment; otherwise the
+// decision passes to the reactions after it in the species' list, each with
+// its own coin.  thr holds the cumulative probabilities of the list as
+// fractions of 2^32, so with a fresh uniform u the first of the remaining
+// reactions to fire is the first k > m with u < 1 - (1 - cum_k) / (1 - cum_m).
+// Returns 2 + reaction, or 0 when none fires.
+__device__ __noinline__ int uni_in_cmpt(const uint32_t *thr, int nuni, int sp, int m, float4 pc, const DevGeo &g,
+                                        ull skey, uint32_t step) {
+  int ix[3];
+  unpack_cell(__float_as_uint(pc.w), ix[0], ix[1], ix[2]);
+  const float u[3] = {pc.x, pc.y, pc.z};
+  double x[3];
+  to_abs(g, ix, u, x);
+  const uint2 key = make_uint2(c_net.key0 ^ 0x2545F491u, c_net.key1 ^ 0x4F6CDD1Du);
+  const double inv32 = 1.0 / 4294967296.0;
+  for (int round = 0; round < kMaxUniPerSpecies && m < nuni; ++round) {
+    const int rx = c_net.uni_list[sp][m];
+    const int c = c_net.cmpt[1][rx];
+    if (!c || pos_in_cmpt(c_cmpt, c - 1, c_panels, x)) return 2 + rx;
+    const uint4 rr = philox(make_uint4((uint32_t)skey, (uint32_t)(skey >> 32), step, 16u + (uint32_t)round), key);
+    const double uu = ((double)rr.x + 0.5) * inv32;
+    const double rest_m = 1.0 - (double)thr[m] * inv32;
+    int next = nuni;
+    for (int k = m + 1; k < nuni; ++k)
+      if (rest_m > 0 && uu < 1.0 - (1.0 - (double)thr[k] * inv32) / rest_m) {
+        next = k;
+        break;
+      }
+    m = next;
+  }
+  return 0;
+}
+
 // Move one molecule by one step (diffuse smolmolec.c:3115, checkwalls
 // smolwall.c:368, unireact decision smolreact.c:2997): returns 0 alive,
 // 1 removed by a wall, 2+r first-order reaction r fired (position is the
@@ -744,7 +582,11 @@ __device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, co
     } else {
       const uint32_t *thr = p.unithr + (size_t)(rep * c_net.nsp + sp) * kMaxUniPerSpecies;
       for (int m = 0; m < nuni; ++m)
-        if (r.w < thr[m]) return 2 + c_net.uni_list[sp][m];
+        if (r.w < thr[m]) {
+          const int rx = c_net.uni_list[sp][m];
+          if (SURF == 2 && c_net.cmpt[1][rx]) return uni_in_cmpt(thr, nuni, sp, m, pc, g, skey, step);
+          return 2 + rx;
+        }
     }
   }
   return 0;
@@ -1172,13 +1014,38 @@ __device__ __forceinline__ bool pair_coin(ull ka, ull kb, int r, uint32_t step, 
 }
 
 // First reaction (in list order) that fires for this pair, or -1.
+// Whether both molecules of a pair (sorted indices ia, ib) lie in compartment
+// c: the compartment test of a restricted bimolecular reaction
+// (morebireact, smolreact.c:3115).
+__device__ __noinline__ bool pair_in_cmpt(const KParams &p, int c, int ia, int ib) {
+  for (int k = 0; k < 2; ++k) {
+    const int idx = k ? ib : ia;
+    const float4 q = p.b_pc[idx];
+    const DevGeo &g = p.geo[id_rep(p.b_id[idx])];
+    int ix[3];
+    unpack_cell(__float_as_uint(q.w), ix[0], ix[1], ix[2]);
+    const float u[3] = {q.x, q.y, q.z};
+    double x[3];
+    to_abs(g, ix, u, x);
+    if (!pos_in_cmpt(c_cmpt, c, c_panels, x)) return false;
+  }
+  return true;
+}
+
+// The reaction a pair at squared distance d2 undergoes this step, or -1: the
+// first of the pair's reactions whose binding radius, coin and (CMPT)
+// compartment test pass (bireact, smolreact.c:3201-3298).
+template <bool CMPT>
 __device__ __forceinline__ int pair_reaction(const KParams &p, int rep, int spa, int spb, float d2,
-                                             ull ka, ull kb, uint32_t step) {
+                                             ull ka, ull kb, uint32_t step, int ia, int ib) {
   const int nl = c_net.pair_n[spa][spb];
   const int nr2 = c_net.nr[2];
   for (int m = 0; m < nl; ++m) {
     const int r = c_net.pair_list[spa][spb][m];
-    if (d2 <= p.bind2[rep * nr2 + r] && pair_coin(ka, kb, r, step, p.pairprob[rep * nr2 + r])) return r;
+    if (d2 <= p.bind2[rep * nr2 + r] && pair_coin(ka, kb, r, step, p.pairprob[rep * nr2 + r])) {
+      if (CMPT && c_net.cmpt[2][r] && !pair_in_cmpt(p, c_net.cmpt[2][r] - 1, ia, ib)) continue;
+      return r;
+    }
   }
   return -1;
 }
@@ -1242,7 +1109,7 @@ __device__ ull search_partner(const KParams &p, int i, float4 pc, ull id, uint32
           const float vy = (q.y - pc.y) + (float)dy * g.h[1];
           const float vz = (q.z - pc.z) + (float)dz * g.h[2];
           const float d2 = vx * vx + vy * vy + vz * vz;
-          if (pair_reaction(p, rep, sp, spj, d2, ka, id_stream(jd), step) < 0) continue;
+          if (pair_reaction<SURF == 2>(p, rep, sp, spj, d2, ka, id_stream(jd), step, i, j) < 0) continue;
           if (SURF && pair_crosses_surface_call<SURF == 2>(g, pc, vx, vy, vz)) continue;
           ncand++;
           const ull k = ((ull)__float_as_uint(d2) << 32) | (uint32_t)j;
@@ -1267,74 +1134,6 @@ __device__ __forceinline__ int register_candidate(const KParams &p, int x, ull k
   return 1;
 }
 
-// Round-1 pair search: every in-radius pair is tested once, by its molecule of
-// the lower species index (or the lower sorted index for like species), and
-// registered on both molecules as packed (dist2 bits << 32 | partner) keys.
-__device__ int search_round1(const KParams &p, int i, float4 pc, ull id, uint32_t step) {
-  const int nsorted = *p.b_n;
-  const int sp = id_species(id);
-  const int rep = id_rep(id);
-  const DevGeo &g = p.geo[rep];
-  const uint32_t mask = c_net.search_mask[sp];
-  int ix, iy, iz;
-  unpack_cell(__float_as_uint(pc.w), ix, iy, iz);
-  const bool px = g.wall[0] == kWallPeriodic, py = g.wall[2] == kWallPeriodic, pz = g.wall[4] == kWallPeriodic;
-  const ull ka = id_stream(id);
-  const float rs = p.rsearch[rep * c_net.nsp + sp];
-  const float rs2 = rs * rs;
-  const float ub0 = (ix == g.n[0] - 1) ? g.whi[0] : g.h[0];
-  const float ub1 = (iy == g.n[1] - 1) ? g.whi[1] : g.h[1];
-  const float ub2 = (iz == g.n[2] - 1) ? g.whi[2] : g.h[2];
-  const int xlo = pc.x < rs ? -1 : 0, xhi = pc.x > ub0 - rs ? 1 : 0;
-  const int ylo = pc.y < rs ? -1 : 0, yhi = pc.y > ub1 - rs ? 1 : 0;
-  const int zlo = pc.z < rs ? -1 : 0, zhi = pc.z > ub2 - rs ? 1 : 0;
-  ull best = ~0ull;
-  int extra = 0;
-  for (int dz = zlo; dz <= zhi; ++dz) {
-    int z = iz + dz;
-    if (z < 0 || z >= g.n[2]) {
-      if (!pz) continue;
-      z = (z < 0) ? z + g.n[2] : z - g.n[2];
-    }
-    for (int dy = ylo; dy <= yhi; ++dy) {
-      int y = iy + dy;
-      if (y < 0 || y >= g.n[1]) {
-        if (!py) continue;
-        y = (y < 0) ? y + g.n[1] : y - g.n[1];
-      }
-      const int rowbase = g.cell0 + (z * g.n[1] + y) * g.n[0];
-      for (int dx = xlo; dx <= xhi; ++dx) {
-        int x = ix + dx;
-        if (x < 0 || x >= g.n[0]) {
-          if (!px) continue;
-          x = (x < 0) ? x + g.n[0] : x - g.n[0];
-        }
-        const int c = rowbase + x;
-        const int s = p.start[c], e = min(p.start[c + 1], nsorted);
-        for (int j = s; j < e; ++j) {
-          const ull jd = p.b_id[j];
-          const int spj = id_species(jd);
-          if (!((mask >> spj) & 1u) || (spj == sp && j <= i)) continue;
-          const float4 q = p.b_pc[j];
-          const float vx = (q.x - pc.x) + (float)dx * g.h[0];
-          const float vy = (q.y - pc.y) + (float)dy * g.h[1];
-          const float vz = (q.z - pc.z) + (float)dz * g.h[2];
-          const float d2 = vx * vx + vy * vy + vz * vz;
-          if (d2 > rs2) continue;
-          if (pair_reaction(p, rep, sp, spj, d2, ka, id_stream(jd), step) < 0) continue;
-          const uint32_t db = __float_as_uint(d2);
-          const ull k = ((ull)db << 32) | (uint32_t)j;
-          if (best != ~0ull) extra++;
-          if (k < best) best = k;
-          extra += register_candidate(p, j, ((ull)db << 32) | (uint32_t)i);
-        }
-      }
-    }
-  }
-  if (best != ~0ull) extra += register_candidate(p, i, best);
-  return extra;
-}
-
 // Pair test shared by the staged and the neighbour-box paths: if i and j react
 // this step, fold the key into i's running best and register i on j.
 template <int SURF>
@@ -1345,7 +1144,7 @@ __device__ __forceinline__ void try_pair(const KParams &p, int i, ull idi, int s
   const int spj = id_species(jd);
   if (spj == kDeadSpecies || !((c_net.pair_mask[sp] >> spj) & 1u)) return;
   if (SURF && pair_crosses_surface_call<SURF == 2>(p.geo[rep], pc, vx, vy, vz)) return;
-  if (pair_reaction(p, rep, sp, spj, d2, id_stream(idi), id_stream(jd), step) < 0) return;
+  if (pair_reaction<SURF == 2>(p, rep, sp, spj, d2, id_stream(idi), id_stream(jd), step, i, j) < 0) return;
   const uint32_t db = __float_as_uint(d2);
   const ull k = ((ull)db << 32) | (uint32_t)j;
   if (best != ~0ull) extra++;
@@ -1482,7 +1281,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_pairs_tile(KParams p) {
           // the reaction test draws from a stateless stream, so it can go
           // before the (rarely needed) surface test
           if (spb != kDeadSpecies && ((c_net.pair_mask[spa] >> spb) & 1u) &&
-              pair_reaction(p, repa, spa, spb, d2, id_stream(ida), id_stream(idb), step) >= 0 &&
+              pair_reaction<SURF == 2>(p, repa, spa, spb, d2, id_stream(ida), id_stream(idb), step, wb + o, wb + tj) >= 0 &&
               !(SURF && pair_crosses_surface<SURF == 2>(p.geo[repa], a, vx, vy, vz)))
             extra += register_pair(p, wb + o, wb + tj, d2);
         }
@@ -1500,7 +1299,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_pairs_tile(KParams p) {
         const ull idb = p.b_id[j];
         const int spb = id_species(idb);
         if (spb != kDeadSpecies && ((c_net.pair_mask[sp] >> spb) & 1u) &&
-            pair_reaction(p, rep, sp, spb, d2, id_stream(idi), id_stream(idb), step) >= 0 &&
+            pair_reaction<SURF == 2>(p, rep, sp, spb, d2, id_stream(idi), id_stream(idb), step, i, j) >= 0 &&
             !(SURF && pair_crosses_surface<SURF == 2>(p.geo[rep], pc, vx, vy, vz)))
           extra += register_pair(p, i, j, d2);
       }
@@ -1688,6 +1487,7 @@ __device__ __forceinline__ float4 pair_site(const KParams &p, int i, int j, int 
   return make_float4(w[0], w[1], w[2], __uint_as_float(pack_cell(cell[0], cell[1], cell[2])));
 }
 
+template <int SURF>
 __global__ void k_commit(KParams p) {
   pdl_launch_dependents();
   pdl_wait();
@@ -1707,7 +1507,7 @@ __global__ void k_commit(KParams p) {
     if (spi == kDeadSpecies || spj == kDeadSpecies) continue;
     const int rep = id_rep(idi);
     const float d2 = __uint_as_float((uint32_t)(bi >> 32));
-    const int r = pair_reaction(p, rep, spi, spj, d2, id_stream(idi), id_stream(idj), step);
+    const int r = pair_reaction<SURF == 2>(p, rep, spi, spj, d2, id_stream(idi), id_stream(idj), step, i, j);
     if (r < 0) continue;
     // reactant 1 of reaction r is molecule a
     const bool i_first = (c_net.rct[2][r][0] == spi);
@@ -1745,6 +1545,44 @@ __device__ __forceinline__ void random_rotation(uint4 r, float m[9]) {
   m[6] = 2.f * (qx * qz - qy * qw); m[7] = 2.f * (qy * qz + qx * qw); m[8] = 1.f - 2.f * (qx * qx + qy * qy);
 }
 
+// Birth position in compartment c (compartrandpos, smolcomparts.c:194-220):
+// uniform points in the system until one lies in the compartment, at most
+// 10000 tries, then one of its interior points.  site/cell hold the first
+// (uniform) try on entry.
+__device__ __noinline__ void birth_in_cmpt(int c, const DevGeo &g, ull ekey, uint32_t step, float site[3],
+                                           int cell[3]) {
+  const uint2 key = make_uint2(c_net.key0 ^ 0x1B873593u, c_net.key1 ^ 0xCC9E2D51u);
+  for (int t = 0; t < 10000; ++t) {
+    double x[3];
+    to_abs(g, cell, site, x);
+    if (pos_in_cmpt(c_cmpt, c, c_panels, x)) return;
+    const uint4 rr = philox(make_uint4((uint32_t)ekey, (uint32_t)(ekey >> 32), step, 32u + (uint32_t)t), key);
+    const uint32_t bits[3] = {rr.x, rr.y, rr.z};
+    for (int d = 0; d < 3; ++d) {
+      if (d >= g.dim) continue;
+      const float L = (float)(g.n[d] - 1) * g.h[d] + g.whi[d];
+      float w = u01f_open(bits[d]) * L;
+      int j = 0;
+      renorm(w, j, g.h[d], g.inv_h[d]);
+      if (j > g.n[d] - 1) { w += (float)(j - (g.n[d] - 1)) * g.h[d]; j = g.n[d] - 1; }
+      clamp_cell(w, j, g, d);
+      site[d] = w;
+      cell[d] = j;
+    }
+  }
+  const DevCmpt &q = c_cmpt[c];
+  if (q.npts <= 0) return;
+  double x[3];
+  for (int d = 0; d < 3; ++d) x[d] = q.pts[(int)(ekey % (ull)q.npts)][d];
+  int ix[3];
+  float u[3];
+  from_abs(g, x, ix, u);
+  for (int d = 0; d < 3; ++d) {
+    site[d] = u[d];
+    cell[d] = ix[d];
+  }
+}
+
 template <int SURF>
 __global__ void k_products(KParams p) {
   pdl_launch_dependents();
@@ -1773,6 +1611,7 @@ __global__ void k_products(KParams p) {
         site[d] = w;
         cell[d] = j;
       }
+      if (SURF == 2 && c_net.cmpt[0][r]) birth_in_cmpt(c_net.cmpt[0][r] - 1, g, e.key, step, site, cell);
     } else {
       site[0] = e.site.x; site[1] = e.site.y; site[2] = e.site.z;
       unpack_cell(__float_as_uint(e.site.w), cell[0], cell[1], cell[2]);
@@ -2087,6 +1926,7 @@ class EngineImpl {
   DevNet dnet{};
   std::vector<DevGeo> geo;
   std::vector<DevPanel> panels;
+  std::vector<DevCmpt> cmpts;
   double dt = 0;
   uint64_t seed = 0;
   long long cap = 0, pcap = 0, evcap = 0, candcap = 0;
@@ -2362,12 +2202,12 @@ class EngineImpl {
     mark("k_pairs");
     launch(k_pairs_faces<SINGLE, SURF>, grid_mol(), 256, 0, p);
     mark("k_pairs_faces");
-    launch(k_commit, grid_small(), 128, 0, p);
+    launch(k_commit<SURF>, grid_small(), 128, 0, p);
     mark("k_commit");
     for (int round = 1; round < dnet.rounds; ++round) {
       launch(k_research<SURF>, grid_small(), 128, 0, p);
       mark("k_research");
-      launch(k_commit, grid_small(), 128, 0, p);
+      launch(k_commit<SURF>, grid_small(), 128, 0, p);
       mark("k_commit");
     }
     launch(k_products<SURF>, grid_small(), 128, 0, p);
@@ -2376,10 +2216,12 @@ class EngineImpl {
 
   // Enqueue one step with the given parity (inputs A/P = buffers `par`).
   void enqueue_step(int par, bool rebin_only) {
-    // surface form: 0 none, 1 rect and sphere panels only, 2 any shape
+    // surface form: 0 none, 1 rect and sphere panels only, 2 any shape or
+    // compartments (whose tests need panels to mean anything)
     int surf = dnet.npanel > 0 ? 1 : 0;
     for (const DevPanel &pn : panels)
       if (pn.shape != 0 && pn.shape != 2) surf = 2;
+    if (surf && dnet.ncmpt > 0) surf = 2;
     if (single_rep()) {
       if (surf == 0) enqueue_step_t<true, 0>(par, rebin_only);
       else if (surf == 1) enqueue_step_t<true, 1>(par, rebin_only);
@@ -2399,6 +2241,9 @@ class EngineImpl {
       CK(cudaMemcpyToSymbolAsync(c_geo0, geo.data(), sizeof(DevGeo), 0, cudaMemcpyHostToDevice, stream));
     if (!panels.empty())
       CK(cudaMemcpyToSymbolAsync(c_panels, panels.data(), panels.size() * sizeof(DevPanel), 0,
+                                 cudaMemcpyHostToDevice, stream));
+    if (!cmpts.empty())
+      CK(cudaMemcpyToSymbolAsync(c_cmpt, cmpts.data(), cmpts.size() * sizeof(DevCmpt), 0,
                                  cudaMemcpyHostToDevice, stream));
     return 0;
   }
@@ -2724,51 +2569,16 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
     if ((int)E.net.panels.size() > kMaxPanels) { if (err) *err = "too many panels (max 16)"; return -6; }
     E.panels.clear();
     for (const PanelSpec &ps : E.net.panels) {
-      DevPanel dp{};
-      const RepSpec &s0 = reps[0];
-      dp.shape = ps.shape;
-      dp.axis = ps.axis;
-      dp.front_sign = ps.front_sign;
-      dp.pos = ps.pos - s0.lo[ps.axis];
-      for (int d = 0; d < 3; ++d) {
-        dp.lo[d] = ps.lo[d] - s0.lo[d];
-        dp.hi[d] = ps.hi[d] - s0.lo[d];
-        dp.center[d] = ps.center[d] - s0.lo[d];
-      }
-      dp.radius = ps.radius;
-      for (int k = 0; k < 3; ++k)
-        for (int d = 0; d < 3; ++d) dp.pt[k][d] = ps.pt[k][d] - s0.lo[d];
-      for (int d = 0; d < 3; ++d) dp.nrm[d] = ps.normal[d];
-      dp.axlen = 0;
-      if (ps.shape == 3)
-        for (int d = 0; d < 3; ++d) dp.axlen += (dp.pt[1][d] - dp.pt[0][d]) * dp.nrm[d];
-      dp.posf = (float)dp.pos;
-      dp.radiusf = (float)dp.radius;
-      dp.curved = (ps.shape == 2 || ps.shape == 3 || ps.shape == 4) ? 1 : 0;
-      for (int d = 0; d < 3; ++d) {
-        dp.centerf[d] = (float)dp.center[d];
-        // screen reference point and unit vector: rect plane point and axis;
-        // tri vertex and normal; disk centre and normal; sph / hemi centre and
-        // no vector; cyl axis start and axis
-        double p0 = 0, n0 = 0;
-        if (ps.shape == 0) { p0 = d == ps.axis ? dp.pos : 0.0; n0 = d == ps.axis ? 1.0 : 0.0; }
-        else if (ps.shape == 1 || ps.shape == 3) { p0 = dp.pt[0][d]; n0 = dp.nrm[d]; }
-        else if (ps.shape == 5) { p0 = dp.center[d]; n0 = dp.nrm[d]; }
-        else { p0 = dp.center[d]; n0 = 0.0; }
-        dp.p0f[d] = (float)p0;
-        dp.nrmf[d] = (float)n0;
-      }
-      dp.act_front = ps.action_front;
-      dp.act_back = ps.action_back;
-      dp.abs_front = ps.absorb_front_mask;
-      dp.abs_back = ps.absorb_back_mask;
-      dp.tr_front = ps.trans_front_mask;
-      dp.tr_back = ps.trans_back_mask;
-      dp.rf_front = ps.refl_front_mask;
-      dp.rf_back = ps.refl_back_mask;
+      const DevPanel dp = make_dev_panel(ps, reps[0].lo);
       E.panels.push_back(dp);
     }
   }
+  E.cmpts.clear();
+  if ((int)E.net.cmpts.size() > kMaxCmpt) { if (err) *err = "too many compartments (max 8)"; return -6; }
+  for (const CmptSpec &cs : E.net.cmpts) E.cmpts.push_back(make_dev_cmpt(cs, reps[0].lo));
+  E.dnet.ncmpt = (int)E.cmpts.size();
+  for (int o = 0; o < 3; ++o)
+    for (int r = 0; r < kMaxRxn; ++r) E.dnet.cmpt[o][r] = (uint8_t)E.net.cmpt[o][r];
   int rc = E.build_rep_tables(err);
   if (rc) return rc;
   E.nsteps = 0;

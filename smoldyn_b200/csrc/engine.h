@@ -21,6 +21,9 @@ constexpr int kMaxProd = 4;       // products per reaction
 constexpr int kMaxUniPerSpecies = 8;
 constexpr int kMaxPairRxn = 4;    // reactions per reactant species pair
 constexpr int kMaxPanels = 16;
+constexpr int kMaxCmpt = 8;         // compartments
+constexpr int kMaxCmptPts = 8;      // interior-defining points per compartment
+constexpr int kMaxCmptLogic = 4;    // logic terms per compartment
 
 enum WallKind : uint8_t { kWallReflect = 0, kWallPeriodic = 1, kWallAbsorb = 2, kWallTransparent = 3 };
 
@@ -48,6 +51,14 @@ struct PanelSpec {
   uint32_t refl_back_mask;
 };
 
+// Compartment: interior points, bounding panels (indices into NetSpec::panels)
+// and logic terms on earlier compartments (see DevCmpt).
+struct CmptSpec {
+  std::vector<std::vector<double>> pts;       // 3 coordinates each
+  uint32_t panel_mask = 0;
+  std::vector<std::pair<int, int>> logic;     // (symbol, compartment)
+};
+
 // Reaction network shared by every replicate.
 struct NetSpec {
   int nspecies = 1;                          // including index 0
@@ -60,6 +71,8 @@ struct NetSpec {
   double bounce_k[kMaxRxn] = {};             // bounce: 1 (unbinding radius given) or 2 (from binding radius)
   int gauss_table_size = 4096;               // power of two (smolmolec.c:781)
   std::vector<PanelSpec> panels;
+  std::vector<CmptSpec> cmpts;
+  int cmpt[3][kMaxRxn] = {};                 // compartment of each reaction + 1 (0: none)
 };
 
 // One replicate's geometry and rate-derived parameters.

@@ -9,6 +9,7 @@
 #include <sstream>
 
 #include "rxnparam.cuh"
+#include "panelgeom.cuh"
 
 namespace smolb {
 
@@ -35,6 +36,12 @@ Sim::Sim() {
 int Sim::species_index(const std::string &name) const {
   for (size_t i = 1; i < species.size(); ++i)
     if (species[i].name == name) return (int)i;
+  return -1;
+}
+
+int Sim::compartment_index(const std::string &name) const {
+  for (size_t c = 0; c < cmpts.size(); ++c)
+    if (cmpts[c].name == name) return (int)c;
   return -1;
 }
 
@@ -106,7 +113,7 @@ int derive_reaction_params(Sim &sim, std::string *err) {
   for (RxnDef &x : sim.rxn[0]) {
     if (x.disabled) { x.prob = 0; continue; }
     if (x.rate < 0) { if (err) *err = "reaction " + x.name + " rate is undefined"; return -8; }
-    x.prob = x.rate * dt * system_volume(sim);
+    x.prob = x.rate * dt * (x.cmpt >= 0 ? compartment_volume(sim, x.cmpt) : system_volume(sim));
   }
   // order 1
   for (size_t r = 0; r < sim.rxn[1].size(); ++r) {
@@ -341,7 +348,8 @@ double calc_rate(const Sim &sim, int order, int r, double *pgem) {
   const double dt = sim.dt;
   double ans = 0;
   if (order == 0) {
-    ans = x.prob < 0 ? 0 : x.prob / dt / system_volume(sim);
+    const double vol = x.cmpt >= 0 ? (x.cmpt < (int)sim.cmpts.size() ? sim.cmpts[x.cmpt].volume : 0) : system_volume(sim);
+    ans = x.prob < 0 || !(vol > 0) ? 0 : x.prob / dt / vol;
   } else if (order == 1) {
     if (x.prob > 0) {
       const int i1 = x.rct[0];
@@ -413,6 +421,107 @@ void set_species_difm(Sim &sim, int sp, const double *m) {
   x.difc = tr / dim;
 }
 
+// ---- compartments ----------------------------------------------------------
+namespace {
+// Index of each surface's first panel in the engine's panel list (surfaces in
+// order, their panels in order).
+std::vector<int> surface_panel_base(const Sim &sim) {
+  std::vector<int> first(sim.surfaces.size());
+  int n = 0;
+  for (size_t k = 0; k < sim.surfaces.size(); ++k) {
+    first[k] = n;
+    n += (int)sim.surfaces[k].panels.size();
+  }
+  return first;
+}
+
+CmptSpec cmpt_spec(const Sim &sim, const CompartDef &c, const std::vector<int> &first) {
+  CmptSpec cs;
+  cs.pts = c.pts;
+  for (int sidx : c.surfaces)
+    for (size_t q = 0; q < sim.surfaces[sidx].panels.size(); ++q) {
+      const int pi = first[sidx] + (int)q;
+      if (pi < 32) cs.panel_mask |= 1u << pi;
+    }
+  cs.logic = c.logic;
+  return cs;
+}
+
+// Panels and compartments in device form for host-side membership tests.
+struct CmptTester {
+  std::vector<DevPanel> panels;
+  std::vector<DevCmpt> cmpts;
+  double lo[3] = {0, 0, 0};
+  explicit CmptTester(const Sim &sim) {
+    for (int d = 0; d < 3; ++d) lo[d] = d < sim.dim ? sim.lo[d] : 0.0;
+    for (const SurfaceDef &sf : sim.surfaces)
+      for (const PanelSpec &ps : sf.panels) panels.push_back(make_dev_panel(ps, lo));
+    panels.resize(std::max<size_t>(panels.size(), 1));
+    const std::vector<int> first = surface_panel_base(sim);
+    for (const CompartDef &c : sim.cmpts) cmpts.push_back(make_dev_cmpt(cmpt_spec(sim, c, first), lo));
+  }
+  bool inside(int c, const double xa[3]) const {
+    const double x[3] = {xa[0] - lo[0], xa[1] - lo[1], xa[2] - lo[2]};
+    return pos_in_cmpt(cmpts.data(), c, panels.data(), x);
+  }
+};
+
+double sys_volume(const Sim &s) {
+  double v = 1;
+  for (int d = 0; d < s.dim; ++d) v *= s.hi[d] - s.lo[d];
+  return v;
+}
+}  // namespace
+
+bool pos_in_compartment(const Sim &sim, int c, const double x[3]) {
+  if (c < 0 || c >= (int)sim.cmpts.size()) return false;
+  return CmptTester(sim).inside(c, x);
+}
+
+void invalidate_compartments(Sim &sim) {
+  for (CompartDef &c : sim.cmpts) c.volume = -1;
+}
+
+// The reference estimates the volume from 100 random points per box
+// (compartupdatebox, smolcomparts.c:700-760); here 2^18 uniform points over
+// the whole system, from a fixed-seed generator so that the derived rates do
+// not depend on the simulation's random stream.
+double compartment_volume(Sim &sim, int c) {
+  if (c < 0 || c >= (int)sim.cmpts.size()) return 0;
+  CompartDef &cd = sim.cmpts[c];
+  if (cd.volume >= 0) return cd.volume;
+  const CmptTester t(sim);
+  uint64_t st = 0x9E3779B97F4A7C15ull ^ (uint64_t)(c + 1) * 0xD1B54A32D192ED03ull;
+  auto next = [&st]() {  // splitmix64
+    uint64_t z = (st += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  };
+  const int n = 1 << 18;
+  int in = 0;
+  for (int k = 0; k < n; ++k) {
+    double x[3] = {0, 0, 0};
+    for (int d = 0; d < sim.dim; ++d)
+      x[d] = sim.lo[d] + ((double)(next() >> 11) + 0.5) * (1.0 / 9007199254740992.0) * (sim.hi[d] - sim.lo[d]);
+    if (t.inside(c, x)) ++in;
+  }
+  cd.volume = sys_volume(sim) * (double)in / (double)n;
+  return cd.volume;
+}
+
+void compartment_random_pos(Sim &sim, int c, double x[3]) {
+  const CmptTester t(sim);
+  for (int k = 0; k < 10000; ++k) {
+    for (int d = 0; d < 3; ++d) x[d] = d < sim.dim ? sim.lo[d] + sim.rand_u01() * (sim.hi[d] - sim.lo[d]) : 0.0;
+    if (t.inside(c, x)) return;
+  }
+  const CompartDef &cd = sim.cmpts[c];
+  if (cd.pts.empty()) return;
+  const size_t k = std::min(cd.pts.size() - 1, (size_t)(sim.rand_u01() * cd.pts.size()));
+  for (int d = 0; d < 3; ++d) x[d] = d < (int)cd.pts[k].size() ? cd.pts[k][d] : 0.0;
+}
+
 int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err) {
   *net = NetSpec();
   *rep = RepSpec();
@@ -435,6 +544,7 @@ int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err) {
       }
       for (int q = 0; q < x.nprod; ++q)
         for (int d = 0; d < 3; ++d) rep->prdpos[o][r][q][d] = x.prdpos[q][d];
+      net->cmpt[o][r] = x.cmpt >= 0 ? x.cmpt + 1 : 0;
       if (o == 0) rep->birth_mean[r] = x.prob;
       if (o == 1) rep->uni_prob[r] = x.prob;
       if (o == 2) {
@@ -478,6 +588,8 @@ int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err) {
       ps.refl_back_mask = sf.refl_back;
       net->panels.push_back(ps);
     }
+  const std::vector<int> first = surface_panel_base(sim);
+  for (const CompartDef &c : sim.cmpts) net->cmpts.push_back(cmpt_spec(sim, c, first));
   return 0;
 }
 
@@ -698,8 +810,48 @@ int read_config_statement(Sim &sim, const std::string &word, const std::string &
       sim.pend_sp.push_back(i);
     }
     sim.need_rebuild = true;
-  } else if (word == "reaction") {
-    return add_reaction_from_words(sim, w, err);
+  } else if (word == "compartment_mol") {  // smolsim.cpp:1072
+    if (!need(3)) return -7;
+    const long long n = atoll(w[0].c_str());
+    const int i = sim.species_index(w[1]);
+    if (i <= 0) { if (err) *err = "compartment_mol: unknown species " + w[1]; return -3; }
+    const int c = sim.compartment_index(w[2]);
+    if (c < 0) { if (err) *err = "compartment_mol: unknown compartment " + w[2]; return -3; }
+    for (long long k = 0; k < n; ++k) {
+      double x[3];
+      compartment_random_pos(sim, c, x);
+      for (int d = 0; d < 3; ++d) sim.pend_pos.push_back(x[d]);
+      sim.pend_sp.push_back(i);
+    }
+    sim.need_rebuild = true;
+  } else if (word == "reaction" || word == "reaction_cmpt") {
+    // reaction_cmpt cname ... (deprecated form) or reaction cmpt=cname ...
+    // (smolreact.c:2436-2470)
+    std::vector<std::string> ww = w;
+    int c = -1;
+    if (word == "reaction_cmpt") {
+      if (ww.empty()) { if (err) *err = "reaction_cmpt: missing compartment"; return -7; }
+      c = sim.compartment_index(ww[0]);
+      if (c < 0) { if (err) *err = "compartment name not recognized"; return -3; }
+      ww.erase(ww.begin());
+    }
+    while (!ww.empty() && ww[0].find('=') != std::string::npos) {
+      const std::string key = ww[0].substr(0, ww[0].find('=')), val = ww[0].substr(ww[0].find('=') + 1);
+      if (key == "cmpt" || key == "compartment") {
+        c = sim.compartment_index(val);
+        if (c < 0) { if (err) *err = "compartment name not recognized"; return -3; }
+      } else {
+        if (err) *err = "reaction restriction not supported by the GPU engine: " + ww[0];
+        return -7;
+      }
+      ww.erase(ww.begin());
+    }
+    size_t before[3] = {sim.rxn[0].size(), sim.rxn[1].size(), sim.rxn[2].size()};
+    const int rc = add_reaction_from_words(sim, ww, err);
+    if (rc) return rc;
+    for (int o = 0; o < 3; ++o)
+      for (size_t r = before[o]; r < sim.rxn[o].size(); ++r) sim.rxn[o][r].cmpt = c;
+    return 0;
   } else if (word == "reaction_rate") {
     if (!need(2)) return -7;
     int o;
@@ -873,6 +1025,53 @@ int make_panel(int dim, int shape, const std::string &axis, const double *prm, i
   return 0;
 }
 
+// compartment block statements (smolcomparts.c:880-930 cmptreadstring)
+static int read_compartment_statement(Sim &sim, int c, const std::string &word, const std::vector<std::string> &w,
+                                      std::string *err) {
+  CompartDef &cd = sim.cmpts[c];
+  if (word == "surface") {
+    if (w.empty()) { if (err) *err = "compartment surface: missing name"; return -7; }
+    int sidx = -1;
+    for (size_t k = 0; k < sim.surfaces.size(); ++k)
+      if (sim.surfaces[k].name == w[0]) sidx = (int)k;
+    if (sidx < 0) { if (err) *err = "compartment surface '" + w[0] + "' not recognized"; return -3; }
+    if (std::find(cd.surfaces.begin(), cd.surfaces.end(), sidx) != cd.surfaces.end()) {
+      if (err) *err = "cannot add surface to compartment more than once";
+      return -7;
+    }
+    cd.surfaces.push_back(sidx);
+  } else if (word == "point") {
+    if ((int)w.size() < sim.dim) { if (err) *err = "compartment point: missing values"; return -7; }
+    if ((int)cd.pts.size() >= kMaxCmptPts) { if (err) *err = "too many compartment points"; return -6; }
+    std::vector<double> p(3, 0.0);
+    for (int d = 0; d < sim.dim; ++d) p[d] = atof(w[d].c_str());
+    cd.pts.push_back(p);
+  } else if (word == "compartment") {
+    if (w.size() < 2) { if (err) *err = "compartment format: symbol name"; return -7; }
+    static const char *syms[] = {"equal", "equalnot", "and", "or", "xor", "andnot", "ornot"};
+    int sym = -1;
+    for (int k = 0; k < 7; ++k)
+      if (w[0] == syms[k]) sym = k;
+    if (sym < 0) { if (err) *err = "unrecognized logic symbol " + w[0]; return -7; }
+    const int other = sim.compartment_index(w[1]);
+    if (other < 0) { if (err) *err = "compartment name not recognized"; return -3; }
+    if (other == c) { if (err) *err = "cannot add a compartment to itself"; return -7; }
+    if ((int)cd.logic.size() >= kMaxCmptLogic) { if (err) *err = "too many compartment logic terms"; return -6; }
+    cd.logic.push_back({sym, other});
+  } else {
+    if (err) *err = "syntax error within compartment block: statement not recognized: " + word;
+    return -7;
+  }
+  invalidate_compartments(sim);
+  sim.need_update = sim.need_rebuild = true;
+  return 0;
+}
+
+int read_compartment_words(Sim &sim, int c, const std::string &word, const std::vector<std::string> &w,
+                           std::string *err) {
+  return read_compartment_statement(sim, c, word, w, err);
+}
+
 // surface block statements (smolsurface.c surfreadstring subset)
 static int read_surface_statement(Sim &sim, SurfaceDef &sf, const std::string &word,
                                   const std::vector<std::string> &w, std::string *err) {
@@ -937,6 +1136,7 @@ static int read_surface_statement(Sim &sim, SurfaceDef &sf, const std::string &w
     if (rc) return rc;
     if ((int)sf.panels.size() >= kMaxPanels) { if (err) *err = "too many panels"; return -6; }
     sf.panels.push_back(p);
+    invalidate_compartments(sim);
   } else if (word == "color" || word == "thickness" || word == "polygon" || word == "stipple" ||
              word == "shininess") {
   } else {
@@ -954,6 +1154,7 @@ int load_config_file(Sim &sim, const std::string &path, const std::string &name,
   std::string line;
   std::vector<int> skip;  // ifdefine nesting: 1 = skipping
   SurfaceDef *cur_srf = nullptr;
+  int cur_cmpt = -1;
   int lineno = 0;
   while (std::getline(in, line)) {
     ++lineno;
@@ -1019,8 +1220,31 @@ int load_config_file(Sim &sim, const std::string &path, const std::string &name,
       cur_srf = nullptr;
       continue;
     }
+    if (word == "start_compartment") {
+      std::string nm;
+      std::istringstream(rest) >> nm;
+      if (nm.empty() || sim.compartment_index(nm) >= 0) {
+        if (err) *err = full + ":" + std::to_string(lineno) + ": start_compartment: missing or repeated name";
+        return -7;
+      }
+      if ((int)sim.cmpts.size() >= kMaxCmpt) {
+        if (err) *err = full + ":" + std::to_string(lineno) + ": too many compartments";
+        return -6;
+      }
+      CompartDef c;
+      c.name = nm;
+      sim.cmpts.push_back(c);
+      cur_cmpt = (int)sim.cmpts.size() - 1;
+      sim.need_rebuild = true;
+      continue;
+    }
+    if (word == "end_compartment") {
+      cur_cmpt = -1;
+      continue;
+    }
     int rc;
     if (cur_srf) rc = read_surface_statement(sim, *cur_srf, word, split_ws(rest), err);
+    else if (cur_cmpt >= 0) rc = read_compartment_statement(sim, cur_cmpt, word, split_ws(rest), err);
     else rc = read_config_statement(sim, word, rest, err);
     if (rc) {
       if (err) *err = full + ":" + std::to_string(lineno) + ": " + *err;

@@ -28,6 +28,7 @@ struct RxnDef {
   int nprod = 0;
   int prd[kMaxProd] = {0, 0, 0, 0};
   double rate = -1;         // requested rate constant; <0 undefined
+  int cmpt = -1;            // compartment the reaction is restricted to (rxn->cmpt), -1 none
   int rparamt = 0;          // RevParam
   double rparam = 0;
   double user_prdpos[kMaxProd][3] = {};  // for offset / fixed placement
@@ -59,6 +60,17 @@ struct Command {
   double next = 0;
 };
 
+// Compartment (smolcomparts.c compartstruct subset): a position is inside when
+// the segment to one of the interior points crosses no panel of the bounding
+// surfaces, combined with logic terms on earlier compartments.
+struct CompartDef {
+  std::string name;
+  std::vector<int> surfaces;               // indices into Sim::surfaces
+  std::vector<std::vector<double>> pts;    // interior-defining points
+  std::vector<std::pair<int, int>> logic;  // (CmptLogic symbol, earlier compartment)
+  double volume = -1;                      // Monte Carlo estimate; < 0 when not yet computed
+};
+
 // One meansqrdisp command's tracker (cmdmeansqrdisp, smolcmd.c:2505-2606):
 // the molecules of `species` present on the command's first run, by
 // (rep << 42) | serial, with their unwrapped start and last positions.
@@ -80,6 +92,7 @@ struct Sim {
   std::vector<SpeciesDef> species;   // [0] = "empty"
   std::vector<RxnDef> rxn[3];
   std::vector<SurfaceDef> surfaces;
+  std::vector<CompartDef> cmpts;
   double tstart = 0, tstop = 0, dt = 0, time = 0;
   bool time_set = false;
   long long seed = 0;
@@ -111,6 +124,7 @@ struct Sim {
 
   Sim();
   int species_index(const std::string &name) const;
+  int compartment_index(const std::string &name) const;
   int reaction_index(const std::string &name, int *order) const;
   double rand_u01();
 };
@@ -118,6 +132,17 @@ struct Sim {
 // molsetdifm (smolmolec.c:833-867): set the diffusion matrix of a species;
 // its difc becomes trace(M*M)/dim.  m is dim x dim, row-major.
 void set_species_difm(Sim &sim, int sp, const double *m);
+// posincompart (smolcomparts.c:119) on the host, absolute coordinates.
+bool pos_in_compartment(const Sim &sim, int c, const double x[3]);
+// Compartment volume (Monte Carlo over the system, fixed seed), cached.
+double compartment_volume(Sim &sim, int c);
+// compartrandpos (smolcomparts.c:194): a uniform position in compartment c.
+void compartment_random_pos(Sim &sim, int c, double x[3]);
+// One statement of a compartment block (surface, point, compartment logic).
+int read_compartment_words(Sim &sim, int c, const std::string &word, const std::vector<std::string> &w,
+                           std::string *err);
+// Forget cached compartment volumes (surfaces or compartments changed).
+void invalidate_compartments(Sim &sim);
 // surfaddpanel (smolsurface.c:2432): a panel from its shape's parameters.
 int make_panel(int dim, int shape, const std::string &axis, const double *prm, int np, PanelSpec *out,
                std::string *err);
