@@ -682,8 +682,11 @@ __device__ void births(const KParams &p, uint32_t step);
 #ifndef SMOLB_SURF_MOVE_BLOCKS
 #define SMOLB_SURF_MOVE_BLOCKS 4
 #endif
+#ifndef SMOLB_MOVE_BLOCKS
+#define SMOLB_MOVE_BLOCKS 4
+#endif
 template <bool SINGLE, int SURF>
-__global__ void __launch_bounds__(256, SURF ? SMOLB_SURF_MOVE_BLOCKS : 4) k_move(KParams p, int rebin_only) {
+__global__ void __launch_bounds__(256, SURF ? SMOLB_SURF_MOVE_BLOCKS : SMOLB_MOVE_BLOCKS) k_move(KParams p, int rebin_only) {
   extern __shared__ float s_gtab[];
   pdl_launch_dependents();
   const float *gtab = rebin_only ? p.gtab : stage_gtab(p, s_gtab);  // constant data: before the wait
