@@ -933,15 +933,21 @@ enum ErrorCode smolgpuSetMolecules(simptr sim, long long n, const double *pos, c
   Sim &s = sim->s;
   for (long long i = 0; i < n; ++i)
     LCHECK(species[i] > 0 && species[i] < (int)s.species.size(), ECbounds, "species index out of range");
-  s.pend_pos.assign(pos, pos + 3 * n);
-  s.pend_sp.assign(species, species + n);
-  s.pend_serno.clear();
+  if (!s.eng || s.need_rebuild) {  // the engine is (re)built around these molecules
+    s.pend_pos.assign(pos, pos + 3 * n);
+    s.pend_sp.assign(species, species + n);
+    if (serno) s.pend_serno.assign(serno, serno + n);
+    else s.pend_serno.clear();
+    return update_sim(s, __func__);
+  }
+  // a current engine takes the caller's arrays directly, without a host copy
   ErrorCode ec = update_sim(s, __func__);
   if (ec != ECok) return ec;
   std::string err;
   if (s.eng->set_molecules(n, pos, species, nullptr, serno, &err)) return set_error(__func__, ECerror, err);
   s.pend_pos.clear();
   s.pend_sp.clear();
+  s.pend_serno.clear();
   s.started = true;
   return ECok;
 }

@@ -1985,6 +1985,45 @@ class EngineImpl {
   // upload generation are unchanged)
   std::vector<long long> counts_cache;
   long long counts_step = -1, counts_gen = -1, upload_gen = 0;
+  // Single-step graphs also copy their step's status word and species counts
+  // into pinned host memory (slot = the step's parity), so that a caller
+  // stepping one step at a time and reading counts after each queues no
+  // separate copies between steps.
+  int *h_tail_status = nullptr;        // [2]
+  long long *h_tail_counts = nullptr;  // [2][tail_ntab], null when the table is large
+  size_t tail_ntab = 0;
+  cudaEvent_t tail_ev[2] = {nullptr, nullptr};
+  int tail_slot = -1;                  // slot of the last single-step launch, -1 if the last run ended otherwise
+  char *d_upload = nullptr;            // device staging of uploads (FP64 positions, species, serials)
+  size_t upload_cap = 0;
+  long long tail_step = -1, tail_gen = -1;
+  int tail_prev_slot = -1;             // lagged status: slot of the previous call's step
+  void tail_free() {  // the graphs that copy into these buffers must be gone already
+    if (h_tail_status && stream) cudaStreamSynchronize(stream);  // no launched copy may still be in flight
+    for (int k = 0; k < 2; ++k) {
+      if (tail_ev[k]) cudaEventDestroy(tail_ev[k]);
+      tail_ev[k] = nullptr;
+    }
+    if (h_tail_status) cudaFreeHost(h_tail_status);
+    if (h_tail_counts) cudaFreeHost(h_tail_counts);
+    h_tail_status = nullptr;
+    h_tail_counts = nullptr;
+    tail_ntab = 0;
+    tail_slot = tail_prev_slot = -1;
+    tail_step = tail_gen = -1;
+  }
+  int tail_setup() {
+    if (h_tail_status) return 0;
+    if (cudaMallocHost(&h_tail_status, 2 * sizeof(int)) != cudaSuccess) { h_tail_status = nullptr; return -1; }
+    for (int k = 0; k < 2; ++k) cudaEventCreateWithFlags(&tail_ev[k], cudaEventDisableTiming);
+    const size_t ntab = reps.size() * (size_t)net.nspecies;
+    if (ntab * sizeof(long long) <= (1u << 20) &&
+        cudaMallocHost(&h_tail_counts, 2 * ntab * sizeof(long long)) == cudaSuccess)
+      tail_ntab = ntab;
+    else
+      h_tail_counts = nullptr;
+    return 0;
+  }
   // mean square displacement trackers (dropped with the molecules on init)
   struct MsdTrack {
     int species = 0;
@@ -2011,6 +2050,10 @@ class EngineImpl {
   void release() {
     invalidate_graph();
     msd_free();
+    tail_free();
+    if (d_upload) cudaFree(d_upload);
+    d_upload = nullptr;
+    upload_cap = 0;
     void *ptrs[] = {d_difm, d_rsearch, d_geo, d_difstep, d_driftdt, d_bind2, d_pairprob, d_prdpos, d_gtab, d_unithr,
                     d_births, d_pc[0], d_pc[1], d_ppc[0], d_ppc[1], d_id[0], d_id[1], d_pid[0],
                     d_pid[1], d_face, d_tmp, d_counts, d_step, d_cnt, d_start, d_scan_ticket, d_scan_status, d_ev, d_cand, d_best,
@@ -2118,8 +2161,15 @@ class EngineImpl {
     ug.dim = s.dim;
     const size_t bpos = (size_t)n * 3 * sizeof(double), bsp = (size_t)n * sizeof(int),
                  bsn = serno ? (size_t)n * sizeof(ull) : 0;
-    char *d = nullptr;
-    CK(cudaMalloc(&d, bpos + bsp + bsn + 16));
+    const size_t need = bpos + bsp + bsn + 32;
+    if (need > upload_cap) {  // staging kept between uploads (grow only)
+      if (d_upload) cudaFree(d_upload);
+      d_upload = nullptr;
+      upload_cap = 0;
+      CK(cudaMalloc(&d_upload, need));
+      upload_cap = need;
+    }
+    char *d = d_upload;
     double *dpos = reinterpret_cast<double *>(d);
     int *dsp = reinterpret_cast<int *>(d + bpos);
     ull *dsn = serno ? reinterpret_cast<ull *>(d + ((bpos + bsp + 15) & ~(size_t)15)) : nullptr;
@@ -2134,7 +2184,6 @@ class EngineImpl {
       e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-    cudaFree(d);
     if (e != cudaSuccess) {
       if (err) *err = std::string("upload: ") + cudaGetErrorString(e);
       return -8;
@@ -2346,6 +2395,12 @@ class EngineImpl {
     const bool was = prof;
     prof = false;
     for (int par = first; par <= last; ++par) enqueue_step(par, false);
+    if (first == last && h_tail_status) {
+      cudaMemcpyAsync(h_tail_status + first, d_counts + 6, sizeof(int), cudaMemcpyDeviceToHost, stream);
+      if (h_tail_counts)
+        cudaMemcpyAsync(h_tail_counts + (size_t)first * tail_ntab, d_spcount, tail_ntab * sizeof(long long),
+                        cudaMemcpyDeviceToHost, stream);
+    }
     prof = was;
     nlaunch = before;
     cudaError_t e = cudaStreamEndCapture(stream, &g);
@@ -2376,11 +2431,16 @@ class EngineImpl {
   // One step of the current parity through its single-step graph.
   int run_one(std::string *err) {
     if (!graph1[parity]) {
+      if (!h_tail_status && tail_setup() == 0) invalidate_graph();  // capture with the copies from now on
       int rc = capture_steps(parity, parity, &graph1[parity], err);
       if (rc) return rc;
     }
     CK(cudaGraphLaunch(graph1[parity], stream));
     nlaunch += launches_per_step();
+    if (h_tail_status) {
+      CK(cudaEventRecord(tail_ev[parity], stream));
+      tail_slot = parity;
+    }
     parity ^= 1;
     return 0;
   }
@@ -2682,6 +2742,7 @@ int Engine::run(long long nsteps, std::string *err) {
     if (nsteps != 1) { if (err) *err = "injected displacements apply to one step"; return -6; }
   }
   long long done = 0;
+  E.tail_slot = -1;
   if (E.use_graph && !inj) {
     // two-step replays start at parity 0
     if (E.parity == 1) {
@@ -2697,6 +2758,7 @@ int Engine::run(long long nsteps, std::string *err) {
       CK(cudaGraphLaunch(E.graph2, E.stream));
       E.nlaunch += 2 * E.launches_per_step();
       done += 2;
+      E.tail_slot = -1;
     }
     if (done < nsteps) {
       int rc = E.run_one(err);
@@ -2708,8 +2770,11 @@ int Engine::run(long long nsteps, std::string *err) {
     E.enqueue_step(E.parity, false);
     E.parity ^= 1;
     done++;
+    E.tail_slot = -1;
   }
   E.nsteps += nsteps;
+  E.tail_step = E.nsteps;
+  E.tail_gen = E.upload_gen;
   CK(cudaGetLastError());
   if (inj) {
     E.dnet.inject = 0;
@@ -2752,8 +2817,15 @@ int Engine::species_counts(std::vector<long long> *out, std::string *err) {
     return 0;
   }
   out->assign(E.reps.size() * E.net.nspecies, 0);
-  CK(cudaMemcpyAsync(out->data(), E.d_spcount, out->size() * sizeof(long long), cudaMemcpyDeviceToHost, E.stream));
-  CK(cudaStreamSynchronize(E.stream));
+  if (E.tail_slot >= 0 && E.tail_step == E.nsteps && E.tail_gen == E.upload_gen && E.h_tail_counts &&
+      E.tail_ntab == out->size()) {  // copied by the step's own graph
+    CK(cudaEventSynchronize(E.tail_ev[E.tail_slot]));
+    memcpy(out->data(), E.h_tail_counts + (size_t)E.tail_slot * E.tail_ntab, out->size() * sizeof(long long));
+  } else {
+    CK(cudaMemcpyAsync(out->data(), E.d_spcount, out->size() * sizeof(long long), cudaMemcpyDeviceToHost,
+                       E.stream));
+    CK(cudaStreamSynchronize(E.stream));
+  }
   E.counts_cache = *out;
   E.counts_step = E.nsteps;
   E.counts_gen = E.upload_gen;
@@ -2762,6 +2834,17 @@ int Engine::species_counts(std::vector<long long> *out, std::string *err) {
 
 int Engine::status_flags_lagged() {
   EngineImpl &E = *impl_;
+  if (E.tail_slot >= 0 && E.tail_step == E.nsteps) {
+    // the step's graph copies its status into its slot; report the previous step's
+    int st = 0;
+    if (E.tail_prev_slot >= 0) {
+      cudaEventSynchronize(E.tail_ev[E.tail_prev_slot]);
+      st = E.h_tail_status[E.tail_prev_slot];
+    }
+    E.tail_prev_slot = E.tail_slot;
+    return st;
+  }
+  E.tail_prev_slot = -1;
   if (!E.h_status) {
     if (cudaMallocHost(&E.h_status, 2 * sizeof(int)) != cudaSuccess) { E.h_status = nullptr; return status_flags(); }
     for (int k = 0; k < 2; ++k) cudaEventCreateWithFlags(&E.st_ev[k], cudaEventDisableTiming);
