@@ -771,29 +771,40 @@ __device__ __forceinline__ void scatter_store(const KParams &p, const ScatterIte
   }
 }
 
+// molecules per thread per iteration of the scatter pass (2 or 4)
+#ifndef SMOLB_SCATTER_ITEMS
+#define SMOLB_SCATTER_ITEMS 2
+#endif
 template <bool SINGLE>
 __global__ void __launch_bounds__(256) k_scatter(KParams p) {
+  constexpr int NI = SMOLB_SCATTER_ITEMS;
   pdl_launch_dependents();
   pdl_wait();
   const int na = *p.a_n, np = *p.p_n;
   const int total = na + np;
   const int lane = threadIdx.x & 31;
   const int stride = gridDim.x * blockDim.x;
-  for (int base = blockIdx.x * blockDim.x; base < total; base += 2 * stride) {
-    const ScatterItem a = scatter_load<SINGLE>(p, base + threadIdx.x, na, total);
-    const ScatterItem b = scatter_load<SINGLE>(p, base + stride + threadIdx.x, na, total);
-    const BoxRun ra = box_run(a.alive, a.cell);
-    const BoxRun rb = box_run(b.alive, b.cell);
+  for (int base = blockIdx.x * blockDim.x; base < total; base += NI * stride) {
+    ScatterItem it[NI];
+    BoxRun run[NI];
+    int old[NI], st[NI];
+#pragma unroll
+    for (int k = 0; k < NI; ++k) it[k] = scatter_load<SINGLE>(p, base + k * stride + threadIdx.x, na, total);
+#pragma unroll
+    for (int k = 0; k < NI; ++k) run[k] = box_run(it[k].alive, it[k].cell);
     // the run's first live lane takes `count` slots from the top of the box
-    int olda = 0, oldb = 0;
-    if (a.alive && ra.rank == 0) olda = atomicSub(&p.cnt[a.cell], ra.count);
-    if (b.alive && rb.rank == 0) oldb = atomicSub(&p.cnt[b.cell], rb.count);
-    const int sa = a.alive ? p.start[a.cell] : 0;
-    const int sb = b.alive ? p.start[b.cell] : 0;
-    olda = __shfl_sync(0xffffffffu, olda, a.alive ? ra.head : lane);
-    oldb = __shfl_sync(0xffffffffu, oldb, b.alive ? rb.head : lane);
-    scatter_store(p, a, sa + olda - ra.count + ra.rank);
-    scatter_store(p, b, sb + oldb - rb.count + rb.rank);
+#pragma unroll
+    for (int k = 0; k < NI; ++k) {
+      old[k] = 0;
+      if (it[k].alive && run[k].rank == 0) old[k] = atomicSub(&p.cnt[it[k].cell], run[k].count);
+    }
+#pragma unroll
+    for (int k = 0; k < NI; ++k) st[k] = it[k].alive ? p.start[it[k].cell] : 0;
+#pragma unroll
+    for (int k = 0; k < NI; ++k) {
+      old[k] = __shfl_sync(0xffffffffu, old[k], it[k].alive ? run[k].head : lane);
+      scatter_store(p, it[k], st[k] + old[k] - run[k].count + run[k].rank);
+    }
   }
 }
 
