@@ -245,6 +245,7 @@ ensptr smolgpuNewEnsemble(simptr templ, int nrep) {
   T.species = S.species;
   for (int o = 0; o < 3; ++o) T.rxn[o] = S.rxn[o];
   T.surfaces = S.surfaces;
+  T.cmpts = S.cmpts;
   T.tstart = S.tstart; T.tstop = S.tstop; T.dt = S.dt; T.time = S.time;
   T.seed = S.seed;
   T.host_rng = S.host_rng;

@@ -143,3 +143,26 @@ def test_births_stay_inside_the_compartment():
     assert abs(len(pos) - expect) < 5 * np.sqrt(expect), (len(pos), expect)
     assert r.max() <= 6.0 + 1e-4, r.max()
     s.close()
+
+
+def test_ensemble_keeps_the_compartment():
+    """An ensemble built from the template keeps its compartments: A -> B
+    inside the sphere only, 16 replicates of 4000 molecules each, against the
+    single simulations' mean."""
+    ref = engine_counts("uni")
+    lib = sb.load()
+    with tempfile.TemporaryDirectory() as d:
+        with open(os.path.join(d, "c.txt"), "w") as f:
+            f.write(config("uni", 1).replace("mol 4000 A u u u\n", ""))
+        simp = C.c_void_p()
+        assert lib.smolLoadSimFromFile((d + "/").encode(), b"c.txt", C.byref(simp), b"") == 0, sb.last_error()
+    t = sb.Sim(ptr=simp.value)
+    e = sb.Ensemble(t, 16)
+    e.add_molecules("A", np.full(16, 4000))
+    e.update()
+    e.run_steps(200)
+    b = e.counts(4)[:, 2].astype(float)
+    r = ref[:, 1]
+    se = np.sqrt(r.var(ddof=1) / len(r) + b.var(ddof=1) / len(b))
+    assert abs(b.mean() - r.mean()) <= 4 * se + 2, (b.mean(), r.mean(), se)
+    assert b.mean() < 0.2 * 4000  # restricted: far fewer than A -> B everywhere (about 2/3 of 4000)
