@@ -10,7 +10,8 @@ tests/golden/<name>.npz with:
   uni                 1 where the reference's first-order reaction fired
   bind2               squared binding radius of A + B -> C (reference value)
   pos1, sp1, serno1   the reference's state after the step
-  L, wall, kf, kr     cube side, boundary type, rate constants
+  L, wall, kf, kr     cube side, boundary type ("t": walls transparent, the
+                      case's surfaces close the box), rate constants
   config              the configuration text the reference ran
 Usage: python tests/golden/make_golden.py   (needs `make -C oracle ref`)
 """
@@ -77,6 +78,41 @@ PLACEMENT_CASES = {
                                      "product_placement fwd bounce 0.6"),
 }
 
+# Surface reflection by every panel shape: a cube closed by reflective
+# rectangles holds a tilted triangle, a cylinder, a hemisphere and a disk,
+# all reflective; no reactions, and a large diffusion coefficient so that many
+# molecules meet a panel in the one recorded step.
+SURFACE_CONFIG = """dim 3
+species A
+difc A 4
+time_start 0
+time_stop 1
+time_step 0.01
+boundaries 0 0 {L}
+boundaries 1 0 {L}
+boundaries 2 0 {L}
+random_seed {seed}
+start_surface walls
+action both all reflect
+panel rect +0 0 0 0 {L} {L}
+panel rect -0 {L} 0 0 {L} {L}
+panel rect +1 0 0 0 {L} {L}
+panel rect -1 0 {L} 0 {L} {L}
+panel rect +2 0 0 0 {L} {L}
+panel rect -2 0 0 {L} {L} {L}
+end_surface
+start_surface shapes
+action both all reflect
+panel tri 1 1 5 9 2 4.5 4 9 5.5
+panel cyl 3 5 2 7 5 8 2 20 20
+panel hemi 7 3 7 2 0.3 -0.5 0.8 20 20
+panel disk 4 7 3 1.5 0.6 0.8 0 20
+end_surface
+mol {nA} A u u u
+end_file
+"""
+SURFACE_CASES = {"onestep_panels": dict(L=10, seed=31, nA=4000)}
+
 CASES = {
     "onestep_reflect": dict(L=20, w="r", seed=11, kf=20, kr=1, nA=1600, nB=1600, nC=800),
     "onestep_periodic": dict(L=20, w="p", seed=12, kf=20, kr=1, nA=1600, nB=1600, nC=800),
@@ -113,10 +149,10 @@ def run_case(name, cfg, template=CONFIG):
         pos0=np.array([d[2:5] for d in D]), sp0=np.array([d[1] for d in D], dtype=np.int32), serno0=serno0,
         disp=np.array([d[5:8] for d in D]),
         uni=np.array([1 if int(s) in uset else 0 for s in serno0], dtype=np.int32),
-        bind2=np.float64(B[0]),
+        bind2=np.float64(B.get(0, 0.0)),
         pos1=np.array([f[2:5] for f in F]), sp1=np.array([f[1] for f in F], dtype=np.int32),
         serno1=np.array([f[0] for f in F], dtype=np.uint64),
-        L=np.float64(cfg["L"]), wall=np.array(cfg.get("w", "p")), kf=np.float64(cfg.get("kf", -1)),
+        L=np.float64(cfg["L"]), wall=np.array(cfg.get("w", "t")), kf=np.float64(cfg.get("kf", -1)),
         kr=np.float64(cfg.get("kr", -1)), config=np.array(text))
     print(name, "molecules", len(D), "->", len(F), "first-order", len(U))
 
@@ -128,3 +164,5 @@ if __name__ == "__main__":
         run_case(k, v)
     for k, v in PLACEMENT_CASES.items():
         run_case(k, v, PLACEMENT_CONFIG)
+    for k, v in SURFACE_CASES.items():
+        run_case(k, v, SURFACE_CONFIG)
