@@ -102,16 +102,30 @@ panel rect +2 0 0 0 {L} {L}
 panel rect -2 0 0 {L} {L} {L}
 end_surface
 start_surface shapes
-action both all reflect
+{actions}
 panel tri 1 1 5 9 2 4.5 4 9 5.5
-panel cyl 3 5 2 7 5 8 2 20 20
-panel hemi 7 3 7 2 0.3 -0.5 0.8 20 20
 panel disk 4 7 3 1.5 0.6 0.8 0 20
+end_surface
+start_surface tube
+{tube_action}
+panel cyl 3 5 2 7 5 8 2 20 20
+end_surface
+start_surface cap
+{cap_action}
+panel hemi 7 3 7 2 0.3 -0.5 0.8 20 20
 end_surface
 mol {nA} A u u u
 end_file
 """
-SURFACE_CASES = {"onestep_panels": dict(L=10, seed=31, nA=4000)}
+SURFACE_CASES = {
+    "onestep_panels": dict(L=10, seed=31, nA=4000, actions="action both all reflect",
+                           tube_action="action both all reflect", cap_action="action both all reflect"),
+    # mixed actions: the triangle absorbs on its front face and reflects on
+    # its back, the cylinder transmits, the hemisphere absorbs
+    "onestep_panels_actions": dict(L=10, seed=32, nA=4000,
+                                   actions="action both all reflect\naction front all absorb",
+                                   tube_action="action both all transmit", cap_action="action both all absorb"),
+}
 
 CASES = {
     "onestep_reflect": dict(L=20, w="r", seed=11, kf=20, kr=1, nA=1600, nB=1600, nC=800),

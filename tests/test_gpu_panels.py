@@ -168,30 +168,32 @@ def test_tetrahedron_contains():
     assert bary.min() >= -1e-6, bary.min()
 
 
-def test_reflections_match_reference_recording():
-    """One step recorded from the reference (tests/golden/onestep_panels.npz,
-    made by make_golden.py with oracle/ref_harness): a cube closed by
-    reflective rectangles with a tilted triangle, a cylinder, a hemisphere and
-    a disk inside, all reflective.  The reference's start state and
-    displacements go in through the injection mode; every molecule must end
-    where the reference put it after its surface interactions (checksurfaces,
-    smolsurface.c:5114), to 2e-5 of the side (FP32 box-local storage and the
-    surface margin)."""
-    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "onestep_panels.npz"))
+@pytest.mark.parametrize("name", ["onestep_panels", "onestep_panels_actions"])
+def test_step_matches_reference_recording(name):
+    """One step recorded from the reference (tests/golden/<name>.npz, made by
+    make_golden.py with oracle/ref_harness): a cube closed by reflective
+    rectangles with a tilted triangle, a cylinder, a hemisphere and a disk
+    inside; all reflective, or with mixed actions (triangle front absorbs,
+    back reflects; cylinder transmits; hemisphere absorbs).  The reference's
+    start state and displacements go in through the injection mode; the same
+    molecules must survive, each where the reference put it after its surface
+    interactions (checksurfaces, smolsurface.c:5114), to 2e-5 of the side
+    (FP32 box-local storage and the surface margin)."""
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", name + ".npz"))
     s = load(str(g["config"]))
     s.set_molecules(g["pos0"], g["sp0"], g["serno0"])
     force = np.full((len(g["serno0"]), 1), -1.0)
     s.inject(g["serno0"], np.concatenate([g["disp"], force], axis=1))
     s.run_steps(1)
     pos, sp, sn = s.molecules()
+    assert sorted(sn.tolist()) == sorted(g["serno1"].tolist())  # the same molecules absorbed
     ref = {int(k): i for i, k in enumerate(g["serno1"].tolist())}
-    assert len(sn) == len(ref)
     idx = np.array([ref[int(k)] for k in sn.tolist()])
     dev = np.linalg.norm(pos - g["pos1"][idx], axis=1)
     moved = g["pos0"] + g["disp"]
     i0 = {int(k): i for i, k in enumerate(g["serno0"].tolist())}
     hit = np.linalg.norm(moved[[i0[int(k)] for k in sn.tolist()]] - g["pos1"][idx], axis=1) > 1e-9
-    print("reflected %d, max deviation %.3g (reflected) %.3g (others)" %
-          (hit.sum(), dev[hit].max(), dev[~hit].max()))
-    assert hit.sum() > 300
+    print("%s: absorbed %d, reflected %d, max deviation %.3g (reflected) %.3g (others)" %
+          (name, len(g["serno0"]) - len(sn), hit.sum(), dev[hit].max() if hit.any() else 0, dev[~hit].max()))
+    assert hit.sum() > 100
     assert dev.max() <= 2e-5 * float(g["L"]), dev.max()
