@@ -106,6 +106,7 @@ struct DevNet {
   int npanel;
   double surf_eps;     // distance kept between a molecule and a panel after an interaction
   float surf_tol;      // FP32 screening margin: eps plus the FP32 rounding of absolute positions
+  float mask_len;      // moves up to this length screen only their start box's panels (0: no box masks)
   int rounds;          // pair conflict-resolution rounds
   uint32_t uni_any;    // species with at least one first-order reaction (bit per species)
   uint32_t pair_any;   // species with at least one second-order reaction

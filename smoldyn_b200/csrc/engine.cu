@@ -49,6 +49,7 @@ struct KParams {
   const float *bind2;      // [rep*nr2 + r]
   const float *pairprob;   // [rep*nr2 + r]
   const float *rsearch;    // [rep*nsp + sp] stencil radius of the pair search
+  const uint16_t *boxmask; // [global box] panels that a short move starting in the box can reach
   const double *births;    // [rep*nr0 + r]
   const float *prdpos;     // [((rep*nrx + k)*kMaxProd + p)*3]
   const float *gtab;       // gaussian table
@@ -293,11 +294,19 @@ __device__ __forceinline__ int panel_action(const DevPanel &pn, int face, int sp
 // distance is 1-Lipschitz along the move, so a segment that starts farther
 // than its length outside cannot reach the surface).
 template <bool GEN>
-__device__ __forceinline__ bool surface_near(const float a0[3], const float a1[3]) {
+__device__ __forceinline__ bool surface_near(const float a0[3], const float a1[3], const uint16_t *boxmask,
+                                             int box0) {
   const float tol = c_net.surf_tol;
   const float sx = a1[0] - a0[0], sy = a1[1] - a0[1], sz = a1[2] - a0[2];
   const float seg = sqrtf(sx * sx + sy * sy + sz * sz);
+  // a short move can only reach the panels listed for its start box
+  uint32_t mask = 0xFFFFFFFFu;
+  if (boxmask && seg <= c_net.mask_len) {
+    mask = boxmask[box0];
+    if (!mask) return false;
+  }
   for (int k = 0; k < c_net.npanel; ++k) {
+    if (!((mask >> k) & 1u)) continue;
     const DevPanel &pn = c_panels[k];
     if (pn.shape == 0) {  // axis-aligned rectangle: its plane along one axis
       const float q0 = a0[pn.axis] - pn.posf, q1 = a1[pn.axis] - pn.posf;
@@ -535,7 +544,7 @@ __device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, co
       a0[d] = (float)ix0[d] * g.h[d] + u0[d];
       a1[d] = (float)ix[d] * g.h[d] + u[d];
     }
-    if (surface_near<SURF == 2>(a0, a1)) {
+    if (surface_near<SURF == 2>(a0, a1, p.boxmask, g.cell0 + (ix0[2] * g.n[1] + ix0[1]) * g.n[0] + ix0[0])) {
       double x0[3], x1[3];
       to_abs(g, ix0, u0, x0);
       to_abs(g, ix, u, x1);
@@ -1956,6 +1965,7 @@ class EngineImpl {
   // device memory
   DevGeo *d_geo = nullptr;
   float *d_rsearch = nullptr;
+  uint16_t *d_boxmask = nullptr;
   float *d_difm = nullptr;
   float *d_difstep = nullptr, *d_driftdt = nullptr, *d_bind2 = nullptr, *d_pairprob = nullptr,
         *d_prdpos = nullptr, *d_gtab = nullptr;
@@ -2065,13 +2075,14 @@ class EngineImpl {
     if (d_upload) cudaFree(d_upload);
     d_upload = nullptr;
     upload_cap = 0;
-    void *ptrs[] = {d_difm, d_rsearch, d_geo, d_difstep, d_driftdt, d_bind2, d_pairprob, d_prdpos, d_gtab, d_unithr,
+    void *ptrs[] = {d_boxmask, d_difm, d_rsearch, d_geo, d_difstep, d_driftdt, d_bind2, d_pairprob, d_prdpos, d_gtab, d_unithr,
                     d_births, d_pc[0], d_pc[1], d_ppc[0], d_ppc[1], d_id[0], d_id[1], d_pid[0],
                     d_pid[1], d_face, d_tmp, d_counts, d_step, d_cnt, d_start, d_scan_ticket, d_scan_status, d_ev, d_cand, d_best,
                     d_counters, d_spcount, d_injkey, d_injval};
     for (void *q : ptrs)
       if (q) cudaFree(q);
     d_rsearch = nullptr;
+    d_boxmask = nullptr;
     d_geo = nullptr; d_difstep = d_driftdt = d_bind2 = d_pairprob = d_prdpos = d_gtab = nullptr;
     d_difm = nullptr;
     d_unithr = nullptr; d_births = nullptr;
@@ -2097,6 +2108,7 @@ class EngineImpl {
     p.bind2 = d_bind2;
     p.pairprob = d_pairprob;
     p.rsearch = d_rsearch;
+    p.boxmask = d_boxmask;
     p.births = d_births;
     p.prdpos = d_prdpos;
     p.gtab = d_gtab;
@@ -2247,6 +2259,124 @@ class EngineImpl {
   }
 
   bool single_rep() const { return reps.size() == 1; }
+
+  // Whether a panel can come within r of the box [lo, hi] (coordinates in
+  // the panels' frame).  Conservative: false only when no point of the panel
+  // lies within r of the box.
+  static bool panel_near_box(const DevPanel &pn, const double lo[3], const double hi[3], double r) {
+    auto dmin = [&](const double c[3]) {  // distance from c to the box
+      double q = 0;
+      for (int d = 0; d < 3; ++d) {
+        const double v = c[d] < lo[d] ? lo[d] - c[d] : c[d] > hi[d] ? c[d] - hi[d] : 0.0;
+        q += v * v;
+      }
+      return std::sqrt(q);
+    };
+    auto dmax = [&](const double c[3]) {  // distance from c to the farthest corner
+      double q = 0;
+      for (int d = 0; d < 3; ++d) {
+        const double v = std::max(std::fabs(c[d] - lo[d]), std::fabs(c[d] - hi[d]));
+        q += v * v;
+      }
+      return std::sqrt(q);
+    };
+    auto plane_apart = [&](const double o[3], const double n[3]) {  // every corner farther than r on one side
+      int above = 0, below = 0;
+      for (int c = 0; c < 8; ++c) {
+        const double x[3] = {(c & 1) ? hi[0] : lo[0], (c & 2) ? hi[1] : lo[1], (c & 4) ? hi[2] : lo[2]};
+        const double sd = (x[0] - o[0]) * n[0] + (x[1] - o[1]) * n[1] + (x[2] - o[2]) * n[2];
+        if (sd > r) ++above;
+        else if (sd < -r) ++below;
+      }
+      return above == 8 || below == 8;
+    };
+    if (pn.shape == 0) {  // rectangle: distance between the two boxes
+      double q = 0;
+      for (int d = 0; d < 3; ++d) {
+        const double plo = d == pn.axis ? pn.pos : pn.lo[d], phi = d == pn.axis ? pn.pos : pn.hi[d];
+        const double gap = std::max(0.0, std::max(plo - hi[d], lo[d] - phi));
+        q += gap * gap;
+      }
+      return std::sqrt(q) <= r;
+    }
+    if (pn.shape == 2 || pn.shape == 4)  // the shell at the radius must meet the widened box
+      return dmin(pn.center) <= pn.radius + r && dmax(pn.center) >= pn.radius - r;
+    if (pn.shape == 3) {
+      double c[3];
+      for (int d = 0; d < 3; ++d) c[d] = 0.5 * (pn.pt[0][d] + pn.pt[1][d]);
+      if (dmin(c) > std::sqrt(0.25 * pn.axlen * pn.axlen + pn.radius * pn.radius) + r) return false;
+      double far = 0;  // radial distance to the axis is convex: its maximum over the box is at a corner
+      for (int k = 0; k < 8; ++k) {
+        const double x[3] = {(k & 1) ? hi[0] : lo[0], (k & 2) ? hi[1] : lo[1], (k & 4) ? hi[2] : lo[2]};
+        double rr[3];
+        cyl_radial(pn, x, rr);
+        far = std::max(far, std::sqrt(dot3(rr, rr)));
+      }
+      return far >= pn.radius - r;
+    }
+    const double *o = pn.shape == 1 ? pn.pt[0] : pn.center;
+    double c[3], rb = pn.radius;
+    if (pn.shape == 1) {
+      for (int d = 0; d < 3; ++d) c[d] = (pn.pt[0][d] + pn.pt[1][d] + pn.pt[2][d]) / 3.0;
+      rb = 0;
+      for (int k = 0; k < 3; ++k) {
+        double q = 0;
+        for (int d = 0; d < 3; ++d) q += (pn.pt[k][d] - c[d]) * (pn.pt[k][d] - c[d]);
+        rb = std::max(rb, std::sqrt(q));
+      }
+    } else {
+      for (int d = 0; d < 3; ++d) c[d] = pn.center[d];
+    }
+    if (dmin(c) > rb + r) return false;
+    return !plane_apart(o, pn.nrm);
+  }
+
+  // Per-box panel masks for the FP32 surface screen: the panels that a move
+  // no longer than mask_len, starting in the box, can come within the screen's
+  // margin of.  mask_len covers 10 standard deviations per axis of the fastest
+  // species' step plus its drift; longer moves screen every panel.
+  int build_box_masks(std::string *err) {
+    dnet.mask_len = 0;
+    if (panels.empty() || panels.size() > 16 || ncell <= 0) return 0;
+    double sig = 0, drift = 0, ext = 0;
+    for (const RepSpec &s : reps) {
+      for (int sp = 1; sp < net.nspecies; ++sp) {
+        double var = 2.0 * s.difc[sp] * dt;
+        if (s.has_difm[sp]) {
+          double f = 0;
+          for (int k = 0; k < 9; ++k) f += s.difm[sp][k] * s.difm[sp][k];
+          var = 2.0 * dt * f;
+        }
+        sig = std::max(sig, std::sqrt(std::max(var, 0.0)));
+        double v = 0;
+        for (int d = 0; d < 3; ++d) v += s.drift[sp][d] * s.drift[sp][d];
+        drift = std::max(drift, std::sqrt(v) * dt);
+      }
+      for (int d = 0; d < 3; ++d) ext = std::max(ext, s.hi[d] - s.lo[d]);
+    }
+    const double len = 10.0 * sig * std::sqrt(3.0) + drift;
+    const double r = len + (double)dnet.surf_tol + 1e-6 * ext;
+    std::vector<uint16_t> mask((size_t)ncell, 0);
+    for (const DevGeo &g : geo)
+      for (int iz = 0; iz < g.n[2]; ++iz)
+        for (int iy = 0; iy < g.n[1]; ++iy)
+          for (int ix = 0; ix < g.n[0]; ++ix) {
+            const int ic[3] = {ix, iy, iz};
+            double lo[3], hi[3];
+            for (int d = 0; d < 3; ++d) {
+              lo[d] = (double)ic[d] * g.h[d];
+              hi[d] = ic[d] == g.n[d] - 1 ? (double)ic[d] * g.h[d] + g.whi[d] : lo[d] + g.h[d];
+            }
+            uint16_t m = 0;
+            for (size_t k = 0; k < panels.size(); ++k)
+              if (panel_near_box(panels[k], lo, hi, r)) m |= (uint16_t)(1u << k);
+            mask[(size_t)g.cell0 + ((size_t)iz * g.n[1] + iy) * g.n[0] + ix] = m;
+          }
+    CK(cudaMalloc(&d_boxmask, mask.size() * sizeof(uint16_t)));
+    CK(cudaMemcpy(d_boxmask, mask.data(), mask.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+    dnet.mask_len = (float)len;
+    return 0;
+  }
   template <bool SINGLE, int SURF>
   void enqueue_step_t(int par, bool rebin_only) {
     KParams p = params(par);
@@ -2653,7 +2783,9 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
   E.dnet.ncmpt = (int)E.cmpts.size();
   for (int o = 0; o < 3; ++o)
     for (int r = 0; r < kMaxRxn; ++r) E.dnet.cmpt[o][r] = (uint8_t)E.net.cmpt[o][r];
-  int rc = E.build_rep_tables(err);
+  int rc = E.build_box_masks(err);
+  if (rc) return rc;
+  rc = E.build_rep_tables(err);
   if (rc) return rc;
   E.nsteps = 0;
   E.parity = 0;
