@@ -244,7 +244,23 @@ int advance_steps(Sim &s, long long n, std::string *err) {
   return 0;
 }
 
-// runtime commands (smolcmd.c docommand subset: molcount, meansqrdisp)
+// molcountincmpt compartment data (smolcmd.c:1054-1100): (time, count of
+// each species in the compartment)
+void record_molcountincmpt(Sim &s, const smolb::Command &c) {
+  char name[256] = {0}, cm[256] = {0}, data[256] = {0};
+  const int nw = sscanf(c.text.c_str(), "%255s %255s %255s", name, cm, data);
+  const int ci = s.compartment_index(cm);
+  if (nw < 2 || ci < 0 || !s.eng) return;
+  std::vector<long long> counts;
+  std::string err;
+  if (s.eng->cmpt_counts(ci, &counts, &err)) return;
+  std::vector<double> row;
+  row.push_back(s.time);
+  for (size_t i = 1; i < s.species.size(); ++i) row.push_back(i < counts.size() ? (double)counts[i] : 0.0);
+  s.outdata[nw >= 3 ? data : "molcountincmpt"].push_back(row);
+}
+
+// runtime commands (smolcmd.c docommand subset: molcount, molcountincmpt, meansqrdisp)
 void do_commands(Sim &s, bool at_start) {
   for (smolb::Command &c : s.cmds) {
     bool run = false;
@@ -263,6 +279,7 @@ void do_commands(Sim &s, bool at_start) {
     if (sscanf(c.text.c_str(), "%255s %255s", name, arg) < 1) continue;
     if (!strcmp(name, "molcount")) record_molcount(s, arg[0] ? arg : "molcount");
     else if (!strcmp(name, "meansqrdisp")) record_meansqrdisp(s, c);
+    else if (!strcmp(name, "molcountincmpt")) record_molcountincmpt(s, c);
   }
 }
 
@@ -273,6 +290,7 @@ void do_end_commands(Sim &s) {
     if (sscanf(c.text.c_str(), "%255s %255s", name, arg) < 1) continue;
     if (!strcmp(name, "molcount")) record_molcount(s, arg[0] ? arg : "molcount");
     else if (!strcmp(name, "meansqrdisp")) record_meansqrdisp(s, c);
+    else if (!strcmp(name, "molcountincmpt")) record_molcountincmpt(s, c);
   }
 }
 

@@ -1895,6 +1895,38 @@ __global__ void __launch_bounds__(kMsdThreads) k_msd(const float4 *a_pc, const u
   }
 }
 
+// Molecules of each species inside compartment c (cmdmolcountincmpt,
+// smolcmd.c:1054-1100): every live molecule of the sorted and product lists,
+// membership by posincompart, per-block shared-memory tallies.
+__global__ void __launch_bounds__(256) k_cmpt_count(const float4 *a_pc, const ull *a_id, const int *a_n,
+                                                    const float4 *p_pc, const ull *p_id, const int *p_n, int pcap,
+                                                    const DevGeo *geo, int nrep, int c, int nsp,
+                                                    unsigned long long *out) {
+  __shared__ unsigned int s_cnt[kMaxSpecies];
+  for (int k = threadIdx.x; k < kMaxSpecies; k += blockDim.x) s_cnt[k] = 0;
+  __syncthreads();
+  const int na = *a_n, np = min(*p_n, pcap);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)na + np;
+       i += (long long)gridDim.x * blockDim.x) {
+    const bool prod = i >= na;
+    const ull x = prod ? p_id[i - na] : a_id[i];
+    const int sp = id_species(x);
+    if (sp == kDeadSpecies || sp >= nsp) continue;
+    const int rp = id_rep(x);
+    if (rp >= nrep) continue;
+    const float4 q = prod ? p_pc[i - na] : a_pc[i];
+    int ix[3];
+    unpack_cell(__float_as_uint(q.w), ix[0], ix[1], ix[2]);
+    const float u[3] = {q.x, q.y, q.z};
+    double xa[3];
+    to_abs(geo[rp], ix, u, xa);
+    if (pos_in_cmpt(c_cmpt, c, c_panels, xa)) atomicAdd(&s_cnt[sp], 1u);
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < nsp; k += blockDim.x)
+    if (s_cnt[k]) atomicAdd(&out[k], (unsigned long long)s_cnt[k]);
+}
+
 // Batched pair-radius derivation (binding radius + reverse unbinding radius),
 // one thread per replicate: the exact FP64 path for ensembles.
 __global__ void k_pair_radii(long long n, const double *kf, const double *dsum, double dt, int same, int rev,
@@ -3205,6 +3237,38 @@ int Engine::msd_last(int handle, std::vector<double> *last, std::string *err) {
 }
 
 int Engine::msd_count() const { return (int)impl_->msd.size(); }
+
+int Engine::cmpt_counts(int c, std::vector<long long> *out, std::string *err) {
+  EngineImpl &E = *impl_;
+  if (c < 0 || c >= (int)E.cmpts.size()) {
+    if (err) *err = "no such compartment";
+    return -6;
+  }
+  const int nsp = E.net.nspecies;
+  unsigned long long *d = nullptr;
+  CK(cudaMalloc(&d, kMaxSpecies * sizeof(unsigned long long)));
+  cudaError_t e = cudaMemsetAsync(d, 0, kMaxSpecies * sizeof(unsigned long long), E.stream);
+  const int in = E.parity;
+  if (e == cudaSuccess) {
+    k_cmpt_count<<<sm_count() * 4, 256, 0, E.stream>>>(E.d_pc[in], E.d_id[in], E.d_counts + in, E.d_ppc[in],
+                                                         E.d_pid[in], E.d_counts + 2 + in, (int)E.pcap, E.d_geo,
+                                                         (int)E.reps.size(), c, nsp, d);
+    e = cudaGetLastError();
+  }
+  std::vector<unsigned long long> h(kMaxSpecies, 0);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), d, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                            E.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
+  cudaFree(d);
+  if (e != cudaSuccess) {
+    if (err) *err = std::string("compartment count: ") + cudaGetErrorString(e);
+    return -8;
+  }
+  ++E.nlaunch;
+  out->assign(nsp, 0);
+  for (int k = 0; k < nsp; ++k) (*out)[k] = (long long)h[k];
+  return 0;
+}
 
 int Engine::profile(long long nsteps, std::vector<std::string> *names, std::vector<double> *ms,
                     std::vector<long long> *launches, std::string *err) {

@@ -174,6 +174,8 @@ class Engine {
   // Last unwrapped positions (3 per key), e.g. to carry a tracker across a rebuild.
   int msd_last(int handle, std::vector<double> *last, std::string *err);
   int msd_count() const;
+  // Molecules of each species inside compartment c: out[sp] (cmdmolcountincmpt).
+  int cmpt_counts(int c, std::vector<long long> *out, std::string *err);
 
  private:
   EngineImpl *impl_;

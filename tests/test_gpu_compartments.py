@@ -166,3 +166,40 @@ def test_ensemble_keeps_the_compartment():
     se = np.sqrt(r.var(ddof=1) / len(r) + b.var(ddof=1) / len(b))
     assert abs(b.mean() - r.mean()) <= 4 * se + 2, (b.mean(), r.mean(), se)
     assert b.mean() < 0.2 * 4000  # restricted: far fewer than A -> B everywhere (about 2/3 of 4000)
+
+
+def test_molcountincmpt_counts_molecules_inside():
+    """molcountincmpt (smolcmd.c:1054): per-species counts inside the
+    compartment equal a host count of the downloaded positions inside the
+    sphere, and agree with the reference's own molcountincmpt output."""
+    text = (HEAD.format(da=1, seed=3) + "mol 4000 A u u u\nmol 2000 B u u u\n"
+            "output_files cnt.txt\ncmd a molcountincmpt inside cnt.txt\nend_file\n")
+    lib = sb.load()
+    with tempfile.TemporaryDirectory() as d:
+        with open(os.path.join(d, "c.txt"), "w") as f:
+            f.write(text)
+        simp = C.c_void_p()
+        assert lib.smolLoadSimFromFile((d + "/").encode(), b"c.txt", C.byref(simp), b"") == 0, sb.last_error()
+    s = sb.Sim(ptr=simp.value)
+    s.run()
+    row = s.output_data("cnt.txt")[-1]
+    pos, sp, _ = s.molecules()
+    inside = np.linalg.norm(pos - 10.0, axis=1) < 6.0
+    host = [int(np.count_nonzero(inside & (sp == k))) for k in (1, 2, 3)]
+    assert [int(v) for v in row[1:4]] == host, (row, host)
+    if not os.path.exists(REF_EXE):
+        return
+    env = dict(os.environ, SMOLDYN_NO_PROMPT="1")
+    ref = []
+    with tempfile.TemporaryDirectory() as d:
+        for seed in range(1, 5):
+            with open(os.path.join(d, "c.txt"), "w") as f:
+                f.write(text.replace("random_seed 3", "random_seed %d" % seed))
+            subprocess.run([REF_EXE, "c.txt", "-qt"], cwd=d, check=True, stdout=subprocess.DEVNULL,
+                           stderr=subprocess.DEVNULL, stdin=subprocess.DEVNULL, env=env, timeout=600)
+            last = [ln.replace(",", " ").split() for ln in open(os.path.join(d, "cnt.txt")) if ln.strip()][-1]
+            ref.append([float(x) for x in last[1:4]])
+    ref = np.array(ref).mean(0)
+    expect = np.array([4000, 2000, 0]) * (4 / 3 * np.pi * 216) / 8000
+    assert np.all(np.abs(ref - expect) <= 5 * np.sqrt(expect / 4) + 1), (ref, expect)
+    assert np.all(np.abs(np.array(host) - expect) <= 5 * np.sqrt(expect) + 1), (host, expect)
