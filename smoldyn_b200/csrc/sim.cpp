@@ -510,8 +510,8 @@ double compartment_volume(Sim &sim, int c) {
   return cd.volume;
 }
 
-void compartment_random_pos(Sim &sim, int c, double x[3]) {
-  const CmptTester t(sim);
+namespace {
+void random_pos_with(Sim &sim, const CmptTester &t, int c, double x[3]) {
   for (int k = 0; k < 10000; ++k) {
     for (int d = 0; d < 3; ++d) x[d] = d < sim.dim ? sim.lo[d] + sim.rand_u01() * (sim.hi[d] - sim.lo[d]) : 0.0;
     if (t.inside(c, x)) return;
@@ -520,6 +520,18 @@ void compartment_random_pos(Sim &sim, int c, double x[3]) {
   if (cd.pts.empty()) return;
   const size_t k = std::min(cd.pts.size() - 1, (size_t)(sim.rand_u01() * cd.pts.size()));
   for (int d = 0; d < 3; ++d) x[d] = d < (int)cd.pts[k].size() ? cd.pts[k][d] : 0.0;
+}
+}  // namespace
+
+void compartment_random_pos(Sim &sim, int c, double x[3]) { random_pos_with(sim, CmptTester(sim), c, x); }
+
+void compartment_random_positions(Sim &sim, int c, long long n, std::vector<double> *out) {
+  const CmptTester t(sim);  // built once for all n positions
+  for (long long k = 0; k < n; ++k) {
+    double x[3];
+    random_pos_with(sim, t, c, x);
+    for (int d = 0; d < 3; ++d) out->push_back(x[d]);
+  }
 }
 
 int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err) {
@@ -817,12 +829,8 @@ int read_config_statement(Sim &sim, const std::string &word, const std::string &
     if (i <= 0) { if (err) *err = "compartment_mol: unknown species " + w[1]; return -3; }
     const int c = sim.compartment_index(w[2]);
     if (c < 0) { if (err) *err = "compartment_mol: unknown compartment " + w[2]; return -3; }
-    for (long long k = 0; k < n; ++k) {
-      double x[3];
-      compartment_random_pos(sim, c, x);
-      for (int d = 0; d < 3; ++d) sim.pend_pos.push_back(x[d]);
-      sim.pend_sp.push_back(i);
-    }
+    compartment_random_positions(sim, c, n, &sim.pend_pos);
+    for (long long k = 0; k < n; ++k) sim.pend_sp.push_back(i);
     sim.need_rebuild = true;
   } else if (word == "reaction" || word == "reaction_cmpt") {
     // reaction_cmpt cname ... (deprecated form) or reaction cmpt=cname ...

@@ -138,6 +138,8 @@ bool pos_in_compartment(const Sim &sim, int c, const double x[3]);
 double compartment_volume(Sim &sim, int c);
 // compartrandpos (smolcomparts.c:194): a uniform position in compartment c.
 void compartment_random_pos(Sim &sim, int c, double x[3]);
+// n such positions appended to out (3 coordinates each).
+void compartment_random_positions(Sim &sim, int c, long long n, std::vector<double> *out);
 // One statement of a compartment block (surface, point, compartment logic).
 int read_compartment_words(Sim &sim, int c, const std::string &word, const std::vector<std::string> &w,
                            std::string *err);
