@@ -373,11 +373,16 @@ int run_chains(std::vector<RdfChain> &chains, int n, double eps, cudaStream_t st
   if (cudaFuncSetAttribute(k_rdf_sweep, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
     cudaGetLastError();
   const long long nch = (long long)chains.size();
-  int cs = 16;
-  while (cs > 1 && nch * cs > sms) cs >>= 1;
-  // 512 threads (one CTA per SM at this register count) while the grid fits
-  // one wave, else 256 so that two CTAs share an SM
-  const int threads = nch * cs <= sms ? kThreads : kThreads / 2;
+  // Cluster size: the largest of 16, 8, 4, 2, 1 whose grid is resident in one
+  // wave, either with 512 threads per CTA (one CTA per SM at this register
+  // count) or with 256 (two CTAs per SM).  The larger cluster wins, 512
+  // threads on a tie; beyond two sweeps per SM, single CTAs of 256 threads.
+  int cs_one = 16;
+  while (cs_one > 0 && nch * cs_one > sms) cs_one >>= 1;
+  int cs_two = 16;
+  while (cs_two > 1 && nch * cs_two > 2 * sms) cs_two >>= 1;
+  int cs = cs_one >= cs_two ? cs_one : cs_two;
+  const int threads = cs_one >= cs_two ? kThreads : kThreads / 2;
   for (;; cs >>= 1) {
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
