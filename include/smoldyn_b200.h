@@ -103,6 +103,29 @@ enum ErrorCode smolAddSolutionMolecules(simptr sim, const char *species, int num
                                         double *lowposition, double *highposition);
 int smolGetMoleculeCount(simptr sim, const char *species, enum MolecState state);
 
+/* Molecule lists (libsmoldyn.h:108-112, libsmoldyn.cpp:954-1035).  The
+ * reference's live lists are a CPU data-structure choice; the engine keeps
+ * one box-sorted array for all species, so list names are recorded and
+ * validated as the reference does (ECwarning for a repeated name, ECsame for
+ * an unknown one in smolAddSpecies/smolSetMolList) and have no other effect. */
+enum ErrorCode smolAddMolList(simptr sim, const char *mollist);
+int smolGetMolListIndex(simptr sim, const char *mollist);
+int smolGetMolListIndexNT(simptr sim, const char *mollist);
+char *smolGetMolListName(simptr sim, int mollistindex, char *mollist);
+enum ErrorCode smolSetMolList(simptr sim, const char *species, enum MolecState state, const char *mollist);
+
+/* Display (libsmoldyn.h:55, :76, :104-105, :118).  No graphics stack is
+ * driven: the arguments are checked as in the reference (libsmoldyn.cpp:
+ * 295, 485, 1147-1216) and otherwise ignored; smolDisplaySim prints a short
+ * text summary of the simulation to stdout (the reference prints its full
+ * parameter listing, simsystemoutput). */
+enum ErrorCode smolDisplaySim(simptr sim);
+enum ErrorCode smolSetGraphicsParams(simptr sim, const char *method, int timesteps, int delay);
+enum ErrorCode smolSetMoleculeColor(simptr sim, const char *species, enum MolecState state, double *color);
+enum ErrorCode smolSetMoleculeSize(simptr sim, const char *species, enum MolecState state, double size);
+enum ErrorCode smolSetMoleculeStyle(simptr sim, const char *species, enum MolecState state, double size,
+                                    double *color);
+
 /* libsmoldyn.h:122-130: walls and surfaces (solution-state actions) */
 enum ErrorCode smolSetBoundaryType(simptr sim, int dimension, int highside, char type);
 enum ErrorCode smolAddSurface(simptr sim, const char *surface);
@@ -224,8 +247,15 @@ enum ErrorCode smolgpuSolveRadii(int mode, long long n, const double *rate, doub
  * solve.  At most 65536 problems per call (ECbounds above that).  The
  * scratch is shared per device and keeps the last call's contents: calls
  * that overlap on the GPU race and must be serialised by the caller.  The
- * first call on a device sets up the scratch address; make it before any
- * stream capture. */
+ * first call on a device sets up the scratch address (cudaGetSymbolAddress);
+ * under CUDA's lazy module loading that can load the library's device code,
+ * which places the scratch in device memory and may synchronise, so make the
+ * first call at set-up time, before HBM is filled and before any stream
+ * capture.  The address is cached per device: after cudaDeviceReset the
+ * library must be reloaded.  Copies are synchronous cudaMemcpy and the kernel
+ * runs on the legacy default stream, which waits for every blocking stream of
+ * the process: the call overlaps only work on streams created with
+ * cudaStreamNonBlocking (the engine's own streams are). */
 enum ErrorCode smolgpuSolveRadiiNoAlloc(int mode, long long n, const double *rate, double dt,
                                         const double *difc, const double *b, int rel, double *out);
 /* Same solver on the host CPU (product path used by parameter updates). */

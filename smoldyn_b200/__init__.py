@@ -64,6 +64,16 @@ PROTOTYPES = {
     "smolGetSpeciesName": (None, [_sim, C.c_int, C.c_char_p]),
     "smolSetSpeciesMobility": (C.c_int, [_sim, C.c_char_p, C.c_int, C.c_double, _dp, _dp]),
     "smolSetMaxMolecules": (C.c_int, [_sim, C.c_int]),
+    "smolAddMolList": (C.c_int, [_sim, C.c_char_p]),
+    "smolGetMolListIndex": (C.c_int, [_sim, C.c_char_p]),
+    "smolGetMolListIndexNT": (C.c_int, [_sim, C.c_char_p]),
+    "smolGetMolListName": (C.c_char_p, [_sim, C.c_int, C.c_char_p]),
+    "smolSetMolList": (C.c_int, [_sim, C.c_char_p, C.c_int, C.c_char_p]),
+    "smolDisplaySim": (C.c_int, [_sim]),
+    "smolSetGraphicsParams": (C.c_int, [_sim, C.c_char_p, C.c_int, C.c_int]),
+    "smolSetMoleculeColor": (C.c_int, [_sim, C.c_char_p, C.c_int, C.c_void_p]),
+    "smolSetMoleculeSize": (C.c_int, [_sim, C.c_char_p, C.c_int, C.c_double]),
+    "smolSetMoleculeStyle": (C.c_int, [_sim, C.c_char_p, C.c_int, C.c_double, C.c_void_p]),
     "smolAddSolutionMolecules": (C.c_int, [_sim, C.c_char_p, C.c_int, _dp, _dp]),
     "smolGetMoleculeCount": (C.c_int, [_sim, C.c_char_p, C.c_int]),
     "smolSetBoundaryType": (C.c_int, [_sim, C.c_int, C.c_int, C.c_char]),

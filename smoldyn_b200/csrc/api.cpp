@@ -502,8 +502,10 @@ enum ErrorCode smolGetOutputData(simptr sim, char *dataname, int *nrow, int *nco
 }
 
 enum ErrorCode smolAddSpecies(simptr sim, const char *species, const char *mollist) {
-  (void)mollist;
   LCHECK(sim && species, ECmissing, "missing sim or species");
+  if (mollist && mollist[0])  // libsmoldyn.cpp:811-814: the list must exist
+    LCHECK(std::find(sim->s.mollists.begin(), sim->s.mollists.end(), mollist) != sim->s.mollists.end(), ECsame,
+           "molecule list not recognized");
   LCHECK(sim->s.species_index(species) < 0, ECsame, "species already exists");
   LCHECK((int)sim->s.species.size() < smolb::kMaxSpecies, ECbounds, "too many species (max 31)");
   sim->s.species.push_back(smolb::SpeciesDef{species});
@@ -522,6 +524,114 @@ int smolGetSpeciesIndexNT(simptr sim, const char *species) {
   if (!strcmp(species, "all")) return (int)ECall;
   const int i = sim->s.species_index(species);
   return i < 0 ? (int)ECnonexist : i;
+}
+
+// ---- molecule lists (libsmoldyn.cpp:954-1035): names only ----
+enum ErrorCode smolAddMolList(simptr sim, const char *mollist) {
+  LCHECK(sim, ECmissing, "missing sim");
+  LCHECK(mollist, ECmissing, "missing mollist");
+  std::vector<std::string> &L = sim->s.mollists;
+  if (std::find(L.begin(), L.end(), mollist) != L.end())
+    return set_error(__func__, ECwarning, "molecule list name has already been used");
+  L.push_back(mollist);
+  return ECok;
+}
+
+int smolGetMolListIndexNT(simptr sim, const char *mollist) {
+  if (!sim || !mollist) return (int)ECmissing;
+  if (sim->s.mollists.empty()) return (int)ECnonexist;
+  if (!strcmp(mollist, "all")) return (int)ECall;
+  const std::vector<std::string> &L = sim->s.mollists;
+  const auto it = std::find(L.begin(), L.end(), mollist);
+  return it == L.end() ? (int)ECnonexist : (int)(it - L.begin());
+}
+
+int smolGetMolListIndex(simptr sim, const char *mollist) {
+  const int ll = smolGetMolListIndexNT(sim, mollist);
+  if (ll == (int)ECmissing) set_error(__func__, ECmissing, "missing sim or mollist");
+  else if (ll == (int)ECall) set_error(__func__, ECall, "molecule list is 'all'");
+  else if (ll < 0) set_error(__func__, ECnonexist, "list name not recognized");
+  return ll;
+}
+
+char *smolGetMolListName(simptr sim, int mollistindex, char *mollist) {
+  if (!sim || !mollist) { set_error(__func__, ECmissing, "missing sim or mollist"); return nullptr; }
+  if (mollistindex < 0) { set_error(__func__, ECbounds, "mollistindex < 0"); return nullptr; }
+  if (mollistindex >= (int)sim->s.mollists.size()) {
+    set_error(__func__, ECnonexist, "molecule list doesn't exist");
+    return nullptr;
+  }
+  strcpy(mollist, sim->s.mollists[mollistindex].c_str());
+  return mollist;
+}
+
+// species "all" or one species; ECsame otherwise (libsmoldyn.cpp:1155-1161 pattern)
+static bool species_or_all(simptr sim, const char *species) {
+  if (!species) return false;
+  if (!strcmp(species, "all")) return true;
+  return sim->s.species_index(species) > 0;
+}
+
+enum ErrorCode smolSetMolList(simptr sim, const char *species, enum MolecState state, const char *mollist) {
+  LCHECK(sim, ECmissing, "missing sim");
+  LCHECK(species_or_all(sim, species), ECsame, "species not recognized");
+  LCHECK((state >= MSsoln && state <= MSbsoln) || state == MSall, ECsyntax, "invalid state");
+  LCHECK(smolGetMolListIndexNT(sim, mollist) >= 0, ECsame, "molecule list not recognized");
+  return ECok;
+}
+
+// ---- display (libsmoldyn.cpp:295, 485, 1147-1216): checked, then ignored ----
+enum ErrorCode smolSetGraphicsParams(simptr sim, const char *method, int timesteps, int delay) {
+  (void)timesteps;
+  (void)delay;
+  LCHECK(sim, ECmissing, "missing sim");
+  if (method)
+    LCHECK(!strcmp(method, "none") || !strcmp(method, "opengl") || !strcmp(method, "opengl_good") ||
+               !strcmp(method, "opengl_better"),
+           ECsyntax, "graphics method not recognized");
+  return ECok;
+}
+
+enum ErrorCode smolSetMoleculeColor(simptr sim, const char *species, enum MolecState state, double *color) {
+  LCHECK(sim, ECmissing, "missing sim");
+  LCHECK(species_or_all(sim, species), ECsame, "species not recognized");
+  LCHECK((state >= MSsoln && state <= MSbsoln) || state == MSall, ECsyntax, "invalid state");
+  LCHECK(color, ECmissing, "missing color");
+  for (int c = 0; c < 3; ++c) LCHECK(color[c] >= 0 && color[c] <= 1, ECbounds, "color value out of bounds");
+  return ECok;
+}
+
+enum ErrorCode smolSetMoleculeSize(simptr sim, const char *species, enum MolecState state, double size) {
+  (void)size;
+  LCHECK(sim, ECmissing, "missing sim");
+  LCHECK(species_or_all(sim, species), ECsame, "species not recognized");
+  LCHECK((state >= MSsoln && state <= MSbsoln) || state == MSall, ECsyntax, "invalid state");
+  return ECok;
+}
+
+enum ErrorCode smolSetMoleculeStyle(simptr sim, const char *species, enum MolecState state, double size,
+                                    double *color) {
+  (void)size;
+  LCHECK(sim, ECmissing, "missing sim");
+  LCHECK(species_or_all(sim, species), ECsame, "species not recognized");
+  LCHECK((state >= MSsoln && state <= MSbsoln) || state == MSall, ECsyntax, "invalid state");
+  if (color)
+    for (int c = 0; c < 3; ++c) LCHECK(color[c] >= 0 && color[c] <= 1, ECbounds, "color value out of bounds");
+  return ECok;
+}
+
+enum ErrorCode smolDisplaySim(simptr sim) {
+  LCHECK(sim, ECmissing, "missing sim");
+  const Sim &s = sim->s;
+  printf("libsmoldyn_b200 simulation: %d dimension(s), time %g to %g step %g\n", s.dim, s.tstart, s.tstop, s.dt);
+  for (int d = 0; d < s.dim; ++d)
+    printf("  axis %d: %g to %g, walls %c %c\n", d, s.lo[d], s.hi[d], s.btype[d][0], s.btype[d][1]);
+  for (size_t i = 1; i < s.species.size(); ++i)
+    printf("  species %s: difc %g\n", s.species[i].name.c_str(), s.species[i].difc);
+  for (int o = 0; o < 3; ++o)
+    for (const smolb::RxnDef &r : s.rxn[o]) printf("  reaction %s: order %d, rate %g\n", r.name.c_str(), o, r.rate);
+  printf("  surfaces %d, compartments %d\n", (int)s.surfaces.size(), (int)s.cmpts.size());
+  return ECok;
 }
 
 void smolGetSpeciesName(simptr sim, int speciesindex, char *species) {

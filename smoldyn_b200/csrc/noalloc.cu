@@ -17,8 +17,16 @@
 //   call while an earlier one is still in flight) race on it and must be
 //   serialised by the caller;
 // - the first call on each device sets up the scratch address
-//   (cudaGetSymbolAddress, with that device current); make that first call
-//   before any stream capture.
+//   (cudaGetSymbolAddress, with that device current).  With lazy module
+//   loading (the CUDA 12 default) that call can load this library's device
+//   code, which places the scratch in device memory and may synchronise, so
+//   the first call belongs at set-up time: before HBM is filled and before
+//   any stream capture.  The address is cached per device; a cudaDeviceReset
+//   invalidates it, so the library must be reloaded after one;
+// - the copies are synchronous cudaMemcpy and the kernel runs on the legacy
+//   default stream, which waits for every blocking stream of the process:
+//   the call overlaps only work on cudaStreamNonBlocking streams (the
+//   engine's own streams are created that way).
 // No scratch slot is read before the same call writes it (inputs are copied
 // in, every output below n is written by the kernel), so nothing has to be
 // cleared between calls.

@@ -93,6 +93,7 @@ struct Sim {
   std::vector<RxnDef> rxn[3];
   std::vector<SurfaceDef> surfaces;
   std::vector<CompartDef> cmpts;
+  std::vector<std::string> mollists; // molecule list names (recorded only; one box-sorted array holds all)
   double tstart = 0, tstop = 0, dt = 0, time = 0;
   bool time_set = false;
   long long seed = 0;

@@ -56,3 +56,20 @@ def test_limit_and_bad_arguments_rejected():
     rate, difc, b = _binding_case(LIMIT, 23)
     out = sb.solve_radii_device_noalloc(0, rate, 0.01, difc, b, rel=1)
     assert np.array_equal(out, sb.solve_radii_device(0, rate, 0.01, difc, b, rel=1), equal_nan=True)
+
+
+def test_call_after_setup_allocates_nothing():
+    """The property the entry point exists for: once the first call has set
+    up the scratch, a full-size call leaves the device's free memory as it
+    was (cudaMemGetInfo before and after)."""
+    import torch
+
+    rate, difc, b = _binding_case(LIMIT, 24)
+    first = sb.solve_radii_device_noalloc(0, rate, 0.01, difc, b, rel=1)  # set-up call
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    again = sb.solve_radii_device_noalloc(0, rate, 0.01, difc, b, rel=1)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    assert np.array_equal(first, again, equal_nan=True)
