@@ -260,6 +260,19 @@ enum ErrorCode smolgpuSolveRadiiNoAlloc(int mode, long long n, const double *rat
                                         const double *difc, const double *b, int rel, double *out);
 /* Same solver on the host CPU (product path used by parameter updates). */
 double smolgpuBindingRadiusHost(double rate, double dt, double difc, double b, int rel);
+/* Reaction probability p < 1 on the host, the product path of every
+ * second-order reaction's parameter derivation: numrxnrateprob
+ * (rxnparam.c:161-518) and bindingradiusprob (rxnparam.c:587-681, prob in/out
+ * as in the reference: with chi < 0 *prob is the given probability, with
+ * chi >= 0 it receives the probability found by the 2-D search). */
+double smolgpuNumRxnRateProbHost(double step, double a, double b, double prob);
+double smolgpuBindingRadiusProbHost(double rate, double dt, double difc, double b, int rel, double chi,
+                                    double *prob);
+/* bindingradiusprob batched on the device, one problem per element:
+ * out[i] = bindingradiusprob(rate[i], dt, difc[i], b[i], rel, chi[i], &prob[i]).
+ * Host arrays of length n; prob is read and written. */
+enum ErrorCode smolgpuSolveRadiiProb(long long n, const double *rate, double dt, const double *difc,
+                                     const double *b, int rel, const double *chi, double *prob, double *out);
 double smolgpuUnbindingRadiusHost(double pgem, double dt, double difc, double a);
 
 /* Radial-distribution-function solver on the device: the numerical method

@@ -90,6 +90,10 @@ int main(int argc, char **argv) {
           const double rate = rxncalcrate(sim, order, r, &pgem);
           fprintf(g_out, "R %d %d %.17g %.17g\n", order, r, rate, pgem);
         }
+    /* second-order parameters as rxnsetrate left them: bindrad2 and prob */
+    if (sim->rxnss[2])
+      for (int r = 0; r < sim->rxnss[2]->totrxn; r++)
+        fprintf(g_out, "P %d %.17g %.17g\n", r, sim->rxnss[2]->rxn[r]->bindrad2, sim->rxnss[2]->rxn[r]->prob);
     fclose(g_out);
     smolFreeSim(sim);
     return 0;

@@ -115,6 +115,10 @@ PROTOTYPES = {
     "smolgpuSolveRadii": (C.c_int, [C.c_int, C.c_longlong, _dp, C.c_double, _dp, _dp, C.c_int, _dp]),
     "smolgpuSolveRadiiNoAlloc": (C.c_int, [C.c_int, C.c_longlong, _dp, C.c_double, _dp, _dp, C.c_int, _dp]),
     "smolgpuBindingRadiusHost": (C.c_double, [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int]),
+    "smolgpuNumRxnRateProbHost": (C.c_double, [C.c_double, C.c_double, C.c_double, C.c_double]),
+    "smolgpuBindingRadiusProbHost": (C.c_double, [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                                                  C.c_double, _dp]),
+    "smolgpuSolveRadiiProb": (C.c_int, [C.c_longlong, _dp, C.c_double, _dp, _dp, C.c_int, _dp, _dp, _dp]),
     "smolgpuUnbindingRadiusHost": (C.c_double, [C.c_double, C.c_double, C.c_double, C.c_double]),
     "smolgpuRdfTable": (C.c_int, [C.c_char, C.c_int, C.c_double, C.c_char, C.c_int, _dp, _dp, _ip, _ip]),
     "smolgpuRdfSteadyState": (C.c_int, [C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp, C.c_double, _dp,
@@ -539,6 +543,21 @@ def solve_radii_device(mode, rate, dt, difc, b, rel=0):
     out = np.zeros_like(rate)
     check(lib.smolgpuSolveRadii(mode, len(rate), dptr(rate), dt, dptr(difc), dptr(b), rel, dptr(out)))
     return out
+
+
+def solve_radii_prob_device(rate, dt, difc, b, rel, chi, prob):
+    """smolgpuSolveRadiiProb: bindingradiusprob on the device; returns
+    (radii, probabilities)."""
+    lib = load()
+    rate = np.ascontiguousarray(rate, dtype=np.float64)
+    difc = np.ascontiguousarray(difc, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    chi = np.ascontiguousarray(chi, dtype=np.float64)
+    prob = np.array(prob, dtype=np.float64, copy=True)
+    out = np.zeros_like(rate)
+    check(lib.smolgpuSolveRadiiProb(len(rate), dptr(rate), dt, dptr(difc), dptr(b), rel, dptr(chi), dptr(prob),
+                                    dptr(out)))
+    return out, prob
 
 
 RDF_ROWS = {"i": 1, "r": 16, "b": 11}

@@ -1223,6 +1223,25 @@ double smolgpuBindingRadiusHost(double rate, double dt, double difc, double b, i
   return smolb::rxnp::bindingradius(rate, dt, difc, b, rel);
 }
 
+double smolgpuNumRxnRateProbHost(double step, double a, double b, double prob) {
+  return smolb::rxnp::numrxnrateprob(step, a, b, prob);
+}
+
+double smolgpuBindingRadiusProbHost(double rate, double dt, double difc, double b, int rel, double chi,
+                                    double *prob) {
+  return smolb::rxnp::bindingradiusprob(rate, dt, difc, b, rel, chi, prob);
+}
+
+enum ErrorCode smolgpuSolveRadiiProb(long long n, const double *rate, double dt, const double *difc,
+                                     const double *b, int rel, const double *chi, double *prob, double *out) {
+  LCHECK(n >= 0, ECbounds, "n must be >= 0");
+  LCHECK(n == 0 || (rate && difc && b && chi && prob && out), ECmissing, "missing arrays");
+  std::string err;
+  if (smolb::solve_radii_prob_device(n, rate, dt, difc, b, rel, chi, prob, out, &err))
+    return set_error(__func__, ECerror, err);
+  return ECok;
+}
+
 double smolgpuUnbindingRadiusHost(double pgem, double dt, double difc, double a) {
   return smolb::rxnp::unbindingradius(pgem, dt, difc, a);
 }

@@ -1950,6 +1950,20 @@ __global__ void k_solve_radii(int mode, long long n, const double *rate, double 
   }
 }
 
+// Batched bindingradiusprob (rxnparam.c:587-681), one thread per problem:
+// with chi[i] < 0 the reaction probability prob[i] is given and the binding
+// radius is searched; with chi[i] >= 0 both are searched and prob[i] receives
+// the probability found.
+__global__ void k_solve_radii_prob(long long n, const double *rate, double dt, const double *difc, const double *b,
+                                   int rel, const double *chi, double *prob, double *out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double p = prob[i];
+    out[i] = rxnp::bindingradiusprob(rate[i], dt, difc[i], b[i], rel, chi[i], &p);
+    prob[i] = p;
+  }
+}
+
 // ===========================================================================
 // Host driver
 // ===========================================================================
@@ -3343,6 +3357,24 @@ int solve_radii_device(int mode, long long n, const double *rate, double dt, con
   k_solve_radii<<<sm_count() * 2, 128>>>(mode, n, d, dt, d + n, d + 2 * n, rel, d + 3 * n);
   CK(cudaGetLastError());
   CK(cudaMemcpy(out, d + 3 * n, n * sizeof(double), cudaMemcpyDeviceToHost));
+  cudaFree(d);
+  return 0;
+}
+
+int solve_radii_prob_device(long long n, const double *rate, double dt, const double *difc, const double *b,
+                            int rel, const double *chi, double *prob, double *out, std::string *err) {
+  if (n <= 0) return 0;
+  double *d = nullptr;
+  CK(cudaMalloc(&d, (size_t)n * 6 * sizeof(double)));
+  CK(cudaMemcpy(d, rate, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d + n, difc, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d + 2 * n, b, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d + 3 * n, chi, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d + 4 * n, prob, n * sizeof(double), cudaMemcpyHostToDevice));
+  k_solve_radii_prob<<<sm_count() * 2, 128>>>(n, d, dt, d + n, d + 2 * n, rel, d + 3 * n, d + 4 * n, d + 5 * n);
+  CK(cudaGetLastError());
+  CK(cudaMemcpy(prob, d + 4 * n, n * sizeof(double), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(out, d + 5 * n, n * sizeof(double), cudaMemcpyDeviceToHost));
   cudaFree(d);
   return 0;
 }

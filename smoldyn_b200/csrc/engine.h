@@ -184,6 +184,9 @@ class Engine {
 // Batched FP64 radius solver on the device (mode 0: binding, 1: unbinding).
 int solve_radii_device(int mode, long long n, const double *rate, double dt, const double *difc,
                        const double *b, int rel, double *out, std::string *err);
+// Batched bindingradiusprob on the device (prob in/out per problem).
+int solve_radii_prob_device(long long n, const double *rate, double dt, const double *difc, const double *b,
+                            int rel, const double *chi, double *prob, double *out, std::string *err);
 
 }  // namespace smolb
 

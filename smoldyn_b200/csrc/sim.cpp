@@ -872,7 +872,19 @@ int read_config_statement(Sim &sim, const std::string &word, const std::string &
     int o;
     const int r = sim.reaction_index(w[0], &o);
     if (r < 0) { if (err) *err = "reaction_probability: unknown reaction"; return -3; }
-    sim.rxn[o][r].prob_user = atof(w[1].c_str());
+    const double v = atof(w[1].c_str());
+    if (v < 0 || v > 1) { if (err) *err = "probability value must be between 0 and 1"; return -6; }
+    sim.rxn[o][r].prob_user = v;
+    sim.need_update = true;
+  } else if (word == "reaction_chi") {  // smolsim.cpp:1799-1821: order 2 only, 0 < chi < 1 or -1
+    if (!need(2)) return -7;
+    int o;
+    const int r = sim.reaction_index(w[0], &o);
+    if (r < 0) { if (err) *err = "reaction_chi: unknown reaction"; return -3; }
+    if (o != 2) { if (err) *err = "reaction chi value is only allowed for order 2 reactions"; return -6; }
+    const double v = atof(w[1].c_str());
+    if (!(v != 0 && v < 1)) { if (err) *err = "reaction chi value must be between 0 and 1 (or -1 to disable)"; return -6; }
+    sim.rxn[2][r].chi = v;
     sim.need_update = true;
   } else if (word == "confspread_radius") {  // smolsim.cpp:1736, smolreact.c:1762
     if (!need(2)) return -7;

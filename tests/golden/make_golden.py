@@ -12,6 +12,7 @@ tests/golden/<name>.npz with:
   pos1, sp1, serno1   the reference's state after the step
   L, wall, kf, kr     cube side, boundary type ("t": walls transparent, the
                       case's surfaces close the box), rate constants
+  ub                  unbinding radius of the unbind case (-1 elsewhere)
   config              the configuration text the reference ran
 Usage: python tests/golden/make_golden.py   (needs `make -C oracle ref`)
 """
@@ -127,6 +128,32 @@ SURFACE_CASES = {
                                    tube_action="action both all transmit", cap_action="action both all absorb"),
 }
 
+# Product placement at the unbinding radius: every C splits into A + B in the
+# recorded step (rate 1000, so the first-order probability 1 - e^-10) with
+# product_placement unbindrad, so each pair of products sits at distance 0.6
+# along one random direction, split by the products' diffusion coefficients
+# (rxnsetproduct, smolreact.c:1545-1548; random orientation in doreact,
+# smolreact.c:2840-2850).  C does not diffuse, so the reaction sites are the
+# start positions.
+UNBIND_CONFIG = """dim 3
+species A B C
+difc A 1
+difc B 0.5
+difc C 0
+time_start 0
+time_stop 1
+time_step 0.01
+boundaries 0 0 {L} p
+boundaries 1 0 {L} p
+boundaries 2 0 {L} p
+random_seed {seed}
+reaction split C -> A + B 1000
+product_placement split unbindrad {ub}
+mol {nC} C u u u
+end_file
+"""
+UNBIND_CASES = {"onestep_unbind": dict(L=100, seed=41, nC=3000, ub=0.6)}
+
 CASES = {
     "onestep_reflect": dict(L=20, w="r", seed=11, kf=20, kr=1, nA=1600, nB=1600, nC=800),
     "onestep_periodic": dict(L=20, w="p", seed=12, kf=20, kr=1, nA=1600, nB=1600, nC=800),
@@ -167,7 +194,7 @@ def run_case(name, cfg, template=CONFIG):
         pos1=np.array([f[2:5] for f in F]), sp1=np.array([f[1] for f in F], dtype=np.int32),
         serno1=np.array([f[0] for f in F], dtype=np.uint64),
         L=np.float64(cfg["L"]), wall=np.array(cfg.get("w", "t")), kf=np.float64(cfg.get("kf", -1)),
-        kr=np.float64(cfg.get("kr", -1)), config=np.array(text))
+        kr=np.float64(cfg.get("kr", -1)), ub=np.float64(cfg.get("ub", -1)), config=np.array(text))
     print(name, "molecules", len(D), "->", len(F), "first-order", len(U))
 
 
@@ -180,3 +207,5 @@ if __name__ == "__main__":
         run_case(k, v, PLACEMENT_CONFIG)
     for k, v in SURFACE_CASES.items():
         run_case(k, v, SURFACE_CONFIG)
+    for k, v in UNBIND_CASES.items():
+        run_case(k, v, UNBIND_CONFIG)

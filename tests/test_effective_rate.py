@@ -47,6 +47,16 @@ CASES = {
     "confspread": (["fwd A + B -> A + C 5"], ["confspread_radius fwd 0.3"]),
     "bounce": (["fwd A + B -> A + B 2"], ["product_placement fwd bounce 0.6"]),
     "anisotropic": (["fwd A + B -> C 1"], ["difm A 1 0.5 0 0 2 0 0 0 0.5"]),
+    # reaction probability p < 1: bindingradiusprob's 1-D search (rxnparam.c:612-636)
+    "probability": (["fwd A + B -> C 0.05"], ["reaction_probability fwd 0.3"]),
+    "probability_reversible": (["fwd A + B -> C 2", "rev C -> A + B 1"],
+                               ["reaction_probability fwd 0.5", "product_placement rev ratio 1.5"]),
+    "probability_unbindrad": (["fwd A + B -> C 5", "rev C -> A + B 3"],
+                              ["reaction_probability fwd 0.2", "product_placement rev unbindrad 0.4"]),
+    # requested chi: the 2-D search over (radius, probability) (rxnparam.c:638-676)
+    "chi": (["fwd A + B -> C 0.05"], ["reaction_chi fwd 0.01"]),
+    "chi_reversible": (["fwd A + B -> C 2", "rev C -> A + B 1"],
+                       ["reaction_chi fwd 0.05", "product_placement rev ratio 1.5"]),
 }
 NAMES = {
     "default_placement": [(2, "fwd"), (1, "rev")],
@@ -58,6 +68,11 @@ NAMES = {
     "confspread": [(2, "fwd")],
     "bounce": [(2, "fwd")],
     "anisotropic": [(2, "fwd")],
+    "probability": [(2, "fwd")],
+    "probability_reversible": [(2, "fwd"), (1, "rev")],
+    "probability_unbindrad": [(2, "fwd"), (1, "rev")],
+    "chi": [(2, "fwd")],
+    "chi_reversible": [(2, "fwd"), (1, "rev")],
 }
 
 
@@ -80,6 +95,8 @@ def reference_rates(d, name):
         t = ln.split()
         if t and t[0] == "R":
             res[(int(t[1]), int(t[2]))] = (float(t[3]), float(t[4]))
+        if t and t[0] == "P":  # second-order binding radius squared and probability
+            res[("P", int(t[1]))] = (float(t[2]), float(t[3]))
     return res
 
 
@@ -104,6 +121,12 @@ def test_effective_rate_matches_reference(case):
             rr, rp = ref[(order, r)]
             assert abs(rate - rr) <= 1e-9 * abs(rr) + 1e-300, (nm, rate, rr)
             assert abs(pgem - rp) <= 1e-9 * max(abs(rp), 1e-12), (nm, pgem, rp)
+            if order == 2 and ("P", r) in ref:
+                # binding radius and reaction probability as derived (rxnsetrate, smolreact.c:1396-1408)
+                b2_ref, p_ref = ref[("P", r)]
+                b, _, p = s.reaction_params(nm)
+                assert abs(b * b - b2_ref) <= 1e-9 * b2_ref + 1e-300, (nm, b * b, b2_ref)
+                assert abs(p - p_ref) <= 1e-9 * max(p_ref, 1e-12), (nm, p, p_ref)
         s.close()
 
 
