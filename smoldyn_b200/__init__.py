@@ -131,6 +131,9 @@ PROTOTYPES = {
     "smolgpuEnsembleSetRadiusMode": (C.c_int, [_vp, C.c_int]),
     "smolgpuEnsembleAttachSurrogate": (C.c_int, [_vp, _vp]),
     "smolgpuEnsembleUpdate": (C.c_int, [_vp]),
+    "smolgpuEnsembleSetEngine": (C.c_int, [_vp, C.c_int]),
+    "smolgpuEnsembleGetEngine": (C.c_int, [_vp]),
+    "smolgpuEnsembleGetMolecules": (C.c_int, [_vp, C.POINTER(C.c_longlong), _dp, _ip, _ip, _u64p]),
     "smolgpuEnsembleRunSteps": (C.c_int, [_vp, C.c_longlong]),
     "smolgpuEnsembleGetCounts": (C.c_int, [_vp, C.POINTER(C.c_longlong)]),
     "smolgpuEnsembleGetReactionParams": (C.c_int, [_vp, C.c_char_p, _dp, _dp]),
@@ -423,6 +426,14 @@ class Ensemble:
         counts = np.ascontiguousarray(counts, dtype=np.int32)
         return check(self.lib.smolgpuEnsembleAddMolecules(self.ptr, species.encode(), counts.ctypes.data_as(_ip)))
 
+    def engine(self, mode=None):
+        """Set the stepping engine (0 automatic, 1 step pipeline, 2
+        persistent kernel) when mode is given; return the engine in use
+        (1 or 2)."""
+        if mode is not None:
+            check(self.lib.smolgpuEnsembleSetEngine(self.ptr, mode))
+        return self.lib.smolgpuEnsembleGetEngine(self.ptr)
+
     def radius_mode(self, mode):
         return check(self.lib.smolgpuEnsembleSetRadiusMode(self.ptr, mode))
 
@@ -434,6 +445,21 @@ class Ensemble:
 
     def run_steps(self, n):
         return check(self.lib.smolgpuEnsembleRunSteps(self.ptr, int(n)))
+
+    def molecules(self):
+        """(positions [n,3], species, replicate, serial) of every molecule."""
+        n = C.c_longlong(0)
+        check(self.lib.smolgpuEnsembleGetMolecules(self.ptr, C.byref(n), None, None, None, None))
+        cnt = max(n.value, 1)
+        pos = np.zeros((cnt, 3), dtype=np.float64)
+        sp = np.zeros(cnt, dtype=np.int32)
+        rp = np.zeros(cnt, dtype=np.int32)
+        sn = np.zeros(cnt, dtype=np.uint64)
+        n = C.c_longlong(cnt)
+        check(self.lib.smolgpuEnsembleGetMolecules(self.ptr, C.byref(n), dptr(pos), sp.ctypes.data_as(_ip),
+                                                   rp.ctypes.data_as(_ip), sn.ctypes.data_as(_u64p)))
+        k = n.value
+        return pos[:k], sp[:k], rp[:k], sn[:k]
 
     def counts(self, nspecies):
         out = np.zeros(self.nrep * nspecies, dtype=np.int64)

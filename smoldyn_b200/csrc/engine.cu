@@ -1606,156 +1606,469 @@ __device__ __noinline__ void birth_in_cmpt(int c, const DevGeo &g, ull ekey, uin
   }
 }
 
+// Products of one event (doreact, smolreact.c:2662-2902; births: zeroreact,
+// smolreact.c:2905-2995): positions from the event site, the unbinding
+// offsets under one random rotation per event (or the confspread / bounce
+// placements), walls and surfaces for the new molecules, serial numbers.
+// emit(position, identity) stores one new molecule.  uni counts the
+// first-order events.
+template <int SURF, class Emit>
+__device__ __forceinline__ void place_event(const KParams &p, const Event &e, uint32_t step, int &uni, Emit emit) {
+  const uint2 key = make_uint2(c_net.key0 ^ 0x68E31DA4u, c_net.key1 ^ 0xB5297A4Du);
+  const int order = (int)(e.rxn >> 8), r = (int)(e.rxn & 0xFF), rep = (int)e.rep;
+  const DevGeo g = p.geo[rep];
+  const uint4 rr = philox(make_uint4((uint32_t)e.key, (uint32_t)(e.key >> 32), step, 7u), key);
+  float site[3];
+  int cell[3];
+  if (order == 0) {  // uniform position in the system (smolwall.c:42)
+    const uint32_t bits[3] = {rr.x, rr.y, rr.z};
+    for (int d = 0; d < 3; ++d) {
+      if (d >= g.dim) { site[d] = 0.f; cell[d] = 0; continue; }
+      const float L = (float)(g.n[d] - 1) * g.h[d] + g.whi[d];
+      float w = u01f_open(bits[d]) * L;
+      int j = 0;
+      renorm(w, j, g.h[d], g.inv_h[d]);
+      if (j > g.n[d] - 1) { w += (float)(j - (g.n[d] - 1)) * g.h[d]; j = g.n[d] - 1; }
+      clamp_cell(w, j, g, d);
+      site[d] = w;
+      cell[d] = j;
+    }
+    if (SURF == 2 && c_net.cmpt[0][r]) birth_in_cmpt(c_net.cmpt[0][r] - 1, g, e.key, step, site, cell);
+  } else {
+    site[0] = e.site.x; site[1] = e.site.y; site[2] = e.site.z;
+    unpack_cell(__float_as_uint(e.site.w), cell[0], cell[1], cell[2]);
+    if (order == 1) {
+      uni++;
+      atomicAdd((unsigned long long *)&p.spcount[rep * c_net.nsp + c_net.rct[1][r][0]],
+                (unsigned long long)(-1ll));
+    }
+  }
+  const int np = c_net.nprod[order][r];
+  // confspread / bounce (doreact, smolreact.c:2736-2805): products 1 and 2
+  // take (confspread) or are pushed apart from (bounce) the reactants'
+  // places, keep the reactants' serial numbers, and the rest sit at the site
+  const int place = order == 2 ? c_net.placement2[r] : 0;
+  float cust[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+  ull keep_sn[2] = {0, 0};
+  if (place) {
+    float va[3], vb[3];
+    int cs[3];
+    unpack_cell(__float_as_uint(e.site.w), cs[0], cs[1], cs[2]);
+    const float us[3] = {e.site.x, e.site.y, e.site.z};
+    for (int k = 0; k < 2; ++k) {
+      const int idx = k == 0 ? e.ia : e.ib;
+      const float4 q = p.b_pc[idx];
+      keep_sn[k] = id_serno(p.b_id[idx]);
+      int cq[3];
+      unpack_cell(__float_as_uint(q.w), cq[0], cq[1], cq[2]);
+      const float uq[3] = {q.x, q.y, q.z};
+      float *v = k == 0 ? va : vb;
+      for (int d = 0; d < 3; ++d) {  // site -> reactant, nearest periodic image
+        int dc = cq[d] - cs[d];
+        if (dc > 1) dc -= g.n[d];
+        else if (dc < -1) dc += g.n[d];
+        v[d] = d < g.dim ? (uq[d] - us[d]) + (float)dc * g.h[d] : 0.f;
+      }
+    }
+    if (place == 1) {
+      for (int d = 0; d < 3; ++d) { cust[0][d] = va[d]; cust[1][d] = vb[d]; }
+    } else {
+      float v[3] = {vb[0] - va[0], vb[1] - va[1], vb[2] - va[2]};
+      float dist = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+      if (dist == 0.f) {
+        dist = sqrtf(p.bind2[rep * c_net.nr[2] + r]);
+        v[0] = dist;
+      }
+      const int kx2 = c_net.rxn_base[2] + r;
+      const float *pp = p.prdpos + (size_t)(rep * c_net.nrx_total + kx2) * kMaxProd * 3;
+      const float p0 = pp[0], p1 = pp[3];
+      const float x = c_net.bounce_k[r] * (1.f / dist - 1.f / (p0 + p1));
+      for (int d = 0; d < 3; ++d) {
+        cust[0][d] = va[d] - x * p0 * v[d];
+        cust[1][d] = vb[d] + x * p1 * v[d];
+      }
+    }
+  }
+  float m[9];
+  bool rot = false;
+  if (!place && c_net.has_offset[order][r] && !c_net.fixed[order][r] && !c_net.inject) {
+    random_rotation(philox(make_uint4((uint32_t)e.key, (uint32_t)(e.key >> 32), step, 8u), key), m);
+    rot = true;
+  }
+  const int kx = c_net.rxn_base[order] + r;
+  for (int q = 0; q < np; ++q) {
+    const int psp = c_net.prd[order][r][q];
+    float off[3] = {0.f, 0.f, 0.f};
+    if (place) {
+      if (q < 2) { off[0] = cust[q][0]; off[1] = cust[q][1]; off[2] = cust[q][2]; }
+    } else if (c_net.has_offset[order][r]) {
+      const float *pp = p.prdpos + ((size_t)(rep * c_net.nrx_total + kx) * kMaxProd + q) * 3;
+      if (rot) {
+        off[0] = m[0] * pp[0] + m[1] * pp[1] + m[2] * pp[2];
+        off[1] = m[3] * pp[0] + m[4] * pp[1] + m[5] * pp[2];
+        off[2] = m[6] * pp[0] + m[7] * pp[1] + m[8] * pp[2];
+      } else {
+        off[0] = pp[0]; off[1] = pp[1]; off[2] = pp[2];
+      }
+    }
+    float w[3];
+    int c[3];
+    bool dead = false;
+    int hits = 0;
+    for (int d = 0; d < 3; ++d) {
+      w[d] = site[d] + (d < g.dim ? off[d] : 0.f);
+      c[d] = cell[d];
+      renorm(w[d], c[d], g.h[d], g.inv_h[d]);
+      if (d < g.dim && (c[d] <= 0 || c[d] >= g.n[d] - 1))
+        if (walls_dim(w[d], c[d], g, d, hits)) dead = true;
+      clamp_cell(w[d], c[d], g, d);
+    }
+    if (SURF && !dead) {
+      // new molecules are checked against surfaces from the reaction site
+      // (smolsim.cpp:2656-2660, reborn pass of checksurfaces)
+      double x0[3], x1[3];
+      to_abs(g, cell, site, x0);
+      to_abs(g, c, w, x1);
+      if (surface_interact<SURF == 2>(psp, x0, x1, c_net.surf_eps, hits)) dead = true;
+      else from_abs(g, x1, c, w);
+    }
+    if (hits) atomicAdd(&p.counters[0], (unsigned long long)hits);
+    if (dead) continue;
+    const ull serno = (place && q < 2) ? keep_sn[q]
+                                       : kProductSernoBit |
+                                             (mix64(e.key ^ ((ull)q << 50) ^ ((ull)step << 20) ^ (ull)(order * 97 + r)) &
+                                              (kProductSernoBit - 1));
+    emit(make_float4(w[0], w[1], w[2], __uint_as_float(pack_cell(c[0], c[1], c[2]))), make_id(psp, rep, serno));
+  }
+}
+
 template <int SURF>
 __global__ void k_products(KParams p) {
   pdl_launch_dependents();
   pdl_wait();
   const int ne = min(*p.nev, p.evcap);
   const uint32_t step = *p.step;
-  const uint2 key = make_uint2(c_net.key0 ^ 0x68E31DA4u, c_net.key1 ^ 0xB5297A4Du);
   int uni = 0;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ne; t += gridDim.x * blockDim.x) {
-    const Event e = p.ev[t];
-    const int order = (int)(e.rxn >> 8), r = (int)(e.rxn & 0xFF), rep = (int)e.rep;
-    const DevGeo g = p.geo[rep];
-    const uint4 rr = philox(make_uint4((uint32_t)e.key, (uint32_t)(e.key >> 32), step, 7u), key);
-    float site[3];
-    int cell[3];
-    if (order == 0) {  // uniform position in the system (smolwall.c:42)
-      const uint32_t bits[3] = {rr.x, rr.y, rr.z};
-      for (int d = 0; d < 3; ++d) {
-        if (d >= g.dim) { site[d] = 0.f; cell[d] = 0; continue; }
-        const float L = (float)(g.n[d] - 1) * g.h[d] + g.whi[d];
-        float w = u01f_open(bits[d]) * L;
-        int j = 0;
-        renorm(w, j, g.h[d], g.inv_h[d]);
-        if (j > g.n[d] - 1) { w += (float)(j - (g.n[d] - 1)) * g.h[d]; j = g.n[d] - 1; }
-        clamp_cell(w, j, g, d);
-        site[d] = w;
-        cell[d] = j;
-      }
-      if (SURF == 2 && c_net.cmpt[0][r]) birth_in_cmpt(c_net.cmpt[0][r] - 1, g, e.key, step, site, cell);
-    } else {
-      site[0] = e.site.x; site[1] = e.site.y; site[2] = e.site.z;
-      unpack_cell(__float_as_uint(e.site.w), cell[0], cell[1], cell[2]);
-      if (order == 1) {
-        uni++;
-        atomicAdd((unsigned long long *)&p.spcount[rep * c_net.nsp + c_net.rct[1][r][0]],
-                  (unsigned long long)(-1ll));
-      }
-    }
-    const int np = c_net.nprod[order][r];
-    // confspread / bounce (doreact, smolreact.c:2736-2805): products 1 and 2
-    // take (confspread) or are pushed apart from (bounce) the reactants'
-    // places, keep the reactants' serial numbers, and the rest sit at the site
-    const int place = order == 2 ? c_net.placement2[r] : 0;
-    float cust[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
-    ull keep_sn[2] = {0, 0};
-    if (place) {
-      float va[3], vb[3];
-      int cs[3];
-      unpack_cell(__float_as_uint(e.site.w), cs[0], cs[1], cs[2]);
-      const float us[3] = {e.site.x, e.site.y, e.site.z};
-      for (int k = 0; k < 2; ++k) {
-        const int idx = k == 0 ? e.ia : e.ib;
-        const float4 q = p.b_pc[idx];
-        keep_sn[k] = id_serno(p.b_id[idx]);
-        int cq[3];
-        unpack_cell(__float_as_uint(q.w), cq[0], cq[1], cq[2]);
-        const float uq[3] = {q.x, q.y, q.z};
-        float *v = k == 0 ? va : vb;
-        for (int d = 0; d < 3; ++d) {  // site -> reactant, nearest periodic image
-          int dc = cq[d] - cs[d];
-          if (dc > 1) dc -= g.n[d];
-          else if (dc < -1) dc += g.n[d];
-          v[d] = d < g.dim ? (uq[d] - us[d]) + (float)dc * g.h[d] : 0.f;
-        }
-      }
-      if (place == 1) {
-        for (int d = 0; d < 3; ++d) { cust[0][d] = va[d]; cust[1][d] = vb[d]; }
-      } else {
-        float v[3] = {vb[0] - va[0], vb[1] - va[1], vb[2] - va[2]};
-        float dist = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-        if (dist == 0.f) {
-          dist = sqrtf(p.bind2[rep * c_net.nr[2] + r]);
-          v[0] = dist;
-        }
-        const int kx2 = c_net.rxn_base[2] + r;
-        const float *pp = p.prdpos + (size_t)(rep * c_net.nrx_total + kx2) * kMaxProd * 3;
-        const float p0 = pp[0], p1 = pp[3];
-        const float x = c_net.bounce_k[r] * (1.f / dist - 1.f / (p0 + p1));
-        for (int d = 0; d < 3; ++d) {
-          cust[0][d] = va[d] - x * p0 * v[d];
-          cust[1][d] = vb[d] + x * p1 * v[d];
-        }
-      }
-    }
-    float m[9];
-    bool rot = false;
-    if (!place && c_net.has_offset[order][r] && !c_net.fixed[order][r] && !c_net.inject) {
-      random_rotation(philox(make_uint4((uint32_t)e.key, (uint32_t)(e.key >> 32), step, 8u), key), m);
-      rot = true;
-    }
-    const int kx = c_net.rxn_base[order] + r;
-    for (int q = 0; q < np; ++q) {
-      const int psp = c_net.prd[order][r][q];
-      float off[3] = {0.f, 0.f, 0.f};
-      if (place) {
-        if (q < 2) { off[0] = cust[q][0]; off[1] = cust[q][1]; off[2] = cust[q][2]; }
-      } else if (c_net.has_offset[order][r]) {
-        const float *pp = p.prdpos + ((size_t)(rep * c_net.nrx_total + kx) * kMaxProd + q) * 3;
-        if (rot) {
-          off[0] = m[0] * pp[0] + m[1] * pp[1] + m[2] * pp[2];
-          off[1] = m[3] * pp[0] + m[4] * pp[1] + m[5] * pp[2];
-          off[2] = m[6] * pp[0] + m[7] * pp[1] + m[8] * pp[2];
-        } else {
-          off[0] = pp[0]; off[1] = pp[1]; off[2] = pp[2];
-        }
-      }
-      float w[3];
-      int c[3];
-      bool dead = false;
-      int hits = 0;
-      for (int d = 0; d < 3; ++d) {
-        w[d] = site[d] + (d < g.dim ? off[d] : 0.f);
-        c[d] = cell[d];
-        renorm(w[d], c[d], g.h[d], g.inv_h[d]);
-        if (d < g.dim && (c[d] <= 0 || c[d] >= g.n[d] - 1))
-          if (walls_dim(w[d], c[d], g, d, hits)) dead = true;
-        clamp_cell(w[d], c[d], g, d);
-      }
-      if (SURF && !dead) {
-        // new molecules are checked against surfaces from the reaction site
-        // (smolsim.cpp:2656-2660, reborn pass of checksurfaces)
-        double x0[3], x1[3];
-        to_abs(g, cell, site, x0);
-        to_abs(g, c, w, x1);
-        if (surface_interact<SURF == 2>(psp, x0, x1, c_net.surf_eps, hits)) dead = true;
-        else from_abs(g, x1, c, w);
-      }
-      if (hits) atomicAdd(&p.counters[0], (unsigned long long)hits);
-      if (dead) continue;
-      const ull serno = (place && q < 2) ? keep_sn[q]
-                                         : kProductSernoBit |
-                                               (mix64(e.key ^ ((ull)q << 50) ^ ((ull)step << 20) ^ (ull)(order * 97 + r)) &
-                                                (kProductSernoBit - 1));
+    place_event<SURF>(p, p.ev[t], step, uni, [&](float4 npc, ull nid) {
       const int slot = atomicAdd(p.q_n, 1);
       if (slot < p.pcap) {
-        const float4 npc = make_float4(w[0], w[1], w[2], __uint_as_float(pack_cell(c[0], c[1], c[2])));
-        const ull nid = make_id(psp, rep, serno);
         p.q_pc[slot] = npc;
         p.q_id[slot] = nid;
-        atomicAdd((unsigned long long *)&p.spcount[rep * c_net.nsp + psp], 1ull);
+        atomicAdd((unsigned long long *)&p.spcount[id_rep(nid) * c_net.nsp + id_species(nid)], 1ull);
       } else {
         atomicOr(p.status, kStProdCap);
       }
-    }
+    });
   }
   if (uni) atomicAdd(&p.counters[2], (unsigned long long)uni);
   // clear the candidate keys of this step
   const int nc = min(*p.ncand, p.candcap);
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nc; t += gridDim.x * blockDim.x)
     p.best[p.cand[t]] = ~0ull;
+}
+
+// ===========================================================================
+// Persistent ensemble engine
+// ===========================================================================
+// Replicates of an ensemble are independent, so they need none of the
+// device-wide synchronisation of the step pipeline above.  One CTA takes a
+// replicate from a work counter (largest replicates first) and runs a whole
+// block of steps on it - move, box sort, pair search, conflict rounds,
+// products - with block barriers between the phases, then takes the next
+// replicate.  Each replicate owns a region of the persistent buffers with
+// room to grow, and its boxes are numbered after the previous replicate's
+// with one spare entry, so its box counts and starts (including the end of
+// its last box) are private to it: a replicate's working set stays in L2
+// while its CTA steps it.  The per-molecule functions are the step
+// pipeline's own (advance_one, search_partner, pair_reaction, pair_site,
+// place_event), keyed by the same serial numbers and step counters, so a
+// replicate follows the trajectory it follows in the step pipeline up to the
+// order in which equidistant candidates are ranked.
+struct PersistArgs {
+  const int *order;  // replicate processing order (largest first)
+  const int *roff;   // region offset of each replicate
+  const int *rcap;   // region capacity of each replicate
+  int *rn;           // entries (live or dead) of each replicate in the current buffer
+  int *queue;        // work counter, zeroed before each launch
+  Event *ev;         // event lists, evslice per CTA
+  int evslice;
+  int *cand;         // pair-candidate lists, candslice per CTA
+  int candslice;
+  int nrep;
+  int nsteps;
+};
+
+constexpr int kPersistThreads = 256;
+#ifndef SMOLB_PERSIST_BLOCKS
+#define SMOLB_PERSIST_BLOCKS 3
+#endif
+
+// Shared state of one CTA's step: event, candidate and product counters and
+// the replicate's sorted count.
+struct PersistShared {
+  int nev, nc, np, ns;
+  int warp[32];
+};
+
+template <int SURF>
+__device__ __forceinline__ void persist_commit(const KParams &p, int rep, const int *cand, int nc, uint32_t step,
+                                               Event *ev, int evcap, PersistShared &sh, int &done) {
+  for (int t = threadIdx.x; t < nc; t += blockDim.x) {
+    const int i = cand[t];
+    const ull bi = p.best[i];
+    if (bi == ~0ull) continue;
+    const int j = (int)(uint32_t)bi;
+    if (j <= i) continue;
+    const ull bj = p.best[j];
+    if ((int)(uint32_t)bj != i) continue;
+    const ull idi = p.b_id[i], idj = p.b_id[j];
+    const int spi = id_species(idi), spj = id_species(idj);
+    if (spi == kDeadSpecies || spj == kDeadSpecies) continue;
+    const float d2 = __uint_as_float((uint32_t)(bi >> 32));
+    const int r = pair_reaction<SURF == 2>(p, rep, spi, spj, d2, id_stream(idi), id_stream(idj), step, i, j);
+    if (r < 0) continue;
+    const bool i_first = (c_net.rct[2][r][0] == spi);
+    const int a = i_first ? i : j, b = i_first ? j : i;
+    Event e;
+    e.site = pair_site(p, a, b, r, rep);
+    const ull ka = id_stream(p.b_id[a]), kb = id_stream(p.b_id[b]);
+    e.key = mix64(ka * 0x9E3779B97F4A7C15ull ^ kb) & ((1ull << kSpShift) - 1);
+    e.rxn = (2u << 8) | (uint32_t)r;
+    e.rep = (uint32_t)rep;
+    e.ia = a;
+    e.ib = b;
+    const int k = atomicAdd(&sh.nev, 1);
+    if (k < evcap) ev[k] = e;
+    else atomicOr(p.status, kStEvCap);
+    p.b_id[i] = id_mark_dead(idi);
+    p.b_id[j] = id_mark_dead(idj);
+    atomicAdd((unsigned long long *)&p.spcount[rep * c_net.nsp + spi], (unsigned long long)(-1ll));
+    atomicAdd((unsigned long long *)&p.spcount[rep * c_net.nsp + spj], (unsigned long long)(-1ll));
+    done++;
+  }
+}
+
+// One time step of replicate `rep` (entries [off, off+n) of p.a_*): returns
+// the entry count of its next state in p.b_*.  All threads of the block call
+// it; it begins and ends at a block barrier.
+template <int SURF>
+__device__ __forceinline__ int persist_step(const KParams &p, int rep, int off, int cap, int n, uint32_t step,
+                                            const float *gtab, Event *ev, int evcap, int *cand, int candcap,
+                                            PersistShared &sh, unsigned long long *acc) {
+  const DevGeo &g = p.geo[rep];
+  const int T = blockDim.x, tid = threadIdx.x;
+  const int nb = g.n[0] * g.n[1] * g.n[2];
+  const int c0 = g.cell0;
+  if (tid == 0) { sh.nev = 0; sh.nc = 0; sh.np = 0; }
+  __syncthreads();
+  // ---- move (diffuse, walls, first-order decisions) and box histogram
+  int hits = 0;
+  for (int i = tid; i < n; i += T) {
+    const int idx = off + i;
+    float4 pc = p.a_pc[idx];
+    const ull id = p.a_id[idx];
+    int fate = -1;
+    if (id_species(id) != kDeadSpecies) fate = advance_one<false, SURF>(pc, id, step, p, gtab, 0, hits);
+    if (fate == 0) {
+      p.tmp[idx] = pc;
+      atomicAdd(&p.cnt[global_cell(g, __float_as_uint(pc.w))], 1);
+    } else {
+      p.tmp[idx] = make_float4(0.f, 0.f, 0.f, __uint_as_float(kTmpGone));
+      if (fate == 1) {
+        atomicAdd((unsigned long long *)&p.spcount[rep * c_net.nsp + id_species(id)], (unsigned long long)(-1ll));
+      } else if (fate >= 2) {
+        Event e;
+        e.site = pc;
+        e.key = id_stream(id);
+        e.rxn = (1u << 8) | (uint32_t)(fate - 2);
+        e.rep = (uint32_t)rep;
+        e.ia = e.ib = -1;
+        const int k = atomicAdd(&sh.nev, 1);
+        if (k < evcap) ev[k] = e;
+        else atomicOr(p.status, kStEvCap);
+      }
+    }
+  }
+  acc[0] += (unsigned long long)hits;
+  // zeroth-order births (the keys of births(): one Poisson draw per reaction)
+  if (tid < c_net.nr[0]) {
+    const int r = tid, nr0 = c_net.nr[0];
+    const uint2 key = make_uint2(c_net.key0 ^ 0x5bd1e995u, c_net.key1);
+    const int nbirth = poisson_sample(p.births[rep * nr0 + r], key, make_uint4((uint32_t)rep, (uint32_t)r, step, 0u));
+    if (nbirth > 0) {
+      const int base = atomicAdd(&sh.nev, nbirth);
+      acc[1] += (unsigned long long)nbirth;
+      for (int k = 0; k < nbirth; ++k) {
+        if (base + k >= evcap) { atomicOr(p.status, kStEvCap); break; }
+        Event e;
+        e.site = make_float4(0.f, 0.f, 0.f, 0.f);
+        e.key = mix64(((ull)rep << 40) ^ ((ull)r << 32) ^ ((ull)step << 8) ^ 0xB17Aull ^
+                      mix64((ull)k + 0x9E37ull * (ull)step)) & ((1ull << kSpShift) - 1);
+        e.rxn = (0u << 8) | (uint32_t)r;
+        e.rep = (uint32_t)rep;
+        e.ia = e.ib = -1;
+        ev[base + k] = e;
+      }
+    }
+  }
+  __syncthreads();
+  // ---- exclusive scan of the box counts into box starts (region offset off)
+  {
+    const int per = (nb + T - 1) / T;
+    const int lo = min(nb, tid * per), hi = min(nb, lo + per);
+    int sum = 0;
+    for (int c = lo; c < hi; ++c) sum += p.cnt[c0 + c];
+    int total;
+    int run = off + block_exclusive_scan(sum, sh.warp, total);
+    for (int c = lo; c < hi; ++c) {
+      p.start[c0 + c] = run;
+      run += p.cnt[c0 + c];
+    }
+    if (tid == 0) {
+      p.start[c0 + nb] = off + total;
+      sh.ns = total;
+    }
+  }
+  __syncthreads();
+  const int ns = sh.ns;
+  if (ns > cap) {  // cannot happen: every counted molecule came from the region
+    if (tid == 0) atomicOr(p.status, kStMolCap);
+    return 0;
+  }
+  // ---- scatter into box order (one slot atomic per run of same-box lanes)
+  for (int base = 0; base < n; base += T) {
+    const int i = base + tid;
+    float4 pc = make_float4(0.f, 0.f, 0.f, __uint_as_float(kTmpGone));
+    if (i < n) pc = p.tmp[off + i];
+    const bool alive = __float_as_uint(pc.w) != kTmpGone;
+    const int cell = alive ? global_cell(g, __float_as_uint(pc.w)) : -1;
+    const BoxRun run = box_run(alive, cell);
+    int old = 0;
+    if (alive && run.rank == 0) old = atomicSub(&p.cnt[cell], run.count);
+    const int st = alive ? p.start[cell] : 0;
+    old = __shfl_sync(0xffffffffu, old, alive ? run.head : (tid & 31));
+    if (alive) {
+      const int slot = st + old - run.count + run.rank;
+      p.b_pc[slot] = pc;
+      p.b_id[slot] = p.a_id[off + i];
+    }
+  }
+  __syncthreads();
+  // ---- pair search, round 1: every molecule with pair reactions finds its
+  // closest reacting partner (search_partner, the step pipeline's re-search)
+  int multi = 0;
+  for (int j = tid; j < ns; j += T) {
+    const int idx = off + j;
+    const ull id = p.b_id[idx];
+    const int sp = id_species(id);
+    if (!((c_net.pair_any >> sp) & 1u)) continue;
+    int ncd = 0;
+    const ull best = search_partner<SURF>(p, idx, p.b_pc[idx], id, step, ncd);
+    if (ncd > 1) multi += ncd - 1;
+    if (best != ~0ull) {
+      p.best[idx] = best;
+      const int k = atomicAdd(&sh.nc, 1);
+      if (k < candcap) cand[k] = idx;
+      else atomicOr(p.status, kStCandCap);
+    }
+  }
+  acc[5] += (unsigned long long)multi;
+  __syncthreads();
+  const int nc = min(sh.nc, candcap);
+  int done = 0;
+  if (nc > 0) {
+    persist_commit<SURF>(p, rep, cand, nc, step, ev, evcap, sh, done);
+    for (int round = 1; round < c_net.rounds; ++round) {
+      __syncthreads();
+      for (int t = tid; t < nc; t += T) {  // losers search again among the molecules still present
+        const int i = cand[t];
+        const ull id = p.b_id[i];
+        if (id_species(id) == kDeadSpecies) continue;
+        int ncd;
+        p.best[i] = search_partner<SURF>(p, i, p.b_pc[i], id, step, ncd);
+      }
+      __syncthreads();
+      persist_commit<SURF>(p, rep, cand, nc, step, ev, evcap, sh, done);
+    }
+  }
+  acc[3] += (unsigned long long)done;
+  __syncthreads();
+  // ---- products (appended after the sorted molecules) and candidate reset
+  const int ne = min(sh.nev, evcap);
+  int uni = 0;
+  for (int t = tid; t < ne; t += T) {
+    place_event<SURF>(p, ev[t], step, uni, [&](float4 npc, ull nid) {
+      const int k = ns + atomicAdd(&sh.np, 1);
+      if (k < cap) {
+        p.b_pc[off + k] = npc;
+        p.b_id[off + k] = nid;
+        atomicAdd((unsigned long long *)&p.spcount[rep * c_net.nsp + id_species(nid)], 1ull);
+      } else {
+        atomicOr(p.status, kStMolCap);
+      }
+    });
+  }
+  acc[2] += (unsigned long long)uni;
+  for (int t = tid; t < nc; t += T) p.best[cand[t]] = ~0ull;
+  __syncthreads();
+  return min(ns + sh.np, cap);
+}
+
+// pA: inputs in buffer P, outputs in the other; pB the reverse.  Step k of
+// the launch uses pA for even k.
+template <int SURF>
+__global__ void __launch_bounds__(kPersistThreads, SMOLB_PERSIST_BLOCKS) k_persist(KParams pA, KParams pB,
+                                                                                    PersistArgs q) {
+  extern __shared__ float s_gtab[];
+  __shared__ PersistShared sh;
+  __shared__ int s_rep;
+  const float *gtab = stage_gtab(pA, s_gtab);
+  const uint32_t step0 = *pA.step;
+  Event *ev = q.ev + (size_t)blockIdx.x * q.evslice;
+  int *cand = q.cand + (size_t)blockIdx.x * q.candslice;
+  unsigned long long acc[6] = {0, 0, 0, 0, 0, 0};
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_rep = atomicAdd(q.queue, 1);
+    __syncthreads();
+    const int t = s_rep;
+    if (t >= q.nrep) break;
+    const int rep = q.order[t];
+    const int off = q.roff[rep], cap = q.rcap[rep];
+    int n = q.rn[rep];
+    for (int k = 0; k < q.nsteps; k += 2) {
+      n = persist_step<SURF>(pA, rep, off, cap, n, step0 + 1 + k, gtab, ev, q.evslice, cand, q.candslice, sh, acc);
+      if (k + 1 < q.nsteps)
+        n = persist_step<SURF>(pB, rep, off, cap, n, step0 + 2 + k, gtab, ev, q.evslice, cand, q.candslice, sh,
+                               acc);
+    }
+    if (threadIdx.x == 0) q.rn[rep] = n;
+  }
+  for (int k = 0; k < 6; ++k)
+    if (acc[k]) atomicAdd(&pA.counters[k], acc[k]);
+}
+
+__global__ void k_bump_step(uint32_t *step, int by) { *step += (uint32_t)by; }
+
+// First entry of every replicate's molecules in the box-sorted buffer
+// (lo[r] = start of its first box; lo[R] = total).
+__global__ void k_rep_ranges(const int *start, const DevGeo *geo, int R, int ncell, int *lo) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r <= R; r += gridDim.x * blockDim.x)
+    lo[r] = (r < R) ? start[geo[r].cell0] : start[ncell];
+}
+
+// Copy replicate ranges between layouts: n[r] entries from src + soff[r] to
+// dst + doff[r] (one block per replicate, grid-stride over replicates).
+__global__ void k_copy_ranges(const float4 *spc, const ull *sid, const int *soff, const int *n, const int *doff,
+                              int R, float4 *dpc, ull *did) {
+  for (int r = blockIdx.x; r < R; r += gridDim.x) {
+    const int a = soff[r], b = doff[r], m = n[r];
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+      dpc[b + i] = spc[a + i];
+      did[b + i] = sid[a + i];
+    }
+  }
 }
 
 // Upload conversion for one replicate: absolute FP64 positions to box-local
@@ -2035,6 +2348,26 @@ class EngineImpl {
   int inj_n = 0;
   bool inj_pending = false;
 
+  // persistent ensemble engine (k_persist): its own molecule layout, one
+  // region per replicate; the step pipeline's buffers are refilled from it
+  // (leave_persist) before anything else reads molecules
+  int persist_mode = 0;       // 0: step pipeline only; 1: persistent kernel when the configuration allows
+  bool in_persist = false;    // molecules currently held in the persistent layout
+  int ppar = 0;               // persistent buffer holding the current state
+  long long qtotal = 0;       // entries allocated in each persistent buffer
+  int qcells = 0;             // box entries allocated (cells + one spare per replicate)
+  float4 *d_qpc[2] = {nullptr, nullptr}, *d_qtmp = nullptr;
+  ull *d_qid[2] = {nullptr, nullptr}, *d_qbest = nullptr;
+  int *d_qcnt = nullptr, *d_qstart = nullptr;
+  DevGeo *d_qgeo = nullptr;
+  int *d_qint = nullptr;      // order[R] | off[R] | cap[R] | n[R] | queue | big
+  Event *d_qev = nullptr;
+  int *d_qcand = nullptr;
+  int qgrid = 0, qevslice = 0, qcandslice = 0, qmaxcap = 0;
+  std::vector<int> h_qoff, h_qcap;
+  cudaGraphExec_t qgraph[2] = {nullptr, nullptr};  // one launch block of qgraph_steps steps, per start parity
+  int qgraph_steps = 0;
+
   ~EngineImpl() {
     release();
     for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
@@ -2114,8 +2447,30 @@ class EngineImpl {
     d_msdpart = nullptr;
   }
 
+  void persist_free() {
+    for (int k = 0; k < 2; ++k) {
+      if (qgraph[k]) cudaGraphExecDestroy(qgraph[k]);
+      qgraph[k] = nullptr;
+    }
+    void *ptrs[] = {d_qpc[0], d_qpc[1], d_qtmp, d_qid[0], d_qid[1], d_qbest, d_qcnt, d_qstart, d_qgeo, d_qint,
+                    d_qev, d_qcand};
+    for (void *q : ptrs)
+      if (q) cudaFree(q);
+    d_qpc[0] = d_qpc[1] = d_qtmp = nullptr;
+    d_qid[0] = d_qid[1] = d_qbest = nullptr;
+    d_qcnt = d_qstart = d_qint = d_qcand = nullptr;
+    d_qgeo = nullptr;
+    d_qev = nullptr;
+    qtotal = 0;
+    qcells = 0;
+    qgrid = 0;
+    qmaxcap = 0;
+    in_persist = false;
+  }
+
   void release() {
     invalidate_graph();
+    persist_free();
     msd_free();
     tail_free();
     if (d_upload) cudaFree(d_upload);
@@ -2615,6 +2970,228 @@ class EngineImpl {
     return capture_steps(0, 1, &graph2, err);
   }
 
+  // The persistent kernel covers ensembles without surfaces, compartments or
+  // injected displacements (the general surface form stays on the pipeline).
+  bool persist_eligible() const {
+    return persist_mode != 0 && dnet.npanel == 0 && dnet.ncmpt == 0 && !dnet.inject && msd.empty();
+  }
+
+  // Persistent-kernel params: a = buffer `in`, b = the other.
+  KParams persist_params(int in) const {
+    KParams p = params(0);
+    p.geo = d_qgeo;
+    p.a_pc = d_qpc[in];
+    p.a_id = d_qid[in];
+    p.b_pc = d_qpc[1 - in];
+    p.b_id = d_qid[1 - in];
+    p.b_n = d_qint + 4 * reps.size() + 1;  // a large count: box starts bound the searches
+    p.tmp = d_qtmp;
+    p.cnt = d_qcnt;
+    p.start = d_qstart;
+    p.best = d_qbest;
+    return p;
+  }
+
+  // Move the state into the persistent layout: one rebin pass merges the
+  // pending products and sorts every replicate into a contiguous range, then
+  // each range is copied into its replicate's region (regions hold twice the
+  // replicate's molecules plus 256, processing order largest first).
+  int enter_persist(std::string *err) {
+    const int R = (int)reps.size();
+    CK(cudaMemsetAsync(d_cnt, 0, ((size_t)ncell + 1) * sizeof(int), stream));
+    enqueue_step(parity, true);
+    parity ^= 1;
+    int *d_lo = nullptr;
+    CK(cudaMalloc(&d_lo, (size_t)(R + 1) * sizeof(int)));
+    k_rep_ranges<<<(R + 256) / 256, 256, 0, stream>>>(d_start, d_geo, R, ncell, d_lo);
+    std::vector<int> lo((size_t)R + 1);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(lo.data(), d_lo, lo.size() * sizeof(int), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+      cudaFree(d_lo);
+      if (err) *err = std::string("persistent layout: ") + cudaGetErrorString(e);
+      return -8;
+    }
+    std::vector<int> n((size_t)R), order((size_t)R);
+    h_qoff.assign(R, 0);
+    h_qcap.assign(R, 0);
+    long long total = 0;
+    int maxcap = 0;
+    for (int r = 0; r < R; ++r) {
+      n[r] = lo[r + 1] - lo[r];
+      const long long c = 2ll * n[r] + 256;
+      h_qoff[r] = (int)total;
+      h_qcap[r] = (int)c;
+      total += c;
+      maxcap = std::max(maxcap, (int)c);
+    }
+    if (total > (1ll << 31) - 2) { cudaFree(d_lo); if (err) *err = "persistent layout too large"; return -9; }
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return n[a] > n[b]; });
+    // buffers (grow only)
+    const int cells = ncell + R + 1;
+    if (total > qtotal || cells > qcells || maxcap > qmaxcap || !d_qgeo) {
+      persist_free();
+      for (int k = 0; k < 2; ++k) {
+        CK(cudaMalloc(&d_qpc[k], (size_t)total * sizeof(float4)));
+        CK(cudaMalloc(&d_qid[k], (size_t)total * sizeof(ull)));
+      }
+      CK(cudaMalloc(&d_qtmp, (size_t)total * sizeof(float4)));
+      CK(cudaMalloc(&d_qbest, (size_t)total * sizeof(ull)));
+      CK(cudaMemsetAsync(d_qbest, 0xFF, (size_t)total * sizeof(ull), stream));
+      CK(cudaMalloc(&d_qcnt, (size_t)cells * sizeof(int)));
+      CK(cudaMalloc(&d_qstart, (size_t)cells * sizeof(int)));
+      CK(cudaMalloc(&d_qgeo, (size_t)R * sizeof(DevGeo)));
+      CK(cudaMalloc(&d_qint, (4 * (size_t)R + 2) * sizeof(int)));
+      qtotal = total;
+      qcells = cells;
+      qmaxcap = maxcap;
+      // CTAs: as many as stay resident (one wave), at most one per replicate
+      int per_sm = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persist<0>, kPersistThreads, adv_smem());
+      qgrid = std::max(1, std::min(R, sm_count() * std::max(1, per_sm)));
+      qevslice = std::max(1024, maxcap / 8);
+      qcandslice = std::max(1024, maxcap / 4);
+      CK(cudaMalloc(&d_qev, (size_t)qgrid * qevslice * sizeof(Event)));
+      CK(cudaMalloc(&d_qcand, (size_t)qgrid * qcandslice * sizeof(int)));
+    }
+    CK(cudaMemsetAsync(d_qcnt, 0, (size_t)qcells * sizeof(int), stream));
+    std::vector<DevGeo> g2 = geo;
+    for (int r = 0; r < R; ++r) g2[r].cell0 += r;  // one spare box entry per replicate
+    std::vector<int> ints(4 * (size_t)R + 2);
+    for (int r = 0; r < R; ++r) {
+      ints[r] = order[r];
+      ints[R + r] = h_qoff[r];
+      ints[2 * R + r] = h_qcap[r];
+      ints[3 * R + r] = n[r];
+    }
+    ints[4 * R] = 0;
+    ints[4 * R + 1] = 0x7FFFFFFF;
+    CK(cudaMemcpyAsync(d_qgeo, g2.data(), g2.size() * sizeof(DevGeo), cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(d_qint, ints.data(), ints.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+    k_copy_ranges<<<std::min(R, sm_count() * 8), 256, 0, stream>>>(d_pc[parity], d_id[parity], d_lo, d_qint + 3 * R,
+                                                                   d_qint + R, R, d_qpc[0], d_qid[0]);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    cudaFree(d_lo);
+    if (e != cudaSuccess) { if (err) *err = std::string("persistent layout: ") + cudaGetErrorString(e); return -8; }
+    nlaunch += 2;
+    ppar = 0;
+    in_persist = true;
+    return 0;
+  }
+
+  // Back to the step pipeline's layout: every replicate's entries are
+  // gathered into the staging buffer and rebinned (dead entries drop out).
+  int leave_persist(std::string *err) {
+    if (!in_persist) return 0;
+    const int R = (int)reps.size();
+    std::vector<int> n((size_t)R);
+    CK(cudaMemcpyAsync(n.data(), d_qint + 3 * R, (size_t)R * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    std::vector<int> soff((size_t)R);
+    long long total = 0;
+    for (int r = 0; r < R; ++r) {
+      soff[r] = (int)total;
+      total += n[r];
+    }
+    if (total > cap) { if (err) *err = "more molecules than the engine capacity"; return -9; }
+    if (total > pcap) {  // the staging (product) buffers take the gathered molecules
+      for (int k = 0; k < 2; ++k) {
+        cudaFree(d_ppc[k]);
+        cudaFree(d_pid[k]);
+        d_ppc[k] = nullptr;
+        d_pid[k] = nullptr;
+      }
+      pcap = total;
+      for (int k = 0; k < 2; ++k) {
+        CK(cudaMalloc(&d_ppc[k], pcap * sizeof(float4)));
+        CK(cudaMalloc(&d_pid[k], pcap * sizeof(ull)));
+      }
+      cudaFree(d_tmp);
+      d_tmp = nullptr;
+      CK(cudaMalloc(&d_tmp, (cap + pcap) * sizeof(float4)));
+      invalidate_graph();
+    }
+    int *d_soff = nullptr;
+    CK(cudaMalloc(&d_soff, (size_t)R * sizeof(int)));
+    CK(cudaMemcpyAsync(d_soff, soff.data(), soff.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+    k_copy_ranges<<<std::min(R, sm_count() * 8), 256, 0, stream>>>(d_qpc[ppar], d_qid[ppar], d_qint + R,
+                                                                   d_qint + 3 * R, d_soff, R, d_ppc[0], d_pid[0]);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    cudaFree(d_soff);
+    if (e != cudaSuccess) { if (err) *err = std::string("persistent layout: ") + cudaGetErrorString(e); return -8; }
+    ++nlaunch;
+    in_persist = false;
+    // the sorted and product counts of the pipeline's buffers are stale
+    CK(cudaMemsetAsync(d_counts, 0, 4 * sizeof(int), stream));
+    // finish_upload recounts species from scratch, which equals the kept counts
+    const long long keep_gen = upload_gen;
+    const int rc = finish_upload(total, err);
+    upload_gen = keep_gen;
+    return rc;
+  }
+
+  // nsteps steps of every replicate through k_persist, in launches of at
+  // most 100 steps; each launch (work-counter reset, kernel, step-counter
+  // bump) is one replay of a captured graph.
+  int run_persist(long long nsteps, std::string *err) {
+    if (!in_persist) {
+      int rc = enter_persist(err);
+      if (rc) return rc;
+    }
+    const int R = (int)reps.size();
+    long long left = nsteps;
+    while (left > 0) {
+      const int K = (int)std::min<long long>(left, 100);
+      auto enqueue = [&](int in) {
+        PersistArgs q;
+        q.order = d_qint;
+        q.roff = d_qint + R;
+        q.rcap = d_qint + 2 * R;
+        q.rn = d_qint + 3 * R;
+        q.queue = d_qint + 4 * R;
+        q.ev = d_qev;
+        q.evslice = qevslice;
+        q.cand = d_qcand;
+        q.candslice = qcandslice;
+        q.nrep = R;
+        q.nsteps = K;
+        cudaMemsetAsync(q.queue, 0, sizeof(int), stream);
+        k_persist<0><<<qgrid, kPersistThreads, adv_smem(), stream>>>(persist_params(in), persist_params(1 - in), q);
+        k_bump_step<<<1, 1, 0, stream>>>(d_step, K);
+      };
+      if (use_graph) {
+        if (K != qgraph_steps) {
+          for (int k = 0; k < 2; ++k) {
+            if (qgraph[k]) cudaGraphExecDestroy(qgraph[k]);
+            qgraph[k] = nullptr;
+          }
+          qgraph_steps = K;
+        }
+        if (!qgraph[ppar]) {
+          cudaGraph_t g = nullptr;
+          CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+          enqueue(ppar);
+          CK(cudaStreamEndCapture(stream, &g));
+          cudaError_t e = cudaGraphInstantiate(&qgraph[ppar], g, 0);
+          cudaGraphDestroy(g);
+          if (e != cudaSuccess) { qgraph[ppar] = nullptr; if (err) *err = std::string("persistent graph: ") + cudaGetErrorString(e); return -8; }
+        }
+        CK(cudaGraphLaunch(qgraph[ppar], stream));
+      } else {
+        enqueue(ppar);
+      }
+      nlaunch += 2;
+      ppar ^= (K & 1);
+      left -= K;
+    }
+    CK(cudaGetLastError());
+    return 0;
+  }
+
   // One step of the current parity through its single-step graph.
   int run_one(std::string *err) {
     if (!graph1[parity]) {
@@ -2859,6 +3436,7 @@ int Engine::update_reps(const std::vector<RepSpec> &reps, std::string *err) {
 int Engine::set_molecules(long long n, const double *pos, const int *species, const int *rep,
                           const uint64_t *serno, std::string *err) {
   EngineImpl &E = *impl_;
+  E.in_persist = false;  // replaced wholesale
   if (n > E.pcap) {
     // grow the product buffers so the upload fits (they are the upload staging area)
     for (int k = 0; k < 2; ++k) {
@@ -2926,6 +3504,19 @@ int Engine::set_molecules(long long n, const double *pos, const int *species, co
 int Engine::run(long long nsteps, std::string *err) {
   EngineImpl &E = *impl_;
   if (nsteps <= 0) return 0;
+  if (E.persist_eligible()) {
+    E.tail_slot = -1;
+    int rc = E.run_persist(nsteps, err);
+    if (rc) return rc;
+    E.nsteps += nsteps;
+    E.tail_step = E.nsteps;
+    E.tail_gen = E.upload_gen;
+    return 0;
+  }
+  if (E.in_persist) {
+    int rc = E.leave_persist(err);
+    if (rc) return rc;
+  }
   const bool inj = E.dnet.inject != 0;
   if (inj) {
     if (nsteps != 1) { if (err) *err = "injected displacements apply to one step"; return -6; }
@@ -3072,6 +3663,7 @@ int Engine::stats(EngineStats *s, std::string *err) {
 int Engine::get_molecules(std::vector<double> *pos, std::vector<int> *species, std::vector<int> *rep,
                           std::vector<uint64_t> *serno, std::string *err) {
   EngineImpl &E = *impl_;
+  if (int rc = E.leave_persist(err)) return rc;
   int c[4];
   CK(cudaStreamSynchronize(E.stream));
   CK(cudaMemcpy(c, E.d_counts, sizeof(c), cudaMemcpyDeviceToHost));
@@ -3125,6 +3717,7 @@ int Engine::get_molecules(std::vector<double> *pos, std::vector<int> *species, s
 int Engine::set_injection(long long n, const uint64_t *sernos, const double *disp, int rep,
                           std::string *err) {
   EngineImpl &E = *impl_;
+  if (int rc = E.leave_persist(err)) return rc;
   if (E.d_injkey) { cudaFree(E.d_injkey); E.d_injkey = nullptr; }
   if (E.d_injval) { cudaFree(E.d_injval); E.d_injval = nullptr; }
   E.inj_n = 0;
@@ -3165,6 +3758,7 @@ int Engine::set_rng_step(uint64_t step, std::string *err) {
 int Engine::msd_track(int species, long long m, const uint64_t *keys, const double *start, const double *last,
                       std::string *err) {
   EngineImpl &E = *impl_;
+  if (int rc = E.leave_persist(err)) return rc;
   if (species <= 0 || species >= E.net.nspecies) {
     if (err) *err = "species index out of range";
     return -6;
@@ -3210,6 +3804,7 @@ int Engine::msd_track(int species, long long m, const uint64_t *keys, const doub
 
 int Engine::msd_update(int handle, int msddim, double *sum2, double *sum4, long long *count, std::string *err) {
   EngineImpl &E = *impl_;
+  if (int rc = E.leave_persist(err)) return rc;
   if (handle < 0 || handle >= (int)E.msd.size()) {
     if (err) *err = "no such tracker";
     return -6;
@@ -3254,6 +3849,7 @@ int Engine::msd_count() const { return (int)impl_->msd.size(); }
 
 int Engine::cmpt_counts(int c, std::vector<long long> *out, std::string *err) {
   EngineImpl &E = *impl_;
+  if (int rc = E.leave_persist(err)) return rc;
   if (c < 0 || c >= (int)E.cmpts.size()) {
     if (err) *err = "no such compartment";
     return -6;
@@ -3287,6 +3883,7 @@ int Engine::cmpt_counts(int c, std::vector<long long> *out, std::string *err) {
 int Engine::profile(long long nsteps, std::vector<std::string> *names, std::vector<double> *ms,
                     std::vector<long long> *launches, std::string *err) {
   EngineImpl &E = *impl_;
+  if (int rc = E.leave_persist(err)) return rc;
   names->clear();
   ms->clear();
   launches->clear();
@@ -3328,6 +3925,16 @@ void Engine::set_stream(void *stream) {
 void *Engine::stream() const { return (void *)impl_->stream; }
 long long Engine::launches() const { return impl_->nlaunch; }
 long long Engine::steps_done() const { return impl_->nsteps; }
+int Engine::set_persistent(int mode, std::string *err) {
+  EngineImpl &E = *impl_;
+  if (mode < 0 || mode > 1) { if (err) *err = "persistent mode must be 0 or 1"; return -6; }
+  if (!mode && E.in_persist) {
+    if (int rc = E.leave_persist(err)) return rc;
+  }
+  E.persist_mode = mode;
+  return 0;
+}
+bool Engine::persistent_active() const { return impl_->persist_eligible(); }
 void Engine::set_use_graph(bool on) {
   impl_->use_graph = on;
   if (!on) impl_->invalidate_graph();

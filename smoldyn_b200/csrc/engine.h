@@ -148,6 +148,12 @@ class Engine {
   // step + 1).  A simulation that rebuilds its engine mid-run sets it to the
   // steps already taken, so that no molecule replays earlier random numbers.
   int set_rng_step(uint64_t step, std::string *err);
+  // Persistent ensemble kernel (mode 1): replicates are stepped by one CTA
+  // each for blocks of up to 100 steps per launch, when the configuration
+  // has no surfaces, compartments or injected displacements; mode 0 keeps
+  // the step pipeline.  persistent_active() tells which one run() uses.
+  int set_persistent(int mode, std::string *err);
+  bool persistent_active() const;
   // Capture the 2-step kernel sequence in a CUDA graph and replay it (on by default).
   void set_use_graph(bool on);
   // Launch shape (kept across init); a change re-captures the step graph.

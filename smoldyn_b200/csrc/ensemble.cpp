@@ -44,6 +44,7 @@ struct smolb_ens {
   long long surrogate_fallbacks = 0;
   std::unique_ptr<smolb::Surrogate> sur;
   smolb::LaunchTuning tuning;  // kernel launch shape (autotuner)
+  int engine_mode = 0;         // 0 persistent kernel when the configuration allows, 1 step pipeline, 2 persistent only
 };
 
 // process-global error record of the C API (api.cpp)
@@ -208,7 +209,12 @@ int build(smolb_ens &e, std::string *err) {
   e.eng.reset(new smolb::Engine());
   rc = e.eng->init(e.net, e.reps, T.dt, (uint64_t)T.seed, cap, err);
   if (!rc) rc = e.eng->set_tuning(e.tuning, err);
+  if (!rc) rc = e.eng->set_persistent(e.engine_mode == 1 ? 0 : 1, err);
   if (rc) return rc;
+  if (e.engine_mode == 2 && !e.eng->persistent_active()) {
+    *err = "the persistent kernel does not cover surfaces, compartments or injected displacements";
+    return -6;
+  }
   std::vector<double> pos;
   std::vector<int> sp, rep;
   pos.reserve(3 * total);
@@ -301,6 +307,25 @@ enum ErrorCode smolgpuEnsembleSetRadiusMode(ensptr ens, int mode) {
   return ECok;
 }
 
+enum ErrorCode smolgpuEnsembleSetEngine(ensptr ens, int mode) {
+  ECHECK(ens, ECmissing, "missing ensemble");
+  ECHECK(mode >= 0 && mode <= 2, ECbounds, "mode must be 0, 1 or 2");
+  ens->engine_mode = mode;
+  if (ens->eng) {
+    std::string err;
+    if (ens->eng->set_persistent(mode == 1 ? 0 : 1, &err)) return ens_error(__func__, ECerror, err);
+    ECHECK(mode != 2 || ens->eng->persistent_active(), ECerror,
+           "the persistent kernel does not cover surfaces, compartments or injected displacements");
+  }
+  return ECok;
+}
+
+int smolgpuEnsembleGetEngine(ensptr ens) {
+  if (!ens) return (int)ens_error(__func__, ECmissing, "missing ensemble");
+  if (!ens->eng) return ens->engine_mode == 1 ? 1 : 2;
+  return ens->eng->persistent_active() ? 2 : 1;
+}
+
 enum ErrorCode smolgpuEnsembleUpdate(ensptr ens) {
   ECHECK(ens, ECmissing, "missing ensemble");
   std::string err;
@@ -327,6 +352,25 @@ enum ErrorCode smolgpuEnsembleGetCounts(ensptr ens, long long *counts) {
   std::string err;
   if (ens->eng->species_counts(&c, &err)) return ens_error(__func__, ECerror, err);
   memcpy(counts, c.data(), c.size() * sizeof(long long));
+  return ECok;
+}
+
+enum ErrorCode smolgpuEnsembleGetMolecules(ensptr ens, long long *n, double *pos, int *species, int *rep,
+                                           uint64_t *serno) {
+  ECHECK(ens && n, ECmissing, "missing argument");
+  ECHECK(ens->eng, ECerror, "ensemble not built");
+  std::vector<double> p;
+  std::vector<int> sp, rp;
+  std::vector<uint64_t> sn;
+  std::string err;
+  if (ens->eng->get_molecules(&p, &sp, &rp, &sn, &err)) return ens_error(__func__, ECerror, err);
+  const long long cnt = (long long)sp.size();
+  ECHECK(*n >= cnt || (!pos && !species && !rep && !serno), ECbounds, "buffer too small");
+  *n = cnt;
+  if (pos) memcpy(pos, p.data(), p.size() * sizeof(double));
+  if (species) memcpy(species, sp.data(), sp.size() * sizeof(int));
+  if (rep) memcpy(rep, rp.data(), rp.size() * sizeof(int));
+  if (serno) memcpy(serno, sn.data(), sn.size() * sizeof(uint64_t));
   return ECok;
 }
 

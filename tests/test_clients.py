@@ -10,11 +10,14 @@
    calls), compiled unchanged against include/libsmoldyn.h and this library
    (oracle/_ref/testcode_b200), and against the reference library
    (oracle/_ref/testcode_ref); `make -C oracle client` builds both where the
-   reference sources are present.  On the GPU the b200 build must run to
-   completion and print the same 19 report lines; its counts are compared
-   with 24 runs of the reference build at every report time (the system sits
-   at the Lotka-Volterra fixed point R = F = 1000 and drifts, so the check is
-   the reference's envelope widened by a factor of two).
+   reference sources are present.  On the GPU both builds must run to
+   completion and print the same 19 report lines.  The client fixes its
+   random seed, so one run of either build is one realisation of a
+   Lotka-Volterra system started at its fixed point (R = F = 1000), which
+   oscillates with a growing random amplitude; the b200 run's counts are
+   therefore compared with the envelope (widened by a factor of two) of 24
+   seeds of the same model written as a configuration file and run by the
+   reference binary.
 """
 import os
 import re
@@ -89,6 +92,28 @@ def test_integration_example_runs():
         assert m and int(m.group(1)) > 0, out.stdout[-2000:]
 
 
+LV_CONFIG = """dim 3
+species rabbit fox
+difc rabbit 100
+difc fox 100
+boundaries 0 -100 100 p
+boundaries 1 -100 100 p
+boundaries 2 -10 10 p
+time_start 0
+time_stop 2
+time_step 0.001
+random_seed %d
+reaction r1 rabbit -> rabbit + rabbit 10
+reaction r2 rabbit + fox -> fox + fox 8000
+reaction r3 fox -> 0 10
+mol 1000 rabbit u u u
+mol 1000 fox u u u
+output_files o.txt
+cmd N 100 molcount o.txt
+end_file
+"""
+
+
 @pytest.mark.gpu
 def test_reference_client_runs_on_b200():
     if not (os.path.exists(B200_CLIENT) and os.path.exists(REF_CLIENT)):
@@ -98,18 +123,25 @@ def test_reference_client_runs_on_b200():
     gpu = parse_report(run.stdout)
     assert gpu.shape == (19, 3), run.stdout[-2000:]
 
-    def ref_once(k):
-        with tempfile.TemporaryDirectory() as d:
-            r = subprocess.run([REF_CLIENT], capture_output=True, text=True, timeout=600, cwd=d,
-                               env=dict(os.environ, SMOLDYN_NO_PROMPT="1"))
-            assert r.returncode == 0
-            return parse_report(r.stdout)
+    with tempfile.TemporaryDirectory() as d:
+        r = subprocess.run([REF_CLIENT], capture_output=True, text=True, timeout=600, cwd=d,
+                           env=dict(os.environ, SMOLDYN_NO_PROMPT="1"))
+    assert r.returncode == 0
+    assert parse_report(r.stdout).shape == (19, 3)
+    ref_exe = os.path.join(oracle_lib.REF_DIR, "smoldyn")
 
-    with ThreadPoolExecutor(max_workers=max(1, min(24, os.cpu_count() or 1))) as ex:
-        refs = [r for r in ex.map(ref_once, range(24))]
-    refs = [r for r in refs if r.shape == (19, 3)]
-    assert len(refs) >= 20
-    R = np.stack(refs)  # [run, time, (t, rabbit, fox)]
+    def ref_seed(seed):
+        with tempfile.TemporaryDirectory() as d:
+            with open(os.path.join(d, "lv.txt"), "w") as f:
+                f.write(LV_CONFIG % seed)
+            subprocess.run([ref_exe, "lv.txt", "-qt"], cwd=d, check=True, stdin=subprocess.DEVNULL,
+                           stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+                           env=dict(os.environ, SMOLDYN_NO_PROMPT="1"), timeout=1200)
+            rows = np.array([[float(x) for x in ln.split()] for ln in open(os.path.join(d, "o.txt")) if ln.strip()])
+        return rows[1:20]  # t = 0.1 .. 1.9, the client's report times
+
+    with ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
+        R = np.stack(list(ex.map(ref_seed, range(1, 25))))  # [seed, time, (t, rabbit, fox)]
     assert np.allclose(gpu[:, 0], R[0, :, 0])
     for col in (1, 2):
         lo = R[:, :, col].min(axis=0) * 0.5
