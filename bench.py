@@ -253,6 +253,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-batched", action="store_true", help="skip the ensemble and surrogate workloads")
     ap.add_argument("--no-tune", action="store_true", help="default launch shape and box width (no autotuner)")
+    ap.add_argument("--batched-steps", type=int, default=2000, help="steps of the 4096-replicate ensemble leg")
+    ap.add_argument("--surrogate-steps", type=int, default=5000,
+                    help="steps of the 65,536-replicate surrogate sweep (rates redrawn every 100)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -412,7 +415,9 @@ def time_on_stream(torch, stream, fn):
 def run_batched(sb, torch, args, rank):
     """Ensemble workload: 4096 replicates, N log-uniform in [1e2, 1e5] at
     density 0.01, kf and kr log-uniform in [1e-3, 1] per replicate, radii from
-    the exact FP64 solver on the device, dt = 0.01."""
+    the exact FP64 solver on the device, dt = 0.01, 2000 steps (the
+    configuration's count; fewer with --batched-steps).  Stepped by the
+    persistent ensemble kernel, with the step pipeline timed beside it."""
     rng = np.random.default_rng(12345 + rank)
     R = 4096
     n, side = draw_replicates(rng, R, 1e2, 1e5)
@@ -428,32 +433,41 @@ def run_batched(sb, torch, args, rank):
     e.radius_mode(1)
     t0 = time.perf_counter()
     e.update()
-    t_tune = time.perf_counter()
-    tune_ms = e.autotune(10) if not args.no_tune else None
-    t_tune = time.perf_counter() - t_tune
     setup = time.perf_counter() - t0
     stream = torch.cuda.Stream()
     e.set_stream(stream.cuda_stream)
     e.run_steps(args.warmup)
-    steps = max(10, args.steps)
+    steps = args.batched_steps
     l0 = e.launches()
     sec = time_on_stream(torch, stream, lambda: e.run_steps(steps))
+    launches = int(e.launches() - l0)
+    engine = {1: "step pipeline", 2: "persistent"}.get(e.engine(), "?")
     tot = float(n.sum())
+    ev = e.events()
+    # the same ensemble on the step pipeline, fewer steps (per-step cost is flat)
+    e.engine(1)
+    e.run_steps(args.warmup)
+    psteps = min(steps, 100)
+    psec = time_on_stream(torch, stream, lambda: e.run_steps(psteps))
     out = {"workload": "4096 replicates, N log-uniform [1e2,1e5] at density 0.01, kf,kr log-uniform [1e-3,1], "
                        "reflective cubes, A+B<->C, dt=0.01, radii by the device FP64 solver",
-           "value": tot * steps / sec, "unit": METRIC, "molecules": int(tot), "replicates": R, "steps": steps,
-           "ms_per_step": sec * 1e3 / steps, "setup_s": setup, "gpu_launches": int(e.launches() - l0),
-           "tuning": e.tuning(), "autotune_s": t_tune, "autotune_best_trial_ms": tune_ms}
+           "engine": engine, "value": tot * steps / sec, "unit": METRIC, "molecules": int(tot), "replicates": R,
+           "steps": steps, "ms_per_step": sec * 1e3 / steps, "setup_s": setup, "gpu_launches": launches,
+           "events": {"rxn1": ev[2], "rxn2": ev[3], "overflow": ev[6]},
+           "step_pipeline": {"value": tot * psteps / psec, "steps": psteps, "ms_per_step": psec * 1e3 / psteps}}
+    out["persistent_vs_pipeline"] = out["value"] / out["step_pipeline"]["value"]
     e.close()
     return out
 
 
 def run_surrogate(sb, torch, args, rank):
     """Surrogate sweep: 65,536 replicates, N log-uniform in [1e2, 1e4] at
-    density 0.01, rates redrawn every 100 steps; radii from the MLP surrogate
-    (exact fallback above 1e-3 estimated rate error).  Compared with the same
-    ensemble on the exact device solver and with the plain form (each
-    replicate its own simulation) on a sample of replicates."""
+    density 0.01, rates redrawn every 100 steps over 5000 steps (fewer with
+    --surrogate-steps); radii from the MLP surrogate (exact fallback above
+    1e-3 estimated rate error).  Compared with the plain form (each replicate
+    its own simulation) on a sample of replicates; the solvers are timed
+    alone on the sweep's 65,536 radius problems; the measured rate-constant
+    error is taken over independent seeds."""
     rng = np.random.default_rng(777 + rank)
     R = 65536
     n, side = draw_replicates(rng, R, 1e2, 1e4)
@@ -479,18 +493,22 @@ def run_surrogate(sb, torch, args, rank):
     stream = torch.cuda.Stream()
     e.set_stream(stream.cuda_stream)
     e.run_steps(args.warmup)
-    steps = 200
+    steps = max(100, args.surrogate_steps // 100 * 100)
     fb = []
+    upd = []
 
     def work():
         for blk in range(steps // 100):
             redraw()
+            t1 = time.perf_counter()
             e.update()
+            upd.append(time.perf_counter() - t1)
             fb.append(e.fallbacks())
             e.run_steps(100)
 
     sec = time_on_stream(torch, stream, work)
     tot = float(n.sum())
+    engine = {1: "step pipeline", 2: "persistent"}.get(e.engine(), "?")
     # solver cost of one redraw: surrogate vs exact device vs exact host
     solver = {}
     for mode, name in ((2, "surrogate"), (1, "exact_device"), (0, "exact_host")):
@@ -502,11 +520,13 @@ def run_surrogate(sb, torch, args, rank):
     out = {"workload": "65536 replicates, N log-uniform [1e2,1e4] at density 0.01, A+B<->C with unbinding ratio "
                        "%.1f, kf,kr log-uniform [1e-3,1] redrawn every 100 steps, dt=0.01, radii from the MLP "
                        "surrogate with exact fallback" % rho,
-           "value": tot * steps / sec, "unit": METRIC, "molecules": int(tot), "replicates": R, "steps": steps,
-           "ms_per_step": sec * 1e3 / steps, "setup_s": setup, "surrogate_train_s": train_s,
-           "surrogate_loss": loss, "fallbacks_per_redraw": fb, "fallback_fraction": float(np.mean(fb)) / R,
-           "update_seconds": solver}
+           "engine": engine, "value": tot * steps / sec, "unit": METRIC, "molecules": int(tot), "replicates": R,
+           "steps": steps, "redraws": len(fb), "ms_per_step": sec * 1e3 / steps, "setup_s": setup,
+           "redraw_update_s_mean": float(np.mean(upd)), "surrogate_train_s": train_s,
+           "surrogate_loss": loss, "fallbacks_per_redraw_mean": float(np.mean(fb)),
+           "fallback_fraction": float(np.mean(fb)) / R, "update_seconds": solver}
     e.close()
+    out["solver_throughput"] = solver_throughput(sb, sur, rng, R, rho)
     # plain form: sampled replicates run one at a time as ordinary simulations
     idx = rng.choice(R, 24, replace=False)
     mol_steps, secs = 0.0, 0.0
@@ -536,18 +556,54 @@ def run_surrogate(sb, torch, args, rank):
     return out
 
 
-def surrogate_rate_check(sb, sur, rng, R=4096, steps=200):
+def solver_throughput(sb, sur, rng, R, rho, dt=DT):
+    """Radius solves per second on the sweep's problem set (R binding radii
+    of A+B with unbinding ratio rho, kf log-uniform [1e-3, 1], D_A + D_B = 2):
+    the MLP surrogate with its secant correction and exact fallback
+    (smolgpuSurrogatePairRadii) against the exact FP64 device solver
+    (smolgpuSolveRadii, doubling plus 15 bisections per problem), each call
+    timed alone (host arrays in and out, best of 5)."""
+    kf = 10 ** rng.uniform(-3, 0, R)
+    ds = np.full(R, DIFC[0] + DIFC[1])
+    res = {}
+    best = 1e30
+    for _ in range(5):
+        t0 = time.perf_counter()
+        b_sur, _, nfb = sur.pair_radii(kf, ds, dt, same=0, rev=1, rparamt=sb.RPratio, rparam=rho)
+        best = min(best, time.perf_counter() - t0)
+    res["surrogate_solves_per_s"] = R / best
+    res["surrogate_fallbacks"] = int(nfb)
+    best = 1e30
+    for _ in range(5):
+        t0 = time.perf_counter()
+        b_ex = sb.solve_radii_device(0, kf, dt, ds, np.full(R, rho), rel=1)
+        best = min(best, time.perf_counter() - t0)
+    res["exact_device_solves_per_s"] = R / best
+    res["surrogate_vs_exact"] = res["surrogate_solves_per_s"] / res["exact_device_solves_per_s"]
+    res["max_radius_rel_diff"] = float(np.max(np.abs(b_sur / b_ex - 1)))
+    res["problems"] = R
+    return res
+
+
+def surrogate_rate_check(sb, sur, rng, R=65536, steps=500, every=25):
     """Measured rate-constant error of the surrogate radii against the exact
-    FP64 solver: the same 4096-replicate ensemble (same seed, rates and
-    molecules) runs once with surrogate radii and once with exact device radii;
-    the forward reaction events (C formed) are compared in aggregate and per
-    replicate."""
+    FP64 solver over independent seeds, at the sweep's configuration
+    (65,536 replicates, N log-uniform [1e2, 1e4], kf, kr log-uniform
+    [1e-3, 1], unbinding ratio 1.5): the ensemble runs once with surrogate
+    radii and once with exact device radii, each with its own seed and
+    molecule placement.  For each run the measured forward rate constant,
+    relative to each replicate's requested one, is
+        (forward events) / sum_r kf_r * integral A_r B_r / V_r dt
+    (counts sampled every 25 steps, trapezoid rule); the error is the
+    surrogate's ratio over the exact run's, with its Poisson standard error."""
     n, side = draw_replicates(rng, R, 1e2, 1e4)
     kf = 10 ** rng.uniform(-3, 0, R)
     kr = 10 ** rng.uniform(-3, 0, R)
+    vol = side ** 3
     res = {}
-    for mode in (2, 1):
+    for mode, seed in ((2, 101), (1, 202)):
         t = ensemble_template(sb, placement=(sb.RPratio, 1.5))
+        t.seed(seed)
         e = sb.Ensemble(t, R)
         e.set_boxes(np.zeros((R, 3)), np.repeat(side[:, None], 3, 1))
         e.set_rates("fwd", kf)
@@ -558,18 +614,27 @@ def surrogate_rate_check(sb, sur, rng, R=4096, steps=200):
             e.attach(sur)
         e.radius_mode(mode)
         e.update()
-        b, _ = e.reaction_params("fwd")
-        e.run_steps(steps)
-        res[mode] = (e.counts(4)[:, 3].astype(float), b)
+        ev0 = e.events()[3]
+        c = e.counts(4)
+        expo = np.zeros(R)
+        prev = c[:, 1].astype(float) * c[:, 2] / vol
+        for _ in range(steps // every):
+            e.run_steps(every)
+            c = e.counts(4)
+            cur = c[:, 1].astype(float) * c[:, 2] / vol
+            expo += 0.5 * (prev + cur) * every * DT
+            prev = cur
+        fwd = e.events()[3] - ev0
+        res[mode] = (float(fwd), float(np.sum(kf * expo)))
         e.close()
-    c_sur, b_sur = res[2]
-    c_ex, b_ex = res[1]
-    agg = abs(c_sur.sum() - c_ex.sum()) / max(c_ex.sum(), 1.0)
-    return {"replicates": R, "steps": steps, "C_formed_surrogate": float(c_sur.sum()),
-            "C_formed_exact": float(c_ex.sum()), "aggregate_rel_diff": agg,
-            "max_radius_rel_diff": float(np.max(np.abs(b_sur / b_ex - 1))),
-            "note": "same seed and molecules; events differ only where a pair sits within the radius difference "
-                    "of the binding radius"}
+    (f_s, x_s), (f_e, x_e) = res[2], res[1]
+    r_s, r_e = f_s / x_s, f_e / x_e
+    err = r_s / r_e - 1
+    se = np.sqrt(1 / max(f_s, 1) + 1 / max(f_e, 1))
+    return {"replicates": R, "steps": steps, "forward_events_surrogate": f_s, "forward_events_exact": f_e,
+            "measured_over_requested_surrogate": r_s, "measured_over_requested_exact": r_e,
+            "rate_constant_rel_error": err, "standard_error": se,
+            "note": "independent seeds and placements; forward events over the exposure sum kf*A*B/V dt"}
 
 
 SURF_CONFIG = """dim 3

@@ -342,6 +342,10 @@ int smolgpuEnsembleGetEngine(ensptr ens);
 enum ErrorCode smolgpuEnsembleUpdate(ensptr ens);
 enum ErrorCode smolgpuEnsembleRunSteps(ensptr ens, long long nsteps);
 enum ErrorCode smolgpuEnsembleGetCounts(ensptr ens, long long *counts);
+/* Event counters summed over the ensemble since it was built, as
+ * smolgpuGetEventCounts: wall hits, zeroth-, first- and second-order events,
+ * unresolved conflicts, extra candidates, status word. */
+enum ErrorCode smolgpuEnsembleGetEventCounts(ensptr ens, long long counts[8]);
 /* All molecules of all replicates, sorted by (replicate, serial number):
  * pos 3*n doubles (absolute coordinates of the replicate's box), species,
  * replicate index and serial number per molecule; *n is in: capacity, out:

@@ -133,6 +133,7 @@ PROTOTYPES = {
     "smolgpuEnsembleUpdate": (C.c_int, [_vp]),
     "smolgpuEnsembleSetEngine": (C.c_int, [_vp, C.c_int]),
     "smolgpuEnsembleGetEngine": (C.c_int, [_vp]),
+    "smolgpuEnsembleGetEventCounts": (C.c_int, [_vp, C.POINTER(C.c_longlong)]),
     "smolgpuEnsembleGetMolecules": (C.c_int, [_vp, C.POINTER(C.c_longlong), _dp, _ip, _ip, _u64p]),
     "smolgpuEnsembleRunSteps": (C.c_int, [_vp, C.c_longlong]),
     "smolgpuEnsembleGetCounts": (C.c_int, [_vp, C.POINTER(C.c_longlong)]),
@@ -445,6 +446,11 @@ class Ensemble:
 
     def run_steps(self, n):
         return check(self.lib.smolgpuEnsembleRunSteps(self.ptr, int(n)))
+
+    def events(self):
+        a = (C.c_longlong * 8)()
+        check(self.lib.smolgpuEnsembleGetEventCounts(self.ptr, a))
+        return list(a)
 
     def molecules(self):
         """(positions [n,3], species, replicate, serial) of every molecule."""

@@ -1075,8 +1075,12 @@ __device__ __forceinline__ int pair_reaction(const KParams &p, int rep, int spa,
 
 // Closest live partner of molecule i within its pair binding radii.
 // Returns packed (dist2 bits << 32 | index) or ~0 when none; *ncand counts candidates.
+// The box starts are read from st[c - base] for global box c: the step
+// pipeline passes its start array (base 0), the persistent kernel a
+// replicate's own table.
 template <int SURF>
-__device__ ull search_partner(const KParams &p, int i, float4 pc, ull id, uint32_t step, int &ncand) {
+__device__ ull search_partner_in(const KParams &p, int i, float4 pc, ull id, uint32_t step, int &ncand,
+                                 const int *st, int base) {
   const int nsorted = *p.b_n;
   const int sp = id_species(id);
   const int rep = id_rep(id);
@@ -1119,8 +1123,8 @@ __device__ ull search_partner(const KParams &p, int i, float4 pc, ull id, uint32
           if (!px) continue;
           x = (x < 0) ? x + g.n[0] : x - g.n[0];
         }
-        const int c = rowbase + x;
-        const int s = p.start[c], e = min(p.start[c + 1], nsorted);
+        const int c = rowbase + x - base;
+        const int s = st[c], e = min(st[c + 1], nsorted);
         for (int j = s; j < e; ++j) {
           if (j == i) continue;
           const ull jd = p.b_id[j];
@@ -1142,6 +1146,12 @@ __device__ ull search_partner(const KParams &p, int i, float4 pc, ull id, uint32
     }
   }
   return best;
+}
+
+template <int SURF>
+__device__ __forceinline__ ull search_partner(const KParams &p, int i, float4 pc, ull id, uint32_t step,
+                                              int &ncand) {
+  return search_partner_in<SURF>(p, i, pc, id, step, ncand, p.start, 0);
 }
 
 // Record candidate key k in best[x]; the first registration of x appends it
@@ -1800,6 +1810,9 @@ struct PersistArgs {
 };
 
 constexpr int kPersistThreads = 256;
+// Replicates with at most this many boxes keep their box counts and starts
+// in shared memory (32 KB); larger ones use their slice of the global arrays.
+constexpr int kPersistSmemBoxes = 4095;
 #ifndef SMOLB_PERSIST_BLOCKS
 #define SMOLB_PERSIST_BLOCKS 3
 #endif
@@ -1852,10 +1865,19 @@ __device__ __forceinline__ void persist_commit(const KParams &p, int rep, const 
 // One time step of replicate `rep` (entries [off, off+n) of p.a_*): returns
 // the entry count of its next state in p.b_*.  All threads of the block call
 // it; it begins and ends at a block barrier.
+// Box index of a packed cell within its replicate.
+__device__ __forceinline__ int local_cell(const DevGeo &g, uint32_t w) {
+  int ix, iy, iz;
+  unpack_cell(w, ix, iy, iz);
+  return (iz * g.n[1] + iy) * g.n[0] + ix;
+}
+
+// cnt / st: the replicate's box counts and starts, indexed by local box
+// (shared memory for small replicates); cnt is zero on entry and on exit.
 template <int SURF>
 __device__ __forceinline__ int persist_step(const KParams &p, int rep, int off, int cap, int n, uint32_t step,
                                             const float *gtab, Event *ev, int evcap, int *cand, int candcap,
-                                            PersistShared &sh, unsigned long long *acc) {
+                                            PersistShared &sh, unsigned long long *acc, int *cnt, int *st) {
   const DevGeo &g = p.geo[rep];
   const int T = blockDim.x, tid = threadIdx.x;
   const int nb = g.n[0] * g.n[1] * g.n[2];
@@ -1872,7 +1894,7 @@ __device__ __forceinline__ int persist_step(const KParams &p, int rep, int off, 
     if (id_species(id) != kDeadSpecies) fate = advance_one<false, SURF>(pc, id, step, p, gtab, 0, hits);
     if (fate == 0) {
       p.tmp[idx] = pc;
-      atomicAdd(&p.cnt[global_cell(g, __float_as_uint(pc.w))], 1);
+      atomicAdd(&cnt[local_cell(g, __float_as_uint(pc.w))], 1);
     } else {
       p.tmp[idx] = make_float4(0.f, 0.f, 0.f, __uint_as_float(kTmpGone));
       if (fate == 1) {
@@ -1918,15 +1940,15 @@ __device__ __forceinline__ int persist_step(const KParams &p, int rep, int off, 
     const int per = (nb + T - 1) / T;
     const int lo = min(nb, tid * per), hi = min(nb, lo + per);
     int sum = 0;
-    for (int c = lo; c < hi; ++c) sum += p.cnt[c0 + c];
+    for (int c = lo; c < hi; ++c) sum += cnt[c];
     int total;
     int run = off + block_exclusive_scan(sum, sh.warp, total);
     for (int c = lo; c < hi; ++c) {
-      p.start[c0 + c] = run;
-      run += p.cnt[c0 + c];
+      st[c] = run;
+      run += cnt[c];
     }
     if (tid == 0) {
-      p.start[c0 + nb] = off + total;
+      st[nb] = off + total;
       sh.ns = total;
     }
   }
@@ -1942,14 +1964,14 @@ __device__ __forceinline__ int persist_step(const KParams &p, int rep, int off, 
     float4 pc = make_float4(0.f, 0.f, 0.f, __uint_as_float(kTmpGone));
     if (i < n) pc = p.tmp[off + i];
     const bool alive = __float_as_uint(pc.w) != kTmpGone;
-    const int cell = alive ? global_cell(g, __float_as_uint(pc.w)) : -1;
+    const int cell = alive ? local_cell(g, __float_as_uint(pc.w)) : -1;
     const BoxRun run = box_run(alive, cell);
     int old = 0;
-    if (alive && run.rank == 0) old = atomicSub(&p.cnt[cell], run.count);
-    const int st = alive ? p.start[cell] : 0;
+    if (alive && run.rank == 0) old = atomicSub(&cnt[cell], run.count);
+    const int s0 = alive ? st[cell] : 0;
     old = __shfl_sync(0xffffffffu, old, alive ? run.head : (tid & 31));
     if (alive) {
-      const int slot = st + old - run.count + run.rank;
+      const int slot = s0 + old - run.count + run.rank;
       p.b_pc[slot] = pc;
       p.b_id[slot] = p.a_id[off + i];
     }
@@ -1964,7 +1986,7 @@ __device__ __forceinline__ int persist_step(const KParams &p, int rep, int off, 
     const int sp = id_species(id);
     if (!((c_net.pair_any >> sp) & 1u)) continue;
     int ncd = 0;
-    const ull best = search_partner<SURF>(p, idx, p.b_pc[idx], id, step, ncd);
+    const ull best = search_partner_in<SURF>(p, idx, p.b_pc[idx], id, step, ncd, st, c0);
     if (ncd > 1) multi += ncd - 1;
     if (best != ~0ull) {
       p.best[idx] = best;
@@ -1986,7 +2008,7 @@ __device__ __forceinline__ int persist_step(const KParams &p, int rep, int off, 
         const ull id = p.b_id[i];
         if (id_species(id) == kDeadSpecies) continue;
         int ncd;
-        p.best[i] = search_partner<SURF>(p, i, p.b_pc[i], id, step, ncd);
+        p.best[i] = search_partner_in<SURF>(p, i, p.b_pc[i], id, step, ncd, st, c0);
       }
       __syncthreads();
       persist_commit<SURF>(p, rep, cand, nc, step, ev, evcap, sh, done);
@@ -2020,10 +2042,14 @@ __device__ __forceinline__ int persist_step(const KParams &p, int rep, int off, 
 template <int SURF>
 __global__ void __launch_bounds__(kPersistThreads, SMOLB_PERSIST_BLOCKS) k_persist(KParams pA, KParams pB,
                                                                                     PersistArgs q) {
-  extern __shared__ float s_gtab[];
+  extern __shared__ float s_gtab[];  // gaussian table, then the box tables of small replicates
   __shared__ PersistShared sh;
   __shared__ int s_rep;
   const float *gtab = stage_gtab(pA, s_gtab);
+  const int gsize = (int)c_net.gmask + 1;
+  int *s_cnt = reinterpret_cast<int *>(s_gtab + (gsize <= 8192 ? gsize : 0));
+  int *s_st = s_cnt + kPersistSmemBoxes + 1;
+  for (int k = threadIdx.x; k <= kPersistSmemBoxes; k += blockDim.x) s_cnt[k] = 0;
   const uint32_t step0 = *pA.step;
   Event *ev = q.ev + (size_t)blockIdx.x * q.evslice;
   int *cand = q.cand + (size_t)blockIdx.x * q.candslice;
@@ -2037,11 +2063,17 @@ __global__ void __launch_bounds__(kPersistThreads, SMOLB_PERSIST_BLOCKS) k_persi
     const int rep = q.order[t];
     const int off = q.roff[rep], cap = q.rcap[rep];
     int n = q.rn[rep];
+    const DevGeo &g = pA.geo[rep];
+    const int nb = g.n[0] * g.n[1] * g.n[2];
+    const bool small = nb <= kPersistSmemBoxes;
+    int *cnt = small ? s_cnt : pA.cnt + g.cell0;
+    int *st = small ? s_st : pA.start + g.cell0;
     for (int k = 0; k < q.nsteps; k += 2) {
-      n = persist_step<SURF>(pA, rep, off, cap, n, step0 + 1 + k, gtab, ev, q.evslice, cand, q.candslice, sh, acc);
+      n = persist_step<SURF>(pA, rep, off, cap, n, step0 + 1 + k, gtab, ev, q.evslice, cand, q.candslice, sh, acc,
+                             cnt, st);
       if (k + 1 < q.nsteps)
         n = persist_step<SURF>(pB, rep, off, cap, n, step0 + 2 + k, gtab, ev, q.evslice, cand, q.candslice, sh,
-                               acc);
+                               acc, cnt, st);
     }
     if (threadIdx.x == 0) q.rn[rep] = n;
   }
@@ -2364,7 +2396,7 @@ class EngineImpl {
   Event *d_qev = nullptr;
   int *d_qcand = nullptr;
   int qgrid = 0, qevslice = 0, qcandslice = 0, qmaxcap = 0;
-  std::vector<int> h_qoff, h_qcap;
+  std::vector<int> h_qoff, h_qcap, h_qn;
   cudaGraphExec_t qgraph[2] = {nullptr, nullptr};  // one launch block of qgraph_steps steps, per start parity
   int qgraph_steps = 0;
 
@@ -2970,6 +3002,8 @@ class EngineImpl {
     return capture_steps(0, 1, &graph2, err);
   }
 
+  size_t persist_smem() const { return adv_smem() + 2 * (kPersistSmemBoxes + 1) * sizeof(int); }
+
   // The persistent kernel covers ensembles without surfaces, compartments or
   // injected displacements (the general surface form stays on the pipeline).
   bool persist_eligible() const {
@@ -2996,7 +3030,23 @@ class EngineImpl {
   // pending products and sorts every replicate into a contiguous range, then
   // each range is copied into its replicate's region (regions hold twice the
   // replicate's molecules plus 256, processing order largest first).
-  int enter_persist(std::string *err) {
+  // Room for zeroth-order births over one launch (100 steps): twice the
+  // expected count plus 64.
+  long long birth_headroom(int r) const {
+    double m = 0;
+    for (int k = 0; k < net.nrxn[0]; ++k) m += reps[r].birth_mean[k];
+    return m > 0 ? (long long)std::ceil(2.0 * m * 100.0) + 64 : 0;
+  }
+  // Whether any reaction makes more molecules than it consumes.
+  bool can_grow() const {
+    if (net.nrxn[0] > 0) return true;
+    for (int o = 1; o < 3; ++o)
+      for (int r = 0; r < net.nrxn[o]; ++r)
+        if (net.nprod[o][r] > o) return true;
+    return false;
+  }
+
+  int enter_persist(std::string *err, const std::vector<long long> *extra = nullptr) {
     const int R = (int)reps.size();
     CK(cudaMemsetAsync(d_cnt, 0, ((size_t)ncell + 1) * sizeof(int), stream));
     enqueue_step(parity, true);
@@ -3020,7 +3070,7 @@ class EngineImpl {
     int maxcap = 0;
     for (int r = 0; r < R; ++r) {
       n[r] = lo[r + 1] - lo[r];
-      const long long c = 2ll * n[r] + 256;
+      const long long c = 2ll * n[r] + 256 + std::max(birth_headroom(r), extra ? (*extra)[r] : 0ll);
       h_qoff[r] = (int)total;
       h_qcap[r] = (int)c;
       total += c;
@@ -3049,7 +3099,8 @@ class EngineImpl {
       qmaxcap = maxcap;
       // CTAs: as many as stay resident (one wave), at most one per replicate
       int per_sm = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persist<0>, kPersistThreads, adv_smem());
+      CK(cudaFuncSetAttribute(k_persist<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)persist_smem()));
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persist<0>, kPersistThreads, persist_smem());
       qgrid = std::max(1, std::min(R, sm_count() * std::max(1, per_sm)));
       qevslice = std::max(1024, maxcap / 8);
       qcandslice = std::max(1024, maxcap / 4);
@@ -3079,7 +3130,41 @@ class EngineImpl {
     nlaunch += 2;
     ppar = 0;
     in_persist = true;
+    h_qn = n;
     return 0;
+  }
+
+  // After a launch: the replicates' entry counts and the status word.  A
+  // replicate whose free room is below three times its growth in the last
+  // launch (or its birth headroom) gets a new layout with more room before
+  // the next launch; a capacity overflow is an error.
+  int persist_check(bool relayout, std::string *err) {
+    const int R = (int)reps.size();
+    std::vector<int> n((size_t)R);
+    int st = 0;
+    CK(cudaMemcpyAsync(n.data(), d_qint + 3 * R, (size_t)R * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CK(cudaMemcpyAsync(&st, d_counts + 6, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    if (st & (kStMolCap | kStEvCap | kStCandCap)) {
+      if (err)
+        *err = std::string("persistent kernel: ") +
+               ((st & kStMolCap) ? "replicate region" : (st & kStEvCap) ? "event list" : "candidate list") +
+               " overflow";
+      return -9;
+    }
+    if (!relayout) { h_qn = n; return 0; }
+    bool need = false;
+    std::vector<long long> extra((size_t)R, 0);
+    for (int r = 0; r < R; ++r) {
+      const long long grow = std::max(0, n[r] - (r < (int)h_qn.size() ? h_qn[r] : n[r]));
+      extra[r] = 3 * grow + birth_headroom(r);
+      if ((long long)h_qcap[r] - n[r] < std::max(256ll, extra[r])) need = true;
+    }
+    h_qn = n;
+    if (!need) return 0;
+    int rc = leave_persist(err);
+    if (!rc) rc = enter_persist(err, &extra);
+    return rc;
   }
 
   // Back to the step pipeline's layout: every replicate's entries are
@@ -3143,6 +3228,7 @@ class EngineImpl {
       if (rc) return rc;
     }
     const int R = (int)reps.size();
+    const bool grow = can_grow();
     long long left = nsteps;
     while (left > 0) {
       const int K = (int)std::min<long long>(left, 100);
@@ -3160,7 +3246,8 @@ class EngineImpl {
         q.nrep = R;
         q.nsteps = K;
         cudaMemsetAsync(q.queue, 0, sizeof(int), stream);
-        k_persist<0><<<qgrid, kPersistThreads, adv_smem(), stream>>>(persist_params(in), persist_params(1 - in), q);
+        k_persist<0><<<qgrid, kPersistThreads, persist_smem(), stream>>>(persist_params(in), persist_params(1 - in),
+                                                                         q);
         k_bump_step<<<1, 1, 0, stream>>>(d_step, K);
       };
       if (use_graph) {
@@ -3187,8 +3274,13 @@ class EngineImpl {
       nlaunch += 2;
       ppar ^= (K & 1);
       left -= K;
+      if (grow) {
+        int rc = persist_check(true, err);
+        if (rc) return rc;
+      }
     }
     CK(cudaGetLastError());
+    if (!grow) return persist_check(false, err);
     return 0;
   }
 

@@ -355,6 +355,18 @@ enum ErrorCode smolgpuEnsembleGetCounts(ensptr ens, long long *counts) {
   return ECok;
 }
 
+enum ErrorCode smolgpuEnsembleGetEventCounts(ensptr ens, long long counts[8]) {
+  ECHECK(ens && counts, ECmissing, "missing argument");
+  for (int k = 0; k < 8; ++k) counts[k] = 0;
+  if (!ens->eng) return ECok;
+  smolb::EngineStats st;
+  std::string err;
+  if (ens->eng->stats(&st, &err)) return ens_error(__func__, ECerror, err);
+  counts[0] = st.wall; counts[1] = st.rxn0; counts[2] = st.rxn1; counts[3] = st.rxn2;
+  counts[4] = st.unresolved; counts[5] = st.multicand; counts[6] = st.overflow;
+  return ECok;
+}
+
 enum ErrorCode smolgpuEnsembleGetMolecules(ensptr ens, long long *n, double *pos, int *species, int *rep,
                                            uint64_t *serno) {
   ECHECK(ens && n, ECmissing, "missing argument");
