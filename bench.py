@@ -416,8 +416,9 @@ def run_batched(sb, torch, args, rank):
     """Ensemble workload: 4096 replicates, N log-uniform in [1e2, 1e5] at
     density 0.01, kf and kr log-uniform in [1e-3, 1] per replicate, radii from
     the exact FP64 solver on the device, dt = 0.01, 2000 steps (the
-    configuration's count; fewer with --batched-steps).  Stepped by the
-    persistent ensemble kernel, with the step pipeline timed beside it."""
+    configuration's count; fewer with --batched-steps).  Stepped by the step
+    pipeline (the ensemble default), with the persistent kernel timed beside
+    it."""
     rng = np.random.default_rng(12345 + rank)
     R = 4096
     n, side = draw_replicates(rng, R, 1e2, 1e5)
@@ -444,8 +445,8 @@ def run_batched(sb, torch, args, rank):
     engine = {1: "step pipeline", 2: "persistent"}.get(e.engine(), "?")
     tot = float(n.sum())
     ev = e.events()
-    # the same ensemble on the step pipeline, fewer steps (per-step cost is flat)
-    e.engine(1)
+    # the same ensemble on the persistent kernel, fewer steps (per-step cost is flat)
+    e.engine(2)
     e.run_steps(args.warmup)
     psteps = min(steps, 100)
     psec = time_on_stream(torch, stream, lambda: e.run_steps(psteps))
@@ -454,8 +455,9 @@ def run_batched(sb, torch, args, rank):
            "engine": engine, "value": tot * steps / sec, "unit": METRIC, "molecules": int(tot), "replicates": R,
            "steps": steps, "ms_per_step": sec * 1e3 / steps, "setup_s": setup, "gpu_launches": launches,
            "events": {"rxn1": ev[2], "rxn2": ev[3], "overflow": ev[6]},
-           "step_pipeline": {"value": tot * psteps / psec, "steps": psteps, "ms_per_step": psec * 1e3 / psteps}}
-    out["persistent_vs_pipeline"] = out["value"] / out["step_pipeline"]["value"]
+           "persistent_kernel": {"value": tot * psteps / psec, "steps": psteps, "ms_per_step": psec * 1e3 / psteps,
+                                 "note": "one thread block per replicate, up to 100 steps per launch"}}
+    out["persistent_vs_pipeline"] = out["persistent_kernel"]["value"] / out["value"]
     e.close()
     return out
 

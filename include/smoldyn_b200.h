@@ -326,17 +326,18 @@ enum ErrorCode smolgpuEnsembleSetRates(ensptr ens, const char *reaction, const d
 enum ErrorCode smolgpuEnsembleAddMolecules(ensptr ens, const char *species, const int *counts);
 enum ErrorCode smolgpuEnsembleSetRadiusMode(ensptr ens, int mode);
 enum ErrorCode smolgpuEnsembleAttachSurrogate(ensptr ens, surptr sur);
-/* Which engine steps the ensemble: mode 0 (default) the persistent kernel
- * whenever the configuration allows it, else the step pipeline; 1 the step
- * pipeline (the device-wide launch sequence of a single simulation, all
- * replicates in each launch); 2 the persistent kernel only (ECerror when the
- * configuration has surfaces, compartments or injected displacements).  The
- * persistent kernel gives each replicate to one thread block, which runs up to
- * 100 whole time steps of it per launch (move, box sort, pair search, conflict
- * rounds, products) from an L2-resident working set; it uses the step
- * pipeline's per-molecule code and random streams, so both engines give the
- * same trajectories up to the ranking of equidistant candidates.
- * smolgpuEnsembleGetEngine returns 1 or 2, the engine the next step uses. */
+/* Which engine steps the ensemble: mode 0 (default) automatic, currently the
+ * step pipeline, which measures faster on B200; 1 the step pipeline (the
+ * device-wide launch sequence of a single simulation, all replicates in each
+ * launch); 2 the persistent kernel (ECerror when the configuration has
+ * surfaces, compartments or injected displacements).  The persistent kernel
+ * gives each replicate to one thread block, which runs up to 100 whole time
+ * steps of it per launch (move, box sort, pair search, conflict rounds,
+ * products), one captured graph per launch, from an L2-resident working set;
+ * it uses the step pipeline's per-molecule code and random streams, so both
+ * engines give the same trajectories up to the ranking of equidistant
+ * candidates.  smolgpuEnsembleGetEngine returns 1 or 2, the engine the next
+ * step uses. */
 enum ErrorCode smolgpuEnsembleSetEngine(ensptr ens, int mode);
 int smolgpuEnsembleGetEngine(ensptr ens);
 enum ErrorCode smolgpuEnsembleUpdate(ensptr ens);

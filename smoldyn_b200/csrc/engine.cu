@@ -1360,18 +1360,34 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_pairs_tile(KParams p) {
   if (extra) atomicAdd(&p.counters[5], (unsigned long long)extra);
 }
 
-// Cross-box pairs of one molecule within the stencil radius of a box face:
-// walk the neighbouring boxes its stencil reaches; a pair across boxes is
-// tested by the molecule in the lower-numbered box.
-template <bool SINGLE, int SURF>
-__device__ __forceinline__ void face_walk(const KParams &p, int i, int n, uint32_t step, int &extra) {
-  const float4 pc = p.b_pc[i];
-  const ull idi = p.b_id[i];
+// Position of the k-th (from 0) set bit of m; k < popc(m).
+__device__ __forceinline__ int nth_set_bit(uint32_t m, int k) {
+  int pos = 0;
+#pragma unroll
+  for (int w = 16; w > 0; w >>= 1) {
+    const uint32_t low = m & ((1u << w) - 1u);
+    const int c = __popc(low);
+    if (k >= c) {
+      k -= c;
+      m >>= w;
+      pos += w;
+    } else {
+      m = low;
+    }
+  }
+  return pos;
+}
+
+// Upward neighbour boxes of molecule i that its stencil reaches: bit
+// (dz+1)*9 + (dy+1)*3 + (dx+1) is set for each offset whose box (after the
+// periodic wrap) has a higher global number than i's own box, the boxes
+// face_walk visits.
+template <bool SINGLE>
+__device__ __forceinline__ uint32_t face_boxes(const KParams &p, float4 pc, ull idi) {
   const int sp = id_species(idi);
   const int rep = SINGLE ? 0 : id_rep(idi);
   const DevGeo &g = geo_of<SINGLE>(p, rep);
   const float rs = p.rsearch[rep * c_net.nsp + sp];
-  const float rs2 = rs * rs;
   int ix, iy, iz;
   unpack_cell(__float_as_uint(pc.w), ix, iy, iz);
   const int cell = global_cell(g, __float_as_uint(pc.w));
@@ -1382,7 +1398,7 @@ __device__ __forceinline__ void face_walk(const KParams &p, int i, int n, uint32
   const int ylo = pc.y < rs ? -1 : 0, yhi = pc.y > ub1 - rs ? 1 : 0;
   const int zlo = pc.z < rs ? -1 : 0, zhi = pc.z > ub2 - rs ? 1 : 0;
   const bool px = g.wall[0] == kWallPeriodic, py = g.wall[2] == kWallPeriodic, pz = g.wall[4] == kWallPeriodic;
-  ull best = ~0ull;
+  uint32_t m = 0;
   for (int dz = zlo; dz <= zhi; ++dz) {
     int z = iz + dz;
     if (z < 0 || z >= g.n[2]) {
@@ -1403,28 +1419,53 @@ __device__ __forceinline__ void face_walk(const KParams &p, int i, int n, uint32
           if (!px) continue;
           x = (x < 0) ? x + g.n[0] : x - g.n[0];
         }
-        const int c = rowbase + x;
-        if (c <= cell) continue;
-        const int s0 = p.start[c], e0 = min(p.start[c + 1], n);
-        for (int j = s0; j < e0; ++j) {
-          const float4 q = p.b_pc[j];
-          const float vx = (q.x - pc.x) + (float)dx * g.h[0];
-          const float vy = (q.y - pc.y) + (float)dy * g.h[1];
-          const float vz = (q.z - pc.z) + (float)dz * g.h[2];
-          const float d2 = vx * vx + vy * vy + vz * vz;
-          if (d2 <= rs2)  // the partner's identity is read only for in-radius pairs
-            try_pair<SURF>(p, i, idi, sp, rep, d2, j, p.b_id[j], rs2, step, best, extra, pc, vx, vy, vz);
-        }
+        if (rowbase + x <= cell) continue;
+        m |= 1u << ((dz + 1) * 9 + (dy + 1) * 3 + (dx + 1));
       }
     }
+  }
+  return m;
+}
+
+// Cross-box pairs of molecule i with the molecules of one upward neighbour
+// box (offset code k of face_boxes); the closest reacting partner found is
+// registered on i, every reacting pair on the partner.
+template <bool SINGLE, int SURF>
+__device__ __forceinline__ void face_box_walk(const KParams &p, int i, float4 pc, ull idi, int k, int n,
+                                              uint32_t step, int &extra) {
+  const int sp = id_species(idi);
+  const int rep = SINGLE ? 0 : id_rep(idi);
+  const DevGeo &g = geo_of<SINGLE>(p, rep);
+  const float rs = p.rsearch[rep * c_net.nsp + sp];
+  const float rs2 = rs * rs;
+  const int dz = k / 9 - 1, dy = (k / 3) % 3 - 1, dx = k % 3 - 1;
+  int ix, iy, iz;
+  unpack_cell(__float_as_uint(pc.w), ix, iy, iz);
+  int x = ix + dx, y = iy + dy, z = iz + dz;
+  if (x < 0) x += g.n[0]; else if (x >= g.n[0]) x -= g.n[0];
+  if (y < 0) y += g.n[1]; else if (y >= g.n[1]) y -= g.n[1];
+  if (z < 0) z += g.n[2]; else if (z >= g.n[2]) z -= g.n[2];
+  const int c = g.cell0 + (z * g.n[1] + y) * g.n[0] + x;
+  const int s0 = p.start[c], e0 = min(p.start[c + 1], n);
+  ull best = ~0ull;
+  for (int j = s0; j < e0; ++j) {
+    const float4 q = p.b_pc[j];
+    const float vx = (q.x - pc.x) + (float)dx * g.h[0];
+    const float vy = (q.y - pc.y) + (float)dy * g.h[1];
+    const float vz = (q.z - pc.z) + (float)dz * g.h[2];
+    const float d2 = vx * vx + vy * vy + vz * vz;
+    if (d2 <= rs2)  // the partner's identity is read only for in-radius pairs
+      try_pair<SURF>(p, i, idi, sp, rep, d2, j, p.b_id[j], rs2, step, best, extra, pc, vx, vy, vz);
   }
   if (best != ~0ull) extra += register_candidate(p, i, best);
 }
 
 // Cross-box pairs for the molecules flagged in the face bitmask by
-// k_pairs_tile.  Each warp reads 32 bitmask words (1024 molecules), numbers
-// their set bits with a warp prefix sum and hands them out 32 at a time, so
-// every lane walks one flagged molecule per round.
+// k_pairs_tile.  Each warp takes one bitmask word (32 molecules): its
+// flagged molecules list the upward neighbour boxes their stencils reach,
+// and the (molecule, neighbour box) items are numbered by a warp prefix sum
+// and handed out 32 at a time, so a molecule that reaches several boxes
+// spreads over several lanes.
 template <bool SINGLE, int SURF>
 __global__ void __launch_bounds__(256) k_pairs_faces(KParams p) {
   pdl_launch_dependents();
@@ -1437,9 +1478,22 @@ __global__ void __launch_bounds__(256) k_pairs_faces(KParams p) {
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   int extra = 0;
-  for (int base = gw * 32; base < nwords; base += nw * 32) {
-    const uint32_t bits = (base + lane < nwords) ? facebits[base + lane] : 0u;
-    const int cnt = __popc(bits);
+  for (int wd = gw; wd < nwords; wd += nw) {
+    const uint32_t bits = facebits[wd];
+    if (!bits) continue;
+    // lane k holds the k-th flagged molecule of the word
+    const int nf = __popc(bits);
+    int i = -1;
+    float4 pc = make_float4(0.f, 0.f, 0.f, 0.f);
+    ull idi = 0;
+    uint32_t boxes = 0;
+    if (lane < nf) {
+      i = (wd << 5) + nth_set_bit(bits, lane);
+      pc = p.b_pc[i];
+      idi = p.b_id[i];
+      boxes = face_boxes<SINGLE>(p, pc, idi);
+    }
+    const int cnt = __popc(boxes);
     int incl = cnt;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -1454,12 +1508,18 @@ __global__ void __launch_bounds__(256) k_pairs_faces(KParams p) {
 #pragma unroll
       for (int st = 16; st > 0; st >>= 1)
         if (__shfl_sync(0xffffffffu, excl, o + st) <= q) o += st;
-      uint32_t m = __shfl_sync(0xffffffffu, bits, o);
       const int r = q - __shfl_sync(0xffffffffu, excl, o);
+      const int io = __shfl_sync(0xffffffffu, i, o);
+      const uint32_t bo = __shfl_sync(0xffffffffu, boxes, o);
+      float4 po;
+      po.x = __shfl_sync(0xffffffffu, pc.x, o);
+      po.y = __shfl_sync(0xffffffffu, pc.y, o);
+      po.z = __shfl_sync(0xffffffffu, pc.z, o);
+      po.w = __shfl_sync(0xffffffffu, pc.w, o);
+      const ull ido = __shfl_sync(0xffffffffu, idi, o);
       if (q < total) {
-        for (int k = 0; k < r; ++k) m &= m - 1;  // drop the r lower set bits
-        const int i = ((base + o) << 5) + __ffs(m) - 1;
-        face_walk<SINGLE, SURF>(p, i, n, step, extra);
+        const int k = nth_set_bit(bo, r);
+        face_box_walk<SINGLE, SURF>(p, io, po, ido, k, n, step, extra);
       }
     }
   }

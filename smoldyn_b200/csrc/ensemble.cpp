@@ -44,7 +44,7 @@ struct smolb_ens {
   long long surrogate_fallbacks = 0;
   std::unique_ptr<smolb::Surrogate> sur;
   smolb::LaunchTuning tuning;  // kernel launch shape (autotuner)
-  int engine_mode = 0;         // 0 persistent kernel when the configuration allows, 1 step pipeline, 2 persistent only
+  int engine_mode = 0;         // 0 automatic (the step pipeline, measured faster), 1 step pipeline, 2 persistent kernel
 };
 
 // process-global error record of the C API (api.cpp)
@@ -209,7 +209,7 @@ int build(smolb_ens &e, std::string *err) {
   e.eng.reset(new smolb::Engine());
   rc = e.eng->init(e.net, e.reps, T.dt, (uint64_t)T.seed, cap, err);
   if (!rc) rc = e.eng->set_tuning(e.tuning, err);
-  if (!rc) rc = e.eng->set_persistent(e.engine_mode == 1 ? 0 : 1, err);
+  if (!rc) rc = e.eng->set_persistent(e.engine_mode == 2 ? 1 : 0, err);
   if (rc) return rc;
   if (e.engine_mode == 2 && !e.eng->persistent_active()) {
     *err = "the persistent kernel does not cover surfaces, compartments or injected displacements";
@@ -313,7 +313,7 @@ enum ErrorCode smolgpuEnsembleSetEngine(ensptr ens, int mode) {
   ens->engine_mode = mode;
   if (ens->eng) {
     std::string err;
-    if (ens->eng->set_persistent(mode == 1 ? 0 : 1, &err)) return ens_error(__func__, ECerror, err);
+    if (ens->eng->set_persistent(mode == 2 ? 1 : 0, &err)) return ens_error(__func__, ECerror, err);
     ECHECK(mode != 2 || ens->eng->persistent_active(), ECerror,
            "the persistent kernel does not cover surfaces, compartments or injected displacements");
   }
@@ -322,7 +322,7 @@ enum ErrorCode smolgpuEnsembleSetEngine(ensptr ens, int mode) {
 
 int smolgpuEnsembleGetEngine(ensptr ens) {
   if (!ens) return (int)ens_error(__func__, ECmissing, "missing ensemble");
-  if (!ens->eng) return ens->engine_mode == 1 ? 1 : 2;
+  if (!ens->eng) return ens->engine_mode == 2 ? 2 : 1;
   return ens->eng->persistent_active() ? 2 : 1;
 }
 

@@ -13,7 +13,8 @@ ranks exactly equidistant reaction candidates differently.  Checked on:
   - the molecules themselves after the run (positions, species, serial
     numbers), read back through the step pipeline's layout;
   - stepping on after the read-back, and switching engines mid-run.
-The engine choice is reported by smolgpuEnsembleGetEngine.
+The engine choice is reported by smolgpuEnsembleGetEngine; the default
+(mode 0) is the step pipeline.
 """
 import numpy as np
 import pytest
@@ -108,6 +109,15 @@ def test_births_decay_absorbing_same_trajectory():
     a, b = run_both(lambda: births_decay(128), [50, 51])
     compare(a, b, "births/decay/absorbing")
     assert a[0][:, 2].sum() > 0 and a[0][:, 3].sum() > 0
+
+
+def test_default_engine_is_pipeline():
+    e = reversible(8)
+    e.update()
+    assert e.engine() == 1
+    e.engine(2)
+    assert e.engine() == 2
+    e.close()
 
 
 def test_switch_engines_mid_run():
