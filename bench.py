@@ -253,6 +253,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-batched", action="store_true", help="skip the ensemble and surrogate workloads")
     ap.add_argument("--no-tune", action="store_true", help="default launch shape and box width (no autotuner)")
+    ap.add_argument("--kernel-tour", action="store_true",
+                    help="run one small case of every kernel of the library (profiler captures) and exit")
     ap.add_argument("--batched-steps", type=int, default=2000, help="steps of the 4096-replicate ensemble leg")
     ap.add_argument("--surrogate-steps", type=int, default=5000,
                     help="steps of the 65,536-replicate surrogate sweep (rates redrawn every 100)")
@@ -265,6 +267,8 @@ def main():
 
     if args.impl == "reference":
         return run_reference_arm(args, rank, world)
+    if args.kernel_tour:
+        return kernel_tour(args)
 
     import torch
     dist = None
@@ -378,6 +382,99 @@ def main():
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
+    return 0
+
+
+TOUR_CONFIG = """dim 3
+species A B C
+difc A 1
+difc B 1
+difc C 0.5
+boundaries 0 0 60 p
+boundaries 1 0 60 p
+boundaries 2 0 60 p
+time_start 0
+time_stop 100
+time_step 0.01
+random_seed 3
+start_surface ball
+action both all transmit
+panel sphere 30 30 30 12 20 20
+end_surface
+start_compartment core
+surface ball
+point 30 30 30
+end_compartment
+reaction fwd A + B -> C 0.5
+reaction rev C -> A + B 0.1
+mol 20000 A u u u
+mol 20000 B u u u
+output_files msd.txt cnt.txt
+cmd N 5 meansqrdisp A all msd.txt
+cmd N 5 molcountincmpt core cnt.txt
+end_file
+"""
+
+
+def kernel_tour(args):
+    """One small case of every kernel of the library, for profiler captures
+    (ncu -k selects the kernel): the step pipeline on the scale-up workload
+    at 4e6 molecules (its density), the device upload path, meansqrdisp and
+    molcountincmpt with a transmitting sphere compartment (surface form of the
+    step kernels), the FP64 radius solvers, the surrogate's sampling,
+    training, inference and radius kernels, the persistent ensemble kernel
+    and its layout changes, and the radial-distribution solver."""
+    import ctypes as C
+    import torch
+    torch.cuda.set_device(0)
+    import smoldyn_b200 as sb
+    lib = sb.load()
+    n = 4_000_000
+    s = build_sim(sb, n, L_SIDE * (n / N_MOL) ** (1.0 / 3.0), 1)
+    s.update()
+    s.run_steps(3)
+    pos, sp, sn = s.molecules()
+    s.set_molecules(pos, sp, sn)     # device upload path
+    s.run_steps(2)
+    s.synchronize()
+    s.close()
+    d = tempfile.mkdtemp(prefix="smoltour_")
+    try:
+        with open(os.path.join(d, "t.txt"), "w") as f:
+            f.write(TOUR_CONFIG)
+        simp = C.c_void_p()
+        assert lib.smolLoadSimFromFile((d + "/").encode(), b"t.txt", C.byref(simp), b"") == 0, sb.last_error()
+        t = sb.Sim(ptr=simp.value)
+        t.run_until(0.1)
+        t.close()
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    rng = np.random.default_rng(1)
+    m = 65536
+    rate, difc = 10 ** rng.uniform(-3, 0, m), np.full(m, 2.0)
+    sb.solve_radii_device(0, rate, DT, difc, np.full(m, 1.5), rel=1)
+    sb.solve_radii_prob_device(rate, DT, difc, np.full(m, -1.0), 0, np.full(m, -1.0), np.full(m, 0.5))
+    sur = sb.Surrogate()
+    sur.train(nsamples=16384, epochs=1, batch=512, lr=3e-3, seed=5)
+    sur.pair_radii(rate, difc, DT, same=0, rev=1, rparamt=sb.RPratio, rparam=1.5)
+    R = 1024
+    nr, side = draw_replicates(rng, R, 1e2, 1e4)
+    e = sb.Ensemble(ensemble_template(sb, placement=(sb.RPratio, 1.5)), R)
+    e.set_boxes(np.zeros((R, 3)), np.repeat(side[:, None], 3, 1))
+    e.set_rates("fwd", 10 ** rng.uniform(-3, 0, R))
+    e.set_rates("rev", 10 ** rng.uniform(-3, 0, R))
+    e.add_molecules("A", nr // 2 + nr % 2)
+    e.add_molecules("B", nr // 2)
+    e.radius_mode(1)
+    e.engine(2)
+    e.update()
+    e.run_steps(10)
+    e.counts(4)
+    e.molecules()
+    e.close()
+    sb.rdf_table("i", 100, 1e-5, "d")
+    torch.cuda.synchronize()
+    print("kernel tour done")
     return 0
 
 
