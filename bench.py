@@ -599,6 +599,7 @@ def run_surrogate(sb, torch, args, rank):
     def work():
         for blk in range(steps // 100):
             redraw()
+            e.synchronize()  # the update's own cost, not the previous block's steps
             t1 = time.perf_counter()
             e.update()
             upd.append(time.perf_counter() - t1)

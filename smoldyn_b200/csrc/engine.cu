@@ -1461,11 +1461,12 @@ __device__ __forceinline__ void face_box_walk(const KParams &p, int i, float4 pc
 }
 
 // Cross-box pairs for the molecules flagged in the face bitmask by
-// k_pairs_tile.  Each warp takes one bitmask word (32 molecules): its
-// flagged molecules list the upward neighbour boxes their stencils reach,
-// and the (molecule, neighbour box) items are numbered by a warp prefix sum
-// and handed out 32 at a time, so a molecule that reaches several boxes
-// spreads over several lanes.
+// k_pairs_tile.  Each warp reads 32 bitmask words (1024 molecules) at once,
+// numbers their set bits with a warp prefix sum and takes the flagged
+// molecules 32 at a time, one per lane; each such molecule lists the upward
+// neighbour boxes its stencil reaches, and a second prefix sum hands the
+// (molecule, neighbour box) items out 32 at a time, so a molecule reaching
+// several boxes spreads over several lanes.
 template <bool SINGLE, int SURF>
 __global__ void __launch_bounds__(256) k_pairs_faces(KParams p) {
   pdl_launch_dependents();
@@ -1478,22 +1479,9 @@ __global__ void __launch_bounds__(256) k_pairs_faces(KParams p) {
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   int extra = 0;
-  for (int wd = gw; wd < nwords; wd += nw) {
-    const uint32_t bits = facebits[wd];
-    if (!bits) continue;
-    // lane k holds the k-th flagged molecule of the word
-    const int nf = __popc(bits);
-    int i = -1;
-    float4 pc = make_float4(0.f, 0.f, 0.f, 0.f);
-    ull idi = 0;
-    uint32_t boxes = 0;
-    if (lane < nf) {
-      i = (wd << 5) + nth_set_bit(bits, lane);
-      pc = p.b_pc[i];
-      idi = p.b_id[i];
-      boxes = face_boxes<SINGLE>(p, pc, idi);
-    }
-    const int cnt = __popc(boxes);
+  for (int base = gw * 32; base < nwords; base += nw * 32) {
+    const uint32_t bits = (base + lane < nwords) ? facebits[base + lane] : 0u;
+    const int cnt = __popc(bits);
     int incl = cnt;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -1508,18 +1496,44 @@ __global__ void __launch_bounds__(256) k_pairs_faces(KParams p) {
 #pragma unroll
       for (int st = 16; st > 0; st >>= 1)
         if (__shfl_sync(0xffffffffu, excl, o + st) <= q) o += st;
+      const uint32_t m = __shfl_sync(0xffffffffu, bits, o);
       const int r = q - __shfl_sync(0xffffffffu, excl, o);
-      const int io = __shfl_sync(0xffffffffu, i, o);
-      const uint32_t bo = __shfl_sync(0xffffffffu, boxes, o);
-      float4 po;
-      po.x = __shfl_sync(0xffffffffu, pc.x, o);
-      po.y = __shfl_sync(0xffffffffu, pc.y, o);
-      po.z = __shfl_sync(0xffffffffu, pc.z, o);
-      po.w = __shfl_sync(0xffffffffu, pc.w, o);
-      const ull ido = __shfl_sync(0xffffffffu, idi, o);
+      int i = 0;
+      float4 pc = make_float4(0.f, 0.f, 0.f, 0.f);
+      ull idi = 0;
+      uint32_t boxes = 0;
       if (q < total) {
-        const int k = nth_set_bit(bo, r);
-        face_box_walk<SINGLE, SURF>(p, io, po, ido, k, n, step, extra);
+        i = ((base + o) << 5) + nth_set_bit(m, r);
+        pc = p.b_pc[i];
+        idi = p.b_id[i];
+        boxes = face_boxes<SINGLE>(p, pc, idi);
+      }
+      // second level: the (molecule, neighbour box) items of these molecules
+      const int c2 = __popc(boxes);
+      int incl2 = c2;
+#pragma unroll
+      for (int u = 1; u < 32; u <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl2, u);
+        if (lane >= u) incl2 += y;
+      }
+      const int excl2 = incl2 - c2;
+      const int total2 = __shfl_sync(0xffffffffu, incl2, 31);
+      for (int q1 = 0; q1 < total2; q1 += 32) {
+        const int qq = q1 + lane;
+        int oo = 0;
+#pragma unroll
+        for (int st = 16; st > 0; st >>= 1)
+          if (__shfl_sync(0xffffffffu, excl2, oo + st) <= qq) oo += st;
+        const int rr = qq - __shfl_sync(0xffffffffu, excl2, oo);
+        const int io = __shfl_sync(0xffffffffu, i, oo);
+        const uint32_t bo = __shfl_sync(0xffffffffu, boxes, oo);
+        float4 po;
+        po.x = __shfl_sync(0xffffffffu, pc.x, oo);
+        po.y = __shfl_sync(0xffffffffu, pc.y, oo);
+        po.z = __shfl_sync(0xffffffffu, pc.z, oo);
+        po.w = __shfl_sync(0xffffffffu, pc.w, oo);
+        const ull ido = __shfl_sync(0xffffffffu, idi, oo);
+        if (qq < total2) face_box_walk<SINGLE, SURF>(p, io, po, ido, nth_set_bit(bo, rr), n, step, extra);
       }
     }
   }
