@@ -82,6 +82,7 @@ struct KParams {
   unsigned long long *counters;  // [0]=wall [1]=rxn0 [2]=rxn1 [3]=rxn2 [4]=unresolved [5]=multicand
   long long *spcount;            // [rep*nsp + sp]
   int *status;
+  unsigned int *bar;             // grid barrier counter of k_resolve (zeroed by k_begin)
   uint32_t *step;
   // deterministic mode
   const ull *inj_key;            // sorted stream keys
@@ -91,7 +92,9 @@ struct KParams {
 
 constexpr uint32_t kTmpGone = 0xFFFFFFFFu;  // tmp[i].w of a molecule that left
 
-enum StatusBits { kStMolCap = 1, kStEvCap = 2, kStProdCap = 4, kStCandCap = 8, kStScanWait = 16, kStUpload = 32 };
+enum StatusBits {
+  kStMolCap = 1, kStEvCap = 2, kStProdCap = 4, kStCandCap = 8, kStScanWait = 16, kStUpload = 32, kStBarrier = 64
+};
 
 // Programmatic dependent launch: the step's kernels are launched so that the
 // next kernel can be scheduled while the current one runs.  Each kernel lets
@@ -626,6 +629,7 @@ __global__ void k_begin(KParams p, int bump_step) {
     *p.nev = 0;
     *p.ncand = 0;
     *p.q_n = 0;
+    *p.bar = 0;
   }
 }
 
@@ -1542,11 +1546,8 @@ __global__ void __launch_bounds__(256) k_pairs_faces(KParams p) {
 
 // Re-search for candidates still alive (conflict-resolution rounds >= 2).
 template <int SURF>
-__global__ void k_research(KParams p) {
-  pdl_launch_dependents();
-  pdl_wait();
+__device__ __forceinline__ void research_body(const KParams &p, uint32_t step) {
   const int nc = min(*p.ncand, p.candcap);
-  const uint32_t step = *p.step;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nc; t += gridDim.x * blockDim.x) {
     const int i = p.cand[t];
     const ull id = p.b_id[i];
@@ -1554,6 +1555,13 @@ __global__ void k_research(KParams p) {
     int ncd;
     p.best[i] = search_partner<SURF>(p, i, p.b_pc[i], id, step, ncd);
   }
+}
+
+template <int SURF>
+__global__ void k_research(KParams p) {
+  pdl_launch_dependents();
+  pdl_wait();
+  research_body<SURF>(p, *p.step);
 }
 
 // Site of a bimolecular reaction, in the local frame of molecule i
@@ -1595,11 +1603,8 @@ __device__ __forceinline__ float4 pair_site(const KParams &p, int i, int j, int 
 }
 
 template <int SURF>
-__global__ void k_commit(KParams p) {
-  pdl_launch_dependents();
-  pdl_wait();
+__device__ __forceinline__ void commit_body(const KParams &p, uint32_t step) {
   const int nc = min(*p.ncand, p.candcap);
-  const uint32_t step = *p.step;
   int done = 0;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nc; t += gridDim.x * blockDim.x) {
     const int i = p.cand[t];
@@ -1635,6 +1640,13 @@ __global__ void k_commit(KParams p) {
     done++;
   }
   if (done) atomicAdd(&p.counters[3], (unsigned long long)done);
+}
+
+template <int SURF>
+__global__ void k_commit(KParams p) {
+  pdl_launch_dependents();
+  pdl_wait();
+  commit_body<SURF>(p, *p.step);
 }
 
 // ---- product placement -----------------------------------------------------
@@ -1827,11 +1839,8 @@ __device__ __forceinline__ void place_event(const KParams &p, const Event &e, ui
 }
 
 template <int SURF>
-__global__ void k_products(KParams p) {
-  pdl_launch_dependents();
-  pdl_wait();
+__device__ __forceinline__ void products_body(const KParams &p, uint32_t step) {
   const int ne = min(*p.nev, p.evcap);
-  const uint32_t step = *p.step;
   int uni = 0;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ne; t += gridDim.x * blockDim.x) {
     place_event<SURF>(p, p.ev[t], step, uni, [&](float4 npc, ull nid) {
@@ -1850,6 +1859,58 @@ __global__ void k_products(KParams p) {
   const int nc = min(*p.ncand, p.candcap);
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nc; t += gridDim.x * blockDim.x)
     p.best[p.cand[t]] = ~0ull;
+}
+
+template <int SURF>
+__global__ void k_products(KParams p) {
+  pdl_launch_dependents();
+  pdl_wait();
+  products_body<SURF>(p, *p.step);
+}
+
+// Conflict resolution and products in one launch: the commit rounds, the
+// re-searches between them and the product placement of k_commit /
+// k_research / k_products, separated by grid barriers instead of kernel
+// boundaries.  All blocks must be resident (the launch is cooperative and
+// sized to one wave).  Each barrier wait is bounded: after kBarSpinLimit
+// polls a block records kStBarrier and proceeds, so a barrier can never hang
+// the device (the step's results are then reported as an error).
+constexpr long long kBarSpinLimit = 1ll << 24;
+
+__device__ __forceinline__ void grid_barrier(unsigned int *bar, unsigned int target, int *status) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(bar, 1u);
+    long long spins = 0;
+    while (*(volatile unsigned int *)bar < target) {
+      if (++spins > kBarSpinLimit) {
+        atomicOr(status, kStBarrier);
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+template <int SURF>
+__global__ void __launch_bounds__(128) k_resolve(KParams p) {
+  pdl_launch_dependents();
+  pdl_wait();
+  const uint32_t step = *p.step;
+  const unsigned int nb = gridDim.x;
+  unsigned int target = 0;
+  commit_body<SURF>(p, step);
+  for (int round = 1; round < c_net.rounds; ++round) {
+    grid_barrier(p.bar, target += nb, p.status);
+    research_body<SURF>(p, step);
+    grid_barrier(p.bar, target += nb, p.status);
+    commit_body<SURF>(p, step);
+  }
+  grid_barrier(p.bar, target += nb, p.status);
+  products_body<SURF>(p, step);
 }
 
 // ===========================================================================
@@ -2422,6 +2483,8 @@ class EngineImpl {
   cudaStream_t own_stream = nullptr, stream = nullptr;
   bool use_graph = true;
   cudaGraphExec_t graph2 = nullptr;  // two steps (even + odd parity)
+  cudaGraphExec_t graph8 = nullptr;  // kGraphBlock steps (kGraphBlock / 2 even-odd pairs)
+  static constexpr int kGraphBlock = 8;
   cudaGraphExec_t graph1[2] = {nullptr, nullptr};  // one step of each parity
   long long nlaunch = 0;
   long long nsteps = 0;
@@ -2641,6 +2704,7 @@ class EngineImpl {
     p.counters = d_counters;
     p.spcount = d_spcount;
     p.status = d_counts + 6;
+    p.bar = reinterpret_cast<unsigned int *>(d_counts + 8);
     p.step = d_step;
     p.inj_key = d_injkey;
     p.inj_val = d_injval;
@@ -2752,17 +2816,31 @@ class EngineImpl {
   bool use_pdl = true;
   template <typename... Args, typename... Act>
   void launch(void (*k)(Args...), int grid, int block, size_t smem, Act &&...args) {
+    launch_ex(k, grid, block, smem, false, std::forward<Act>(args)...);
+  }
+  // cooperative: all blocks resident at once (k_resolve's grid barriers)
+  template <typename... Args, typename... Act>
+  cudaError_t launch_ex(void (*k)(Args...), int grid, int block, size_t smem, bool cooperative, Act &&...args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)grid);
     cfg.blockDim = dim3((unsigned)block);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = stream;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchAttribute at[2];
+    int na = 0;
+    if (use_pdl) {
+      at[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      at[na].val.programmaticStreamSerializationAllowed = 1;
+      ++na;
+    }
+    if (cooperative) {
+      at[na].id = cudaLaunchAttributeCooperative;
+      at[na].val.cooperative = 1;
+      ++na;
+    }
     cfg.attrs = at;
-    cfg.numAttrs = use_pdl ? 1 : 0;
-    cudaLaunchKernelEx(&cfg, k, std::forward<Act>(args)...);
+    cfg.numAttrs = na;
+    return cudaLaunchKernelEx(&cfg, k, std::forward<Act>(args)...);
   }
 
   bool single_rep() const { return reps.size() == 1; }
@@ -2902,6 +2980,14 @@ class EngineImpl {
     mark("k_pairs");
     launch(k_pairs_faces<SINGLE, SURF>, grid_mol(), 256, 0, p);
     mark("k_pairs_faces");
+    if (use_resolve) {
+      if (launch_ex(k_resolve<SURF>, resolve_grid<SURF>(), 128, 0, true, p) == cudaSuccess) {
+        mark("k_resolve");
+        return;
+      }
+      cudaGetLastError();  // not launchable here: the separate kernels from now on
+      use_resolve = false;
+    }
     launch(k_commit<SURF>, grid_small(), 128, 0, p);
     mark("k_commit");
     for (int round = 1; round < dnet.rounds; ++round) {
@@ -2912,6 +2998,21 @@ class EngineImpl {
     }
     launch(k_products<SURF>, grid_small(), 128, 0, p);
     mark("k_products");
+  }
+
+  // One wave of k_resolve blocks (every block resident, as its grid barriers
+  // require): the SM count times the blocks the kernel fits per SM, at most 4.
+  bool use_resolve = true;
+  int resolve_blocks[3] = {0, 0, 0};
+  template <int SURF>
+  int resolve_grid() {
+    int &b = resolve_blocks[SURF];
+    if (!b) {
+      int per_sm = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_resolve<SURF>, 128, 0);
+      b = sm_count() * std::max(1, std::min(per_sm, 4));
+    }
+    return b;
   }
 
   // Enqueue one step with the given parity (inputs A/P = buffers `par`).
@@ -2933,7 +3034,7 @@ class EngineImpl {
     }
   }
 
-  int launches_per_step() const { return 8 + 2 * (dnet.rounds - 1); }
+  int launches_per_step() const { return use_resolve ? 7 : 8 + 2 * (dnet.rounds - 1); }
 
   int upload_const(std::string *err) {
     CK(cudaMemcpyToSymbolAsync(c_net, &dnet, sizeof(DevNet), 0, cudaMemcpyHostToDevice, stream));
@@ -3029,20 +3130,24 @@ class EngineImpl {
   void invalidate_graph() {
     if (graph2) cudaGraphExecDestroy(graph2);
     graph2 = nullptr;
+    if (graph8) cudaGraphExecDestroy(graph8);
+    graph8 = nullptr;
     for (int k = 0; k < 2; ++k) {
       if (graph1[k]) cudaGraphExecDestroy(graph1[k]);
       graph1[k] = nullptr;
     }
   }
 
-  // Capture the steps of parities first..last (one or two steps) into *out.
-  int capture_steps(int first, int last, cudaGraphExec_t *out, std::string *err) {
+  // Capture the steps of parities first..last (one or two steps), `reps`
+  // times over, into *out.
+  int capture_steps(int first, int last, cudaGraphExec_t *out, std::string *err, int reps = 1) {
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     const long long before = nlaunch;
     const bool was = prof;
     prof = false;
-    for (int par = first; par <= last; ++par) enqueue_step(par, false);
+    for (int k = 0; k < reps; ++k)
+      for (int par = first; par <= last; ++par) enqueue_step(par, false);
     if (first == last && h_tail_status) {
       cudaMemcpyAsync(h_tail_status + first, d_counts + 6, sizeof(int), cudaMemcpyDeviceToHost, stream);
       if (h_tail_counts)
@@ -3058,11 +3163,17 @@ class EngineImpl {
     }
     if (e != cudaSuccess) {
       *out = nullptr;
+      if (use_resolve) {  // the fused resolve kernel (cooperative) could not be captured
+        cudaGetLastError();
+        invalidate_graph();
+        use_resolve = false;
+        return capture_steps(first, last, out, err, reps);
+      }
       if (use_pdl) {  // capture without programmatic edges instead
         cudaGetLastError();
         invalidate_graph();
         use_pdl = false;
-        return capture_steps(first, last, out, err);
+        return capture_steps(first, last, out, err, reps);
       }
       if (err) *err = std::string("step graph: ") + cudaGetErrorString(e);
       return -8;
@@ -3074,6 +3185,13 @@ class EngineImpl {
     if (graph2) cudaGraphExecDestroy(graph2);
     graph2 = nullptr;
     return capture_steps(0, 1, &graph2, err);
+  }
+  // Longer replays amortise the graph-launch boundary, at which the
+  // programmatic overlap between consecutive kernels is lost.
+  int build_graph8(std::string *err) {
+    if (graph8) cudaGraphExecDestroy(graph8);
+    graph8 = nullptr;
+    return capture_steps(0, 1, &graph8, err, kGraphBlock / 2);
   }
 
   size_t persist_smem() const { return adv_smem() + 2 * (kPersistSmemBoxes + 1) * sizeof(int); }
@@ -3695,6 +3813,16 @@ int Engine::run(long long nsteps, std::string *err) {
       int rc = E.run_one(err);
       if (rc) return rc;
       done++;
+    }
+    if (nsteps - done >= EngineImpl::kGraphBlock && !E.graph8) {
+      int rc = E.build_graph8(err);
+      if (rc) return rc;
+    }
+    while (nsteps - done >= EngineImpl::kGraphBlock) {
+      CK(cudaGraphLaunch(E.graph8, E.stream));
+      E.nlaunch += EngineImpl::kGraphBlock * E.launches_per_step();
+      done += EngineImpl::kGraphBlock;
+      E.tail_slot = -1;
     }
     if (nsteps - done >= 2 && !E.graph2) {
       int rc = E.build_graph(err);

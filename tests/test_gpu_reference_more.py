@@ -2,7 +2,7 @@
 births with first-order decay, branching first-order reactions, drift.
 
 Each case runs the same text configuration through the reference binary
-(oracle/_ref/smoldyn, 12 seeds in parallel, molcount at the end) and through
+(oracle/_ref/smoldyn, 32 seeds in parallel, molcount at the end) and through
 the engine as an ensemble of 48 replicates built from the same configuration
 (config reader → template simulation → smolgpuNewEnsemble).  The mean end
 count of each species agrees within 3 combined standard errors (+1 molecule
@@ -22,7 +22,7 @@ from tests import oracle_lib
 pytestmark = pytest.mark.gpu
 
 REF_EXE = os.path.join(oracle_lib.REF_DIR, "smoldyn")
-SEEDS, NREP = 12, 48
+SEEDS, NREP = 32, 48
 
 HEAD = """dim 3
 species A B C

@@ -6,14 +6,20 @@ placement for the reverse reaction; 10^4 A and 10^4 B placed uniformly;
 dt = 0.01; 1000 steps.
 
 The reference binary (oracle/_ref/smoldyn, built from the reference sources)
-runs 16 seeds in parallel and records molcount every 50 steps; the engine runs
+runs 32 seeds in parallel and records molcount every 50 steps; the engine runs
 128 replicates of the same workload in one ensemble.  Checks:
   - the mean C count agrees at every recorded time within 3 combined standard
     errors (+1 molecule for the discreteness of counts);
   - two-sample KS tests on the C counts at t = 5 and t = 10 do not reject
     (p > 0.001);
   - the effective forward rate constant measured from the first 2 time units,
-    k = <C(2)> / (2 * A * B / V), agrees within 3 combined standard errors.
+    k = <C(2)> / (2 * A * B / V), agrees within 3 combined standard errors;
+  - the steady-state forward rate constant, from the rate balance
+    dC/dt = kf A B / V - kr C over t in [0.5, 10] (after the initial
+    transient of the pair distribution, whose relaxation time is of order
+    binding radius^2 / D, a fraction of a step):
+        kf = (C(10) - C(0.5) + kr * integral C dt) / integral A B / V dt,
+    per seed and per replicate, agrees within 3 combined standard errors.
 """
 import os
 import subprocess
@@ -30,7 +36,7 @@ pytestmark = pytest.mark.gpu
 
 REF_EXE = os.path.join(oracle_lib.REF_DIR, "smoldyn")
 SIDE, N, KF, KR, DT, STEPS, EVERY = 100.0, 10000, 0.05, 0.1, 0.01, 1000, 50
-SEEDS = 16
+SEEDS = 32
 NREP = 128
 
 CONFIG = """dim 3
@@ -90,12 +96,12 @@ def engine_runs():
     e.add_molecules("A", np.full(NREP, N))
     e.add_molecules("B", np.full(NREP, N))
     e.update()
-    times, cs = [0.0], [e.counts(4)[:, 3].copy()]
+    times, cs = [0.0], [e.counts(4)[:, 1:4].copy()]
     for k in range(STEPS // EVERY):
         e.run_steps(EVERY)
         times.append((k + 1) * EVERY * DT)
-        cs.append(e.counts(4)[:, 3].copy())
-    return np.array(times), np.array(cs).T  # [rep, time]
+        cs.append(e.counts(4)[:, 1:4].copy())
+    return np.array(times), np.array(cs).transpose(1, 0, 2)  # [rep, time, species A B C]
 
 
 @pytest.fixture(scope="module")
@@ -103,8 +109,17 @@ def runs():
     if not os.path.exists(REF_EXE):
         pytest.skip("reference binary not built")
     ref = reference_runs()
-    times, gpu = engine_runs()
-    return ref, times, gpu
+    times, full = engine_runs()
+    return ref, times, full[:, :, 2], full
+
+
+def _steady_kf(t, a, b, c, t1=0.5, t2=10.0):
+    """Forward rate constant from the rate balance over [t1, t2] (trapezoid
+    rule over the recorded times)."""
+    sel = (t >= t1 - 1e-9) & (t <= t2 + 1e-9)
+    t, a, b, c = t[sel], a[sel].astype(float), b[sel].astype(float), c[sel].astype(float)
+    expo = np.trapezoid(a * b / SIDE ** 3, t)
+    return (c[-1] - c[0] + KR * np.trapezoid(c, t)) / expo
 
 
 def _ref_at(ref, t):
@@ -117,7 +132,7 @@ def _ref_at(ref, t):
 
 
 def test_mean_trajectory_within_3_sigma(runs):
-    ref, times, gpu = runs
+    ref, times, gpu, _ = runs
     worst = 0.0
     for k, t in enumerate(times):
         r = _ref_at(ref, t)
@@ -131,7 +146,7 @@ def test_mean_trajectory_within_3_sigma(runs):
 
 @pytest.mark.parametrize("t", [5.0, 10.0])
 def test_ks_on_counts(runs, t):
-    ref, times, gpu = runs
+    ref, times, gpu, _ = runs
     k = int(np.argmin(np.abs(times - t)))
     p = stats.ks_2samp(_ref_at(ref, t), gpu[:, k]).pvalue
     print("KS p-value of C counts at t=%g: %.3f" % (t, p))
@@ -139,7 +154,7 @@ def test_ks_on_counts(runs, t):
 
 
 def test_effective_forward_rate(runs):
-    ref, times, gpu = runs
+    ref, times, gpu, _ = runs
     t = 2.0
     k = int(np.argmin(np.abs(times - t)))
     scale = t * N * N / SIDE ** 3
@@ -148,4 +163,14 @@ def test_effective_forward_rate(runs):
     se = np.sqrt(kr_.var(ddof=1) / len(kr_) + kg.var(ddof=1) / len(kg))
     print("effective kf: reference %.4f +- %.4f, engine %.4f +- %.4f" %
           (kr_.mean(), kr_.std(ddof=1) / np.sqrt(len(kr_)), kg.mean(), kg.std(ddof=1) / np.sqrt(len(kg))))
+    assert abs(kr_.mean() - kg.mean()) <= 3 * se
+
+
+def test_steady_state_forward_rate(runs):
+    ref, times, _, full = runs
+    kr_ = np.array([_steady_kf(rows[:, 0], rows[:, 1], rows[:, 2], rows[:, 3]) for rows in ref])
+    kg = np.array([_steady_kf(times, full[k, :, 0], full[k, :, 1], full[k, :, 2]) for k in range(len(full))])
+    se = np.sqrt(kr_.var(ddof=1) / len(kr_) + kg.var(ddof=1) / len(kg))
+    print("steady-state kf: reference %.5f +- %.5f, engine %.5f +- %.5f (requested %.3f)" %
+          (kr_.mean(), kr_.std(ddof=1) / np.sqrt(len(kr_)), kg.mean(), kg.std(ddof=1) / np.sqrt(len(kg)), KF))
     assert abs(kr_.mean() - kg.mean()) <= 3 * se

@@ -80,13 +80,16 @@ def run_engine(cfg_dir, cfg_name, out="out.txt"):
 def test_absorbing_plane_matches_reference():
     if not os.path.exists(REF_EXE):
         pytest.skip("reference binary not built")
+    from concurrent.futures import ThreadPoolExecutor
+    seeds = range(1, 33)  # 32 seeds each
     ref, eng = [], []
     with tempfile.TemporaryDirectory() as d:
-        for seed in range(1, 13):
-            out = "out%d.txt" % seed
-            absorbing_plane_config(os.path.join(d, "c%d.txt" % seed), seed, out=out)
-            ref.append(run_reference(d, "c%d.txt" % seed, out))
-            n, s = run_engine(d, "c%d.txt" % seed, out)
+        for seed in seeds:
+            absorbing_plane_config(os.path.join(d, "c%d.txt" % seed), seed, out="out%d.txt" % seed)
+        with ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
+            ref = list(ex.map(lambda k: run_reference(d, "c%d.txt" % k, "out%d.txt" % k), seeds))
+        for seed in seeds:
+            n, s = run_engine(d, "c%d.txt" % seed, "out%d.txt" % seed)
             eng.append(n)
             s.close()
     ref, eng = np.array(ref), np.array(eng)
