@@ -1465,8 +1465,9 @@ __device__ __forceinline__ void face_box_walk(const KParams &p, int i, float4 pc
 }
 
 // Cross-box pairs for the molecules flagged in the face bitmask by
-// k_pairs_tile.  Each warp reads 32 bitmask words (1024 molecules) at once,
-// numbers their set bits with a warp prefix sum and takes the flagged
+// k_pairs_tile.  Each warp reads up to 32 bitmask words (1024 molecules; fewer
+// when the system is too small to give every warp 32) at once, numbers their
+// set bits with a warp prefix sum and takes the flagged
 // molecules 32 at a time, one per lane; each such molecule lists the upward
 // neighbour boxes its stencil reaches, and a second prefix sum hands the
 // (molecule, neighbour box) items out 32 at a time, so a molecule reaching
@@ -1482,9 +1483,13 @@ __global__ void __launch_bounds__(256) k_pairs_faces(KParams p) {
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
+  // words per warp: 32 when there are enough words to keep every warp busy,
+  // fewer for small systems (a power of two from 1 to 32)
+  int wpw = 32;
+  while (wpw > 1 && (long long)nw * wpw > nwords) wpw >>= 1;
   int extra = 0;
-  for (int base = gw * 32; base < nwords; base += nw * 32) {
-    const uint32_t bits = (base + lane < nwords) ? facebits[base + lane] : 0u;
+  for (int base = gw * wpw; base < nwords; base += nw * wpw) {
+    const uint32_t bits = (lane < wpw && base + lane < nwords) ? facebits[base + lane] : 0u;
     const int cnt = __popc(bits);
     int incl = cnt;
 #pragma unroll
