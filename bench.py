@@ -532,6 +532,9 @@ def run_batched(sb, torch, args, rank):
     t0 = time.perf_counter()
     e.update()
     setup = time.perf_counter() - t0
+    t_tune = time.perf_counter()
+    tune_ms = e.autotune(10) if not args.no_tune else None
+    t_tune = time.perf_counter() - t_tune
     stream = torch.cuda.Stream()
     e.set_stream(stream.cuda_stream)
     e.run_steps(args.warmup)
@@ -551,6 +554,7 @@ def run_batched(sb, torch, args, rank):
                        "reflective cubes, A+B<->C, dt=0.01, radii by the device FP64 solver",
            "engine": engine, "value": tot * steps / sec, "unit": METRIC, "molecules": int(tot), "replicates": R,
            "steps": steps, "ms_per_step": sec * 1e3 / steps, "setup_s": setup, "gpu_launches": launches,
+           "tuning": e.tuning(), "autotune_s": t_tune, "autotune_best_trial_ms": tune_ms,
            "events": {"rxn1": ev[2], "rxn2": ev[3], "overflow": ev[6]},
            "persistent_kernel": {"value": tot * psteps / psec, "steps": psteps, "ms_per_step": psec * 1e3 / psteps,
                                  "note": "one thread block per replicate, up to 100 steps per launch"}}

@@ -82,7 +82,6 @@ struct KParams {
   unsigned long long *counters;  // [0]=wall [1]=rxn0 [2]=rxn1 [3]=rxn2 [4]=unresolved [5]=multicand
   long long *spcount;            // [rep*nsp + sp]
   int *status;
-  unsigned int *bar;             // grid barrier counter of k_resolve (zeroed by k_begin)
   uint32_t *step;
   // deterministic mode
   const ull *inj_key;            // sorted stream keys
@@ -92,9 +91,7 @@ struct KParams {
 
 constexpr uint32_t kTmpGone = 0xFFFFFFFFu;  // tmp[i].w of a molecule that left
 
-enum StatusBits {
-  kStMolCap = 1, kStEvCap = 2, kStProdCap = 4, kStCandCap = 8, kStScanWait = 16, kStUpload = 32, kStBarrier = 64
-};
+enum StatusBits { kStMolCap = 1, kStEvCap = 2, kStProdCap = 4, kStCandCap = 8, kStScanWait = 16, kStUpload = 32 };
 
 // Programmatic dependent launch: the step's kernels are launched so that the
 // next kernel can be scheduled while the current one runs.  Each kernel lets
@@ -629,7 +626,6 @@ __global__ void k_begin(KParams p, int bump_step) {
     *p.nev = 0;
     *p.ncand = 0;
     *p.q_n = 0;
-    *p.bar = 0;
   }
 }
 
@@ -1483,10 +1479,11 @@ __global__ void __launch_bounds__(256) k_pairs_faces(KParams p) {
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
-  // words per warp: 32 when there are enough words to keep every warp busy,
-  // fewer for small systems (a power of two from 1 to 32)
+  // words per warp: 32 (most words are sparse, and a group's fixed cost is
+  // paid once for 32 of them) unless the system is so small that fewer than
+  // one warp in eight would get a group; then fewer (a power of two, >= 1)
   int wpw = 32;
-  while (wpw > 1 && (long long)nw * wpw > nwords) wpw >>= 1;
+  while (wpw > 1 && 8ll * nwords < (long long)nw * wpw) wpw >>= 1;
   int extra = 0;
   for (int base = gw * wpw; base < nwords; base += nw * wpw) {
     const uint32_t bits = (lane < wpw && base + lane < nwords) ? facebits[base + lane] : 0u;
@@ -1871,51 +1868,6 @@ __global__ void k_products(KParams p) {
   pdl_launch_dependents();
   pdl_wait();
   products_body<SURF>(p, *p.step);
-}
-
-// Conflict resolution and products in one launch: the commit rounds, the
-// re-searches between them and the product placement of k_commit /
-// k_research / k_products, separated by grid barriers instead of kernel
-// boundaries.  All blocks must be resident (the launch is cooperative and
-// sized to one wave).  Each barrier wait is bounded: after kBarSpinLimit
-// polls a block records kStBarrier and proceeds, so a barrier can never hang
-// the device (the step's results are then reported as an error).
-constexpr long long kBarSpinLimit = 1ll << 24;
-
-__device__ __forceinline__ void grid_barrier(unsigned int *bar, unsigned int target, int *status) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(bar, 1u);
-    long long spins = 0;
-    while (*(volatile unsigned int *)bar < target) {
-      if (++spins > kBarSpinLimit) {
-        atomicOr(status, kStBarrier);
-        break;
-      }
-      __nanosleep(64);
-    }
-    __threadfence();
-  }
-  __syncthreads();
-}
-
-template <int SURF>
-__global__ void __launch_bounds__(128) k_resolve(KParams p) {
-  pdl_launch_dependents();
-  pdl_wait();
-  const uint32_t step = *p.step;
-  const unsigned int nb = gridDim.x;
-  unsigned int target = 0;
-  commit_body<SURF>(p, step);
-  for (int round = 1; round < c_net.rounds; ++round) {
-    grid_barrier(p.bar, target += nb, p.status);
-    research_body<SURF>(p, step);
-    grid_barrier(p.bar, target += nb, p.status);
-    commit_body<SURF>(p, step);
-  }
-  grid_barrier(p.bar, target += nb, p.status);
-  products_body<SURF>(p, step);
 }
 
 // ===========================================================================
@@ -2488,8 +2440,6 @@ class EngineImpl {
   cudaStream_t own_stream = nullptr, stream = nullptr;
   bool use_graph = true;
   cudaGraphExec_t graph2 = nullptr;  // two steps (even + odd parity)
-  cudaGraphExec_t graph8 = nullptr;  // kGraphBlock steps (kGraphBlock / 2 even-odd pairs)
-  static constexpr int kGraphBlock = 8;
   cudaGraphExec_t graph1[2] = {nullptr, nullptr};  // one step of each parity
   long long nlaunch = 0;
   long long nsteps = 0;
@@ -2709,7 +2659,6 @@ class EngineImpl {
     p.counters = d_counters;
     p.spcount = d_spcount;
     p.status = d_counts + 6;
-    p.bar = reinterpret_cast<unsigned int *>(d_counts + 8);
     p.step = d_step;
     p.inj_key = d_injkey;
     p.inj_val = d_injval;
@@ -2821,31 +2770,17 @@ class EngineImpl {
   bool use_pdl = true;
   template <typename... Args, typename... Act>
   void launch(void (*k)(Args...), int grid, int block, size_t smem, Act &&...args) {
-    launch_ex(k, grid, block, smem, false, std::forward<Act>(args)...);
-  }
-  // cooperative: all blocks resident at once (k_resolve's grid barriers)
-  template <typename... Args, typename... Act>
-  cudaError_t launch_ex(void (*k)(Args...), int grid, int block, size_t smem, bool cooperative, Act &&...args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)grid);
     cfg.blockDim = dim3((unsigned)block);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = stream;
-    cudaLaunchAttribute at[2];
-    int na = 0;
-    if (use_pdl) {
-      at[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-      at[na].val.programmaticStreamSerializationAllowed = 1;
-      ++na;
-    }
-    if (cooperative) {
-      at[na].id = cudaLaunchAttributeCooperative;
-      at[na].val.cooperative = 1;
-      ++na;
-    }
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
-    cfg.numAttrs = na;
-    return cudaLaunchKernelEx(&cfg, k, std::forward<Act>(args)...);
+    cfg.numAttrs = use_pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, k, std::forward<Act>(args)...);
   }
 
   bool single_rep() const { return reps.size() == 1; }
@@ -2985,14 +2920,6 @@ class EngineImpl {
     mark("k_pairs");
     launch(k_pairs_faces<SINGLE, SURF>, grid_mol(), 256, 0, p);
     mark("k_pairs_faces");
-    if (use_resolve) {
-      if (launch_ex(k_resolve<SURF>, resolve_grid<SURF>(), 128, 0, true, p) == cudaSuccess) {
-        mark("k_resolve");
-        return;
-      }
-      cudaGetLastError();  // not launchable here: the separate kernels from now on
-      use_resolve = false;
-    }
     launch(k_commit<SURF>, grid_small(), 128, 0, p);
     mark("k_commit");
     for (int round = 1; round < dnet.rounds; ++round) {
@@ -3005,20 +2932,6 @@ class EngineImpl {
     mark("k_products");
   }
 
-  // One wave of k_resolve blocks (every block resident, as its grid barriers
-  // require): the SM count times the blocks the kernel fits per SM, at most 4.
-  bool use_resolve = true;
-  int resolve_blocks[3] = {0, 0, 0};
-  template <int SURF>
-  int resolve_grid() {
-    int &b = resolve_blocks[SURF];
-    if (!b) {
-      int per_sm = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_resolve<SURF>, 128, 0);
-      b = sm_count() * std::max(1, std::min(per_sm, 4));
-    }
-    return b;
-  }
 
   // Enqueue one step with the given parity (inputs A/P = buffers `par`).
   void enqueue_step(int par, bool rebin_only) {
@@ -3039,7 +2952,7 @@ class EngineImpl {
     }
   }
 
-  int launches_per_step() const { return use_resolve ? 7 : 8 + 2 * (dnet.rounds - 1); }
+  int launches_per_step() const { return 8 + 2 * (dnet.rounds - 1); }
 
   int upload_const(std::string *err) {
     CK(cudaMemcpyToSymbolAsync(c_net, &dnet, sizeof(DevNet), 0, cudaMemcpyHostToDevice, stream));
@@ -3135,8 +3048,6 @@ class EngineImpl {
   void invalidate_graph() {
     if (graph2) cudaGraphExecDestroy(graph2);
     graph2 = nullptr;
-    if (graph8) cudaGraphExecDestroy(graph8);
-    graph8 = nullptr;
     for (int k = 0; k < 2; ++k) {
       if (graph1[k]) cudaGraphExecDestroy(graph1[k]);
       graph1[k] = nullptr;
@@ -3168,12 +3079,6 @@ class EngineImpl {
     }
     if (e != cudaSuccess) {
       *out = nullptr;
-      if (use_resolve) {  // the fused resolve kernel (cooperative) could not be captured
-        cudaGetLastError();
-        invalidate_graph();
-        use_resolve = false;
-        return capture_steps(first, last, out, err, reps);
-      }
       if (use_pdl) {  // capture without programmatic edges instead
         cudaGetLastError();
         invalidate_graph();
@@ -3191,13 +3096,7 @@ class EngineImpl {
     graph2 = nullptr;
     return capture_steps(0, 1, &graph2, err);
   }
-  // Longer replays amortise the graph-launch boundary, at which the
-  // programmatic overlap between consecutive kernels is lost.
-  int build_graph8(std::string *err) {
-    if (graph8) cudaGraphExecDestroy(graph8);
-    graph8 = nullptr;
-    return capture_steps(0, 1, &graph8, err, kGraphBlock / 2);
-  }
+
 
   size_t persist_smem() const { return adv_smem() + 2 * (kPersistSmemBoxes + 1) * sizeof(int); }
 
@@ -3818,16 +3717,6 @@ int Engine::run(long long nsteps, std::string *err) {
       int rc = E.run_one(err);
       if (rc) return rc;
       done++;
-    }
-    if (nsteps - done >= EngineImpl::kGraphBlock && !E.graph8) {
-      int rc = E.build_graph8(err);
-      if (rc) return rc;
-    }
-    while (nsteps - done >= EngineImpl::kGraphBlock) {
-      CK(cudaGraphLaunch(E.graph8, E.stream));
-      E.nlaunch += EngineImpl::kGraphBlock * E.launches_per_step();
-      done += EngineImpl::kGraphBlock;
-      E.tail_slot = -1;
     }
     if (nsteps - done >= 2 && !E.graph2) {
       int rc = E.build_graph(err);
