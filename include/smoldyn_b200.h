@@ -186,18 +186,6 @@ double smolgpuGetTime(simptr sim);
 long long smolgpuGetStepCount(simptr sim);
 /* Number of live molecules (all species). */
 long long smolgpuGetTotalMolecules(simptr sim);
-/* Molecule layout of the engine (no reference counterpart).  With enable = 1
- * (the default) a simulation without surfaces, compartments, injected
- * displacements or displacement trackers keeps its molecules in fixed-
- * capacity per-box buckets (32 slots per virtual box, a spill list for full
- * boxes): each step moves every molecule straight into its destination box,
- * with no box scan and no permutation pass.  enable = 0 keeps the sorted
- * layout (one box-sorted array with box start offsets).  Trajectories are the
- * same in both layouts (same per-molecule code and random streams) up to the
- * ranking of equidistant reaction candidates.  smolgpuGetBucketLayout
- * returns 1 while the state is held in buckets. */
-enum ErrorCode smolgpuSetBucketLayout(simptr sim, int enable);
-int smolgpuGetBucketLayout(simptr sim);
 /* Copy all molecules to host arrays (pos: 3*n doubles, absolute coordinates;
  * species: n ints; serno: n uint64).  *n is in: capacity, out: count. */
 enum ErrorCode smolgpuGetMolecules(simptr sim, long long *n, double *pos, int *species,

@@ -132,8 +132,6 @@ PROTOTYPES = {
     "smolgpuEnsembleAttachSurrogate": (C.c_int, [_vp, _vp]),
     "smolgpuEnsembleUpdate": (C.c_int, [_vp]),
     "smolgpuEnsembleSetEngine": (C.c_int, [_vp, C.c_int]),
-    "smolgpuSetBucketLayout": (C.c_int, [_sim, C.c_int]),
-    "smolgpuGetBucketLayout": (C.c_int, [_sim]),
     "smolgpuEnsembleGetEngine": (C.c_int, [_vp]),
     "smolgpuEnsembleGetEventCounts": (C.c_int, [_vp, C.POINTER(C.c_longlong)]),
     "smolgpuEnsembleGetMolecules": (C.c_int, [_vp, C.POINTER(C.c_longlong), _dp, _ip, _ip, _u64p]),
@@ -312,13 +310,6 @@ class Sim:
 
     def synchronize(self):
         return check(self.lib.smolgpuSynchronize(self.ptr))
-
-    def bucket_layout(self, enable=None):
-        """Choose the bucketed molecule layout (1, default) or the sorted one
-        (0) when enable is given; return 1 while the state is in buckets."""
-        if enable is not None:
-            check(self.lib.smolgpuSetBucketLayout(self.ptr, int(enable)))
-        return self.lib.smolgpuGetBucketLayout(self.ptr)
 
     def autotune(self, trial_steps=20):
         """Pick box width and kernel launch shape by timed trials (before the

@@ -104,7 +104,6 @@ ErrorCode update_sim(Sim &s, const char *func) {
     if (!s.eng) s.eng.reset(new smolb::Engine());
     rc = s.eng->init(net, {rep}, s.dt, (uint64_t)s.seed, cap, &err);
     if (!rc) rc = s.eng->set_tuning(s.tuning, &err);
-    if (!rc) rc = s.eng->set_bucket_layout(s.bucket_layout, &err);
     if (rc) { s.eng.reset(); return set_error(func, from_rc(rc), err); }
     std::vector<uint64_t> sn;
     if (!s.pend_serno.empty()) {  // serials kept from a pull; molecules added since get new ones
@@ -1109,22 +1108,6 @@ enum ErrorCode smolgpuSetStream(simptr sim, void *stream) {
   if (ec != ECok) return ec;
   sim->s.eng->set_stream(stream);
   return ECok;
-}
-
-enum ErrorCode smolgpuSetBucketLayout(simptr sim, int enable) {
-  LCHECK(sim, ECmissing, "missing sim");
-  LCHECK(enable == 0 || enable == 1, ECbounds, "enable must be 0 or 1");
-  sim->s.bucket_layout = enable != 0;
-  if (sim->s.eng) {
-    std::string err;
-    if (sim->s.eng->set_bucket_layout(enable != 0, &err)) return set_error(__func__, ECerror, err);
-  }
-  return ECok;
-}
-
-int smolgpuGetBucketLayout(simptr sim) {
-  if (!sim) return (int)set_error(__func__, ECmissing, "missing sim");
-  return (sim->s.eng && sim->s.eng->bucket_layout_active()) ? 1 : 0;
 }
 
 enum ErrorCode smolgpuAutotune(simptr sim, int trial_steps, double *ms_per_step) {

@@ -70,13 +70,6 @@ struct KParams {
   int cap, pcap;
   int *cnt;
   int *start;
-  // bucketed layout: per-box molecule counts of the input and output buffers,
-  // and the staged molecules of an upload
-  int *a_cnt;
-  int *b_cnt;
-  const float4 *u_pc;
-  const ull *u_id;
-  int u_n;
   int ncell;
   Event *ev;
   int *nev;
@@ -1367,11 +1360,6 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_pairs_tile(KParams p) {
   if (extra) atomicAdd(&p.counters[5], (unsigned long long)extra);
 }
 
-// Bucketed layout (see the section of that name below): box b owns slots
-// [b*kBucket, (b+1)*kBucket), the first min(count, kBucket) of them filled.
-constexpr int kBucket = 32;
-constexpr int kBucketShift = 5;
-
 // Position of the k-th (from 0) set bit of m; k < popc(m).
 __device__ __forceinline__ int nth_set_bit(uint32_t m, int k) {
   int pos = 0;
@@ -1442,7 +1430,7 @@ __device__ __forceinline__ uint32_t face_boxes(const KParams &p, float4 pc, ull 
 // Cross-box pairs of molecule i with the molecules of one upward neighbour
 // box (offset code k of face_boxes); the closest reacting partner found is
 // registered on i, every reacting pair on the partner.
-template <bool SINGLE, int SURF, bool BUCKET>
+template <bool SINGLE, int SURF>
 __device__ __forceinline__ void face_box_walk(const KParams &p, int i, float4 pc, ull idi, int k, int n,
                                               uint32_t step, int &extra) {
   const int sp = id_species(idi);
@@ -1458,10 +1446,7 @@ __device__ __forceinline__ void face_box_walk(const KParams &p, int i, float4 pc
   if (y < 0) y += g.n[1]; else if (y >= g.n[1]) y -= g.n[1];
   if (z < 0) z += g.n[2]; else if (z >= g.n[2]) z -= g.n[2];
   const int c = g.cell0 + (z * g.n[1] + y) * g.n[0] + x;
-  // bucketed: the box's slots (its spill entries, if any, search for
-  // themselves in the spill pass)
-  const int s0 = BUCKET ? (c << kBucketShift) : p.start[c];
-  const int e0 = BUCKET ? s0 + min(p.b_cnt[c], kBucket) : min(p.start[c + 1], n);
+  const int s0 = p.start[c], e0 = min(p.start[c + 1], n);
   ull best = ~0ull;
   for (int j = s0; j < e0; ++j) {
     const float4 q = p.b_pc[j];
@@ -1475,95 +1460,6 @@ __device__ __forceinline__ void face_box_walk(const KParams &p, int i, float4 pc
   if (best != ~0ull) extra += register_candidate(p, i, best);
 }
 
-// Partners of a bucketed molecule i within its stencil (bucket slots of the
-// stencil's boxes, and spill entries of those boxes that overflowed):
-// returns the closest reacting one as (dist2 bits << 32 | index), or ~0.
-// skip_below: spill entries with a lower spill index are not partners (the
-// spill pass tests each spill-spill pair once).
-__device__ ull bucket_partners(const KParams &p, int i, float4 pc, ull id, uint32_t step, int &ncand, bool reg,
-                               int spill_from) {
-  const DevGeo &g = c_geo0;
-  const int sp = id_species(id);
-  const uint32_t mask = c_net.pair_mask[sp];
-  const float rs = p.rsearch[sp];
-  const float rs2 = rs * rs;
-  int ix, iy, iz;
-  unpack_cell(__float_as_uint(pc.w), ix, iy, iz);
-  const bool px = g.wall[0] == kWallPeriodic, py = g.wall[2] == kWallPeriodic, pz = g.wall[4] == kWallPeriodic;
-  const float ub0 = (ix == g.n[0] - 1) ? g.whi[0] : g.h[0];
-  const float ub1 = (iy == g.n[1] - 1) ? g.whi[1] : g.h[1];
-  const float ub2 = (iz == g.n[2] - 1) ? g.whi[2] : g.h[2];
-  const int xlo = pc.x < rs ? -1 : 0, xhi = pc.x > ub0 - rs ? 1 : 0;
-  const int ylo = pc.y < rs ? -1 : 0, yhi = pc.y > ub1 - rs ? 1 : 0;
-  const int zlo = pc.z < rs ? -1 : 0, zhi = pc.z > ub2 - rs ? 1 : 0;
-  const int spill0 = p.ncell << kBucketShift;
-  const int nsp = min(*p.q_n, p.pcap);
-  const ull ka = id_stream(id);
-  ull best = ~0ull;
-  ncand = 0;
-  for (int dz = zlo; dz <= zhi; ++dz) {
-    int z = iz + dz;
-    if (z < 0 || z >= g.n[2]) {
-      if (!pz) continue;
-      z = (z < 0) ? z + g.n[2] : z - g.n[2];
-    }
-    for (int dy = ylo; dy <= yhi; ++dy) {
-      int y = iy + dy;
-      if (y < 0 || y >= g.n[1]) {
-        if (!py) continue;
-        y = (y < 0) ? y + g.n[1] : y - g.n[1];
-      }
-      for (int dx = xlo; dx <= xhi; ++dx) {
-        int x = ix + dx;
-        if (x < 0 || x >= g.n[0]) {
-          if (!px) continue;
-          x = (x < 0) ? x + g.n[0] : x - g.n[0];
-        }
-        const int c = (z * g.n[1] + y) * g.n[0] + x;
-        const int cc = p.b_cnt[c];
-        const int s0 = c << kBucketShift, e0 = s0 + min(cc, kBucket);
-        for (int pass = 0; pass < 2; ++pass) {
-          if (pass == 1 && cc <= kBucket) break;  // spill entries of an overflowing box
-          const int lo = pass ? spill0 + spill_from : s0, hi = pass ? spill0 + nsp : e0;
-          for (int j = lo; j < hi; ++j) {
-            if (j == i) continue;
-            const float4 q = p.b_pc[j];
-            if (pass == 1 && (int)__float_as_uint(q.w) != (int)pack_cell(x, y, z)) continue;
-            const float vx = (q.x - pc.x) + (float)dx * g.h[0];
-            const float vy = (q.y - pc.y) + (float)dy * g.h[1];
-            const float vz = (q.z - pc.z) + (float)dz * g.h[2];
-            const float d2 = vx * vx + vy * vy + vz * vz;
-            if (d2 > rs2) continue;
-            const ull jd = p.b_id[j];
-            const int spj = id_species(jd);
-            if (spj == kDeadSpecies || !((mask >> spj) & 1u)) continue;
-            if (pair_reaction<false>(p, 0, sp, spj, d2, ka, id_stream(jd), step, i, j) < 0) continue;
-            ncand++;
-            const ull k = ((ull)__float_as_uint(d2) << 32) | (uint32_t)j;
-            if (k < best) best = k;
-            if (reg) register_candidate(p, j, ((ull)__float_as_uint(d2) << 32) | (uint32_t)i);
-          }
-        }
-      }
-    }
-  }
-  return best;
-}
-
-// Spill pass: spill entry t of the output buffer searches its whole stencil
-// (bucket slots, and spill entries after it) and registers every reacting
-// pair on both molecules; bucket molecules never visit spill entries, so
-// each pair is tested once.
-__device__ __noinline__ void spill_walk(const KParams &p, int t, uint32_t step, int &extra) {
-  const int i = (p.ncell << kBucketShift) + t;
-  const ull id = p.b_id[i];
-  const int sp = id_species(id);
-  if (sp == kDeadSpecies || !((c_net.pair_any >> sp) & 1u)) return;
-  int ncd = 0;
-  const ull best = bucket_partners(p, i, p.b_pc[i], id, step, ncd, true, t + 1);
-  if (best != ~0ull) extra += register_candidate(p, i, best);
-}
-
 // Cross-box pairs for the molecules flagged in the face bitmask by
 // k_pairs_tile.  Each warp reads up to 32 bitmask words (1024 molecules; fewer
 // when the system is too small to give every warp 32) at once, numbers their
@@ -1572,14 +1468,12 @@ __device__ __noinline__ void spill_walk(const KParams &p, int t, uint32_t step, 
 // neighbour boxes its stencil reaches, and a second prefix sum hands the
 // (molecule, neighbour box) items out 32 at a time, so a molecule reaching
 // several boxes spreads over several lanes.
-// BUCKET: one bitmask word per box (bit s = slot s), and after the face
-// items the spill pass (spill_walk) for molecules in the output spill list.
-template <bool SINGLE, int SURF, bool BUCKET = false>
+template <bool SINGLE, int SURF>
 __global__ void __launch_bounds__(256) k_pairs_faces(KParams p) {
   pdl_launch_dependents();
   pdl_wait();
-  const int n = BUCKET ? 0x7FFFFFFF : *p.b_n;
-  const int nwords = BUCKET ? p.ncell : (n + 31) >> 5;
+  const int n = *p.b_n;
+  const int nwords = (n + 31) >> 5;
   const uint32_t step = *p.step;
   const uint32_t *facebits = reinterpret_cast<const uint32_t *>(p.face);
   const int lane = threadIdx.x & 31;
@@ -1645,14 +1539,9 @@ __global__ void __launch_bounds__(256) k_pairs_faces(KParams p) {
         po.z = __shfl_sync(0xffffffffu, pc.z, oo);
         po.w = __shfl_sync(0xffffffffu, pc.w, oo);
         const ull ido = __shfl_sync(0xffffffffu, idi, oo);
-        if (qq < total2) face_box_walk<SINGLE, SURF, BUCKET>(p, io, po, ido, nth_set_bit(bo, rr), n, step, extra);
+        if (qq < total2) face_box_walk<SINGLE, SURF>(p, io, po, ido, nth_set_bit(bo, rr), n, step, extra);
       }
     }
-  }
-  if (BUCKET) {
-    const int nsp = min(*p.q_n, p.pcap);
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nsp; t += gridDim.x * blockDim.x)
-      spill_walk(p, t, step, extra);
   }
   if (extra) atomicAdd(&p.counters[5], (unsigned long long)extra);
 }
@@ -1979,315 +1868,6 @@ __global__ void k_products(KParams p) {
   pdl_launch_dependents();
   pdl_wait();
   products_body<SURF>(p, *p.step);
-}
-
-// ===========================================================================
-// Bucketed layout
-// ===========================================================================
-// A single simulation without surfaces, compartments or injected
-// displacements keeps its molecules in per-box buckets: box b owns the
-// kBucket slots [b*kBucket, (b+1)*kBucket) of each buffer, of which the
-// first min(count[b], kBucket) are filled; a molecule that finds its box full
-// goes to the buffer's spill list, stored after the last box's slots (index
-// ncell*kBucket + j), so every molecule has one index in one array.  The move
-// (k_bmove) reads each molecule once and writes it straight into its
-// destination box of the other buffer - one slot atomic per run of lanes
-// bound for the same box - so the step needs no box histogram scan, no
-// permutation pass and no scratch copy of the moved positions; the pair pass
-// (k_bpairs) takes the boxes' counts and enumerates the same-box pairs of 32
-// boxes flat across the warp.  Products of the step are inserted into the
-// output buckets directly.  Reference step order as for the other layout
-// (smolsim.cpp:2607-2692).
-
-// Moves the lane's molecule (have: the lane holds one) and inserts it into
-// its destination box of the output buffer; called by all 32 lanes.
-__device__ __forceinline__ void bucket_move_insert(const KParams &p, bool have, float4 pc, ull id, uint32_t step,
-                                                   const float *gtab, int rebin_only, int &hits) {
-  int fate = -1;
-  if (have && id_species(id) != kDeadSpecies) fate = advance_one<true, 0>(pc, id, step, p, gtab, rebin_only, hits);
-  const bool alive = fate == 0;
-  if (fate == 1) {
-    atomicAdd((unsigned long long *)&p.spcount[id_species(id)], (unsigned long long)(-1ll));
-  } else if (fate >= 2) {
-    Event e;
-    e.site = pc;
-    e.key = id_stream(id);
-    e.rxn = (1u << 8) | (uint32_t)(fate - 2);
-    e.rep = 0;
-    e.ia = e.ib = -1;
-    push_event(p, e);
-  }
-  const int cell = alive ? global_cell(c_geo0, __float_as_uint(pc.w)) : -1;
-  const BoxRun run = box_run(alive, cell);
-  int old = 0;
-  if (alive && run.rank == 0) old = atomicAdd(&p.b_cnt[cell], run.count);
-  old = __shfl_sync(0xffffffffu, old, alive ? run.head : (threadIdx.x & 31));
-  if (alive) {
-    const int slot = old + run.rank;
-    if (slot < kBucket) {
-      const int k = (cell << kBucketShift) + slot;
-      p.b_pc[k] = pc;
-      p.b_id[k] = id;
-    } else {
-      const int j = atomicAdd(p.q_n, 1);
-      if (j < p.pcap) {
-        const int k = (p.ncell << kBucketShift) + j;
-        p.b_pc[k] = pc;
-        p.b_id[k] = id;
-      } else {
-        atomicOr(p.status, kStMolCap);
-      }
-    }
-  }
-}
-
-// Warp prefix sum of v over the lanes: returns the exclusive prefix; *total
-// receives the sum.
-__device__ __forceinline__ int warp_excl_scan(int v, int &total) {
-  const int lane = threadIdx.x & 31;
-  int incl = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += y;
-  }
-  total = __shfl_sync(0xffffffffu, incl, 31);
-  return incl - v;
-}
-
-// Lane whose range [excl, excl + count) holds item q (excl non-decreasing).
-__device__ __forceinline__ int warp_owner(int excl, int q) {
-  int o = 0;
-#pragma unroll
-  for (int st = 16; st > 0; st >>= 1)
-    if (__shfl_sync(0xffffffffu, excl, o + st) <= q) o += st;
-  return o;
-}
-
-// Move pass of the bucketed layout: each warp takes 32 boxes of the input
-// buffer (their counts, zeroed for the buffer's next use as output) and
-// their molecules 32 at a time; then the input spill list.  rebin_only: the
-// staged molecules of an upload (u_*) are binned without moving.  Births as
-// in k_move.
-__global__ void __launch_bounds__(256, SMOLB_MOVE_BLOCKS) k_bmove(KParams p, int rebin_only) {
-  extern __shared__ float s_gtab[];
-  pdl_launch_dependents();
-  const float *gtab = rebin_only ? p.gtab : stage_gtab(p, s_gtab);
-  pdl_wait();
-  const uint32_t step = *p.step;
-  const int lane = threadIdx.x & 31;
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
-  int hits = 0;
-  if (!rebin_only) {
-    const int ngroups = (p.ncell + 31) >> 5;
-    for (int grp = gw; grp < ngroups; grp += nw) {
-      const int box = (grp << 5) + lane;
-      int c = 0;
-      if (box < p.ncell) {
-        c = min(p.a_cnt[box], kBucket);
-        p.a_cnt[box] = 0;
-      }
-      int total;
-      const int excl = warp_excl_scan(c, total);
-      for (int q0 = 0; q0 < total; q0 += 32) {
-        const int q = q0 + lane;
-        const int o = warp_owner(excl, q);
-        const int r = q - __shfl_sync(0xffffffffu, excl, o);
-        const bool have = q < total;
-        float4 pc = make_float4(0.f, 0.f, 0.f, 0.f);
-        ull id = 0;
-        if (have) {
-          const int k = (((grp << 5) + o) << kBucketShift) + r;
-          pc = p.a_pc[k];
-          id = p.a_id[k];
-        }
-        bucket_move_insert(p, have, pc, id, step, gtab, 0, hits);
-      }
-    }
-  }
-  const int spill0 = p.ncell << kBucketShift;
-  const int ns = rebin_only ? p.u_n : min(*p.p_n, p.pcap);
-  for (int base = gw << 5; base < ns; base += nw << 5) {
-    const int i = base + lane;
-    const bool have = i < ns;
-    float4 pc = make_float4(0.f, 0.f, 0.f, 0.f);
-    ull id = 0;
-    if (have) {
-      pc = rebin_only ? p.u_pc[i] : p.a_pc[spill0 + i];
-      id = rebin_only ? p.u_id[i] : p.a_id[spill0 + i];
-    }
-    bucket_move_insert(p, have, pc, id, step, gtab, rebin_only, hits);
-  }
-  if (hits) atomicAdd(&p.counters[0], (unsigned long long)hits);
-  if (!rebin_only) births(p, step);
-}
-
-// Same-box pairs of the bucketed layout: each warp takes 32 boxes, numbers
-// their c(c-1)/2 same-box pairs with a warp prefix sum and tests 32 pairs per
-// round (pair k of a box is (i, j) with j(j-1)/2 <= k < j(j+1)/2, i = k -
-// j(j-1)/2); then the same boxes' molecules 32 at a time set their face bits
-// (one word per box, bit s for slot s) when their stencil reaches a
-// higher-numbered box, as in k_pairs_tile.
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_bpairs(KParams p) {
-  constexpr int NW = BLOCK / 32;
-  __shared__ uint32_t s_face[NW][32];
-  __shared__ float s_rsv[kMaxSpecies];
-  pdl_launch_dependents();
-  pdl_wait();
-  for (int k = threadIdx.x; k < kMaxSpecies; k += blockDim.x) s_rsv[k] = k < c_net.nsp ? p.rsearch[k] : 0.f;
-  __syncthreads();
-  float rsmax = 0.f;
-  for (int k = 0; k < c_net.nsp; ++k) rsmax = fmaxf(rsmax, s_rsv[k]);
-  const float rsmax2 = rsmax * rsmax;
-  const uint32_t step = *p.step;
-  const DevGeo &g = c_geo0;
-  const int lane = threadIdx.x & 31;
-  const int w = threadIdx.x >> 5;
-  const int gw = blockIdx.x * NW + w, nw = gridDim.x * NW;
-  uint32_t *facebits = reinterpret_cast<uint32_t *>(p.face);
-  int extra = 0;
-  const int ngroups = (p.ncell + 31) >> 5;
-  for (int grp = gw; grp < ngroups; grp += nw) {
-    const int box = (grp << 5) + lane;
-    const int c = box < p.ncell ? min(p.b_cnt[box], kBucket) : 0;
-    s_face[w][lane] = 0u;
-    __syncwarp();
-    // same-box pairs
-    int total;
-    const int excl = warp_excl_scan(c * (c - 1) / 2, total);
-    for (int q0 = 0; q0 < total; q0 += 32) {
-      const int q = q0 + lane;
-      const int o = warp_owner(excl, q);
-      const int kk = q - __shfl_sync(0xffffffffu, excl, o);
-      if (q < total) {
-        int j = (int)((1.f + sqrtf(1.f + 8.f * (float)kk)) * 0.5f);
-        while (j * (j - 1) / 2 > kk) --j;
-        while ((j + 1) * j / 2 <= kk) ++j;
-        const int i = kk - j * (j - 1) / 2;
-        const int bx = ((grp << 5) + o) << kBucketShift;
-        const int ia = bx + i, ib = bx + j;
-        const float4 a = p.b_pc[ia], b = p.b_pc[ib];
-        const float vx = b.x - a.x, vy = b.y - a.y, vz = b.z - a.z;
-        const float d2 = vx * vx + vy * vy + vz * vz;
-        if (d2 <= rsmax2) {  // identities are read only for pairs within the largest stencil
-          const ull ida = p.b_id[ia], idb = p.b_id[ib];
-          const int spa = id_species(ida), spb = id_species(idb);
-          if (spa != kDeadSpecies && spb != kDeadSpecies && ((c_net.pair_mask[spa] >> spb) & 1u) &&
-              pair_reaction<false>(p, 0, spa, spb, d2, id_stream(ida), id_stream(idb), step, ia, ib) >= 0)
-            extra += register_pair(p, ia, ib, d2);
-        }
-      }
-    }
-    // face bits
-    int total2;
-    const int excl2 = warp_excl_scan(c, total2);
-    for (int q0 = 0; q0 < total2; q0 += 32) {
-      const int q = q0 + lane;
-      const int o = warp_owner(excl2, q);
-      const int r = q - __shfl_sync(0xffffffffu, excl2, o);
-      if (q < total2) {
-        const int idx = (((grp << 5) + o) << kBucketShift) + r;
-        const float4 pc = p.b_pc[idx];
-        const int sp = id_species(p.b_id[idx]);
-        if (sp != kDeadSpecies && ((c_net.pair_any >> sp) & 1u)) {
-          const float rs = s_rsv[sp];
-          int ix, iy, iz;
-          unpack_cell(__float_as_uint(pc.w), ix, iy, iz);
-          const float ub0 = (ix == g.n[0] - 1) ? g.whi[0] : g.h[0];
-          const float ub1 = (iy == g.n[1] - 1) ? g.whi[1] : g.h[1];
-          const float ub2 = (iz == g.n[2] - 1) ? g.whi[2] : g.h[2];
-          const bool face = pc.x > ub0 - rs || pc.y > ub1 - rs || pc.z > ub2 - rs ||
-                            (pc.x < rs && ix == 0 && g.wall[0] == kWallPeriodic) ||
-                            (pc.y < rs && iy == 0 && g.wall[2] == kWallPeriodic) ||
-                            (pc.z < rs && iz == 0 && g.wall[4] == kWallPeriodic);
-          if (face) atomicOr(&s_face[w][o], 1u << r);
-        }
-      }
-    }
-    __syncwarp();
-    if (box < p.ncell) facebits[box] = s_face[w][lane];
-    __syncwarp();
-  }
-  if (extra) atomicAdd(&p.counters[5], (unsigned long long)extra);
-}
-
-// Re-search of the bucketed layout (conflict rounds >= 2).
-__global__ void k_bresearch(KParams p) {
-  pdl_launch_dependents();
-  pdl_wait();
-  const int nc = min(*p.ncand, p.candcap);
-  const uint32_t step = *p.step;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nc; t += gridDim.x * blockDim.x) {
-    const int i = p.cand[t];
-    const ull id = p.b_id[i];
-    if (id_species(id) == kDeadSpecies) continue;
-    int ncd;
-    p.best[i] = bucket_partners(p, i, p.b_pc[i], id, step, ncd, false, 0);
-  }
-}
-
-// Products of the bucketed layout, inserted into the output buckets.
-__global__ void k_bproducts(KParams p) {
-  pdl_launch_dependents();
-  pdl_wait();
-  const int ne = min(*p.nev, p.evcap);
-  const uint32_t step = *p.step;
-  int uni = 0;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ne; t += gridDim.x * blockDim.x) {
-    place_event<0>(p, p.ev[t], step, uni, [&](float4 npc, ull nid) {
-      const int cell = global_cell(c_geo0, __float_as_uint(npc.w));
-      const int slot = atomicAdd(&p.b_cnt[cell], 1);
-      int k = -1;
-      if (slot < kBucket) {
-        k = (cell << kBucketShift) + slot;
-      } else {
-        const int j = atomicAdd(p.q_n, 1);
-        if (j < p.pcap) k = (p.ncell << kBucketShift) + j;
-      }
-      if (k >= 0) {
-        p.b_pc[k] = npc;
-        p.b_id[k] = nid;
-        atomicAdd((unsigned long long *)&p.spcount[id_species(nid)], 1ull);
-      } else {
-        atomicOr(p.status, kStMolCap);
-      }
-    });
-  }
-  if (uni) atomicAdd(&p.counters[2], (unsigned long long)uni);
-  const int nc = min(*p.ncand, p.candcap);
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nc; t += gridDim.x * blockDim.x)
-    p.best[p.cand[t]] = ~0ull;
-}
-
-// Every molecule of a bucketed buffer (slots, then spill) into a compact list
-// (order arbitrary); *n_out receives the count.
-__global__ void k_bgather(const float4 *pc, const ull *id, const int *cnt, int ncell, const int *nspill, int pcap,
-                          float4 *out_pc, ull *out_id, int *n_out, int cap, int *status) {
-  const int spill0 = ncell << kBucketShift;
-  const int ns = min(*nspill, pcap);
-  const long long total = (long long)ncell * kBucket + ns;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    int k;
-    if (t < spill0) {
-      const int box = (int)(t >> kBucketShift), s = (int)(t & (kBucket - 1));
-      if (s >= min(cnt[box], kBucket)) continue;
-      k = (int)t;
-    } else {
-      k = (int)t;
-    }
-    const ull x = id[k];
-    if (id_species(x) == kDeadSpecies) continue;
-    const int j = atomicAdd(n_out, 1);
-    if (j < cap) {
-      out_pc[j] = pc[k];
-      out_id[j] = x;
-    } else {
-      atomicOr(status, kStMolCap);
-    }
-  }
 }
 
 // ===========================================================================
@@ -2892,18 +2472,6 @@ class EngineImpl {
   int inj_n = 0;
   bool inj_pending = false;
 
-  // bucketed layout (k_bmove / k_bpairs): box b's molecules in slots
-  // [b*kBucket, (b+1)*kBucket) of d_bpc/d_bid, the spill list after the last
-  // box's slots; per-box counts d_bcnt; spill counts in d_counts[2 + k]
-  bool bucket_enabled = true;
-  bool in_bucket = false;
-  float4 *d_bpc[2] = {nullptr, nullptr};
-  ull *d_bid[2] = {nullptr, nullptr};
-  int *d_bcnt[2] = {nullptr, nullptr};
-  ull *d_bbest = nullptr;
-  int *d_bface = nullptr;
-  long long bslots = 0;   // slots allocated per buffer (boxes * kBucket + spill capacity)
-
   // persistent ensemble engine (k_persist): its own molecule layout, one
   // region per replicate; the step pipeline's buffers are refilled from it
   // (leave_persist) before anything else reads molecules
@@ -3024,22 +2592,8 @@ class EngineImpl {
     in_persist = false;
   }
 
-  void bucket_free() {
-    void *ptrs[] = {d_bpc[0], d_bpc[1], d_bid[0], d_bid[1], d_bcnt[0], d_bcnt[1], d_bbest, d_bface};
-    for (void *q : ptrs)
-      if (q) cudaFree(q);
-    d_bpc[0] = d_bpc[1] = nullptr;
-    d_bid[0] = d_bid[1] = nullptr;
-    d_bcnt[0] = d_bcnt[1] = nullptr;
-    d_bbest = nullptr;
-    d_bface = nullptr;
-    bslots = 0;
-    in_bucket = false;
-  }
-
   void release() {
     invalidate_graph();
-    bucket_free();
     persist_free();
     msd_free();
     tail_free();
@@ -3110,145 +2664,6 @@ class EngineImpl {
     p.inj_val = d_injval;
     p.inj_n = inj_n;
     return p;
-  }
-
-  // Kernel parameters of the bucketed layout: inputs in buffer par.
-  KParams bparams(int par) const {
-    KParams p = params(par);
-    const int in = par, out = 1 - par;
-    p.a_pc = d_bpc[in];
-    p.a_id = d_bid[in];
-    p.b_pc = d_bpc[out];
-    p.b_id = d_bid[out];
-    p.a_cnt = d_bcnt[in];
-    p.b_cnt = d_bcnt[out];
-    p.best = d_bbest;
-    p.face = d_bface;
-    p.pcap = (int)pcap;
-    return p;
-  }
-
-  // The bucketed layout serves a single simulation without surfaces,
-  // compartments, injected displacements or displacement trackers, whose
-  // boxes hold few enough molecules on average that a box rarely fills its
-  // kBucket slots (mean at most kBucket / 4).
-  bool bucket_static_ok() const {
-    return bucket_enabled && single_rep() && dnet.npanel == 0 && dnet.ncmpt == 0 && !dnet.inject && msd.empty() &&
-           ncell > 0 && (long long)ncell * kBucket + pcap < (1ll << 31) - 1;
-  }
-  bool bucket_ok(long long n) const { return bucket_static_ok() && n <= (long long)ncell * (kBucket / 4); }
-  bool bucket_recheck = false;  // left the bucketed layout for a reason that may pass
-
-  int bucket_alloc(std::string *err) {
-    const long long need = (long long)ncell * kBucket + pcap;
-    if (d_bpc[0] && bslots >= need) return 0;
-    bucket_free();
-    for (int k = 0; k < 2; ++k) {
-      CK(cudaMalloc(&d_bpc[k], (size_t)need * sizeof(float4)));
-      CK(cudaMalloc(&d_bid[k], (size_t)need * sizeof(ull)));
-      CK(cudaMalloc(&d_bcnt[k], (size_t)ncell * sizeof(int)));
-    }
-    CK(cudaMalloc(&d_bbest, (size_t)need * sizeof(ull)));
-    CK(cudaMemsetAsync(d_bbest, 0xFF, (size_t)need * sizeof(ull), stream));
-    CK(cudaMalloc(&d_bface, (size_t)ncell * sizeof(uint32_t)));
-    bslots = need;
-    return 0;
-  }
-
-  // Bin n staged molecules (positions and identities on the device) into
-  // bucket buffer 1, which becomes the input of the next step.
-  int bucket_rebin(const float4 *u_pc, const ull *u_id, long long n, std::string *err) {
-    int rc = bucket_alloc(err);
-    if (rc) return rc;
-    invalidate_graph();
-    CK(cudaMemsetAsync(d_bcnt[0], 0, (size_t)ncell * sizeof(int), stream));
-    CK(cudaMemsetAsync(d_bcnt[1], 0, (size_t)ncell * sizeof(int), stream));
-    CK(cudaMemsetAsync(d_counts, 0, 4 * sizeof(int), stream));
-    KParams p = bparams(0);
-    p.u_pc = u_pc;
-    p.u_id = u_id;
-    p.u_n = (int)n;
-    launch(k_begin, 1, 32, 0, p, 0);
-    launch(k_bmove, grid_mol(), 256, 0, p, 1);
-    nlaunch += 2;
-    parity = 1;
-    in_bucket = true;
-    return 0;
-  }
-
-  // Every molecule of the current bucket buffer into (out_pc, out_id);
-  // returns the count (device synchronised).
-  int bucket_gather(float4 *out_pc, ull *out_id, long long capn, long long *n, std::string *err) {
-    const int in = parity;
-    CK(cudaMemsetAsync(d_counts + 12, 0, sizeof(int), stream));
-    k_bgather<<<sm_count() * 8, 256, 0, stream>>>(d_bpc[in], d_bid[in], d_bcnt[in], ncell, d_counts + 2 + in,
-                                                  (int)pcap, out_pc, out_id, d_counts + 12, (int)capn,
-                                                  d_counts + 6);
-    CK(cudaGetLastError());
-    ++nlaunch;
-    int c = 0;
-    CK(cudaMemcpyAsync(&c, d_counts + 12, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    CK(cudaStreamSynchronize(stream));
-    *n = std::min<long long>(c, capn);
-    return 0;
-  }
-
-  // From the bucketed layout to the sorted one: gather into the staging
-  // buffer (product buffer 0) and rebin.
-  int leave_bucket(std::string *err) {
-    if (!in_bucket) return 0;
-    invalidate_graph();
-    long long n = 0;
-    int rc = bucket_gather(d_pc[0], d_id[0], cap, &n, err);  // the sorted buffers are free in this layout
-    if (rc) return rc;
-    if (n > pcap) {
-      for (int k = 0; k < 2; ++k) {
-        cudaFree(d_ppc[k]);
-        cudaFree(d_pid[k]);
-        d_ppc[k] = nullptr;
-        d_pid[k] = nullptr;
-      }
-      pcap = n;
-      for (int k = 0; k < 2; ++k) {
-        CK(cudaMalloc(&d_ppc[k], pcap * sizeof(float4)));
-        CK(cudaMalloc(&d_pid[k], pcap * sizeof(ull)));
-      }
-      cudaFree(d_tmp);
-      d_tmp = nullptr;
-      CK(cudaMalloc(&d_tmp, (cap + pcap) * sizeof(float4)));
-      bucket_free();  // sized with the old spill capacity
-    }
-    if (n) {
-      CK(cudaMemcpyAsync(d_ppc[0], d_pc[0], (size_t)n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
-      CK(cudaMemcpyAsync(d_pid[0], d_id[0], (size_t)n * sizeof(ull), cudaMemcpyDeviceToDevice, stream));
-    }
-    in_bucket = false;
-    CK(cudaMemsetAsync(d_counts, 0, 4 * sizeof(int), stream));
-    const long long keep_gen = upload_gen;
-    const bool keep = bucket_enabled;
-    bucket_enabled = false;  // this rebin goes to the sorted layout
-    rc = finish_upload(n, err);
-    bucket_enabled = keep;
-    upload_gen = keep_gen;
-    return rc;
-  }
-
-  // From the sorted layout to the bucketed one: a rebin pass merges the
-  // pending products, then the sorted buffer is binned into buckets.
-  int enter_bucket(std::string *err) {
-    if (in_bucket) return 0;
-    CK(cudaMemsetAsync(d_cnt, 0, ((size_t)ncell + 1) * sizeof(int), stream));
-    enqueue_step(parity, true);
-    parity ^= 1;
-    int n = 0;
-    CK(cudaMemcpyAsync(&n, d_counts + parity, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    CK(cudaStreamSynchronize(stream));
-    const int src = parity;
-    int rc = bucket_rebin(d_pc[src], d_id[src], n, err);
-    if (rc) return rc;
-    CK(cudaStreamSynchronize(stream));
-    CK(cudaGetLastError());
-    return 0;
   }
 
   LaunchTuning tune;  // kept across init
@@ -3332,22 +2747,6 @@ class EngineImpl {
   int finish_upload(long long n, std::string *err) {
     ++upload_gen;
     int staged = (int)n;
-    if (bucket_ok(n)) {
-      int rc = bucket_rebin(d_ppc[0], d_pid[0], n, err);
-      if (rc) return rc;
-      CK(cudaMemcpyAsync(d_counts + 10, &staged, sizeof(int), cudaMemcpyHostToDevice, stream));
-      CK(cudaMemsetAsync(d_spcount, 0, reps.size() * net.nspecies * sizeof(long long), stream));
-      k_species_count<<<grid_mol(), 256, 0, stream>>>(d_pid[0], d_counts + 10, d_spcount, net.nspecies,
-                                                      (int)reps.size() * net.nspecies);
-      nlaunch++;
-      CK(cudaStreamSynchronize(stream));
-      CK(cudaGetLastError());
-      int st = 0;
-      CK(cudaMemcpy(&st, d_counts + 6, sizeof(int), cudaMemcpyDeviceToHost));
-      if (st) { if (err) *err = "capacity overflow during upload"; return -9; }
-      return 0;
-    }
-    in_bucket = false;
     parity = 0;
     CK(cudaMemcpyAsync(d_counts + 2, &staged, sizeof(int), cudaMemcpyHostToDevice, stream));
     CK(cudaMemsetAsync(d_cnt, 0, ((size_t)ncell + 1) * sizeof(int), stream));
@@ -3534,36 +2933,8 @@ class EngineImpl {
   }
 
 
-  // One step of the bucketed layout (inputs in bucket buffer par).
-  void enqueue_bstep(int par) {
-    KParams p = bparams(par);
-    launch(k_begin, 1, 32, 0, p, 1);
-    mark("k_begin");
-    launch(k_bmove, grid_mol(), 256, adv_smem(), p, 0);
-    mark("k_move_bin");
-    if (tune.pair_tile == 128) launch(k_bpairs<128>, grid_tiles(), 128, 0, p);
-    else launch(k_bpairs<256>, grid_tiles(), 256, 0, p);
-    mark("k_pairs");
-    launch(k_pairs_faces<true, 0, true>, grid_mol(), 256, 0, p);
-    mark("k_pairs_faces");
-    launch(k_commit<0>, grid_small(), 128, 0, p);
-    mark("k_commit");
-    for (int round = 1; round < dnet.rounds; ++round) {
-      launch(k_bresearch, grid_small(), 128, 0, p);
-      mark("k_research");
-      launch(k_commit<0>, grid_small(), 128, 0, p);
-      mark("k_commit");
-    }
-    launch(k_bproducts, grid_small(), 128, 0, p);
-    mark("k_products");
-  }
-
   // Enqueue one step with the given parity (inputs A/P = buffers `par`).
   void enqueue_step(int par, bool rebin_only) {
-    if (in_bucket && !rebin_only) {
-      enqueue_bstep(par);
-      return;
-    }
     // surface form: 0 none, 1 rect and sphere panels only, 2 any shape or
     // compartments (whose tests need panels to mean anything)
     int surf = dnet.npanel > 0 ? 1 : 0;
@@ -3581,7 +2952,7 @@ class EngineImpl {
     }
   }
 
-  int launches_per_step() const { return (in_bucket ? 6 : 8) + 2 * (dnet.rounds - 1); }
+  int launches_per_step() const { return 8 + 2 * (dnet.rounds - 1); }
 
   int upload_const(std::string *err) {
     CK(cudaMemcpyToSymbolAsync(c_net, &dnet, sizeof(DevNet), 0, cudaMemcpyHostToDevice, stream));
@@ -4334,21 +3705,6 @@ int Engine::run(long long nsteps, std::string *err) {
     int rc = E.leave_persist(err);
     if (rc) return rc;
   }
-  // the bucketed layout when the configuration allows it: left when that
-  // stops (injection, displacement trackers), entered again at the next run
-  // that allows it (uploads choose for themselves)
-  if (E.in_bucket && !E.bucket_static_ok()) {
-    if (int rc = E.leave_bucket(err)) return rc;
-    E.bucket_recheck = true;
-  } else if (!E.in_bucket && E.bucket_recheck && E.bucket_static_ok()) {
-    E.bucket_recheck = false;
-    std::vector<long long> sc;
-    if (int rc = species_counts(&sc, err)) return rc;
-    long long n = 0;
-    for (long long v : sc) n += v;
-    if (E.bucket_ok(n))
-      if (int rc = E.enter_bucket(err)) return rc;
-  }
   const bool inj = E.dnet.inject != 0;
   if (inj) {
     if (nsteps != 1) { if (err) *err = "injected displacements apply to one step"; return -6; }
@@ -4500,19 +3856,10 @@ int Engine::get_molecules(std::vector<double> *pos, std::vector<int> *species, s
   CK(cudaStreamSynchronize(E.stream));
   CK(cudaMemcpy(c, E.d_counts, sizeof(c), cudaMemcpyDeviceToHost));
   const int in = E.parity;
-  int na = c[in], np = std::min<int>(c[2 + in], (int)E.pcap);
-  if (E.in_bucket) {  // gathered into the (unused) sorted buffer 0 of the other layout
-    long long n = 0;
-    if (int rc = E.bucket_gather(E.d_pc[0], E.d_id[0], E.cap, &n, err)) return rc;
-    na = (int)n;
-    np = 0;
-  }
+  const int na = c[in], np = std::min<int>(c[2 + in], (int)E.pcap);
   std::vector<float4> pc((size_t)na + np);
   std::vector<ull> id((size_t)na + np);
-  if (E.in_bucket && na) {
-    CK(cudaMemcpy(pc.data(), E.d_pc[0], (size_t)na * sizeof(float4), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(id.data(), E.d_id[0], (size_t)na * sizeof(ull), cudaMemcpyDeviceToHost));
-  } else if (na) {
+  if (na) {
     CK(cudaMemcpy(pc.data(), E.d_pc[in], (size_t)na * sizeof(float4), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(id.data(), E.d_id[in], (size_t)na * sizeof(ull), cudaMemcpyDeviceToHost));
   }
@@ -4559,10 +3906,6 @@ int Engine::set_injection(long long n, const uint64_t *sernos, const double *dis
                           std::string *err) {
   EngineImpl &E = *impl_;
   if (int rc = E.leave_persist(err)) return rc;
-  if (E.in_bucket) {
-    if (int rc = E.leave_bucket(err)) return rc;
-    E.bucket_recheck = true;
-  }
   if (E.d_injkey) { cudaFree(E.d_injkey); E.d_injkey = nullptr; }
   if (E.d_injval) { cudaFree(E.d_injval); E.d_injval = nullptr; }
   E.inj_n = 0;
@@ -4604,10 +3947,6 @@ int Engine::msd_track(int species, long long m, const uint64_t *keys, const doub
                       std::string *err) {
   EngineImpl &E = *impl_;
   if (int rc = E.leave_persist(err)) return rc;
-  if (E.in_bucket) {
-    if (int rc = E.leave_bucket(err)) return rc;
-    E.bucket_recheck = true;
-  }
   if (species <= 0 || species >= E.net.nspecies) {
     if (err) *err = "species index out of range";
     return -6;
@@ -4654,10 +3993,6 @@ int Engine::msd_track(int species, long long m, const uint64_t *keys, const doub
 int Engine::msd_update(int handle, int msddim, double *sum2, double *sum4, long long *count, std::string *err) {
   EngineImpl &E = *impl_;
   if (int rc = E.leave_persist(err)) return rc;
-  if (E.in_bucket) {
-    if (int rc = E.leave_bucket(err)) return rc;
-    E.bucket_recheck = true;
-  }
   if (handle < 0 || handle >= (int)E.msd.size()) {
     if (err) *err = "no such tracker";
     return -6;
@@ -4703,10 +4038,6 @@ int Engine::msd_count() const { return (int)impl_->msd.size(); }
 int Engine::cmpt_counts(int c, std::vector<long long> *out, std::string *err) {
   EngineImpl &E = *impl_;
   if (int rc = E.leave_persist(err)) return rc;
-  if (E.in_bucket) {
-    if (int rc = E.leave_bucket(err)) return rc;
-    E.bucket_recheck = true;
-  }
   if (c < 0 || c >= (int)E.cmpts.size()) {
     if (err) *err = "no such compartment";
     return -6;
@@ -4792,14 +4123,6 @@ int Engine::set_persistent(int mode, std::string *err) {
   return 0;
 }
 bool Engine::persistent_active() const { return impl_->persist_eligible(); }
-int Engine::set_bucket_layout(bool on, std::string *err) {
-  EngineImpl &E = *impl_;
-  E.bucket_enabled = on;
-  if (!on && E.in_bucket) return E.leave_bucket(err);
-  if (on && !E.in_bucket) E.bucket_recheck = true;
-  return 0;
-}
-bool Engine::bucket_layout_active() const { return impl_->in_bucket; }
 void Engine::set_use_graph(bool on) {
   impl_->use_graph = on;
   if (!on) impl_->invalidate_graph();

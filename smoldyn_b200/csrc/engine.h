@@ -154,13 +154,6 @@ class Engine {
   // the step pipeline.  persistent_active() tells which one run() uses.
   int set_persistent(int mode, std::string *err);
   bool persistent_active() const;
-  // Bucketed molecule layout (on by default): a single simulation without
-  // surfaces, compartments, injected displacements or displacement trackers
-  // keeps its molecules in fixed-capacity per-box buckets, which removes the
-  // box scan and the permutation pass of every step.  bucket_layout_active()
-  // tells whether the current state is held that way.
-  int set_bucket_layout(bool on, std::string *err);
-  bool bucket_layout_active() const;
   // Capture the 2-step kernel sequence in a CUDA graph and replay it (on by default).
   void set_use_graph(bool on);
   // Launch shape (kept across init); a change re-captures the step graph.

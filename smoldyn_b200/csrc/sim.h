@@ -100,7 +100,6 @@ struct Sim {
   double molperbox = -1, boxsize = -1;
   double auto_molperbox = -1;   // box width picked by the autotuner when neither is set
   LaunchTuning tuning;          // kernel launch shape (autotuner)
-  bool bucket_layout = true;    // bucketed molecule layout when the configuration allows it
   int gauss_table_size = 4096;
   long long max_mol = -1;
   int accuracy = 10;
