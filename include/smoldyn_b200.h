@@ -126,7 +126,9 @@ enum ErrorCode smolSetMoleculeSize(simptr sim, const char *species, enum MolecSt
 enum ErrorCode smolSetMoleculeStyle(simptr sim, const char *species, enum MolecState state, double size,
                                     double *color);
 
-/* libsmoldyn.h:122-130: walls and surfaces (solution-state actions) */
+/* libsmoldyn.h:122-130: walls and surfaces.  Actions reflect, transmit and
+ * absorb, for the solution, front and back states, optionally changing the
+ * species (jump and port are not supported). */
 enum ErrorCode smolSetBoundaryType(simptr sim, int dimension, int highside, char type);
 enum ErrorCode smolAddSurface(simptr sim, const char *surface);
 enum ErrorCode smolSetSurfaceAction(simptr sim, const char *surface, enum PanelFace face,
@@ -134,6 +136,31 @@ enum ErrorCode smolSetSurfaceAction(simptr sim, const char *surface, enum PanelF
                                     enum SrfAction action, const char *newspecies);
 enum ErrorCode smolAddPanel(simptr sim, const char *surface, enum PanelShape panelshape,
                             const char *panel, const char *axisstring, double *params);
+
+/* Surface-bound states (libsmoldyn.h:116, :129, :136-137; smolsurface.c
+ * surfsetrate :2278, surfsetneighbors :3150, addsurfmol smolmolec.c:2744).
+ * Single simulations only.  States soln, front, back and bsoln; rates of
+ * adsorption, desorption, flips between faces and one-way transmission
+ * (isinternal: the value is a probability per event); molecules bound to a
+ * panel diffuse on it (rect, tri, sph, disk panels) and continue onto
+ * neighbouring panels.  The up and down states, surface drift, and
+ * reactions of bound molecules are not supported. */
+enum ErrorCode smolSetSurfaceRate(simptr sim, const char *surface, const char *species, enum MolecState state,
+                                  enum MolecState state1, enum MolecState state2, double rate,
+                                  const char *newspecies, int isinternal);
+enum ErrorCode smolAddSurfaceMolecules(simptr sim, const char *species, enum MolecState state, int number,
+                                       const char *surface, enum PanelShape panelshape, const char *panel,
+                                       double *position);
+enum ErrorCode smolAddPanelNeighbor(simptr sim, const char *surface1, const char *panel1, const char *surface2,
+                                    const char *panel2, int reciprocal);
+enum ErrorCode smolSetSurfaceSimParams(simptr sim, const char *parameter, double value);
+/* The action of (surface, species, state soln/front/back, face front/back/
+ * none) and, for a rate-based action, the probabilities derived from its
+ * rates (surfupdateparams, smolsurface.c:3735-3800): prob, cumprob and
+ * revprob, 6 destination states each (MolecState order soln..bsoln). */
+enum ErrorCode smolgpuGetSurfaceRule(simptr sim, const char *surface, const char *species, enum MolecState state,
+                                     enum PanelFace face, int *action, double *prob, double *cumprob,
+                                     double *revprob);
 
 /* Compartments (libsmoldyn.h:115, :142-148, :157): interior-defining points,
  * bounding surfaces and logic on earlier compartments; molecules placed
@@ -186,10 +213,15 @@ double smolgpuGetTime(simptr sim);
 long long smolgpuGetStepCount(simptr sim);
 /* Number of live molecules (all species). */
 long long smolgpuGetTotalMolecules(simptr sim);
-/* Copy all molecules to host arrays (pos: 3*n doubles, absolute coordinates;
- * species: n ints; serno: n uint64).  *n is in: capacity, out: count. */
+/* Copy the solution-phase molecules to host arrays (pos: 3*n doubles,
+ * absolute coordinates; species: n ints; serno: n uint64).  *n is in:
+ * capacity, out: count. */
 enum ErrorCode smolgpuGetMolecules(simptr sim, long long *n, double *pos, int *species,
                                    uint64_t *serno);
+/* The same for surface-bound molecules, with their state (MSfront, MSback),
+ * surface index and panel index within the surface; sorted by serial number. */
+enum ErrorCode smolgpuGetSurfaceMolecules(simptr sim, long long *n, double *pos, int *species, int *state,
+                                          int *surface, int *panel, uint64_t *serno);
 /* Replace the molecule set (absolute coordinates; serno 0 = assign). */
 enum ErrorCode smolgpuSetMolecules(simptr sim, long long n, const double *pos, const int *species,
                                    const uint64_t *serno);

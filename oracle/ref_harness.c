@@ -19,8 +19,14 @@
  *   U <serno>                          killed by a first-order reaction
  *   F <serno> <ident> <x> <y> <z>      state after the step
  *   R <order> <rxn> <rate> <pgem>      rxncalcrate (smolreact.c:1592) after update
- * Usage: ref_harness <dir/> <file.txt> <out.txt> [rates]
- * With "rates" only the R lines are written (no step is run).
+ *   A <surface> <species> <state> <face> <action>
+ *   S <surface> <species> <state> <face> <prob x6> <cumprob x6> <revprob x6>
+ *                                      surface actions and, for rate-based ones,
+ *                                      the probabilities surfupdateparams
+ *                                      (smolsurface.c:3735) derived
+ * Usage: ref_harness <dir/> <file.txt> <out.txt> [rates|surfprobs]
+ * With "rates" only the R lines are written, with "surfprobs" only the A and
+ * S lines (no step is run).
  */
 #include <cstdio>
 #include <cstdlib>
@@ -94,6 +100,28 @@ int main(int argc, char **argv) {
     if (sim->rxnss[2])
       for (int r = 0; r < sim->rxnss[2]->totrxn; r++)
         fprintf(g_out, "P %d %.17g %.17g\n", r, sim->rxnss[2]->rxn[r]->bindrad2, sim->rxnss[2]->rxn[r]->prob);
+    fclose(g_out);
+    smolFreeSim(sim);
+    return 0;
+  }
+  if (argc > 4 && !strcmp(argv[4], "surfprobs")) {
+    if (sim->srfss)
+      for (int s = 0; s < sim->srfss->nsrf; s++) {
+        surfaceptr srf = sim->srfss->srflist[s];
+        for (int i = 1; i < sim->mols->nspecies; i++)
+          for (int ms = 0; ms < 3; ms++)
+            for (int face = 0; face < 3; face++) {
+              const int act = (int)srf->action[i][ms][face];
+              fprintf(g_out, "A %d %d %d %d %d\n", s, i, ms, face, act);
+              surfactionptr ad = srf->actdetails[i][ms][face];
+              if (act != (int)SAmult || !ad) continue;
+              fprintf(g_out, "S %d %d %d %d", s, i, ms, face);
+              for (int k = 0; k < 6; k++) fprintf(g_out, " %.17g", ad->srfprob[k]);
+              for (int k = 0; k < 6; k++) fprintf(g_out, " %.17g", ad->srfcumprob[k]);
+              for (int k = 0; k < 6; k++) fprintf(g_out, " %.17g", ad->srfrevprob[k]);
+              fprintf(g_out, "\n");
+            }
+      }
     fclose(g_out);
     smolFreeSim(sim);
     return 0;

@@ -89,6 +89,16 @@ PROTOTYPES = {
     "smolSetReactionRegion": (C.c_int, [_sim, C.c_char_p, C.c_char_p, C.c_char_p]),
     "smolSetSurfaceAction": (C.c_int, [_sim, C.c_char_p, C.c_int, C.c_char_p, C.c_int, C.c_int, C.c_char_p]),
     "smolAddPanel": (C.c_int, [_sim, C.c_char_p, C.c_int, C.c_char_p, C.c_char_p, _dp]),
+    "smolSetSurfaceRate": (C.c_int, [_sim, C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_double,
+                                     C.c_char_p, C.c_int]),
+    "smolAddSurfaceMolecules": (C.c_int, [_sim, C.c_char_p, C.c_int, C.c_int, C.c_char_p, C.c_int, C.c_char_p, _dp]),
+    "smolAddPanelNeighbor": (C.c_int, [_sim, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int]),
+    "smolSetSurfaceSimParams": (C.c_int, [_sim, C.c_char_p, C.c_double]),
+    "smolgpuGetSurfaceRule": (C.c_int, [_sim, C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.POINTER(C.c_int), _dp, _dp,
+                                        _dp]),
+    "smolgpuGetSurfaceMolecules": (C.c_int, [_sim, C.POINTER(C.c_longlong), _dp, C.POINTER(C.c_int),
+                                             C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                             C.POINTER(C.c_uint64)]),
     "smolAddReaction": (C.c_int, [_sim, C.c_char_p, C.c_char_p, C.c_int, C.c_char_p, C.c_int, C.c_int,
                                   C.POINTER(C.c_char_p), _ip, C.c_double]),
     "smolGetReactionIndex": (C.c_int, [_sim, _ip, C.c_char_p]),
@@ -233,6 +243,15 @@ class Sim:
             check(ECerror)
         return cls(ptr=ptr)
 
+    @classmethod
+    def load_file(cls, path, flags=""):
+        """Read a configuration file without building the engine (no GPU needed)."""
+        lib = load()
+        d, f = os.path.split(os.path.abspath(path))
+        ptr = _sim()
+        check(lib.smolLoadSimFromFile((d + "/").encode(), f.encode(), C.byref(ptr), flags.encode()))
+        return cls(ptr=ptr.value)
+
     def close(self):
         if self.ptr:
             self.lib.smolFreeSim(self.ptr)
@@ -325,10 +344,34 @@ class Sim:
         return self.lib.smolgpuGetLaunchCount(self.ptr)
 
     # ---- state
-    def count(self, species="all"):
-        n = self.lib.smolGetMoleculeCount(self.ptr, species.encode(), MSsoln)
+    def count(self, species="all", state=MSall):
+        n = self.lib.smolGetMoleculeCount(self.ptr, species.encode(), state)
         check(n if n < 0 else 0)
         return n
+
+    def surface_rule(self, surface, species, state, face):
+        """(action, prob, cumprob, revprob) of a surface interaction."""
+        a = C.c_int(0)
+        pr, cu, rv = np.zeros(6), np.zeros(6), np.zeros(6)
+        check(self.lib.smolgpuGetSurfaceRule(self.ptr, surface.encode(), species.encode(), state, face, C.byref(a),
+                                             dptr(pr), dptr(cu), dptr(rv)))
+        return a.value, pr, cu, rv
+
+    def surface_molecules(self):
+        """Surface-bound molecules: positions (n, 3), species, state (MSfront /
+        MSback), surface index, panel index and serial number, by serial."""
+        n = C.c_longlong(0)
+        check(self.lib.smolgpuGetSurfaceMolecules(self.ptr, C.byref(n), None, None, None, None, None, None))
+        cnt = max(n.value, 1)
+        pos = np.zeros((cnt, 3))
+        ints = [np.zeros(cnt, dtype=np.int32) for _ in range(4)]
+        sn = np.zeros(cnt, dtype=np.uint64)
+        n = C.c_longlong(cnt)
+        ip = [a.ctypes.data_as(C.POINTER(C.c_int)) for a in ints]
+        check(self.lib.smolgpuGetSurfaceMolecules(self.ptr, C.byref(n), dptr(pos), ip[0], ip[1], ip[2], ip[3],
+                                                  sn.ctypes.data_as(C.POINTER(C.c_uint64))))
+        k = n.value
+        return pos[:k], ints[0][:k], ints[1][:k], ints[2][:k], ints[3][:k], sn[:k]
 
     def total(self):
         return self.lib.smolgpuGetTotalMolecules(self.ptr)

@@ -11,8 +11,10 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsmoldyn_b200.so")
-SOURCES = ["engine.cu", "surrogate.cu", "noalloc.cu", "rdf.cu", "sim.cpp", "api.cpp", "ensemble.cpp", "autotune.cpp"]
+SOURCES = ["engine.cu", "surrogate.cu", "noalloc.cu", "rdf.cu", "sim.cpp", "surface.cpp", "api.cpp", "ensemble.cpp",
+           "autotune.cpp"]
 HEADERS = ["engine.h", "devcommon.cuh", "rxnparam.cuh", "panelgeom.cuh", "sim.h", "surrogate.h", "autotune.h", "_gen/rxntables.h",
+           "boundgeom.cuh", "surfparam.h", "_gen/srftables.h",
            os.path.join("..", "..", "include", "smoldyn_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

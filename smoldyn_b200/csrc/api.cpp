@@ -80,8 +80,51 @@ int pull_molecules(Sim &s, std::string *err) {
   s.pend_pos = pos;
   s.pend_sp = sp;
   s.pend_serno = serno;
+  // surface-bound molecules: engine panel index back to (surface, panel)
+  std::vector<double> bpos;
+  std::vector<int> bsp, bst, bpn;
+  std::vector<uint64_t> bsn;
+  rc = s.eng->get_bound(&bpos, &bsp, &bst, &bpn, &bsn, err);
+  if (rc) return rc;
+  s.pend_bound.clear();
+  for (size_t k = 0; k < bsp.size(); ++k) {
+    smolb::PendBound b;
+    for (int d = 0; d < 3; ++d) b.pos[d] = bpos[3 * k + d];
+    b.species = bsp[k];
+    b.state = bst[k];
+    b.serno = bsn[k];
+    int g = bpn[k];
+    for (size_t q = 0; q < s.surfaces.size(); ++q) {
+      if (g < (int)s.surfaces[q].panels.size()) { b.surface = (int)q; b.panel = g; break; }
+      g -= (int)s.surfaces[q].panels.size();
+    }
+    s.pend_bound.push_back(b);
+  }
   s.started = false;
   return 0;
+}
+
+// Upload the pending surface-bound molecules into a freshly built engine;
+// molecules without a serial number get ones after every solution molecule's.
+int push_bound(Sim &s, long long nsol, std::string *err) {
+  uint64_t base = (uint64_t)nsol + 1;
+  for (uint64_t v : s.pend_serno) base = std::max<uint64_t>(base, v + 1);
+  for (const smolb::PendBound &b : s.pend_bound) base = std::max<uint64_t>(base, b.serno + 1);
+  std::vector<double> pos;
+  std::vector<int> sp, st, pn;
+  std::vector<uint64_t> sn;
+  std::vector<int> first(s.surfaces.size());
+  for (size_t q = 0, k = 0; q < s.surfaces.size(); ++q) { first[q] = (int)k; k += s.surfaces[q].panels.size(); }
+  for (const smolb::PendBound &b : s.pend_bound) {
+    for (int d = 0; d < 3; ++d) pos.push_back(b.pos[d]);
+    sp.push_back(b.species);
+    st.push_back(b.state);
+    pn.push_back(first[b.surface] + b.panel);
+    sn.push_back(b.serno ? b.serno : base++);
+  }
+  const int rc = s.eng->set_bound((long long)sp.size(), pos.data(), sp.data(), st.data(), pn.data(), sn.data(), err);
+  if (!rc) s.pend_bound.clear();
+  return rc;
 }
 
 // simupdate equivalent: derive parameters, (re)build the engine, upload molecules.
@@ -111,6 +154,7 @@ ErrorCode update_sim(Sim &s, const char *func) {
       for (size_t k = 0; k < s.pend_serno.size() && k < sn.size(); ++k) sn[k] = s.pend_serno[k];
     }
     rc = s.eng->set_molecules(n, s.pend_pos.data(), s.pend_sp.data(), nullptr, sn.empty() ? nullptr : sn.data(), &err);
+    if (!rc && (!s.pend_bound.empty() || net.bound)) rc = push_bound(s, n, &err);
     // a rebuild mid-run continues the random streams where they were
     if (!rc && s.steps > 0) rc = s.eng->set_rng_step((uint64_t)s.steps, &err);
     if (rc) { s.eng.reset(); return set_error(func, from_rc(rc), err); }
@@ -643,8 +687,22 @@ void smolGetSpeciesName(simptr sim, int speciesindex, char *species) {
 enum ErrorCode smolSetSpeciesMobility(simptr sim, const char *species, enum MolecState state, double difc,
                                       double *drift, double *difmatrix) {
   LCHECK(sim && species, ECmissing, "missing sim or species");
-  LCHECK(state == MSsoln || state == MSall, ECbounds, "only solution-state species are supported");
+  LCHECK(state == MSsoln || state == MSall || state == MSfront || state == MSback, ECbounds,
+         "the up, down and bsoln states are not supported");
   LCHECK(difc >= 0 || difmatrix, ECbounds, "difc must be >= 0");
+  if (state == MSfront || state == MSback) {  // surface-bound states: isotropic diffusion only
+    LCHECK(!drift && !difmatrix, ECbounds, "drift and diffusion matrices of surface-bound states are not supported");
+    std::vector<int> ids;
+    if (!strcmp(species, "all")) for (size_t i = 1; i < sim->s.species.size(); ++i) ids.push_back((int)i);
+    else {
+      const int i = sim->s.species_index(species);
+      LCHECK(i > 0, ECnonexist, "species not found");
+      ids.push_back(i);
+    }
+    for (int i : ids) sim->s.species[i].difc_bound[state == MSfront ? 0 : 1] = difc;
+    sim->s.need_update = sim->s.need_rebuild = true;
+    return ECok;
+  }
   std::vector<int> ids;
   if (!strcmp(species, "all")) for (size_t i = 1; i < sim->s.species.size(); ++i) ids.push_back((int)i);
   else {
@@ -654,6 +712,7 @@ enum ErrorCode smolSetSpeciesMobility(simptr sim, const char *species, enum Mole
   }
   for (int i : ids) {  // libsmoldyn.cpp:917: difc, then drift, then the matrix (which resets difc)
     if (difc >= 0) sim->s.species[i].difc = difc;
+    if (difc >= 0 && state == MSall) sim->s.species[i].difc_bound[0] = sim->s.species[i].difc_bound[1] = difc;
     if (drift) for (int d = 0; d < sim->s.dim; ++d) sim->s.species[i].drift[d] = drift[d];
     if (difmatrix) smolb::set_species_difm(sim->s, i, difmatrix);
   }
@@ -697,25 +756,39 @@ enum ErrorCode smolAddSolutionMolecules(simptr sim, const char *species, int num
 }
 
 int smolGetMoleculeCount(simptr sim, const char *species, enum MolecState state) {
-  (void)state;
   if (!sim || !species) return (int)set_error(__func__, ECmissing, "missing sim or species");
+  if (state != MSall && state != MSsoln && state != MSfront && state != MSback && state != MSsome)
+    return (int)set_error(__func__, ECbounds, "state not supported");
   Sim &s = sim->s;
   int idx = -1;
   if (strcmp(species, "all")) {
     idx = s.species_index(species);
     if (idx < 0) return (int)set_error(__func__, ECnonexist, "species not found");
   }
-  long long n = 0;
+  long long n = 0, nb[3] = {0, 0, 0};  // all states, then bound molecules by state
   if (s.eng && s.started && !s.need_rebuild) {
     std::vector<long long> c;
     std::string err;
     if (s.eng->species_counts(&c, &err)) return (int)set_error(__func__, ECerror, err);
     for (size_t i = 1; i < s.species.size(); ++i)
       if (idx < 0 || (int)i == idx) n += c[i];
+    if (state != MSall && state != MSsome) {
+      std::vector<double> bpos;
+      std::vector<int> bsp, bst, bpn;
+      std::vector<uint64_t> bsn;
+      if (s.eng->get_bound(&bpos, &bsp, &bst, &bpn, &bsn, &err)) return (int)set_error(__func__, ECerror, err);
+      for (size_t k = 0; k < bsp.size(); ++k)
+        if ((idx < 0 || bsp[k] == idx) && bst[k] >= 1 && bst[k] <= 2) nb[bst[k]]++;
+    }
   } else {
     for (int sp : s.pend_sp)
       if (idx < 0 || sp == idx) n++;
+    for (const smolb::PendBound &b : s.pend_bound)
+      if (idx < 0 || b.species == idx) { n++; nb[b.state]++; }
   }
+  if (state == MSsoln) n -= nb[1] + nb[2];
+  else if (state == MSfront) n = nb[1];
+  else if (state == MSback) n = nb[2];
   return (int)n;
 }
 
@@ -743,42 +816,126 @@ enum ErrorCode smolAddSurface(simptr sim, const char *surface) {
   return ECok;
 }
 
+namespace {
+const char *ms_word(int ms) {
+  static const char *w[] = {"soln", "front", "back", "up", "down", "bsoln", "all"};
+  return (ms >= 0 && ms <= 6) ? w[ms] : "none";
+}
+
+int surface_index(const Sim &s, const char *name) {
+  for (size_t k = 0; k < s.surfaces.size(); ++k)
+    if (s.surfaces[k].name == name) return (int)k;
+  return -1;
+}
+}  // namespace
+
 enum ErrorCode smolSetSurfaceAction(simptr sim, const char *surface, enum PanelFace face, const char *species,
                                     enum MolecState state, enum SrfAction action, const char *newspecies) {
-  (void)state;
   LCHECK(sim && surface && species, ECmissing, "missing argument");
-  LCHECK(!newspecies || !newspecies[0], ECbounds, "species conversion at surfaces is not supported");
-  int a;
-  if (action == SAreflect) a = 0;
-  else if (action == SAtrans) a = 1;
-  else if (action == SAabsorb) a = 2;
-  else return set_error(__func__, ECbounds, "surface action not supported by the GPU engine");
-  smolb::SurfaceDef *sf = nullptr;
-  for (smolb::SurfaceDef &x : sim->s.surfaces)
-    if (x.name == surface) sf = &x;
-  LCHECK(sf, ECnonexist, "surface not found");
-  const bool f = (face == PFfront || face == PFboth), b = (face == PFback || face == PFboth);
-  if (!strcmp(species, "all")) {
-    if (f) { sf->act_front = a; sf->absorb_front = sf->trans_front = sf->refl_front = 0; }
-    if (b) { sf->act_back = a; sf->absorb_back = sf->trans_back = sf->refl_back = 0; }
-  } else {
-    const int i = sim->s.species_index(species);
-    LCHECK(i > 0, ECnonexist, "species not found");
-    const uint32_t bit = 1u << i;
-    auto apply = [&](uint32_t &abs, uint32_t &tr, uint32_t &rf) {
-      abs &= ~bit; tr &= ~bit; rf &= ~bit;
-      if (a == 2) abs |= bit; else if (a == 1) tr |= bit; else rf |= bit;
-    };
-    if (f) apply(sf->absorb_front, sf->trans_front, sf->refl_front);
-    if (b) apply(sf->absorb_back, sf->trans_back, sf->refl_back);
-  }
+  const int sidx = surface_index(sim->s, surface);
+  LCHECK(sidx >= 0, ECnonexist, "surface not found");
+  LCHECK(face == PFfront || face == PFback || face == PFboth, ECbounds, "face must be front, back or both");
+  const char *an = action == SAreflect ? "reflect" : action == SAtrans ? "transmit" : action == SAabsorb ? "absorb" : nullptr;
+  LCHECK(an, ECbounds, "surface action not supported by the GPU engine");
+  std::vector<std::string> w = {std::string(species) + "(" + ms_word(state) + ")",
+                                face == PFfront ? "front" : face == PFback ? "back" : "both", an};
+  if (newspecies && newspecies[0]) w.push_back(newspecies);
+  std::string err;
+  const int rc = smolb::read_surface_rule_statement(sim->s, sidx, "action", w, &err);
+  if (rc) return set_error(__func__, from_rc(rc), err);
+  sim->s.need_update = sim->s.need_rebuild = true;
+  return ECok;
+}
+
+enum ErrorCode smolSetSurfaceRate(simptr sim, const char *surface, const char *species, enum MolecState state,
+                                  enum MolecState state1, enum MolecState state2, double rate, const char *newspecies,
+                                  int isinternal) {
+  LCHECK(sim && surface && species, ECmissing, "missing argument");
+  const int sidx = surface_index(sim->s, surface);
+  LCHECK(sidx >= 0, ECnonexist, "surface not found");
+  std::vector<std::string> w = {std::string(species) + "(" + ms_word(state) + ")", ms_word(state1), ms_word(state2)};
+  char buf[64];
+  snprintf(buf, sizeof(buf), "%.17g", rate);
+  w.push_back(buf);
+  if (newspecies && newspecies[0]) w.push_back(newspecies);
+  std::string err;
+  const int rc = smolb::read_surface_rule_statement(sim->s, sidx, isinternal ? "rate_internal" : "rate", w, &err);
+  if (rc) return set_error(__func__, from_rc(rc), err);
+  sim->s.need_update = sim->s.need_rebuild = true;
+  return ECok;
+}
+
+enum ErrorCode smolAddPanelNeighbor(simptr sim, const char *surface1, const char *panel1, const char *surface2,
+                                    const char *panel2, int reciprocal) {
+  LCHECK(sim && surface1 && panel1 && surface2 && panel2, ECmissing, "missing argument");
+  const int s1 = surface_index(sim->s, surface1), s2 = surface_index(sim->s, surface2);
+  LCHECK(s1 >= 0 && s2 >= 0, ECnonexist, "surface not found");
+  std::string err;
+  int rc = smolb::read_surface_rule_statement(sim->s, s1, "neighbors",
+                                              {panel1, std::string(surface2) + ":" + panel2}, &err);
+  if (!rc && reciprocal)
+    rc = smolb::read_surface_rule_statement(sim->s, s2, "neighbors", {panel2, std::string(surface1) + ":" + panel1}, &err);
+  if (rc) return set_error(__func__, from_rc(rc), err);
   sim->s.need_rebuild = true;
+  return ECok;
+}
+
+enum ErrorCode smolgpuGetSurfaceRule(simptr sim, const char *surface, const char *species, enum MolecState state,
+                                     enum PanelFace face, int *action, double *prob, double *cumprob,
+                                     double *revprob) {
+  LCHECK(sim && surface && species && action && prob && cumprob && revprob, ECmissing, "missing argument");
+  const int sidx = surface_index(sim->s, surface);
+  LCHECK(sidx >= 0, ECnonexist, "surface not found");
+  const int i = sim->s.species_index(species);
+  LCHECK(i > 0, ECnonexist, "species not found");
+  std::string err;
+  const int rc = smolb::surface_rule_info(sim->s, sidx, i, (int)state, (int)face, action, prob, cumprob, revprob, &err);
+  if (rc) return set_error(__func__, from_rc(rc), err);
+  return ECok;
+}
+
+enum ErrorCode smolSetSurfaceSimParams(simptr sim, const char *parameter, double value) {
+  LCHECK(sim && parameter, ECmissing, "missing argument");
+  LCHECK(value >= 0, ECbounds, "value must be >= 0");
+  if (!strcmp(parameter, "epsilon")) sim->s.srf_epsilon = value;
+  else if (!strcmp(parameter, "margin")) sim->s.srf_margin = value;
+  else if (!strcmp(parameter, "neighbordist")) sim->s.srf_neighdist = value;
+  else return set_error(__func__, ECsyntax, "parameter not recognized");
+  sim->s.need_rebuild = true;
+  return ECok;
+}
+
+enum ErrorCode smolAddSurfaceMolecules(simptr sim, const char *species, enum MolecState state, int number,
+                                       const char *surface, enum PanelShape panelshape, const char *panel,
+                                       double *position) {
+  LCHECK(sim && species && surface, ECmissing, "missing argument");
+  LCHECK(number >= 0, ECbounds, "number must be >= 0");
+  LCHECK(state == MSfront || state == MSback, ECbounds, "state must be front or back");
+  Sim &s = sim->s;
+  const int sp = s.species_index(species);
+  LCHECK(sp > 0, ECnonexist, "species not found");
+  int sidx = -1;
+  if (strcmp(surface, "all")) {
+    sidx = surface_index(s, surface);
+    LCHECK(sidx >= 0, ECnonexist, "surface not found");
+  }
+  int q = -1;
+  if (panel && strcmp(panel, "all")) {
+    LCHECK(sidx >= 0, ECbounds, "a named panel needs a named surface");
+    q = smolb::find_panel(s, sidx, panel, nullptr);
+    LCHECK(q >= 0, ECnonexist, "panel not found");
+  }
+  std::string err;
+  if (s.eng && s.started)
+    if (pull_molecules(s, &err)) return set_error(__func__, ECerror, err);
+  const int shape = (panelshape == PSall || panelshape == PSnone) ? -1 : (int)panelshape;
+  const int rc = smolb::add_surface_molecules(s, number, sp, (int)state, sidx, shape, q, position, &err);
+  if (rc) return set_error(__func__, from_rc(rc), err);
   return ECok;
 }
 
 enum ErrorCode smolAddPanel(simptr sim, const char *surface, enum PanelShape panelshape, const char *panel,
                             const char *axisstring, double *params) {
-  (void)panel;
   LCHECK(sim && surface && params, ECmissing, "missing argument");
   smolb::SurfaceDef *sf = nullptr;
   for (smolb::SurfaceDef &x : sim->s.surfaces)
@@ -799,6 +956,7 @@ enum ErrorCode smolAddPanel(simptr sim, const char *surface, enum PanelShape pan
   std::string err;
   const int rc = smolb::make_panel(dim, (int)panelshape, axisstring ? axisstring : "", params, np, &p, &err);
   if (rc) return set_error(__func__, from_rc(rc), err);
+  sf->pnames.push_back(smolb::new_panel_name(*sf, (int)panelshape, panel ? panel : ""));
   sf->panels.push_back(p);
   smolb::invalidate_compartments(sim->s);
   sim->s.need_rebuild = true;
@@ -1052,6 +1210,47 @@ enum ErrorCode smolgpuGetMolecules(simptr sim, long long *n, double *pos, int *s
   if (pos) memcpy(pos, p.data(), p.size() * sizeof(double));
   if (species) memcpy(species, sp.data(), sp.size() * sizeof(int));
   if (serno) memcpy(serno, sn.data(), sn.size() * sizeof(uint64_t));
+  return ECok;
+}
+
+enum ErrorCode smolgpuGetSurfaceMolecules(simptr sim, long long *n, double *pos, int *species, int *state,
+                                          int *surface, int *panel, uint64_t *serno) {
+  LCHECK(sim && n, ECmissing, "missing argument");
+  Sim &s = sim->s;
+  std::string err;
+  std::vector<smolb::PendBound> b;
+  if (s.eng && s.started && !s.need_rebuild) {
+    std::vector<double> bpos;
+    std::vector<int> bsp, bst, bpn;
+    std::vector<uint64_t> bsn;
+    if (s.eng->get_bound(&bpos, &bsp, &bst, &bpn, &bsn, &err)) return set_error(__func__, ECerror, err);
+    for (size_t k = 0; k < bsp.size(); ++k) {
+      smolb::PendBound x;
+      for (int d = 0; d < 3; ++d) x.pos[d] = bpos[3 * k + d];
+      x.species = bsp[k];
+      x.state = bst[k];
+      x.serno = bsn[k];
+      int g = bpn[k];
+      for (size_t q = 0; q < s.surfaces.size(); ++q) {
+        if (g < (int)s.surfaces[q].panels.size()) { x.surface = (int)q; x.panel = g; break; }
+        g -= (int)s.surfaces[q].panels.size();
+      }
+      b.push_back(x);
+    }
+  } else {
+    b = s.pend_bound;
+  }
+  const long long cnt = (long long)b.size();
+  LCHECK(*n >= cnt || (!pos && !species && !state && !surface && !panel && !serno), ECbounds, "buffer too small");
+  *n = cnt;
+  for (long long k = 0; k < cnt; ++k) {
+    if (pos) for (int d = 0; d < 3; ++d) pos[3 * k + d] = b[k].pos[d];
+    if (species) species[k] = b[k].species;
+    if (state) state[k] = b[k].state;
+    if (surface) surface[k] = b[k].surface;
+    if (panel) panel[k] = b[k].panel;
+    if (serno) serno[k] = b[k].serno;
+  }
   return ECok;
 }
 

@@ -127,6 +127,21 @@ struct DevNet {
   float bounce_k[kMaxRxn];   // bounce scaling: 1 (given unbinding radius) or 2 (from the binding radius)
   int ncmpt;
   uint8_t cmpt[3][kMaxRxn];  // compartment of each reaction + 1 (0: anywhere)
+  // surface-bound states (single simulations)
+  int bound;                       // 1: surface rules and bound molecules in use
+  double beps, bmargin, bneighdist; // surfacessstruct epsilon, margin, neighdist for bound molecules
+  double bstep[kMaxSpecies][2];    // sqrt(2 D dt) of the front and back states
+  double sstep[kMaxSpecies];       // sqrt(2 D dt) of the solution state, FP64 (desorption distance)
+};
+
+// A molecule bound to a panel: absolute position (relative to the system's
+// low corner), id as for solution molecules, engine panel index and state
+// (1 front, 2 back; MolecState numbering).
+struct BoundMol {
+  double x[3];
+  ull id;
+  int pnl;
+  int ms;
 };
 
 // Per-replicate geometry.  Cells are cubes of size h; the last cell in each
@@ -160,6 +175,9 @@ struct DevPanel {
   float posf, radiusf, centerf[3];   // FP32 copies for the screening test
   float p0f[3], nrmf[3];             // screen reference point and unit vector (zero for sph, hemi)
   int curved;                        // screen: 1 sph, cyl, hemi (radial test); 0 flat (plane test)
+  int srf;                           // surface index (rule table)
+  int nneigh, neighhop;              // neighbouring panels for surface-bound molecules; 1: hop
+  int neigh[kMaxNeigh];
 };
 
 // Compartment (smolcomparts.c compartstruct subset): interior points, the

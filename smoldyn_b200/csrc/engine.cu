@@ -32,6 +32,7 @@
 #include "engine.h"
 #include "rxnparam.cuh"
 #include "panelgeom.cuh"
+#include "boundgeom.cuh"
 
 namespace smolb {
 
@@ -87,11 +88,23 @@ struct KParams {
   const ull *inj_key;            // sorted stream keys
   const float4 *inj_val;         // dx, dy, dz, forced order-1 reaction (or -1)
   int inj_n;
+  // surface-bound molecules (single simulations with surface-bound states)
+  const SrfRule *srfrule;        // [((surface*kMaxSpecies + sp)*3 + state)*3 + face]
+  const BoundMol *bd_in;
+  const int *bd_in_n;
+  BoundMol *bd_out;
+  int *bd_out_n;
+  int bcap;
 };
 
 constexpr uint32_t kTmpGone = 0xFFFFFFFFu;  // tmp[i].w of a molecule that left
+// Set in the packed box word of a product-list entry that has already been
+// moved this step (a molecule that desorbed from a surface): the move pass
+// only re-bins it and draws its first-order reactions.
+constexpr uint32_t kMovedBit = 1u << 30;
 
-enum StatusBits { kStMolCap = 1, kStEvCap = 2, kStProdCap = 4, kStCandCap = 8, kStScanWait = 16, kStUpload = 32 };
+enum StatusBits { kStMolCap = 1, kStEvCap = 2, kStProdCap = 4, kStCandCap = 8, kStScanWait = 16, kStUpload = 32,
+                  kStBoundCap = 64 };
 
 // Programmatic dependent launch: the step's kernels are launched so that the
 // next kernel can be scheduled while the current one runs.  Each kernel lets
@@ -431,6 +444,409 @@ __device__ __noinline__ bool pair_crosses_surface_call(const DevGeo &g, float4 p
   return pair_crosses_surface<GEN>(g, pc, vx, vy, vz);
 }
 
+// ---- surface-bound states --------------------------------------------------
+// Adsorption, desorption, flips and surface-bound diffusion (dosurfinteract
+// smolsurface.c:4930, surfaction :4330, checksurfacebound :5184,
+// movemol2closepanel :4726), for single simulations.  Solution molecules meet
+// panels in the move pass and may adsorb; bound molecules live in their own
+// list (FP64 absolute positions, panel and state) that k_bound steps before
+// the move pass: diffusion projected onto the panel, crossings of other
+// panels, then the per-step desorption / flip coin.  A molecule that desorbs
+// joins the product list already moved (kMovedBit), so the move pass only
+// bins it and draws its first-order reactions, as the reference lets a
+// desorbed molecule react in the step it desorbs.
+
+enum SrfActs { kSAreflect = 0, kSAtrans = 1, kSAabsorb = 2, kSAjump = 3, kSAport = 4, kSAmult = 5, kSAno = 6,
+               kSAnone = 7, kSAadsorb = 8, kSArevdes = 9, kSAirrevdes = 10, kSAflip = 11 };
+enum MolStates { kMSsoln = 0, kMSfront = 1, kMSback = 2, kMSbsoln = 5 };
+
+// random word streams of a molecule (Philox counter word 3) for the surface paths
+constexpr uint32_t kCtrSrfWalk = 0x100u;   // + iteration: collision coins of a solution molecule
+constexpr uint32_t kCtrSrfWalk2 = 0x200u;  // + iteration: the same for the placement walk after desorption
+constexpr uint32_t kCtrSrfBound = 0x300u;  // desorption / flip coin and desorption distance
+constexpr uint32_t kCtrSrfDiff = 0x301u;   // diffusion of a bound molecule
+constexpr uint32_t kCtrSrfBWalk = 0x400u;  // + iteration: collision coins of a bound molecule
+constexpr uint32_t kCtrSrfEdge = 0x1000u;  // + 64 * iteration (+ 1 + neighbour): panel-edge choices
+
+__device__ __forceinline__ uint4 srf_draw(ull skey, uint32_t step, uint32_t word) {
+  const uint2 key = make_uint2(c_net.key0 ^ 0x68E31DA4u, c_net.key1 ^ 0xB5297A4Du);
+  return philox(make_uint4((uint32_t)skey, (uint32_t)(skey >> 32), step, word), key);
+}
+// [0,1) with 32-bit resolution (randCOD), and [0,1] (randCCD)
+__device__ __forceinline__ double u01co(uint32_t x) { return (double)x * (1.0 / 4294967296.0); }
+__device__ __forceinline__ double u01cc(uint32_t x) { return (double)x * (1.0 / 4294967295.0); }
+
+__device__ __forceinline__ const SrfRule &srf_rule(const KParams &p, int srf, int sp, int ms, int face) {
+  return p.srfrule[((srf * kMaxSpecies + sp) * 3 + (ms == kMSbsoln ? 0 : ms)) * 3 + face];
+}
+
+// surfaction (smolsurface.c:4330-4385): the action for species sp in state ms
+// meeting `face` of a panel of surface srf (kFaceNone: the per-step coin of
+// a bound molecule), with the species and state it ends in.
+__device__ int srf_action(const KParams &p, int srf, int sp, int ms, int face, uint32_t coin, int &sp2, int &ms2) {
+  const SrfRule &r = srf_rule(p, srf, sp, ms, face);
+  int act = r.act;
+  if (act != kSAmult) {
+    ms2 = ms == kMSbsoln ? kMSsoln : ms;
+    sp2 = r.newspec[ms2];
+    return act;
+  }
+  const double u = u01co(coin);
+  int k = 0;
+  while (k < 5 && !(u < r.cum[k])) ++k;
+  ms2 = k;
+  sp2 = r.newspec[k];
+  const bool to_soln = k == kMSsoln || k == kMSbsoln;
+  if (sp2 == 0) return kSAabsorb;
+  if (ms != kMSsoln && face == kFaceNone) {
+    if (k == ms) return kSAno;
+    if (to_soln) return ((r.rev >> k) & 1u) ? kSArevdes : kSAirrevdes;
+    return kSAflip;
+  }
+  if (face == kFaceFront) return k == kMSsoln ? kSAreflect : k == kMSbsoln ? kSAtrans : kSAadsorb;
+  return k == kMSsoln ? kSAtrans : k == kMSbsoln ? kSAreflect : kSAadsorb;
+}
+
+// desorbdist (SurfaceParam.c:202-220): distance from the surface at which a
+// desorbing molecule is placed, from a uniform y in [0,1]; rational fits for
+// irreversible and for reversible desorption.
+__device__ __forceinline__ double desorb_dist(double step, bool reversible, double y) {
+  const double y2 = y * y;
+  if (reversible) return step * (0.729614 * y - 0.70252 * y2) / (1.0 - 1.47494 * y + 0.484371 * y2);
+  return step * (0.571825 * y - 0.552246 * y2) / (1.0 - 1.53908 * y + 0.546424 * y2);
+}
+
+__device__ __forceinline__ int ms_face(int ms) { return ms == kMSback ? kFaceBack : kFaceFront; }
+
+// movemol2closepanel (smolsurface.c:4726-4818): bring a bound molecule that
+// diffused from posx (on panel pnl) to pos back onto the surface.  The move
+// is projected onto the panel; if it leaves the panel's outline it continues
+// on a neighbouring panel that shares the exit point (picked uniformly among
+// those that do), rotated about the shared edge into that panel's plane, or
+// bounces off the edge when there is none.
+__device__ void move_to_close_panel(double pos[3], const double posx[3], int &pnl, int ms, ull skey, uint32_t step) {
+  const int face = ms_face(ms);
+  const double eps = c_net.beps, margin = c_net.bmargin, nd = c_net.bneighdist;
+  int cur = pnl;
+  fix_to_panel(c_panels[cur], pos, face, eps);
+  if (pt_in_panel(c_panels[cur], pos)) return;
+  double via[3];
+  if (pt_in_panel(c_panels[cur], posx))
+    for (int d = 0; d < 3; ++d) via[d] = posx[d];
+  else
+    closest_panel_pt(c_panels[cur], pos, via, 0.0);
+  for (int iter = 1;; ++iter) {
+    const DevPanel &pc = c_panels[cur];
+    double edge[3];
+    int exitside = 1;
+    const int er = line_exit_panel(pc, via, pos, edge, &exitside);
+    if (er || iter > 50) {
+      move_into_panel(pc, pos, margin);
+      fix_to_panel(pc, pos, face, eps);
+      break;
+    }
+    const uint4 rr = srf_draw(skey, step, kCtrSrfEdge + 64u * (uint32_t)iter);
+    int nn = 0, newp = -1, newedge = 0;
+    double newpt[3] = {0, 0, 0};
+    for (int q = 0; q < pc.nneigh; ++q) {  // a random neighbour meeting this edge point
+      double pt[3];
+      const int en = closest_panel_pt(c_panels[pc.neigh[q]], edge, pt, 1000.0 * nd);
+      double d2 = 0;
+      for (int d = 0; d < 3; ++d) d2 += (pt[d] - edge[d]) * (pt[d] - edge[d]);
+      if (d2 < nd) {
+        ++nn;
+        if (nn == 1 || u01co(srf_draw(skey, step, kCtrSrfEdge + 64u * (uint32_t)iter + 1u + (uint32_t)q).x) < 1.0 / nn) {
+          newp = pc.neigh[q];
+          newedge = en;
+          for (int d = 0; d < 3; ++d) newpt[d] = pt[d];
+        }
+      }
+    }
+    if (nn) {
+      for (int d = 0; d < 3; ++d) pos[d] += newpt[d] - edge[d];  // close any gap between the edges
+      const DevPanel &pn = c_panels[newp];
+      double nnew[3];
+      face_normal(pn, newpt, face, nnew);
+      if (newedge) {  // the path crosses onto the new panel through its edge
+        double nold[3], en[3], np[3];
+        face_normal(pc, edge, face, nold);
+        panel_edge_normal(pn, newpt, newedge, en);
+        double dt = 0;
+        for (int d = 0; d < 3; ++d) dt += (pos[d] - newpt[d]) * en[d];
+        const int ts = dt > 0 ? -1 : 1;
+        rotate_with_normals(newpt, pos, np, nold, nnew, ts);
+        if (fabs(dt) < 0.01) {  // check the side when in doubt
+          double d2 = 0;
+          for (int d = 0; d < 3; ++d) d2 += (np[d] - newpt[d]) * en[d];
+          if (d2 > 0) rotate_with_normals(newpt, pos, np, nold, nnew, -ts);
+        }
+        for (int d = 0; d < 3; ++d) pos[d] = np[d];
+      } else {  // enters mid-panel: the reference rotates from a random direction
+        const double ro[3] = {2.0 * u01cc(rr.x) - 1.0, 2.0 * u01cc(rr.y) - 1.0, 2.0 * u01cc(rr.z) - 1.0};
+        double np[3];
+        rotate_with_normals(newpt, pos, np, ro, nnew, 0);
+        for (int d = 0; d < 3; ++d) pos[d] = np[d];
+      }
+      cur = newp;
+    } else {  // no neighbour: bounce off the edge
+      double en[3];
+      panel_edge_normal(pc, edge, exitside, en);
+      double dt = 0;
+      for (int d = 0; d < 3; ++d) dt += (pos[d] - edge[d]) * en[d];
+      for (int d = 0; d < 3; ++d) pos[d] -= 2.0 * en[d] * dt;
+      for (int d = 0; d < 3; ++d) newpt[d] = edge[d];
+    }
+    fix_to_panel(c_panels[cur], pos, face, eps);
+    for (int d = 0; d < 3; ++d) via[d] = newpt[d];
+    if (pt_in_panel(c_panels[cur], pos)) break;
+  }
+  pnl = cur;
+}
+
+// checksurfaces (smolsurface.c:5114-5182) for a solution molecule moving
+// p0 -> p1 when surface rules are in use: each crossing applies the rule of
+// the panel's surface for (species, solution, face).  Returns 0 in solution
+// at p1 (species sp possibly changed), 1 removed, 2 adsorbed: p1 is then its
+// place on panel *pnl_out in state *ms_out.  Solution molecules are kept
+// surf_eps off panels, as in surface_interact.
+__device__ int walk_soln_rules(const KParams &p, int &sp, const double p0_in[3], double p1[3], int &hits, ull skey,
+                               uint32_t step, uint32_t ctr, int &pnl_out, int &ms_out) {
+  const int np = c_net.npanel;
+  const double eps = c_net.surf_eps;
+  double p0[3] = {p0_in[0], p0_in[1], p0_in[2]};
+  for (int it = 0; it < 100; ++it) {
+    double tmin = 2.0;
+    int kmin = -1, fmin = 0;
+    for (int k = 0; k < np; ++k) {
+      int f = 0;
+      const double t = panel_cross<true>(c_panels[k], p0, p1, f);
+      if (t < tmin) { tmin = t; kmin = k; fmin = f; }
+    }
+    if (kmin < 0) {
+      for (int k = 0; k < np; ++k) {
+        const double sd = panel_sdist<true>(c_panels[k], p1);
+        if (fabs(sd) < eps) {
+          double n[3];
+          panel_normal<true>(c_panels[k], p1, n);
+          const double side = (sd > 0 || (sd == 0 && panel_sdist<true>(c_panels[k], p0) > 0)) ? 1.0 : -1.0;
+          for (int d = 0; d < 3; ++d) p1[d] += (side * eps - sd) * n[d];
+        }
+      }
+      return 0;
+    }
+    hits++;
+    const DevPanel &pn = c_panels[kmin];
+    int sp2, ms2;
+    const int act = srf_action(p, pn.srf, sp, kMSsoln, fmin, srf_draw(skey, step, ctr + (uint32_t)it).x, sp2, ms2);
+    if (act == kSAabsorb) return 1;
+    double x[3], n[3];
+    for (int d = 0; d < 3; ++d) x[d] = p0[d] + tmin * (p1[d] - p0[d]);
+    if (act == kSAadsorb) {
+      for (int d = 0; d < 3; ++d) p1[d] = x[d];
+      if (!pt_in_panel(pn, p1)) move_into_panel(pn, p1, c_net.bmargin);
+      fix_to_panel(pn, p1, ms_face(ms2), c_net.beps);
+      sp = sp2;
+      pnl_out = kmin;
+      ms_out = ms2;
+      return 2;
+    }
+    panel_normal<true>(pn, x, n);
+    const double side = (fmin == 0) ? 1.0 : -1.0;
+    if (act == kSAreflect) {
+      double dot = 0;
+      for (int d = 0; d < 3; ++d) dot += (p1[d] - x[d]) * n[d];
+      for (int d = 0; d < 3; ++d) p1[d] -= 2.0 * dot * n[d];
+      for (int d = 0; d < 3; ++d) p0[d] = x[d] + side * eps * n[d];
+    } else {
+      for (int d = 0; d < 3; ++d) p0[d] = x[d] - side * eps * n[d];
+    }
+    if (sp2 != sp) {  // molchangeident: the rest of the step at the new species' diffusion
+      const double f = c_net.sstep[sp] > 0 ? c_net.sstep[sp2] / c_net.sstep[sp] : 1.0;
+      for (int d = 0; d < 3; ++d) p1[d] = x[d] + f * (p1[d] - x[d]);
+      sp = sp2;
+    }
+  }
+  for (int d = 0; d < 3; ++d) p1[d] = p0_in[d];
+  return 0;
+}
+
+// The per-step coin of a bound molecule (checksurfacebound :5184 through
+// dosurfinteract with no face, :5022-5052): returns 0 still bound (a flip
+// changes state and species in place), 1 removed, 2 desorbed - x0 is then
+// the point on the panel it leaves from, x1 its place in solution
+// (desorbdist along the face's normal) and sp its species.
+__device__ int bound_coin(const KParams &p, BoundMol &m, int &sp, ull skey, uint32_t step, double x0[3], double x1[3]) {
+  const DevPanel &pn = c_panels[m.pnl];
+  const uint4 r = srf_draw(skey, step, kCtrSrfBound);
+  int sp2, ms2;
+  const int act = srf_action(p, pn.srf, sp, m.ms, kFaceNone, r.x, sp2, ms2);
+  if (act == kSAabsorb) return 1;
+  if (act == kSArevdes || act == kSAirrevdes) {
+    const int f = ms2 == kMSsoln ? kFaceFront : kFaceBack;
+    for (int d = 0; d < 3; ++d) x0[d] = m.x[d];
+    fix_to_panel(pn, x0, f, c_net.beps);
+    const double dist = desorb_dist(c_net.sstep[sp2], act == kSArevdes, u01cc(r.y));
+    double n[3];
+    face_normal(pn, x0, f, n);
+    for (int d = 0; d < 3; ++d) x1[d] = x0[d] + dist * n[d];
+    sp = sp2;
+    return 2;
+  }
+  if (act == kSAflip) {
+    m.ms = ms2;
+    sp = sp2;
+    fix_to_panel(pn, m.x, ms_face(ms2), c_net.beps);
+  }
+  return 0;
+}
+
+// Crossings of other panels by a bound molecule's move from posx (on panel
+// pnlx) to m.x (checksurfaces on a surface-bound molecule, dosurfinteract
+// :4930-5020): a neighbouring panel is crossed (transmit) or, with
+// neighbor_action hop, hopped onto with probability 1/2; other panels apply
+// their surface's rule for the molecule's state.  Returns 0 still bound, 1
+// removed.
+__device__ int walk_bound(const KParams &p, BoundMol &m, int &sp, const double posx[3], int pnlx, int &hits, ull skey,
+                          uint32_t step) {
+  const int np = c_net.npanel;
+  const double eps = c_net.beps;
+  double via[3] = {posx[0], posx[1], posx[2]};
+  for (int it = 0; it < 100; ++it) {
+    double tmin = 2.0;
+    int kmin = -1, fmin = 0;
+    for (int k = 0; k < np; ++k) {
+      if (k == m.pnl) continue;
+      int f = 0;
+      const double t = panel_cross<true>(c_panels[k], via, m.x, f);
+      if (t < tmin) { tmin = t; kmin = k; fmin = f; }
+    }
+    if (kmin < 0) return 0;
+    hits++;
+    double x[3];
+    for (int d = 0; d < 3; ++d) x[d] = via[d] + tmin * (m.x[d] - via[d]);
+    const DevPanel &pk = c_panels[kmin];
+    const DevPanel &pm = c_panels[m.pnl];
+    bool neigh = false;
+    for (int q = 0; q < pm.nneigh; ++q) neigh = neigh || pm.neigh[q] == kmin;
+    const uint4 r = srf_draw(skey, step, kCtrSrfBWalk + (uint32_t)it);
+    int act, sp2 = sp, ms2 = m.ms;
+    if (neigh) act = (pm.neighhop && u01co(r.y) < 0.5) ? kSAadsorb : kSAtrans;
+    else act = srf_action(p, pk.srf, sp, m.ms, fmin, r.x, sp2, ms2);
+    if (act == kSAabsorb) return 1;
+    if (act == kSAadsorb) {  // onto panel kmin
+      const int old = m.pnl, oldms = m.ms;
+      for (int d = 0; d < 3; ++d) m.x[d] = x[d];
+      if (!pt_in_panel(pk, m.x)) move_into_panel(pk, m.x, c_net.bmargin);
+      fix_to_panel(c_panels[old], m.x, ms_face(oldms), eps);
+      fix_to_panel(pk, m.x, ms_face(ms2), eps);
+      m.pnl = kmin;
+      m.ms = ms2;
+      sp = sp2;
+      return 0;
+    }
+    if (act == kSAreflect) {  // reflection within the plane of the starting panel (surfacereflect :4852-4868)
+      double n[3], n2[3];
+      face_normal(pk, x, fmin, n);
+      face_normal(c_panels[pnlx], x, kFaceFront, n2);
+      const double c = dot3(n, n2);
+      for (int d = 0; d < 3; ++d) n[d] -= c * n2[d];
+      double l = sqrt(dot3(n, n));
+      if (l == 0) l = 1;
+      for (int d = 0; d < 3; ++d) n[d] /= l;
+      double a = 0, b = 0;
+      for (int d = 0; d < 3; ++d) a += (m.x[d] - x[d]) * n2[d];
+      for (int d = 0; d < 3; ++d) m.x[d] -= n2[d] * a;
+      for (int d = 0; d < 3; ++d) b += (m.x[d] - x[d]) * n[d];
+      for (int d = 0; d < 3; ++d) m.x[d] -= 2.0 * n[d] * b;
+      fix_to_panel(pk, x, fmin, eps);
+      m.pnl = pnlx;
+      move_to_close_panel(m.x, posx, m.pnl, m.ms, skey, step);
+      if (panel_side(pk, m.x, nullptr) != fmin) {  // went to the wrong side: back to the prior place
+        for (int d = 0; d < 3; ++d) m.x[d] = posx[d];
+        m.pnl = pnlx;
+        return 0;
+      }
+    } else {  // transmit (and no action)
+      fix_to_panel(pk, x, fmin == kFaceFront ? kFaceBack : kFaceFront, eps);
+    }
+    if (sp2 != sp) {
+      const double f = c_net.bstep[sp][m.ms - 1] > 0 ? c_net.bstep[sp2][m.ms - 1] / c_net.bstep[sp][m.ms - 1] : 1.0;
+      for (int d = 0; d < 3; ++d) m.x[d] = x[d] + f * (m.x[d] - x[d]);
+      sp = sp2;
+    }
+    for (int d = 0; d < 3; ++d) via[d] = x[d];
+  }
+  for (int d = 0; d < 3; ++d) m.x[d] = posx[d];
+  m.pnl = pnlx;
+  return 0;
+}
+
+__device__ __forceinline__ void push_bound(const KParams &p, const BoundMol &m) {
+  const int k = atomicAdd(p.bd_out_n, 1);
+  if (k < p.bcap) {
+    p.bd_out[k] = m;
+  } else {
+    atomicSub(p.bd_out_n, 1);
+    atomicOr(p.status, kStBoundCap);
+  }
+}
+
+// species count moves with a species change (single simulations: replicate 0)
+__device__ __forceinline__ void move_count(const KParams &p, int from, int to) {
+  if (from == to) return;
+  atomicAdd((unsigned long long *)&p.spcount[from], (unsigned long long)(-1ll));
+  atomicAdd((unsigned long long *)&p.spcount[to], 1ull);
+}
+
+// The move pass's surface step for a solution molecule when surface rules are
+// in use.  Returns 1 when the molecule is removed, 3 when it was bound
+// (appended to the output bound list after its per-step coin), else 0 with
+// the molecule in solution at x1 (a molecule that adsorbs and desorbs again
+// within the step stays in solution at its desorbed place); species changes
+// update *id and the species counts.
+__device__ __noinline__ int soln_surface_bound(const KParams &p, ull &id, const double x0[3], double x1[3], int &hits,
+                                               uint32_t step) {
+  const ull skey = id_stream(id);
+  const int sp0 = id_species(id);
+  int sp = sp0, pnl = 0, ms = 0;
+  const int w = walk_soln_rules(p, sp, x0, x1, hits, skey, step, kCtrSrfWalk, pnl, ms);
+  if (w == 1) return 1;
+  if (w == 2) {
+    BoundMol m;
+    for (int d = 0; d < 3; ++d) m.x[d] = x1[d];
+    m.pnl = pnl;
+    m.ms = ms;
+    double y0[3], y1[3];
+    const int c = bound_coin(p, m, sp, skey, step, y0, y1);
+    if (c == 1) return 1;
+    bool bound = true;
+    if (c == 2) {
+      int pnl2 = 0, ms2 = 0;
+      const int w2 = walk_soln_rules(p, sp, y0, y1, hits, skey, step, kCtrSrfWalk2, pnl2, ms2);
+      if (w2 == 1) return 1;
+      if (w2 == 0) {
+        bound = false;
+        for (int d = 0; d < 3; ++d) x1[d] = y1[d];
+      } else {
+        for (int d = 0; d < 3; ++d) m.x[d] = y1[d];
+        m.pnl = pnl2;
+        m.ms = ms2;
+      }
+    }
+    if (bound) {
+      m.id = make_id(sp, 0, id_serno(id));
+      push_bound(p, m);
+      move_count(p, sp0, sp);
+      return 3;
+    }
+  }
+  if (sp != sp0) {
+    move_count(p, sp0, sp);
+    id = make_id(sp, 0, id_serno(id));
+  }
+  return 0;
+}
+
 // First-order decision when the reaction whose coin succeeded (list slot m)
 // is restricted to a compartment (unireact, smolreact.c:3040-3050): it fires
 // only if the molecule's new position lies in the compartment; otherwise the
@@ -466,14 +882,17 @@ __device__ __noinline__ int uni_in_cmpt(const uint32_t *thr, int nuni, int sp, i
   return 0;
 }
 
+// advance_one's result for a molecule that became surface-bound
+constexpr int kFateBound = -2;
+
 // Move one molecule by one step (diffuse smolmolec.c:3115, checkwalls
 // smolwall.c:368, unireact decision smolreact.c:2997): returns 0 alive,
 // 1 removed by a wall, 2+r first-order reaction r fired (position is the
 // post-move position).
 template <bool SINGLE, int SURF>
-__device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, const KParams &p,
+__device__ __forceinline__ int advance_one(float4 &pc, ull &id, uint32_t step, const KParams &p,
                                            const float *gtab, int rebin_only, int &hits) {
-  const int sp = id_species(id);
+  int sp = id_species(id);
   const int rep = SINGLE ? 0 : id_rep(id);
   const DevGeo &g = geo_of<SINGLE>(p, rep);
   int ix[3];
@@ -523,61 +942,72 @@ __device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, co
       dsp[2] = fadd(dsp[2], dr[2]);
     }
   }
-  const int ix0[3] = {ix[0], ix[1], ix[2]};
-  const float u0[3] = {u[0], u[1], u[2]};
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    if (d >= g.dim) continue;
-    float w = fadd(u[d], dsp[d]);
-    int j = ix[d];
-    renorm(w, j, g.h[d], g.inv_h[d]);
-    if (j <= 0 || j >= g.n[d] - 1) {
-      if (walls_dim(w, j, g, d, hits)) return 1;
-      clamp_cell(w, j, g, d);
-    }
-    u[d] = w;
-    ix[d] = j;
-  }
-  if (SURF) {
-    float a0[3], a1[3];
-    for (int d = 0; d < 3; ++d) {
-      a0[d] = (float)ix0[d] * g.h[d] + u0[d];
-      a1[d] = (float)ix[d] * g.h[d] + u[d];
-    }
-    if (surface_near<SURF == 2>(a0, a1, p.boxmask, g.cell0 + (ix0[2] * g.n[1] + ix0[1]) * g.n[0] + ix0[0])) {
-      double x0[3], x1[3];
-      to_abs(g, ix0, u0, x0);
-      to_abs(g, ix, u, x1);
-      if (surface_interact<SURF == 2>(sp, x0, x1, c_net.surf_eps, hits)) return 1;
-      from_abs(g, x1, ix, u);
-    }
-  }
-  if (c_net.any_absorb && !c_net.inject) {
-    // Absorbing walls also remove molecules that stayed inside with probability
-    // exp(-2*dold*dnew/step^2) (smolwall.c:417-420); the reference applies that
-    // test in both wall passes of a step (smolsim.cpp:2625 and :2662), so the
-    // survival probability is (1-p)^2.
-    const float ds = p.difstep[rep * c_net.nsp + sp];
-    const float inv2 = (ds > 0.f) ? __frcp_rn(fmul(ds, ds)) : 0.f;
-    uint4 r2 = make_uint4(0, 0, 0, 0);
-    int have = 0;
+  // a molecule that desorbed this step was placed already: only binned here
+  const bool moved = SURF == 3 && (__float_as_uint(pc.w) & kMovedBit);
+  if (!moved) {
+    const int ix0[3] = {ix[0], ix[1], ix[2]};
+    const float u0[3] = {u[0], u[1], u[2]};
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       if (d >= g.dim) continue;
+      float w = fadd(u[d], dsp[d]);
+      int j = ix[d];
+      renorm(w, j, g.h[d], g.inv_h[d]);
+      if (j <= 0 || j >= g.n[d] - 1) {
+        if (walls_dim(w, j, g, d, hits)) return 1;
+        clamp_cell(w, j, g, d);
+      }
+      u[d] = w;
+      ix[d] = j;
+    }
+    if (SURF) {
+      float a0[3], a1[3];
+      for (int d = 0; d < 3; ++d) {
+        a0[d] = (float)ix0[d] * g.h[d] + u0[d];
+        a1[d] = (float)ix[d] * g.h[d] + u[d];
+      }
+      if (surface_near<(SURF >= 2)>(a0, a1, p.boxmask, g.cell0 + (ix0[2] * g.n[1] + ix0[1]) * g.n[0] + ix0[0])) {
+        double x0[3], x1[3];
+        to_abs(g, ix0, u0, x0);
+        to_abs(g, ix, u, x1);
+        if (SURF == 3) {
+          const int r = soln_surface_bound(p, id, x0, x1, hits, step);
+          if (r == 1) return 1;
+          if (r == 3) return kFateBound;
+          sp = id_species(id);
+        } else if (surface_interact<(SURF >= 2)>(sp, x0, x1, c_net.surf_eps, hits)) {
+          return 1;
+        }
+        from_abs(g, x1, ix, u);
+      }
+    }
+    if (c_net.any_absorb && !c_net.inject) {
+      // Absorbing walls also remove molecules that stayed inside with probability
+      // exp(-2*dold*dnew/step^2) (smolwall.c:417-420); the reference applies that
+      // test in both wall passes of a step (smolsim.cpp:2625 and :2662), so the
+      // survival probability is (1-p)^2.
+      const float ds = p.difstep[rep * c_net.nsp + sp];
+      const float inv2 = (ds > 0.f) ? __frcp_rn(fmul(ds, ds)) : 0.f;
+      uint4 r2 = make_uint4(0, 0, 0, 0);
+      int have = 0;
 #pragma unroll
-      for (int side = 0; side < 2; ++side) {
-        if (g.wall[2 * d + side] != kWallAbsorb || ds <= 0.f) continue;
-        float dn, dold;
-        if (side == 0) { dn = dist_low(ix[d], u[d], g.h[d]); dold = dist_low(ix0[d], u0[d], g.h[d]); }
-        else { dn = dist_high(ix[d], u[d], g, d); dold = dist_high(ix0[d], u0[d], g, d); }
-        const float x = fmul(fmul(2.f, fmul(dn, dold)), inv2);
-        if (x > 80.f) continue;
-        const float pr = __expf(-x);
-        const float pe = fmul(pr, fsub(2.f, pr));  // 1-(1-p)^2
-        if (!have) { r2 = philox(make_uint4((uint32_t)skey, (uint32_t)(skey >> 32), step, 1u), key); have = 1; }
-        const uint32_t bits = (d == 0) ? (side ? r2.y : r2.x) : (d == 1) ? (side ? r2.w : r2.z)
-                                        : (side ? (r2.x ^ r2.w) : (r2.y ^ r2.z));
-        if (u01f_open(bits) < pe) { hits++; return 1; }
+      for (int d = 0; d < 3; ++d) {
+        if (d >= g.dim) continue;
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+          if (g.wall[2 * d + side] != kWallAbsorb || ds <= 0.f) continue;
+          float dn, dold;
+          if (side == 0) { dn = dist_low(ix[d], u[d], g.h[d]); dold = dist_low(ix0[d], u0[d], g.h[d]); }
+          else { dn = dist_high(ix[d], u[d], g, d); dold = dist_high(ix0[d], u0[d], g, d); }
+          const float x = fmul(fmul(2.f, fmul(dn, dold)), inv2);
+          if (x > 80.f) continue;
+          const float pr = __expf(-x);
+          const float pe = fmul(pr, fsub(2.f, pr));  // 1-(1-p)^2
+          if (!have) { r2 = philox(make_uint4((uint32_t)skey, (uint32_t)(skey >> 32), step, 1u), key); have = 1; }
+          const uint32_t bits = (d == 0) ? (side ? r2.y : r2.x) : (d == 1) ? (side ? r2.w : r2.z)
+                                          : (side ? (r2.x ^ r2.w) : (r2.y ^ r2.z));
+          if (u01f_open(bits) < pe) { hits++; return 1; }
+        }
       }
     }
   }
@@ -593,7 +1023,7 @@ __device__ __forceinline__ int advance_one(float4 &pc, ull id, uint32_t step, co
       for (int m = 0; m < nuni; ++m)
         if (r.w < thr[m]) {
           const int rx = c_net.uni_list[sp][m];
-          if (SURF == 2 && c_net.cmpt[1][rx]) return uni_in_cmpt(thr, nuni, sp, m, pc, g, skey, step);
+          if (SURF >= 2 && c_net.cmpt[1][rx]) return uni_in_cmpt(thr, nuni, sp, m, pc, g, skey, step);
           return 2 + rx;
         }
     }
@@ -626,6 +1056,7 @@ __global__ void k_begin(KParams p, int bump_step) {
     *p.nev = 0;
     *p.ncand = 0;
     *p.q_n = 0;
+    if (bump_step && p.bd_out_n) *p.bd_out_n = 0;  // a re-binning pass leaves the bound list alone
   }
 }
 
@@ -731,11 +1162,16 @@ __global__ void __launch_bounds__(256, SURF ? SMOLB_SURF_MOVE_BLOCKS : SMOLB_MOV
     }
     int fate = -1;
     int hits = 0;
+    const ull id_in = id;
     if (valid) fate = advance_one<SINGLE, SURF>(pc, id, step, p, gtab, rebin_only, hits);
+    if (SURF == 3 && id != id_in && fate != kFateBound) {  // species changed at a surface
+      if (i < na) p.a_id[i] = id;
+      else const_cast<ull *>(p.p_id)[i - na] = id;
+    }
     const bool alive = (fate == 0);
     if (i < total) p.tmp[i] = alive ? pc : make_float4(0.f, 0.f, 0.f, __uint_as_float(kTmpGone));
     count_box<SINGLE>(p, alive, pc, id);
-    if (valid && !alive) {
+    if (valid && !alive && fate != kFateBound) {
       if (fate == 1) {
         atomicAdd((unsigned long long *)&p.spcount[id_rep(id) * c_net.nsp + id_species(id)],
                   (unsigned long long)(-1ll));
@@ -753,6 +1189,91 @@ __global__ void __launch_bounds__(256, SURF ? SMOLB_SURF_MOVE_BLOCKS : SMOLB_MOV
   }
   if (hits_acc) atomicAdd(&p.counters[0], (unsigned long long)hits_acc);
   if (!rebin_only) births(p, step);
+}
+
+// Step of the surface-bound molecules, launched before the move pass: a
+// mobile bound state diffuses with the move's Gaussian table and is brought
+// back onto the surface (movemol2closepanel), its path is checked against
+// the other panels, then the per-step desorption / flip coin is drawn
+// (diffuse smolmolec.c:3164-3168, checksurfaces, checksurfacebound).
+// Molecules still bound go to the output bound list; desorbed ones, after
+// their placement walk, to the product list with kMovedBit set.
+__global__ void __launch_bounds__(256) k_bound(KParams p) {
+  pdl_launch_dependents();
+  pdl_wait();
+  const int n = *p.bd_in_n;
+  const uint32_t step = *p.step;
+  int hits_acc = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    BoundMol m = p.bd_in[i];
+    const int sp0 = id_species(m.id);
+    int sp = sp0;
+    const ull skey = id_stream(m.id);
+    const double posx[3] = {m.x[0], m.x[1], m.x[2]};
+    const int pnlx = m.pnl;
+    int hits = 0;
+    bool dead = false, bound = true;
+    const double ds = c_net.bstep[sp][m.ms - 1];
+    if (ds > 0) {
+      const uint4 r = srf_draw(skey, step, kCtrSrfDiff);
+      const uint32_t gm = c_net.gmask;
+      m.x[0] += ds * (double)p.gtab[r.x & gm];
+      m.x[1] += ds * (double)p.gtab[r.y & gm];
+      m.x[2] += ds * (double)p.gtab[r.z & gm];
+      move_to_close_panel(m.x, posx, m.pnl, m.ms, skey, step);
+      dead = walk_bound(p, m, sp, posx, pnlx, hits, skey, step) == 1;
+    }
+    if (!dead) {
+      double x0[3], x1[3];
+      const int c = bound_coin(p, m, sp, skey, step, x0, x1);
+      if (c == 1) {
+        dead = true;
+      } else if (c == 2) {
+        int pnl2 = 0, ms2 = 0;
+        const int w = walk_soln_rules(p, sp, x0, x1, hits, skey, step, kCtrSrfWalk2, pnl2, ms2);
+        if (w == 1) {
+          dead = true;
+        } else if (w == 2) {
+          for (int d = 0; d < 3; ++d) m.x[d] = x1[d];
+          m.pnl = pnl2;
+          m.ms = ms2;
+        } else {  // into the product list, already moved
+          bound = false;
+          int ix[3];
+          float u[3];
+          from_abs(c_geo0, x1, ix, u);
+          const float4 pc = make_float4(u[0], u[1], u[2], __uint_as_float(pack_cell(ix[0], ix[1], ix[2]) | kMovedBit));
+          int *pn = const_cast<int *>(p.p_n);
+          const int k = atomicAdd(pn, 1);
+          if (k < p.pcap) {
+            const_cast<float4 *>(p.p_pc)[k] = pc;
+            const_cast<ull *>(p.p_id)[k] = make_id(sp, 0, id_serno(m.id));
+          } else {
+            atomicSub(pn, 1);
+            atomicOr(p.status, kStProdCap);
+            dead = true;
+          }
+        }
+      }
+    }
+    if (dead) {
+      atomicAdd((unsigned long long *)&p.spcount[sp0], (unsigned long long)(-1ll));
+    } else {
+      move_count(p, sp0, sp);
+      if (bound) {
+        m.id = make_id(sp, 0, id_serno(m.id));
+        push_bound(p, m);
+      }
+    }
+    hits_acc += hits;
+  }
+  if (hits_acc) atomicAdd(&p.counters[0], (unsigned long long)hits_acc);
+}
+
+// Species counts of an uploaded bound list (added to the solution counts).
+__global__ void k_bound_species_count(const BoundMol *m, const int *n, long long *spcount) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < *n; i += gridDim.x * blockDim.x)
+    atomicAdd((unsigned long long *)&spcount[id_species(m[i].id)], 1ull);
 }
 
 // Scatter pass: a pure permutation of the moved molecules into box order.
@@ -1151,8 +1672,8 @@ __device__ ull search_partner_in(const KParams &p, int i, float4 pc, ull id, uin
           const float vy = (q.y - pc.y) + (float)dy * g.h[1];
           const float vz = (q.z - pc.z) + (float)dz * g.h[2];
           const float d2 = vx * vx + vy * vy + vz * vz;
-          if (pair_reaction<SURF == 2>(p, rep, sp, spj, d2, ka, id_stream(jd), step, i, j) < 0) continue;
-          if (SURF && pair_crosses_surface_call<SURF == 2>(g, pc, vx, vy, vz)) continue;
+          if (pair_reaction<(SURF >= 2)>(p, rep, sp, spj, d2, ka, id_stream(jd), step, i, j) < 0) continue;
+          if (SURF && pair_crosses_surface_call<(SURF >= 2)>(g, pc, vx, vy, vz)) continue;
           ncand++;
           const ull k = ((ull)__float_as_uint(d2) << 32) | (uint32_t)j;
           if (k < best) best = k;
@@ -1191,8 +1712,8 @@ __device__ __forceinline__ void try_pair(const KParams &p, int i, ull idi, int s
   if (d2 > rs2) return;
   const int spj = id_species(jd);
   if (spj == kDeadSpecies || !((c_net.pair_mask[sp] >> spj) & 1u)) return;
-  if (SURF && pair_crosses_surface_call<SURF == 2>(p.geo[rep], pc, vx, vy, vz)) return;
-  if (pair_reaction<SURF == 2>(p, rep, sp, spj, d2, id_stream(idi), id_stream(jd), step, i, j) < 0) return;
+  if (SURF && pair_crosses_surface_call<(SURF >= 2)>(p.geo[rep], pc, vx, vy, vz)) return;
+  if (pair_reaction<(SURF >= 2)>(p, rep, sp, spj, d2, id_stream(idi), id_stream(jd), step, i, j) < 0) return;
   const uint32_t db = __float_as_uint(d2);
   const ull k = ((ull)db << 32) | (uint32_t)j;
   if (best != ~0ull) extra++;
@@ -1329,8 +1850,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_pairs_tile(KParams p) {
           // the reaction test draws from a stateless stream, so it can go
           // before the (rarely needed) surface test
           if (spb != kDeadSpecies && ((c_net.pair_mask[spa] >> spb) & 1u) &&
-              pair_reaction<SURF == 2>(p, repa, spa, spb, d2, id_stream(ida), id_stream(idb), step, wb + o, wb + tj) >= 0 &&
-              !(SURF && pair_crosses_surface<SURF == 2>(p.geo[repa], a, vx, vy, vz)))
+              pair_reaction<(SURF >= 2)>(p, repa, spa, spb, d2, id_stream(ida), id_stream(idb), step, wb + o, wb + tj) >= 0 &&
+              !(SURF && pair_crosses_surface<(SURF >= 2)>(p.geo[repa], a, vx, vy, vz)))
             extra += register_pair(p, wb + o, wb + tj, d2);
         }
       }
@@ -1347,8 +1868,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_pairs_tile(KParams p) {
         const ull idb = p.b_id[j];
         const int spb = id_species(idb);
         if (spb != kDeadSpecies && ((c_net.pair_mask[sp] >> spb) & 1u) &&
-            pair_reaction<SURF == 2>(p, rep, sp, spb, d2, id_stream(idi), id_stream(idb), step, i, j) >= 0 &&
-            !(SURF && pair_crosses_surface<SURF == 2>(p.geo[rep], pc, vx, vy, vz)))
+            pair_reaction<(SURF >= 2)>(p, rep, sp, spb, d2, id_stream(idi), id_stream(idb), step, i, j) >= 0 &&
+            !(SURF && pair_crosses_surface<(SURF >= 2)>(p.geo[rep], pc, vx, vy, vz)))
           extra += register_pair(p, i, j, d2);
       }
     }
@@ -1636,7 +2157,7 @@ __device__ __forceinline__ void commit_body(const KParams &p, uint32_t step) {
     if (spi == kDeadSpecies || spj == kDeadSpecies) continue;
     const int rep = id_rep(idi);
     const float d2 = __uint_as_float((uint32_t)(bi >> 32));
-    const int r = pair_reaction<SURF == 2>(p, rep, spi, spj, d2, id_stream(idi), id_stream(idj), step, i, j);
+    const int r = pair_reaction<(SURF >= 2)>(p, rep, spi, spj, d2, id_stream(idi), id_stream(idj), step, i, j);
     if (r < 0) continue;
     // reactant 1 of reaction r is molecule a
     const bool i_first = (c_net.rct[2][r][0] == spi);
@@ -1746,7 +2267,7 @@ __device__ __forceinline__ void place_event(const KParams &p, const Event &e, ui
       site[d] = w;
       cell[d] = j;
     }
-    if (SURF == 2 && c_net.cmpt[0][r]) birth_in_cmpt(c_net.cmpt[0][r] - 1, g, e.key, step, site, cell);
+    if (SURF >= 2 && c_net.cmpt[0][r]) birth_in_cmpt(c_net.cmpt[0][r] - 1, g, e.key, step, site, cell);
   } else {
     site[0] = e.site.x; site[1] = e.site.y; site[2] = e.site.z;
     unpack_cell(__float_as_uint(e.site.w), cell[0], cell[1], cell[2]);
@@ -1836,22 +2357,44 @@ __device__ __forceinline__ void place_event(const KParams &p, const Event &e, ui
         if (walls_dim(w[d], c[d], g, d, hits)) dead = true;
       clamp_cell(w[d], c[d], g, d);
     }
+    const ull serno = (place && q < 2) ? keep_sn[q]
+                                       : kProductSernoBit |
+                                             (mix64(e.key ^ ((ull)q << 50) ^ ((ull)step << 20) ^ (ull)(order * 97 + r)) &
+                                              (kProductSernoBit - 1));
+    int fsp = psp;
     if (SURF && !dead) {
       // new molecules are checked against surfaces from the reaction site
       // (smolsim.cpp:2656-2660, reborn pass of checksurfaces)
       double x0[3], x1[3];
       to_abs(g, cell, site, x0);
       to_abs(g, c, w, x1);
-      if (surface_interact<SURF == 2>(psp, x0, x1, c_net.surf_eps, hits)) dead = true;
-      else from_abs(g, x1, c, w);
+      if (SURF == 3) {
+        int pnl = 0, ms = 0;
+        const int res = walk_soln_rules(p, fsp, x0, x1, hits, id_stream(make_id(psp, rep, serno)), step, kCtrSrfWalk,
+                                        pnl, ms);
+        if (res == 1) {
+          dead = true;
+        } else if (res == 2) {  // adsorbed on placement: into the bound list
+          BoundMol bm;
+          for (int d = 0; d < 3; ++d) bm.x[d] = x1[d];
+          bm.id = make_id(fsp, 0, serno);
+          bm.pnl = pnl;
+          bm.ms = ms;
+          push_bound(p, bm);
+          atomicAdd((unsigned long long *)&p.spcount[fsp], 1ull);
+          dead = true;
+        } else {
+          from_abs(g, x1, c, w);
+        }
+      } else if (surface_interact<(SURF >= 2)>(psp, x0, x1, c_net.surf_eps, hits)) {
+        dead = true;
+      } else {
+        from_abs(g, x1, c, w);
+      }
     }
     if (hits) atomicAdd(&p.counters[0], (unsigned long long)hits);
     if (dead) continue;
-    const ull serno = (place && q < 2) ? keep_sn[q]
-                                       : kProductSernoBit |
-                                             (mix64(e.key ^ ((ull)q << 50) ^ ((ull)step << 20) ^ (ull)(order * 97 + r)) &
-                                              (kProductSernoBit - 1));
-    emit(make_float4(w[0], w[1], w[2], __uint_as_float(pack_cell(c[0], c[1], c[2]))), make_id(psp, rep, serno));
+    emit(make_float4(w[0], w[1], w[2], __uint_as_float(pack_cell(c[0], c[1], c[2]))), make_id(fsp, rep, serno));
   }
 }
 
@@ -1946,7 +2489,7 @@ __device__ __forceinline__ void persist_commit(const KParams &p, int rep, const 
     const int spi = id_species(idi), spj = id_species(idj);
     if (spi == kDeadSpecies || spj == kDeadSpecies) continue;
     const float d2 = __uint_as_float((uint32_t)(bi >> 32));
-    const int r = pair_reaction<SURF == 2>(p, rep, spi, spj, d2, id_stream(idi), id_stream(idj), step, i, j);
+    const int r = pair_reaction<(SURF >= 2)>(p, rep, spi, spj, d2, id_stream(idi), id_stream(idj), step, i, j);
     if (r < 0) continue;
     const bool i_first = (c_net.rct[2][r][0] == spi);
     const int a = i_first ? i : j, b = i_first ? j : i;
@@ -1996,7 +2539,7 @@ __device__ __forceinline__ int persist_step(const KParams &p, int rep, int off, 
   for (int i = tid; i < n; i += T) {
     const int idx = off + i;
     float4 pc = p.a_pc[idx];
-    const ull id = p.a_id[idx];
+    ull id = p.a_id[idx];  // the persistent kernel runs without surfaces: id is not changed
     int fate = -1;
     if (id_species(id) != kDeadSpecies) fate = advance_one<false, SURF>(pc, id, step, p, gtab, 0, hits);
     if (fate == 0) {
@@ -2486,6 +3029,10 @@ class EngineImpl {
   float4 *d_injval = nullptr;
   int inj_n = 0;
   bool inj_pending = false;
+  // surface-bound molecules: lists by parity (as the sorted buffers), rules
+  BoundMol *d_bd[2] = {nullptr, nullptr};
+  long long bcap = 0;
+  SrfRule *d_srfrule = nullptr;
 
   // persistent ensemble engine (k_persist): its own molecule layout, one
   // region per replicate; the step pipeline's buffers are refilled from it
@@ -2618,9 +3165,12 @@ class EngineImpl {
     void *ptrs[] = {d_boxmask, d_difm, d_rsearch, d_geo, d_difstep, d_driftdt, d_bind2, d_pairprob, d_prdpos, d_gtab, d_unithr,
                     d_births, d_pc[0], d_pc[1], d_ppc[0], d_ppc[1], d_id[0], d_id[1], d_pid[0],
                     d_pid[1], d_face, d_tmp, d_counts, d_step, d_cnt, d_start, d_scan_ticket, d_scan_status, d_ev, d_cand, d_best,
-                    d_counters, d_spcount, d_injkey, d_injval};
+                    d_counters, d_spcount, d_injkey, d_injval, d_bd[0], d_bd[1], d_srfrule};
     for (void *q : ptrs)
       if (q) cudaFree(q);
+    d_bd[0] = d_bd[1] = nullptr;
+    d_srfrule = nullptr;
+    bcap = 0;
     d_rsearch = nullptr;
     d_boxmask = nullptr;
     d_geo = nullptr; d_difstep = d_driftdt = d_bind2 = d_pairprob = d_prdpos = d_gtab = nullptr;
@@ -2678,6 +3228,14 @@ class EngineImpl {
     p.inj_key = d_injkey;
     p.inj_val = d_injval;
     p.inj_n = inj_n;
+    if (dnet.bound) {
+      p.srfrule = d_srfrule;
+      p.bd_in = d_bd[in];
+      p.bd_in_n = d_counts + 8 + in;
+      p.bd_out = d_bd[out];
+      p.bd_out_n = d_counts + 8 + out;
+      p.bcap = (int)bcap;
+    }
     return p;
   }
 
@@ -2736,7 +3294,7 @@ class EngineImpl {
     double *dpos = reinterpret_cast<double *>(d);
     int *dsp = reinterpret_cast<int *>(d + bpos);
     ull *dsn = serno ? reinterpret_cast<ull *>(d + ((bpos + bsp + 15) & ~(size_t)15)) : nullptr;
-    int zero[16] = {0};
+    int zero[8] = {0};  // [8], [9]: bound-list counts, carried by finish_upload
     cudaError_t e = cudaMemcpyAsync(d_counts, zero, sizeof(zero), cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dpos, pos, bpos, cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dsp, species, bsp, cudaMemcpyHostToDevice, stream);
@@ -2762,6 +3320,13 @@ class EngineImpl {
   int finish_upload(long long n, std::string *err) {
     ++upload_gen;
     int staged = (int)n;
+    if (dnet.bound && parity != 1) {  // the bound list follows the sorted buffers to parity 1
+      int nb = 0;
+      CK(cudaMemcpyAsync(&nb, d_counts + 8 + parity, sizeof(int), cudaMemcpyDeviceToHost, stream));
+      CK(cudaStreamSynchronize(stream));
+      if (nb > 0) CK(cudaMemcpyAsync(d_bd[1], d_bd[parity], (size_t)nb * sizeof(BoundMol), cudaMemcpyDeviceToDevice, stream));
+      CK(cudaMemcpyAsync(d_counts + 9, &nb, sizeof(int), cudaMemcpyHostToDevice, stream));
+    }
     parity = 0;
     CK(cudaMemcpyAsync(d_counts + 2, &staged, sizeof(int), cudaMemcpyHostToDevice, stream));
     CK(cudaMemsetAsync(d_cnt, 0, ((size_t)ncell + 1) * sizeof(int), stream));
@@ -2773,6 +3338,10 @@ class EngineImpl {
     k_species_count<<<grid_mol(), 256, 0, stream>>>(d_id[1], d_counts + 1, d_spcount, net.nspecies,
                                                     (int)reps.size() * net.nspecies);
     nlaunch++;
+    if (dnet.bound) {
+      k_bound_species_count<<<grid_small(), 256, 0, stream>>>(d_bd[1], d_counts + 9, d_spcount);
+      nlaunch++;
+    }
     CK(cudaStreamSynchronize(stream));
     CK(cudaGetLastError());
     int st = 0;
@@ -2922,6 +3491,10 @@ class EngineImpl {
     KParams p = params(par);
     launch(k_begin, 1, 32, 0, p, rebin_only ? 0 : 1);
     mark("k_begin");
+    if (dnet.bound && !rebin_only) {
+      launch(k_bound, grid_small(), 256, 0, p);
+      mark("k_bound");
+    }
     launch(k_move<SINGLE, SURF>, grid_mol(), 256, rebin_only ? 0 : adv_smem(), p, rebin_only ? 1 : 0);
     mark("k_move");
     launch(k_scan_lookback, nscanblocks, kScanThreads, 0, (const int *)d_cnt, ncell, nscanblocks, d_scan_ticket,
@@ -2951,15 +3524,18 @@ class EngineImpl {
   // Enqueue one step with the given parity (inputs A/P = buffers `par`).
   void enqueue_step(int par, bool rebin_only) {
     // surface form: 0 none, 1 rect and sphere panels only, 2 any shape or
-    // compartments (whose tests need panels to mean anything)
+    // compartments (whose tests need panels to mean anything), 3 as 2 with
+    // surface-bound states
     int surf = dnet.npanel > 0 ? 1 : 0;
     for (const DevPanel &pn : panels)
       if (pn.shape != 0 && pn.shape != 2) surf = 2;
-    if (surf && dnet.ncmpt > 0) surf = 2;
+    if (surf && (dnet.ncmpt > 0 || dnet.bound)) surf = 2;
+    if (dnet.bound) surf = 3;  // 3: any shape plus surface-bound states (single simulations)
     if (single_rep()) {
       if (surf == 0) enqueue_step_t<true, 0>(par, rebin_only);
       else if (surf == 1) enqueue_step_t<true, 1>(par, rebin_only);
-      else enqueue_step_t<true, 2>(par, rebin_only);
+      else if (surf == 2) enqueue_step_t<true, 2>(par, rebin_only);
+      else enqueue_step_t<true, 3>(par, rebin_only);
     } else {
       if (surf == 0) enqueue_step_t<false, 0>(par, rebin_only);
       else if (surf == 1) enqueue_step_t<false, 1>(par, rebin_only);
@@ -2967,7 +3543,7 @@ class EngineImpl {
     }
   }
 
-  int launches_per_step() const { return 8 + 2 * (dnet.rounds - 1); }
+  int launches_per_step() const { return 8 + 2 * (dnet.rounds - 1) + (dnet.bound ? 1 : 0); }
 
   int upload_const(std::string *err) {
     CK(cudaMemcpyToSymbolAsync(c_net, &dnet, sizeof(DevNet), 0, cudaMemcpyHostToDevice, stream));
@@ -3603,6 +4179,26 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
       E.panels.push_back(dp);
     }
   }
+  if (net.bound) {
+    // surface-bound states: single simulations through the step pipeline
+    if (reps.size() != 1) { if (err) *err = "surface-bound states need a single simulation"; return -6; }
+    if (net.panels.empty()) { if (err) *err = "surface-bound states need surfaces"; return -6; }
+    const size_t nrule = (size_t)std::max(1, net.nsrf) * kMaxSpecies * 9;
+    if (net.srf_rules.size() != nrule) { if (err) *err = "surface rule table has the wrong size"; return -6; }
+    D.bound = 1;
+    D.beps = net.srf_eps;
+    D.bmargin = net.srf_margin;
+    D.bneighdist = net.srf_neighdist;
+    for (int i = 0; i < net.nspecies; ++i) {
+      D.sstep[i] = std::sqrt(2.0 * reps[0].difc[i] * dt);
+      for (int k = 0; k < 2; ++k) D.bstep[i][k] = std::sqrt(2.0 * net.difc_bound[i][k] * dt);
+    }
+    E.bcap = E.cap;
+    for (int k = 0; k < 2; ++k) CK(cudaMalloc(&E.d_bd[k], E.bcap * sizeof(BoundMol)));
+    CK(cudaMalloc(&E.d_srfrule, nrule * sizeof(SrfRule)));
+    CK(cudaMemcpyAsync(E.d_srfrule, net.srf_rules.data(), nrule * sizeof(SrfRule), cudaMemcpyHostToDevice, E.stream));
+    CK(cudaStreamSynchronize(E.stream));
+  }
   E.cmpts.clear();
   if ((int)E.net.cmpts.size() > kMaxCmpt) { if (err) *err = "too many compartments (max 8)"; return -6; }
   for (const CmptSpec &cs : E.net.cmpts) E.cmpts.push_back(make_dev_cmpt(cs, reps[0].lo));
@@ -3697,7 +4293,7 @@ int Engine::set_molecules(long long n, const double *pos, const int *species, co
     ull sn = (serno && serno[i]) ? (ull)serno[i] : next_serno[rp]++;
     id[i] = make_id(sp, rp, sn);
   }
-  int zero[16] = {0};
+  int zero[8] = {0};  // [8], [9]: bound-list counts, carried by finish_upload
   CK(cudaMemcpyAsync(E.d_counts, zero, sizeof(zero), cudaMemcpyHostToDevice, E.stream));
   CK(cudaMemcpyAsync(E.d_ppc[0], pc.data(), n * sizeof(float4), cudaMemcpyHostToDevice, E.stream));
   CK(cudaMemcpyAsync(E.d_pid[0], id.data(), n * sizeof(ull), cudaMemcpyHostToDevice, E.stream));
@@ -3860,6 +4456,77 @@ int Engine::stats(EngineStats *s, std::string *err) {
   s->unresolved = (long long)c[4];
   s->multicand = (long long)c[5];
   s->overflow = st;
+  return 0;
+}
+
+int Engine::set_bound(long long n, const double *pos, const int *species, const int *state, const int *panel,
+                      const uint64_t *serno, std::string *err) {
+  EngineImpl &E = *impl_;
+  if (!E.dnet.bound) {
+    if (n == 0) return 0;
+    if (err) *err = "surface-bound molecules need surface rules with bound states";
+    return -6;
+  }
+  if (n > E.bcap) { if (err) *err = "more surface-bound molecules than the engine capacity"; return -9; }
+  std::vector<BoundMol> m((size_t)n);
+  for (long long i = 0; i < n; ++i) {
+    const int sp = species[i];
+    if (sp <= 0 || sp >= E.net.nspecies) { if (err) *err = "species index out of range"; return -6; }
+    if (state[i] != 1 && state[i] != 2) { if (err) *err = "bound state must be front or back"; return -6; }
+    if (panel[i] < 0 || panel[i] >= (int)E.panels.size()) { if (err) *err = "panel index out of range"; return -6; }
+    for (int d = 0; d < 3; ++d) m[i].x[d] = pos[3 * i + d] - E.reps[0].lo[d];
+    m[i].pnl = panel[i];
+    m[i].ms = state[i];
+    const ull sn = (serno && serno[i]) ? (ull)serno[i] : ((1ull << 40) + (ull)i);
+    m[i].id = make_id(sp, 0, sn);
+  }
+  const int in = E.parity;
+  const int nn = (int)n;
+  CK(cudaStreamSynchronize(E.stream));
+  if (n) CK(cudaMemcpy(E.d_bd[in], m.data(), (size_t)n * sizeof(BoundMol), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(E.d_counts + 8 + in, &nn, sizeof(int), cudaMemcpyHostToDevice));
+  // species counts: solution (sorted and product lists) plus the new bound
+  // list; a product count past the capacity (an overflow already flagged)
+  // is clamped first, as the next step would
+  int pn = 0;
+  CK(cudaMemcpy(&pn, E.d_counts + 2 + in, sizeof(int), cudaMemcpyDeviceToHost));
+  if (pn > (int)E.pcap) {
+    pn = (int)E.pcap;
+    CK(cudaMemcpy(E.d_counts + 2 + in, &pn, sizeof(int), cudaMemcpyHostToDevice));
+  }
+  const size_t nt = E.reps.size() * E.net.nspecies;
+  CK(cudaMemsetAsync(E.d_spcount, 0, nt * sizeof(long long), E.stream));
+  k_species_count<<<E.grid_mol(), 256, 0, E.stream>>>(E.d_id[in], E.d_counts + in, E.d_spcount, E.net.nspecies, (int)nt);
+  k_species_count<<<E.grid_mol(), 256, 0, E.stream>>>(E.d_pid[in], E.d_counts + 2 + in, E.d_spcount, E.net.nspecies,
+                                                      (int)nt);
+  k_bound_species_count<<<E.grid_small(), 256, 0, E.stream>>>(E.d_bd[in], E.d_counts + 8 + in, E.d_spcount);
+  E.nlaunch += 3;
+  CK(cudaStreamSynchronize(E.stream));
+  CK(cudaGetLastError());
+  ++E.upload_gen;
+  return 0;
+}
+
+int Engine::get_bound(std::vector<double> *pos, std::vector<int> *species, std::vector<int> *state,
+                      std::vector<int> *panel, std::vector<uint64_t> *serno, std::string *err) {
+  EngineImpl &E = *impl_;
+  pos->clear(); species->clear(); state->clear(); panel->clear(); serno->clear();
+  if (!E.dnet.bound) return 0;
+  const int in = E.parity;
+  int nb = 0;
+  CK(cudaStreamSynchronize(E.stream));
+  CK(cudaMemcpy(&nb, E.d_counts + 8 + in, sizeof(int), cudaMemcpyDeviceToHost));
+  nb = std::max(0, std::min<int>(nb, (int)E.bcap));
+  std::vector<BoundMol> m((size_t)nb);
+  if (nb) CK(cudaMemcpy(m.data(), E.d_bd[in], (size_t)nb * sizeof(BoundMol), cudaMemcpyDeviceToHost));
+  std::sort(m.begin(), m.end(), [](const BoundMol &a, const BoundMol &b) { return id_serno(a.id) < id_serno(b.id); });
+  for (const BoundMol &b : m) {
+    for (int d = 0; d < 3; ++d) pos->push_back(b.x[d] + E.reps[0].lo[d]);
+    species->push_back(id_species(b.id));
+    state->push_back(b.ms);
+    panel->push_back(b.pnl);
+    serno->push_back(id_serno(b.id));
+  }
   return 0;
 }
 

@@ -24,6 +24,7 @@ constexpr int kMaxPanels = 16;
 constexpr int kMaxCmpt = 8;         // compartments
 constexpr int kMaxCmptPts = 8;      // interior-defining points per compartment
 constexpr int kMaxCmptLogic = 4;    // logic terms per compartment
+constexpr int kMaxNeigh = 8;        // neighbouring panels per panel (surface-bound molecules)
 
 enum WallKind : uint8_t { kWallReflect = 0, kWallPeriodic = 1, kWallAbsorb = 2, kWallTransparent = 3 };
 
@@ -49,6 +50,24 @@ struct PanelSpec {
   uint32_t trans_back_mask;
   uint32_t refl_front_mask;     // species bitmask overriding to reflect on front
   uint32_t refl_back_mask;
+  int srf;                      // index of the panel's surface
+  int nneigh;                   // neighbouring panels (engine panel indices) for surface-bound molecules
+  int neigh[kMaxNeigh];
+  int neighhop;                 // the surface's neighbor_action: 1 hop, 0 stay
+};
+
+// One (surface, species, state, face) interaction in device form
+// (surfaction, smolsurface.c:4330): the SrfAction, and for rate-based
+// actions (SAmult) the cumulative probabilities of the destination states
+// (MolecState order soln, front, back, up, down, bsoln), the species after
+// each outcome (0: removed), and whether the reverse of each outcome has a
+// nonzero probability (reversible desorption places the molecule
+// differently).
+struct SrfRule {
+  double cum[6];
+  int8_t act;
+  int8_t newspec[6];
+  uint8_t rev;
 };
 
 // Compartment: interior points, bounding panels (indices into NetSpec::panels)
@@ -73,6 +92,14 @@ struct NetSpec {
   std::vector<PanelSpec> panels;
   std::vector<CmptSpec> cmpts;
   int cmpt[3][kMaxRxn] = {};                 // compartment of each reaction + 1 (0: none)
+  // surface-bound states (single simulations only): rules by
+  // ((surface * kMaxSpecies + species) * 3 + state) * 3 + face, state 0..2 =
+  // soln, front, back and face 0..2 = front, back, none
+  int bound = 0;
+  int nsrf = 0;
+  std::vector<SrfRule> srf_rules;
+  double difc_bound[kMaxSpecies][2] = {};    // diffusion coefficients of the front and back states
+  double srf_eps = 0, srf_margin = 0, srf_neighdist = 0;  // surfacessstruct epsilon, margin, neighdist
 };
 
 // One replicate's geometry and rate-derived parameters.
@@ -122,6 +149,13 @@ class Engine {
                     const uint64_t *serno, std::string *err);
   // Advance `nsteps` time steps (asynchronous unless sync is requested).
   int run(long long nsteps, std::string *err);
+  // Surface-bound molecules (single simulations): replace them, or copy them
+  // back sorted by serial number.  state: 1 front, 2 back; panel: engine
+  // panel index; serno 0 entries get serial numbers after every molecule's.
+  int set_bound(long long n, const double *pos, const int *species, const int *state, const int *panel,
+                const uint64_t *serno, std::string *err);
+  int get_bound(std::vector<double> *pos, std::vector<int> *species, std::vector<int> *state,
+                std::vector<int> *panel, std::vector<uint64_t> *serno, std::string *err);
   // Copy molecules back (absolute coordinates, sorted by (rep, serno)).
   int get_molecules(std::vector<double> *pos, std::vector<int> *species, std::vector<int> *rep,
                     std::vector<uint64_t> *serno, std::string *err);

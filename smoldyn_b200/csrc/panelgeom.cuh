@@ -261,6 +261,10 @@ inline DevPanel make_dev_panel(const PanelSpec &ps, const double lo[3]) {
   dp.tr_back = ps.trans_back_mask;
   dp.rf_front = ps.refl_front_mask;
   dp.rf_back = ps.refl_back_mask;
+  dp.srf = ps.srf;
+  dp.nneigh = ps.nneigh < kMaxNeigh ? ps.nneigh : kMaxNeigh;
+  for (int k = 0; k < dp.nneigh; ++k) dp.neigh[k] = ps.neigh[k];
+  dp.neighhop = ps.neighhop;
   return dp;
 }
 

@@ -602,7 +602,9 @@ int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err) {
     }
   const std::vector<int> first = surface_panel_base(sim);
   for (const CompartDef &c : sim.cmpts) net->cmpts.push_back(cmpt_spec(sim, c, first));
-  return 0;
+  int rc = derive_surface_params(sim, err);
+  if (!rc) rc = build_surface_rules(sim, net, err);
+  return rc;
 }
 
 // ---------------------------------------------------------------------------
@@ -725,8 +727,20 @@ int read_config_statement(Sim &sim, const std::string &word, const std::string &
     std::vector<int> ids;
     if (species_arg(sim, w[0], &ids)) { if (err) *err = "difc: unknown species " + w[0]; return -3; }
     if (!parse_double(w[1], &v)) { if (err) *err = "difc: bad value"; return -7; }
-    for (int i : ids) sim.species[i].difc = v;
-    sim.need_update = true;
+    if (v < 0) { if (err) *err = "diffusion coefficient needs to be >=0"; return -6; }
+    // species[(state)]: the solution state unless one is given (molsetdifc)
+    std::string st;
+    const size_t paren = w[0].find('(');
+    if (paren != std::string::npos) st = w[0].substr(paren + 1, w[0].find(')', paren) - paren - 1);
+    const bool soln = st.empty() || st == "solution" || st == "soln" || st == "fsoln" || st == "aq" || st == "all";
+    const bool front = st == "front" || st == "all", back = st == "back" || st == "all";
+    if (!soln && !front && !back) { if (err) *err = "difc: state not supported by the GPU engine: " + st; return -7; }
+    for (int i : ids) {
+      if (soln) sim.species[i].difc = v;
+      if (front) sim.species[i].difc_bound[0] = v;
+      if (back) sim.species[i].difc_bound[1] = v;
+    }
+    sim.need_update = sim.need_rebuild = true;
   } else if (word == "difm") {  // smolsim.cpp:863: species then dim*dim values
     if (!need(1 + (size_t)sim.dim * sim.dim)) return -7;
     std::vector<int> ids;
@@ -821,6 +835,15 @@ int read_config_statement(Sim &sim, const std::string &word, const std::string &
       }
       sim.pend_sp.push_back(i);
     }
+    sim.need_rebuild = true;
+  } else if (word == "surface_mol") {  // smolsim.cpp:1027
+    const int rc = read_surface_mol(sim, w, err);
+    if (rc) return rc;
+  } else if (word == "epsilon" || word == "margin" || word == "neighbor_dist" || word == "neighbour_dist") {
+    // surface simulation parameters (smolsurface.c:2060-2093)
+    if (!need(1) || !parse_double(w[0], &v)) { if (err) *err = word + ": bad value"; return -7; }
+    if (v < 0) { if (err) *err = word + " needs to be >= 0"; return -6; }
+    (word == "epsilon" ? sim.srf_epsilon : word == "margin" ? sim.srf_margin : sim.srf_neighdist) = v;
     sim.need_rebuild = true;
   } else if (word == "compartment_mol") {  // smolsim.cpp:1072
     if (!need(3)) return -7;
@@ -1101,35 +1124,11 @@ static int read_surface_statement(Sim &sim, SurfaceDef &sf, const std::string &w
     if (s == "absorb" || s == "a") return 2;
     return -1;
   };
+  const int sidx = (int)(&sf - sim.surfaces.data());
+  const int rr = read_surface_rule_statement(sim, sidx, word, w, err);
+  if (rr != 1) return rr;
   if (word == "name") {
     if (!w.empty()) sf.name = w[0];
-  } else if (word == "action") {
-    // action face species action
-    if (w.size() < 3) { if (err) *err = "action: missing parameters"; return -7; }
-    const std::string &face = w[0];
-    const int a = act_of(w[2]);
-    if (a < 0) { if (err) *err = "surface action not supported: " + w[2]; return -7; }
-    std::vector<int> ids;
-    const bool all = (w[1] == "all" || w[1] == "all(all)");
-    if (!all && species_arg(sim, w[1], &ids)) { if (err) *err = "action: unknown species " + w[1]; return -3; }
-    const bool f = (face == "front" || face == "both" || face == "all");
-    const bool b = (face == "back" || face == "both" || face == "all");
-    if (all) {
-      if (f) { sf.act_front = a; sf.absorb_front = sf.trans_front = sf.refl_front = 0; }
-      if (b) { sf.act_back = a; sf.absorb_back = sf.trans_back = sf.refl_back = 0; }
-    } else {
-      for (int i : ids) {
-        const uint32_t bit = 1u << i;
-        auto setmask = [&](uint32_t &abs, uint32_t &tr, uint32_t &rf) {
-          abs &= ~bit; tr &= ~bit; rf &= ~bit;
-          if (a == 2) abs |= bit;
-          else if (a == 1) tr |= bit;
-          else rf |= bit;
-        };
-        if (f) setmask(sf.absorb_front, sf.trans_front, sf.refl_front);
-        if (b) setmask(sf.absorb_back, sf.trans_back, sf.refl_back);
-      }
-    }
   } else if (word == "panel") {
     if (w.empty()) { if (err) *err = "panel: missing shape"; return -7; }
     const std::string &sh = w[0];
@@ -1154,8 +1153,19 @@ static int read_surface_statement(Sim &sim, SurfaceDef &sf, const std::string &w
     PanelSpec p{};
     const int rc = make_panel(sim.dim, shape, axis, prm.data(), (int)prm.size(), &p, err);
     if (rc) return rc;
-    if ((int)sf.panels.size() >= kMaxPanels) { if (err) *err = "too many panels"; return -6; }
-    sf.panels.push_back(p);
+    const std::string name = new_panel_name(sf, shape, k < w.size() ? w[k] : std::string());
+    // a name used before replaces that panel (surfaddpanel, smolsurface.c:2642-2651)
+    int same = -1;
+    for (size_t q = 0; q < sf.pnames.size(); ++q)
+      if (sf.pnames[q] == name) same = (int)q;
+    if (same >= 0) {
+      if (sf.panels[same].shape != shape) { if (err) *err = "panel name was used before for a different shape"; return -6; }
+      sf.panels[same] = p;
+    } else {
+      if ((int)sf.panels.size() >= kMaxPanels) { if (err) *err = "too many panels"; return -6; }
+      sf.panels.push_back(p);
+      sf.pnames.push_back(name);
+    }
     invalidate_compartments(sim);
   } else if (word == "color" || word == "thickness" || word == "polygon" || word == "stipple" ||
              word == "shininess") {

@@ -14,6 +14,7 @@ namespace smolb {
 struct SpeciesDef {
   std::string name;
   double difc = 0;
+  double difc_bound[2] = {0, 0};  // difc[i][MSfront], difc[i][MSback] (0 unless set)
   double drift[3] = {0, 0, 0};
   bool has_difm = false;   // anisotropic diffusion (difm statement, smolmolec.c:833)
   double difm[9] = {};     // matrix M, row-major in a 3x3 layout: step = M * sqrt(2 dt) * gaussian
@@ -43,6 +44,26 @@ struct RxnDef {
   double prdpos[kMaxProd][3] = {};
 };
 
+// Rate-based surface interaction of one (species, state, face)
+// (surfactionstruct, smoldyn.h:540-548): requested rates or probabilities by
+// destination state (MolecState order, soln..bsoln), their source (1 rate,
+// 2 probability, 3 only a new species), the species after the action, and
+// the probabilities derived from them (surfupdateparams,
+// smolsurface.c:3735-3800).
+struct SrfDetail {
+  double rate[6] = {0, 0, 0, 0, 0, 0};
+  double prob_req[6] = {0, 0, 0, 0, 0, 0};
+  int datasrc[6] = {0, 0, 0, 0, 0, 0};
+  int newspec[6] = {0, 0, 0, 0, 0, 0};
+  double prob[6] = {0, 0, 0, 0, 0, 0};
+  double cum[6] = {0, 0, 0, 0, 0, 0};
+  double rev[6] = {0, 0, 0, 0, 0, 0};
+};
+
+// Molecule states a surface's action table covers: solution, front, back
+// (MolecState 0..2); up and down are not supported.
+constexpr int kSrfStates = 3;
+
 struct SurfaceDef {
   std::string name;
   // action per face for all species unless overridden: 0 reflect 1 transmit 2 absorb
@@ -50,6 +71,26 @@ struct SurfaceDef {
   uint32_t absorb_front = 0, absorb_back = 0, trans_front = 0, trans_back = 0, refl_front = 0,
            refl_back = 0;
   std::vector<PanelSpec> panels;
+  std::vector<std::string> pnames;   // panel names (default: shape name + index within the shape)
+  // SrfAction by [species][state][face] (face 0 front, 1 back, 2 none) set
+  // by action or rate statements; -1 leaves the default (solution: the masks
+  // above; bound states: transmit at faces, no action otherwise)
+  int act[kMaxSpecies][kSrfStates][3];
+  std::map<int, SrfDetail> det;      // by (species * kSrfStates + state) * 3 + face
+  std::vector<std::vector<std::pair<int, int>>> neigh;  // per panel: (surface, panel) neighbours
+  int neighhop = 0;                  // neighbor_action: 0 stay, 1 hop
+  SurfaceDef() {
+    for (int i = 0; i < kMaxSpecies; ++i)
+      for (int m = 0; m < kSrfStates; ++m)
+        for (int f = 0; f < 3; ++f) act[i][m][f] = -1;
+  }
+};
+
+// A molecule bound to a panel, waiting to be uploaded (absolute position).
+struct PendBound {
+  double pos[3] = {0, 0, 0};
+  int species = 0, state = 1, surface = 0, panel = 0;
+  uint64_t serno = 0;
 };
 
 struct Command {
@@ -107,6 +148,10 @@ struct Sim {
   std::vector<double> pend_pos;
   std::vector<int> pend_sp;
   std::vector<uint64_t> pend_serno;   // serial numbers of the first pend_serno.size() pending molecules
+  std::vector<PendBound> pend_bound;  // surface-bound molecules waiting to be uploaded
+  // surface simulation parameters (surfacessalloc, smolsurface.c:1235-1237)
+  double srf_epsilon = 100 * 2.220446049250313e-16, srf_margin = 100 * 2.220446049250313e-16,
+         srf_neighdist = 10 * 2.220446049250313e-16;
   std::map<std::string, MsdState> msd; // meansqrdisp trackers by command text
   uint64_t host_rng = 0x853C49E6748FEA9Bull;
   // runtime commands and output data tables
@@ -153,6 +198,35 @@ int make_panel(int dim, int shape, const std::string &axis, const double *prm, i
 int derive_reaction_params(Sim &sim, std::string *err);
 // rxncalcrate (smolreact.c:1592-1680): effective rate from derived parameters.
 double calc_rate(const Sim &sim, int order, int r, double *pgem);
+// surfupdateparams (smolsurface.c:3735-3800): derived probabilities of every
+// rate-based surface interaction.
+int derive_surface_params(Sim &sim, std::string *err);
+// Whether any surface action can make or hold surface-bound molecules.
+bool surface_bound_mode(const Sim &sim);
+// Index (surface, panel) of a panel named `name` ("panel" in surface s, or
+// "surface:panel"); -1 when not found.
+int find_panel(const Sim &sim, int s, const std::string &name, int *srf_out);
+// addsurfmol (smolmolec.c:2744): n molecules of species sp in state ms
+// (1 front, 2 back) on the panels matching surface srf, shape and panel pnl
+// (-1: any), chosen by area and placed uniformly on the panel, or all at pos
+// when given (one panel must match).
+int add_surface_molecules(Sim &sim, long long n, int sp, int ms, int srf, int shape, int pnl, const double *pos,
+                          std::string *err);
+// The surface_mol statement (smolsim.cpp:1027-1070).
+int read_surface_mol(Sim &sim, const std::vector<std::string> &w, std::string *err);
+// Surface statements for surface-bound states (action with states, rate,
+// rate_internal, neighbors, neighbor_action) of surface sidx; returns 1 when
+// `word` is not one of them.
+int read_surface_rule_statement(Sim &sim, int sidx, const std::string &word, const std::vector<std::string> &w,
+                                std::string *err);
+// Name of a new panel (the given one, else shape name + index in shape).
+std::string new_panel_name(const SurfaceDef &sf, int shape, const std::string &given);
+// The action of (surface s, species i, state ms 0..2, face 0..2) and, for a
+// rate-based one, its derived probabilities (6 destination states each).
+int surface_rule_info(Sim &sim, int s, int i, int ms, int face, int *act, double *prob, double *cum, double *rev,
+                      std::string *err);
+// Surface rule table, bound diffusion and panel neighbours for the engine.
+int build_surface_rules(const Sim &sim, NetSpec *net, std::string *err);
 // Build engine inputs for a single-replicate simulation.
 int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err);
 // Text configuration reader (statement subset of smolsim.cpp:626 simreadstring).
