@@ -288,6 +288,35 @@ int advance_steps(Sim &s, long long n, std::string *err) {
   return 0;
 }
 
+// Molecules of species idx (-1: all) in a state (MSall / MSsome: any state),
+// solution molecules from the species counts less the bound ones; -1 on error.
+long long species_state_count(Sim &s, int idx, int state, std::string *err) {
+  long long n = 0, nb[3] = {0, 0, 0};  // all states, then bound molecules by state
+  if (s.eng && s.started && !s.need_rebuild) {
+    std::vector<long long> c;
+    if (s.eng->species_counts(&c, err)) return -1;
+    for (size_t i = 1; i < s.species.size(); ++i)
+      if (idx < 0 || (int)i == idx) n += c[i];
+    if (state != MSall && state != MSsome) {
+      std::vector<double> bpos;
+      std::vector<int> bsp, bst, bpn;
+      std::vector<uint64_t> bsn;
+      if (s.eng->get_bound(&bpos, &bsp, &bst, &bpn, &bsn, err)) return -1;
+      for (size_t k = 0; k < bsp.size(); ++k)
+        if ((idx < 0 || bsp[k] == idx) && bst[k] >= 1 && bst[k] <= 2) nb[bst[k]]++;
+    }
+  } else {
+    for (int sp : s.pend_sp)
+      if (idx < 0 || sp == idx) n++;
+    for (const smolb::PendBound &b : s.pend_bound)
+      if (idx < 0 || b.species == idx) { n++; nb[b.state]++; }
+  }
+  if (state == MSsoln) n -= nb[1] + nb[2];
+  else if (state == MSfront) n = nb[1];
+  else if (state == MSback) n = nb[2];
+  return n;
+}
+
 // molcountincmpt compartment data (smolcmd.c:1054-1100): (time, count of
 // each species in the compartment)
 void record_molcountincmpt(Sim &s, const smolb::Command &c) {
@@ -304,7 +333,67 @@ void record_molcountincmpt(Sim &s, const smolb::Command &c) {
   s.outdata[nw >= 3 ? data : "molcountincmpt"].push_back(row);
 }
 
-// runtime commands (smolcmd.c docommand subset: molcount, molcountincmpt, meansqrdisp)
+// molcountonsurf surface data (smolcmd.c:1236-1285): (time, count of each
+// species bound to the surface's panels)
+void record_molcountonsurf(Sim &s, const smolb::Command &c) {
+  char name[256] = {0}, sn[256] = {0}, data[256] = {0};
+  const int nw = sscanf(c.text.c_str(), "%255s %255s %255s", name, sn, data);
+  if (nw < 2 || !s.eng) return;
+  int si = -1;
+  for (size_t k = 0; k < s.surfaces.size(); ++k)
+    if (s.surfaces[k].name == sn) si = (int)k;
+  if (si < 0) return;
+  int first = 0;
+  for (int k = 0; k < si; ++k) first += (int)s.surfaces[k].panels.size();
+  const int last = first + (int)s.surfaces[si].panels.size();
+  std::vector<double> bpos;
+  std::vector<int> bsp, bst, bpn;
+  std::vector<uint64_t> bsn;
+  std::string err;
+  if (s.eng->get_bound(&bpos, &bsp, &bst, &bpn, &bsn, &err)) return;
+  std::vector<double> row(s.species.size(), 0.0);
+  row[0] = s.time;
+  for (size_t k = 0; k < bsp.size(); ++k)
+    if (bpn[k] >= first && bpn[k] < last && bsp[k] > 0 && bsp[k] < (int)row.size()) row[bsp[k]] += 1;
+  s.outdata[nw >= 3 ? data : "molcountonsurf"].push_back(row);
+}
+
+// molcountspecies species[(state)] data (smolcmd.c:1972-1992): (time, count
+// of the species in that state; all states for "all")
+void record_molcountspecies(Sim &s, const smolb::Command &c) {
+  char name[256] = {0}, spn[256] = {0}, data[256] = {0};
+  const int nw = sscanf(c.text.c_str(), "%255s %255s %255s", name, spn, data);
+  if (nw < 2 || !s.eng) return;
+  std::string nm = spn, st = "solution";
+  const size_t paren = nm.find('(');
+  if (paren != std::string::npos) {
+    st = nm.substr(paren + 1, nm.find(')', paren) - paren - 1);
+    nm = nm.substr(0, paren);
+  }
+  int ms = MSsoln;
+  if (st == "front") ms = MSfront;
+  else if (st == "back") ms = MSback;
+  else if (st == "all") ms = MSall;
+  else if (!(st == "solution" || st == "soln" || st == "fsoln" || st == "aq")) return;
+  const int idx = nm == "all" ? -1 : s.species_index(nm);
+  if (idx == 0 || (idx < 0 && nm != "all")) return;
+  std::string err;
+  const long long n = species_state_count(s, idx, ms, &err);
+  s.outdata[nw >= 3 ? data : "molcountspecies"].push_back({s.time, (double)std::max(0ll, n)});
+}
+
+void run_command(Sim &s, const smolb::Command &c) {
+  char name[256] = {0}, arg[256] = {0};
+  if (sscanf(c.text.c_str(), "%255s %255s", name, arg) < 1) return;
+  if (!strcmp(name, "molcount")) record_molcount(s, arg[0] ? arg : "molcount");
+  else if (!strcmp(name, "meansqrdisp")) record_meansqrdisp(s, c);
+  else if (!strcmp(name, "molcountincmpt")) record_molcountincmpt(s, c);
+  else if (!strcmp(name, "molcountonsurf")) record_molcountonsurf(s, c);
+  else if (!strcmp(name, "molcountspecies")) record_molcountspecies(s, c);
+}
+
+// runtime commands (smolcmd.c docommand subset: molcount, molcountincmpt,
+// molcountonsurf, meansqrdisp)
 void do_commands(Sim &s, bool at_start) {
   for (smolb::Command &c : s.cmds) {
     bool run = false;
@@ -319,22 +408,14 @@ void do_commands(Sim &s, bool at_start) {
       }
     }
     if (!run) continue;
-    char name[256] = {0}, arg[256] = {0};
-    if (sscanf(c.text.c_str(), "%255s %255s", name, arg) < 1) continue;
-    if (!strcmp(name, "molcount")) record_molcount(s, arg[0] ? arg : "molcount");
-    else if (!strcmp(name, "meansqrdisp")) record_meansqrdisp(s, c);
-    else if (!strcmp(name, "molcountincmpt")) record_molcountincmpt(s, c);
+    run_command(s, c);
   }
 }
 
 void do_end_commands(Sim &s) {
   for (smolb::Command &c : s.cmds) {
     if (c.type != 'a' && c.type != 'e') continue;
-    char name[256] = {0}, arg[256] = {0};
-    if (sscanf(c.text.c_str(), "%255s %255s", name, arg) < 1) continue;
-    if (!strcmp(name, "molcount")) record_molcount(s, arg[0] ? arg : "molcount");
-    else if (!strcmp(name, "meansqrdisp")) record_meansqrdisp(s, c);
-    else if (!strcmp(name, "molcountincmpt")) record_molcountincmpt(s, c);
+    run_command(s, c);
   }
 }
 
@@ -501,8 +582,7 @@ enum ErrorCode smolSetTimeStep(simptr sim, double t) {
 }
 enum ErrorCode smolSetRandomSeed(simptr sim, long int seed) {
   LCHECK(sim, ECmissing, "missing sim");
-  sim->s.seed = seed;
-  sim->s.host_rng = (uint64_t)seed * 0x9E3779B97F4A7C15ull + 0x2545F4914F6CDD1Dull;
+  sim->s.set_seed(seed);
   sim->s.need_rebuild = true;
   return ECok;
 }
@@ -765,30 +845,9 @@ int smolGetMoleculeCount(simptr sim, const char *species, enum MolecState state)
     idx = s.species_index(species);
     if (idx < 0) return (int)set_error(__func__, ECnonexist, "species not found");
   }
-  long long n = 0, nb[3] = {0, 0, 0};  // all states, then bound molecules by state
-  if (s.eng && s.started && !s.need_rebuild) {
-    std::vector<long long> c;
-    std::string err;
-    if (s.eng->species_counts(&c, &err)) return (int)set_error(__func__, ECerror, err);
-    for (size_t i = 1; i < s.species.size(); ++i)
-      if (idx < 0 || (int)i == idx) n += c[i];
-    if (state != MSall && state != MSsome) {
-      std::vector<double> bpos;
-      std::vector<int> bsp, bst, bpn;
-      std::vector<uint64_t> bsn;
-      if (s.eng->get_bound(&bpos, &bsp, &bst, &bpn, &bsn, &err)) return (int)set_error(__func__, ECerror, err);
-      for (size_t k = 0; k < bsp.size(); ++k)
-        if ((idx < 0 || bsp[k] == idx) && bst[k] >= 1 && bst[k] <= 2) nb[bst[k]]++;
-    }
-  } else {
-    for (int sp : s.pend_sp)
-      if (idx < 0 || sp == idx) n++;
-    for (const smolb::PendBound &b : s.pend_bound)
-      if (idx < 0 || b.species == idx) { n++; nb[b.state]++; }
-  }
-  if (state == MSsoln) n -= nb[1] + nb[2];
-  else if (state == MSfront) n = nb[1];
-  else if (state == MSback) n = nb[2];
+  std::string err;
+  const long long n = species_state_count(s, idx, (int)state, &err);
+  if (n < 0) return (int)set_error(__func__, ECerror, err);
   return (int)n;
 }
 

@@ -497,6 +497,11 @@ __device__ int srf_action(const KParams &p, int srf, int sp, int ms, int face, u
   ms2 = k;
   sp2 = r.newspec[k];
   const bool to_soln = k == kMSsoln || k == kMSbsoln;
+  if (k != kMSsoln && k != kMSfront && k != kMSback && k != kMSbsoln) {  // up / down: never built
+    ms2 = ms;
+    sp2 = sp;
+    return face == kFaceNone ? kSAno : kSAtrans;
+  }
   if (sp2 == 0) return kSAabsorb;
   if (ms != kMSsoln && face == kFaceNone) {
     if (k == ms) return kSAno;

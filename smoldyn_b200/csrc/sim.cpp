@@ -55,6 +55,17 @@ int Sim::reaction_index(const std::string &name, int *order) const {
   return -1;
 }
 
+// The placement stream starts at a hash of the seed: a start proportional to
+// the seed would make seed k+1's stream seed k's shifted by one number, so
+// neighbouring seeds would place molecules almost identically.
+void Sim::set_seed(long long s) {
+  seed = s;
+  uint64_t z = (uint64_t)s + 0x2545F4914F6CDD1Dull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  host_rng = z ^ (z >> 31);
+}
+
 double Sim::rand_u01() {
   // SplitMix64 stream for host-side placement of initial molecules
   uint64_t z = (host_rng += 0x9E3779B97F4A7C15ull);
@@ -788,8 +799,7 @@ int read_config_statement(Sim &sim, const std::string &word, const std::string &
     sim.time = atof(w[0].c_str());
   } else if (word == "random_seed") {
     if (!need(1)) return -7;
-    sim.seed = atoll(w[0].c_str());
-    sim.host_rng = (uint64_t)sim.seed * 0x9E3779B97F4A7C15ull + 0x2545F4914F6CDD1Dull;
+    sim.set_seed(atoll(w[0].c_str()));
     sim.need_rebuild = true;
   } else if (word == "molperbox") {
     if (!need(1)) return -7;
@@ -948,7 +958,9 @@ int read_config_statement(Sim &sim, const std::string &word, const std::string &
   } else if (word == "start_surface" || word == "new_surface") {
     SurfaceDef s;
     s.name = w.empty() ? "surf" + std::to_string(sim.surfaces.size()) : w[0];
-    sim.surfaces.push_back(s);
+    bool exists = false;  // a known name continues that surface (surfaddsurface)
+    for (const SurfaceDef &x : sim.surfaces) exists = exists || x.name == s.name;
+    if (!exists) sim.surfaces.push_back(s);
     sim.need_rebuild = true;
   } else if (word == "output_files") {
     for (const std::string &s : w) sim.outfiles.push_back(s);
@@ -1241,8 +1253,13 @@ int load_config_file(Sim &sim, const std::string &path, const std::string &name,
       std::istringstream(rest) >> nm;
       SurfaceDef s;
       s.name = nm.empty() ? "surf" + std::to_string(sim.surfaces.size()) : nm;
-      sim.surfaces.push_back(s);
-      cur_srf = &sim.surfaces.back();
+      cur_srf = nullptr;  // a known name continues that surface (surfaddsurface)
+      for (SurfaceDef &x : sim.surfaces)
+        if (x.name == s.name) cur_srf = &x;
+      if (!cur_srf) {
+        sim.surfaces.push_back(s);
+        cur_srf = &sim.surfaces.back();
+      }
       sim.need_rebuild = true;
       continue;
     }

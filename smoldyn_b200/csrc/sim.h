@@ -173,6 +173,7 @@ struct Sim {
   int compartment_index(const std::string &name) const;
   int reaction_index(const std::string &name, int *order) const;
   double rand_u01();
+  void set_seed(long long s);  // random_seed: engine key and host placement stream
 };
 
 // molsetdifm (smolmolec.c:833-867): set the diffusion matrix of a species;
