@@ -416,12 +416,53 @@ end_file
 """
 
 
+# surface-bound states: adsorption onto / desorption from a sphere with bound
+# diffusion, plus a bimolecular reaction (the bound-state form of the step
+# kernels and k_bound)
+TOUR_BOUND_CONFIG = """dim 3
+species A B C
+difc A 1
+difc B 1
+difc C 0.5
+difc A(front) 0.5
+boundaries 0 0 60
+boundaries 1 0 60
+boundaries 2 0 60
+time_start 0
+time_stop 100
+time_step 0.01
+random_seed 4
+start_surface walls
+action both all reflect
+panel rect +0 0 0 0 60 60
+panel rect -0 60 0 0 60 60
+panel rect +1 0 0 0 60 60
+panel rect -1 0 60 0 60 60
+panel rect +2 0 0 0 60 60
+panel rect -2 0 0 60 60 60
+end_surface
+start_surface cell
+action both all reflect
+rate A fsoln front 2
+rate A front fsoln 1
+panel sphere 30 30 30 12 20 20 s1
+end_surface
+reaction fwd A + B -> C 0.5
+reaction rev C -> A + B 0.1
+mol 20000 A u u u
+mol 20000 B u u u
+surface_mol 20000 A(front) cell sph all
+end_file
+"""
+
+
 def kernel_tour(args):
     """One small case of every kernel of the library, for profiler captures
     (ncu -k selects the kernel): the step pipeline on the scale-up workload
     at 4e6 molecules (its density), the device upload path, meansqrdisp and
     molcountincmpt with a transmitting sphere compartment (surface form of the
-    step kernels), the FP64 radius solvers, the surrogate's sampling,
+    step kernels), adsorption, desorption and bound diffusion on a sphere
+    (k_bound and the bound-state form), the FP64 radius solvers, the surrogate's sampling,
     training, inference and radius kernels, the persistent ensemble kernel
     and its layout changes, and the radial-distribution solver."""
     import ctypes as C
@@ -447,6 +488,13 @@ def kernel_tour(args):
         t = sb.Sim(ptr=simp.value)
         t.run_until(0.1)
         t.close()
+        with open(os.path.join(d, "b.txt"), "w") as f:
+            f.write(TOUR_BOUND_CONFIG)
+        b = sb.Sim.load_file(os.path.join(d, "b.txt"))
+        b.update()
+        b.run_steps(10)
+        b.synchronize()
+        b.close()
     finally:
         shutil.rmtree(d, ignore_errors=True)
     rng = np.random.default_rng(1)

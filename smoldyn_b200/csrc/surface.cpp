@@ -173,7 +173,7 @@ namespace {
 
 // srfcalcprob (smolsurface.c:3070-3146): probability of (ms1, face) -> ms2
 // for species i of surface s from the requested rates.  *err is set (and
-// -3 returned) for the reversible transmission case, which is not built.
+// -3 returned) when a transmission probability cannot be computed.
 double calc_prob(const Sim &sim, const SurfaceDef &sf, int i, int ms1, int face, int ms2, std::string *err) {
   if (ms1 == MSsoln && face == PFnone) return 0;
   if (eff_act(sf, i, ms1, face) != SAmult) return -1;
