@@ -143,7 +143,8 @@ enum ErrorCode smolAddPanel(simptr sim, const char *surface, enum PanelShape pan
  * adsorption, desorption, flips between faces and one-way transmission
  * (isinternal: the value is a probability per event); molecules bound to a
  * panel diffuse on it (rect, tri, sph, disk panels) and continue onto
- * neighbouring panels.  The up and down states, surface drift, and
+ * neighbouring panels; first-order reactions of bound molecules with at
+ * most one product.  The up and down states, surface drift and bimolecular
  * reactions of bound molecules are not supported. */
 enum ErrorCode smolSetSurfaceRate(simptr sim, const char *surface, const char *species, enum MolecState state,
                                   enum MolecState state1, enum MolecState state2, double rate,

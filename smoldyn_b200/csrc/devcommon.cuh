@@ -132,6 +132,12 @@ struct DevNet {
   double beps, bmargin, bneighdist; // surfacessstruct epsilon, margin, neighdist for bound molecules
   double bstep[kMaxSpecies][2];    // sqrt(2 D dt) of the front and back states
   double sstep[kMaxSpecies];       // sqrt(2 D dt) of the solution state, FP64 (desorption distance)
+  // first-order reactions of bound molecules by (species, front/back): the
+  // reactions in list order and their cumulative thresholds (fractions of 2^32)
+  uint8_t buni_n[kMaxSpecies][2];
+  uint8_t buni_list[kMaxSpecies][2][kMaxUniPerSpecies];
+  uint32_t bthr[kMaxSpecies][2][kMaxUniPerSpecies];
+  uint8_t pstate1[kMaxRxn];        // product state of each first-order reaction
 };
 
 // A molecule bound to a panel: absolute position (relative to the system's

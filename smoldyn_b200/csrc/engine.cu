@@ -465,6 +465,7 @@ constexpr uint32_t kCtrSrfWalk = 0x100u;   // + iteration: collision coins of a 
 constexpr uint32_t kCtrSrfWalk2 = 0x200u;  // + iteration: the same for the placement walk after desorption
 constexpr uint32_t kCtrSrfBound = 0x300u;  // desorption / flip coin and desorption distance
 constexpr uint32_t kCtrSrfDiff = 0x301u;   // diffusion of a bound molecule
+constexpr uint32_t kCtrSrfRxn = 0x302u;    // first-order reaction coin of a bound molecule
 constexpr uint32_t kCtrSrfBWalk = 0x400u;  // + iteration: collision coins of a bound molecule
 constexpr uint32_t kCtrSrfEdge = 0x1000u;  // + 64 * iteration (+ 1 + neighbour): panel-edge choices
 
@@ -705,6 +706,57 @@ __device__ int bound_coin(const KParams &p, BoundMol &m, int &sp, ull skey, uint
   return 0;
 }
 
+// First-order reactions of a bound molecule (unireact on the bound state,
+// smolreact.c:2997-3056, after the surface actions as in the reference's step
+// order), with the sequential-coin thresholds of its species and state.
+// The one product takes the reactant's place (doreact, smolreact.c:2806-2834):
+// a bound product is put on the reactant's panel on its state's side; a
+// solution product at the reactant's place just off the panel's front (soln)
+// or back (bsoln) side, into the output product list, so that, like the
+// reference's products, it first moves in the next step.  Returns 0 no
+// reaction, 1 reacted without product, 2 bound product (m, sp updated),
+// 3 solution product written (sp updated).
+__device__ int bound_first_order(const KParams &p, BoundMol &m, int &sp, ull skey, uint32_t step) {
+  const int st = m.ms - 1;
+  const int nr = c_net.buni_n[sp][st];
+  if (!nr) return 0;
+  const uint32_t u = srf_draw(skey, step, kCtrSrfRxn).x;
+  int r = -1;
+  for (int k = 0; k < nr; ++k)
+    if (u < c_net.bthr[sp][st][k]) { r = c_net.buni_list[sp][st][k]; break; }
+  if (r < 0) return 0;
+  atomicAdd(&p.counters[2], 1ull);
+  if (c_net.nprod[1][r] == 0) return 1;
+  const int psp = c_net.prd[1][r][0], pst = c_net.pstate1[r];
+  const DevPanel &pn = c_panels[m.pnl];
+  if (pst == kMSfront || pst == kMSback) {
+    sp = psp;
+    m.ms = pst;
+    fix_to_panel(pn, m.x, ms_face(pst), c_net.beps);
+    return 2;
+  }
+  double x[3] = {m.x[0], m.x[1], m.x[2]};
+  const int f = pst == kMSbsoln ? kFaceBack : kFaceFront;
+  double n[3];
+  face_normal(pn, x, f, n);
+  fix_to_panel(pn, x, f, c_net.beps);
+  const double sd = fabs(panel_sdist<true>(pn, x));
+  if (sd < c_net.surf_eps)  // kept surf_eps off the panel, as solution molecules are
+    for (int d = 0; d < 3; ++d) x[d] += (c_net.surf_eps - sd) * n[d];
+  int ix[3];
+  float w[3];
+  from_abs(c_geo0, x, ix, w);
+  sp = psp;
+  const int slot = atomicAdd(p.q_n, 1);
+  if (slot < p.pcap) {
+    p.q_pc[slot] = make_float4(w[0], w[1], w[2], __uint_as_float(pack_cell(ix[0], ix[1], ix[2])));
+    p.q_id[slot] = make_id(psp, 0, id_serno(m.id));
+  } else {
+    atomicOr(p.status, kStProdCap);
+  }
+  return 3;
+}
+
 // Crossings of other panels by a bound molecule's move from posx (on panel
 // pnlx) to m.x (checksurfaces on a surface-bound molecule, dosurfinteract
 // :4930-5020): a neighbouring panel is crossed (transmit) or, with
@@ -805,7 +857,8 @@ __device__ __forceinline__ void move_count(const KParams &p, int from, int to) {
 
 // The move pass's surface step for a solution molecule when surface rules are
 // in use.  Returns 1 when the molecule is removed, 3 when it was bound
-// (appended to the output bound list after its per-step coin), else 0 with
+// (appended to the output bound list after its per-step coin and first-order
+// reactions, or turned by one into a product in the product list), else 0 with
 // the molecule in solution at x1 (a molecule that adsorbs and desorbs again
 // within the step stays in solution at its desorbed place); species changes
 // update *id and the species counts.
@@ -824,6 +877,14 @@ __device__ __noinline__ int soln_surface_bound(const KParams &p, ull &id, const 
     double y0[3], y1[3];
     const int c = bound_coin(p, m, sp, skey, step, y0, y1);
     if (c == 1) return 1;
+    if (c == 0) {  // still bound: its first-order reactions this step
+      const int r = bound_first_order(p, m, sp, skey, step);
+      if (r == 1) return 1;
+      if (r == 3) {  // a solution product, in the output product list
+        move_count(p, sp0, sp);
+        return 3;
+      }
+    }
     bool bound = true;
     if (c == 2) {
       int pnl2 = 0, ms2 = 0;
@@ -1231,6 +1292,11 @@ __global__ void __launch_bounds__(256) k_bound(KParams p) {
     if (!dead) {
       double x0[3], x1[3];
       const int c = bound_coin(p, m, sp, skey, step, x0, x1);
+      if (c == 0) {  // still bound: its first-order reactions
+        const int r = bound_first_order(p, m, sp, skey, step);
+        if (r == 1) dead = true;
+        else if (r == 3) bound = false;
+      }
       if (c == 1) {
         dead = true;
       } else if (c == 2) {
@@ -3599,6 +3665,16 @@ class EngineImpl {
           const double t = std::min(4294967295.0, std::floor(cum * 4294967296.0));
           unithr[((size_t)rp * nsp + sp) * kMaxUniPerSpecies + m] = (uint32_t)t;
         }
+        if (rp == 0)  // the same thresholds for the bound states' reactions (single simulations)
+          for (int st = 0; st < 2; ++st) {
+            double bsurv = 1.0, bcum = 0.0;
+            for (int m = 0; m < dnet.buni_n[sp][st]; ++m) {
+              const double pr = std::min(1.0, std::max(0.0, s.uni_prob[dnet.buni_list[sp][st][m]]));
+              bcum += pr * bsurv;
+              bsurv *= (1.0 - pr);
+              dnet.bthr[sp][st][m] = (uint32_t)std::min(4294967295.0, std::floor(bcum * 4294967296.0));
+            }
+          }
       }
       for (int r = 0; r < net.nrxn[2]; ++r) {
         bind2[(size_t)rp * nr2 + r] = (float)s.bind2[r];
@@ -4038,10 +4114,18 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
   D.surf_eps = 0;
   for (int r = 0; r < net.nrxn[1]; ++r) {
     const int sp = net.rct[1][r][0];
+    D.rct[1][r][0] = (uint8_t)sp;
+    D.pstate1[r] = (uint8_t)net.pstate1[r];
+    const int st = net.rstate1[r];
+    if (st == 1 || st == 2) {  // a surface-bound reactant: the bound list's own table
+      uint8_t &nb = D.buni_n[sp][st - 1];
+      if (nb >= kMaxUniPerSpecies) { if (err) *err = "too many first-order reactions for one species"; return -6; }
+      D.buni_list[sp][st - 1][nb++] = (uint8_t)r;
+      continue;
+    }
     if (D.uni_n[sp] >= kMaxUniPerSpecies) { if (err) *err = "too many first-order reactions for one species"; return -6; }
     D.uni_list[sp][D.uni_n[sp]++] = (uint8_t)r;
     D.uni_any |= 1u << sp;
-    D.rct[1][r][0] = (uint8_t)sp;
   }
   for (int r = 0; r < net.nrxn[2]; ++r) {
     const int a = net.rct[2][r][0], b = net.rct[2][r][1];

@@ -92,6 +92,10 @@ struct NetSpec {
   std::vector<PanelSpec> panels;
   std::vector<CmptSpec> cmpts;
   int cmpt[3][kMaxRxn] = {};                 // compartment of each reaction + 1 (0: none)
+  // first-order reactions of surface-bound reactants: reactant state (0 soln,
+  // 1 front, 2 back) and product state (0 soln, 1 front, 2 back, 5 bsoln)
+  int rstate1[kMaxRxn] = {};
+  int pstate1[kMaxRxn] = {};
   // surface-bound states (single simulations only): rules by
   // ((surface * kMaxSpecies + species) * 3 + state) * 3 + face, state 0..2 =
   // soln, front, back and face 0..2 = front, back, none

@@ -133,15 +133,16 @@ int derive_reaction_params(Sim &sim, std::string *err) {
     else if (x.rate < 0) { if (err) *err = "reaction " + x.name + " rate is undefined"; return -8; }
     else if (x.rate == 0) x.prob = 0;
     else {
-      const int i = x.rct[0];
+      // the reactions of the same reactant species and state compete
+      const int i = x.rct[0], st = x.rstate[0];
       double sum = 0;
       for (const RxnDef &y : sim.rxn[1])
-        if (y.rct[0] == i && y.rate > 0) sum += y.rate;
+        if (y.rct[0] == i && y.rstate[0] == st && y.rate > 0) sum += y.rate;
       x.prob = x.rate / sum * (1.0 - std::exp(-sum * dt));
       double product = 1.0;
       for (size_t k = 0; k < r; ++k) {
         const RxnDef &y = sim.rxn[1][k];
-        if (y.rct[0] != i) continue;
+        if (y.rct[0] != i || y.rstate[0] != st) continue;
         const double pr = y.prob * product;
         product *= 1.0 - pr;
       }
@@ -152,7 +153,7 @@ int derive_reaction_params(Sim &sim, std::string *err) {
       }
     }
     int o2, r2;
-    const int rev = find_reverse(sim, 1, (int)r, &o2, &r2);
+    const int rev = x.rstate[0] == 0 ? find_reverse(sim, 1, (int)r, &o2, &r2) : 0;
     if (rev > 0 && o2 == 2 && x.rparamt == RP_none) {
       x.rparamt = RP_pgemmaxw;
       x.rparam = 0.2;
@@ -561,6 +562,10 @@ int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err) {
       net->nprod[o][r] = x.nprod;
       for (int q = 0; q < x.nprod; ++q) net->prd[o][r][q] = x.prd[q];
       net->fixed_placement[o][r] = (x.rparamt == RP_fixed) ? 1 : 0;
+      if (o == 1) {
+        net->rstate1[r] = x.rstate[0];
+        net->pstate1[r] = x.nprod ? x.pstate[0] : 0;
+      }
       if (o == 2) {
         net->placement2[r] = x.rparamt == RP_confspread ? 1 : x.rparamt == RP_bounce ? 2 : 0;
         net->bounce_k[r] = x.rparam >= 0 ? 1.0 : 2.0;
@@ -671,7 +676,8 @@ static int add_reaction_from_words(Sim &sim, const std::vector<std::string> &w, 
   size_t end = w.size();
   while (end > arrow + 1) {
     double v;
-    if (!parse_double(w[end - 1], &v) || sim.species_index(w[end - 1]) >= 0) break;
+    if (!parse_double(w[end - 1], &v) || sim.species_index(w[end - 1]) >= 0 || w[end - 1].find('(') != std::string::npos)
+      break;
     if (end - 1 == arrow + 1 && w[end - 1] == "0") break;  // "-> 0" with no rate
     rates.insert(rates.begin(), v);
     --end;
@@ -681,21 +687,56 @@ static int add_reaction_from_words(Sim &sim, const std::vector<std::string> &w, 
   if (rct.size() == 1 && rct[0] == "0") rct.clear();
   if (prd.size() == 1 && prd[0] == "0") prd.clear();
   if (rct.size() > 2 || prd.size() > (size_t)kMaxProd) { if (err) *err = "reaction: too many reactants or products"; return -7; }
+  // species[(state)]: solution unless a state is given (molstring2index1)
+  auto split = [&](const std::string &w, int *st) -> int {
+    std::string nm = w, sn;
+    *st = 0;
+    const size_t paren = w.find('(');
+    if (paren != std::string::npos) {
+      nm = w.substr(0, paren);
+      sn = w.substr(paren + 1, w.find(')', paren) - paren - 1);
+      if (sn == "front") *st = 1;
+      else if (sn == "back") *st = 2;
+      else if (sn == "bsoln") *st = 5;
+      else if (!(sn == "soln" || sn == "solution" || sn == "fsoln" || sn == "aq")) *st = -1;
+    }
+    return sim.species_index(nm);
+  };
   auto mk = [&](const std::string &nm, const std::vector<std::string> &r, const std::vector<std::string> &p,
                 double rate) -> int {
     RxnDef x;
     x.name = nm;
     x.order = (int)r.size();
     for (size_t q = 0; q < r.size(); ++q) {
-      const int i = sim.species_index(r[q]);
+      int st = 0;
+      const int i = split(r[q], &st);
       if (i < 0) { if (err) *err = "unknown species " + r[q]; return -3; }
+      if (st < 0 || st == 5) { if (err) *err = "reactant state not supported by the GPU engine: " + r[q]; return -7; }
       x.rct[q] = i;
+      x.rstate[q] = st;
     }
     x.nprod = (int)p.size();
     for (size_t q = 0; q < p.size(); ++q) {
-      const int i = sim.species_index(p[q]);
+      int st = 0;
+      const int i = split(p[q], &st);
       if (i < 0) { if (err) *err = "unknown species " + p[q]; return -3; }
+      if (st < 0) { if (err) *err = "product state not supported by the GPU engine: " + p[q]; return -7; }
       x.prd[q] = i;
+      x.pstate[q] = st;
+    }
+    // surface states in reactions: first-order reactions of a bound reactant
+    // with at most one product (mol_rxn states of smolreact.c:2662-2902)
+    bool bound = false;
+    for (int q = 0; q < x.order; ++q) bound = bound || x.rstate[q] != 0;
+    bool bprod = false;
+    for (int q = 0; q < x.nprod; ++q) bprod = bprod || x.pstate[q] != 0;
+    if (bound && (x.order != 1 || x.nprod > 1)) {
+      if (err) *err = "reactions of surface-bound molecules are supported as first order with at most one product";
+      return -7;
+    }
+    if (!bound && bprod) {
+      if (err) *err = "products in surface states need a surface-bound reactant";
+      return -7;
     }
     x.rate = rate;
     if ((int)sim.rxn[x.order].size() >= kMaxRxn) { if (err) *err = "too many reactions"; return -6; }

@@ -26,8 +26,10 @@ struct RxnDef {
   std::string name;
   int order = 0;
   int rct[2] = {0, 0};
+  int rstate[2] = {0, 0};   // reactant states (MolecState: 0 soln, 1 front, 2 back)
   int nprod = 0;
   int prd[kMaxProd] = {0, 0, 0, 0};
+  int pstate[kMaxProd] = {0, 0, 0, 0};  // product states (0 soln, 1 front, 2 back, 5 bsoln)
   double rate = -1;         // requested rate constant; <0 undefined
   int cmpt = -1;            // compartment the reaction is restricted to (rxn->cmpt), -1 none
   int rparamt = 0;          // RevParam

@@ -15,7 +15,9 @@ changes the species, so `molcount` separates the two sides.
      surface, with neighbour lists: bound diffusion carries them across the
      edges onto the other faces (counts per face);
   4. flips between the front and back states of a plane;
-  5. one-way transmission through a membrane at a given rate.
+  5. one-way transmission through a membrane at a given rate;
+  6. first-order reactions of bound molecules: A(front) -> B(front),
+     B(front) -> C(soln) (released into solution), A(front) -> 0.
 Engine-side geometric checks: bound molecules stay on their panel's surface
 (sphere radius; cube faces) to 1e-6.
 """
@@ -117,6 +119,25 @@ surface_mol 2000 B(front) plane rect p1
 output_files out.txt outb.txt
 cmd N 10 molcount out.txt
 cmd N 10 molcountspecies B(back) outb.txt
+end_file
+"""
+
+BOUNDRXN = HEAD + """species A B C
+difc A(front) 0.5
+difc B(front) 0.5
+difc C 1
+""" + WALLS + """start_surface plane
+action both all reflect
+panel rect +0 10 0 0 20 20 p1
+end_surface
+reaction r1 A(front) -> B(front) 1
+reaction r2 B(front) -> C(soln) 0.5
+reaction r3 A(front) -> 0 0.2
+surface_mol 2000 A(front) plane rect p1
+output_files out.txt outa.txt outb.txt
+cmd N 10 molcount out.txt
+cmd N 10 molcountspecies A(front) outa.txt
+cmd N 10 molcountspecies B(front) outb.txt
 end_file
 """
 
@@ -243,3 +264,15 @@ def test_one_way_transmission_rate():
     _, gpu = compare(text, ["out.txt"], [1, 2], "transmit")
     B = np.stack([g[0][:, 2] for g in gpu])
     assert B[:, -1].mean() > 50
+
+
+def test_first_order_reactions_of_bound_molecules():
+    text = fill(BOUNDRXN, L=20, T=2.0, dt=0.01)
+    _, gpu = compare(text, ["out.txt", "outa.txt", "outb.txt"], [1], "boundrxn")
+    A = np.stack([g[1] for g in gpu])
+    t, a = A[0, :, 0], A[:, :, 1].mean(0)
+    # A(front) leaves by two first-order reactions, 1 + 0.2 per unit time
+    assert np.all(np.abs(a - 2000 * np.exp(-1.2 * t)) < 40), (a, 2000 * np.exp(-1.2 * t))
+    C = np.stack([g[0][:, 3] for g in gpu]).mean(0)
+    assert C[-1] > 300  # B(front) -> C(soln) released molecules into solution
+
