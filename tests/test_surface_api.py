@@ -1,0 +1,113 @@
+"""Surface-bound states through the libsmoldyn C entry points (no GPU).
+
+The same configuration is built twice: from a text configuration, and by the
+C API calls a libsmoldyn client would make (smolAddSurface, smolAddPanel with
+panel names, smolSetSurfaceAction, smolSetSurfaceRate, smolAddPanelNeighbor,
+smolSetSpeciesMobility for the front state, smolAddSurfaceMolecules); the
+derived surface rules (smolgpuGetSurfaceRule) must be identical, and the
+surface-bound molecules (smolgpuGetSurfaceMolecules) must sit on their panel
+on the requested side.  Error paths: an unknown panel, a state the engine
+does not build, reactions with surface states other than first order.
+"""
+import ctypes as C
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import smoldyn_b200 as sb
+
+TEXT = """dim 3
+species A B
+difc A 1
+difc A(front) 0.3
+time_step 0.01
+boundaries 0 0 10
+boundaries 1 0 10
+boundaries 2 0 10
+random_seed 7
+start_surface membrane
+action both all reflect
+rate A fsoln front 1.5
+rate A front fsoln 2
+rate A front back 0.5 B
+panel rect +0 5 0 0 10 10 m1
+panel rect +0 5 0 10 10 10 m2
+neighbors m1 m2
+end_surface
+surface_mol 100 A(front) membrane rect m1
+end_file
+"""
+
+
+def from_text():
+    d = tempfile.mkdtemp()
+    with open(os.path.join(d, "c.txt"), "w") as f:
+        f.write(TEXT)
+    return sb.Sim.load_file(os.path.join(d, "c.txt"))
+
+
+def from_api():
+    lib = sb.load()
+    s = sb.Sim(3, (0, 0, 0), (10, 10, 10))
+    s.add_species("A", 1.0)
+    s.add_species("B")
+    assert lib.smolSetSpeciesMobility(s.ptr, b"A", sb.MSfront, 0.3, None, None) == 0
+    s.set_times(0, 1, 0.01)
+    s.seed(7)
+    assert lib.smolAddSurface(s.ptr, b"membrane") == 0
+    assert lib.smolSetSurfaceAction(s.ptr, b"membrane", sb.PFboth, b"all", sb.MSsoln, sb.SAreflect, None) == 0
+    assert lib.smolSetSurfaceRate(s.ptr, b"membrane", b"A", sb.MSsoln, sb.MSsoln, sb.MSfront, 1.5, None, 0) == 0
+    assert lib.smolSetSurfaceRate(s.ptr, b"membrane", b"A", sb.MSfront, sb.MSfront, sb.MSsoln, 2.0, None, 0) == 0
+    assert lib.smolSetSurfaceRate(s.ptr, b"membrane", b"A", sb.MSfront, sb.MSfront, sb.MSback, 0.5, b"B", 0) == 0
+    for name, y in ((b"m1", 0.0), (b"m2", 10.0)):
+        prm = np.array([5.0, 0.0, y, 10.0, 10.0])
+        assert lib.smolAddPanel(s.ptr, b"membrane", sb.PSrect, name, b"+0", sb.dptr(prm)) == 0
+    assert lib.smolAddPanelNeighbor(s.ptr, b"membrane", b"m1", b"membrane", b"m2", 0) == 0
+    assert lib.smolAddSurfaceMolecules(s.ptr, b"A", sb.MSfront, 100, b"membrane", sb.PSrect, b"m1", None) == 0
+    return s
+
+
+@pytest.mark.parametrize("make", [from_text, from_api])
+def test_bound_molecules_on_their_panel(make):
+    s = make()
+    pos, sp, st, srf, pnl, sn = s.surface_molecules()
+    assert len(pos) == 100 and np.all(sp == 1) and np.all(st == sb.MSfront) and np.all(pnl == 0)
+    assert np.all(pos[:, 0] > 5.0) and np.all(pos[:, 0] - 5.0 < 1e-12)  # just on the front (+x) side
+    assert np.all((pos[:, 1] >= 0) & (pos[:, 1] <= 10) & (pos[:, 2] >= 0) & (pos[:, 2] <= 10))
+    assert s.count("A", sb.MSfront) == 100 and s.count("A", sb.MSsoln) == 0
+    s.close()
+
+
+def test_api_and_text_derive_the_same_rules():
+    a, b = from_text(), from_api()
+    for sp in ("A", "B"):
+        for ms in (sb.MSsoln, sb.MSfront, sb.MSback):
+            for face in (sb.PFfront, sb.PFback, sb.PFnone):
+                ra, rb = a.surface_rule("membrane", sp, ms, face), b.surface_rule("membrane", sp, ms, face)
+                assert ra[0] == rb[0], (sp, ms, face, ra[0], rb[0])
+                for x, y in zip(ra[1:], rb[1:]):
+                    assert np.array_equal(x, y), (sp, ms, face, x, y)
+    # adsorption from the front, desorption and the flip are rate-based (SAmult = 5)
+    assert a.surface_rule("membrane", "A", sb.MSsoln, sb.PFfront)[0] == 5
+    act, pr, cu, rv = a.surface_rule("membrane", "A", sb.MSfront, sb.PFnone)
+    assert act == 5 and pr[sb.MSsoln] > 0 and pr[sb.MSback] > 0 and abs(cu[-1] - 1.0) < 1e-12
+    a.close()
+    b.close()
+
+
+def test_errors():
+    lib = sb.load()
+    s = from_api()
+    assert lib.smolAddPanelNeighbor(s.ptr, b"membrane", b"m1", b"membrane", b"nope", 0) != 0
+    assert lib.smolAddSurfaceMolecules(s.ptr, b"A", sb.MSup, 5, b"membrane", sb.PSrect, b"m1", None) != 0
+    assert lib.smolSetSurfaceRate(s.ptr, b"membrane", b"A", sb.MSup, sb.MSup, sb.MSsoln, 1.0, None, 0) != 0
+    s.close()
+    for stmt in ("reaction r A(front) + B -> A(front) 1", "reaction r A(front) -> B(front) + B(front) 1",
+                 "reaction r A -> B(front) 1"):
+        d = tempfile.mkdtemp()
+        with open(os.path.join(d, "c.txt"), "w") as f:
+            f.write(TEXT.replace("end_file", stmt + "\nend_file"))
+        with pytest.raises(RuntimeError):
+            sb.Sim.load_file(os.path.join(d, "c.txt"))
