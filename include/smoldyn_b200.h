@@ -142,7 +142,7 @@ enum ErrorCode smolAddPanel(simptr sim, const char *surface, enum PanelShape pan
  * Single simulations only.  States soln, front, back and bsoln; rates of
  * adsorption, desorption, flips between faces and one-way transmission
  * (isinternal: the value is a probability per event); molecules bound to a
- * panel diffuse on it (rect, tri, sph, disk panels) and continue onto
+ * panel diffuse on it (any panel shape) and continue onto
  * neighbouring panels; first-order reactions of bound molecules with at
  * most one product.  The up and down states, surface drift and bimolecular
  * reactions of bound molecules are not supported. */

@@ -10,7 +10,9 @@
 // Shapes use the engine's panel form (DevPanel).  Rectangle edges are coded
 // 1 / 2 for the low / high side along the first in-plane axis and 3 / 4
 // along the second; triangle edges 1, 2, 3 run v0->v1, v1->v2, v2->v0; a
-// disk has the single edge 1 (its rim).  Edge code 0 means "inside".
+// disk and a hemisphere have the single edge 1 (the rim), a cylinder the
+// edges 1 and 2 (the rims at its first and second axis end).  Edge code 0
+// means "inside".
 // Coordinates are relative to the system's low corner, FP64 throughout.
 #pragma once
 
@@ -175,6 +177,33 @@ SMOLB_HDI int closest_panel_pt(const DevPanel &pn, const double x[3], double out
       for (int d = 0; d < 3; ++d) out[d] = pn.center[d] + f * w[d];
       return edge;
     }
+    case 3: {  // cylinder: the nearest point of its side, an end rim within margin (Geo_NearestCylinderPt)
+      double w[3];
+      for (int d = 0; d < 3; ++d) w[d] = x[d] - pn.pt[0][d];
+      double s = dot3(w, pn.nrm) / pn.axlen;  // axial fraction
+      const double m = margin / pn.axlen;
+      if (s <= m) { s = 0; edge = 1; }
+      else if (s >= 1 - m) { s = 1; edge = 2; }
+      double rad[3];
+      cyl_radial(pn, x, rad);
+      const double l = sqrt(dot3(rad, rad));
+      for (int d = 0; d < 3; ++d) out[d] = pn.pt[0][d] + s * pn.axlen * pn.nrm[d] + (l > 0 ? pn.radius / l : 0.0) * rad[d];
+      return edge;
+    }
+    case 4: {  // hemisphere: the sphere's nearest point, or the rim's (Geo_NearestRingPt)
+      double w[3];
+      for (int d = 0; d < 3; ++d) w[d] = x[d] - pn.center[d];
+      const double s = dot3(w, pn.nrm);
+      if (s < -margin) {
+        const double l = sqrt(dot3(w, w));
+        for (int d = 0; d < 3; ++d) out[d] = pn.center[d] + (l > 0 ? pn.radius / l : 0.0) * w[d];
+        return 0;
+      }
+      for (int d = 0; d < 3; ++d) w[d] -= s * pn.nrm[d];
+      const double l = sqrt(dot3(w, w));
+      for (int d = 0; d < 3; ++d) out[d] = pn.center[d] + (l > 0 ? pn.radius / l : 0.0) * w[d];
+      return 1;
+    }
     default:
       for (int d = 0; d < 3; ++d) out[d] = x[d];
       return 0;
@@ -225,6 +254,13 @@ SMOLB_HDI void move_into_panel(const DevPanel &pn, double x[3], double margin) {
     const double s = dot3(w, pn.nrm);
     if (s > 0)
       for (int d = 0; d < 3; ++d) x[d] -= s * pn.nrm[d] + margin;
+  } else if (pn.shape == 3) {  // between the end planes, margin inside (Geo_NearestSlabPt)
+    double w[3];
+    for (int d = 0; d < 3; ++d) w[d] = x[d] - pn.pt[0][d];
+    const double s = dot3(w, pn.nrm);
+    const double lo = margin, hi = pn.axlen - margin;
+    const double t = s < lo ? lo : s > hi ? hi : s;
+    for (int d = 0; d < 3; ++d) x[d] += (t - s) * pn.nrm[d];
   }
 }
 
@@ -265,7 +301,38 @@ SMOLB_HDI int line_exit_panel(const DevPanel &pn, const double a[3], const doubl
     if (tk[2] < tk[k]) k = 2;
     t = tk[k];
     *edge = k + 1;
-  } else {  // disk (rim as a sphere of the disk's radius), and the curved shapes' rims likewise
+  } else if (pn.shape == 3) {
+    // cylinder: through the end the path heads for, where it meets that end's
+    // plane, taken to the rim (Geo_LineExitCylinder)
+    const double v[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+    const double dv = dot3(v, pn.nrm);
+    const int end = dv > 0 ? 2 : 1;
+    double c[3];
+    for (int d = 0; d < 3; ++d) c[d] = pn.pt[end - 1][d];
+    const double w[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+    t = dv != 0 ? dot3(w, pn.nrm) / dv : 0.0;
+    double q[3];
+    for (int d = 0; d < 3; ++d) q[d] = a[d] + t * v[d];
+    double rad[3];  // out to that end's rim
+    cyl_radial(pn, q, rad);
+    const double l = sqrt(dot3(rad, rad));
+    for (int d = 0; d < 3; ++d) out[d] = c[d] + (l > 0 ? pn.radius / l : 0.0) * rad[d];
+    *edge = end;
+    return 0;
+  } else if (pn.shape == 4) {
+    // hemisphere: where the path meets the rim's plane, out to the rim
+    // (Geo_LineExitHemisphere)
+    const double v[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+    const double w[3] = {pn.center[0] - a[0], pn.center[1] - a[1], pn.center[2] - a[2]};
+    const double dv = dot3(v, pn.nrm);
+    t = dv != 0 ? dot3(w, pn.nrm) / dv : 0.0;
+    double q[3];
+    for (int d = 0; d < 3; ++d) q[d] = a[d] + t * v[d] - pn.center[d];
+    const double l = sqrt(dot3(q, q));
+    for (int d = 0; d < 3; ++d) out[d] = pn.center[d] + (l > 0 ? pn.radius / l : 0.0) * q[d];
+    *edge = 1;
+    return 0;
+  } else {  // disk (rim as a sphere of the disk's radius)
     double v[3], w[3];
     for (int d = 0; d < 3; ++d) { v[d] = b[d] - a[d]; w[d] = pn.center[d] - a[d]; }
     const double qa = dot3(v, v), qb = -2.0 * dot3(w, v), qc = dot3(w, w) - pn.radius * pn.radius;
@@ -287,6 +354,10 @@ SMOLB_HDI void panel_edge_normal(const DevPanel &pn, const double e[3], int edge
     n[u[(edge - 1) / 2]] = (edge % 2) ? -1.0 : 1.0;
   } else if (pn.shape == 1) {
     tri_edge_out(pn, (edge - 1) % 3, n);
+  } else if (pn.shape == 3) {  // cylinder ends: along the axis, outward
+    for (int d = 0; d < 3; ++d) n[d] = (edge == 2 ? 1.0 : -1.0) * pn.nrm[d];
+  } else if (pn.shape == 4) {  // hemisphere rim: out of the open side
+    for (int d = 0; d < 3; ++d) n[d] = pn.nrm[d];
   } else {
     for (int d = 0; d < 3; ++d) n[d] = e[d] - pn.center[d];
     if (pn.shape == 5) {

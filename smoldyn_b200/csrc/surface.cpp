@@ -646,10 +646,8 @@ int build_surface_rules(const Sim &sim, NetSpec *net, std::string *err) {
   const int ns = (int)sim.species.size(), nsrf = (int)sim.surfaces.size();
   net->nsrf = nsrf;
   net->srf_rules.assign((size_t)std::max(1, nsrf) * kMaxSpecies * 9, SrfRule{});
-  bool cyl_hemi_bound = false;
   for (int s = 0; s < nsrf; ++s) {
     const SurfaceDef &sf = sim.surfaces[s];
-    bool holds = false;
     for (int i = 0; i < ns && i < kMaxSpecies; ++i)
       for (int ms = 0; ms < kSrfStates; ++ms)
         for (int f = 0; f < 3; ++f) {
@@ -663,23 +661,11 @@ int build_surface_rules(const Sim &sim, NetSpec *net, std::string *err) {
             r.cum[k] = d ? d->cum[k] : 0.0;
             if (d && d->rev[k] > 0) r.rev |= (uint8_t)(1u << k);
           }
-          if (r.act == SAmult && d && (d->prob[MSfront] > 0 || d->prob[MSback] > 0)) holds = true;
-          if (ms != MSsoln && sf.act[i][ms][f] >= 0) holds = true;
         }
-    for (const PendBound &b : sim.pend_bound) holds = holds || b.surface == s;
-    if (holds)
-      for (const PanelSpec &p : sf.panels) cyl_hemi_bound = cyl_hemi_bound || p.shape == 3 || p.shape == 4;
   }
-  bool mobile = false;
   for (int i = 0; i < ns && i < kMaxSpecies; ++i)
-    for (int k = 0; k < 2; ++k) {
-      net->difc_bound[i][k] = sim.species[i].difc_bound[k];
-      mobile = mobile || sim.species[i].difc_bound[k] > 0;
-    }
-  if (mobile && cyl_hemi_bound) {
-    if (err) *err = "surface-bound diffusion on cylinder and hemisphere panels is not supported by the GPU engine";
-    return -6;
-  }
+    for (int k = 0; k < 2; ++k) net->difc_bound[i][k] = sim.species[i].difc_bound[k];
+
   net->srf_eps = sim.srf_epsilon;
   net->srf_margin = sim.srf_margin;
   net->srf_neighdist = sim.srf_neighdist;

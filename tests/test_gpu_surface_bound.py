@@ -17,7 +17,9 @@ changes the species, so `molcount` separates the two sides.
   4. flips between the front and back states of a plane;
   5. one-way transmission through a membrane at a given rate;
   6. first-order reactions of bound molecules: A(front) -> B(front),
-     B(front) -> C(soln) (released into solution), A(front) -> 0.
+     B(front) -> C(soln) (released into solution), A(front) -> 0;
+  7. a capsule: a cylinder with hemisphere caps, neighbours across the rims
+     (counts on the body and on the caps).
 Engine-side geometric checks: bound molecules stay on their panel's surface
 (sphere radius; cube faces) to 1e-6.
 """
@@ -119,6 +121,29 @@ surface_mol 2000 B(front) plane rect p1
 output_files out.txt outb.txt
 cmd N 10 molcount out.txt
 cmd N 10 molcountspecies B(back) outb.txt
+end_file
+"""
+
+CAPSULE = HEAD + """species B
+difc B(front) 1
+""" + WALLS + """start_surface body
+panel cyl 8 10 10 12 10 10 2 20 20 c1
+end_surface
+start_surface caps
+panel hemi 8 10 10 2 1 0 0 20 20 h1
+panel hemi 12 10 10 2 -1 0 0 20 20 h2
+end_surface
+start_surface body
+neighbors c1 caps:h1 caps:h2
+end_surface
+start_surface caps
+neighbors h1 body:c1
+neighbors h2 body:c1
+end_surface
+surface_mol 2000 B(front) body cyl c1
+output_files out_body.txt out_caps.txt
+cmd N 20 molcountonsurf body out_body.txt
+cmd N 20 molcountonsurf caps out_caps.txt
 end_file
 """
 
@@ -275,4 +300,19 @@ def test_first_order_reactions_of_bound_molecules():
     assert np.all(np.abs(a - 2000 * np.exp(-1.2 * t)) < 40), (a, 2000 * np.exp(-1.2 * t))
     C = np.stack([g[0][:, 3] for g in gpu]).mean(0)
     assert C[-1] > 300  # B(front) -> C(soln) released molecules into solution
+
+
+def test_capsule_cylinder_and_hemisphere_caps():
+    def on_capsule(s):
+        pos, sp, st, srf, pnl, sn = s.surface_molecules()
+        assert len(pos) == 2000
+        x = pos[:, 0]
+        c = np.where(x < 8, 8.0, np.where(x > 12, 12.0, x))  # nearest point of the axis segment
+        r = np.sqrt((x - c) ** 2 + (pos[:, 1] - 10) ** 2 + (pos[:, 2] - 10) ** 2)
+        assert np.all(np.abs(r - 2.0) < 1e-6), np.abs(r - 2.0).max()
+        assert set(srf.tolist()) == {1, 2}
+    text = fill(CAPSULE, L=20, T=2.0, dt=0.01)
+    _, gpu = compare(text, ["out_body.txt", "out_caps.txt"], [1], "capsule", check=on_capsule)
+    caps = np.stack([g[1][:, 1] for g in gpu]).mean(0)
+    assert caps[-1] > 500  # the caps (half the area) fill from the cylinder
 
