@@ -661,14 +661,19 @@ def run_surrogate(sb, torch, args, rank):
     sec = time_on_stream(torch, stream, work)
     tot = float(n.sum())
     engine = {1: "step pipeline", 2: "persistent"}.get(e.engine(), "?")
-    # solver cost of one redraw: surrogate vs exact device vs exact host
+    # cost of one redraw's update by radius mode: surrogate vs exact device vs
+    # exact host (median of 3 redraws each, after the engine is idle)
     solver = {}
     for mode, name in ((2, "surrogate"), (1, "exact_device"), (0, "exact_host")):
         e.radius_mode(mode)
-        redraw()
-        t1 = time.perf_counter()
-        e.update()
-        solver[name + "_s"] = time.perf_counter() - t1
+        ts = []
+        for _ in range(3):
+            redraw()
+            e.synchronize()
+            t1 = time.perf_counter()
+            e.update()
+            ts.append(time.perf_counter() - t1)
+        solver[name + "_s"] = float(np.median(ts))
     out = {"workload": "65536 replicates, N log-uniform [1e2,1e4] at density 0.01, A+B<->C with unbinding ratio "
                        "%.1f, kf,kr log-uniform [1e-3,1] redrawn every 100 steps, dt=0.01, radii from the MLP "
                        "surrogate with exact fallback" % rho,
