@@ -138,6 +138,13 @@ struct DevNet {
   uint8_t buni_list[kMaxSpecies][2][kMaxUniPerSpecies];
   uint32_t bthr[kMaxSpecies][2][kMaxUniPerSpecies];
   uint8_t pstate1[kMaxRxn];        // product state of each first-order reaction
+  // second-order reactions of a bound and a solution reactant, in list
+  // order: the reaction, the bound reactant's species and state (1 front,
+  // 2 back), the solution reactant's species and the product's state; per
+  // bound (species, front/back) the solution species it reacts with
+  int bpair_n;
+  uint8_t bpair_rxn[kMaxRxn], bpair_bsp[kMaxRxn], bpair_bst[kMaxRxn], bpair_ssp[kMaxRxn], bpair_pst[kMaxRxn];
+  uint32_t bpair_mask[kMaxSpecies][2];
 };
 
 // A molecule bound to a panel: absolute position (relative to the system's

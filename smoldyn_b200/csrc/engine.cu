@@ -95,6 +95,11 @@ struct KParams {
   BoundMol *bd_out;
   int *bd_out_n;
   int bcap;
+  // bound-solution pair reactions: per sorted molecule the best claim of a
+  // bound molecule (all ones when unclaimed), per bound molecule its
+  // candidate (partner, reaction, squared distance bits, state)
+  ull *bclaim;
+  int4 *bcand;
 };
 
 constexpr uint32_t kTmpGone = 0xFFFFFFFFu;  // tmp[i].w of a molecule that left
@@ -1273,6 +1278,7 @@ __global__ void __launch_bounds__(256) k_bound(KParams p) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     BoundMol m = p.bd_in[i];
     const int sp0 = id_species(m.id);
+    if (sp0 == kDeadSpecies) continue;  // reacted with a solution molecule
     int sp = sp0;
     const ull skey = id_stream(m.id);
     const double posx[3] = {m.x[0], m.x[1], m.x[2]};
@@ -1344,7 +1350,215 @@ __global__ void __launch_bounds__(256) k_bound(KParams p) {
 // Species counts of an uploaded bound list (added to the solution counts).
 __global__ void k_bound_species_count(const BoundMol *m, const int *n, long long *spcount) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < *n; i += gridDim.x * blockDim.x)
-    atomicAdd((unsigned long long *)&spcount[id_species(m[i].id)], 1ull);
+    if (id_species(m[i].id) != kDeadSpecies) atomicAdd((unsigned long long *)&spcount[id_species(m[i].id)], 1ull);
+}
+
+// ---- bound-solution pair reactions -------------------------------------------
+// Second-order reactions of a surface-bound and a solution reactant (bireact
+// smolreact.c:3201-3300, morebireact :3109-3157), after the solution pairs of
+// the step as in the reference's list order.  A pair reacts when the solution
+// molecule lies within the binding radius of the bound one, on the front side
+// of the bound one's panel (a solution reactant's state is read from the
+// side of that panel, :3134-3137), inside the reaction's compartment if it
+// has one, and the reaction's coin passes; of a pair's reactions the first in
+// list order that passes is taken.  The reference takes pairs in the order of
+// its molecule lists, which has nothing to do with geometry; here every pair
+// gets a random priority (a hash of both identities and the step) and the
+// pairs react as if taken in priority order: each bound molecule claims its
+// partner of lowest priority value (an atomic minimum of priority and
+// bound-list index on the partner's claim word), the claim holding the
+// minimum reacts, and bound molecules whose partner went to another claim
+// again, for kBPairRounds rounds in all.
+constexpr uint32_t kCtrBPair = 0x500u;  // + list entry: coin of a bound-solution pair
+constexpr int kBPairRounds = 4;
+constexpr uint32_t kCtrBProd = 0x5A5A5A5Au;  // stream offset of a product's placement
+
+// absolute position of sorted molecule j, as the displacement-nearest image
+// of x0 in periodic dimensions
+__device__ __forceinline__ void bpair_partner_pos(const KParams &p, int j, const double x0[3], double xs[3]) {
+  const DevGeo &g = c_geo0;
+  const float4 q = p.b_pc[j];
+  int jx[3];
+  unpack_cell(__float_as_uint(q.w), jx[0], jx[1], jx[2]);
+  const float u[3] = {q.x, q.y, q.z};
+  to_abs(g, jx, u, xs);
+  for (int d = 0; d < g.dim; ++d)
+    if (g.wall[2 * d] == kWallPeriodic) {
+      const double L = (double)(g.n[d] - 1) * g.h[d] + g.whi[d];
+      const double v = xs[d] - x0[d];
+      if (v > 0.5 * L) xs[d] -= L;
+      else if (v < -0.5 * L) xs[d] += L;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_bpair_claim(KParams p, int round) {
+  pdl_launch_dependents();
+  pdl_wait();
+  const int nb = min(*p.bd_out_n, p.bcap);
+  const int n = *p.b_n;
+  const uint32_t step = *p.step;
+  const DevGeo &g = c_geo0;
+  const uint2 key = make_uint2(c_net.key0 ^ 0x7F4A7C15u, c_net.key1 ^ 0x94D049BBu);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nb; k += gridDim.x * blockDim.x) {
+    int4 c = p.bcand[k];
+    if (round > 0 && !(c.x >= 0 && c.w == 0)) continue;  // later rounds: the molecules that lost their partner
+    c = make_int4(-1, 0, 0, 0);
+    const BoundMol m = p.bd_out[k];
+    const int sp = id_species(m.id);
+    const uint32_t mask = sp == kDeadSpecies ? 0u : c_net.bpair_mask[sp][m.ms - 1];
+    if (mask) {
+      const DevPanel &pn = c_panels[m.pnl];
+      const ull kb = id_stream(m.id);
+      int ix[3];
+      float u[3];
+      from_abs(g, m.x, ix, u);
+      uint32_t bestp = 0xFFFFFFFFu;
+      for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+          for (int dx = -1; dx <= 1; ++dx) {
+            const int off[3] = {dx, dy, dz};
+            int cc[3];
+            bool ok = true;
+            for (int d = 0; d < 3; ++d) {
+              if (d >= g.dim && off[d] != 0) ok = false;
+              cc[d] = ix[d] + off[d];
+              if (cc[d] < 0 || cc[d] >= g.n[d]) {
+                if (g.wall[2 * d] != kWallPeriodic || g.n[d] < 3) ok = false;
+                cc[d] = cc[d] < 0 ? cc[d] + g.n[d] : cc[d] - g.n[d];
+              }
+            }
+            if (!ok) continue;
+            const int cell = g.cell0 + (cc[2] * g.n[1] + cc[1]) * g.n[0] + cc[0];
+            const int e0 = min(p.start[cell + 1], n);
+            for (int j = p.start[cell]; j < e0; ++j) {
+              const ull idj = p.b_id[j];
+              const int sj = id_species(idj);
+              if (sj == kDeadSpecies || !((mask >> sj) & 1u)) continue;
+              double xs[3];
+              bpair_partner_pos(p, j, m.x, xs);
+              const double d2 = (xs[0] - m.x[0]) * (xs[0] - m.x[0]) + (xs[1] - m.x[1]) * (xs[1] - m.x[1]) +
+                                (xs[2] - m.x[2]) * (xs[2] - m.x[2]);
+              const ull pk = mix64((kb * 0x9E3779B97F4A7C15ull ^ id_stream(idj)) + (ull)step * 0xD1B54A32D192ED03ull);
+              const uint32_t prio = (uint32_t)(pk >> 32);
+              if (c.x >= 0 && prio >= bestp) continue;
+              int side = -1;  // the panel side, read once a reaction is in range
+              for (int e = 0; e < c_net.bpair_n; ++e) {
+                if (c_net.bpair_bsp[e] != sp || c_net.bpair_bst[e] != m.ms || c_net.bpair_ssp[e] != sj) continue;
+                const int r = c_net.bpair_rxn[e];
+                if (d2 > (double)p.bind2[r]) continue;
+                const float prob = p.pairprob[r];
+                if (prob < 1.f) {
+                  const ull kk = mix64(kb * 0x9E3779B97F4A7C15ull ^ id_stream(idj));
+                  const uint4 rr = philox(make_uint4((uint32_t)kk, (uint32_t)(kk >> 32), step, kCtrBPair + (uint32_t)e), key);
+                  if (!(u01co(rr.x) < (double)prob)) continue;
+                }
+                if (side < 0) side = panel_side(pn, xs, nullptr) == kFaceBack ? 0 : 1;
+                if (!side) break;  // behind the panel: the solution state is bsoln, which no reaction takes
+                const int cm = c_net.cmpt[2][r];
+                if (cm && !(pos_in_cmpt(c_cmpt, cm - 1, c_panels, xs) && pos_in_cmpt(c_cmpt, cm - 1, c_panels, m.x)))
+                  continue;
+                bestp = prio;
+                c = make_int4(j, e, (int)prio, 0);
+                break;
+              }
+            }
+          }
+    }
+    p.bcand[k] = c;
+    if (c.x >= 0) atomicMin(&p.bclaim[c.x], ((ull)(uint32_t)c.z << 32) | (ull)(uint32_t)k);
+  }
+}
+
+// The claims holding their partner's minimum react (doreact smolreact.c:2662-
+// 2902 for one product): both reactants are removed and the product is placed
+// at the diffusion-weighted reaction position, on the bound reactant's panel
+// when the position projects inside it, else on the nearest panel of its
+// surface; a bound product is brought onto that panel on its state's side
+// (fixpt2panel, movemol2closepanel) and takes the bound reactant's entry, a
+// solution product is put just off the front (soln) or back (bsoln) side into
+// the output product list, so that both first move in the next step.
+__global__ void __launch_bounds__(256) k_bpair_resolve(KParams p) {
+  pdl_launch_dependents();
+  pdl_wait();
+  const int nb = min(*p.bd_out_n, p.bcap);
+  const uint32_t step = *p.step;
+  int done = 0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nb; k += gridDim.x * blockDim.x) {
+    const int4 c = p.bcand[k];
+    if (c.x < 0 || c.w != 0) continue;
+    const int j = c.x;
+    if (p.bclaim[j] != (((ull)(uint32_t)c.z << 32) | (ull)(uint32_t)k)) continue;  // another claim comes first
+    p.bclaim[j] = ~0ull;  // the winner clears the word; losers compare against their own key only
+    p.bcand[k].w = 1;
+    done++;
+    BoundMol m = p.bd_out[k];
+    const int spb = id_species(m.id);
+    const ull ids = p.b_id[j];
+    const int sps = id_species(ids);
+    p.b_id[j] = id_mark_dead(ids);
+    atomicAdd((unsigned long long *)&p.spcount[sps], (unsigned long long)(-1ll));
+    atomicAdd((unsigned long long *)&p.spcount[spb], (unsigned long long)(-1ll));
+    const int e = c.y, r = c_net.bpair_rxn[e];
+    if (c_net.nprod[2][r] == 0) {
+      p.bd_out[k].id = id_mark_dead(m.id);
+      continue;
+    }
+    const int psp = c_net.prd[2][r][0], pst = c_net.bpair_pst[e];
+    double xs[3];
+    bpair_partner_pos(p, j, m.x, xs);
+    const double sb = c_net.bstep[spb][m.ms - 1], ss = c_net.sstep[sps];
+    const double db = sb * sb, ds = ss * ss;  // proportional to the diffusion coefficients
+    const double f = (db == 0 && ds == 0) ? 0.5 : ds / (db + ds);  // weight of the bound reactant
+    double x[3];
+    for (int d = 0; d < 3; ++d) x[d] = f * m.x[d] + (1.0 - f) * xs[d];
+    int pnl = m.pnl;
+    if (!pt_in_panel(c_panels[pnl], x)) {  // closestsurfacept over the bound reactant's surface
+      const int srf = c_panels[m.pnl].srf;
+      double bestd = 1e300;
+      for (int q = 0; q < c_net.npanel; ++q) {
+        if (c_panels[q].srf != srf) continue;
+        double pt[3];
+        closest_panel_pt(c_panels[q], x, pt, 0.0);
+        const double dd = (pt[0] - x[0]) * (pt[0] - x[0]) + (pt[1] - x[1]) * (pt[1] - x[1]) + (pt[2] - x[2]) * (pt[2] - x[2]);
+        if (dd < bestd) { bestd = dd; pnl = q; }
+      }
+    }
+    const ull skey = mix64(id_stream(m.id) ^ kCtrBProd) & ((1ull << kSpShift) - 1);
+    atomicAdd((unsigned long long *)&p.spcount[psp], 1ull);
+    if (pst == kMSfront || pst == kMSback) {
+      fix_to_panel(c_panels[pnl], x, ms_face(pst), c_net.beps);
+      const double x0[3] = {x[0], x[1], x[2]};
+      move_to_close_panel(x, x0, pnl, pst, skey, step);
+      for (int d = 0; d < 3; ++d) m.x[d] = x[d];
+      m.pnl = pnl;
+      m.ms = pst;
+      m.id = make_id(psp, 0, id_serno(m.id));
+      p.bd_out[k] = m;
+      continue;
+    }
+    p.bd_out[k].id = id_mark_dead(m.id);
+    const int face = pst == kMSbsoln ? kFaceBack : kFaceFront;
+    fix_to_panel(c_panels[pnl], x, face, c_net.beps);
+    const double x0[3] = {x[0], x[1], x[2]};
+    move_to_close_panel(x, x0, pnl, face == kFaceBack ? kMSback : kMSfront, skey, step);
+    const DevPanel &pn = c_panels[pnl];
+    double nrm[3];
+    face_normal(pn, x, face, nrm);
+    const double sd = fabs(panel_sdist<true>(pn, x));
+    if (sd < c_net.surf_eps)  // kept surf_eps off the panel, as solution molecules are
+      for (int d = 0; d < 3; ++d) x[d] += (c_net.surf_eps - sd) * nrm[d];
+    int ix[3];
+    float w[3];
+    from_abs(c_geo0, x, ix, w);
+    const int slot = atomicAdd(p.q_n, 1);
+    if (slot < p.pcap) {
+      p.q_pc[slot] = make_float4(w[0], w[1], w[2], __uint_as_float(pack_cell(ix[0], ix[1], ix[2])));
+      p.q_id[slot] = make_id(psp, 0, id_serno(m.id));
+    } else {
+      atomicOr(p.status, kStProdCap);
+    }
+  }
+  if (done) atomicAdd(&p.counters[3], (unsigned long long)done);
 }
 
 // Scatter pass: a pure permutation of the moved molecules into box order.
@@ -3103,6 +3317,8 @@ class EngineImpl {
   // surface-bound molecules: lists by parity (as the sorted buffers), rules
   BoundMol *d_bd[2] = {nullptr, nullptr};
   long long bcap = 0;
+  ull *d_bclaim = nullptr;  // bound-solution pair reactions: claim word per sorted molecule
+  int4 *d_bcand = nullptr;  // and candidate per bound molecule
   SrfRule *d_srfrule = nullptr;
 
   // persistent ensemble engine (k_persist): its own molecule layout, one
@@ -3236,10 +3452,12 @@ class EngineImpl {
     void *ptrs[] = {d_boxmask, d_difm, d_rsearch, d_geo, d_difstep, d_driftdt, d_bind2, d_pairprob, d_prdpos, d_gtab, d_unithr,
                     d_births, d_pc[0], d_pc[1], d_ppc[0], d_ppc[1], d_id[0], d_id[1], d_pid[0],
                     d_pid[1], d_face, d_tmp, d_counts, d_step, d_cnt, d_start, d_scan_ticket, d_scan_status, d_ev, d_cand, d_best,
-                    d_counters, d_spcount, d_injkey, d_injval, d_bd[0], d_bd[1], d_srfrule};
+                    d_counters, d_spcount, d_injkey, d_injval, d_bd[0], d_bd[1], d_srfrule, d_bclaim, d_bcand};
     for (void *q : ptrs)
       if (q) cudaFree(q);
     d_bd[0] = d_bd[1] = nullptr;
+    d_bclaim = nullptr;
+    d_bcand = nullptr;
     d_srfrule = nullptr;
     bcap = 0;
     d_rsearch = nullptr;
@@ -3306,6 +3524,8 @@ class EngineImpl {
       p.bd_out = d_bd[out];
       p.bd_out_n = d_counts + 8 + out;
       p.bcap = (int)bcap;
+      p.bclaim = d_bclaim;
+      p.bcand = d_bcand;
     }
     return p;
   }
@@ -3587,6 +3807,14 @@ class EngineImpl {
       launch(k_commit<SURF>, grid_small(), 128, 0, p);
       mark("k_commit");
     }
+    if (SURF == 3 && dnet.bpair_n) {
+      for (int round = 0; round < kBPairRounds; ++round) {
+        launch(k_bpair_claim, grid_small(), 256, 0, p, round);
+        mark("k_bpair_claim");
+        launch(k_bpair_resolve, grid_small(), 256, 0, p);
+        mark("k_bpair_resolve");
+      }
+    }
     launch(k_products<SURF>, grid_small(), 128, 0, p);
     mark("k_products");
   }
@@ -3614,7 +3842,9 @@ class EngineImpl {
     }
   }
 
-  int launches_per_step() const { return 8 + 2 * (dnet.rounds - 1) + (dnet.bound ? 1 : 0); }
+  int launches_per_step() const {
+    return 8 + 2 * (dnet.rounds - 1) + (dnet.bound ? 1 : 0) + (dnet.bound && dnet.bpair_n ? 2 * kBPairRounds : 0);
+  }
 
   int upload_const(std::string *err) {
     CK(cudaMemcpyToSymbolAsync(c_net, &dnet, sizeof(DevNet), 0, cudaMemcpyHostToDevice, stream));
@@ -3679,6 +3909,7 @@ class EngineImpl {
       for (int r = 0; r < net.nrxn[2]; ++r) {
         bind2[(size_t)rp * nr2 + r] = (float)s.bind2[r];
         pairprob[(size_t)rp * nr2 + r] = (float)s.pair_prob[r];
+        if (net.rstate2[r][0] != 0 || net.rstate2[r][1] != 0) continue;  // searched from the bound list
         // stencil radius: largest binding radius of the species' pair reactions,
         // padded so FP32 rounding of a distance at the radius cannot fall outside
         const double hmin = std::min(geo[rp].h[0], std::min(geo[rp].h[1], geo[rp].h[2]));
@@ -4131,6 +4362,19 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
     const int a = net.rct[2][r][0], b = net.rct[2][r][1];
     D.rct[2][r][0] = (uint8_t)a;
     D.rct[2][r][1] = (uint8_t)b;
+    const int sa = net.rstate2[r][0], sb = net.rstate2[r][1];
+    if (sa != 0 || sb != 0) {  // one bound reactant: the bound list's pair pass
+      if (!net.bound) { if (err) *err = "reactions of surface-bound molecules need surface rules with bound states"; return -6; }
+      const int k = D.bpair_n++;
+      const bool first = sa != 0;
+      D.bpair_rxn[k] = (uint8_t)r;
+      D.bpair_bsp[k] = (uint8_t)(first ? a : b);
+      D.bpair_bst[k] = (uint8_t)(first ? sa : sb);
+      D.bpair_ssp[k] = (uint8_t)(first ? b : a);
+      D.bpair_pst[k] = (uint8_t)net.pstate2[r];
+      D.bpair_mask[D.bpair_bsp[k]][D.bpair_bst[k] - 1] |= 1u << D.bpair_ssp[k];
+      continue;
+    }
     for (int pass = 0; pass < (a == b ? 1 : 2); ++pass) {
       const int x = pass ? b : a, y = pass ? a : b;
       if (D.pair_n[x][y] >= kMaxPairRxn) { if (err) *err = "too many reactions for one reactant pair"; return -6; }
@@ -4284,6 +4528,12 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
     }
     E.bcap = E.cap;
     for (int k = 0; k < 2; ++k) CK(cudaMalloc(&E.d_bd[k], E.bcap * sizeof(BoundMol)));
+    if (D.bpair_n) {
+      CK(cudaMalloc(&E.d_bclaim, E.cap * sizeof(ull)));
+      CK(cudaMemsetAsync(E.d_bclaim, 0xFF, E.cap * sizeof(ull), E.stream));
+      CK(cudaMalloc(&E.d_bcand, E.bcap * sizeof(int4)));
+      CK(cudaMemsetAsync(E.d_bcand, 0xFF, E.bcap * sizeof(int4), E.stream));
+    }
     CK(cudaMalloc(&E.d_srfrule, nrule * sizeof(SrfRule)));
     CK(cudaMemcpyAsync(E.d_srfrule, net.srf_rules.data(), nrule * sizeof(SrfRule), cudaMemcpyHostToDevice, E.stream));
     CK(cudaStreamSynchronize(E.stream));
@@ -4610,6 +4860,7 @@ int Engine::get_bound(std::vector<double> *pos, std::vector<int> *species, std::
   if (nb) CK(cudaMemcpy(m.data(), E.d_bd[in], (size_t)nb * sizeof(BoundMol), cudaMemcpyDeviceToHost));
   std::sort(m.begin(), m.end(), [](const BoundMol &a, const BoundMol &b) { return id_serno(a.id) < id_serno(b.id); });
   for (const BoundMol &b : m) {
+    if (id_species(b.id) == kDeadSpecies) continue;
     for (int d = 0; d < 3; ++d) pos->push_back(b.x[d] + E.reps[0].lo[d]);
     species->push_back(id_species(b.id));
     state->push_back(b.ms);

@@ -96,6 +96,10 @@ struct NetSpec {
   // 1 front, 2 back) and product state (0 soln, 1 front, 2 back, 5 bsoln)
   int rstate1[kMaxRxn] = {};
   int pstate1[kMaxRxn] = {};
+  // second-order reactions with one surface-bound reactant: reactant states
+  // and the product's state
+  int rstate2[kMaxRxn][2] = {};
+  int pstate2[kMaxRxn] = {};
   // surface-bound states (single simulations only): rules by
   // ((surface * kMaxSpecies + species) * 3 + state) * 3 + face, state 0..2 =
   // soln, front, back and face 0..2 = front, back, none

@@ -93,6 +93,9 @@ static int find_reverse(const Sim &s, int order, int r, int *o2, int *r2) {
   int rev = 0;
   for (size_t k = 0; k < s.rxn[orr].size(); ++k) {
     const RxnDef &y = s.rxn[orr][k];
+    // the products here are in solution: a reaction of bound reactants is
+    // not permitted for them
+    if (y.rstate[0] != 0 || (orr == 2 && y.rstate[1] != 0)) continue;
     bool rct_match = (orr == 1) ? (y.rct[0] == x.prd[0]) : same_set2(y.rct[0], y.rct[1], x.prd[0], x.prd[1]);
     if (!rct_match) continue;
     if (rev != 1 && y.nprod == order) {
@@ -178,11 +181,16 @@ int derive_reaction_params(Sim &sim, std::string *err) {
       if (err) *err = "reaction rate " + x.name + " is undefined";
       return -8;
     }
+    // a bound reactant: the rate doubles (one surface, one solution reactant)
+    // and its state's diffusion coefficient counts (smolreact.c:1371-1374)
+    const int s1 = x.rstate[0], s2 = x.rstate[1];
     double rate3 = x.rate;
     if (i1 == i2) rate3 *= 2;
-    const double dsum = sim.species[i1].difc + sim.species[i2].difc;
-    int o2, r2;
-    const int rev = find_reverse(sim, 2, (int)r, &o2, &r2);
+    if ((s1 == 0) != (s2 == 0)) rate3 *= 2;
+    const double dsum = (s1 ? sim.species[i1].difc_bound[s1 - 1] : sim.species[i1].difc) +
+                        (s2 ? sim.species[i2].difc_bound[s2 - 1] : sim.species[i2].difc);
+    int o2 = 0, r2 = 0;
+    const int rev = (s1 == 0 && s2 == 0) ? find_reverse(sim, 2, (int)r, &o2, &r2) : 0;
     if (rev > 0 && o2 == 2 && x.rparamt == RP_none) {
       x.rparamt = RP_pgemmaxw;
       x.rparam = 0.2;
@@ -347,7 +355,7 @@ static void choose_grid(const Sim &s, long long nmol, int ncell[3]) {
 }
 
 // Effective rate constant implied by the derived parameters (rxncalcrate,
-// smolreact.c:1592-1680), for solution-phase reactions: order 0 from the
+// smolreact.c:1592-1680): order 0 from the
 // births per step, order 1 from the per-step probabilities of the species'
 // list (undoing the correction for earlier reactions), order 2 from the
 // tabulated per-step rate at the binding radius (with the reverse products'
@@ -382,10 +390,13 @@ double calc_rate(const Sim &sim, int order, int r, double *pgem) {
       ans = -std::log(1.0 - x.prob) / dt;
     } else {
       const int i1 = x.rct[0], i2 = x.rct[1];
-      const double step = std::sqrt(2.0 * (sim.species[i1].difc + sim.species[i2].difc) * dt);
+      const int s1 = x.rstate[0], s2 = x.rstate[1];
+      const double dsum = (s1 ? sim.species[i1].difc_bound[s1 - 1] : sim.species[i1].difc) +
+                          (s2 ? sim.species[i2].difc_bound[s2 - 1] : sim.species[i2].difc);
+      const double step = std::sqrt(2.0 * dsum * dt);
       const double a = std::sqrt(x.bindrad2);
       int o2 = 0, r2 = 0;
-      const int rev = find_reverse(sim, 2, r, &o2, &r2);
+      const int rev = (s1 == 0 && s2 == 0) ? find_reverse(sim, 2, r, &o2, &r2) : 0;
       const int rpt = rev == 1 ? sim.rxn[o2][r2].rparamt : RP_none;
       if (rpt == RP_pgem || rpt == RP_pgemmax || rpt == RP_pgemmaxw || rpt == RP_ratio || rpt == RP_unbindrad) {
         const RxnDef &rv = sim.rxn[o2][r2];
@@ -399,6 +410,7 @@ double calc_rate(const Sim &sim, int order, int r, double *pgem) {
         ans = rxnp::numrxnrateprob(step, a, -1, x.prob) / dt;
       }
       if (i1 == i2) ans /= 2.0;
+      if (s1 != 0 || s2 != 0) ans /= 2.0;  // one surface-bound reactant
     }
   }
   if (pgem) {
@@ -567,6 +579,19 @@ int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err) {
         net->pstate1[r] = x.nprod ? x.pstate[0] : 0;
       }
       if (o == 2) {
+        net->rstate2[r][0] = x.rstate[0];
+        net->rstate2[r][1] = x.rstate[1];
+        net->pstate2[r] = x.nprod ? x.pstate[0] : 0;
+        bool off = false;
+        for (int q = 0; q < x.nprod; ++q)
+          for (int d = 0; d < 3; ++d) off = off || x.prdpos[q][d] != 0;
+        if ((x.rstate[0] || x.rstate[1]) &&
+            (x.rparamt == RP_confspread || x.rparamt == RP_bounce || x.rparamt == RP_fixed || off)) {
+          if (err) *err = "reaction " + x.name + ": a surface-bound reactant takes the default product placement only";
+          return -7;
+        }
+      }
+      if (o == 2) {
         net->placement2[r] = x.rparamt == RP_confspread ? 1 : x.rparamt == RP_bounce ? 2 : 0;
         net->bounce_k[r] = x.rparam >= 0 ? 1.0 : 2.0;
       }
@@ -724,14 +749,17 @@ static int add_reaction_from_words(Sim &sim, const std::vector<std::string> &w, 
       x.prd[q] = i;
       x.pstate[q] = st;
     }
-    // surface states in reactions: first-order reactions of a bound reactant
-    // with at most one product (mol_rxn states of smolreact.c:2662-2902)
-    bool bound = false;
-    for (int q = 0; q < x.order; ++q) bound = bound || x.rstate[q] != 0;
+    // surface states in reactions: a first-order reaction of a bound reactant,
+    // or a second-order one of a bound and a solution reactant, with at most
+    // one product (reactant and product states of smolreact.c:2662-2902)
+    int nbound = 0;
+    for (int q = 0; q < x.order; ++q) nbound += x.rstate[q] != 0;
+    const bool bound = nbound > 0;
     bool bprod = false;
     for (int q = 0; q < x.nprod; ++q) bprod = bprod || x.pstate[q] != 0;
-    if (bound && (x.order != 1 || x.nprod > 1)) {
-      if (err) *err = "reactions of surface-bound molecules are supported as first order with at most one product";
+    if (bound && (x.order == 0 || nbound > 1 || x.nprod > 1)) {
+      if (err) *err = "reactions of surface-bound molecules are supported as first order, or second order with one "
+                      "solution reactant, with at most one product";
       return -7;
     }
     if (!bound && bprod) {
@@ -985,6 +1013,10 @@ int read_config_statement(Sim &sim, const std::string &word, const std::string &
     const int rp = rp_from_string(w[1]);
     if (rp < 0) { if (err) *err = "product_placement: unknown type " + w[1]; return -7; }
     RxnDef &x = sim.rxn[o][r];
+    if ((x.rstate[0] != 0 || (o == 2 && x.rstate[1] != 0)) && rp != RP_none && rp != RP_irrev) {
+      if (err) *err = "product_placement: a reaction of a surface-bound reactant takes the default placement only";
+      return -7;
+    }
     x.rparamt = rp;
     x.rparam = (w.size() > 2) ? atof(w[2].c_str()) : 0;
     if ((rp == RP_offset || rp == RP_fixed) && w.size() >= 3 + 1 + (size_t)sim.dim) {

@@ -19,7 +19,17 @@ changes the species, so `molcount` separates the two sides.
   6. first-order reactions of bound molecules: A(front) -> B(front),
      B(front) -> C(soln) (released into solution), A(front) -> 0;
   7. a capsule: a cylinder with hemisphere caps, neighbours across the rims
-     (counts on the body and on the caps).
+     (counts on the body and on the caps);
+  8. second-order reactions of a bound and a solution reactant, with a
+     bound product, a solution product and none; solution molecules behind
+     the panel do not react.  The bound molecules sit within one binding
+     radius of each other, so bound molecules contest solution molecules; the
+     reference settles a contest by its molecule-list order, and with one
+     list for all states it favours products of earlier steps (they fill the
+     list slots of reacted molecules, ahead of the solution molecules).  The
+     configuration keeps bound and solution molecules in separate lists, the
+     layout in which the reference's order carries no such preference (its
+     C(front) count then agrees with the engine's random-priority contests).
 Engine-side geometric checks: bound molecules stay on their panel's surface
 (sphere radius; cube faces) to 1e-6.
 """
@@ -163,6 +173,35 @@ output_files out.txt outa.txt outb.txt
 cmd N 10 molcount out.txt
 cmd N 10 molcountspecies A(front) outa.txt
 cmd N 10 molcountspecies B(front) outb.txt
+end_file
+"""
+
+BIRXN = HEAD + """species A B C D
+difc A(front) 0.2
+difc B 1
+difc C(front) 0.2
+difc D 1
+""" + WALLS + """start_surface plane
+action both all reflect
+panel rect +0 10 0 0 20 20 p1
+end_surface
+reaction r1 A(front) + B -> C(front) 4
+reaction r2 B + C(front) -> D 4
+reaction r3 A(front) + D -> 0 1
+start_compartment behind
+surface plane
+point 5 10 10
+end_compartment
+molecule_lists blist bndlist
+mol_list B blist
+mol_list D blist
+mol_list A(front) bndlist
+mol_list C(front) bndlist
+surface_mol 2000 A(front) plane rect p1
+mol 4000 B u u u
+output_files out.txt outb.txt
+cmd N 10 molcount out.txt
+cmd N 10 molcountincmpt behind outb.txt
 end_file
 """
 
@@ -316,3 +355,17 @@ def test_capsule_cylinder_and_hemisphere_caps():
     caps = np.stack([g[1][:, 1] for g in gpu]).mean(0)
     assert caps[-1] > 500  # the caps (half the area) fill from the cylinder
 
+
+
+def test_bound_solution_pair_reactions():
+    def on_plane(s):
+        pos, sp, st, srf, pnl, sn = s.surface_molecules()
+        assert len(pos) > 100
+        assert np.all(np.abs(pos[:, 0] - 10.0) < 1e-6) and np.all(pos[:, 0] > 10.0)  # the front side
+        assert set(sp.tolist()) <= {1, 3}  # A and C
+    text = fill(BIRXN, L=20, T=3.0, dt=0.01)
+    _, gpu = compare(text, ["out.txt", "outb.txt"], [1, 2, 3, 4], "birxn", check=on_plane)
+    G = np.stack([g[0] for g in gpu]).mean(0)
+    assert G[-1, 1] < 1800 and G[-1, 3] > 200 and G[:, 4].max() > 3  # A reacted; C formed; D released
+    Bk = np.stack([g[1] for g in gpu]).mean(0)
+    assert np.all(Bk[:, 2] > 1800)  # B behind the panel (x < 10) does not react

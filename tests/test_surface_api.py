@@ -6,8 +6,12 @@ panel names, smolSetSurfaceAction, smolSetSurfaceRate, smolAddPanelNeighbor,
 smolSetSpeciesMobility for the front state, smolAddSurfaceMolecules); the
 derived surface rules (smolgpuGetSurfaceRule) must be identical, and the
 surface-bound molecules (smolgpuGetSurfaceMolecules) must sit on their panel
-on the requested side.  Error paths: an unknown panel, a state the engine
-does not build, reactions with surface states other than first order.
+on the requested side.  Second-order reactions of a bound and a solution
+reactant: binding radii and effective rates against the values the
+reference binary prints for the same configurations (golden fixture).
+Error paths: an unknown panel, a state the engine does not build, reactions
+with two bound reactants, solution reactants with bound products, and
+bound-reactant reactions with a non-default product placement.
 """
 import ctypes as C
 import os
@@ -104,10 +108,34 @@ def test_errors():
     assert lib.smolAddSurfaceMolecules(s.ptr, b"A", sb.MSup, 5, b"membrane", sb.PSrect, b"m1", None) != 0
     assert lib.smolSetSurfaceRate(s.ptr, b"membrane", b"A", sb.MSup, sb.MSup, sb.MSsoln, 1.0, None, 0) != 0
     s.close()
-    for stmt in ("reaction r A(front) + B -> A(front) 1", "reaction r A(front) -> B(front) + B(front) 1",
-                 "reaction r A -> B(front) 1"):
+    for stmt in ("reaction r A(front) + A(back) -> A(front) 1", "reaction r A(front) -> B(front) + B(front) 1",
+                 "reaction r A -> B(front) 1", "reaction r A(front) + B -> A(front) 1\nproduct_placement r bounce -2",
+                 "reaction r A(front) + B -> A(front) + B 1"):
         d = tempfile.mkdtemp()
         with open(os.path.join(d, "c.txt"), "w") as f:
             f.write(TEXT.replace("end_file", stmt + "\nend_file"))
         with pytest.raises(RuntimeError):
             sb.Sim.load_file(os.path.join(d, "c.txt"))
+
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "bound_pair_params.npz")
+
+
+def test_bound_solution_reaction_parameters_match_reference():
+    """Binding radius and effective rate of A(front) + B style reactions: the
+    rate doubles for one surface and one solution reactant and the bound
+    state's diffusion coefficient counts (smolreact.c:1371-1377); the
+    reference prints both to six significant digits."""
+    z = np.load(GOLDEN)
+    d = tempfile.mkdtemp()
+    for text, names, rates, radii in zip(z["texts"], z["names"], z["rates"], z["radii"]):
+        path = os.path.join(d, "c.txt")
+        with open(path, "w") as f:
+            f.write(str(text))
+        s = sb.Sim.load_file(path)
+        for nm, rate, rad in zip(str(names).split(","), rates, radii):
+            b, _, _ = s.reaction_params(nm)
+            k, _ = s.effective_rate(nm)
+            assert abs(b - rad) <= 2e-5 * rad + 1e-9, (nm, b, rad, str(text))
+            assert abs(k - rate) <= 2e-5 * rate + 1e-9, (nm, k, rate, str(text))
+        s.close()
