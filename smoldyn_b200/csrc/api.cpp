@@ -1130,7 +1130,6 @@ enum ErrorCode smolSetReactionRegion(simptr sim, const char *reaction, const cha
 enum ErrorCode smolAddReaction(simptr sim, const char *reaction, const char *reactant1, enum MolecState rstate1,
                                const char *reactant2, enum MolecState rstate2, int nproduct,
                                const char **productspecies, enum MolecState *productstates, double rate) {
-  (void)rstate1; (void)rstate2; (void)productstates;
   LCHECK(sim && reaction, ECmissing, "missing sim or reaction name");
   Sim &s = sim->s;
   LCHECK(s.reaction_index(reaction, nullptr) < 0, ECsame, "reaction already exists");
@@ -1139,23 +1138,33 @@ enum ErrorCode smolAddReaction(simptr sim, const char *reaction, const char *rea
   x.name = reaction;
   int order = 0;
   const char *rr[2] = {reactant1, reactant2};
+  const enum MolecState rs[2] = {rstate1, rstate2};
   for (int k = 0; k < 2; ++k) {
     if (rr[k] && rr[k][0]) {
       const int i = s.species_index(rr[k]);
       LCHECK(i > 0, ECnonexist, "reactant species not found");
-      x.rct[order++] = i;
+      LCHECK(rs[k] >= MSsoln && rs[k] <= MSsome, ECbounds, "invalid reactant state");
+      x.rct[order] = i;
+      // MSall, MSnone and MSsome name the solution state here: surface-bound
+      // reactants are given by their state
+      x.rstate[order] = (rs[k] == MSall || rs[k] == MSnone || rs[k] == MSsome) ? MSsoln : (int)rs[k];
+      order++;
     }
   }
   x.order = order;
   x.nprod = nproduct;
+  LCHECK(nproduct == 0 || productspecies, ECmissing, "missing product species");
   for (int q = 0; q < nproduct; ++q) {
     const int i = s.species_index(productspecies[q]);
     LCHECK(i > 0, ECnonexist, "product species not found");
     x.prd[q] = i;
+    // product states default to solution when the caller gives none
+    x.pstate[q] = productstates ? (int)productstates[q] : MSsoln;
   }
   x.rate = rate;
-  LCHECK((int)s.rxn[order].size() < smolb::kMaxRxn, ECbounds, "too many reactions of this order (max 16)");
-  s.rxn[order].push_back(x);
+  std::string err;
+  if (smolb::add_reaction_def(s, x, &err))
+    return set_error(__func__, err.find("too many") != std::string::npos ? ECbounds : ECsyntax, err);
   s.need_update = s.need_rebuild = true;
   return ECok;
 }

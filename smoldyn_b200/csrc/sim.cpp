@@ -680,6 +680,38 @@ static int species_arg(Sim &sim, const std::string &w, std::vector<int> *out) {
   return 0;
 }
 
+// Append a reaction after checking its reactant and product states: solution
+// reactions, a first-order reaction of a bound reactant, or a second-order
+// one of a bound and a solution reactant, with at most one product (the
+// reactant and product states of doreact, smolreact.c:2662-2902, that the
+// engine builds).
+int add_reaction_def(Sim &sim, const RxnDef &x, std::string *err) {
+  int nbound = 0;
+  for (int q = 0; q < x.order; ++q) {
+    if (x.rstate[q] < 0 || x.rstate[q] > 2) { if (err) *err = "reactant state not supported by the GPU engine"; return -7; }
+    nbound += x.rstate[q] != 0;
+  }
+  const bool bound = nbound > 0;
+  bool bprod = false;
+  for (int q = 0; q < x.nprod; ++q) {
+    const int st = x.pstate[q];
+    if (st < 0 || (st > 2 && st != 5)) { if (err) *err = "product state not supported by the GPU engine"; return -7; }
+    bprod = bprod || st != 0;
+  }
+  if (bound && (x.order == 0 || nbound > 1 || x.nprod > 1)) {
+    if (err) *err = "reactions of surface-bound molecules are supported as first order, or second order with one "
+                    "solution reactant, with at most one product";
+    return -7;
+  }
+  if (!bound && bprod) {
+    if (err) *err = "products in surface states need a surface-bound reactant";
+    return -7;
+  }
+  if ((int)sim.rxn[x.order].size() >= kMaxRxn) { if (err) *err = "too many reactions"; return -6; }
+  sim.rxn[x.order].push_back(x);
+  return 0;
+}
+
 static int add_reaction_from_words(Sim &sim, const std::vector<std::string> &w, std::string *err) {
   // reaction [name] r1 [+ r2] -> p1 [+ p2 ...] [rate]
   if (w.size() < 3) { if (err) *err = "reaction: too few words"; return -7; }
@@ -749,27 +781,8 @@ static int add_reaction_from_words(Sim &sim, const std::vector<std::string> &w, 
       x.prd[q] = i;
       x.pstate[q] = st;
     }
-    // surface states in reactions: a first-order reaction of a bound reactant,
-    // or a second-order one of a bound and a solution reactant, with at most
-    // one product (reactant and product states of smolreact.c:2662-2902)
-    int nbound = 0;
-    for (int q = 0; q < x.order; ++q) nbound += x.rstate[q] != 0;
-    const bool bound = nbound > 0;
-    bool bprod = false;
-    for (int q = 0; q < x.nprod; ++q) bprod = bprod || x.pstate[q] != 0;
-    if (bound && (x.order == 0 || nbound > 1 || x.nprod > 1)) {
-      if (err) *err = "reactions of surface-bound molecules are supported as first order, or second order with one "
-                      "solution reactant, with at most one product";
-      return -7;
-    }
-    if (!bound && bprod) {
-      if (err) *err = "products in surface states need a surface-bound reactant";
-      return -7;
-    }
     x.rate = rate;
-    if ((int)sim.rxn[x.order].size() >= kMaxRxn) { if (err) *err = "too many reactions"; return -6; }
-    sim.rxn[x.order].push_back(x);
-    return 0;
+    return add_reaction_def(sim, x, err);
   };
   int rc = mk(reversible ? name + "fwd" : name, rct, prd, rates.empty() ? -1 : rates[0]);
   if (rc) return rc;

@@ -199,6 +199,9 @@ int make_panel(int dim, int shape, const std::string &axis, const double *prm, i
                std::string *err);
 // Restatements of the reference's parameter derivation.
 int derive_reaction_params(Sim &sim, std::string *err);
+// Append reaction x (order, reactants, products and their states set) after
+// checking the states the engine builds; 0 or an error code with *err set.
+int add_reaction_def(Sim &sim, const RxnDef &x, std::string *err);
 // rxncalcrate (smolreact.c:1592-1680): effective rate from derived parameters.
 double calc_rate(const Sim &sim, int order, int r, double *pgem);
 // surfupdateparams (smolsurface.c:3735-3800): derived probabilities of every

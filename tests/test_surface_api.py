@@ -139,3 +139,30 @@ def test_bound_solution_reaction_parameters_match_reference():
             assert abs(b - rad) <= 2e-5 * rad + 1e-9, (nm, b, rad, str(text))
             assert abs(k - rate) <= 2e-5 * rate + 1e-9, (nm, k, rate, str(text))
         s.close()
+
+
+def test_add_reaction_with_states_through_the_c_api():
+    """smolAddReaction takes reactant and product states as the text form
+    does (libsmoldyn.cpp smolAddReaction): the same derived parameters, and
+    the same refusals."""
+    lib = sb.load()
+    text = TEXT.replace("end_file", "difc B 0.7\nreaction r A(front) + B -> A(front) 1.2\nend_file")
+    d = tempfile.mkdtemp()
+    with open(os.path.join(d, "c.txt"), "w") as f:
+        f.write(text)
+    a = sb.Sim.load_file(os.path.join(d, "c.txt"))
+    b = from_api()
+    assert lib.smolSetSpeciesMobility(b.ptr, b"B", sb.MSsoln, 0.7, None, None) == 0
+    prods = (C.c_char_p * 1)(b"A")
+    states = (C.c_int * 1)(sb.MSfront)
+    assert lib.smolAddReaction(b.ptr, b"r", b"A", sb.MSfront, b"B", sb.MSsoln, 1, prods,
+                               C.cast(states, C.POINTER(C.c_int)), 1.2) == 0
+    assert a.reaction_params("r") == b.reaction_params("r")
+    assert a.effective_rate("r") == b.effective_rate("r")
+    # two bound reactants, and a bound product of solution reactants, are refused
+    assert lib.smolAddReaction(b.ptr, b"r2", b"A", sb.MSfront, b"A", sb.MSback, 1, prods,
+                               C.cast(states, C.POINTER(C.c_int)), 1.0) != 0
+    assert lib.smolAddReaction(b.ptr, b"r3", b"B", sb.MSsoln, None, sb.MSsoln, 1, prods,
+                               C.cast(states, C.POINTER(C.c_int)), 1.0) != 0
+    a.close()
+    b.close()
