@@ -145,6 +145,7 @@ struct DevNet {
   int bpair_n;
   uint8_t bpair_rxn[kMaxRxn], bpair_bsp[kMaxRxn], bpair_bst[kMaxRxn], bpair_ssp[kMaxRxn], bpair_pst[kMaxRxn];
   uint32_t bpair_mask[kMaxSpecies][2];
+  float bpair_rmax;  // largest binding radius of these reactions, padded as the stencil radii are
 };
 
 // A molecule bound to a panel: absolute position (relative to the system's

@@ -1391,6 +1391,10 @@ __device__ __forceinline__ void bpair_partner_pos(const KParams &p, int j, const
     }
 }
 
+// One warp per bound molecule: lanes 0..26 take the neighbour boxes that the
+// largest binding radius of these reactions reaches from the molecule's place
+// in its box, a warp prefix sum numbers their molecules, and the lanes test
+// them 32 at a time; a warp minimum picks the claim.
 __global__ void __launch_bounds__(256) k_bpair_claim(KParams p, int round) {
   pdl_launch_dependents();
   pdl_wait();
@@ -1399,73 +1403,110 @@ __global__ void __launch_bounds__(256) k_bpair_claim(KParams p, int round) {
   const uint32_t step = *p.step;
   const DevGeo &g = c_geo0;
   const uint2 key = make_uint2(c_net.key0 ^ 0x7F4A7C15u, c_net.key1 ^ 0x94D049BBu);
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nb; k += gridDim.x * blockDim.x) {
-    int4 c = p.bcand[k];
-    if (round > 0 && !(c.x >= 0 && c.w == 0)) continue;  // later rounds: the molecules that lost their partner
-    c = make_int4(-1, 0, 0, 0);
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const float rmax = c_net.bpair_rmax;
+  for (int k = gw; k < nb; k += nw) {
+    const int4 c0 = p.bcand[k];
+    if (round > 0 && !(c0.x >= 0 && c0.w == 0)) continue;  // later rounds: the molecules that lost their partner
     const BoundMol m = p.bd_out[k];
     const int sp = id_species(m.id);
     const uint32_t mask = sp == kDeadSpecies ? 0u : c_net.bpair_mask[sp][m.ms - 1];
+    ull best = ~0ull;  // (priority << 32 | lane) of this lane's best partner
+    int bj = -1, be = 0;
     if (mask) {
       const DevPanel &pn = c_panels[m.pnl];
       const ull kb = id_stream(m.id);
       int ix[3];
       float u[3];
       from_abs(g, m.x, ix, u);
-      uint32_t bestp = 0xFFFFFFFFu;
-      for (int dz = -1; dz <= 1; ++dz)
-        for (int dy = -1; dy <= 1; ++dy)
-          for (int dx = -1; dx <= 1; ++dx) {
-            const int off[3] = {dx, dy, dz};
-            int cc[3];
-            bool ok = true;
-            for (int d = 0; d < 3; ++d) {
-              if (d >= g.dim && off[d] != 0) ok = false;
-              cc[d] = ix[d] + off[d];
-              if (cc[d] < 0 || cc[d] >= g.n[d]) {
-                if (g.wall[2 * d] != kWallPeriodic || g.n[d] < 3) ok = false;
-                cc[d] = cc[d] < 0 ? cc[d] + g.n[d] : cc[d] - g.n[d];
-              }
-            }
-            if (!ok) continue;
-            const int cell = g.cell0 + (cc[2] * g.n[1] + cc[1]) * g.n[0] + cc[0];
-            const int e0 = min(p.start[cell + 1], n);
-            for (int j = p.start[cell]; j < e0; ++j) {
-              const ull idj = p.b_id[j];
-              const int sj = id_species(idj);
-              if (sj == kDeadSpecies || !((mask >> sj) & 1u)) continue;
-              double xs[3];
-              bpair_partner_pos(p, j, m.x, xs);
-              const double d2 = (xs[0] - m.x[0]) * (xs[0] - m.x[0]) + (xs[1] - m.x[1]) * (xs[1] - m.x[1]) +
-                                (xs[2] - m.x[2]) * (xs[2] - m.x[2]);
-              const ull pk = mix64((kb * 0x9E3779B97F4A7C15ull ^ id_stream(idj)) + (ull)step * 0xD1B54A32D192ED03ull);
-              const uint32_t prio = (uint32_t)(pk >> 32);
-              if (c.x >= 0 && prio >= bestp) continue;
-              int side = -1;  // the panel side, read once a reaction is in range
-              for (int e = 0; e < c_net.bpair_n; ++e) {
-                if (c_net.bpair_bsp[e] != sp || c_net.bpair_bst[e] != m.ms || c_net.bpair_ssp[e] != sj) continue;
-                const int r = c_net.bpair_rxn[e];
-                if (d2 > (double)p.bind2[r]) continue;
-                const float prob = p.pairprob[r];
-                if (prob < 1.f) {
-                  const ull kk = mix64(kb * 0x9E3779B97F4A7C15ull ^ id_stream(idj));
-                  const uint4 rr = philox(make_uint4((uint32_t)kk, (uint32_t)(kk >> 32), step, kCtrBPair + (uint32_t)e), key);
-                  if (!(u01co(rr.x) < (double)prob)) continue;
-                }
-                if (side < 0) side = panel_side(pn, xs, nullptr) == kFaceBack ? 0 : 1;
-                if (!side) break;  // behind the panel: the solution state is bsoln, which no reaction takes
-                const int cm = c_net.cmpt[2][r];
-                if (cm && !(pos_in_cmpt(c_cmpt, cm - 1, c_panels, xs) && pos_in_cmpt(c_cmpt, cm - 1, c_panels, m.x)))
-                  continue;
-                bestp = prio;
-                c = make_int4(j, e, (int)prio, 0);
-                break;
-              }
-            }
+      int s0 = 0, cnt = 0;
+      if (lane < 27) {
+        const int off[3] = {lane % 3 - 1, (lane / 3) % 3 - 1, lane / 9 - 1};
+        int cc[3];
+        bool ok = true;
+        for (int d = 0; d < 3; ++d) {
+          if (d >= g.dim && off[d] != 0) ok = false;
+          const float ub = (ix[d] == g.n[d] - 1) ? g.whi[d] : g.h[d];
+          if (off[d] < 0 && !(u[d] < rmax)) ok = false;
+          if (off[d] > 0 && !(u[d] > ub - rmax)) ok = false;
+          cc[d] = ix[d] + off[d];
+          if (cc[d] < 0 || cc[d] >= g.n[d]) {
+            if (g.wall[2 * d] != kWallPeriodic || g.n[d] < 3) ok = false;
+            cc[d] = cc[d] < 0 ? cc[d] + g.n[d] : cc[d] - g.n[d];
           }
+        }
+        if (ok) {
+          const int cell = g.cell0 + (cc[2] * g.n[1] + cc[1]) * g.n[0] + cc[0];
+          s0 = p.start[cell];
+          cnt = max(0, min(p.start[cell + 1], n) - s0);
+        }
+      }
+      int incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(full, incl, o);
+        if (lane >= o) incl += y;
+      }
+      const int excl = incl - cnt;
+      const int total = __shfl_sync(full, incl, 31);
+      for (int t0 = 0; t0 < total; t0 += 32) {
+        const int t = t0 + lane;
+        int o = 0;  // the last lane whose first number is <= t
+#pragma unroll
+        for (int st = 16; st > 0; st >>= 1)
+          if (__shfl_sync(full, excl, o + st) <= t) o += st;
+        const int j = __shfl_sync(full, s0, o) + (t - __shfl_sync(full, excl, o));
+        if (t >= total) continue;
+        const ull idj = p.b_id[j];
+        const int sj = id_species(idj);
+        if (sj == kDeadSpecies || !((mask >> sj) & 1u)) continue;
+        double xs[3];
+        bpair_partner_pos(p, j, m.x, xs);
+        const double d2 = (xs[0] - m.x[0]) * (xs[0] - m.x[0]) + (xs[1] - m.x[1]) * (xs[1] - m.x[1]) +
+                          (xs[2] - m.x[2]) * (xs[2] - m.x[2]);
+        const ull pk = mix64((kb * 0x9E3779B97F4A7C15ull ^ id_stream(idj)) + (ull)step * 0xD1B54A32D192ED03ull);
+        const uint32_t prio = (uint32_t)(pk >> 32);
+        const ull pkey = ((ull)prio << 32) | (uint32_t)lane;
+        if (pkey >= best) continue;
+        int side = -1;  // the panel side, read once a reaction is in range
+        for (int e = 0; e < c_net.bpair_n; ++e) {
+          if (c_net.bpair_bsp[e] != sp || c_net.bpair_bst[e] != m.ms || c_net.bpair_ssp[e] != sj) continue;
+          const int r = c_net.bpair_rxn[e];
+          if (d2 > (double)p.bind2[r]) continue;
+          const float prob = p.pairprob[r];
+          if (prob < 1.f) {
+            const ull kk = mix64(kb * 0x9E3779B97F4A7C15ull ^ id_stream(idj));
+            const uint4 rr = philox(make_uint4((uint32_t)kk, (uint32_t)(kk >> 32), step, kCtrBPair + (uint32_t)e), key);
+            if (!(u01co(rr.x) < (double)prob)) continue;
+          }
+          if (side < 0) side = panel_side(pn, xs, nullptr) == kFaceBack ? 0 : 1;
+          if (!side) break;  // behind the panel: the solution state is bsoln, which no reaction takes
+          const int cm = c_net.cmpt[2][r];
+          if (cm && !(pos_in_cmpt(c_cmpt, cm - 1, c_panels, xs) && pos_in_cmpt(c_cmpt, cm - 1, c_panels, m.x)))
+            continue;
+          best = pkey;
+          bj = j;
+          be = e;
+          break;
+        }
+      }
     }
-    p.bcand[k] = c;
-    if (c.x >= 0) atomicMin(&p.bclaim[c.x], ((ull)(uint32_t)c.z << 32) | (ull)(uint32_t)k);
+    // warp minimum: the lowest priority (ties to the lower lane)
+    ull wmin = best;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const ull y = __shfl_xor_sync(full, wmin, o);
+      wmin = y < wmin ? y : wmin;
+    }
+    if (wmin != ~0ull && best == wmin) {  // the winning lane
+      p.bcand[k] = make_int4(bj, be, (int)(uint32_t)(wmin >> 32), 0);
+      atomicMin(&p.bclaim[bj], (wmin & 0xFFFFFFFF00000000ull) | (ull)(uint32_t)k);
+    } else if (wmin == ~0ull && lane == 0) {
+      p.bcand[k] = make_int4(-1, 0, 0, 0);
+    }
   }
 }
 
@@ -3867,6 +3908,7 @@ class EngineImpl {
     const int nr2 = std::max(1, net.nrxn[2]), nr0 = std::max(1, net.nrxn[0]);
     std::vector<float> bind2((size_t)R * nr2, 0.f), pairprob((size_t)R * nr2, 1.f);
     std::vector<float> rsearch((size_t)R * nsp, 0.f);
+    float bpair_rmax = 0.f;
     std::vector<double> births((size_t)R * nr0, 0.0);
     const int nrx = std::max(1, dnet.nrx_total);
     std::vector<float> prdpos((size_t)R * nrx * kMaxProd * 3, 0.f);
@@ -3909,7 +3951,12 @@ class EngineImpl {
       for (int r = 0; r < net.nrxn[2]; ++r) {
         bind2[(size_t)rp * nr2 + r] = (float)s.bind2[r];
         pairprob[(size_t)rp * nr2 + r] = (float)s.pair_prob[r];
-        if (net.rstate2[r][0] != 0 || net.rstate2[r][1] != 0) continue;  // searched from the bound list
+        if (net.rstate2[r][0] != 0 || net.rstate2[r][1] != 0) {  // searched from the bound list
+          const double hmin0 = std::min(geo[rp].h[0], std::min(geo[rp].h[1], geo[rp].h[2]));
+          const double rb = std::sqrt(std::max(0.0, s.bind2[r])) * (1.0 + 1e-4) + 1e-6 * hmin0;
+          if (rp == 0) bpair_rmax = std::max(bpair_rmax, (float)rb);
+          continue;
+        }
         // stencil radius: largest binding radius of the species' pair reactions,
         // padded so FP32 rounding of a distance at the radius cannot fall outside
         const double hmin = std::min(geo[rp].h[0], std::min(geo[rp].h[1], geo[rp].h[2]));
@@ -3929,6 +3976,7 @@ class EngineImpl {
     }
     dnet.any_drift = any_drift ? 1 : 0;
     dnet.difm_any = difm_any;
+    dnet.bpair_rmax = bpair_rmax;
     auto put = [&](void **dst, const void *src, size_t bytes) -> int {
       if (!*dst) CK(cudaMalloc(dst, bytes));
       CK(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, stream));
