@@ -137,7 +137,7 @@ struct DevNet {
   uint8_t buni_n[kMaxSpecies][2];
   uint8_t buni_list[kMaxSpecies][2][kMaxUniPerSpecies];
   uint32_t bthr[kMaxSpecies][2][kMaxUniPerSpecies];
-  uint8_t pstate1[kMaxRxn];        // product state of each first-order reaction
+  uint8_t pstate1[kMaxRxn][2];     // product states of each first-order reaction (first two products)
   // second-order reactions of a bound and a solution reactant, in list
   // order: the reaction, the bound reactant's species and state (1 front,
   // 2 back), the solution reactant's species and the product's state; per

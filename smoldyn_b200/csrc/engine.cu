@@ -471,6 +471,7 @@ constexpr uint32_t kCtrSrfWalk2 = 0x200u;  // + iteration: the same for the plac
 constexpr uint32_t kCtrSrfBound = 0x300u;  // desorption / flip coin and desorption distance
 constexpr uint32_t kCtrSrfDiff = 0x301u;   // diffusion of a bound molecule
 constexpr uint32_t kCtrSrfRxn = 0x302u;    // first-order reaction coin of a bound molecule
+constexpr uint32_t kCtrSrfRot = 0x303u;    // rotation of that reaction's product offsets
 constexpr uint32_t kCtrSrfBWalk = 0x400u;  // + iteration: collision coins of a bound molecule
 constexpr uint32_t kCtrSrfEdge = 0x1000u;  // + 64 * iteration (+ 1 + neighbour): panel-edge choices
 
@@ -711,16 +712,44 @@ __device__ int bound_coin(const KParams &p, BoundMol &m, int &sp, ull skey, uint
   return 0;
 }
 
+__device__ __forceinline__ void random_rotation(uint4 r, float m[9]);
+__device__ __forceinline__ void push_bound(const KParams &p, const BoundMol &m);
+
+// Place product q of first-order reaction r of bound molecule m (doreact,
+// smolreact.c:2806-2880): the reactant's place, kept on the product state's
+// side of its panel (fixpt2panel), displaced by the product's offset under
+// the reaction's random rotation R, and brought back onto the surface
+// (movemol2closepanel; a solution product takes the front or back state for
+// that, as the reference does, so its offset off the panel is dropped).
+__device__ void bound_product_place(const KParams &p, const BoundMol &m, int r, int q, int pst, const float R[9],
+                                    bool rot, ull skey, uint32_t step, double x[3], int &pnl) {
+  const int f = (pst == kMSback || pst == kMSbsoln) ? kFaceBack : kFaceFront;
+  double x0[3] = {m.x[0], m.x[1], m.x[2]};
+  fix_to_panel(c_panels[m.pnl], x0, f, c_net.beps);
+  for (int d = 0; d < 3; ++d) x[d] = x0[d];
+  if (rot) {
+    const float *pp = p.prdpos + ((size_t)(c_net.rxn_base[1] + r) * kMaxProd + q) * 3;  // single simulation
+    for (int d = 0; d < 3; ++d)
+      x[d] += (double)R[3 * d] * pp[0] + (double)R[3 * d + 1] * pp[1] + (double)R[3 * d + 2] * pp[2];
+  }
+  pnl = m.pnl;
+  const ull k2 = mix64(skey ^ (0xB0A1ull + (ull)q)) & ((1ull << kSpShift) - 1);  // its own edge choices
+  move_to_close_panel(x, x0, pnl, f == kFaceBack ? kMSback : kMSfront, k2, step);
+}
+
 // First-order reactions of a bound molecule (unireact on the bound state,
 // smolreact.c:2997-3056, after the surface actions as in the reference's step
 // order), with the sequential-coin thresholds of its species and state.
-// The one product takes the reactant's place (doreact, smolreact.c:2806-2834):
-// a bound product is put on the reactant's panel on its state's side; a
-// solution product at the reactant's place just off the panel's front (soln)
-// or back (bsoln) side, into the output product list, so that, like the
-// reference's products, it first moves in the next step.  Returns 0 no
-// reaction, 1 reacted without product, 2 bound product (m, sp updated),
-// 3 solution product written (sp updated).
+// Products (doreact, smolreact.c:2662-2902) start from the reactant's place:
+// bound ones on its panel on their state's side, solution ones just off the
+// panel's front (soln) or back (bsoln) side in the output product list, so
+// that, like the reference's products, they first move in the next step;
+// with two products, their offsets (unbinding radius split by diffusion
+// coefficients) turn under one random rotation.  The first bound product, or
+// else the first product, takes over the reactant's entry and count; another
+// product is counted here.  Returns 0 no reaction, 1 reacted without product,
+// 2 the reactant's entry became a bound product (m, sp updated), 3 it became
+// a solution product in the product list (sp updated).
 __device__ int bound_first_order(const KParams &p, BoundMol &m, int &sp, ull skey, uint32_t step) {
   const int st = m.ms - 1;
   const int nr = c_net.buni_n[sp][st];
@@ -731,35 +760,65 @@ __device__ int bound_first_order(const KParams &p, BoundMol &m, int &sp, ull ske
     if (u < c_net.bthr[sp][st][k]) { r = c_net.buni_list[sp][st][k]; break; }
   if (r < 0) return 0;
   atomicAdd(&p.counters[2], 1ull);
-  if (c_net.nprod[1][r] == 0) return 1;
-  const int psp = c_net.prd[1][r][0], pst = c_net.pstate1[r];
-  const DevPanel &pn = c_panels[m.pnl];
-  if (pst == kMSfront || pst == kMSback) {
-    sp = psp;
-    m.ms = pst;
-    fix_to_panel(pn, m.x, ms_face(pst), c_net.beps);
-    return 2;
+  const int np = min((int)c_net.nprod[1][r], 2);
+  if (np == 0) return 1;
+  float R[9];
+  const bool rot = c_net.has_offset[1][r] != 0;
+  if (rot) random_rotation(srf_draw(skey, step, kCtrSrfRot), R);
+  int q0 = 0;  // the product that takes over the reactant's entry
+  for (int q = np - 1; q >= 0; --q)
+    if (c_net.pstate1[r][q] == kMSfront || c_net.pstate1[r][q] == kMSback) q0 = q;
+  const BoundMol m0 = m;
+  int ret = 0;
+  for (int q = 0; q < np; ++q) {
+    const int psp = c_net.prd[1][r][q], pst = c_net.pstate1[r][q];
+    double x[3];
+    int pnl;
+    bound_product_place(p, m0, r, q, pst, R, rot, skey, step, x, pnl);
+    const ull sn = q == q0 ? id_serno(m0.id)
+                           : kProductSernoBit | (mix64(skey ^ ((ull)step << 20) ^ ((ull)(q + 1) << 50) ^ 0x51D0ull) &
+                                                 (kProductSernoBit - 1));
+    if (pst == kMSfront || pst == kMSback) {
+      BoundMol b;
+      for (int d = 0; d < 3; ++d) b.x[d] = x[d];
+      b.pnl = pnl;
+      b.ms = pst;
+      b.id = make_id(psp, 0, sn);
+      if (q == q0) {
+        m = b;
+        sp = psp;
+        ret = 2;
+      } else {
+        push_bound(p, b);
+        atomicAdd((unsigned long long *)&p.spcount[psp], 1ull);
+      }
+      continue;
+    }
+    const int f = pst == kMSbsoln ? kFaceBack : kFaceFront;
+    const DevPanel &pn = c_panels[pnl];
+    double n[3];
+    face_normal(pn, x, f, n);
+    const double sd = fabs(panel_sdist<true>(pn, x));
+    if (sd < c_net.surf_eps)  // kept surf_eps off the panel, as solution molecules are
+      for (int d = 0; d < 3; ++d) x[d] += (c_net.surf_eps - sd) * n[d];
+    int ix[3];
+    float w[3];
+    from_abs(c_geo0, x, ix, w);
+    const int slot = atomicAdd(p.q_n, 1);
+    if (slot < p.pcap) {
+      p.q_pc[slot] = make_float4(w[0], w[1], w[2], __uint_as_float(pack_cell(ix[0], ix[1], ix[2])));
+      p.q_id[slot] = make_id(psp, 0, sn);
+    } else {
+      atomicOr(p.status, kStProdCap);
+    }
+    if (q == q0) {
+      sp = psp;
+      ret = 3;
+    } else {
+      atomicAdd((unsigned long long *)&p.spcount[psp], 1ull);
+    }
   }
-  double x[3] = {m.x[0], m.x[1], m.x[2]};
-  const int f = pst == kMSbsoln ? kFaceBack : kFaceFront;
-  double n[3];
-  face_normal(pn, x, f, n);
-  fix_to_panel(pn, x, f, c_net.beps);
-  const double sd = fabs(panel_sdist<true>(pn, x));
-  if (sd < c_net.surf_eps)  // kept surf_eps off the panel, as solution molecules are
-    for (int d = 0; d < 3; ++d) x[d] += (c_net.surf_eps - sd) * n[d];
-  int ix[3];
-  float w[3];
-  from_abs(c_geo0, x, ix, w);
-  sp = psp;
-  const int slot = atomicAdd(p.q_n, 1);
-  if (slot < p.pcap) {
-    p.q_pc[slot] = make_float4(w[0], w[1], w[2], __uint_as_float(pack_cell(ix[0], ix[1], ix[2])));
-    p.q_id[slot] = make_id(psp, 0, id_serno(m.id));
-  } else {
-    atomicOr(p.status, kStProdCap);
-  }
-  return 3;
+  return ret;
 }
 
 // Crossings of other panels by a bound molecule's move from posx (on panel
@@ -879,6 +938,7 @@ __device__ __noinline__ int soln_surface_bound(const KParams &p, ull &id, const 
     for (int d = 0; d < 3; ++d) m.x[d] = x1[d];
     m.pnl = pnl;
     m.ms = ms;
+    m.id = make_id(sp, 0, id_serno(id));
     double y0[3], y1[3];
     const int c = bound_coin(p, m, sp, skey, step, y0, y1);
     if (c == 1) return 1;
@@ -4394,7 +4454,7 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
   for (int r = 0; r < net.nrxn[1]; ++r) {
     const int sp = net.rct[1][r][0];
     D.rct[1][r][0] = (uint8_t)sp;
-    D.pstate1[r] = (uint8_t)net.pstate1[r];
+    for (int q = 0; q < 2; ++q) D.pstate1[r][q] = (uint8_t)net.pstate1[r][q];
     const int st = net.rstate1[r];
     if (st == 1 || st == 2) {  // a surface-bound reactant: the bound list's own table
       uint8_t &nb = D.buni_n[sp][st - 1];

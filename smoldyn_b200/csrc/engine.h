@@ -95,7 +95,7 @@ struct NetSpec {
   // first-order reactions of surface-bound reactants: reactant state (0 soln,
   // 1 front, 2 back) and product state (0 soln, 1 front, 2 back, 5 bsoln)
   int rstate1[kMaxRxn] = {};
-  int pstate1[kMaxRxn] = {};
+  int pstate1[kMaxRxn][2] = {};
   // second-order reactions with one surface-bound reactant: reactant states
   // and the product's state
   int rstate2[kMaxRxn][2] = {};

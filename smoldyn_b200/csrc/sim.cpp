@@ -80,8 +80,12 @@ static bool same_set2(int a0, int a1, int b0, int b1) {
 }
 
 // findreverserxn (smolreact.c:345-381): rev=1 when a reaction of order nprod
-// consumes exactly this reaction's products and makes its reactants; rev=2
+// consumes exactly this reaction's products (species and states: the
+// reaction's permit for the product states) and makes its reactants; rev=2
 // when the products only react onward.
+static bool same_set_st(int a1, int s1, int a2, int s2, int b1, int t1, int b2, int t2) {
+  return (a1 == b1 && s1 == t1 && a2 == b2 && s2 == t2) || (a1 == b2 && s1 == t2 && a2 == b1 && s2 == t1);
+}
 static int find_reverse(const Sim &s, int order, int r, int *o2, int *r2) {
   const RxnDef &x = s.rxn[order][r];
   *o2 = 0;
@@ -93,13 +97,16 @@ static int find_reverse(const Sim &s, int order, int r, int *o2, int *r2) {
   int rev = 0;
   for (size_t k = 0; k < s.rxn[orr].size(); ++k) {
     const RxnDef &y = s.rxn[orr][k];
-    // the products here are in solution: a reaction of bound reactants is
-    // not permitted for them
-    if (y.rstate[0] != 0 || (orr == 2 && y.rstate[1] != 0)) continue;
-    bool rct_match = (orr == 1) ? (y.rct[0] == x.prd[0]) : same_set2(y.rct[0], y.rct[1], x.prd[0], x.prd[1]);
+    const bool rct_match =
+        (orr == 1) ? (y.rct[0] == x.prd[0] && y.rstate[0] == x.pstate[0])
+                   : same_set_st(y.rct[0], y.rstate[0], y.rct[1], y.rstate[1], x.prd[0], x.pstate[0], x.prd[1],
+                                 x.pstate[1]);
     if (!rct_match) continue;
     if (rev != 1 && y.nprod == order) {
-      bool back = (order == 1) ? (y.prd[0] == x.rct[0]) : same_set2(y.prd[0], y.prd[1], x.rct[0], x.rct[1]);
+      const bool back =
+          (order == 1) ? (y.prd[0] == x.rct[0] && y.pstate[0] == x.rstate[0])
+                       : same_set_st(y.prd[0], y.pstate[0], y.prd[1], y.pstate[1], x.rct[0], x.rstate[0], x.rct[1],
+                                     x.rstate[1]);
       if (back) {
         rev = 1;
         *r2 = (int)k;
@@ -156,7 +163,7 @@ int derive_reaction_params(Sim &sim, std::string *err) {
       }
     }
     int o2, r2;
-    const int rev = x.rstate[0] == 0 ? find_reverse(sim, 1, (int)r, &o2, &r2) : 0;
+    const int rev = find_reverse(sim, 1, (int)r, &o2, &r2);
     if (rev > 0 && o2 == 2 && x.rparamt == RP_none) {
       x.rparamt = RP_pgemmaxw;
       x.rparam = 0.2;
@@ -190,7 +197,7 @@ int derive_reaction_params(Sim &sim, std::string *err) {
     const double dsum = (s1 ? sim.species[i1].difc_bound[s1 - 1] : sim.species[i1].difc) +
                         (s2 ? sim.species[i2].difc_bound[s2 - 1] : sim.species[i2].difc);
     int o2 = 0, r2 = 0;
-    const int rev = (s1 == 0 && s2 == 0) ? find_reverse(sim, 2, (int)r, &o2, &r2) : 0;
+    const int rev = find_reverse(sim, 2, (int)r, &o2, &r2);
     if (rev > 0 && o2 == 2 && x.rparamt == RP_none) {
       x.rparamt = RP_pgemmaxw;
       x.rparam = 0.2;
@@ -263,7 +270,13 @@ int derive_reaction_params(Sim &sim, std::string *err) {
         x.prdpos[0][0] = len * dc1;
         x.prdpos[1][0] = len * dc2;
       } else {
-        double dc1 = sim.species[x.prd[0]].difc, dc2 = sim.species[x.prd[1]].difc;
+        // the products' diffusion coefficients in their states (MolCalcDifcSum;
+        // bsoln counts as solution)
+        auto pdifc = [&](int q) {
+          const int st = x.pstate[q];
+          return (st == 1 || st == 2) ? sim.species[x.prd[q]].difc_bound[st - 1] : sim.species[x.prd[q]].difc;
+        };
+        double dc1 = pdifc(0), dc2 = pdifc(1);
         const double dsum = dc1 + dc2;
         if (dsum == 0) dc1 = dc2 = 0.5;
         else { dc1 /= dsum; dc2 /= dsum; }
@@ -374,8 +387,8 @@ double calc_rate(const Sim &sim, int order, int r, double *pgem) {
     if (x.prob > 0) {
       const int i1 = x.rct[0];
       double probthis = 0, product = 1.0, sum = 0;
-      for (const RxnDef &y : sim.rxn[1]) {
-        if (y.rct[0] != i1 || !(y.prob > 0)) continue;
+      for (const RxnDef &y : sim.rxn[1]) {  // the reactions of this species in this state
+        if (y.rct[0] != i1 || y.rstate[0] != x.rstate[0] || !(y.prob > 0)) continue;
         const double pr = y.prob * product;
         if (&y == &x) probthis = pr;
         sum += pr;
@@ -396,7 +409,7 @@ double calc_rate(const Sim &sim, int order, int r, double *pgem) {
       const double step = std::sqrt(2.0 * dsum * dt);
       const double a = std::sqrt(x.bindrad2);
       int o2 = 0, r2 = 0;
-      const int rev = (s1 == 0 && s2 == 0) ? find_reverse(sim, 2, r, &o2, &r2) : 0;
+      const int rev = find_reverse(sim, 2, r, &o2, &r2);
       const int rpt = rev == 1 ? sim.rxn[o2][r2].rparamt : RP_none;
       if (rpt == RP_pgem || rpt == RP_pgemmax || rpt == RP_pgemmaxw || rpt == RP_ratio || rpt == RP_unbindrad) {
         const RxnDef &rv = sim.rxn[o2][r2];
@@ -418,7 +431,11 @@ double calc_rate(const Sim &sim, int order, int r, double *pgem) {
     if (x.nprod != 2 || find_reverse(sim, order, r, &o2, &r2) == 0) {
       *pgem = -1;
     } else {
-      const double step = std::sqrt(2.0 * (sim.species[x.prd[0]].difc + sim.species[x.prd[1]].difc) * dt);
+      auto pdifc = [&](int q) {
+        const int st = x.pstate[q];
+        return (st == 1 || st == 2) ? sim.species[x.prd[q]].difc_bound[st - 1] : sim.species[x.prd[q]].difc;
+      };
+      const double step = std::sqrt(2.0 * (pdifc(0) + pdifc(1)) * dt);
       double b2 = 0;
       for (int d = 0; d < sim.dim; ++d) {
         const double v = x.prdpos[0][d] - x.prdpos[1][d];
@@ -576,18 +593,20 @@ int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err) {
       net->fixed_placement[o][r] = (x.rparamt == RP_fixed) ? 1 : 0;
       if (o == 1) {
         net->rstate1[r] = x.rstate[0];
-        net->pstate1[r] = x.nprod ? x.pstate[0] : 0;
+        for (int q = 0; q < 2; ++q) net->pstate1[r][q] = q < x.nprod ? x.pstate[q] : 0;
+        if (x.rstate[0] && (x.rparamt == RP_confspread || x.rparamt == RP_bounce || x.rparamt == RP_fixed ||
+                            x.rparamt == RP_offset)) {
+          if (err) *err = "reaction " + x.name + ": confspread, bounce, offset and fixed are not built for surface-bound reactants";
+          return -7;
+        }
       }
       if (o == 2) {
         net->rstate2[r][0] = x.rstate[0];
         net->rstate2[r][1] = x.rstate[1];
         net->pstate2[r] = x.nprod ? x.pstate[0] : 0;
-        bool off = false;
-        for (int q = 0; q < x.nprod; ++q)
-          for (int d = 0; d < 3; ++d) off = off || x.prdpos[q][d] != 0;
-        if ((x.rstate[0] || x.rstate[1]) &&
-            (x.rparamt == RP_confspread || x.rparamt == RP_bounce || x.rparamt == RP_fixed || off)) {
-          if (err) *err = "reaction " + x.name + ": a surface-bound reactant takes the default product placement only";
+        if ((x.rstate[0] || x.rstate[1]) && (x.rparamt == RP_confspread || x.rparamt == RP_bounce ||
+                                              x.rparamt == RP_fixed || x.rparamt == RP_offset)) {
+          if (err) *err = "reaction " + x.name + ": confspread, bounce, offset and fixed are not built for surface-bound reactants";
           return -7;
         }
       }
@@ -681,10 +700,10 @@ static int species_arg(Sim &sim, const std::string &w, std::vector<int> *out) {
 }
 
 // Append a reaction after checking its reactant and product states: solution
-// reactions, a first-order reaction of a bound reactant, or a second-order
-// one of a bound and a solution reactant, with at most one product (the
-// reactant and product states of doreact, smolreact.c:2662-2902, that the
-// engine builds).
+// reactions, a first-order reaction of a bound reactant with at most two
+// products, or a second-order one of a bound and a solution reactant with at
+// most one product (the reactant and product states of doreact,
+// smolreact.c:2662-2902, that the engine builds).
 int add_reaction_def(Sim &sim, const RxnDef &x, std::string *err) {
   int nbound = 0;
   for (int q = 0; q < x.order; ++q) {
@@ -698,9 +717,9 @@ int add_reaction_def(Sim &sim, const RxnDef &x, std::string *err) {
     if (st < 0 || (st > 2 && st != 5)) { if (err) *err = "product state not supported by the GPU engine"; return -7; }
     bprod = bprod || st != 0;
   }
-  if (bound && (x.order == 0 || nbound > 1 || x.nprod > 1)) {
-    if (err) *err = "reactions of surface-bound molecules are supported as first order, or second order with one "
-                    "solution reactant, with at most one product";
+  if (bound && (x.order == 0 || nbound > 1 || x.nprod > (x.order == 1 ? 2 : 1))) {
+    if (err) *err = "reactions of surface-bound molecules are supported as first order with at most two products, "
+                    "or second order with one solution reactant and at most one product";
     return -7;
   }
   if (!bound && bprod) {
@@ -1026,8 +1045,9 @@ int read_config_statement(Sim &sim, const std::string &word, const std::string &
     const int rp = rp_from_string(w[1]);
     if (rp < 0) { if (err) *err = "product_placement: unknown type " + w[1]; return -7; }
     RxnDef &x = sim.rxn[o][r];
-    if ((x.rstate[0] != 0 || (o == 2 && x.rstate[1] != 0)) && rp != RP_none && rp != RP_irrev) {
-      if (err) *err = "product_placement: a reaction of a surface-bound reactant takes the default placement only";
+    if ((x.rstate[0] != 0 || (o == 2 && x.rstate[1] != 0)) &&
+        (rp == RP_confspread || rp == RP_bounce || rp == RP_offset || rp == RP_fixed)) {
+      if (err) *err = "product_placement: confspread, bounce, offset and fixed are not built for surface-bound reactants";
       return -7;
     }
     x.rparamt = rp;

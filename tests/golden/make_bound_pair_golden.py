@@ -1,13 +1,17 @@
 """Generate tests/golden/bound_pair_params.npz from the reference binary.
 
-Seeded random configurations with second-order reactions between a
-surface-bound reactant (front or back state, first or second reactant) and a
-solution reactant are loaded by oracle/_ref/smoldyn with `-t` (text output,
-no simulation past the start); its "Reaction details" block prints, per
-reaction, the requested and actual rate constants and the binding radius
-(rxnsetrate smolreact.c:1364-1410, rxncalcrate :1592-1680).  Stored: the
-configuration texts, the reaction names and the printed actual rates and
-binding radii.
+Seeded random configurations with reactions of surface-bound reactants are
+loaded by oracle/_ref/smoldyn with `-t` (text output, no simulation past the
+start): second-order reactions between a bound reactant (front or back
+state, first or second reactant) and a solution reactant, reversible surface
+binding (`A(front) + B <-> C(front)`, whose reverse is a first-order bound
+reaction with a bound and a solution product) and emission from a bound
+molecule (`A(front) -> A(front) + B`).  Its "Reaction details" block prints,
+per reaction, the requested and actual rate constants, the binding radius
+(second order) and the unbinding radius (two products) (rxnsetrate
+smolreact.c:1307-1410, rxnsetproduct :1431-1577, rxncalcrate :1592-1680).
+Stored: the configuration texts, the reaction names and the printed actual
+rates, binding radii and unbinding radii (NaN where not printed).
 Usage: python tests/golden/make_bound_pair_golden.py   (needs `make -C oracle ref`)
 """
 import os
@@ -20,7 +24,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 REF = os.path.join(ROOT, "oracle", "_ref", "smoldyn")
-NCASE = 24
+NCASE = 32
 
 
 def make_config(rng):
@@ -36,12 +40,18 @@ def make_config(rng):
               "panel rect +0 5 0 0 10 10 r1", "end_surface"]
     names = []
     forms = ["A(front) + B -> C(front)", "B + A(back) -> C", "A(front) + C -> 0", "C + A(front) -> A(front)",
-             "A(back) + B -> C(bsoln)", "A(front) + A -> A(front)"]
+             "A(back) + B -> C(bsoln)", "A(front) + A -> A(front)", "A(front) + B <-> C(front)",
+             "C(front) -> A(front) + B", "A(front) -> A(front) + B", "A(back) -> C(front) + B(bsoln)"]
     pick = rng.choice(len(forms), size=3, replace=False)
     for q, f in enumerate(pick):
         nm = "r%d" % q
-        names.append(nm)
-        lines.append("reaction %s %s %.6g" % (nm, forms[f], 10 ** rng.uniform(-1.5, 0.5)))
+        if "<->" in forms[f]:
+            names += [nm + "fwd", nm + "rev"]
+            lines.append("reaction %s %s %.6g %.6g" % (nm, forms[f], 10 ** rng.uniform(-1.5, 0.5),
+                                                       10 ** rng.uniform(-1.5, 0.5)))
+        else:
+            names.append(nm)
+            lines.append("reaction %s %s %.6g" % (nm, forms[f], 10 ** rng.uniform(-1.5, 0.5)))
     lines.append("end_file")
     return "\n".join(lines) + "\n", names
 
@@ -53,25 +63,33 @@ def run_ref(text):
         out = subprocess.run([REF, "c.txt", "-t"], cwd=d, capture_output=True, text=True, timeout=120,
                              stdin=subprocess.DEVNULL, env=dict(os.environ, SMOLDYN_NO_PROMPT="1")).stdout
     res = {}
-    for m in re.finditer(r"Reaction (\w+):[^\n]*\n\s*requested and actual rate constants : ([^,]+), (\S+)\n"
-                         r"\s*binding radius: (\S+)", out):
-        res[m.group(1)] = (float(m.group(3)), float(m.group(4)))
+    blocks = re.split(r"\n\s*Reaction (?=\w+:)", out)
+    for blk in blocks[1:]:
+        name = blk.split(":", 1)[0]
+        m = re.search(r"requested and actual rate constants : [^,]+, (\S+)", blk)
+        if not m:
+            continue
+        b = re.search(r"\n\s*binding radius: (\S+)", blk)
+        u = re.search(r"\n\s*unbinding radius: (\S+)", blk)
+        res[name] = (float(m.group(1)), float(b.group(1)) if b else float("nan"),
+                     float(u.group(1)) if u else float("nan"))
     return res
 
 
 def main():
     rng = np.random.default_rng(20260611)
-    texts, names, rates, radii = [], [], [], []
+    texts, names, rates, radii, uradii = [], [], [], [], []
     for _ in range(NCASE):
         text, nms = make_config(rng)
         res = run_ref(text)
-        assert set(res) == set(nms), (res, nms, text)
+        assert set(nms) <= set(res), (res, nms, text)
         texts.append(text)
         names.append(",".join(nms))
-        rates.append([res[n][0] for n in nms])
-        radii.append([res[n][1] for n in nms])
+        rates.append([res[n][0] for n in nms] + [np.nan] * (6 - len(nms)))
+        radii.append([res[n][1] for n in nms] + [np.nan] * (6 - len(nms)))
+        uradii.append([res[n][2] for n in nms] + [np.nan] * (6 - len(nms)))
     np.savez(os.path.join(HERE, "bound_pair_params.npz"), texts=np.array(texts), names=np.array(names),
-             rates=np.array(rates), radii=np.array(radii))
+             rates=np.array(rates), radii=np.array(radii), uradii=np.array(uradii))
     print("wrote", NCASE, "cases")
 
 

@@ -20,6 +20,9 @@ changes the species, so `molcount` separates the two sides.
      B(front) -> C(soln) (released into solution), A(front) -> 0;
   7. a capsule: a cylinder with hemisphere caps, neighbours across the rims
      (counts on the body and on the caps);
+  9. reversible surface binding A(front) + B <-> C(front) (the reverse is a
+     first-order bound reaction with a bound and a solution product, placed
+     at the geminate unbinding radius) and emission A(front) -> A(front) + D;
   8. second-order reactions of a bound and a solution reactant, with a
      bound product, a solution product and none; solution molecules behind
      the panel do not react.  The bound molecules sit within one binding
@@ -205,6 +208,59 @@ cmd N 10 molcountincmpt behind outb.txt
 end_file
 """
 
+BIRXN_BACK = HEAD + """species A B C
+difc A(back) 0.2
+difc B 1
+difc C 1
+""" + WALLS + """start_surface plane
+action both all reflect
+panel rect +0 10 0 0 20 20 p1
+end_surface
+reaction r1 A(back) + B -> C(bsoln) 4
+start_compartment behind
+surface plane
+point 5 10 10
+end_compartment
+molecule_lists blist bndlist
+mol_list B blist
+mol_list C blist
+mol_list A(back) bndlist
+surface_mol 1000 A(back) plane rect p1
+mol 4000 B u u u
+output_files out.txt outb.txt
+cmd N 10 molcount out.txt
+cmd N 10 molcountincmpt behind outb.txt
+end_file
+"""
+
+REVBIND = HEAD + """species A B C D
+difc A(front) 0.2
+difc B 1
+difc C(front) 0.1
+difc D 1
+""" + WALLS + """start_surface plane
+action both all reflect
+panel rect +0 10 0 0 20 20 p1
+end_surface
+reaction r1 A(front) + B <-> C(front) 2 1
+reaction e1 A(front) -> A(front) + D 0.2
+start_compartment behind
+surface plane
+point 5 10 10
+end_compartment
+molecule_lists blist bndlist
+mol_list B blist
+mol_list D blist
+mol_list A(front) bndlist
+mol_list C(front) bndlist
+surface_mol 1000 A(front) plane rect p1
+mol 4000 B u u u
+output_files out.txt outb.txt
+cmd N 10 molcount out.txt
+cmd N 10 molcountincmpt behind outb.txt
+end_file
+"""
+
 TRANSMIT = HEAD + """species A B
 difc A 1
 difc B 1
@@ -369,3 +425,30 @@ def test_bound_solution_pair_reactions():
     assert G[-1, 1] < 1800 and G[-1, 3] > 200 and G[:, 4].max() > 3  # A reacted; C formed; D released
     Bk = np.stack([g[1] for g in gpu]).mean(0)
     assert np.all(Bk[:, 2] > 1800)  # B behind the panel (x < 10) does not react
+
+
+def test_bound_solution_pair_reaction_back_state():
+    """A(back) + B -> C(bsoln): the solution reactant is read against the
+    panel's front side (morebireact), the product starts behind the panel."""
+    def on_back(s):
+        pos, sp, st, srf, pnl, sn = s.surface_molecules()
+        assert len(pos) > 100 and np.all(st == sb.MSback) and np.all(pos[:, 0] < 10.0)
+    text = fill(BIRXN_BACK, L=20, T=2.0, dt=0.01)
+    _, gpu = compare(text, ["out.txt", "outb.txt"], [1, 2, 3], "birxn_back", check=on_back)
+    G = np.stack([g[0] for g in gpu]).mean(0)
+    Bk = np.stack([g[1] for g in gpu]).mean(0)
+    assert G[-1, 3] > 50  # C formed
+    assert np.all(np.abs(Bk[:, 3] - G[:, 3]) < 1e-9)  # every C starts (and, reflected, stays) behind
+
+
+def test_reversible_surface_binding_and_emission():
+    def on_plane(s):
+        pos, sp, st, srf, pnl, sn = s.surface_molecules()
+        assert np.all(np.abs(pos[:, 0] - 10.0) < 1e-6) and np.all(pos[:, 0] > 10.0)
+        assert set(sp.tolist()) <= {1, 3} and len(pos) == 1000  # A and C: bound molecules are conserved
+    text = fill(REVBIND, L=20, T=3.0, dt=0.01)
+    _, gpu = compare(text, ["out.txt", "outb.txt"], [1, 2, 3, 4], "revbind", check=on_plane)
+    G = np.stack([g[0] for g in gpu]).mean(0)
+    assert G[-1, 3] > 50 and G[-1, 4] > 300  # complexes formed; D emitted
+    Bk = np.stack([g[1] for g in gpu]).mean(0)
+    assert np.all(Bk[:, 4] < 1e-9)  # D starts in front of the panel and stays there

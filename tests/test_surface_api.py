@@ -10,8 +10,9 @@ on the requested side.  Second-order reactions of a bound and a solution
 reactant: binding radii and effective rates against the values the
 reference binary prints for the same configurations (golden fixture).
 Error paths: an unknown panel, a state the engine does not build, reactions
-with two bound reactants, solution reactants with bound products, and
-bound-reactant reactions with a non-default product placement.
+with two bound reactants, bound reactants with more products than built,
+solution reactants with bound products, and bound-reactant reactions with a
+bounce placement.
 """
 import ctypes as C
 import os
@@ -108,7 +109,7 @@ def test_errors():
     assert lib.smolAddSurfaceMolecules(s.ptr, b"A", sb.MSup, 5, b"membrane", sb.PSrect, b"m1", None) != 0
     assert lib.smolSetSurfaceRate(s.ptr, b"membrane", b"A", sb.MSup, sb.MSup, sb.MSsoln, 1.0, None, 0) != 0
     s.close()
-    for stmt in ("reaction r A(front) + A(back) -> A(front) 1", "reaction r A(front) -> B(front) + B(front) 1",
+    for stmt in ("reaction r A(front) + A(back) -> A(front) 1", "reaction r A(front) -> B(front) + B(front) + B 1",
                  "reaction r A -> B(front) 1", "reaction r A(front) + B -> A(front) 1\nproduct_placement r bounce -2",
                  "reaction r A(front) + B -> A(front) + B 1"):
         d = tempfile.mkdtemp()
@@ -121,24 +122,32 @@ def test_errors():
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "bound_pair_params.npz")
 
 
-def test_bound_solution_reaction_parameters_match_reference():
-    """Binding radius and effective rate of A(front) + B style reactions: the
-    rate doubles for one surface and one solution reactant and the bound
-    state's diffusion coefficient counts (smolreact.c:1371-1377); the
-    reference prints both to six significant digits."""
+def test_bound_reaction_parameters_match_reference():
+    """Reactions of surface-bound reactants: A(front) + B style reactions
+    (the rate doubles for one surface and one solution reactant and the bound
+    state's diffusion coefficient counts, smolreact.c:1371-1377), reversible
+    surface binding (the reverse found with states, the default pgemmaxw
+    placement, the unbinding radius from the products' state diffusion
+    coefficients) and emission from a bound molecule: actual rate, binding
+    radius and unbinding radius as the reference prints them (six digits)."""
     z = np.load(GOLDEN)
     d = tempfile.mkdtemp()
-    for text, names, rates, radii in zip(z["texts"], z["names"], z["rates"], z["radii"]):
+    nchecked = 0
+    for text, names, rates, radii, uradii in zip(z["texts"], z["names"], z["rates"], z["radii"], z["uradii"]):
         path = os.path.join(d, "c.txt")
         with open(path, "w") as f:
             f.write(str(text))
         s = sb.Sim.load_file(path)
-        for nm, rate, rad in zip(str(names).split(","), rates, radii):
-            b, _, _ = s.reaction_params(nm)
-            k, _ = s.effective_rate(nm)
-            assert abs(b - rad) <= 2e-5 * rad + 1e-9, (nm, b, rad, str(text))
-            assert abs(k - rate) <= 2e-5 * rate + 1e-9, (nm, k, rate, str(text))
+        for k, nm in enumerate(str(names).split(",")):
+            b, u, _ = s.reaction_params(nm)
+            rate, _ = s.effective_rate(nm)
+            for got, want in ((rate, rates[k]), (b, radii[k]), (u, uradii[k])):
+                if np.isnan(want):
+                    continue
+                assert abs(got - want) <= 2e-5 * abs(want) + 1e-9, (nm, got, want, str(text))
+                nchecked += 1
         s.close()
+    assert nchecked > 150
 
 
 def test_add_reaction_with_states_through_the_c_api():
