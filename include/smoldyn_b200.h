@@ -178,8 +178,9 @@ enum ErrorCode smolAddCompartmentPoint(simptr sim, const char *compartment, doub
 enum ErrorCode smolAddCompartmentLogic(simptr sim, const char *compartment, enum CmptLogic logic,
                                        const char *compartment2);
 enum ErrorCode smolAddCompartmentMolecules(simptr sim, const char *species, int number, const char *compartment);
-/* surface must be NULL: surface-restricted reactions need surface-bound
- * molecules, which the engine does not model. */
+/* A surface restriction applies to reactions of surface-bound reactants
+ * (they fire only for molecules bound to that surface); for other reactions
+ * it is refused. */
 enum ErrorCode smolSetReactionRegion(simptr sim, const char *reaction, const char *compartment, const char *surface);
 
 /* libsmoldyn.h:152-158 */

@@ -1112,7 +1112,6 @@ enum ErrorCode smolAddCompartmentMolecules(simptr sim, const char *species, int 
 
 enum ErrorCode smolSetReactionRegion(simptr sim, const char *reaction, const char *compartment, const char *surface) {
   LCHECK(sim && reaction, ECmissing, "missing argument");
-  LCHECK(!surface, ECbounds, "surface-restricted reactions are not supported by the GPU engine");
   Sim &s = sim->s;
   int o = 0;
   const int r = s.reaction_index(reaction, &o);
@@ -1122,6 +1121,14 @@ enum ErrorCode smolSetReactionRegion(simptr sim, const char *reaction, const cha
     c = s.compartment_index(compartment);
     LCHECK(c >= 0, ECnonexist, "compartment not found");
   }
+  int sf = -1;
+  if (surface) {
+    for (size_t k = 0; k < s.surfaces.size(); ++k)
+      if (s.surfaces[k].name == surface) sf = (int)k;
+    LCHECK(sf >= 0, ECnonexist, "surface not found");
+  }
+  std::string err;
+  if (smolb::set_reaction_surface(s, s.rxn[o][r], sf, &err)) return set_error(__func__, ECbounds, err);
   s.rxn[o][r].cmpt = c;
   s.need_update = s.need_rebuild = true;
   return ECok;

@@ -127,6 +127,7 @@ struct DevNet {
   float bounce_k[kMaxRxn];   // bounce scaling: 1 (given unbinding radius) or 2 (from the binding radius)
   int ncmpt;
   uint8_t cmpt[3][kMaxRxn];  // compartment of each reaction + 1 (0: anywhere)
+  uint8_t rsrf[3][kMaxRxn];  // surface of each reaction + 1 (0: any); only reactions of bound reactants
   // surface-bound states (single simulations)
   int bound;                       // 1: surface rules and bound molecules in use
   double beps, bmargin, bneighdist; // surfacessstruct epsilon, margin, neighdist for bound molecules

@@ -755,10 +755,27 @@ __device__ int bound_first_order(const KParams &p, BoundMol &m, int &sp, ull ske
   const int nr = c_net.buni_n[sp][st];
   if (!nr) return 0;
   const uint32_t u = srf_draw(skey, step, kCtrSrfRxn).x;
-  int r = -1;
-  for (int k = 0; k < nr; ++k)
-    if (u < c_net.bthr[sp][st][k]) { r = c_net.buni_list[sp][st][k]; break; }
-  if (r < 0) return 0;
+  const uint32_t *thr = c_net.bthr[sp][st];
+  int k = 0;
+  while (k < nr && !(u < thr[k])) ++k;
+  // A reaction restricted to a surface or a compartment fires only on that
+  // surface or inside it (unireact smolreact.c:3040-3050); otherwise the
+  // decision passes to the reactions after it in the list, each with its own
+  // coin: with a fresh uniform, the first k' > k with
+  // u' < 1 - (1 - cum_k') / (1 - cum_k), as for solution molecules.
+  for (int round = 0; k < nr; ++round) {
+    const int rk = c_net.buni_list[sp][st][k];
+    const int rs = c_net.rsrf[1][rk], cm = c_net.cmpt[1][rk];
+    if ((!rs || c_panels[m.pnl].srf == rs - 1) && (!cm || pos_in_cmpt(c_cmpt, cm - 1, c_panels, m.x))) break;
+    const double uu = ((double)srf_draw(skey, step, kCtrSrfRxn + 0x10u + (uint32_t)round).x + 0.5) * (1.0 / 4294967296.0);
+    const double rest = 1.0 - (double)thr[k] * (1.0 / 4294967296.0);
+    int next = nr;
+    for (int k2 = k + 1; k2 < nr; ++k2)
+      if (rest > 0 && uu < 1.0 - (1.0 - (double)thr[k2] * (1.0 / 4294967296.0)) / rest) { next = k2; break; }
+    k = next;
+  }
+  if (k >= nr) return 0;
+  const int r = c_net.buni_list[sp][st][k];
   atomicAdd(&p.counters[2], 1ull);
   const int np = min((int)c_net.nprod[1][r], 2);
   if (np == 0) return 1;
@@ -1420,7 +1437,8 @@ __global__ void k_bound_species_count(const BoundMol *m, const int *n, long long
 // molecule lies within the binding radius of the bound one, on the front side
 // of the bound one's panel (a solution reactant's state is read from the
 // side of that panel, :3134-3137), inside the reaction's compartment if it
-// has one, and the reaction's coin passes; of a pair's reactions the first in
+// has one, on its surface if it is restricted to one, and the reaction's coin
+// passes; of a pair's reactions the first in
 // list order that passes is taken.  The reference takes pairs in the order of
 // its molecule lists, which has nothing to do with geometry; here every pair
 // gets a random priority (a hash of both identities and the step) and the
@@ -1547,6 +1565,8 @@ __global__ void __launch_bounds__(256) k_bpair_claim(KParams p, int round) {
           const int cm = c_net.cmpt[2][r];
           if (cm && !(pos_in_cmpt(c_cmpt, cm - 1, c_panels, xs) && pos_in_cmpt(c_cmpt, cm - 1, c_panels, m.x)))
             continue;
+          const int rs = c_net.rsrf[2][r];
+          if (rs && pn.srf != rs - 1) continue;  // restricted to another surface (morebireact :3116)
           best = pkey;
           bj = j;
           be = e;
@@ -4651,7 +4671,10 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
   for (const CmptSpec &cs : E.net.cmpts) E.cmpts.push_back(make_dev_cmpt(cs, reps[0].lo));
   E.dnet.ncmpt = (int)E.cmpts.size();
   for (int o = 0; o < 3; ++o)
-    for (int r = 0; r < kMaxRxn; ++r) E.dnet.cmpt[o][r] = (uint8_t)E.net.cmpt[o][r];
+    for (int r = 0; r < kMaxRxn; ++r) {
+      E.dnet.cmpt[o][r] = (uint8_t)E.net.cmpt[o][r];
+      E.dnet.rsrf[o][r] = (uint8_t)E.net.rsrf[o][r];
+    }
   int rc = E.build_box_masks(err);
   if (rc) return rc;
   rc = E.build_rep_tables(err);

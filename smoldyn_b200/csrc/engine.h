@@ -92,6 +92,7 @@ struct NetSpec {
   std::vector<PanelSpec> panels;
   std::vector<CmptSpec> cmpts;
   int cmpt[3][kMaxRxn] = {};                 // compartment of each reaction + 1 (0: none)
+  int rsrf[3][kMaxRxn] = {};                 // surface of each reaction + 1 (0: none)
   // first-order reactions of surface-bound reactants: reactant state (0 soln,
   // 1 front, 2 back) and product state (0 soln, 1 front, 2 back, 5 bsoln)
   int rstate1[kMaxRxn] = {};

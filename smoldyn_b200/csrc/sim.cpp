@@ -617,6 +617,7 @@ int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err) {
       for (int q = 0; q < x.nprod; ++q)
         for (int d = 0; d < 3; ++d) rep->prdpos[o][r][q][d] = x.prdpos[q][d];
       net->cmpt[o][r] = x.cmpt >= 0 ? x.cmpt + 1 : 0;
+      net->rsrf[o][r] = x.srf >= 0 ? x.srf + 1 : 0;
       if (o == 0) rep->birth_mean[r] = x.prob;
       if (o == 1) rep->uni_prob[r] = x.prob;
       if (o == 2) {
@@ -696,6 +697,22 @@ static int species_arg(Sim &sim, const std::string &w, std::vector<int> *out) {
   const int i = sim.species_index(name);
   if (i < 0) return -3;
   out->push_back(i);
+  return 0;
+}
+
+// Restrict reaction x to surface sf (rxn->srf: it fires only where a reactant
+// is bound to that surface, smolreact.c:3048, :3093, :3116).  Built for
+// reactions of a surface-bound reactant; elsewhere refused.
+int set_reaction_surface(Sim &sim, RxnDef &x, int sf, std::string *err) {
+  (void)sim;
+  if (sf < 0) { x.srf = -1; return 0; }
+  bool bound = false;
+  for (int q = 0; q < x.order; ++q) bound = bound || x.rstate[q] != 0;
+  if (!bound) {
+    if (err) *err = "reaction " + x.name + ": a surface restriction is built for reactions of surface-bound reactants";
+    return -7;
+  }
+  x.srf = sf;
   return 0;
 }
 
@@ -966,15 +983,25 @@ int read_config_statement(Sim &sim, const std::string &word, const std::string &
     compartment_random_positions(sim, c, n, &sim.pend_pos);
     for (long long k = 0; k < n; ++k) sim.pend_sp.push_back(i);
     sim.need_rebuild = true;
-  } else if (word == "reaction" || word == "reaction_cmpt") {
-    // reaction_cmpt cname ... (deprecated form) or reaction cmpt=cname ...
-    // (smolreact.c:2436-2470)
+  } else if (word == "reaction" || word == "reaction_cmpt" || word == "reaction_surface") {
+    // reaction_cmpt cname ... / reaction_surface sname ... (deprecated forms)
+    // or reaction cmpt=cname ... / reaction srf=sname ... (smolreact.c:2436-2490)
     std::vector<std::string> ww = w;
-    int c = -1;
+    int c = -1, sf = -1;
+    auto surface_index = [&](const std::string &nm) {
+      for (size_t k = 0; k < sim.surfaces.size(); ++k)
+        if (sim.surfaces[k].name == nm) return (int)k;
+      return -1;
+    };
     if (word == "reaction_cmpt") {
       if (ww.empty()) { if (err) *err = "reaction_cmpt: missing compartment"; return -7; }
       c = sim.compartment_index(ww[0]);
       if (c < 0) { if (err) *err = "compartment name not recognized"; return -3; }
+      ww.erase(ww.begin());
+    } else if (word == "reaction_surface") {
+      if (ww.empty()) { if (err) *err = "reaction_surface: missing surface"; return -7; }
+      sf = surface_index(ww[0]);
+      if (sf < 0) { if (err) *err = "surface " + ww[0] + " not recognized"; return -3; }
       ww.erase(ww.begin());
     }
     while (!ww.empty() && ww[0].find('=') != std::string::npos) {
@@ -982,6 +1009,9 @@ int read_config_statement(Sim &sim, const std::string &word, const std::string &
       if (key == "cmpt" || key == "compartment") {
         c = sim.compartment_index(val);
         if (c < 0) { if (err) *err = "compartment name not recognized"; return -3; }
+      } else if (key == "srf" || key == "surface") {
+        sf = surface_index(val);
+        if (sf < 0) { if (err) *err = "surface " + val + " not recognized"; return -3; }
       } else {
         if (err) *err = "reaction restriction not supported by the GPU engine: " + ww[0];
         return -7;
@@ -992,7 +1022,13 @@ int read_config_statement(Sim &sim, const std::string &word, const std::string &
     const int rc = add_reaction_from_words(sim, ww, err);
     if (rc) return rc;
     for (int o = 0; o < 3; ++o)
-      for (size_t r = before[o]; r < sim.rxn[o].size(); ++r) sim.rxn[o][r].cmpt = c;
+      for (size_t r = before[o]; r < sim.rxn[o].size(); ++r) {
+        RxnDef &x = sim.rxn[o][r];
+        x.cmpt = c;
+        if (sf >= 0) {
+          if (const int e = set_reaction_surface(sim, x, sf, err)) return e;
+        }
+      }
     return 0;
   } else if (word == "reaction_rate") {
     if (!need(2)) return -7;

@@ -32,6 +32,7 @@ struct RxnDef {
   int pstate[kMaxProd] = {0, 0, 0, 0};  // product states (0 soln, 1 front, 2 back, 5 bsoln)
   double rate = -1;         // requested rate constant; <0 undefined
   int cmpt = -1;            // compartment the reaction is restricted to (rxn->cmpt), -1 none
+  int srf = -1;             // surface the reaction is restricted to (rxn->srf), -1 none
   int rparamt = 0;          // RevParam
   double rparam = 0;
   double user_prdpos[kMaxProd][3] = {};  // for offset / fixed placement
@@ -202,6 +203,9 @@ int derive_reaction_params(Sim &sim, std::string *err);
 // Append reaction x (order, reactants, products and their states set) after
 // checking the states the engine builds; 0 or an error code with *err set.
 int add_reaction_def(Sim &sim, const RxnDef &x, std::string *err);
+// Restrict reaction x to surface sf (-1 lifts it); built for reactions of
+// surface-bound reactants.
+int set_reaction_surface(Sim &sim, RxnDef &x, int sf, std::string *err);
 // rxncalcrate (smolreact.c:1592-1680): effective rate from derived parameters.
 double calc_rate(const Sim &sim, int order, int r, double *pgem);
 // surfupdateparams (smolsurface.c:3735-3800): derived probabilities of every

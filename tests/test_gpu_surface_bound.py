@@ -23,6 +23,8 @@ changes the species, so `molcount` separates the two sides.
   9. reversible surface binding A(front) + B <-> C(front) (the reverse is a
      first-order bound reaction with a bound and a solution product, placed
      at the geminate unbinding radius) and emission A(front) -> A(front) + D;
+  10. reactions restricted to a surface (`srf=`, `reaction_surface`): a
+     first-order and a bound-solution reaction, each on one of two planes;
   8. second-order reactions of a bound and a solution reactant, with a
      bound product, a solution product and none; solution molecules behind
      the panel do not react.  The bound molecules sit within one binding
@@ -261,6 +263,33 @@ cmd N 10 molcountincmpt behind outb.txt
 end_file
 """
 
+SRFRXN = HEAD + """species A B C
+difc A(front) 0.1
+difc B(front) 0.1
+difc C 1
+""" + WALLS + """start_surface s1
+action both all reflect
+panel rect +0 6 0 0 20 20 p1
+end_surface
+start_surface s2
+action both all reflect
+panel rect +0 14 0 0 20 20 p2
+end_surface
+reaction srf=s1 r1 A(front) -> B(front) 1
+reaction_surface s2 r2 A(front) + C -> A(front) 2
+molecule_lists blist bndlist
+mol_list C blist
+mol_list A(front) bndlist
+mol_list B(front) bndlist
+surface_mol 1000 A(front) s1 rect p1
+surface_mol 1000 A(front) s2 rect p2
+mol 3000 C u u u
+output_files out.txt out1.txt
+cmd N 10 molcount out.txt
+cmd N 10 molcountonsurf s1 out1.txt
+end_file
+"""
+
 TRANSMIT = HEAD + """species A B
 difc A 1
 difc B 1
@@ -452,3 +481,15 @@ def test_reversible_surface_binding_and_emission():
     assert G[-1, 3] > 50 and G[-1, 4] > 300  # complexes formed; D emitted
     Bk = np.stack([g[1] for g in gpu]).mean(0)
     assert np.all(Bk[:, 4] < 1e-9)  # D starts in front of the panel and stays there
+
+
+def test_surface_restricted_reactions():
+    def per_surface(s):
+        pos, sp, st, srf, pnl, sn = s.surface_molecules()
+        assert np.all(sp[srf == 2] == 1)  # A(front) on s2 does not convert (r1 is restricted to s1)
+    text = fill(SRFRXN, L=20, T=2.0, dt=0.01)
+    _, gpu = compare(text, ["out.txt", "out1.txt"], [1, 2, 3], "srfrxn", check=per_surface)
+    G = np.stack([g[0] for g in gpu]).mean(0)
+    t, b = G[:, 0], np.stack([g[1][:, 2] for g in gpu]).mean(0)  # B(front) on s1
+    assert np.all(np.abs(b - 1000 * (1 - np.exp(-t))) < 40)  # only the 1000 molecules on s1 convert
+    assert G[-1, 3] < 2950  # C reacts at s2

@@ -175,3 +175,29 @@ def test_add_reaction_with_states_through_the_c_api():
                                C.cast(states, C.POINTER(C.c_int)), 1.0) != 0
     a.close()
     b.close()
+
+
+def test_surface_restricted_reactions_parse_and_refuse():
+    """srf= / reaction_surface / smolSetReactionRegion(surface): built for
+    reactions of bound reactants, refused for solution reactions and unknown
+    surfaces."""
+    lib = sb.load()
+    ok = TEXT.replace("end_file", "reaction srf=membrane r1 A(front) -> B(front) 1\n"
+                                  "reaction_surface membrane r2 A(front) + B -> A(front) 1\nend_file")
+    d = tempfile.mkdtemp()
+    with open(os.path.join(d, "c.txt"), "w") as f:
+        f.write(ok)
+    s = sb.Sim.load_file(os.path.join(d, "c.txt"))
+    assert lib.smolSetReactionRegion(s.ptr, b"r1", None, b"membrane") == 0
+    assert lib.smolSetReactionRegion(s.ptr, b"r1", None, b"nope") != 0
+    s.close()
+    for stmt in ("reaction srf=membrane r A -> B 1", "reaction srf=nope r A(front) -> B(front) 1",
+                 "reaction_surface membrane r A + B -> A 1"):
+        with open(os.path.join(d, "c.txt"), "w") as f:
+            f.write(TEXT.replace("end_file", stmt + "\nend_file"))
+        with pytest.raises(RuntimeError):
+            sb.Sim.load_file(os.path.join(d, "c.txt"))
+    b = from_api()
+    assert lib.smolAddReaction(b.ptr, b"rs", b"B", sb.MSsoln, None, sb.MSsoln, 0, None, None, 1.0) == 0
+    assert lib.smolSetReactionRegion(b.ptr, b"rs", None, b"membrane") != 0
+    b.close()
