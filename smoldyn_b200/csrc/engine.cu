@@ -712,7 +712,7 @@ __device__ int bound_coin(const KParams &p, BoundMol &m, int &sp, ull skey, uint
   return 0;
 }
 
-__device__ __forceinline__ void random_rotation(uint4 r, float m[9]);
+__device__ __forceinline__ void random_orientation(uint4 r, int dim, float m[9]);
 __device__ __forceinline__ void push_bound(const KParams &p, const BoundMol &m);
 
 // Place product q of first-order reaction r of bound molecule m (doreact,
@@ -781,7 +781,7 @@ __device__ int bound_first_order(const KParams &p, BoundMol &m, int &sp, ull ske
   if (np == 0) return 1;
   float R[9];
   const bool rot = c_net.has_offset[1][r] != 0;
-  if (rot) random_rotation(srf_draw(skey, step, kCtrSrfRot), R);
+  if (rot) random_orientation(srf_draw(skey, step, kCtrSrfRot), c_geo0.dim, R);
   int q0 = 0;  // the product that takes over the reactant's entry
   for (int q = np - 1; q >= 0; --q)
     if (c_net.pstate1[r][q] == kMSfront || c_net.pstate1[r][q] == kMSback) q0 = q;
@@ -1366,9 +1366,10 @@ __global__ void __launch_bounds__(256) k_bound(KParams p) {
     if (ds > 0) {
       const uint4 r = srf_draw(skey, step, kCtrSrfDiff);
       const uint32_t gm = c_net.gmask;
+      const int dim = c_geo0.dim;  // in 2-D the panels are lines and circles in the plane
       m.x[0] += ds * (double)p.gtab[r.x & gm];
-      m.x[1] += ds * (double)p.gtab[r.y & gm];
-      m.x[2] += ds * (double)p.gtab[r.z & gm];
+      if (dim > 1) m.x[1] += ds * (double)p.gtab[r.y & gm];
+      if (dim > 2) m.x[2] += ds * (double)p.gtab[r.z & gm];
       move_to_close_panel(m.x, posx, m.pnl, m.ms, skey, step);
       dead = walk_bound(p, m, sp, posx, pnlx, hits, skey, step) == 1;
     }
@@ -2608,6 +2609,26 @@ __device__ __forceinline__ void random_rotation(uint4 r, float m[9]) {
   m[6] = 2.f * (qx * qz - qy * qw); m[7] = 2.f * (qy * qz + qx * qw); m[8] = 1.f - 2.f * (qx * qx + qy * qy);
 }
 
+// The random orientation of a reaction's product offsets in the system's
+// dimension (doreact smolreact.c:2840-2851): a uniformly random rotation in
+// 3-D, a rotation by a uniform angle in the plane in 2-D (DirCosM2D), and a
+// random sign in 1-D, so the offsets keep their length.
+__device__ __forceinline__ void random_orientation(uint4 r, int dim, float m[9]) {
+  if (dim >= 3) {
+    random_rotation(r, m);
+    return;
+  }
+  for (int k = 0; k < 9; ++k) m[k] = (k % 4 == 0) ? 1.f : 0.f;
+  if (dim == 2) {
+    float sn, cs;
+    __sincosf(u01f_open(r.x) * 6.28318530718f, &sn, &cs);
+    m[0] = cs; m[1] = -sn;
+    m[3] = sn; m[4] = cs;
+  } else {
+    m[0] = (r.x & 1u) ? 1.f : -1.f;
+  }
+}
+
 // Birth position in compartment c (compartrandpos, smolcomparts.c:194-220):
 // uniform points in the system until one lies in the compartment, at most
 // 10000 tries, then one of its interior points.  site/cell hold the first
@@ -2732,7 +2753,7 @@ __device__ __forceinline__ void place_event(const KParams &p, const Event &e, ui
   float m[9];
   bool rot = false;
   if (!place && c_net.has_offset[order][r] && !c_net.fixed[order][r] && !c_net.inject) {
-    random_rotation(philox(make_uint4((uint32_t)e.key, (uint32_t)(e.key >> 32), step, 8u), key), m);
+    random_orientation(philox(make_uint4((uint32_t)e.key, (uint32_t)(e.key >> 32), step, 8u), key), g.dim, m);
     rot = true;
   }
   const int kx = c_net.rxn_base[order] + r;

@@ -462,8 +462,12 @@ std::string new_panel_name(const SurfaceDef &sf, int shape, const std::string &g
 
 namespace {
 
-double panel_area(const PanelSpec &p) {
+// panelarea: area in 3-D, length in 2-D (a rectangle is a segment, a
+// sphere a circle), 1 in 1-D
+double panel_area(const PanelSpec &p, int dim) {
   const double pi = 3.14159265358979323846;
+  if (dim == 1) return 1.0;
+  if (dim == 2) return p.shape == 2 ? 2 * pi * p.radius : std::fabs(p.hi[1 - p.axis] - p.lo[1 - p.axis]);
   switch (p.shape) {
     case 0: {
       double a = 1;
@@ -516,6 +520,13 @@ void panel_rand_pos(Sim &sim, const PanelSpec &p, double x[3]) {
     }
     case 2:
     case 4: {
+      if (sim.dim == 2) {  // a circle in the plane
+        const double ph = 2 * pi * sim.rand_u01();
+        x[0] = p.center[0] + p.radius * std::cos(ph);
+        x[1] = p.center[1] + p.radius * std::sin(ph);
+        x[2] = 0;
+        return;
+      }
       const double z = 2 * sim.rand_u01() - 1, ph = 2 * pi * sim.rand_u01(), s = std::sqrt(std::max(0.0, 1 - z * z));
       double u[3] = {s * std::cos(ph), s * std::sin(ph), z};
       if (p.shape == 4 && u[0] * p.normal[0] + u[1] * p.normal[1] + u[2] * p.normal[2] > 0)
@@ -556,7 +567,7 @@ int add_surface_molecules(Sim &sim, long long n, int sp, int ms, int srf, int sh
       if (pnl >= 0 && q != pnl) continue;
       if (shape >= 0 && shape < 6 && sf.panels[q].shape != shape) continue;
       cand.push_back({s, q});
-      area.push_back(panel_area(sf.panels[q]));
+      area.push_back(panel_area(sf.panels[q], sim.dim));
     }
   }
   if (cand.empty()) { if (err) *err = "in surface_mol, no panels match the given description"; return -3; }

@@ -1,5 +1,7 @@
 """More behaviour against reference ensembles: absorbing walls, zeroth-order
-births with first-order decay, branching first-order reactions, drift.
+births with first-order decay, branching first-order reactions, drift, and
+reversible A + B <-> C in one and two dimensions (the products' unbinding
+offsets take a random sign in 1-D and a random in-plane angle in 2-D).
 
 Each case runs the same text configuration through the reference binary
 (oracle/_ref/smoldyn, 32 seeds in parallel, molcount at the end) and through
@@ -24,7 +26,7 @@ pytestmark = pytest.mark.gpu
 REF_EXE = os.path.join(oracle_lib.REF_DIR, "smoldyn")
 SEEDS, NREP = 32, 48
 
-HEAD = """dim 3
+HEAD = """dim {dim}
 species A B C
 difc A 1
 difc B 0.5
@@ -58,12 +60,24 @@ reaction toA C -> A 0.2
 reaction toB C -> B 0.1
 mol 5000 C u u u
 """),
+    # reversible binding in the plane and on a line (default pgemmaxw placement)
+    "reversible_2d": dict(steps=300, dim=2, init=[("A", 1500), ("B", 1500)], body="""boundaries 0 0 40 r
+boundaries 1 0 40 r
+reaction fwd A + B <-> C 5 0.5
+mol 1500 A u u
+mol 1500 B u u
+"""),
+    "reversible_1d": dict(steps=300, dim=1, init=[("A", 400), ("B", 400)], body="""boundaries 0 0 200 r
+reaction fwd A + B <-> C 2 0.5
+mol 400 A u
+mol 400 B u
+"""),
 }
 
 
 def config(case, seed, out):
     c = CASES[case]
-    return (HEAD.format(tstop=c["steps"] * 0.01, seed=seed) + c["body"] +
+    return (HEAD.format(dim=c.get("dim", 3), tstop=c["steps"] * 0.01, seed=seed) + c["body"] +
             "output_files %s\ncmd a molcount %s\nend_file\n" % (out, out))
 
 
@@ -94,9 +108,9 @@ def engine_counts(case):
         assert lib.smolLoadSimFromFile((d + "/").encode(), b"c.txt", C.byref(simp), b"") == 0, sb.last_error()
     t = sb.Sim(ptr=simp.value)
     e = sb.Ensemble(t, NREP)
-    init = {"absorbing_walls": ("A", 2000), "branching": ("C", 5000)}.get(case)
-    if init:
-        e.add_molecules(init[0], np.full(NREP, init[1]))
+    init = {"absorbing_walls": [("A", 2000)], "branching": [("C", 5000)]}.get(case, CASES[case].get("init", []))
+    for sp, n in init:
+        e.add_molecules(sp, np.full(NREP, n))
     e.update()
     e.run_steps(CASES[case]["steps"])
     return e.counts(4)[:, 1:4].astype(float)

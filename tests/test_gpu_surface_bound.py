@@ -25,6 +25,8 @@ changes the species, so `molcount` separates the two sides.
      at the geminate unbinding radius) and emission A(front) -> A(front) + D;
   10. reactions restricted to a surface (`srf=`, `reaction_surface`): a
      first-order and a bound-solution reaction, each on one of two planes;
+  11. the same in two dimensions: adsorption and desorption on a circle,
+     diffusion along it, reversible binding (products offset in the plane);
   8. second-order reactions of a bound and a solution reactant, with a
      bound product, a solution product and none; solution molecules behind
      the panel do not react.  The bound molecules sit within one binding
@@ -290,6 +292,46 @@ cmd N 10 molcountonsurf s1 out1.txt
 end_file
 """
 
+PLANAR = """dim 2
+boundaries 0 0 100
+boundaries 1 0 100
+time_start 0
+time_stop {T}
+time_step {dt}
+random_seed {seed}
+species A B C
+difc A 3
+difc A(front) 0.5
+difc B 1
+difc C(front) 0.2
+start_surface walls
+action both all reflect
+panel rect +0 0 0 100
+panel rect -0 100 0 100
+panel rect +1 0 0 100
+panel rect -1 0 100 100
+end_surface
+start_surface stick
+action both all reflect
+rate A fsoln front 1
+rate A front fsoln 0.2
+panel sph 50 50 20 40
+end_surface
+reaction r1 A(front) + B <-> C(front) 20 0.5
+molecule_lists blist bndlist
+mol_list A blist
+mol_list B blist
+mol_list A(front) bndlist
+mol_list C(front) bndlist
+mol 1000 A u u
+mol 1000 B u u
+surface_mol 300 A(front) stick all all
+output_files out.txt outs.txt
+cmd N 20 molcount out.txt
+cmd N 20 molcountonsurf stick outs.txt
+end_file
+"""
+
 TRANSMIT = HEAD + """species A B
 difc A 1
 difc B 1
@@ -493,3 +535,14 @@ def test_surface_restricted_reactions():
     t, b = G[:, 0], np.stack([g[1][:, 2] for g in gpu]).mean(0)  # B(front) on s1
     assert np.all(np.abs(b - 1000 * (1 - np.exp(-t))) < 40)  # only the 1000 molecules on s1 convert
     assert G[-1, 3] < 2950  # C reacts at s2
+
+
+def test_planar_bound_states():
+    def on_circle(s):
+        pos, sp, st, srf, pnl, sn = s.surface_molecules()
+        r = np.hypot(pos[:, 0] - 50.0, pos[:, 1] - 50.0)
+        assert len(pos) > 100 and np.all(np.abs(r - 20.0) < 1e-6) and np.all(pos[:, 2] == 0)
+    text = fill(PLANAR, T=4.0, dt=0.01)
+    _, gpu = compare(text, ["out.txt", "outs.txt"], [1, 2, 3], "planar", check=on_circle)
+    G = np.stack([g[1] for g in gpu]).mean(0)
+    assert G[-1, 3] > 20  # complexes on the circle
