@@ -127,7 +127,9 @@ struct DevNet {
   float bounce_k[kMaxRxn];   // bounce scaling: 1 (given unbinding radius) or 2 (from the binding radius)
   int ncmpt;
   uint8_t cmpt[3][kMaxRxn];  // compartment of each reaction + 1 (0: anywhere)
-  uint8_t rsrf[3][kMaxRxn];  // surface of each reaction + 1 (0: any); only reactions of bound reactants
+  uint8_t rsrf[3][kMaxRxn];  // surface of each reaction + 1 (0: any): births on it (order 0), or bound reactants
+  uint8_t pstate0[kMaxRxn][kMaxProd];  // product states of order-0 reactions (births on a surface)
+  double parea[kMaxPanels];  // area of each panel (length in 2-D), for births on a surface
   // surface-bound states (single simulations)
   int bound;                       // 1: surface rules and bound molecules in use
   double beps, bmargin, bneighdist; // surfacessstruct epsilon, margin, neighdist for bound molecules

@@ -2671,6 +2671,9 @@ __device__ __noinline__ void birth_in_cmpt(int c, const DevGeo &g, ull ekey, uin
 // smolreact.c:2905-2995): positions from the event site, the unbinding
 // offsets under one random rotation per event (or the confspread / bounce
 // placements), walls and surfaces for the new molecules, serial numbers.
+template <int SURF, class Emit>
+__device__ void surface_birth(const KParams &p, const Event &e, int r, int rep, uint32_t step, Emit emit);
+
 // emit(position, identity) stores one new molecule.  uni counts the
 // first-order events.
 template <int SURF, class Emit>
@@ -2681,6 +2684,10 @@ __device__ __forceinline__ void place_event(const KParams &p, const Event &e, ui
   const uint4 rr = philox(make_uint4((uint32_t)e.key, (uint32_t)(e.key >> 32), step, 7u), key);
   float site[3];
   int cell[3];
+  if (SURF && order == 0 && c_net.rsrf[0][r]) {  // births on a surface
+    surface_birth<SURF>(p, e, r, rep, step, emit);
+    return;
+  }
   if (order == 0) {  // uniform position in the system (smolwall.c:42)
     const uint32_t bits[3] = {rr.x, rr.y, rr.z};
     for (int d = 0; d < 3; ++d) {
@@ -2822,6 +2829,126 @@ __device__ __forceinline__ void place_event(const KParams &p, const Event &e, ui
     if (hits) atomicAdd(&p.counters[0], (unsigned long long)hits);
     if (dead) continue;
     emit(make_float4(w[0], w[1], w[2], __uint_as_float(pack_cell(c[0], c[1], c[2]))), make_id(fsp, rep, serno));
+  }
+}
+
+// A uniformly random point of a panel (panelrandpos, smolsurface.c), from
+// three uniforms: a rectangle's extent, a triangle by the square-root rule, a
+// sphere's surface (a circle in 2-D), a cylinder's side, the closed side of
+// a hemisphere, a disk by the square-root rule.
+__device__ void panel_random_point(const DevPanel &pn, int dim, uint32_t a, uint32_t b, uint32_t c, double x[3]) {
+  const double u1 = u01co(a), u2 = u01co(b), u3 = u01co(c), tau = 6.283185307179586;
+  auto basis = [&](const double n[3], double e1[3], double e2[3]) {  // two unit vectors perpendicular to n
+    const double t[3] = {fabs(n[0]) < 0.9 ? 1.0 : 0.0, fabs(n[0]) < 0.9 ? 0.0 : 1.0, 0.0};
+    e1[0] = t[1] * n[2] - t[2] * n[1];
+    e1[1] = t[2] * n[0] - t[0] * n[2];
+    e1[2] = t[0] * n[1] - t[1] * n[0];
+    const double l = sqrt(dot3(e1, e1));
+    for (int d = 0; d < 3; ++d) e1[d] /= l;
+    e2[0] = n[1] * e1[2] - n[2] * e1[1];
+    e2[1] = n[2] * e1[0] - n[0] * e1[2];
+    e2[2] = n[0] * e1[1] - n[1] * e1[0];
+  };
+  switch (pn.shape) {
+    case 0: {
+      const double us[3] = {u1, u2, u3};
+      for (int d = 0; d < 3; ++d) x[d] = d == pn.axis ? pn.pos : pn.lo[d] + us[d] * (pn.hi[d] - pn.lo[d]);
+      return;
+    }
+    case 1: {
+      const double r1 = sqrt(u1);
+      for (int d = 0; d < 3; ++d) x[d] = (1 - r1) * pn.pt[0][d] + r1 * (1 - u2) * pn.pt[1][d] + r1 * u2 * pn.pt[2][d];
+      return;
+    }
+    case 2:
+    case 4: {
+      if (dim == 2) {
+        x[0] = pn.center[0] + pn.radius * cos(tau * u1);
+        x[1] = pn.center[1] + pn.radius * sin(tau * u1);
+        x[2] = 0;
+        return;
+      }
+      const double z = 2 * u1 - 1, s = sqrt(fmax(0.0, 1 - z * z));
+      double v[3] = {s * cos(tau * u2), s * sin(tau * u2), z};
+      if (pn.shape == 4 && dot3(v, pn.nrm) > 0)
+        for (int d = 0; d < 3; ++d) v[d] = -v[d];
+      for (int d = 0; d < 3; ++d) x[d] = pn.center[d] + pn.radius * v[d];
+      return;
+    }
+    case 3: {
+      double e1[3], e2[3];
+      basis(pn.nrm, e1, e2);
+      for (int d = 0; d < 3; ++d)
+        x[d] = pn.pt[0][d] + u1 * (pn.pt[1][d] - pn.pt[0][d]) +
+               pn.radius * (cos(tau * u2) * e1[d] + sin(tau * u2) * e2[d]);
+      return;
+    }
+    default: {
+      double e1[3], e2[3];
+      basis(pn.nrm, e1, e2);
+      const double rr = pn.radius * sqrt(u1);
+      for (int d = 0; d < 3; ++d) x[d] = pn.center[d] + rr * (cos(tau * u2) * e1[d] + sin(tau * u2) * e2[d]);
+      return;
+    }
+  }
+}
+
+// Births of an order-0 reaction restricted to a surface (zeroreact,
+// smolreact.c:2949-2992, surfrandpos): a panel of the surface chosen by area,
+// a uniform point of it, and the products there (doreact with the panel):
+// bound products on the panel on their state's side (into the output bound
+// list), solution products just off its front (soln) or back (bsoln) side.
+template <int SURF, class Emit>
+__device__ void surface_birth(const KParams &p, const Event &e, int r, int rep, uint32_t step, Emit emit) {
+  const DevGeo g = p.geo[rep];
+  const int s = c_net.rsrf[0][r] - 1;
+  const uint2 key = make_uint2(c_net.key0 ^ 0x3C6EF372u, c_net.key1 ^ 0xA54FF53Au);
+  const uint4 rr = philox(make_uint4((uint32_t)e.key, (uint32_t)(e.key >> 32), step, 9u), key);
+  double total = 0;
+  for (int q = 0; q < c_net.npanel; ++q)
+    if (c_panels[q].srf == s) total += c_net.parea[q];
+  double u = u01co(rr.x) * total;
+  int pk = -1;
+  for (int q = 0; q < c_net.npanel; ++q) {
+    if (c_panels[q].srf != s) continue;
+    pk = q;
+    if (u < c_net.parea[q]) break;
+    u -= c_net.parea[q];
+  }
+  if (pk < 0) return;
+  const DevPanel &pn = c_panels[pk];
+  double x0[3];
+  panel_random_point(pn, g.dim, rr.y, rr.z, rr.w, x0);
+  const int np = c_net.nprod[0][r];
+  for (int q = 0; q < np; ++q) {
+    const int psp = c_net.prd[0][r][q], pst = c_net.pstate0[r][q];
+    const ull serno = kProductSernoBit |
+                      (mix64(e.key ^ ((ull)q << 50) ^ ((ull)step << 20) ^ (ull)r) & (kProductSernoBit - 1));
+    double x[3] = {x0[0], x0[1], x0[2]};
+    if (pst == kMSfront || pst == kMSback) {
+      if (SURF == 3) {
+        fix_to_panel(pn, x, ms_face(pst), c_net.beps);
+        BoundMol bm;
+        for (int d = 0; d < 3; ++d) bm.x[d] = x[d];
+        bm.id = make_id(psp, 0, serno);
+        bm.pnl = pk;
+        bm.ms = pst;
+        push_bound(p, bm);
+        atomicAdd((unsigned long long *)&p.spcount[psp], 1ull);
+      }
+      continue;
+    }
+    const int f = pst == kMSbsoln ? kFaceBack : kFaceFront;
+    fix_to_panel(pn, x, f, c_net.beps);
+    double n[3];
+    face_normal(pn, x, f, n);
+    const double sd = fabs(panel_sdist<true>(pn, x));
+    if (sd < c_net.surf_eps)  // kept surf_eps off the panel, as solution molecules are
+      for (int d = 0; d < 3; ++d) x[d] += (c_net.surf_eps - sd) * n[d];
+    int c[3];
+    float w[3];
+    from_abs(g, x, c, w);
+    emit(make_float4(w[0], w[1], w[2], __uint_as_float(pack_cell(c[0], c[1], c[2]))), make_id(psp, rep, serno));
   }
 }
 
@@ -4695,7 +4822,10 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
     for (int r = 0; r < kMaxRxn; ++r) {
       E.dnet.cmpt[o][r] = (uint8_t)E.net.cmpt[o][r];
       E.dnet.rsrf[o][r] = (uint8_t)E.net.rsrf[o][r];
+      if (o == 0)
+        for (int q = 0; q < kMaxProd; ++q) E.dnet.pstate0[r][q] = (uint8_t)E.net.pstate0[r][q];
     }
+  for (int k = 0; k < kMaxPanels; ++k) E.dnet.parea[k] = E.net.panel_area[k];
   int rc = E.build_box_masks(err);
   if (rc) return rc;
   rc = E.build_rep_tables(err);

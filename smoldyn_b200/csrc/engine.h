@@ -93,6 +93,8 @@ struct NetSpec {
   std::vector<CmptSpec> cmpts;
   int cmpt[3][kMaxRxn] = {};                 // compartment of each reaction + 1 (0: none)
   int rsrf[3][kMaxRxn] = {};                 // surface of each reaction + 1 (0: none)
+  int pstate0[kMaxRxn][kMaxProd] = {};       // product states of order-0 reactions (surface births)
+  double panel_area[kMaxPanels] = {};        // area (2-D: length) of each engine panel
   // first-order reactions of surface-bound reactants: reactant state (0 soln,
   // 1 front, 2 back) and product state (0 soln, 1 front, 2 back, 5 bsoln)
   int rstate1[kMaxRxn] = {};

@@ -134,7 +134,10 @@ int derive_reaction_params(Sim &sim, std::string *err) {
   for (RxnDef &x : sim.rxn[0]) {
     if (x.disabled) { x.prob = 0; continue; }
     if (x.rate < 0) { if (err) *err = "reaction " + x.name + " rate is undefined"; return -8; }
-    x.prob = x.rate * dt * (x.cmpt >= 0 ? compartment_volume(sim, x.cmpt) : system_volume(sim));
+    // births per step: rate x dt x the compartment's volume, the surface's
+    // area or the system's volume (smolreact.c:1325-1330)
+    x.prob = x.rate * dt * (x.cmpt >= 0 ? compartment_volume(sim, x.cmpt)
+                            : x.srf >= 0 ? surface_area(sim, x.srf) : system_volume(sim));
   }
   // order 1
   for (size_t r = 0; r < sim.rxn[1].size(); ++r) {
@@ -381,7 +384,8 @@ double calc_rate(const Sim &sim, int order, int r, double *pgem) {
   const double dt = sim.dt;
   double ans = 0;
   if (order == 0) {
-    const double vol = x.cmpt >= 0 ? (x.cmpt < (int)sim.cmpts.size() ? sim.cmpts[x.cmpt].volume : 0) : system_volume(sim);
+    const double vol = x.cmpt >= 0 ? (x.cmpt < (int)sim.cmpts.size() ? sim.cmpts[x.cmpt].volume : 0)
+                       : x.srf >= 0 ? surface_area(sim, x.srf) : system_volume(sim);
     ans = x.prob < 0 || !(vol > 0) ? 0 : x.prob / dt / vol;
   } else if (order == 1) {
     if (x.prob > 0) {
@@ -591,6 +595,8 @@ int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err) {
       net->nprod[o][r] = x.nprod;
       for (int q = 0; q < x.nprod; ++q) net->prd[o][r][q] = x.prd[q];
       net->fixed_placement[o][r] = (x.rparamt == RP_fixed) ? 1 : 0;
+      if (o == 0)
+        for (int q = 0; q < kMaxProd; ++q) net->pstate0[r][q] = q < x.nprod ? x.pstate[q] : 0;
       if (o == 1) {
         net->rstate1[r] = x.rstate[0];
         for (int q = 0; q < 2; ++q) net->pstate1[r][q] = q < x.nprod ? x.pstate[q] : 0;
@@ -659,6 +665,7 @@ int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err) {
       ps.trans_back_mask = sf.trans_back;
       ps.refl_front_mask = sf.refl_front;
       ps.refl_back_mask = sf.refl_back;
+      if (net->panels.size() < (size_t)kMaxPanels) net->panel_area[net->panels.size()] = panel_area_dim(ps, sim.dim);
       net->panels.push_back(ps);
     }
   const std::vector<int> first = surface_panel_base(sim);
@@ -705,11 +712,20 @@ static int species_arg(Sim &sim, const std::string &w, std::vector<int> *out) {
 // reactions of a surface-bound reactant; elsewhere refused.
 int set_reaction_surface(Sim &sim, RxnDef &x, int sf, std::string *err) {
   (void)sim;
-  if (sf < 0) { x.srf = -1; return 0; }
-  bool bound = false;
+  bool bound = false, bprod = false;
   for (int q = 0; q < x.order; ++q) bound = bound || x.rstate[q] != 0;
-  if (!bound) {
-    if (err) *err = "reaction " + x.name + ": a surface restriction is built for reactions of surface-bound reactants";
+  for (int q = 0; q < x.nprod; ++q) bprod = bprod || x.pstate[q] != 0;
+  if (sf < 0) {
+    if (x.order == 0 && bprod) {
+      if (err) *err = "enter a surface for order 0 reactions with surface-bound products";
+      return -7;
+    }
+    x.srf = -1;
+    return 0;
+  }
+  if (!bound && x.order != 0) {
+    if (err) *err = "reaction " + x.name + ": a surface restriction is built for order 0 reactions and reactions "
+                    "of surface-bound reactants";
     return -7;
   }
   x.srf = sf;
@@ -739,8 +755,8 @@ int add_reaction_def(Sim &sim, const RxnDef &x, std::string *err) {
                     "or second order with one solution reactant and at most one product";
     return -7;
   }
-  if (!bound && bprod) {
-    if (err) *err = "products in surface states need a surface-bound reactant";
+  if (!bound && bprod && !(x.order == 0 && x.srf >= 0)) {
+    if (err) *err = "products in surface states need a surface-bound reactant, or a surface for order 0 reactions";
     return -7;
   }
   if ((int)sim.rxn[x.order].size() >= kMaxRxn) { if (err) *err = "too many reactions"; return -6; }
@@ -748,7 +764,7 @@ int add_reaction_def(Sim &sim, const RxnDef &x, std::string *err) {
   return 0;
 }
 
-static int add_reaction_from_words(Sim &sim, const std::vector<std::string> &w, std::string *err) {
+static int add_reaction_from_words(Sim &sim, const std::vector<std::string> &w, std::string *err, int srf = -1) {
   // reaction [name] r1 [+ r2] -> p1 [+ p2 ...] [rate]
   if (w.size() < 3) { if (err) *err = "reaction: too few words"; return -7; }
   size_t k = 0;
@@ -818,6 +834,7 @@ static int add_reaction_from_words(Sim &sim, const std::vector<std::string> &w, 
       x.pstate[q] = st;
     }
     x.rate = rate;
+    x.srf = srf;
     return add_reaction_def(sim, x, err);
   };
   int rc = mk(reversible ? name + "fwd" : name, rct, prd, rates.empty() ? -1 : rates[0]);
@@ -1019,7 +1036,7 @@ int read_config_statement(Sim &sim, const std::string &word, const std::string &
       ww.erase(ww.begin());
     }
     size_t before[3] = {sim.rxn[0].size(), sim.rxn[1].size(), sim.rxn[2].size()};
-    const int rc = add_reaction_from_words(sim, ww, err);
+    const int rc = add_reaction_from_words(sim, ww, err, sf);
     if (rc) return rc;
     for (int o = 0; o < 3; ++o)
       for (size_t r = before[o]; r < sim.rxn[o].size(); ++r) {

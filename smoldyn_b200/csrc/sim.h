@@ -206,6 +206,9 @@ int add_reaction_def(Sim &sim, const RxnDef &x, std::string *err);
 // Restrict reaction x to surface sf (-1 lifts it); built for reactions of
 // surface-bound reactants.
 int set_reaction_surface(Sim &sim, RxnDef &x, int sf, std::string *err);
+// Area of surface s (length in 2-D; surfacearea).
+double surface_area(const Sim &sim, int s);
+double panel_area_dim(const PanelSpec &p, int dim);
 // rxncalcrate (smolreact.c:1592-1680): effective rate from derived parameters.
 double calc_rate(const Sim &sim, int order, int r, double *pgem);
 // surfupdateparams (smolsurface.c:3735-3800): derived probabilities of every

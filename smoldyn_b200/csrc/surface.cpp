@@ -292,6 +292,13 @@ int derive_surface_params(Sim &sim, std::string *err) {
 
 bool surface_bound_mode(const Sim &sim) {
   if (!sim.pend_bound.empty()) return true;
+  for (int o = 0; o < 3; ++o)  // reactions of bound reactants or with bound products
+    for (const RxnDef &x : sim.rxn[o]) {
+      for (int q = 0; q < x.order; ++q)
+        if (x.rstate[q] != 0) return true;
+      for (int q = 0; q < x.nprod; ++q)
+        if (x.pstate[q] == MSfront || x.pstate[q] == MSback) return true;
+    }
   for (const SurfaceDef &sf : sim.surfaces)
     for (size_t i = 1; i < sim.species.size() && i < (size_t)kMaxSpecies; ++i)
       for (int ms = 0; ms < kSrfStates; ++ms)
@@ -553,6 +560,15 @@ void panel_rand_pos(Sim &sim, const PanelSpec &p, double x[3]) {
 }
 
 }  // namespace
+
+double panel_area_dim(const PanelSpec &p, int dim) { return panel_area(p, dim); }
+
+double surface_area(const Sim &sim, int s) {
+  double a = 0;
+  if (s < 0 || s >= (int)sim.surfaces.size()) return 0;
+  for (const PanelSpec &p : sim.surfaces[s].panels) a += panel_area(p, sim.dim);
+  return a;
+}
 
 int add_surface_molecules(Sim &sim, long long n, int sp, int ms, int srf, int shape, int pnl, const double *pos,
                           std::string *err) {

@@ -27,6 +27,8 @@ changes the species, so `molcount` separates the two sides.
      first-order and a bound-solution reaction, each on one of two planes;
   11. the same in two dimensions: adsorption and desorption on a circle,
      diffusion along it, reversible binding (products offset in the plane);
+  12. births on a surface (order 0 restricted to a surface): bound products
+     placed by area on a sphere, solution products on its back (inner) side;
   8. second-order reactions of a bound and a solution reactant, with a
      bound product, a solution product and none; solution molecules behind
      the panel do not react.  The bound molecules sit within one binding
@@ -332,6 +334,26 @@ cmd N 20 molcountonsurf stick outs.txt
 end_file
 """
 
+SRFBIRTH = HEAD + """species A B
+difc A(front) 0.2
+difc B 1
+""" + WALLS + """start_surface ball
+action both all reflect
+panel sph 10 10 10 4 20 20 s1
+end_surface
+start_compartment inside
+surface ball
+point 10 10 10
+end_compartment
+reaction srf=ball g 0 -> A(front) 2
+reaction_surface ball h 0 -> B(bsoln) 1
+reaction decay A(front) -> 0 0.5
+output_files out.txt outi.txt
+cmd N 10 molcount out.txt
+cmd N 10 molcountincmpt inside outi.txt
+end_file
+"""
+
 TRANSMIT = HEAD + """species A B
 difc A 1
 difc B 1
@@ -546,3 +568,18 @@ def test_planar_bound_states():
     _, gpu = compare(text, ["out.txt", "outs.txt"], [1, 2, 3], "planar", check=on_circle)
     G = np.stack([g[1] for g in gpu]).mean(0)
     assert G[-1, 3] > 20  # complexes on the circle
+
+
+def test_births_on_a_surface():
+    def on_sphere(s):
+        pos, sp, st, srf, pnl, sn = s.surface_molecules()
+        r = np.linalg.norm(pos - 10.0, axis=1)
+        assert len(pos) > 100 and np.all(np.abs(r - 4.0) < 1e-6)
+        assert np.abs((pos - 10.0).mean(0)).max() < 1.0  # spread over the sphere
+    text = fill(SRFBIRTH, L=20, T=3.0, dt=0.01)
+    _, gpu = compare(text, ["out.txt", "outi.txt"], [1, 2], "srfbirth", check=on_sphere)
+    G = np.stack([g[0] for g in gpu]).mean(0)
+    t, a = G[:, 0], G[:, 1]
+    area = 4 * np.pi * 16
+    # births at 2 per unit area and time, decay at 0.5: A(t) = 4 area (1 - exp(-t/2))
+    assert np.all(np.abs(a - 4 * area * (1 - np.exp(-0.5 * t))) < 30), (a, 4 * area * (1 - np.exp(-0.5 * t)))

@@ -201,3 +201,20 @@ def test_surface_restricted_reactions_parse_and_refuse():
     assert lib.smolAddReaction(b.ptr, b"rs", b"B", sb.MSsoln, None, sb.MSsoln, 0, None, None, 1.0) == 0
     assert lib.smolSetReactionRegion(b.ptr, b"rs", None, b"membrane") != 0
     b.close()
+
+
+def test_births_on_a_surface_parse():
+    """Order-0 reactions on a surface: births per step are rate x dt x the
+    surface's area (smolreact.c:1328); bound products need the surface."""
+    ok = TEXT.replace("end_file", "reaction srf=membrane b0 0 -> A(front) 0.5\nend_file")
+    d = tempfile.mkdtemp()
+    with open(os.path.join(d, "c.txt"), "w") as f:
+        f.write(ok)
+    s = sb.Sim.load_file(os.path.join(d, "c.txt"))
+    assert abs(s.reaction_params("b0")[2] - 0.5 * 0.01 * 200.0) < 1e-12  # two 10 x 10 panels
+    assert abs(s.effective_rate("b0")[0] - 0.5) < 1e-12
+    s.close()
+    with open(os.path.join(d, "c.txt"), "w") as f:
+        f.write(TEXT.replace("end_file", "reaction b0 0 -> A(front) 0.5\nend_file"))
+    with pytest.raises(RuntimeError):
+        sb.Sim.load_file(os.path.join(d, "c.txt"))
