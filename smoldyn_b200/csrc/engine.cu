@@ -2684,7 +2684,7 @@ __device__ __forceinline__ void place_event(const KParams &p, const Event &e, ui
   const uint4 rr = philox(make_uint4((uint32_t)e.key, (uint32_t)(e.key >> 32), step, 7u), key);
   float site[3];
   int cell[3];
-  if (SURF && order == 0 && c_net.rsrf[0][r]) {  // births on a surface
+  if (SURF && order == 0 && c_net.rsrf[0][r] && !c_net.cmpt[0][r]) {  // births on a surface (a compartment wins)
     surface_birth<SURF>(p, e, r, rep, step, emit);
     return;
   }

@@ -122,7 +122,12 @@ def test_api_builds_the_same_compartment():
     assert lib.smolAddCompartmentMolecules(s.ptr, b"A", 500, b"in") == 0
     s.add_reaction("birth", None, None, ["A"], 2.0)
     assert lib.smolSetReactionRegion(s.ptr, b"birth", b"out", None) == 0
-    assert lib.smolSetReactionRegion(s.ptr, b"birth", b"out", b"ball") < 0
+    # a surface too: the compartment takes precedence for births (zeroreact
+    # smolreact.c:2949-2992); a surface restriction of a solution reaction of
+    # order 1 is refused
+    assert lib.smolSetReactionRegion(s.ptr, b"birth", b"out", b"ball") == 0
+    s.add_reaction("decay", "A", None, [], 1.0)
+    assert lib.smolSetReactionRegion(s.ptr, b"decay", None, b"ball") < 0
     _, _, prob = s.reaction_params("birth")
     assert abs(prob / (2.0 * 0.01) / (8000 - 4 / 3 * np.pi * 216) - 1) < 0.02
     s.close()
