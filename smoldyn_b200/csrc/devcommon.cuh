@@ -149,6 +149,13 @@ struct DevNet {
   uint8_t bpair_rxn[kMaxRxn], bpair_bsp[kMaxRxn], bpair_bst[kMaxRxn], bpair_ssp[kMaxRxn], bpair_pst[kMaxRxn];
   uint32_t bpair_mask[kMaxSpecies][2];
   float bpair_rmax;  // largest binding radius of these reactions, padded as the stencil radii are
+  // second-order reactions of two bound reactants (same panel), in list
+  // order: the reaction, both reactants' species and states, the product's
+  // state; per bound (species, front/back) the bound species it reacts with
+  int bb_n;
+  uint8_t bb_rxn[kMaxRxn], bb_sp[kMaxRxn][2], bb_st[kMaxRxn][2], bb_pst[kMaxRxn];
+  uint32_t bb_mask[kMaxSpecies][2];
+  float bb_rmax;
 };
 
 // A molecule bound to a panel: absolute position (relative to the system's

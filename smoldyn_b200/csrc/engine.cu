@@ -100,6 +100,12 @@ struct KParams {
   // candidate (partner, reaction, squared distance bits, state)
   ull *bclaim;
   int4 *bcand;
+  // bound-bound pair reactions: hash-grid heads, per bound molecule the next
+  // entry of its bucket, its box, and its best partner (priority << 32 | index)
+  int *bbhead;
+  int *bbnext;
+  int *bbcell;
+  ull *bbbest;
 };
 
 constexpr uint32_t kTmpGone = 0xFFFFFFFFu;  // tmp[i].w of a molecule that left
@@ -1681,6 +1687,234 @@ __global__ void __launch_bounds__(256) k_bpair_resolve(KParams p) {
     }
   }
   if (done) atomicAdd(&p.counters[3], (unsigned long long)done);
+}
+
+// ---- bound-bound pair reactions ----------------------------------------------
+// Second-order reactions of two surface-bound reactants (bireact with both
+// molecules in a bound state, morebireact smolreact.c:3109-3157: molecules on
+// different panels do not react, the product takes the diffusion-weighted
+// place on their panel, doreact :2690-2706).  The bound molecules with such a
+// reaction go into a hash grid of their boxes (a bucket head per hashed box,
+// linked through the molecules); each round every molecule finds, in the
+// boxes its largest binding radius reaches, its partner of lowest random
+// priority (a symmetric hash of both identities and the step) among those on
+// its panel within the binding radius whose coin passes; mutual choices react
+// (the lower index carries the reaction out), and the others look again, for
+// kBPairRounds rounds.  A kernel at the end empties the buckets it used.
+constexpr int kBBHashBits = 20;
+constexpr ull kBBReacted = ~0ull - 1;  // bbbest of a molecule that reacted this step
+
+__device__ __forceinline__ int bb_bucket(int cell) { return (int)(((uint32_t)cell * 2654435761u) >> (32 - kBBHashBits)); }
+
+__device__ __forceinline__ bool bb_candidate(const KParams &p, int k) {
+  const BoundMol &m = p.bd_out[k];
+  const int sp = id_species(m.id);
+  if (sp == kDeadSpecies || !c_net.bb_mask[sp][m.ms - 1]) return false;
+  // an entry that reacted with a solution molecule this step holds a product
+  if (c_net.bpair_n && p.bcand[k].x >= 0 && p.bcand[k].w == 1) return false;
+  return true;
+}
+
+__global__ void __launch_bounds__(256) k_bb_insert(KParams p) {
+  pdl_launch_dependents();
+  pdl_wait();
+  const int nb = min(*p.bd_out_n, p.bcap);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nb; k += gridDim.x * blockDim.x) {
+    p.bbbest[k] = ~0ull;
+    if (!bb_candidate(p, k)) {
+      p.bbcell[k] = -1;
+      continue;
+    }
+    int ix[3];
+    float u[3];
+    from_abs(c_geo0, p.bd_out[k].x, ix, u);
+    const int cell = (ix[2] * c_geo0.n[1] + ix[1]) * c_geo0.n[0] + ix[0];
+    p.bbcell[k] = cell;
+    p.bbnext[k] = atomicExch(&p.bbhead[bb_bucket(cell)], k);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_bb_best(KParams p) {
+  pdl_launch_dependents();
+  pdl_wait();
+  const int nb = min(*p.bd_out_n, p.bcap);
+  const uint32_t step = *p.step;
+  const DevGeo &g = c_geo0;
+  const uint2 key = make_uint2(c_net.key0 ^ 0x2F8A6B1Du, c_net.key1 ^ 0x5C4E9A37u);
+  const float rmax = c_net.bb_rmax;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nb; k += gridDim.x * blockDim.x) {
+    if (p.bbcell[k] < 0 || p.bbbest[k] == kBBReacted) continue;
+    const BoundMol m = p.bd_out[k];
+    const int sp = id_species(m.id);
+    const uint32_t mask = c_net.bb_mask[sp][m.ms - 1];
+    const ull kk = id_stream(m.id);
+    int ix[3];
+    float u[3];
+    from_abs(g, m.x, ix, u);
+    ull best = ~0ull;
+    for (int q = 0; q < 27; ++q) {
+      const int off[3] = {q % 3 - 1, (q / 3) % 3 - 1, q / 9 - 1};
+      int cc[3];
+      bool ok = true;
+      for (int d = 0; d < 3; ++d) {
+        if (d >= g.dim && off[d] != 0) ok = false;
+        const float ub = (ix[d] == g.n[d] - 1) ? g.whi[d] : g.h[d];
+        if (off[d] < 0 && !(u[d] < rmax)) ok = false;
+        if (off[d] > 0 && !(u[d] > ub - rmax)) ok = false;
+        cc[d] = ix[d] + off[d];
+        if (cc[d] < 0 || cc[d] >= g.n[d]) ok = false;  // bound molecules do not meet across periodic walls
+      }
+      if (!ok) continue;
+      const int cell = (cc[2] * g.n[1] + cc[1]) * g.n[0] + cc[0];
+      for (int j = p.bbhead[bb_bucket(cell)]; j >= 0; j = p.bbnext[j]) {
+        if (j == k || p.bbcell[j] != cell || p.bbbest[j] == kBBReacted) continue;
+        const BoundMol mj = p.bd_out[j];
+        const int sj = id_species(mj.id);
+        if (mj.pnl != m.pnl || !((mask >> sj) & 1u)) continue;
+        const double d2 = (mj.x[0] - m.x[0]) * (mj.x[0] - m.x[0]) + (mj.x[1] - m.x[1]) * (mj.x[1] - m.x[1]) +
+                          (mj.x[2] - m.x[2]) * (mj.x[2] - m.x[2]);
+        const ull kj = id_stream(mj.id);
+        const ull lo = kk < kj ? kk : kj, hi = kk < kj ? kj : kk;  // symmetric in the pair
+        const ull pk = mix64((lo * 0x9E3779B97F4A7C15ull ^ hi) + (ull)step * 0xD1B54A32D192ED03ull);
+        const ull key2 = (pk & 0xFFFFFFFF00000000ull) | (uint32_t)j;
+        if (key2 >= best) continue;
+        for (int e = 0; e < c_net.bb_n; ++e) {
+          const bool fw = c_net.bb_sp[e][0] == sp && c_net.bb_st[e][0] == m.ms && c_net.bb_sp[e][1] == sj &&
+                          c_net.bb_st[e][1] == mj.ms;
+          const bool bw = c_net.bb_sp[e][1] == sp && c_net.bb_st[e][1] == m.ms && c_net.bb_sp[e][0] == sj &&
+                          c_net.bb_st[e][0] == mj.ms;
+          if (!fw && !bw) continue;
+          const int r = c_net.bb_rxn[e];
+          if (d2 > (double)p.bind2[r]) continue;
+          const float prob = p.pairprob[r];
+          if (prob < 1.f) {
+            const ull h = mix64(lo * 0x9E3779B97F4A7C15ull ^ hi);
+            const uint4 rr = philox(make_uint4((uint32_t)h, (uint32_t)(h >> 32), step, (uint32_t)e), key);
+            if (!(u01co(rr.x) < (double)prob)) continue;
+          }
+          const int cm = c_net.cmpt[2][r], rs = c_net.rsrf[2][r];
+          if (cm && !(pos_in_cmpt(c_cmpt, cm - 1, c_panels, m.x) && pos_in_cmpt(c_cmpt, cm - 1, c_panels, mj.x)))
+            continue;
+          if (rs && c_panels[m.pnl].srf != rs - 1) continue;
+          best = key2;
+          break;
+        }
+      }
+    }
+    p.bbbest[k] = best;
+  }
+}
+
+// The reaction of one mutual pair (k the lower index): its first reaction in
+// list order that passed, found again from the pair's species and states.
+__global__ void __launch_bounds__(256) k_bb_resolve(KParams p) {
+  pdl_launch_dependents();
+  pdl_wait();
+  const int nb = min(*p.bd_out_n, p.bcap);
+  const uint32_t step = *p.step;
+  int done = 0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nb; k += gridDim.x * blockDim.x) {
+    if (p.bbcell[k] < 0) continue;
+    const ull bk = p.bbbest[k];
+    if (bk == ~0ull || bk == kBBReacted) continue;
+    const int j = (int)(uint32_t)bk;
+    if (j <= k) continue;
+    const ull bj = p.bbbest[j];
+    if (bj == kBBReacted || (int)(uint32_t)bj != k) continue;
+    // mutual: k reacts with j
+    BoundMol m = p.bd_out[k];
+    const BoundMol mj = p.bd_out[j];
+    const int sp = id_species(m.id), sj = id_species(mj.id);
+    const double d2 = (mj.x[0] - m.x[0]) * (mj.x[0] - m.x[0]) + (mj.x[1] - m.x[1]) * (mj.x[1] - m.x[1]) +
+                      (mj.x[2] - m.x[2]) * (mj.x[2] - m.x[2]);
+    const ull kk = id_stream(m.id), kj = id_stream(mj.id);
+    const ull lo = kk < kj ? kk : kj, hi = kk < kj ? kj : kk;
+    const uint2 key = make_uint2(c_net.key0 ^ 0x2F8A6B1Du, c_net.key1 ^ 0x5C4E9A37u);
+    int e = 0;
+    for (; e < c_net.bb_n; ++e) {  // the same tests as the search, in the same order
+      const bool fw = c_net.bb_sp[e][0] == sp && c_net.bb_st[e][0] == m.ms && c_net.bb_sp[e][1] == sj &&
+                      c_net.bb_st[e][1] == mj.ms;
+      const bool bw = c_net.bb_sp[e][1] == sp && c_net.bb_st[e][1] == m.ms && c_net.bb_sp[e][0] == sj &&
+                      c_net.bb_st[e][0] == mj.ms;
+      if (!fw && !bw) continue;
+      const int r = c_net.bb_rxn[e];
+      if (d2 > (double)p.bind2[r]) continue;
+      const float prob = p.pairprob[r];
+      if (prob < 1.f) {
+        const ull h = mix64(lo * 0x9E3779B97F4A7C15ull ^ hi);
+        const uint4 rr = philox(make_uint4((uint32_t)h, (uint32_t)(h >> 32), step, (uint32_t)e), key);
+        if (!(u01co(rr.x) < (double)prob)) continue;
+      }
+      const int cm = c_net.cmpt[2][r], rs = c_net.rsrf[2][r];
+      if (cm && !(pos_in_cmpt(c_cmpt, cm - 1, c_panels, m.x) && pos_in_cmpt(c_cmpt, cm - 1, c_panels, mj.x)))
+        continue;
+      if (rs && c_panels[m.pnl].srf != rs - 1) continue;
+      break;
+    }
+    if (e >= c_net.bb_n) continue;  // cannot happen: the search found this pair
+    p.bbbest[k] = kBBReacted;
+    p.bbbest[j] = kBBReacted;
+    done++;
+    atomicAdd((unsigned long long *)&p.spcount[sp], (unsigned long long)(-1ll));
+    atomicAdd((unsigned long long *)&p.spcount[sj], (unsigned long long)(-1ll));
+    p.bd_out[j].id = id_mark_dead(mj.id);
+    const int r = c_net.bb_rxn[e];
+    if (c_net.nprod[2][r] == 0) {
+      p.bd_out[k].id = id_mark_dead(m.id);
+      continue;
+    }
+    const int psp = c_net.prd[2][r][0], pst = c_net.bb_pst[e];
+    const double sa = c_net.bstep[sp][m.ms - 1], sb = c_net.bstep[sj][mj.ms - 1];
+    const double da = sa * sa, db = sb * sb;  // proportional to the diffusion coefficients
+    const double f = (da == 0 && db == 0) ? 0.5 : db / (da + db);  // weight of molecule k
+    double x[3];
+    for (int d = 0; d < 3; ++d) x[d] = f * m.x[d] + (1.0 - f) * mj.x[d];
+    int pnl = m.pnl;
+    const ull skey = mix64(kk ^ kCtrBProd) & ((1ull << kSpShift) - 1);
+    atomicAdd((unsigned long long *)&p.spcount[psp], 1ull);
+    if (pst == kMSfront || pst == kMSback) {
+      fix_to_panel(c_panels[pnl], x, ms_face(pst), c_net.beps);
+      const double x0[3] = {x[0], x[1], x[2]};
+      move_to_close_panel(x, x0, pnl, pst, skey, step);
+      for (int d = 0; d < 3; ++d) m.x[d] = x[d];
+      m.pnl = pnl;
+      m.ms = pst;
+      m.id = make_id(psp, 0, id_serno(m.id));
+      p.bd_out[k] = m;
+      continue;
+    }
+    p.bd_out[k].id = id_mark_dead(m.id);
+    const int face = pst == kMSbsoln ? kFaceBack : kFaceFront;
+    fix_to_panel(c_panels[pnl], x, face, c_net.beps);
+    const double x0[3] = {x[0], x[1], x[2]};
+    move_to_close_panel(x, x0, pnl, face == kFaceBack ? kMSback : kMSfront, skey, step);
+    const DevPanel &pn = c_panels[pnl];
+    double nrm[3];
+    face_normal(pn, x, face, nrm);
+    const double sd = fabs(panel_sdist<true>(pn, x));
+    if (sd < c_net.surf_eps)
+      for (int d = 0; d < 3; ++d) x[d] += (c_net.surf_eps - sd) * nrm[d];
+    int ix[3];
+    float w[3];
+    from_abs(c_geo0, x, ix, w);
+    const int slot = atomicAdd(p.q_n, 1);
+    if (slot < p.pcap) {
+      p.q_pc[slot] = make_float4(w[0], w[1], w[2], __uint_as_float(pack_cell(ix[0], ix[1], ix[2])));
+      p.q_id[slot] = make_id(psp, 0, id_serno(m.id));
+    } else {
+      atomicOr(p.status, kStProdCap);
+    }
+  }
+  if (done) atomicAdd(&p.counters[3], (unsigned long long)done);
+}
+
+// Empty the hash-grid buckets used this step (all ones between steps).
+__global__ void __launch_bounds__(256) k_bb_clear(KParams p) {
+  pdl_launch_dependents();
+  pdl_wait();
+  const int nb = min(*p.bd_out_n, p.bcap);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nb; k += gridDim.x * blockDim.x)
+    if (p.bbcell[k] >= 0) p.bbhead[bb_bucket(p.bbcell[k])] = -1;
 }
 
 // Scatter pass: a pure permutation of the moved molecules into box order.
@@ -3588,6 +3822,8 @@ class EngineImpl {
   long long bcap = 0;
   ull *d_bclaim = nullptr;  // bound-solution pair reactions: claim word per sorted molecule
   int4 *d_bcand = nullptr;  // and candidate per bound molecule
+  int *d_bbhead = nullptr, *d_bbnext = nullptr, *d_bbcell = nullptr;  // bound-bound reactions: hash grid
+  ull *d_bbbest = nullptr;
   SrfRule *d_srfrule = nullptr;
 
   // persistent ensemble engine (k_persist): its own molecule layout, one
@@ -3721,12 +3957,14 @@ class EngineImpl {
     void *ptrs[] = {d_boxmask, d_difm, d_rsearch, d_geo, d_difstep, d_driftdt, d_bind2, d_pairprob, d_prdpos, d_gtab, d_unithr,
                     d_births, d_pc[0], d_pc[1], d_ppc[0], d_ppc[1], d_id[0], d_id[1], d_pid[0],
                     d_pid[1], d_face, d_tmp, d_counts, d_step, d_cnt, d_start, d_scan_ticket, d_scan_status, d_ev, d_cand, d_best,
-                    d_counters, d_spcount, d_injkey, d_injval, d_bd[0], d_bd[1], d_srfrule, d_bclaim, d_bcand};
+                    d_counters, d_spcount, d_injkey, d_injval, d_bd[0], d_bd[1], d_srfrule, d_bclaim, d_bcand, d_bbhead, d_bbnext, d_bbcell, d_bbbest};
     for (void *q : ptrs)
       if (q) cudaFree(q);
     d_bd[0] = d_bd[1] = nullptr;
     d_bclaim = nullptr;
     d_bcand = nullptr;
+    d_bbhead = d_bbnext = d_bbcell = nullptr;
+    d_bbbest = nullptr;
     d_srfrule = nullptr;
     bcap = 0;
     d_rsearch = nullptr;
@@ -3795,6 +4033,10 @@ class EngineImpl {
       p.bcap = (int)bcap;
       p.bclaim = d_bclaim;
       p.bcand = d_bcand;
+      p.bbhead = d_bbhead;
+      p.bbnext = d_bbnext;
+      p.bbcell = d_bbcell;
+      p.bbbest = d_bbbest;
     }
     return p;
   }
@@ -4084,6 +4326,18 @@ class EngineImpl {
         mark("k_bpair_resolve");
       }
     }
+    if (SURF == 3 && dnet.bb_n) {
+      launch(k_bb_insert, grid_small(), 256, 0, p);
+      mark("k_bb_insert");
+      for (int round = 0; round < kBPairRounds; ++round) {
+        launch(k_bb_best, grid_small(), 256, 0, p);
+        mark("k_bb_best");
+        launch(k_bb_resolve, grid_small(), 256, 0, p);
+        mark("k_bb_resolve");
+      }
+      launch(k_bb_clear, grid_small(), 256, 0, p);
+      mark("k_bb_clear");
+    }
     launch(k_products<SURF>, grid_small(), 128, 0, p);
     mark("k_products");
   }
@@ -4112,7 +4366,8 @@ class EngineImpl {
   }
 
   int launches_per_step() const {
-    return 8 + 2 * (dnet.rounds - 1) + (dnet.bound ? 1 : 0) + (dnet.bound && dnet.bpair_n ? 2 * kBPairRounds : 0);
+    return 8 + 2 * (dnet.rounds - 1) + (dnet.bound ? 1 : 0) + (dnet.bound && dnet.bpair_n ? 2 * kBPairRounds : 0) +
+           (dnet.bound && dnet.bb_n ? 2 + 2 * kBPairRounds : 0);
   }
 
   int upload_const(std::string *err) {
@@ -4136,7 +4391,7 @@ class EngineImpl {
     const int nr2 = std::max(1, net.nrxn[2]), nr0 = std::max(1, net.nrxn[0]);
     std::vector<float> bind2((size_t)R * nr2, 0.f), pairprob((size_t)R * nr2, 1.f);
     std::vector<float> rsearch((size_t)R * nsp, 0.f);
-    float bpair_rmax = 0.f;
+    float bpair_rmax = 0.f, bb_rmax = 0.f;
     std::vector<double> births((size_t)R * nr0, 0.0);
     const int nrx = std::max(1, dnet.nrx_total);
     std::vector<float> prdpos((size_t)R * nrx * kMaxProd * 3, 0.f);
@@ -4182,7 +4437,10 @@ class EngineImpl {
         if (net.rstate2[r][0] != 0 || net.rstate2[r][1] != 0) {  // searched from the bound list
           const double hmin0 = std::min(geo[rp].h[0], std::min(geo[rp].h[1], geo[rp].h[2]));
           const double rb = std::sqrt(std::max(0.0, s.bind2[r])) * (1.0 + 1e-4) + 1e-6 * hmin0;
-          if (rp == 0) bpair_rmax = std::max(bpair_rmax, (float)rb);
+          if (rp == 0) {
+            if (net.rstate2[r][0] != 0 && net.rstate2[r][1] != 0) bb_rmax = std::max(bb_rmax, (float)rb);
+            else bpair_rmax = std::max(bpair_rmax, (float)rb);
+          }
           continue;
         }
         // stencil radius: largest binding radius of the species' pair reactions,
@@ -4205,6 +4463,7 @@ class EngineImpl {
     dnet.any_drift = any_drift ? 1 : 0;
     dnet.difm_any = difm_any;
     dnet.bpair_rmax = bpair_rmax;
+    dnet.bb_rmax = bb_rmax;
     auto put = [&](void **dst, const void *src, size_t bytes) -> int {
       if (!*dst) CK(cudaMalloc(dst, bytes));
       CK(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, stream));
@@ -4639,6 +4898,19 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
     D.rct[2][r][0] = (uint8_t)a;
     D.rct[2][r][1] = (uint8_t)b;
     const int sa = net.rstate2[r][0], sb = net.rstate2[r][1];
+    if (sa != 0 && sb != 0) {  // two bound reactants: the bound list's own pair pass
+      if (!net.bound) { if (err) *err = "reactions of surface-bound molecules need surface rules with bound states"; return -6; }
+      const int k = D.bb_n++;
+      D.bb_rxn[k] = (uint8_t)r;
+      D.bb_sp[k][0] = (uint8_t)a;
+      D.bb_sp[k][1] = (uint8_t)b;
+      D.bb_st[k][0] = (uint8_t)sa;
+      D.bb_st[k][1] = (uint8_t)sb;
+      D.bb_pst[k] = (uint8_t)net.pstate2[r];
+      D.bb_mask[a][sa - 1] |= 1u << b;
+      D.bb_mask[b][sb - 1] |= 1u << a;
+      continue;
+    }
     if (sa != 0 || sb != 0) {  // one bound reactant: the bound list's pair pass
       if (!net.bound) { if (err) *err = "reactions of surface-bound molecules need surface rules with bound states"; return -6; }
       const int k = D.bpair_n++;
@@ -4809,6 +5081,13 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
       CK(cudaMemsetAsync(E.d_bclaim, 0xFF, E.cap * sizeof(ull), E.stream));
       CK(cudaMalloc(&E.d_bcand, E.bcap * sizeof(int4)));
       CK(cudaMemsetAsync(E.d_bcand, 0xFF, E.bcap * sizeof(int4), E.stream));
+    }
+    if (D.bb_n) {
+      CK(cudaMalloc(&E.d_bbhead, ((size_t)1 << kBBHashBits) * sizeof(int)));
+      CK(cudaMemsetAsync(E.d_bbhead, 0xFF, ((size_t)1 << kBBHashBits) * sizeof(int), E.stream));
+      CK(cudaMalloc(&E.d_bbnext, E.bcap * sizeof(int)));
+      CK(cudaMalloc(&E.d_bbcell, E.bcap * sizeof(int)));
+      CK(cudaMalloc(&E.d_bbbest, E.bcap * sizeof(ull)));
     }
     CK(cudaMalloc(&E.d_srfrule, nrule * sizeof(SrfRule)));
     CK(cudaMemcpyAsync(E.d_srfrule, net.srf_rules.data(), nrule * sizeof(SrfRule), cudaMemcpyHostToDevice, E.stream));

@@ -102,7 +102,7 @@ struct NetSpec {
   // second-order reactions with one surface-bound reactant: reactant states
   // and the product's state
   int rstate2[kMaxRxn][2] = {};
-  int pstate2[kMaxRxn] = {};
+  int pstate2[kMaxRxn] = {};  // (both reactants bound: bound-bound reactions, same panel only)
   // surface-bound states (single simulations only): rules by
   // ((surface * kMaxSpecies + species) * 3 + state) * 3 + face, state 0..2 =
   // soln, front, back and face 0..2 = front, back, none

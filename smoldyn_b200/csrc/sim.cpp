@@ -734,8 +734,8 @@ int set_reaction_surface(Sim &sim, RxnDef &x, int sf, std::string *err) {
 
 // Append a reaction after checking its reactant and product states: solution
 // reactions, a first-order reaction of a bound reactant with at most two
-// products, or a second-order one of a bound and a solution reactant with at
-// most one product (the reactant and product states of doreact,
+// products, or a second-order one with one or two bound reactants and at most
+// one product (the reactant and product states of doreact,
 // smolreact.c:2662-2902, that the engine builds).
 int add_reaction_def(Sim &sim, const RxnDef &x, std::string *err) {
   int nbound = 0;
@@ -750,9 +750,9 @@ int add_reaction_def(Sim &sim, const RxnDef &x, std::string *err) {
     if (st < 0 || (st > 2 && st != 5)) { if (err) *err = "product state not supported by the GPU engine"; return -7; }
     bprod = bprod || st != 0;
   }
-  if (bound && (x.order == 0 || nbound > 1 || x.nprod > (x.order == 1 ? 2 : 1))) {
+  if (bound && (x.order == 0 || x.nprod > (x.order == 1 ? 2 : 1))) {
     if (err) *err = "reactions of surface-bound molecules are supported as first order with at most two products, "
-                    "or second order with one solution reactant and at most one product";
+                    "or second order with at most one product";
     return -7;
   }
   if (!bound && bprod && !(x.order == 0 && x.srf >= 0)) {

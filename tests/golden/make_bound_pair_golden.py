@@ -5,8 +5,9 @@ loaded by oracle/_ref/smoldyn with `-t` (text output, no simulation past the
 start): second-order reactions between a bound reactant (front or back
 state, first or second reactant) and a solution reactant, reversible surface
 binding (`A(front) + B <-> C(front)`, whose reverse is a first-order bound
-reaction with a bound and a solution product) and emission from a bound
-molecule (`A(front) -> A(front) + B`).  Its "Reaction details" block prints,
+reaction with a bound and a solution product), emission from a bound
+molecule (`A(front) -> A(front) + B`) and reactions of two bound molecules
+(`A(front) + C(front) -> A(front)`, reversible dimerization).  Its "Reaction details" block prints,
 per reaction, the requested and actual rate constants, the binding radius
 (second order) and the unbinding radius (two products) (rxnsetrate
 smolreact.c:1307-1410, rxnsetproduct :1431-1577, rxncalcrate :1592-1680).
@@ -24,7 +25,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 REF = os.path.join(ROOT, "oracle", "_ref", "smoldyn")
-NCASE = 32
+NCASE = 40
 
 
 def make_config(rng):
@@ -41,7 +42,9 @@ def make_config(rng):
     names = []
     forms = ["A(front) + B -> C(front)", "B + A(back) -> C", "A(front) + C -> 0", "C + A(front) -> A(front)",
              "A(back) + B -> C(bsoln)", "A(front) + A -> A(front)", "A(front) + B <-> C(front)",
-             "C(front) -> A(front) + B", "A(front) -> A(front) + B", "A(back) -> C(front) + B(bsoln)"]
+             "C(front) -> A(front) + B", "A(front) -> A(front) + B", "A(back) -> C(front) + B(bsoln)",
+             "A(front) + C(front) -> A(front)", "A(front) + A(front) -> C(front)", "A(back) + A(front) -> 0",
+             "A(front) + A(front) <-> C(front)"]
     pick = rng.choice(len(forms), size=3, replace=False)
     for q, f in enumerate(pick):
         nm = "r%d" % q

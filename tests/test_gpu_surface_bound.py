@@ -29,6 +29,10 @@ changes the species, so `molcount` separates the two sides.
      diffusion along it, reversible binding (products offset in the plane);
   12. births on a surface (order 0 restricted to a surface): bound products
      placed by area on a sphere, solution products on its back (inner) side;
+  13. reactions of two bound molecules on one panel: reversible dimerization
+     (the reverse with two bound products) and mutual removal (no reactant
+     shared between the two, so the reference's list order decides no
+     contest between them);
   8. second-order reactions of a bound and a solution reactant, with a
      bound product, a solution product and none; solution molecules behind
      the panel do not react.  The bound molecules sit within one binding
@@ -354,6 +358,25 @@ cmd N 10 molcountincmpt inside outi.txt
 end_file
 """
 
+BBRXN = HEAD + """species A C D E
+difc A(front) 0.5
+difc C(front) 0.2
+difc D(front) 0.3
+difc E(front) 0.3
+""" + WALLS + """start_surface plane
+action both all reflect
+panel rect +0 10 0 0 20 20 p1
+end_surface
+reaction d A(front) + A(front) <-> C(front) 0.5 0.5
+reaction h D(front) + E(front) -> 0 1
+surface_mol 1000 A(front) plane rect p1
+surface_mol 500 D(front) plane rect p1
+surface_mol 500 E(front) plane rect p1
+output_files out.txt
+cmd N 10 molcount out.txt
+end_file
+"""
+
 TRANSMIT = HEAD + """species A B
 difc A 1
 difc B 1
@@ -583,3 +606,13 @@ def test_births_on_a_surface():
     area = 4 * np.pi * 16
     # births at 2 per unit area and time, decay at 0.5: A(t) = 4 area (1 - exp(-t/2))
     assert np.all(np.abs(a - 4 * area * (1 - np.exp(-0.5 * t))) < 30), (a, 4 * area * (1 - np.exp(-0.5 * t)))
+
+
+def test_bound_bound_reactions():
+    def on_plane(s):
+        pos, sp, st, srf, pnl, sn = s.surface_molecules()
+        assert np.all(np.abs(pos[:, 0] - 10.0) < 1e-6) and np.all(pos[:, 0] > 10.0)
+    text = fill(BBRXN, L=20, T=3.0, dt=0.01)
+    _, gpu = compare(text, ["out.txt"], [1, 2, 3, 4], "bbrxn", check=on_plane)
+    G = np.stack([g[0] for g in gpu]).mean(0)
+    assert G[-1, 2] > 50 and G[-1, 3] < 450  # dimers formed; D and E removed each other

@@ -9,8 +9,8 @@ surface-bound molecules (smolgpuGetSurfaceMolecules) must sit on their panel
 on the requested side.  Second-order reactions of a bound and a solution
 reactant: binding radii and effective rates against the values the
 reference binary prints for the same configurations (golden fixture).
-Error paths: an unknown panel, a state the engine does not build, reactions
-with two bound reactants, bound reactants with more products than built,
+Error paths: an unknown panel, a state the engine does not build, bound
+reactants with more products than built,
 solution reactants with bound products, and bound-reactant reactions with a
 bounce placement.
 """
@@ -109,7 +109,7 @@ def test_errors():
     assert lib.smolAddSurfaceMolecules(s.ptr, b"A", sb.MSup, 5, b"membrane", sb.PSrect, b"m1", None) != 0
     assert lib.smolSetSurfaceRate(s.ptr, b"membrane", b"A", sb.MSup, sb.MSup, sb.MSsoln, 1.0, None, 0) != 0
     s.close()
-    for stmt in ("reaction r A(front) + A(back) -> A(front) 1", "reaction r A(front) -> B(front) + B(front) + B 1",
+    for stmt in ("reaction r A(front) + A(back) -> A(front) + B 1", "reaction r A(front) -> B(front) + B(front) + B 1",
                  "reaction r A -> B(front) 1", "reaction r A(front) + B -> A(front) 1\nproduct_placement r bounce -2",
                  "reaction r A(front) + B -> A(front) + B 1"):
         d = tempfile.mkdtemp()
@@ -168,9 +168,14 @@ def test_add_reaction_with_states_through_the_c_api():
                                C.cast(states, C.POINTER(C.c_int)), 1.2) == 0
     assert a.reaction_params("r") == b.reaction_params("r")
     assert a.effective_rate("r") == b.effective_rate("r")
-    # two bound reactants, and a bound product of solution reactants, are refused
+    # two bound reactants react on one panel; with two products they are
+    # refused, as is a bound product of solution reactants
     assert lib.smolAddReaction(b.ptr, b"r2", b"A", sb.MSfront, b"A", sb.MSback, 1, prods,
-                               C.cast(states, C.POINTER(C.c_int)), 1.0) != 0
+                               C.cast(states, C.POINTER(C.c_int)), 1.0) == 0
+    prods2 = (C.c_char_p * 2)(b"A", b"B")
+    states2 = (C.c_int * 2)(sb.MSfront, sb.MSsoln)
+    assert lib.smolAddReaction(b.ptr, b"r4", b"A", sb.MSfront, b"A", sb.MSback, 2, prods2,
+                               C.cast(states2, C.POINTER(C.c_int)), 1.0) != 0
     assert lib.smolAddReaction(b.ptr, b"r3", b"B", sb.MSsoln, None, sb.MSsoln, 1, prods,
                                C.cast(states, C.POINTER(C.c_int)), 1.0) != 0
     a.close()
