@@ -166,7 +166,10 @@ struct BoundMol {
   ull id;
   int pnl;
   int ms;
+  uint32_t born;  // step in which a reaction made it (it reacts again from the next step), else all ones
+  uint32_t pad;
 };
+constexpr uint32_t kBornNever = 0xFFFFFFFFu;
 
 // Per-replicate geometry.  Cells are cubes of size h; the last cell in each
 // dimension extends to the high wall, which sits at local coordinate whi.

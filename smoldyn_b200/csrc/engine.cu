@@ -807,6 +807,7 @@ __device__ int bound_first_order(const KParams &p, BoundMol &m, int &sp, ull ske
       b.pnl = pnl;
       b.ms = pst;
       b.id = make_id(psp, 0, sn);
+      b.born = step;  // products react from the next step on, as the reference's join its lists then
       if (q == q0) {
         m = b;
         sp = psp;
@@ -962,6 +963,7 @@ __device__ __noinline__ int soln_surface_bound(const KParams &p, ull &id, const 
     m.pnl = pnl;
     m.ms = ms;
     m.id = make_id(sp, 0, id_serno(id));
+    m.born = kBornNever;
     double y0[3], y1[3];
     const int c = bound_coin(p, m, sp, skey, step, y0, y1);
     if (c == 1) return 1;
@@ -1498,7 +1500,8 @@ __global__ void __launch_bounds__(256) k_bpair_claim(KParams p, int round) {
     if (round > 0 && !(c0.x >= 0 && c0.w == 0)) continue;  // later rounds: the molecules that lost their partner
     const BoundMol m = p.bd_out[k];
     const int sp = id_species(m.id);
-    const uint32_t mask = sp == kDeadSpecies ? 0u : c_net.bpair_mask[sp][m.ms - 1];
+    // a product of this step reacts from the next step on
+    const uint32_t mask = (sp == kDeadSpecies || m.born == step) ? 0u : c_net.bpair_mask[sp][m.ms - 1];
     ull best = ~0ull;  // (priority << 32 | lane) of this lane's best partner
     int bj = -1, be = 0;
     if (mask) {
@@ -1661,6 +1664,7 @@ __global__ void __launch_bounds__(256) k_bpair_resolve(KParams p) {
       m.pnl = pnl;
       m.ms = pst;
       m.id = make_id(psp, 0, id_serno(m.id));
+      m.born = step;
       p.bd_out[k] = m;
       continue;
     }
@@ -1706,10 +1710,11 @@ constexpr ull kBBReacted = ~0ull - 1;  // bbbest of a molecule that reacted this
 
 __device__ __forceinline__ int bb_bucket(int cell) { return (int)(((uint32_t)cell * 2654435761u) >> (32 - kBBHashBits)); }
 
-__device__ __forceinline__ bool bb_candidate(const KParams &p, int k) {
+__device__ __forceinline__ bool bb_candidate(const KParams &p, int k, uint32_t step) {
   const BoundMol &m = p.bd_out[k];
   const int sp = id_species(m.id);
   if (sp == kDeadSpecies || !c_net.bb_mask[sp][m.ms - 1]) return false;
+  if (m.born == step) return false;  // a product of this step reacts from the next step on
   // an entry that reacted with a solution molecule this step holds a product
   if (c_net.bpair_n && p.bcand[k].x >= 0 && p.bcand[k].w == 1) return false;
   return true;
@@ -1719,9 +1724,10 @@ __global__ void __launch_bounds__(256) k_bb_insert(KParams p) {
   pdl_launch_dependents();
   pdl_wait();
   const int nb = min(*p.bd_out_n, p.bcap);
+  const uint32_t step = *p.step;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nb; k += gridDim.x * blockDim.x) {
     p.bbbest[k] = ~0ull;
-    if (!bb_candidate(p, k)) {
+    if (!bb_candidate(p, k, step)) {
       p.bbcell[k] = -1;
       continue;
     }
@@ -1880,6 +1886,7 @@ __global__ void __launch_bounds__(256) k_bb_resolve(KParams p) {
       m.pnl = pnl;
       m.ms = pst;
       m.id = make_id(psp, 0, id_serno(m.id));
+      m.born = step;
       p.bd_out[k] = m;
       continue;
     }
@@ -3048,6 +3055,7 @@ __device__ __forceinline__ void place_event(const KParams &p, const Event &e, ui
           bm.id = make_id(fsp, 0, serno);
           bm.pnl = pnl;
           bm.ms = ms;
+          bm.born = step;
           push_bound(p, bm);
           atomicAdd((unsigned long long *)&p.spcount[fsp], 1ull);
           dead = true;
@@ -3167,6 +3175,7 @@ __device__ void surface_birth(const KParams &p, const Event &e, int r, int rep, 
         bm.id = make_id(psp, 0, serno);
         bm.pnl = pk;
         bm.ms = pst;
+        bm.born = step;
         push_bound(p, bm);
         atomicAdd((unsigned long long *)&p.spcount[psp], 1ull);
       }
@@ -5377,6 +5386,8 @@ int Engine::set_bound(long long n, const double *pos, const int *species, const 
     for (int d = 0; d < 3; ++d) m[i].x[d] = pos[3 * i + d] - E.reps[0].lo[d];
     m[i].pnl = panel[i];
     m[i].ms = state[i];
+    m[i].born = kBornNever;
+    m[i].pad = 0;
     const ull sn = (serno && serno[i]) ? (ull)serno[i] : ((1ull << 40) + (ull)i);
     m[i].id = make_id(sp, 0, sn);
   }
