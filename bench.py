@@ -450,6 +450,7 @@ end_surface
 reaction fwd A + B -> C 0.5
 reaction rev C -> A + B 0.1
 reaction bnd A(front) + B -> A(front) 0.2
+reaction dim A(front) + A(front) -> A(front) 0.05
 mol 20000 A u u u
 mol 20000 B u u u
 surface_mol 20000 A(front) cell sph all
@@ -463,8 +464,8 @@ def kernel_tour(args):
     at 4e6 molecules (its density), the device upload path, meansqrdisp and
     molcountincmpt with a transmitting sphere compartment (surface form of the
     step kernels), adsorption, desorption and bound diffusion on a sphere
-    with a bound-solution reaction (k_bound, the bound-state form and the
-    bound-pair kernels), the FP64 radius solvers, the surrogate's sampling,
+    with a bound-solution and a bound-bound reaction (k_bound, the bound-state
+    form and the bound-pair kernels), the FP64 radius solvers, the surrogate's sampling,
     training, inference and radius kernels, the persistent ensemble kernel
     and its layout changes, and the radial-distribution solver."""
     import ctypes as C
