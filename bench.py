@@ -349,11 +349,12 @@ def main():
         e2e = run_e2e(sb, args, rank, world, dist, barrier)
 
     # ---- batched ensemble and surrogate sweep (extra workloads, same GPU)
-    batched = surrogate = surfaces = rdf = None
+    batched = surrogate = surfaces = bound = rdf = None
     if not args.no_batched:
         batched = run_batched(sb, torch, args, rank)
         surrogate = run_surrogate(sb, torch, args, rank)
         surfaces = run_surfaces(sb, torch, args, rank)
+        bound = run_surface_bound(sb, torch, args, rank)
         rdf = run_rdf_tables(sb, args, rank, world)
 
     # ---- CPU baseline (rank 0, single GPU run only)
@@ -377,6 +378,7 @@ def main():
             "e2e": e2e, "gpu_launches": int(launches),
             "roofline": roof, "step_roofline_frac": step_frac, "kernels": kernels, "cpu_baseline": cpu,
             "clocks": ck, "batched": batched, "batched_surrogate": surrogate, "surfaces": surfaces,
+            "surface_bound": bound,
             "rdf_tables": rdf,
         }
         print(json.dumps(line))
@@ -880,6 +882,74 @@ def run_surfaces(sb, torch, args, rank):
                "value": 0.5 * (n0 + n1) * steps / sec, "unit": METRIC, "molecules_start": int(n0),
                "molecules_end": int(n1), "steps": steps, "ms_per_step": sec * 1e3 / steps,
                "tuning": s.tuning(), "autotune_best_trial_ms": tune_ms}
+        s.close()
+        return out
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+BOUND_CONFIG = """dim 3
+species A B
+difc A 1
+difc B 1
+difc A(front) 0.1
+boundaries 0 0 100
+boundaries 1 0 100
+boundaries 2 0 100
+time_start 0
+time_stop 1000
+time_step 0.01
+random_seed %d
+start_surface walls
+action both all reflect
+panel rect +0 0 0 0 100 100
+panel rect -0 100 0 0 100 100
+panel rect +1 0 0 0 100 100
+panel rect -1 0 100 0 100 100
+panel rect +2 0 0 0 100 100
+panel rect -2 0 0 100 100 100
+end_surface
+start_surface cell
+action both all reflect
+rate A fsoln front 2
+rate A front fsoln 0.5
+panel sph 50 50 50 30 20 20
+end_surface
+reaction bnd A(front) + B -> A(front) 0.5
+reaction birth 0 -> B 0.005
+mol 500000 A u u u
+mol 500000 B u u u
+surface_mol 200000 A(front) cell sph all
+end_file
+"""
+
+
+def run_surface_bound(sb, torch, args, rank):
+    """Surface-bound states: cube 100 closed by reflective panels, a sphere of
+    radius 30 where A adsorbs (rate 2) and desorbs (0.5) and diffuses bound
+    (D 0.1); bound A removes solution B (A(front) + B -> A(front), 0.5), B is
+    born in the volume (0.005); 5e5 A and 5e5 B in solution, 2e5 A bound;
+    dt = 0.01.  Molecule-steps count solution and bound molecules."""
+    d = tempfile.mkdtemp(prefix="smolbound_")
+    try:
+        with open(os.path.join(d, "bound.txt"), "w") as f:
+            f.write(BOUND_CONFIG % (9 + rank))
+        s = sb.Sim.load_file(os.path.join(d, "bound.txt"))
+        s.update()
+        stream = torch.cuda.Stream()
+        s.set_stream(stream.cuda_stream)
+        s.run_steps(args.warmup)
+        count = lambda: sum(s.count(nm, sb.MSall) for nm in ("A", "B"))
+        n0, b0 = count(), s.count("A", sb.MSfront)
+        steps = 200
+        sec = time_on_stream(torch, stream, lambda: s.run_steps(steps))
+        n1, b1 = count(), s.count("A", sb.MSfront)
+        out = {"workload": "surface-bound states: cube 100 closed by reflective panels, sphere r=30 with A "
+                           "adsorbing (2) and desorbing (0.5), bound diffusion 0.1, A(front) + B -> A(front) 0.5, "
+                           "0 -> B 0.005; 5e5 A, 5e5 B in solution, 2e5 A bound; dt=0.01",
+               "value": 0.5 * (n0 + n1) * steps / sec, "unit": METRIC, "molecules_start": int(n0),
+               "molecules_end": int(n1), "bound_start": int(b0), "bound_end": int(b1), "steps": steps,
+               "ms_per_step": sec * 1e3 / steps}
         s.close()
         return out
     finally:
