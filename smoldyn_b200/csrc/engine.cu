@@ -1460,11 +1460,10 @@ constexpr uint32_t kCtrBPair = 0x500u;  // + list entry: coin of a bound-solutio
 constexpr int kBPairRounds = 4;
 constexpr uint32_t kCtrBProd = 0x5A5A5A5Au;  // stream offset of a product's placement
 
-// absolute position of sorted molecule j, as the displacement-nearest image
-// of x0 in periodic dimensions
-__device__ __forceinline__ void bpair_partner_pos(const KParams &p, int j, const double x0[3], double xs[3]) {
+// absolute position of a sorted molecule's entry q, as the
+// displacement-nearest image of x0 in periodic dimensions
+__device__ __forceinline__ void bpair_partner_xyz(const float4 q, const double x0[3], double xs[3]) {
   const DevGeo &g = c_geo0;
-  const float4 q = p.b_pc[j];
   int jx[3];
   unpack_cell(__float_as_uint(q.w), jx[0], jx[1], jx[2]);
   const float u[3] = {q.x, q.y, q.z};
@@ -1482,7 +1481,7 @@ __device__ __forceinline__ void bpair_partner_pos(const KParams &p, int j, const
 // largest binding radius of these reactions reaches from the molecule's place
 // in its box, a warp prefix sum numbers their molecules, and the lanes test
 // them 32 at a time; a warp minimum picks the claim.
-__global__ void __launch_bounds__(256) k_bpair_claim(KParams p, int round) {
+__global__ void __launch_bounds__(256, 3) k_bpair_claim(KParams p, int round) {
   pdl_launch_dependents();
   pdl_wait();
   const int nb = min(*p.bd_out_n, p.bcap);
@@ -1495,107 +1494,127 @@ __global__ void __launch_bounds__(256) k_bpair_claim(KParams p, int round) {
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   const float rmax = c_net.bpair_rmax;
-  for (int k = gw; k < nb; k += nw) {
-    const int4 c0 = p.bcand[k];
-    if (round > 0 && !(c0.x >= 0 && c0.w == 0)) continue;  // later rounds: the molecules that lost their partner
-    const BoundMol m = p.bd_out[k];
-    const int sp = id_species(m.id);
-    // a product of this step reacts from the next step on
-    const uint32_t mask = (sp == kDeadSpecies || m.born == step) ? 0u : c_net.bpair_mask[sp][m.ms - 1];
-    ull best = ~0ull;  // (priority << 32 | lane) of this lane's best partner
-    int bj = -1, be = 0;
-    if (mask) {
-      const DevPanel &pn = c_panels[m.pnl];
-      const ull kb = id_stream(m.id);
-      int ix[3];
-      float u[3];
-      from_abs(g, m.x, ix, u);
-      int s0 = 0, cnt = 0;
-      if (lane < 27) {
-        const int off[3] = {lane % 3 - 1, (lane / 3) % 3 - 1, lane / 9 - 1};
-        int cc[3];
-        bool ok = true;
-        for (int d = 0; d < 3; ++d) {
-          if (d >= g.dim && off[d] != 0) ok = false;
-          const float ub = (ix[d] == g.n[d] - 1) ? g.whi[d] : g.h[d];
-          if (off[d] < 0 && !(u[d] < rmax)) ok = false;
-          if (off[d] > 0 && !(u[d] > ub - rmax)) ok = false;
-          cc[d] = ix[d] + off[d];
-          if (cc[d] < 0 || cc[d] >= g.n[d]) {
-            if (g.wall[2 * d] != kWallPeriodic || g.n[d] < 3) ok = false;
-            cc[d] = cc[d] < 0 ? cc[d] + g.n[d] : cc[d] - g.n[d];
-          }
-        }
-        if (ok) {
-          const int cell = g.cell0 + (cc[2] * g.n[1] + cc[1]) * g.n[0] + cc[0];
-          s0 = p.start[cell];
-          cnt = max(0, min(p.start[cell + 1], n) - s0);
-        }
-      }
-      int incl = cnt;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(full, incl, o);
-        if (lane >= o) incl += y;
-      }
-      const int excl = incl - cnt;
-      const int total = __shfl_sync(full, incl, 31);
-      for (int t0 = 0; t0 < total; t0 += 32) {
-        const int t = t0 + lane;
-        int o = 0;  // the last lane whose first number is <= t
-#pragma unroll
-        for (int st = 16; st > 0; st >>= 1)
-          if (__shfl_sync(full, excl, o + st) <= t) o += st;
-        const int j = __shfl_sync(full, s0, o) + (t - __shfl_sync(full, excl, o));
-        if (t >= total) continue;
-        const ull idj = p.b_id[j];
-        const int sj = id_species(idj);
-        if (sj == kDeadSpecies || !((mask >> sj) & 1u)) continue;
-        double xs[3];
-        bpair_partner_pos(p, j, m.x, xs);
-        const double d2 = (xs[0] - m.x[0]) * (xs[0] - m.x[0]) + (xs[1] - m.x[1]) * (xs[1] - m.x[1]) +
-                          (xs[2] - m.x[2]) * (xs[2] - m.x[2]);
-        const ull pk = mix64((kb * 0x9E3779B97F4A7C15ull ^ id_stream(idj)) + (ull)step * 0xD1B54A32D192ED03ull);
-        const uint32_t prio = (uint32_t)(pk >> 32);
-        const ull pkey = ((ull)prio << 32) | (uint32_t)lane;
-        if (pkey >= best) continue;
-        int side = -1;  // the panel side, read once a reaction is in range
-        for (int e = 0; e < c_net.bpair_n; ++e) {
-          if (c_net.bpair_bsp[e] != sp || c_net.bpair_bst[e] != m.ms || c_net.bpair_ssp[e] != sj) continue;
-          const int r = c_net.bpair_rxn[e];
-          if (d2 > (double)p.bind2[r]) continue;
-          const float prob = p.pairprob[r];
-          if (prob < 1.f) {
-            const ull kk = mix64(kb * 0x9E3779B97F4A7C15ull ^ id_stream(idj));
-            const uint4 rr = philox(make_uint4((uint32_t)kk, (uint32_t)(kk >> 32), step, kCtrBPair + (uint32_t)e), key);
-            if (!(u01co(rr.x) < (double)prob)) continue;
-          }
-          if (side < 0) side = panel_side(pn, xs, nullptr) == kFaceBack ? 0 : 1;
-          if (!side) break;  // behind the panel: the solution state is bsoln, which no reaction takes
-          const int cm = c_net.cmpt[2][r];
-          if (cm && !(pos_in_cmpt(c_cmpt, cm - 1, c_panels, xs) && pos_in_cmpt(c_cmpt, cm - 1, c_panels, m.x)))
-            continue;
-          const int rs = c_net.rsrf[2][r];
-          if (rs && pn.srf != rs - 1) continue;  // restricted to another surface (morebireact :3116)
-          best = pkey;
-          bj = j;
-          be = e;
-          break;
-        }
+  // each warp takes 32 bound molecules at a time, one per lane, and searches
+  // for those that need it one after the other: in the first round the live
+  // ones with such a reaction, later the ones that lost their partner
+  for (int k0 = gw * 32; k0 < nb; k0 += nw * 32) {
+    bool need = false;
+    if (k0 + lane < nb) {
+      const int kl = k0 + lane;
+      if (round == 0) {
+        const BoundMol &ml = p.bd_out[kl];
+        const int spl = id_species(ml.id);
+        // a product of this step reacts from the next step on
+        need = spl != kDeadSpecies && ml.born != step && c_net.bpair_mask[spl][ml.ms - 1] != 0u;
+        if (!need) p.bcand[kl] = make_int4(-1, 0, 0, 0);
+      } else {
+        const int4 cl = p.bcand[kl];
+        need = cl.x >= 0 && cl.w == 0;
       }
     }
-    // warp minimum: the lowest priority (ties to the lower lane)
-    ull wmin = best;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const ull y = __shfl_xor_sync(full, wmin, o);
-      wmin = y < wmin ? y : wmin;
-    }
-    if (wmin != ~0ull && best == wmin) {  // the winning lane
-      p.bcand[k] = make_int4(bj, be, (int)(uint32_t)(wmin >> 32), 0);
-      atomicMin(&p.bclaim[bj], (wmin & 0xFFFFFFFF00000000ull) | (ull)(uint32_t)k);
-    } else if (wmin == ~0ull && lane == 0) {
-      p.bcand[k] = make_int4(-1, 0, 0, 0);
+    unsigned todo = __ballot_sync(full, need);
+    while (todo) {
+      const int k = k0 + __ffs(todo) - 1;
+      todo &= todo - 1;
+      const BoundMol m = p.bd_out[k];
+      const int sp = id_species(m.id);
+      const uint32_t mask = c_net.bpair_mask[sp][m.ms - 1];
+      ull best = ~0ull;  // (priority << 32 | lane) of this lane's best partner
+      int bj = -1, be = 0;
+      if (mask) {
+        const DevPanel &pn = c_panels[m.pnl];
+        const ull kb = id_stream(m.id);
+        int ix[3];
+        float u[3];
+        from_abs(g, m.x, ix, u);
+        int s0 = 0, cnt = 0;
+        if (lane < 27) {
+          const int off[3] = {lane % 3 - 1, (lane / 3) % 3 - 1, lane / 9 - 1};
+          int cc[3];
+          bool ok = true;
+          for (int d = 0; d < 3; ++d) {
+            if (d >= g.dim && off[d] != 0) ok = false;
+            const float ub = (ix[d] == g.n[d] - 1) ? g.whi[d] : g.h[d];
+            if (off[d] < 0 && !(u[d] < rmax)) ok = false;
+            if (off[d] > 0 && !(u[d] > ub - rmax)) ok = false;
+            cc[d] = ix[d] + off[d];
+            if (cc[d] < 0 || cc[d] >= g.n[d]) {
+              if (g.wall[2 * d] != kWallPeriodic || g.n[d] < 3) ok = false;
+              cc[d] = cc[d] < 0 ? cc[d] + g.n[d] : cc[d] - g.n[d];
+            }
+          }
+          if (ok) {
+            const int cell = g.cell0 + (cc[2] * g.n[1] + cc[1]) * g.n[0] + cc[0];
+            s0 = p.start[cell];
+            cnt = max(0, min(p.start[cell + 1], n) - s0);
+          }
+        }
+        int incl = cnt;
+  #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(full, incl, o);
+          if (lane >= o) incl += y;
+        }
+        const int excl = incl - cnt;
+        const int total = __shfl_sync(full, incl, 31);
+        for (int t0 = 0; t0 < total; t0 += 32) {
+          const int t = t0 + lane;
+          int o = 0;  // the last lane whose first number is <= t
+  #pragma unroll
+          for (int st = 16; st > 0; st >>= 1)
+            if (__shfl_sync(full, excl, o + st) <= t) o += st;
+          const int j = __shfl_sync(full, s0, o) + (t - __shfl_sync(full, excl, o));
+          if (t >= total) continue;
+          const ull idj = p.b_id[j];
+          const float4 qj = p.b_pc[j];  // loaded with the identity, not after it
+          const int sj = id_species(idj);
+          if (sj == kDeadSpecies || !((mask >> sj) & 1u)) continue;
+          double xs[3];
+          bpair_partner_xyz(qj, m.x, xs);
+          const double d2 = (xs[0] - m.x[0]) * (xs[0] - m.x[0]) + (xs[1] - m.x[1]) * (xs[1] - m.x[1]) +
+                            (xs[2] - m.x[2]) * (xs[2] - m.x[2]);
+          const ull pk = mix64((kb * 0x9E3779B97F4A7C15ull ^ id_stream(idj)) + (ull)step * 0xD1B54A32D192ED03ull);
+          const uint32_t prio = (uint32_t)(pk >> 32);
+          const ull pkey = ((ull)prio << 32) | (uint32_t)lane;
+          if (pkey >= best) continue;
+          int side = -1;  // the panel side, read once a reaction is in range
+          for (int e = 0; e < c_net.bpair_n; ++e) {
+            if (c_net.bpair_bsp[e] != sp || c_net.bpair_bst[e] != m.ms || c_net.bpair_ssp[e] != sj) continue;
+            const int r = c_net.bpair_rxn[e];
+            if (d2 > (double)p.bind2[r]) continue;
+            const float prob = p.pairprob[r];
+            if (prob < 1.f) {
+              const ull kk = mix64(kb * 0x9E3779B97F4A7C15ull ^ id_stream(idj));
+              const uint4 rr = philox(make_uint4((uint32_t)kk, (uint32_t)(kk >> 32), step, kCtrBPair + (uint32_t)e), key);
+              if (!(u01co(rr.x) < (double)prob)) continue;
+            }
+            if (side < 0) side = panel_side(pn, xs, nullptr) == kFaceBack ? 0 : 1;
+            if (!side) break;  // behind the panel: the solution state is bsoln, which no reaction takes
+            const int cm = c_net.cmpt[2][r];
+            if (cm && !(pos_in_cmpt(c_cmpt, cm - 1, c_panels, xs) && pos_in_cmpt(c_cmpt, cm - 1, c_panels, m.x)))
+              continue;
+            const int rs = c_net.rsrf[2][r];
+            if (rs && pn.srf != rs - 1) continue;  // restricted to another surface (morebireact :3116)
+            best = pkey;
+            bj = j;
+            be = e;
+            break;
+          }
+        }
+      }
+      // warp minimum: the lowest priority (ties to the lower lane)
+      ull wmin = best;
+  #pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const ull y = __shfl_xor_sync(full, wmin, o);
+        wmin = y < wmin ? y : wmin;
+      }
+      if (wmin != ~0ull && best == wmin) {  // the winning lane
+        p.bcand[k] = make_int4(bj, be, (int)(uint32_t)(wmin >> 32), 0);
+        atomicMin(&p.bclaim[bj], (wmin & 0xFFFFFFFF00000000ull) | (ull)(uint32_t)k);
+      } else if (wmin == ~0ull && lane == 0) {
+        p.bcand[k] = make_int4(-1, 0, 0, 0);
+      }
     }
   }
 }
@@ -1636,7 +1655,7 @@ __global__ void __launch_bounds__(256) k_bpair_resolve(KParams p) {
     }
     const int psp = c_net.prd[2][r][0], pst = c_net.bpair_pst[e];
     double xs[3];
-    bpair_partner_pos(p, j, m.x, xs);
+    bpair_partner_xyz(p.b_pc[j], m.x, xs);
     const double sb = c_net.bstep[spb][m.ms - 1], ss = c_net.sstep[sps];
     const double db = sb * sb, ds = ss * ss;  // proportional to the diffusion coefficients
     const double f = (db == 0 && ds == 0) ? 0.5 : ds / (db + ds);  // weight of the bound reactant
@@ -4303,7 +4322,7 @@ class EngineImpl {
     launch(k_begin, 1, 32, 0, p, rebin_only ? 0 : 1);
     mark("k_begin");
     if (dnet.bound && !rebin_only) {
-      launch(k_bound, grid_small(), 256, 0, p);
+      launch(k_bound, grid_mol(), 256, 0, p);  // latency-bound FP64 work: many blocks in flight
       mark("k_bound");
     }
     launch(k_move<SINGLE, SURF>, grid_mol(), 256, rebin_only ? 0 : adv_smem(), p, rebin_only ? 1 : 0);
@@ -4329,7 +4348,7 @@ class EngineImpl {
     }
     if (SURF == 3 && dnet.bpair_n) {
       for (int round = 0; round < kBPairRounds; ++round) {
-        launch(k_bpair_claim, grid_small(), 256, 0, p, round);
+        launch(k_bpair_claim, grid_mol(), 256, 0, p, round);
         mark("k_bpair_claim");
         launch(k_bpair_resolve, grid_small(), 256, 0, p);
         mark("k_bpair_resolve");
@@ -4339,7 +4358,7 @@ class EngineImpl {
       launch(k_bb_insert, grid_small(), 256, 0, p);
       mark("k_bb_insert");
       for (int round = 0; round < kBPairRounds; ++round) {
-        launch(k_bb_best, grid_small(), 256, 0, p);
+        launch(k_bb_best, grid_mol(), 256, 0, p);
         mark("k_bb_best");
         launch(k_bb_resolve, grid_small(), 256, 0, p);
         mark("k_bb_resolve");
