@@ -199,6 +199,8 @@ struct DevPanel {
   double axlen;     // cyl: axis length
   int act_front, act_back;   // default action per face: 0 reflect 1 transmit 2 absorb
   uint32_t abs_front, abs_back, tr_front, tr_back, rf_front, rf_back;  // per-species overrides
+  uint32_t jp_front, jp_back;        // species that jump at the front / back face
+  int jump_pnl[2], jump_face[2];     // per face: the panel a jump leads to (-1 none) and its face
   float posf, radiusf, centerf[3];   // FP32 copies for the screening test
   float p0f[3], nrmf[3];             // screen reference point and unit vector (zero for sph, hemi)
   int curved;                        // screen: 1 sph, cyl, hemi (radial test); 0 flat (plane test)

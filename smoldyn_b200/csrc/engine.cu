@@ -298,15 +298,71 @@ __device__ __forceinline__ const DevGeo &geo_of(const KParams &p, int rep) {
 __device__ __forceinline__ int panel_action(const DevPanel &pn, int face, int sp) {
   const uint32_t bit = 1u << sp;
   if (face == 0) {
+    if (pn.jp_front & bit) return 3;
     if (pn.abs_front & bit) return 2;
     if (pn.tr_front & bit) return 1;
     if (pn.rf_front & bit) return 0;
     return pn.act_front;
   }
+  if (pn.jp_back & bit) return 3;
   if (pn.abs_back & bit) return 2;
   if (pn.tr_back & bit) return 1;
   if (pn.rf_back & bit) return 0;
   return pn.act_back;
+}
+
+// Jump (surfacejump, smolsurface.c:4873-4927): a solution molecule that
+// crosses `face` of panel pn at x moves to the partner panel by the shape's
+// offset (rectangle, triangle, disk: between the panels' centres; sphere,
+// hemisphere, cylinder: the crossing point scaled between the two radii),
+// with the rest of its path; the crossing point is put on the partner's face,
+// and the path is reflected there when the two faces point the same way.
+// Returns false when the face leads nowhere (the molecule then transmits);
+// else x is the new crossing point (on the partner's face), out the unit
+// normal pointing to that face's side, and p1 the path's end.
+template <bool GEN>
+__device__ __noinline__ bool panel_jump(const DevPanel &pn, int face, double x[3], double p1[3], double out[3]) {
+  const int k2 = pn.jump_pnl[face];
+  if (k2 < 0) return false;
+  const DevPanel &pn2 = c_panels[k2];
+  const int face2 = pn.jump_face[face];
+  double delta[3];
+  int dir = 1;
+  if (pn.shape == 0) {
+    for (int d = 0; d < 3; ++d) {
+      const double c1 = d == pn.axis ? pn.pos : 0.5 * (pn.lo[d] + pn.hi[d]);
+      const double c2 = d == pn2.axis ? pn2.pos : 0.5 * (pn2.lo[d] + pn2.hi[d]);
+      delta[d] = c2 - c1;
+    }
+    dir = pn.front_sign == pn2.front_sign ? 1 : -1;
+  } else if (pn.shape == 1 || pn.shape == 5) {
+    for (int d = 0; d < 3; ++d)
+      delta[d] = pn.shape == 1 ? ((pn2.pt[0][d] + pn2.pt[1][d] + pn2.pt[2][d]) - (pn.pt[0][d] + pn.pt[1][d] + pn.pt[2][d])) / 3.0
+                               : pn2.center[d] - pn.center[d];
+    dir = dot3(pn.nrm, pn2.nrm) > 0 ? 1 : -1;
+  } else {
+    const double *o1 = pn.shape == 3 ? pn.pt[0] : pn.center, *o2 = pn2.shape == 3 ? pn2.pt[0] : pn2.center;
+    const double f = pn.radius > 0 ? pn2.radius / pn.radius : 1.0;
+    for (int d = 0; d < 3; ++d) delta[d] = (x[d] - o1[d]) * f + o2[d] - x[d];
+    dir = pn.front_sign == pn2.front_sign ? 1 : -1;
+  }
+  for (int d = 0; d < 3; ++d) {
+    x[d] += delta[d];
+    p1[d] += delta[d];
+  }
+  fix_to_panel(pn2, x, face2 == 0 ? kFaceFront : kFaceBack, 0.0);
+  if (face == face2) dir = -dir;
+  if (dir == -1) {  // the path would leave on the wrong side: it turns back at the partner (surfacereflect)
+    double n[3];
+    panel_normal<GEN>(pn2, x, n);
+    double dt = 0;
+    for (int d = 0; d < 3; ++d) dt += (p1[d] - x[d]) * n[d];
+    for (int d = 0; d < 3; ++d) p1[d] -= 2.0 * dt * n[d];
+  }
+  panel_normal<GEN>(pn2, x, out);
+  if (face2 != 0)
+    for (int d = 0; d < 3; ++d) out[d] = -out[d];
+  return true;
 }
 
 // Returns 1 if the molecule is absorbed; p1 is updated in place.
@@ -397,6 +453,10 @@ __device__ int surface_interact(int sp, const double p0_in[3], double p1[3], dou
     if (act == 2) return 1;
     double x[3], n[3];
     for (int d = 0; d < 3; ++d) x[d] = p0[d] + tmin * (p1[d] - p0[d]);
+    if (GEN && act == 3 && panel_jump<GEN>(pn, fmin, x, p1, n)) {  // on from just off the partner's face (general form)
+      for (int d = 0; d < 3; ++d) p0[d] = x[d] + eps * n[d];
+      continue;
+    }
     panel_normal<GEN>(pn, x, n);
     const double side = (fmin == 0) ? 1.0 : -1.0;  // incoming side along n
     if (act == 0) {
@@ -659,6 +719,10 @@ __device__ int walk_soln_rules(const KParams &p, int &sp, const double p0_in[3],
     if (act == kSAabsorb) return 1;
     double x[3], n[3];
     for (int d = 0; d < 3; ++d) x[d] = p0[d] + tmin * (p1[d] - p0[d]);
+    if (act == kSAjump && panel_jump<true>(pn, fmin, x, p1, n)) {  // on from just off the partner's face
+      for (int d = 0; d < 3; ++d) p0[d] = x[d] + eps * n[d];
+      continue;
+    }
     if (act == kSAadsorb) {
       for (int d = 0; d < 3; ++d) p1[d] = x[d];
       if (!pt_in_panel(pn, p1)) move_into_panel(pn, p1, c_net.bmargin);
@@ -4373,12 +4437,12 @@ class EngineImpl {
 
   // Enqueue one step with the given parity (inputs A/P = buffers `par`).
   void enqueue_step(int par, bool rebin_only) {
-    // surface form: 0 none, 1 rect and sphere panels only, 2 any shape or
-    // compartments (whose tests need panels to mean anything), 3 as 2 with
-    // surface-bound states
+    // surface form: 0 none, 1 rect and sphere panels only, 2 any shape,
+    // jumps or compartments (whose tests need panels to mean anything), 3 as
+    // 2 with surface-bound states
     int surf = dnet.npanel > 0 ? 1 : 0;
     for (const DevPanel &pn : panels)
-      if (pn.shape != 0 && pn.shape != 2) surf = 2;
+      if ((pn.shape != 0 && pn.shape != 2) || pn.jp_front || pn.jp_back) surf = 2;  // jumps: the general form
     if (surf && (dnet.ncmpt > 0 || dnet.bound)) surf = 2;
     if (dnet.bound) surf = 3;  // 3: any shape plus surface-bound states (single simulations)
     if (single_rep()) {

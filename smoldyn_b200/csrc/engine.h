@@ -50,6 +50,10 @@ struct PanelSpec {
   uint32_t trans_back_mask;
   uint32_t refl_front_mask;     // species bitmask overriding to reflect on front
   uint32_t refl_back_mask;
+  uint32_t jump_front_mask;     // species bitmask overriding to jump on front
+  uint32_t jump_back_mask;
+  int jump_pnl[2];              // per face: the engine panel a jump leads to (-1 none), and its face
+  int jump_face[2];
   int srf;                      // index of the panel's surface
   int nneigh;                   // neighbouring panels (engine panel indices) for surface-bound molecules
   int neigh[kMaxNeigh];

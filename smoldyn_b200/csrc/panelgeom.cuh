@@ -261,6 +261,12 @@ inline DevPanel make_dev_panel(const PanelSpec &ps, const double lo[3]) {
   dp.tr_back = ps.trans_back_mask;
   dp.rf_front = ps.refl_front_mask;
   dp.rf_back = ps.refl_back_mask;
+  dp.jp_front = ps.jump_front_mask;
+  dp.jp_back = ps.jump_back_mask;
+  for (int f = 0; f < 2; ++f) {
+    dp.jump_pnl[f] = ps.jump_pnl[f];
+    dp.jump_face[f] = ps.jump_face[f];
+  }
   dp.srf = ps.srf;
   dp.nneigh = ps.nneigh < kMaxNeigh ? ps.nneigh : kMaxNeigh;
   for (int k = 0; k < dp.nneigh; ++k) dp.neigh[k] = ps.neigh[k];

@@ -655,8 +655,19 @@ int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err) {
     for (int d = 0; d < 3; ++d) rep->drift[i][d] = (d < sim.dim) ? sim.species[i].drift[d] : 0;
   }
   choose_grid(sim, (long long)sim.pend_sp.size(), rep->ncell);
-  for (const SurfaceDef &sf : sim.surfaces)
-    for (PanelSpec ps : sf.panels) {
+  const std::vector<int> base = surface_panel_base(sim);
+  for (size_t si = 0; si < sim.surfaces.size(); ++si) {
+    const SurfaceDef &sf = sim.surfaces[si];
+    for (size_t q = 0; q < sf.panels.size(); ++q) {
+      PanelSpec ps = sf.panels[q];
+      ps.jump_front_mask = sf.jump_front;
+      ps.jump_back_mask = sf.jump_back;
+      for (int f = 0; f < 2; ++f) ps.jump_pnl[f] = ps.jump_face[f] = -1;
+      for (const std::array<int, 4> &j : sf.jumps)
+        if (j[0] == (int)q) {
+          ps.jump_pnl[j[1]] = base[si] + j[2];
+          ps.jump_face[j[1]] = j[3];
+        }
       ps.action_front = sf.act_front;
       ps.action_back = sf.act_back;
       ps.absorb_front_mask = sf.absorb_front;
@@ -668,6 +679,7 @@ int build_engine_specs(Sim &sim, NetSpec *net, RepSpec *rep, std::string *err) {
       if (net->panels.size() < (size_t)kMaxPanels) net->panel_area[net->panels.size()] = panel_area_dim(ps, sim.dim);
       net->panels.push_back(ps);
     }
+  }
   const std::vector<int> first = surface_panel_base(sim);
   for (const CompartDef &c : sim.cmpts) net->cmpts.push_back(cmpt_spec(sim, c, first));
   int rc = derive_surface_params(sim, err);

@@ -5,6 +5,7 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <array>
 #include <vector>
 
 #include "engine.h"
@@ -72,7 +73,10 @@ struct SurfaceDef {
   // action per face for all species unless overridden: 0 reflect 1 transmit 2 absorb
   int act_front = 1, act_back = 1;
   uint32_t absorb_front = 0, absorb_back = 0, trans_front = 0, trans_back = 0, refl_front = 0,
-           refl_back = 0;
+           refl_back = 0, jump_front = 0, jump_back = 0;
+  // jump statements: (panel, face, partner panel, partner face), panel
+  // indices within this surface, faces 0 front 1 back
+  std::vector<std::array<int, 4>> jumps;
   std::vector<PanelSpec> panels;
   std::vector<std::string> pnames;   // panel names (default: shape name + index within the shape)
   // SrfAction by [species][state][face] (face 0 front, 1 back, 2 none) set

@@ -351,7 +351,12 @@ int read_surface_rule_statement(Sim &sim, int sidx, const std::string &word, con
     if (an == "reflect" || an == "r") a = SAreflect;
     else if (an == "transmit" || an == "t") a = SAtrans;
     else if (an == "absorb" || an == "a") a = SAabsorb;
+    else if (an == "jump" || an == "j" || an == "periodic") a = SAjump;  // solution molecules only (dosurfinteract)
     if (a < 0) { if (err) *err = "surface action not supported by the GPU engine: " + an; return -7; }
+    if (a == SAjump && ms != MSsoln && ms != MSall) {
+      if (err) *err = "the jump action applies to solution molecules";
+      return -7;
+    }
     if (ms == MSup || ms == MSdown || ms == MSbsoln || ms == MSnone) {
       if (err) *err = "surface action state not supported by the GPU engine";
       return -7;
@@ -361,7 +366,7 @@ int read_surface_rule_statement(Sim &sim, int sidx, const std::string &word, con
       newsp = sim.species_index(w[3]);
       if (newsp <= 0) { if (err) *err = "final word of line is not an individual species name"; return -3; }
     }
-    const int lo = ms == MSall ? 0 : ms, hi = ms == MSall ? kSrfStates - 1 : ms;
+    const int lo = ms == MSall ? 0 : ms, hi = (ms == MSall && a != SAjump) ? kSrfStates - 1 : lo;
     for (int i : ids)
       for (int m = lo; m <= hi; ++m)
         for (int f = 0; f < 2; ++f) {
@@ -370,9 +375,9 @@ int read_surface_rule_statement(Sim &sim, int sidx, const std::string &word, con
           if (m == MSsoln) {  // the per-species masks of the solution state
             const uint32_t bit = 1u << i;
             uint32_t &ab = f ? sf.absorb_back : sf.absorb_front, &tr = f ? sf.trans_back : sf.trans_front,
-                     &rf = f ? sf.refl_back : sf.refl_front;
-            ab &= ~bit; tr &= ~bit; rf &= ~bit;
-            (a == SAabsorb ? ab : a == SAtrans ? tr : rf) |= bit;
+                     &rf = f ? sf.refl_back : sf.refl_front, &jp = f ? sf.jump_back : sf.jump_front;
+            ab &= ~bit; tr &= ~bit; rf &= ~bit; jp &= ~bit;
+            (a == SAabsorb ? ab : a == SAtrans ? tr : a == SAjump ? jp : rf) |= bit;
           }
           if (newsp) {
             SrfDetail &d = get_detail(sf, i, m, f);
@@ -380,6 +385,29 @@ int read_surface_rule_statement(Sim &sim, int sidx, const std::string &word, con
             d.newspec[m] = newsp;
           }
         }
+    return 0;
+  }
+  if (word == "jump") {
+    // jump panel1 face1 -> panel2 face2, or <-> for both directions
+    // (smolsurface.c:3574-3600): panels of this surface with the same shape
+    if (w.size() != 5) { if (err) *err = "format for jump: panel1 face1 -> panel2 face2"; return -7; }
+    int q[2] = {-1, -1}, f[2];
+    const std::string pn[2] = {w[0], w[3]}, fn[2] = {w[1], w[4]};
+    for (int k = 0; k < 2; ++k) {
+      for (size_t j = 0; j < sf.pnames.size(); ++j)
+        if (sf.pnames[j] == pn[k]) q[k] = (int)j;
+      if (q[k] < 0) { if (err) *err = "panel name listed in jump is not recognized"; return -3; }
+      f[k] = fn[k] == "front" ? 0 : fn[k] == "back" ? 1 : -1;
+      if (f[k] < 0) { if (err) *err = "face listed in jump needs to be 'front' or 'back'"; return -7; }
+    }
+    if (sf.panels[q[0]].shape != sf.panels[q[1]].shape) {
+      if (err) *err = "second panel name listed in jump is not recognized, or not same shape as first panel";
+      return -3;
+    }
+    if (q[0] == q[1]) { if (err) *err = "two different panels need to be listed in a jump statement"; return -7; }
+    if (w[2] != "->" && w[2] != "<->") { if (err) *err = "jump operator needs to be -> or <->"; return -7; }
+    sf.jumps.push_back({q[0], f[0], q[1], f[1]});
+    if (w[2] == "<->") sf.jumps.push_back({q[1], f[1], q[0], f[0]});
     return 0;
   }
   if (word == "rate" || word == "rate_internal") {
@@ -680,7 +708,8 @@ int build_surface_rules(const Sim &sim, NetSpec *net, std::string *err) {
         for (int f = 0; f < 3; ++f) {
           SrfRule &r = net->srf_rules[((size_t)(s * kMaxSpecies + i) * 3 + ms) * 3 + f];
           r.act = (int8_t)eff_act(sf, i, ms, f);
-          if (r.act == SAjump || r.act == SAport) { if (err) *err = "jump and port surface actions are not supported by the GPU engine"; return -6; }
+          if (r.act == SAport) { if (err) *err = "port surface actions are not supported by the GPU engine"; return -6; }
+          if (r.act == SAjump && ms != MSsoln) { if (err) *err = "the jump action applies to solution molecules"; return -6; }
           const SrfDetail *d = find_detail(sf, i, ms, f);
           r.rev = 0;
           for (int k = 0; k < 6; ++k) {

@@ -33,6 +33,8 @@ changes the species, so `molcount` separates the two sides.
      (the reverse with two bound products) and mutual removal (no reactant
      shared between the two, so the reference's list order decides no
      contest between them);
+  14. jump surfaces: two end panels that send solution molecules to each
+     other (a periodic box made of panels), counts in the left half;
   8. second-order reactions of a bound and a solution reactant, with a
      bound product, a solution product and none; solution molecules behind
      the panel do not react.  The bound molecules sit within one binding
@@ -377,6 +379,36 @@ cmd N 10 molcount out.txt
 end_file
 """
 
+JUMP = HEAD + """species A
+difc A 1
+start_surface sides
+action both all reflect
+panel rect +1 0 0 0 20 20
+panel rect -1 0 20 0 20 20
+panel rect +2 0 0 0 20 20
+panel rect -2 0 0 20 20 20
+end_surface
+start_surface ends
+action both all jump
+panel rect +0 0 0 0 20 20 left
+panel rect -0 20 0 0 20 20 right
+jump left front <-> right front
+end_surface
+start_surface mid
+action both all transmit
+panel rect +0 10 0 0 20 20 m
+end_surface
+start_compartment lefthalf
+surface mid
+point 5 10 10
+end_compartment
+mol 2000 A 1 u u
+output_files out.txt outl.txt
+cmd N 10 molcount out.txt
+cmd N 10 molcountincmpt lefthalf outl.txt
+end_file
+"""
+
 TRANSMIT = HEAD + """species A B
 difc A 1
 difc B 1
@@ -616,3 +648,11 @@ def test_bound_bound_reactions():
     _, gpu = compare(text, ["out.txt"], [1, 2, 3, 4], "bbrxn", check=on_plane)
     G = np.stack([g[0] for g in gpu]).mean(0)
     assert G[-1, 2] > 50 and G[-1, 3] < 450  # dimers formed; D and E removed each other
+
+
+def test_jump_surfaces():
+    text = fill(JUMP, L=20, T=3.0, dt=0.01)
+    _, gpu = compare(text, ["out.txt", "outl.txt"], [1], "jump")
+    L = np.stack([g[1][:, 1] for g in gpu]).mean(0)
+    assert np.all(np.stack([g[0][:, 1] for g in gpu]) == 2000)  # nothing lost at the ends
+    assert L[-1] < 1900  # molecules crossed the left end into the right half
