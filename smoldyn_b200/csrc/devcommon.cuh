@@ -156,6 +156,7 @@ struct DevNet {
   uint8_t bb_rxn[kMaxRxn], bb_sp[kMaxRxn][2], bb_st[kMaxRxn][2], bb_pst[kMaxRxn];
   uint32_t bb_mask[kMaxSpecies][2];
   float bb_rmax;
+  double bb_inv_cs;  // 1 / cell side of the bound-bound grid (the largest binding radius)
 };
 
 // A molecule bound to a panel: absolute position (relative to the system's

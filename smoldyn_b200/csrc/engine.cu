@@ -104,7 +104,7 @@ struct KParams {
   // entry of its bucket, its box, and its best partner (priority << 32 | index)
   int *bbhead;
   int *bbnext;
-  int *bbcell;
+  ull *bbcell;
   ull *bbbest;
 };
 
@@ -1791,7 +1791,20 @@ __global__ void __launch_bounds__(256) k_bpair_resolve(KParams p) {
 constexpr int kBBHashBits = 20;
 constexpr ull kBBReacted = ~0ull - 1;  // bbbest of a molecule that reacted this step
 
-__device__ __forceinline__ int bb_bucket(int cell) { return (int)(((uint32_t)cell * 2654435761u) >> (32 - kBBHashBits)); }
+__device__ __forceinline__ int bb_bucket(ull cell) { return (int)(mix64(cell) >> (64 - kBBHashBits)); }
+constexpr ull kBBNone = ~0ull;  // bbcell of a molecule not in the grid
+
+// Cell of the bound-bound grid: cubes of the largest binding radius of these
+// reactions (bound molecules crowd on surfaces, so the solution boxes would
+// hold far too many of them), coordinates offset to stay positive and packed
+// 21 bits each.
+__device__ __forceinline__ void bb_cell_coords(const double x[3], int c[3]) {
+  const double inv = c_net.bb_inv_cs;
+  for (int d = 0; d < 3; ++d) c[d] = (int)floor(x[d] * inv) + (1 << 20);
+}
+__device__ __forceinline__ ull bb_cell_key(const int c[3]) {
+  return ((ull)(c[0] & 0x1FFFFF)) | ((ull)(c[1] & 0x1FFFFF) << 21) | ((ull)(c[2] & 0x1FFFFF) << 42);
+}
 
 __device__ __forceinline__ bool bb_candidate(const KParams &p, int k, uint32_t step) {
   const BoundMol &m = p.bd_out[k];
@@ -1811,13 +1824,12 @@ __global__ void __launch_bounds__(256) k_bb_insert(KParams p) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nb; k += gridDim.x * blockDim.x) {
     p.bbbest[k] = ~0ull;
     if (!bb_candidate(p, k, step)) {
-      p.bbcell[k] = -1;
+      p.bbcell[k] = kBBNone;
       continue;
     }
-    int ix[3];
-    float u[3];
-    from_abs(c_geo0, p.bd_out[k].x, ix, u);
-    const int cell = (ix[2] * c_geo0.n[1] + ix[1]) * c_geo0.n[0] + ix[0];
+    int c[3];
+    bb_cell_coords(p.bd_out[k].x, c);
+    const ull cell = bb_cell_key(c);
     p.bbcell[k] = cell;
     p.bbnext[k] = atomicExch(&p.bbhead[bb_bucket(cell)], k);
   }
@@ -1830,31 +1842,20 @@ __global__ void __launch_bounds__(256) k_bb_best(KParams p) {
   const uint32_t step = *p.step;
   const DevGeo &g = c_geo0;
   const uint2 key = make_uint2(c_net.key0 ^ 0x2F8A6B1Du, c_net.key1 ^ 0x5C4E9A37u);
-  const float rmax = c_net.bb_rmax;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nb; k += gridDim.x * blockDim.x) {
-    if (p.bbcell[k] < 0 || p.bbbest[k] == kBBReacted) continue;
+    if (p.bbcell[k] == kBBNone || p.bbbest[k] == kBBReacted) continue;
     const BoundMol m = p.bd_out[k];
     const int sp = id_species(m.id);
     const uint32_t mask = c_net.bb_mask[sp][m.ms - 1];
     const ull kk = id_stream(m.id);
     int ix[3];
-    float u[3];
-    from_abs(g, m.x, ix, u);
+    bb_cell_coords(m.x, ix);
     ull best = ~0ull;
-    for (int q = 0; q < 27; ++q) {
+    for (int q = 0; q < 27; ++q) {  // cells are one binding radius wide: the 27 around cover every partner
       const int off[3] = {q % 3 - 1, (q / 3) % 3 - 1, q / 9 - 1};
-      int cc[3];
-      bool ok = true;
-      for (int d = 0; d < 3; ++d) {
-        if (d >= g.dim && off[d] != 0) ok = false;
-        const float ub = (ix[d] == g.n[d] - 1) ? g.whi[d] : g.h[d];
-        if (off[d] < 0 && !(u[d] < rmax)) ok = false;
-        if (off[d] > 0 && !(u[d] > ub - rmax)) ok = false;
-        cc[d] = ix[d] + off[d];
-        if (cc[d] < 0 || cc[d] >= g.n[d]) ok = false;  // bound molecules do not meet across periodic walls
-      }
-      if (!ok) continue;
-      const int cell = (cc[2] * g.n[1] + cc[1]) * g.n[0] + cc[0];
+      if ((g.dim < 3 && off[2] != 0) || (g.dim < 2 && off[1] != 0)) continue;
+      const int cc[3] = {ix[0] + off[0], ix[1] + off[1], ix[2] + off[2]};
+      const ull cell = bb_cell_key(cc);
       for (int j = p.bbhead[bb_bucket(cell)]; j >= 0; j = p.bbnext[j]) {
         if (j == k || p.bbcell[j] != cell || p.bbbest[j] == kBBReacted) continue;
         const BoundMol mj = p.bd_out[j];
@@ -1903,7 +1904,7 @@ __global__ void __launch_bounds__(256) k_bb_resolve(KParams p) {
   const uint32_t step = *p.step;
   int done = 0;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nb; k += gridDim.x * blockDim.x) {
-    if (p.bbcell[k] < 0) continue;
+    if (p.bbcell[k] == kBBNone) continue;
     const ull bk = p.bbbest[k];
     if (bk == ~0ull || bk == kBBReacted) continue;
     const int j = (int)(uint32_t)bk;
@@ -2004,7 +2005,7 @@ __global__ void __launch_bounds__(256) k_bb_clear(KParams p) {
   pdl_wait();
   const int nb = min(*p.bd_out_n, p.bcap);
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nb; k += gridDim.x * blockDim.x)
-    if (p.bbcell[k] >= 0) p.bbhead[bb_bucket(p.bbcell[k])] = -1;
+    if (p.bbcell[k] != kBBNone) p.bbhead[bb_bucket(p.bbcell[k])] = -1;
 }
 
 // Scatter pass: a pure permutation of the moved molecules into box order.
@@ -3914,8 +3915,8 @@ class EngineImpl {
   long long bcap = 0;
   ull *d_bclaim = nullptr;  // bound-solution pair reactions: claim word per sorted molecule
   int4 *d_bcand = nullptr;  // and candidate per bound molecule
-  int *d_bbhead = nullptr, *d_bbnext = nullptr, *d_bbcell = nullptr;  // bound-bound reactions: hash grid
-  ull *d_bbbest = nullptr;
+  int *d_bbhead = nullptr, *d_bbnext = nullptr;  // bound-bound reactions: hash grid
+  ull *d_bbcell = nullptr, *d_bbbest = nullptr;
   SrfRule *d_srfrule = nullptr;
 
   // persistent ensemble engine (k_persist): its own molecule layout, one
@@ -4055,8 +4056,8 @@ class EngineImpl {
     d_bd[0] = d_bd[1] = nullptr;
     d_bclaim = nullptr;
     d_bcand = nullptr;
-    d_bbhead = d_bbnext = d_bbcell = nullptr;
-    d_bbbest = nullptr;
+    d_bbhead = d_bbnext = nullptr;
+    d_bbcell = d_bbbest = nullptr;
     d_srfrule = nullptr;
     bcap = 0;
     d_rsearch = nullptr;
@@ -4556,6 +4557,7 @@ class EngineImpl {
     dnet.difm_any = difm_any;
     dnet.bpair_rmax = bpair_rmax;
     dnet.bb_rmax = bb_rmax;
+    dnet.bb_inv_cs = bb_rmax > 0 ? 1.0 / (double)bb_rmax : 1.0;
     auto put = [&](void **dst, const void *src, size_t bytes) -> int {
       if (!*dst) CK(cudaMalloc(dst, bytes));
       CK(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, stream));
@@ -5178,7 +5180,7 @@ int Engine::init(const NetSpec &net, const std::vector<RepSpec> &reps, double dt
       CK(cudaMalloc(&E.d_bbhead, ((size_t)1 << kBBHashBits) * sizeof(int)));
       CK(cudaMemsetAsync(E.d_bbhead, 0xFF, ((size_t)1 << kBBHashBits) * sizeof(int), E.stream));
       CK(cudaMalloc(&E.d_bbnext, E.bcap * sizeof(int)));
-      CK(cudaMalloc(&E.d_bbcell, E.bcap * sizeof(int)));
+      CK(cudaMalloc(&E.d_bbcell, E.bcap * sizeof(ull)));
       CK(cudaMalloc(&E.d_bbbest, E.bcap * sizeof(ull)));
     }
     CK(cudaMalloc(&E.d_srfrule, nrule * sizeof(SrfRule)));
