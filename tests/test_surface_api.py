@@ -9,6 +9,7 @@ surface-bound molecules (smolgpuGetSurfaceMolecules) must sit on their panel
 on the requested side.  Second-order reactions of a bound and a solution
 reactant: binding radii and effective rates against the values the
 reference binary prints for the same configurations (golden fixture).
+Jump statements parse and their malformed forms are refused.
 Error paths: an unknown panel, a state the engine does not build, bound
 reactants with more products than built,
 solution reactants with bound products, and bound-reactant reactions with a
@@ -223,3 +224,41 @@ def test_births_on_a_surface_parse():
         f.write(TEXT.replace("end_file", "reaction b0 0 -> A(front) 0.5\nend_file"))
     with pytest.raises(RuntimeError):
         sb.Sim.load_file(os.path.join(d, "c.txt"))
+
+
+def test_jump_statements_parse_and_refuse():
+    """jump panel1 face1 -> / <-> panel2 face2 (smolsurface.c:3574-3600): panels
+    of one surface with the same shape, faces front or back; the jump action
+    applies to solution molecules."""
+    base = """dim 3
+species A
+difc A 1
+time_step 0.01
+boundaries 0 0 10
+boundaries 1 0 10
+boundaries 2 0 10
+start_surface ends
+action both all jump
+panel rect +0 0 0 0 10 10 left
+panel rect -0 10 0 0 10 10 right
+panel sph 5 5 5 1 10 10 ball
+%s
+end_surface
+end_file
+"""
+    d = tempfile.mkdtemp()
+    path = os.path.join(d, "c.txt")
+    with open(path, "w") as f:
+        f.write(base % "jump left front <-> right front")
+    sb.Sim.load_file(path).close()
+    for stmt in ("jump left front <-> nope front", "jump left front <-> ball front", "jump left up -> right front",
+                 "jump left front => right front", "jump left front -> left back"):
+        with open(path, "w") as f:
+            f.write(base % stmt)
+        with pytest.raises(RuntimeError):
+            sb.Sim.load_file(path)
+    with open(path, "w") as f:
+        f.write((base % "jump left front <-> right front").replace("action both all jump",
+                                                                   "action both A(front) jump"))
+    with pytest.raises(RuntimeError):
+        sb.Sim.load_file(path)
